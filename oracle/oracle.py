@@ -1,0 +1,248 @@
+"""CPU oracle of the low-order frequency-domain BEM path -- TEST INFRASTRUCTURE ONLY.
+
+This module is the checker: only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import it, and never as the thing measured or shipped.  It drives the plain-C FP64
+restatement ``libhb_oracle.so`` (``hb_oracle.c``) of HydroBEM's diagnostic double-precision path
+and adds, in numpy, the steps that are short formulas of ``crates/hydrobem/src/``:
+
+- incident wave and boundary values  ``low_order.rs:1397-1485``, ``lo_frequency.rs:214-273``
+- right-hand sides -S u and the dense solve  ``lo_frequency.rs:823-955`` (LU with partial pivoting:
+  LAPACK ``zgesv`` through numpy, standing in for faer's blocked LU, ``linalg.rs:134-252``)
+- pressure integration A, B, X, FK, SC  ``lo_frequency.rs:1039-1115``
+
+Parity: pinned against the reference's golden kernel files (``tests/data/green_inf_reference.txt``,
+``green_fin_reference.txt``, ``panel_reference.txt``, ``dispersion_reference.txt``) and against the
+reference's own solver outputs (``tests/data/regression/lo_cylinder_drift.npz``) -- see
+``tests/test_oracle_golden.py``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "libhb_oracle.so"
+TABLES = HERE.parent / "hydrobem_b200" / "tables" / "green_tables.bin"
+GRAVITY = 9.80665
+DENSITY = 1000.0
+WET, INTERIOR = 0, 1
+
+
+class Panel(ctypes.Structure):
+    _fields_ = [
+        ("nv", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
+        ("v", ctypes.c_double * 12),
+        ("c", ctypes.c_double * 3),
+        ("n", ctypes.c_double * 3),
+        ("area", ctypes.c_double),
+        ("radius", ctypes.c_double),
+        ("elen", ctypes.c_double * 4),
+        ("em", ctypes.c_double * 12),
+        ("gx", ctypes.c_double * 27),
+        ("gw", ctypes.c_double * 9),
+    ]
+
+
+_lib = None
+
+
+def build() -> None:
+    """Compile the oracle library (make in this directory)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB.exists():
+        build()
+    L = ctypes.CDLL(str(LIB))
+    dp = ctypes.POINTER(ctypes.c_double)
+    ip = ctypes.POINTER(ctypes.c_int32)
+    pp = ctypes.POINTER(Panel)
+    L.hbo_load_tables.argtypes = [ctypes.c_char_p]
+    L.hbo_make_panels_kinds.argtypes = [ctypes.c_int, dp, ip, pp]
+    L.hbo_wave_kernel.argtypes = [ctypes.c_double, ctypes.c_double, dp]
+    L.hbo_dispersion_x0.argtypes = [ctypes.c_double]
+    L.hbo_dispersion_x0.restype = ctypes.c_double
+    L.hbo_dispersion_xn.argtypes = [ctypes.c_double, ctypes.c_int]
+    L.hbo_dispersion_xn.restype = ctypes.c_double
+    L.hbo_finite_kernel.argtypes = [ctypes.c_double] * 2 + [ctypes.c_int] + [ctypes.c_double] * 3 + [dp]
+    L.hbo_rankine.argtypes = [pp, dp, dp]
+    L.hbo_log_singularity.argtypes = [pp, dp, dp]
+    L.hbo_log_in_plane.argtypes = [pp, dp]
+    L.hbo_log_in_plane.restype = ctypes.c_double
+    L.hbo_statics.argtypes = [ctypes.c_int, pp, ip, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp]
+    L.hbo_assemble.argtypes = [ctypes.c_int, pp, ip, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_int, dp, dp]
+    L.hbo_wavenumber.argtypes = [ctypes.c_double] * 3
+    L.hbo_wavenumber.restype = ctypes.c_double
+    rc = L.hbo_load_tables(str(TABLES).encode())
+    if rc != 0:
+        raise RuntimeError(f"oracle: cannot load the Green-function tables {TABLES} (code {rc})")
+    _lib = L
+    return L
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _ip(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+# ------------------------------------------------------------------ kernels (golden-vector tests)
+def wave_kernel(X: float, Y: float) -> np.ndarray:
+    out = np.zeros(7)
+    lib().hbo_wave_kernel(X, Y, _dp(out))
+    return out
+
+
+def finite_kernel(h, K, mode, R, z, zeta) -> np.ndarray:
+    out = np.zeros(8)
+    lib().hbo_finite_kernel(h, K, mode, R, z, zeta, _dp(out))
+    return out
+
+
+def dispersion_x0(H):
+    return lib().hbo_dispersion_x0(H)
+
+
+def dispersion_xn(H, n):
+    return lib().hbo_dispersion_xn(H, n)
+
+
+# ------------------------------------------------------------------ panels and statics
+def make_panels(verts: np.ndarray, kinds=None):
+    v = np.ascontiguousarray(verts, dtype=np.float64).reshape(-1, 12)
+    n = v.shape[0]
+    k = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
+    arr = (Panel * n)()
+    rc = lib().hbo_make_panels_kinds(n, _dp(v), None if k is None else _ip(k), arr)
+    if rc != 0:
+        raise ValueError(f"invalid panel {rc - 1}")
+    return arr
+
+
+def panel_arrays(panels):
+    """Centroid, normal and area of every panel as numpy arrays."""
+    c = np.array([list(p.c) for p in panels])
+    n = np.array([list(p.n) for p in panels])
+    a = np.array([p.area for p in panels])
+    return c, n, a
+
+
+def rankine(panel, x):
+    out = np.zeros(2)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    lib().hbo_rankine(ctypes.byref(panel), _dp(xx), _dp(out))
+    return out
+
+
+def log_singularity(panel, image):
+    out = np.zeros(2)
+    xx = np.ascontiguousarray(image, dtype=np.float64)
+    lib().hbo_log_singularity(ctypes.byref(panel), _dp(xx), _dp(out))
+    return out
+
+
+def statics(panels, kinds, depth, logint=True, tol=1e-4) -> np.ndarray:
+    n = len(panels)
+    out = np.zeros((n, n, 4))
+    k = np.zeros(n, np.int32) if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
+    d = depth if (depth is not None and np.isfinite(depth) and depth > 0) else np.inf
+    lib().hbo_statics(n, panels, _ip(k), d, int(logint), tol, _dp(out))
+    return out
+
+
+def assemble(panels, kinds, st, depth, omega, grav=GRAVITY, logint=True):
+    """(S, A) complex128 N x N (entry [k, n]) of one ordinary frequency."""
+    n = len(panels)
+    S = np.zeros((n, n), dtype=np.complex128, order="F")
+    A = np.zeros((n, n), dtype=np.complex128, order="F")
+    k = np.zeros(n, np.int32) if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
+    d = depth if (depth is not None and np.isfinite(depth) and depth > 0) else np.inf
+    lib().hbo_assemble(n, panels, _ip(k), _dp(st), d, omega, grav, int(logint),
+                       S.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                       A.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return S, A
+
+
+# ------------------------------------------------------------------ one frequency
+def incident(c, depth, k, omega, beta, grav=GRAVITY):
+    """(phi_I, grad phi_I) at the points c (low_order.rs:1441-1459, frame at the origin, yaw 0)."""
+    cb, sb = np.cos(beta), np.sin(beta)
+    phase = -k * (c[:, 0] * cb + c[:, 1] * sb)
+    Z = np.exp(k * c[:, 2])
+    Zz = k * Z
+    if depth is not None and np.isfinite(depth) and depth > 0:
+        b = np.exp(-k * (c[:, 2] + 2.0 * depth))
+        dd = 1.0 + np.exp(-2.0 * k * depth)
+        Zz = k * (Z - b) / dd
+        Z = (Z + b) / dd
+    e = (1j * grav / omega) * (np.cos(phase) + 1j * np.sin(phase))
+    phi = e * Z
+    grad = np.stack([phi * (-1j * k * cb), phi * (-1j * k * sb), e * Zz], axis=1)
+    return phi, grad
+
+
+def rigid_normals(c, n, kinds):
+    """n_j = (n, c x n) about the origin; 0 off the wetted surface (lo_geometry.rs:805-811)."""
+    nj = np.concatenate([n, np.cross(c, n)], axis=1)
+    if kinds is not None:
+        nj[np.asarray(kinds) != WET] = 0.0
+    return nj
+
+
+def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY, rho=DENSITY, logint=True,
+                    want_matrices=False):
+    """A, B [6][6], X, FK, SC [H][6] of one frequency, all in float64 (complex128)."""
+    c, n, area = panel_arrays(panels)
+    N = len(panels)
+    S, A = assemble(panels, kinds, st, depth, omega, grav, logint)
+    k = lib().hbo_wavenumber(omega, depth if depth else np.inf, grav)
+    wet = np.ones(N, bool) if kinds is None else (np.asarray(kinds) == WET)
+    nj = rigid_normals(c, n, kinds)
+    H = len(headings_rad)
+    u = np.zeros((N, 6 + H), dtype=np.complex128)
+    u[:, :6] = nj
+    phiI = np.zeros((H, N), dtype=np.complex128)
+    for h, beta in enumerate(headings_rad):
+        pI, gr = incident(c, depth, k, omega, beta, grav)
+        phiI[h] = pI
+        d = (gr * n).sum(axis=1)
+        u[:, 6 + h] = np.where(wet, -d, 0.0)
+    rhs = S @ (-u)
+    phi = np.linalg.solve(A, rhs)
+    w = (nj * area[:, None]) * wet[:, None]          # n_i A_j on the body panels
+    z = -rho * (w.T @ phi[:, :6])                    # [i][c]
+    out = {"A": z.real, "B": -omega * z.imag}
+    if H:
+        x = w.T @ (phi[:, 6:] + phiI.T)              # [i][h]
+        fk = w.T @ phiI.T
+        iwr = 1j * omega * rho
+        out["X"] = (iwr * x).T
+        out["FK"] = (iwr * fk).T
+        out["SC"] = (iwr * (x - fk)).T
+    if want_matrices:
+        out["S"], out["Amat"], out["rhs"], out["phi"] = S, A, rhs, phi
+    return out
+
+
+def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GRAVITY, rho=DENSITY, logint=True,
+               tol=1e-4):
+    """The whole path for one body: statics once, then every frequency. Arrays [F][6][6], [F][H][6]."""
+    panels = make_panels(verts, kinds)
+    st = statics(panels, kinds, depth, logint, tol)
+    heads = np.radians(np.asarray(headings_deg, dtype=float))
+    res = [solve_frequency(panels, kinds, st, depth, w, heads, grav, rho, logint) for w in omegas]
+    out = {k: np.array([r[k] for r in res]) for k in res[0]}
+    return out
