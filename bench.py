@@ -1,0 +1,321 @@
+"""Benchmark of the low-order frequency-domain BEM hot path on B200.
+
+Workload (one step): the finite-depth cylinder of 4096 panels -- radius 1 m, draft 0.5 m, 64 x 32 side
+and 64 x 32 bottom panels, depth h = 5 m, 40 wave periods evenly spaced 1.5-20 s, 4 headings
+(0/30/60/90 deg) -- solved end to end: panel geometry and statics once, then for every frequency the
+assembly of S and A, the right-hand sides of 6 radiation + 4 diffraction problems, the LU and
+substitution, and the pressure integration to A, B, X.  Metric: frequency solves per second.
+Inputs are synthetic (the reference's procedural mesh of that shape); every matrix (537 MB FP64 per
+frequency) is larger than the 126 MB L2, so no L2 flush is needed between steps.
+
+Arms:
+  (default)         this library, through its C ABI (hbg_solve_batch), precision --precision
+  --impl reference  the CPU restatement of the reference's path (oracle/, C + LAPACK) on the host
+                    cores, timed on a bounded sample of the same workload (statics + a few
+                    frequencies), scaled to the whole job.
+
+Multi-GPU (torchrun): every rank solves its own copy of the job on its own GPU (independent
+(body, frequency) units, no collective on the data path: weak scaling); the step time is the max
+over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_PERIODS = 40
+HEADINGS = [0.0, 30.0, 60.0, 90.0]
+DEPTH = 5.0
+WORKLOAD = "cylinder r=1 m d=0.5 m, 4096 panels (64x32 side + 64x32 bottom), h=5 m, 40 periods 1.5-20 s, 4 headings"
+
+
+CASE = "c2"
+
+
+def workload():
+    """The benchmark body and frequencies; --case small is a 2048-panel, 4-frequency cut of the same
+    family for profiler captures (each matrix 67 MB, the batch still larger than L2)."""
+    from hydrobem_b200 import meshes
+
+    if CASE == "small":
+        return meshes.cylinder(1.0, 0.5, 32, 16, 16), 2.0 * math.pi / np.linspace(1.5, 20.0, 4)
+    v = meshes.cylinder(1.0, 0.5, 64, 32, 32)
+    periods = np.linspace(1.5, 20.0, N_PERIODS)
+    return v, 2.0 * math.pi / periods
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def cpu_reference(args, world, rank, pg):
+    """The reference's CPU path (the oracle restatement: C + LAPACK) on the host cores."""
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+
+    v, omegas = workload()
+    heads = np.radians(HEADINGS)
+    cores = os.cpu_count()
+    O.lib()
+    sample_f = 2
+
+    def one_step():
+        t0 = time.perf_counter()
+        pan = O.make_panels(v)
+        st = O.statics(pan, None, DEPTH)
+        t1 = time.perf_counter()
+        for w in omegas[:: max(1, len(omegas) // sample_f)][:sample_f]:
+            O.solve_frequency(pan, None, st, DEPTH, w, heads)
+        t2 = time.perf_counter()
+        per_freq = (t2 - t1) / sample_f
+        return (t1 - t0) + len(omegas) * per_freq, t1 - t0, per_freq
+
+    for _ in range(min(args.warmup, 1)):
+        one_step()
+    times = [one_step() for _ in range(args.steps)]
+    job = float(np.mean([t[0] for t in times]))
+    value = len(omegas) / job
+    sample = (f"statics + {sample_f} of the {len(omegas)} frequencies per step, job time = statics + 40 x the "
+              f"mean per-frequency time (statics {np.mean([t[1] for t in times]):.2f} s, "
+              f"{np.mean([t[2] for t in times]):.2f} s per frequency)")
+    line = {"metric": "freq solves/s at N=4096", "value": value, "unit": "freq solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": job * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "form": "FP64 (the reference's diagnostic double path)",
+                       "l2": "inputs larger than L2"},
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "freq solves/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "freq solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    return line
+
+
+def ours(args, world, rank, local, pg):
+    import torch
+
+    from hydrobem_b200 import native as nv
+
+    device = local if torch.cuda.is_available() else 0
+    torch.cuda.set_device(device)
+    v, omegas = workload()
+    precision = nv.HBG_MIXED if args.precision == "mixed" else nv.HBG_FP64
+    body = nv.Body(v, omegas, HEADINGS)
+    arr = (nv.HbgProblem * 1)(body.problem())
+    opt = nv.default_options(precision=precision, depth=DEPTH, device=device)
+    import ctypes
+
+    L = nv.lib()
+
+    def step():
+        nv.check(L.hbg_solve_batch(arr, 1, ctypes.byref(opt)))
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    # timed region: K steps bracketed by barrier + synchronize; device time by CUDA events
+    nv.profile_kernels(False)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    dev_ms = []
+    with Clocks(device) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            step()
+            dev_ms.append(nv.last_profile()["total"])
+        e1.record()
+        torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    step_ms = float(np.mean(dev_ms))
+    if pg is not None:
+        t = torch.tensor([step_ms, e2e_ms], device=f"cuda:{device}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        step_ms, e2e_ms = float(t[0]), float(t[1])
+    launches = nv.last_launch_count()
+    # one more step with kernel-family timing for the roofline (outside the timed region)
+    nv.profile_kernels(True)
+    step()
+    prof = nv.kernel_profile()
+    nv.profile_kernels(False)
+    phases = nv.last_profile()
+    if rank != 0:
+        return None
+    F = len(omegas)
+    value = world * F / (step_ms * 1e-3)
+    e2e = world * F / (e2e_ms * 1e-3)
+    peaks, peak_kind = measured_peaks()
+    fam, (ms, n, work) = max(prof.items(), key=lambda kv: kv[1][0])
+    flops = fam in nv.FLOP_FAMILIES
+    achieved = work / (ms * 1e-3) / (1e12 if flops else 1e9) if ms > 0 else None
+    if flops:
+        if fam == "mixed_gemm":
+            peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
+            pk = f"bf16 dense sustained ({peak_kind})"
+        else:
+            peak = args.fp64_peak
+            pk = "fp64 (datasheet 40 TFLOP/s; no measured FP64 peak on this pool)"
+        bound, unit = "tensor", "TFLOP/s"
+    else:
+        peak, bound, unit, pk = peaks["hbm_gbs"], "hbm", "GB/s", f"hbm copy ({peak_kind})"
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(f"{args.precision}:{fam}")
+    clocks = clk.summary()
+    line = {"metric": "freq solves/s at N=4096", "value": value, "unit": "freq solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == nv.HBG_FP64 else "c64+tf32/bf16",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "form": args.precision, "l2": "inputs larger than L2 (no flush)",
+                       "parallelism": f"replicas x{world}"},
+            "e2e": {"value": e2e, "unit": "freq solves/s", "h2d_bytes_per_step": int(v.nbytes + omegas.nbytes + 32),
+                    "d2h_bytes_per_step": int(F * (72 + 3 * len(HEADINGS) * 12) * 8)},
+            "gpu_launches": int(launches) * args.steps,
+            "roofline": {"bound": bound, "kernel": fam, "achieved": achieved, "peak": peak, "unit": unit,
+                         "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
+                         "peak_kind": pk, "launches": n, "ms": ms},
+            "phases_ms": {k: round(x, 3) for k, x in phases.items()},
+            "kernels_ms": {k: round(x[0], 3) for k, x in prof.items() if x[1]},
+            "clocks": clocks}
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_quick()
+    return line
+
+
+def cpu_baseline_quick():
+    """The oracle on a bounded sample of the same workload (statics + 2 frequencies), scaled."""
+    from oracle import oracle as O
+
+    v, omegas = workload()
+    heads = np.radians(HEADINGS)
+    t0 = time.perf_counter()
+    pan = O.make_panels(v)
+    st = O.statics(pan, None, DEPTH)
+    t1 = time.perf_counter()
+    for w in (omegas[0], omegas[len(omegas) // 2]):
+        O.solve_frequency(pan, None, st, DEPTH, w, heads)
+    t2 = time.perf_counter()
+    per = (t2 - t1) / 2
+    job = (t1 - t0) + len(omegas) * per
+    return {"value": len(omegas) / job, "unit": "freq solves/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"statics ({t1 - t0:.2f} s) + 2 of 40 frequencies ({per:.2f} s each), scaled to the job"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--fp64-peak", type=float, default=40.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", default="c2", choices=["c2", "small"])
+    args = ap.parse_args()
+    global CASE
+    CASE = args.case
+    world, rank, local, pg = dist_setup()
+    try:
+        if args.impl == "reference":
+            line = cpu_reference(args, world, rank, pg)
+        else:
+            line = ours(args, world, rank, local, pg)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,742 @@
+// hbg_api.cu -- host orchestration and the C ABI of libhydrobem_gpu.so.
+//
+// The solve of one body: panel geometry and the static influence data once (device), then the
+// frequencies in batches sized to the free device memory: per batch the finite-depth tiles, the
+// assembly of S and A, boundary values, right-hand sides, LU, substitution and forces, all on one
+// stream, results copied back once per batch.  The host only computes per-frequency scalars
+// (dispersion roots and the finite-depth power table, solve_common.rs:44-71) and checks statuses.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/hydrobem_gpu.h"
+#include "hbg_internal.h"
+#include "hbg_mixed.h"
+
+extern "C" const unsigned char hbg_tables_blob[];
+extern "C" const unsigned char hbg_tables_blob_end[];
+
+namespace hbg {
+
+// ------------------------------------------------------------------ errors (per thread)
+static thread_local std::string g_error;
+static thread_local HbLocation g_location = {-1, -1, -1, -1, -1, -1};
+static thread_local double g_profile[6];
+static thread_local int64_t g_launches;
+
+static thread_local KernelProfiler* g_prof = nullptr;
+KernelProfiler& profiler() {
+    if (!g_prof) g_prof = new KernelProfiler();
+    return *g_prof;
+}
+
+struct Failure {
+    HbStatus code;
+    std::string msg;
+    int64_t body = -1, frequency = -1;
+};
+
+static HbStatus fail(const Failure& f) {
+    g_error = f.msg;
+    g_location = HbLocation{f.body, -1, -1, -1, -1, f.frequency};
+    return f.code;
+}
+
+#define CUDA_OK(expr)                                                                                   \
+    do {                                                                                                \
+        cudaError_t _e = (expr);                                                                        \
+        if (_e != cudaSuccess) throw Failure{HB_ERR_INTERNAL, std::string("CUDA: ") + cudaGetErrorString(_e)}; \
+    } while (0)
+
+// ------------------------------------------------------------------ tables
+struct HostTables {
+    const double* arr[8] = {};
+    size_t len[8] = {};
+    bool ok = false;
+    std::string why;
+};
+
+static uint64_t fnv1a(const double* v, size_t n, uint64_t h) {
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(v);
+    for (size_t i = 0; i < n * 8; i++) {
+        h ^= b[i];
+        h *= 0x100000001B3ull;
+    }
+    return h;
+}
+
+// The embedded blob (tables/green_tables.bin): header, then eight float64 arrays; the checksums of
+// the reference (green_inf.rs:268-283, green_fin.rs:853-868).
+static const HostTables& host_tables() {
+    static HostTables t;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const unsigned char* p = hbg_tables_blob;
+        size_t size = (size_t)(hbg_tables_blob_end - hbg_tables_blob);
+        if (size < 16 || memcmp(p, "HBGTBL01", 8) != 0) {
+            t.why = "Green-function tables: bad header";
+            return;
+        }
+        uint64_t cnt;
+        memcpy(&cnt, p + 8, 8);
+        if (cnt != 8) {
+            t.why = "Green-function tables: unexpected array count";
+            return;
+        }
+        static const size_t want[8] = {2040, 115200, 176400, 56, 65, 24570, 130, 1728};
+        size_t off = 16 + 8 * 24;
+        for (int i = 0; i < 8; i++) {
+            uint64_t n;
+            memcpy(&n, p + 16 + i * 24 + 16, 8);
+            if (n != want[i]) {
+                t.why = "Green-function tables: unexpected array length";
+                return;
+            }
+            t.arr[i] = reinterpret_cast<const double*>(p + off);
+            t.len[i] = n;
+            off += n * 8;
+        }
+        if (off != size) {
+            t.why = "Green-function tables: size mismatch";
+            return;
+        }
+        uint64_t hi = 0xCBF29CE484222325ull, hf = 0xCBF29CE484222325ull;
+        for (int i = 0; i < 4; i++) hi = fnv1a(t.arr[i], t.len[i], hi);
+        for (int i = 4; i < 8; i++) hf = fnv1a(t.arr[i], t.len[i], hf);
+        if (hi != 0xCAC816A5E6E5C8F2ull || hf != 0x4982F563A8976372ull) {
+            t.why = "Green-function tables fail their checksum";
+            return;
+        }
+        t.ok = true;
+    });
+    return t;
+}
+
+// Gauss-Legendre nodes and weights of orders 1..16 (quadrature.rs:17-62: Newton on P_n)
+static void gauss_legendre(int n, double* x, double* w) {
+    double nf = n;
+    for (int i = 0; i < (n + 1) / 2; i++) {
+        double z = std::cos(PI * (i + 0.75) / (nf + 0.5)), dp = 1.0;
+        for (int it = 0; it < 100; it++) {
+            double p0 = 1.0, p1 = z;
+            for (int k = 2; k <= n; k++) {
+                double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = nf * (z * p1 - p0) / (z * z - 1.0);
+            double dz = p1 / dp;
+            z -= dz;
+            if (std::fabs(dz) <= 1e-16) break;
+        }
+        double p0 = 1.0, p1 = z;
+        for (int k = 2; k <= n; k++) {
+            double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+            p0 = p1;
+            p1 = p2;
+        }
+        dp = nf * (z * p1 - p0) / (z * z - 1.0);
+        x[i] = -z;
+        x[n - 1 - i] = z;
+        double wi = 2.0 / ((1.0 - z * z) * dp * dp);
+        w[i] = wi;
+        w[n - 1 - i] = wi;
+    }
+    if (n % 2 == 1) x[n / 2] = 0.0;
+}
+
+struct DeviceCtx {
+    bool ready = false;
+    double* tables = nullptr;
+    Tables tab{};
+};
+
+static std::mutex g_dev_mutex;
+static DeviceCtx g_dev[16];
+
+static DeviceCtx& device_ctx(int dev) {
+    std::lock_guard<std::mutex> lock(g_dev_mutex);
+    if (dev < 0 || dev >= 16) throw Failure{HB_ERR_ARGUMENT, "device ordinal out of range"};
+    DeviceCtx& d = g_dev[dev];
+    if (d.ready) return d;
+    const HostTables& ht = host_tables();
+    if (!ht.ok) throw Failure{HB_ERR_INTERNAL, ht.why};
+    // every array at a 256-byte boundary (the kernels read the tables as double2)
+    auto padded = [](size_t n) { return (n + 31) / 32 * 32; };
+    size_t total = 0;
+    for (int i = 0; i < 8; i++) total += padded(ht.len[i]);
+    CUDA_OK(cudaMalloc(&d.tables, total * sizeof(double)));
+    size_t off = 0;
+    const double* dp[8];
+    for (int i = 0; i < 8; i++) {
+        CUDA_OK(cudaMemcpy(d.tables + off, ht.arr[i], ht.len[i] * sizeof(double), cudaMemcpyHostToDevice));
+        dp[i] = d.tables + off;
+        off += padded(ht.len[i]);
+    }
+    d.tab = Tables{dp[0], dp[1], dp[2], dp[3], dp[4], dp[5], dp[6], dp[7]};
+    static double glx[17][16], glw[17][16];
+    memset(glx, 0, sizeof glx);
+    memset(glw, 0, sizeof glw);
+    for (int n = 1; n <= 16; n++) gauss_legendre(n, glx[n], glw[n]);
+    set_constants(glx, glw, d.tab);
+    CUDA_OK(cudaGetLastError());
+    d.ready = true;
+    return d;
+}
+
+// ------------------------------------------------------------------ finite-depth scalars (host)
+// dispersion.rs:19-95
+static double dispersion_x0(double H) {
+    if (!(H > 0.0)) return 0.0;
+    if (H >= 40.0) return H;
+    double lo = std::max(H, std::sqrt(H)), hi = 0.5 * (H + std::sqrt(H * H + 4.0 * H));
+    double x = H < 1.0 ? std::sqrt(H) * (1.0 + H / 6.0) : H;
+    x = std::min(std::max(x, lo), hi);
+    double prev = -1.0;
+    for (int it = 0; it < 200; it++) {
+        double t = std::tanh(x), f = x * t - H;
+        if (f < 0.0) lo = x;
+        else hi = x;
+        double fp = t + x * (1.0 - t * t);
+        double xn = x - f / fp;
+        if (!(xn >= lo && xn <= hi)) xn = 0.5 * (lo + hi);
+        if (xn == x || xn == prev) break;
+        prev = x;
+        x = xn;
+    }
+    return x;
+}
+
+static double dispersion_xn(double H, int n) {
+    double npi = n * PI;
+    if (!(H > 0.0)) return npi;
+    if (std::isinf(H)) return npi - 0.5 * PI;
+    double lo = 0.0, hi = 0.5 * PI, d = std::atan(H / (npi - 0.25 * PI)), prev = -1.0;
+    for (int it = 0; it < 200; it++) {
+        double s = std::sin(d), c = std::cos(d);
+        double g = (npi - d) * s - H * c;
+        if (g < 0.0) lo = d;
+        else hi = d;
+        double gp = (npi - d) * c + (H - 1.0) * s;
+        double dn = d - g / gp;
+        if (!(dn > lo && dn < hi)) dn = 0.5 * (lo + hi);
+        if (dn == d || dn == prev) break;
+        prev = d;
+        d = dn;
+    }
+    return npi - d;
+}
+
+// green_fin.rs:345-392 region coefficients and power table, 874-934 make_finite_depth (ordinary)
+static void make_fd_params(double h, double K, FdParams& fd) {
+    const HostTables& ht = host_tables();
+    const double *meta = ht.arr[4], *Q = ht.arr[5], *L0 = ht.arr[6];
+    memset(&fd, 0, sizeof fd);
+    fd.mode = 0;
+    fd.h = h;
+    for (int p = 0; p < 6; p++) fd.sign[p] = 1.0;
+    fd.K = K;
+    fd.H = K * h;
+    double x0 = dispersion_x0(fd.H);
+    fd.k0 = x0 / h;
+    fd.A0 = 2.0 * PI * fd.k0 / (-std::expm1(-4.0 * x0) + 4.0 * x0 * std::exp(-2.0 * x0));
+    for (int n = 1; n <= FIN_ROOTS; n++) {
+        double k = dispersion_xn(fd.H, n) / h;
+        fd.kn[n - 1] = k;
+        fd.cn[n - 1] = 4.0 * (k * k + K * K) / (k * k * h + K * K * h - K);
+    }
+    double cw[(FM + 1) * NC];
+    auto region = [&](int r, double x) {
+        const double* m = meta + 5 * r;
+        double a = m[1], b = m[2];
+        int n = (int)m[3];
+        const double* c = Q + (size_t)m[4];
+        double y = 2.0 * (x - a) / (b - a) - 1.0, Tx[64];
+        Tx[0] = 1.0;
+        Tx[1] = y;
+        for (int j = 2; j <= n; j++) Tx[j] = 2.0 * y * Tx[j - 1] - Tx[j - 2];
+        for (int mm = 0; mm <= FM; mm++)
+            for (int jw = 0; jw < NC; jw++) {
+                double s = 0.0;
+                for (int jx = 0; jx <= n; jx++) s += c[(mm * (n + 1) + jx) * NC + jw] * Tx[jx];
+                cw[mm * NC + jw] = s;
+            }
+    };
+    if (fd.H < 1e-12) {
+        memcpy(cw, L0, sizeof cw);
+        cw[0] -= 0.5 * std::log(fd.H);
+    } else if (fd.H >= 50.0) {
+        region(REGIONS - 1, 1.0 / fd.H);
+    } else {
+        double tau = std::log(fd.H);
+        int r = 0;
+        while (r + 2 < REGIONS && tau > meta[5 * r + 2]) r++;
+        region(r, tau);
+    }
+    double a[NC][NC] = {};
+    a[0][0] = 1.0;
+    a[1][1] = 1.0;
+    for (int j = 2; j < NC; j++)
+        for (int k = 0; k < NC; k++) a[j][k] = (k > 0 ? 2.0 * a[j - 1][k - 1] : 0.0) - a[j - 2][k];
+    for (int m = 0; m <= FM; m++) {
+        const double* c = cw + m * NC;
+        double* p = fd.P + m * NC;
+        for (int k = 0; k < NC; k++) p[k] = c[0] * a[0][k] + c[1] * a[1][k];
+        for (int j = 2; j < NC; j++)
+            for (int k = 0; k < NC; k++) p[k] += c[j] * a[j][k];
+    }
+}
+
+// ------------------------------------------------------------------ device buffers
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    void alloc(size_t b) {
+        if (b <= bytes) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        CUDA_OK(cudaMalloc(&p, b));
+        bytes = b;
+    }
+    template <class T>
+    T* as() const {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
+struct EventTimer {
+    cudaEvent_t a{}, b{};
+    cudaStream_t s;
+    double* acc;
+    EventTimer(cudaStream_t st, double* target) : s(st), acc(target) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, s);
+    }
+    void stop() {
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        *acc += ms;
+    }
+    ~EventTimer() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+};
+
+static bool finite_depth(double d) { return std::isfinite(d) && d > 0.0; }
+
+// One body through the whole path; outputs to the caller's host arrays.
+static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t body_index, cudaStream_t s) {
+    const int64_t N64 = pr.body.n_panels;
+    if (N64 < 1 || N64 > 60000) throw Failure{HB_ERR_VALUE, "panel count outside 1..60000", body_index};
+    const int N = (int)N64;
+    const int F = (int)pr.n_omega, H = (int)pr.n_heading;
+    for (int i = 0; i < F; i++)
+        if (!(pr.omegas[i] > 0.0) || !std::isfinite(pr.omegas[i]))
+            throw Failure{HB_ERR_VALUE, "an omega is not positive and finite (the limits are not on this route)",
+                          body_index, i};
+    if (H > 26) throw Failure{HB_ERR_UNSUPPORTED, "more than 26 headings per solve", body_index};
+    const bool fin = finite_depth(opt.depth);
+    const double depth = fin ? opt.depth : 0.0;
+    if (fin && !(opt.depth > 0.0)) throw Failure{HB_ERR_VALUE, "depth must be positive", body_index};
+    if (fin) {
+        for (int64_t j = 0; j < N64 * 4; j++)
+            if (pr.body.vertices[3 * j + 2] < -opt.depth * (1.0 + 1e-12))
+                throw Failure{HB_ERR_VALUE, "a vertex lies below the sea bottom", body_index};
+    }
+    // ---- geometry and statics
+    DevBuf dverts, dkind, dplanes, dbad, dst, dwork, dnwork;
+    dverts.alloc(sizeof(double) * 12 * N);
+    dkind.alloc(sizeof(int32_t) * N);
+    dplanes.alloc(sizeof(double) * P_PLANES * N);
+    dbad.alloc(sizeof(int32_t));
+    CUDA_OK(cudaMemcpyAsync(dverts.p, pr.body.vertices, sizeof(double) * 12 * N, cudaMemcpyHostToDevice, s));
+    std::vector<int32_t> kinds(N, 0);
+    if (pr.body.kinds)
+        for (int j = 0; j < N; j++) {
+            int k = pr.body.kinds[j];
+            if (k != HBG_WET && k != HBG_INTERIOR) throw Failure{HB_ERR_UNSUPPORTED, "panel kind not on this route", body_index};
+            kinds[j] = k;
+        }
+    CUDA_OK(cudaMemcpyAsync(dkind.p, kinds.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
+    int32_t big = 0x7fffffff;
+    CUDA_OK(cudaMemcpyAsync(dbad.p, &big, sizeof big, cudaMemcpyHostToDevice, s));
+    double* prof = g_profile;
+    {
+        EventTimer t(s, &prof[0]);
+        KernelProfiler& P = profiler();
+        P.begin(s);
+        launch_panel_geometry(N, dverts.as<double>(), dkind.as<int32_t>(), dplanes.as<double>(), dbad.as<int32_t>(), s);
+        P.end(KF_GEOMETRY, 0.0, s);
+        g_launches++;
+        int32_t bad = 0;
+        CUDA_OK(cudaMemcpyAsync(&bad, dbad.p, sizeof bad, cudaMemcpyDeviceToHost, s));
+        CUDA_OK(cudaStreamSynchronize(s));
+        if (bad != big) {
+            Failure f{HB_ERR_VALUE, "invalid panel " + std::to_string(bad + 1) + " (degenerate, non-convex or non-finite)", body_index};
+            throw f;
+        }
+        PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
+        const size_t NN = (size_t)N * N;
+        dst.alloc(sizeof(double) * 4 * NN);
+        const int work_cap = std::max(1 << 16, 16 * N);
+        dwork.alloc(sizeof(int32_t) * 2 * work_cap);
+        dnwork.alloc(sizeof(int32_t));
+        CUDA_OK(cudaMemsetAsync(dnwork.p, 0, sizeof(int32_t), s));
+        P.begin(s);
+        launch_statics(pv, depth, opt.logarithmic, opt.log_tolerance, dst.as<double>(), dwork.as<int32_t>(),
+                       dnwork.as<int32_t>(), work_cap, s);
+        // algorithmic bytes: the four FP64 planes written
+        P.end(KF_STATICS, 32.0 * (double)NN, s);
+        int32_t nwork = 0;
+        CUDA_OK(cudaMemcpyAsync(&nwork, dnwork.p, sizeof nwork, cudaMemcpyDeviceToHost, s));
+        CUDA_OK(cudaStreamSynchronize(s));
+        if (nwork > work_cap) throw Failure{HB_ERR_INTERNAL, "adaptive log-integral worklist overflow", body_index};
+        P.begin(s);
+        launch_statics_adaptive(pv, dwork.as<int32_t>(), nwork, dst.as<double>(), s);
+        P.end(KF_STATICS_ADAPTIVE, 16.0 * nwork, s);
+        g_launches += 1 + (nwork > 0);
+        t.stop();
+        P.flush();
+    }
+    PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
+    if (F == 0) return;
+    const int nrhs = 6 + H;
+    if (opt.precision == HBG_MIXED) {
+        const char* msg = "";
+        int64_t fq = -1;
+        int rc = mixed_solve_frequencies(pv, dst.as<double>(), pr, opt, fin, depth, s, prof, &g_launches, &msg, &fq);
+        if (rc != 0) throw Failure{rc, msg, body_index, fq};
+        return;
+    }
+    // ---- frequency batches
+    const size_t NN = (size_t)N * N;
+    size_t per_freq = 2 * NN * sizeof(double2) + (size_t)(3 * nrhs + H) * N * sizeof(double2) +
+                      (size_t)N * sizeof(int32_t) + (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)FP_PLANES * N * 8 +
+                                                              (size_t)6912 * 3 * 8
+                                                        : 0);
+    size_t freeb = 0, totalb = 0;
+    CUDA_OK(cudaMemGetInfo(&freeb, &totalb));
+    int B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)freeb) / per_freq);
+    if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
+    B = std::min(B, F);
+    DevBuf dS, dA, du, drhs, dX, dphiI, dipiv, dinfo, dfi, dfd, dtiles, dscr, dfpt, dheads, dout;
+    dS.alloc(sizeof(double2) * NN * B);
+    dA.alloc(sizeof(double2) * NN * B);
+    du.alloc(sizeof(double2) * (size_t)nrhs * N * B);
+    drhs.alloc(sizeof(double2) * (size_t)nrhs * N * B);
+    dX.alloc(sizeof(double2) * (size_t)nrhs * N * B);
+    dphiI.alloc(sizeof(double2) * (size_t)std::max(H, 1) * N * B);
+    dipiv.alloc(sizeof(int32_t) * (size_t)N * B);
+    dinfo.alloc(sizeof(int32_t) * B);
+    dfi.alloc(sizeof(FreqInfo) * B);
+    dfd.alloc(sizeof(FdParams) * B);
+    if (fin) {
+        dtiles.alloc(sizeof(double) * (size_t)(T1_SIZE + T2_SIZE) * B);
+        dscr.alloc(sizeof(double) * (size_t)6912 * 3 * B);
+        dfpt.alloc(sizeof(double) * (size_t)FP_PLANES * N * B);
+    }
+    std::vector<double> heads(std::max(H, 1));
+    for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
+    dheads.alloc(sizeof(double) * heads.size());
+    CUDA_OK(cudaMemcpyAsync(dheads.p, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s));
+    // outputs per batch: A, B [6][6], X, FK, SC [H][6]
+    const size_t out_per = 72 * sizeof(double) + 3 * (size_t)H * 6 * sizeof(double2);
+    dout.alloc(out_per * B);
+    std::vector<unsigned char> hout(out_per * B);
+    std::vector<FreqInfo> fi(B);
+    std::vector<FdParams> fdh(B);
+    std::vector<int32_t> info(B);
+    for (int f0 = 0; f0 < F; f0 += B) {
+        if (opt.cancel && *opt.cancel) throw Failure{HB_ERR_CANCELLED, "the solve was cancelled", body_index, f0};
+        const int nb = std::min(B, F - f0);
+        for (int i = 0; i < nb; i++) {
+            double w = pr.omegas[f0 + i], K = w * w / opt.gravity;
+            fi[i].omega = w;
+            fi[i].K = K;
+            fi[i].k = fin ? dispersion_x0(K * depth) / depth : K;
+            fi[i].logc = opt.logarithmic ? 1.0 : 0.0;
+            if (fin) make_fd_params(depth, K, fdh[i]);
+        }
+        CUDA_OK(cudaMemcpyAsync(dfi.p, fi.data(), sizeof(FreqInfo) * nb, cudaMemcpyHostToDevice, s));
+        if (fin) {
+            CUDA_OK(cudaMemcpyAsync(dfd.p, fdh.data(), sizeof(FdParams) * nb, cudaMemcpyHostToDevice, s));
+        }
+        {
+            EventTimer t(s, &prof[1]);
+            KernelProfiler& P = profiler();
+            if (fin) {
+                P.begin(s);
+                launch_fd_tiles(nb, dfd.as<FdParams>(), dtiles.as<double>(), dscr.as<double>(), s);
+                launch_fin_points(pv, nb, dfd.as<FdParams>(), dfpt.as<double>(), s);
+                P.end(KF_FD_TILES, 0.0, s);
+                g_launches += 3;
+            }
+            P.begin(s);
+            launch_assemble_f64(pv, dst.as<double>(), nb, dfi.as<FreqInfo>(), dfd.as<FdParams>(), dtiles.as<double>(),
+                                dfpt.as<double>(), fin, dS.as<double2>(), dA.as<double2>(), NN, s);
+            // algorithmic bytes per pair: 4 statics read (32 B), S and A written (32 B)
+            P.end(KF_ASSEMBLE, 64.0 * (double)NN * nb, s);
+            P.begin(s);
+            launch_boundary(pv, nb, dfi.as<FreqInfo>(), H, dheads.as<double>(), depth, opt.gravity, du.as<double2>(),
+                            dphiI.as<double2>(), s);
+            P.end(KF_BOUNDARY, 0.0, s);
+            P.begin(s);
+            launch_rhs_f64(N, nb, nrhs, dS.as<double2>(), NN, du.as<double2>(), drhs.as<double2>(), s);
+            // S read once (16 B per entry)
+            P.end(KF_RHS, 16.0 * (double)NN * nb, s);
+            g_launches += 3;
+            t.stop();
+        }
+        {
+            EventTimer t(s, &prof[2]);
+            lu_factor_f64(N, nb, dA.as<double2>(), NN, dipiv.as<int32_t>(), dinfo.as<int32_t>(), s, &g_launches);
+            t.stop();
+        }
+        {
+            EventTimer t(s, &prof[3]);
+            KernelProfiler& P = profiler();
+            P.begin(s);
+            if (lu_solve_f64(N, nb, dA.as<double2>(), NN, dipiv.as<int32_t>(), nrhs, drhs.as<double2>(),
+                             dX.as<double2>(), s))
+                throw Failure{HB_ERR_UNSUPPORTED, "too many right-hand sides or panels for the substitution kernel", body_index};
+            // the factors read once (16 B per entry)
+            P.end(KF_LU_SOLVE, 16.0 * (double)NN * nb, s);
+            g_launches += 1;
+            t.stop();
+        }
+        {
+            EventTimer t(s, &prof[4]);
+            double* base = dout.as<double>();
+            double* dAo = base;
+            double* dBo = base + 36 * (size_t)nb;
+            double2* dXo = reinterpret_cast<double2*>(base + 72 * (size_t)nb);
+            double2* dFK = dXo + (size_t)H * 6 * nb;
+            double2* dSC = dFK + (size_t)H * 6 * nb;
+            KernelProfiler& P = profiler();
+            P.begin(s);
+            launch_forces(pv, nb, dfi.as<FreqInfo>(), H, dX.as<double2>(), dphiI.as<double2>(), opt.density, dAo, dBo,
+                          dXo, dFK, dSC, s);
+            P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
+            g_launches += 1;
+            CUDA_OK(cudaMemcpyAsync(hout.data(), dout.p, out_per * nb, cudaMemcpyDeviceToHost, s));
+            CUDA_OK(cudaMemcpyAsync(info.data(), dinfo.p, sizeof(int32_t) * nb, cudaMemcpyDeviceToHost, s));
+            t.stop();
+        }
+        CUDA_OK(cudaStreamSynchronize(s));
+        CUDA_OK(cudaGetLastError());
+        profiler().flush();
+        const double* hb = reinterpret_cast<const double*>(hout.data());
+        const double* hA = hb;
+        const double* hB = hb + 36 * (size_t)nb;
+        const double* hX = hb + 72 * (size_t)nb;
+        const double* hFK = hX + (size_t)H * 12 * nb;
+        const double* hSC = hFK + (size_t)H * 12 * nb;
+        for (int i = 0; i < nb; i++) {
+            if (info[i] != 0)
+                throw Failure{HB_ERR_NUMERICAL, "singular system matrix (zero pivot " + std::to_string(info[i]) + ")",
+                              body_index, f0 + i};
+            for (int q = 0; q < 36; q++)
+                if (!std::isfinite(hA[36 * i + q]) || !std::isfinite(hB[36 * i + q]))
+                    throw Failure{HB_ERR_NUMERICAL, "non-finite solution", body_index, f0 + i};
+            const size_t fo = (size_t)(f0 + i);
+            if (pr.out.added_mass) memcpy(pr.out.added_mass + fo * 36, hA + 36 * i, 36 * sizeof(double));
+            if (pr.out.radiation_damping) memcpy(pr.out.radiation_damping + fo * 36, hB + 36 * i, 36 * sizeof(double));
+            const size_t hx = (size_t)H * 12;
+            if (pr.out.excitation) memcpy(pr.out.excitation + fo * hx, hX + hx * i, hx * sizeof(double));
+            if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
+            if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
+        }
+    }
+}
+
+}  // namespace hbg
+
+using namespace hbg;
+
+// ==================================================================== C ABI: batched entry
+extern "C" void hbg_default_options(HbgOptions* opt) {
+    if (!opt) return;
+    opt->precision = HBG_FP64;
+    opt->logarithmic = 1;
+    opt->log_tolerance = 1e-4;
+    opt->gravity = 9.80665;
+    opt->density = 1000.0;
+    opt->depth = INFINITY;
+    opt->max_batch = 0;
+    opt->device = 0;
+    opt->cancel = nullptr;
+}
+
+extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_problems, const HbgOptions* opt) {
+    try {
+        if (!problems || !opt || n_problems < 0) return fail({HB_ERR_ARGUMENT, "null argument"});
+        for (int i = 0; i < 6; i++) g_profile[i] = 0.0;
+        g_launches = 0;
+        profiler().reset();
+        for (int64_t p = 0; p < n_problems; p++) {
+            const HbgProblem& pr = problems[p];
+            if (!pr.body.vertices || pr.n_omega < 0 || pr.n_heading < 0 || (pr.n_omega > 0 && !pr.omegas) ||
+                (pr.n_heading > 0 && !pr.headings_deg))
+                return fail({HB_ERR_ARGUMENT, "problem with a null array", p});
+        }
+        if (opt->precision != HBG_FP64 && opt->precision != HBG_MIXED)
+            return fail({HB_ERR_VALUE, "unknown precision form"});
+        if (!(opt->gravity > 0.0) || !(opt->density > 0.0) || opt->log_tolerance < 0.0)
+            return fail({HB_ERR_VALUE, "gravity and density must be positive, log_tolerance nonnegative"});
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            return fail({HB_ERR_UNSUPPORTED, "no CUDA device: this library runs the path on the GPU only"});
+        if (opt->device < 0 || opt->device >= ndev) return fail({HB_ERR_ARGUMENT, "device ordinal out of range"});
+        CUDA_OK(cudaSetDevice(opt->device));
+        device_ctx(opt->device);
+        cudaStream_t s;
+        CUDA_OK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        cudaEvent_t e0, e1;
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0, s);
+        try {
+            for (int64_t p = 0; p < n_problems; p++) solve_problem(problems[p], *opt, p, s);
+        } catch (...) {
+            cudaStreamSynchronize(s);
+            cudaStreamDestroy(s);
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw;
+        }
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        g_profile[5] = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaStreamDestroy(s);
+        return HB_OK;
+    } catch (const Failure& f) {
+        return fail(f);
+    } catch (const std::exception& e) {
+        return fail({HB_ERR_INTERNAL, std::string("internal error: ") + e.what()});
+    } catch (...) {
+        return fail({HB_ERR_INTERNAL, "internal error"});
+    }
+}
+
+extern "C" HbStatus hbg_last_profile(double* ms6) {
+    if (!ms6) return fail({HB_ERR_ARGUMENT, "null argument"});
+    for (int i = 0; i < 6; i++) ms6[i] = g_profile[i];
+    return HB_OK;
+}
+
+extern "C" HbStatus hbg_profile_kernels(int32_t on) {
+    profiler().on = on != 0;
+    return HB_OK;
+}
+
+extern "C" HbStatus hbg_kernel_profile(int32_t family, double* ms, int64_t* launches, double* work) {
+    if (!ms || !launches || !work) return fail({HB_ERR_ARGUMENT, "null argument"});
+    if (family < 0 || family >= KF_COUNT) return fail({HB_ERR_ARGUMENT, "kernel family out of range"});
+    KernelProfiler& P = profiler();
+    *ms = P.ms[family];
+    *launches = P.launches[family];
+    *work = P.work[family];
+    return HB_OK;
+}
+
+extern "C" HbStatus hbg_last_launch_count(int64_t* count) {
+    if (!count) return fail({HB_ERR_ARGUMENT, "null argument"});
+    *count = g_launches;
+    return HB_OK;
+}
+
+// Test support: the statics and the matrices S, A of one body at one frequency, FP64.
+extern "C" HbStatus hbg_debug_matrices(const HbgBody* body, double omega, const HbgOptions* opt, double* statics,
+                                       double* S, double* A) {
+    try {
+        if (!body || !opt || !body->vertices) return fail({HB_ERR_ARGUMENT, "null argument"});
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            return fail({HB_ERR_UNSUPPORTED, "no CUDA device: this library runs the path on the GPU only"});
+        CUDA_OK(cudaSetDevice(opt->device));
+        device_ctx(opt->device);
+        const int N = (int)body->n_panels;
+        const bool fin = finite_depth(opt->depth);
+        const double depth = fin ? opt->depth : 0.0;
+        cudaStream_t s = 0;
+        DevBuf dverts, dkind, dplanes, dbad, dst, dwork, dnwork, dS, dA, dfi, dfd, dtiles, dscr, dfpt;
+        dverts.alloc(sizeof(double) * 12 * N);
+        dkind.alloc(sizeof(int32_t) * N);
+        dplanes.alloc(sizeof(double) * P_PLANES * N);
+        dbad.alloc(sizeof(int32_t));
+        CUDA_OK(cudaMemcpy(dverts.p, body->vertices, sizeof(double) * 12 * N, cudaMemcpyHostToDevice));
+        std::vector<int32_t> kinds(N, 0);
+        if (body->kinds)
+            for (int j = 0; j < N; j++) kinds[j] = body->kinds[j];
+        CUDA_OK(cudaMemcpy(dkind.p, kinds.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
+        int32_t big = 0x7fffffff;
+        CUDA_OK(cudaMemcpy(dbad.p, &big, sizeof big, cudaMemcpyHostToDevice));
+        launch_panel_geometry(N, dverts.as<double>(), dkind.as<int32_t>(), dplanes.as<double>(), dbad.as<int32_t>(), s);
+        PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
+        const size_t NN = (size_t)N * N;
+        dst.alloc(sizeof(double) * 4 * NN);
+        const int cap = std::max(1 << 16, 16 * N);
+        dwork.alloc(sizeof(int32_t) * 2 * cap);
+        dnwork.alloc(sizeof(int32_t));
+        CUDA_OK(cudaMemset(dnwork.p, 0, sizeof(int32_t)));
+        launch_statics(pv, depth, opt->logarithmic, opt->log_tolerance, dst.as<double>(), dwork.as<int32_t>(),
+                       dnwork.as<int32_t>(), cap, s);
+        int32_t nwork = 0;
+        CUDA_OK(cudaMemcpy(&nwork, dnwork.p, sizeof nwork, cudaMemcpyDeviceToHost));
+        if (nwork > cap) return fail({HB_ERR_INTERNAL, "worklist overflow"});
+        launch_statics_adaptive(pv, dwork.as<int32_t>(), nwork, dst.as<double>(), s);
+        FreqInfo fi{omega, omega * omega / opt->gravity, 0.0, opt->logarithmic ? 1.0 : 0.0};
+        FdParams fdh;
+        dfi.alloc(sizeof fi);
+        dfd.alloc(sizeof fdh);
+        CUDA_OK(cudaMemcpy(dfi.p, &fi, sizeof fi, cudaMemcpyHostToDevice));
+        if (fin) {
+            make_fd_params(depth, fi.K, fdh);
+            CUDA_OK(cudaMemcpy(dfd.p, &fdh, sizeof fdh, cudaMemcpyHostToDevice));
+            dtiles.alloc(sizeof(double) * (T1_SIZE + T2_SIZE));
+            dscr.alloc(sizeof(double) * 6912 * 3);
+            dfpt.alloc(sizeof(double) * FP_PLANES * N);
+            launch_fd_tiles(1, dfd.as<FdParams>(), dtiles.as<double>(), dscr.as<double>(), s);
+            launch_fin_points(pv, 1, dfd.as<FdParams>(), dfpt.as<double>(), s);
+        }
+        dS.alloc(sizeof(double2) * NN);
+        dA.alloc(sizeof(double2) * NN);
+        launch_assemble_f64(pv, dst.as<double>(), 1, dfi.as<FreqInfo>(), dfd.as<FdParams>(), dtiles.as<double>(),
+                            dfpt.as<double>(), fin, dS.as<double2>(), dA.as<double2>(), NN, s);
+        CUDA_OK(cudaDeviceSynchronize());
+        CUDA_OK(cudaGetLastError());
+        if (statics) CUDA_OK(cudaMemcpy(statics, dst.p, sizeof(double) * 4 * NN, cudaMemcpyDeviceToHost));
+        if (S) CUDA_OK(cudaMemcpy(S, dS.p, sizeof(double2) * NN, cudaMemcpyDeviceToHost));
+        if (A) CUDA_OK(cudaMemcpy(A, dA.p, sizeof(double2) * NN, cudaMemcpyDeviceToHost));
+        return HB_OK;
+    } catch (const Failure& f) {
+        return fail(f);
+    } catch (...) {
+        return fail({HB_ERR_INTERNAL, "internal error"});
+    }
+}
+
+extern "C" const char* hb_last_error_message(void) { return g_error.c_str(); }
+
+extern "C" HbStatus hb_last_error_location(HbLocation* location) {
+    if (!location) return HB_ERR_ARGUMENT;
+    *location = g_location;
+    return HB_OK;
+}
+
+extern "C" uint32_t hb_abi_version(void) { return HBG_ABI_VERSION; }

@@ -1,0 +1,436 @@
+// hbg_freq.cu -- the per-frequency kernels of the FP64 form: finite-depth tiles and fin points,
+// assembly of S and A = 2 pi I - D, boundary values, right-hand sides -S u, pressure forces.
+#include "hbg_device.cuh"
+#include "hbg_internal.h"
+
+namespace hbg {
+
+// ------------------------------------------------------------------ finite-depth tiles
+// green_fin.rs:493-564 build_tiles: the values and both derivatives of Phi1, Phi2 at the
+// first-kind Chebyshev nodes of each tile (one thread per node), then per tile and quantity the
+// discrete cosine transform to Chebyshev coefficients and the power basis (one thread each).
+constexpr int NODES1 = TS * TW * TN * TN, NODES2 = TS * TV * TN * TN, NODES = NODES1 + NODES2;
+
+__device__ __forceinline__ double cheb_node(int i) { return cos(PI * (i + 0.5) / TN); }
+
+__global__ void k_fd_nodes(int F, const FdParams* __restrict__ fdp, double* __restrict__ scratch) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = blockIdx.y;
+    if (t >= NODES || f >= F) return;
+    const FdParams& fd = fdp[f];
+    int which = t < NODES1 ? 1 : 2;
+    int id = t < NODES1 ? t : t - NODES1;
+    int ny = which == 1 ? TW : TV;
+    double ymax = which == 1 ? 1.0 : 2.0;
+    int j = id % TN, i = (id / TN) % TN, iy = (id / (TN * TN)) % ny, ix = id / (TN * TN * ny);
+    double dx = XMAX / TS, dy = ymax / ny;
+    double v[3];
+    phi_direct(fd, which, dx * (ix + 0.5 * (cheb_node(i) + 1.0)), dy * (iy + 0.5 * (cheb_node(j) + 1.0)), v);
+    double* o = scratch + ((size_t)f * NODES + t) * 3;
+    o[0] = v[0];
+    o[1] = v[1];
+    o[2] = v[2];
+}
+
+__global__ void k_fd_fit(int F, const double* __restrict__ scratch, double* __restrict__ tiles) {
+    constexpr int N = TN;
+    constexpr int TILES1 = TS * TW, TILES2 = TS * TV;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = blockIdx.y;
+    if (t >= 3 * (TILES1 + TILES2) || f >= F) return;
+    int q = t % 3, tile = t / 3;
+    int which = tile < TILES1 ? 1 : 2;
+    int tid = tile < TILES1 ? tile : tile - TILES1;
+    const double* s = scratch + (size_t)f * NODES * 3 + (which == 1 ? 0 : (size_t)NODES1 * 3) + (size_t)tid * N * N * 3;
+    double fv[N][N];
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) fv[i][j] = s[(i * N + j) * 3 + q];
+    double cs[N][N], a[N][N];
+    for (int jj = 0; jj < N; jj++)
+        for (int i = 0; i < N; i++) cs[jj][i] = cos(PI * jj * (i + 0.5) / N);
+    for (int jj = 0; jj < N; jj++)
+        for (int k = 0; k < N; k++) a[jj][k] = 0.0;
+    a[0][0] = 1.0;
+    a[1][1] = 1.0;
+    for (int jj = 2; jj < N; jj++)
+        for (int k = 0; k < N; k++) a[jj][k] = (k > 0 ? 2.0 * a[jj - 1][k - 1] : 0.0) - a[jj - 2][k];
+    double c[N][N];
+    for (int ji = 0; ji < N; ji++)
+        for (int jj = 0; jj < N; jj++) {
+            double acc = 0.0;
+            for (int i = 0; i < N; i++)
+                for (int j = 0; j < N; j++) acc += fv[i][j] * cs[ji][i] * cs[jj][j];
+            c[ji][jj] = acc * (ji != 0 ? 2.0 : 1.0) * (jj != 0 ? 2.0 : 1.0) / (double)(N * N);
+        }
+    double pw[N * N];
+    for (int k = 0; k < N * N; k++) pw[k] = 0.0;
+    for (int ji = 0; ji < N; ji++)
+        for (int jj = 0; jj < N; jj++)
+            for (int ki = 0; ki <= ji; ki++)
+                for (int kj = 0; kj <= jj; kj++) pw[ki * N + kj] += c[ji][jj] * a[ji][ki] * a[jj][kj];
+    double* o = tiles + (size_t)f * (T1_SIZE + T2_SIZE) + (which == 1 ? 0 : T1_SIZE) + ((size_t)tid * 3 + q) * N * N;
+    for (int k = 0; k < N * N; k++) o[k] = pw[k];
+}
+
+void launch_fd_tiles(int F, const FdParams* fd, double* tiles, double* scratch, cudaStream_t s) {
+    k_fd_nodes<<<dim3((NODES + 127) / 128, F), 128, 0, s>>>(F, fd, scratch);
+    int nfit = 3 * (TS * TW + TS * TV);
+    k_fd_fit<<<dim3((nfit + 63) / 64, F), 64, 0, s>>>(F, scratch, tiles);
+}
+
+// green_fin.rs:937-952 fin_point, planes [F][FP_PLANES][N]: d a b c, then cos, sin k_n (z + h)
+__global__ void k_fin_points(PanelsView pv, int F, const FdParams* __restrict__ fdp, double* __restrict__ fpt) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = blockIdx.y;
+    if (j >= pv.N) return;
+    const FdParams& fd = fdp[f];
+    int N = pv.N;
+    double z = pv.at(P_C + 2, j), h = fd.h, k0 = fd.k0;
+    double* o = fpt + (size_t)f * FP_PLANES * N;
+    double d = 0, a = 0, b = 0, c = 0;
+    if (fd.mode == 0) {
+        d = exp(k0 * z);
+        a = exp(-k0 * (z + h));
+        b = exp(-k0 * (h - z));
+        c = exp(-k0 * (z + 2.0 * h));
+    }
+    o[0 * N + j] = d;
+    o[1 * N + j] = a;
+    o[2 * N + j] = b;
+    o[3 * N + j] = c;
+    for (int n = 0; n < FIN_ROOTS; n++) {
+        double sn, cn;
+        sincos(fd.kn[n] * (z + h), &sn, &cn);
+        o[(4 + 2 * n) * N + j] = cn;
+        o[(5 + 2 * n) * N + j] = sn;
+    }
+}
+
+void launch_fin_points(const PanelsView& pv, int F, const FdParams* fd, double* fpt, cudaStream_t s) {
+    k_fin_points<<<dim3((pv.N + 127) / 128, F), 128, 0, s>>>(pv, F, fd, fpt);
+}
+
+// ------------------------------------------------------------------ assembly
+// low_order.rs:738-769 apply_kernel + 781-790 kind_column: (S, D-column) of panel j at x.
+__device__ __forceinline__ void apply_kernel(double rs, double rd, double dl, double dd, double area, double nx,
+                                             double ny, double nz, int kindj, const double* x, const double* cj,
+                                             double K, double logc, const Kern& k, double R, bool swapped,
+                                             double2& S, double2& D) {
+    double a = R > 0.0 ? ((x[0] - cj[0]) * nx + (x[1] - cj[1]) * ny) / R : 0.0;
+    double rz = swapped ? k.Wrz : k.WrZ;
+    double iz = swapped ? k.Wiz : k.WiZ;
+    S.x = rs + area * k.Wr - 2.0 * K * logc * dl;
+    S.y = area * k.Wi;
+    D.x = rd + area * (-k.WrR * a + rz * nz) - 2.0 * K * logc * dd;
+    D.y = area * (-k.WiR * a + iz * nz);
+    if (kindj == 1) {  // interior free surface: K S (dG/dzeta = K G on zeta = 0)
+        D.x = K * S.x;
+        D.y = K * S.y;
+    }
+}
+
+__device__ __forceinline__ double free_term(int kind) { return kind == 1 ? -4.0 * PI : 2.0 * PI; }
+
+// One tile pair (K0 <= N0) of 32 x 32 panels for one frequency: the pair kernel once per
+// unordered pair (G(x, xi) = G(xi, x), the swapped source derivative for (n, k):
+// lo_frequency.rs:399-537), the (n, k) statics read and the (n, k) entries written through shared
+// memory transposes so that every global access is coalesced along the rows.
+template <bool FINITE>
+__global__ void __launch_bounds__(256) k_assemble_f64(PanelsView pv, const double* __restrict__ st,
+                                                      const FreqInfo* __restrict__ fi,
+                                                      const FdParams* __restrict__ fdp,
+                                                      const double* __restrict__ tiles,
+                                                      const double* __restrict__ fpt, double2* __restrict__ S,
+                                                      double2* __restrict__ A, size_t mat_stride) {
+    // statics (n, k) [q][k_local][n_local]; each (k_local, n_local) slot is read and then
+    // overwritten with the results (S, A) of entry (n, k) by the one thread that owns it
+    __shared__ double sT[4][32][33];
+    const int N = pv.N;
+    const int nt = (N + 31) / 32;
+    // tile pair from the linear index: row-block kb <= column-block nb
+    int idx = blockIdx.x, kb = 0;
+    while (idx >= nt - kb) {
+        idx -= nt - kb;
+        kb++;
+    }
+    const int nb = kb + idx;
+    const int f = blockIdx.y;
+    const int K0 = kb * 32, N0 = nb * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const size_t NN = (size_t)N * N;
+    const FreqInfo info = fi[f];
+    const double K = info.K, logc = info.logc;
+    S += (size_t)f * mat_stride;
+    A += (size_t)f * mat_stride;
+    // statics of (n, k): rows n in N0, panels k in K0
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int n = N0 + tx, k = K0 + ty + 8 * i;
+        if (n < N && k < N)
+#pragma unroll
+            for (int q = 0; q < 4; q++) sT[q][ty + 8 * i][tx] = __ldg(st + q * NN + (size_t)n + (size_t)k * N);
+    }
+    __syncthreads();
+    const int k = K0 + tx;
+    double xk[3] = {0, 0, 0}, nk[3] = {0, 0, 0}, ak = 0;
+    int kindk = 0;
+    if (k < N) {
+        for (int d = 0; d < 3; d++) {
+            xk[d] = pv.at(P_C + d, k);
+            nk[d] = pv.at(P_N + d, k);
+        }
+        ak = pv.at(P_AREA, k);
+        kindk = pv.kind[k];
+    }
+    const FdParams* fd = FINITE ? fdp + f : nullptr;
+    const double* T1 = FINITE ? tiles + (size_t)f * (T1_SIZE + T2_SIZE) : nullptr;
+    const double* T2 = FINITE ? T1 + T1_SIZE : nullptr;
+    const double* fp = FINITE ? fpt + (size_t)f * FP_PLANES * N : nullptr;
+#pragma unroll 1
+    for (int i = 0; i < 4; i++) {
+        const int nl = ty + 8 * i, n = N0 + nl;
+        bool live = k < N && n < N && (kb != nb || k <= n);
+        if (!live) continue;
+        double xn[3], nn3[3];
+        for (int d = 0; d < 3; d++) {
+            xn[d] = pv.at(P_C + d, n);
+            nn3[d] = pv.at(P_N + d, n);
+        }
+        double an = pv.at(P_AREA, n);
+        int kindn = pv.kind[n];
+        double dx = xk[0] - xn[0], dy = xk[1] - xn[1];
+        double R = sqrt(dx * dx + dy * dy);
+        Kern w;
+        if (FINITE) {
+            w = finite_kernel(*fd, T1, T2, R, xk[2], xn[2], fp + k, fp + n, N);
+        } else {
+            w = pair_kernel_inf(K, R, xk[2], xn[2]);
+        }
+        // entry (k, n): the field point x_k against panel n
+        size_t o1 = (size_t)k + (size_t)n * N;
+        double2 s1, d1;
+        apply_kernel(__ldg(st + o1), __ldg(st + NN + o1), __ldg(st + 2 * NN + o1), __ldg(st + 3 * NN + o1), an,
+                     nn3[0], nn3[1], nn3[2], kindn, xk, xn, K, logc, w, R, false, s1, d1);
+        S[o1] = s1;
+        A[o1] = make_double2((k == n ? free_term(kindk) : 0.0) - d1.x, -d1.y);
+        if (n != k) {
+            double2 s2, d2;
+            apply_kernel(sT[0][tx][nl], sT[1][tx][nl], sT[2][tx][nl], sT[3][tx][nl], ak, nk[0], nk[1], nk[2], kindk,
+                         xn, xk, K, logc, w, R, true, s2, d2);
+            sT[0][tx][nl] = s2.x;
+            sT[1][tx][nl] = s2.y;
+            sT[2][tx][nl] = -d2.x;
+            sT[3][tx][nl] = -d2.y;
+        }
+    }
+    __syncthreads();
+    // write the (n, k) entries: n = N0 + tx (coalesced), k = K0 + ty + 8 i
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int n = N0 + tx, kl = ty + 8 * i, kk = K0 + kl;
+        if (n < N && kk < N && (kb != nb || n > kk)) {
+            size_t o2 = (size_t)n + (size_t)kk * N;
+            S[o2] = make_double2(sT[0][kl][tx], sT[1][kl][tx]);
+            A[o2] = make_double2(sT[2][kl][tx], sT[3][kl][tx]);
+        }
+    }
+}
+
+void launch_assemble_f64(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
+                         const double* tiles, const double* fpt, bool finite, double2* S, double2* A,
+                         size_t mat_stride, cudaStream_t s) {
+    int nt = (pv.N + 31) / 32;
+    dim3 grid(nt * (nt + 1) / 2, F);
+    if (finite)
+        k_assemble_f64<true><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, S, A, mat_stride);
+    else
+        k_assemble_f64<false><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, S, A, mat_stride);
+}
+
+// ------------------------------------------------------------------ boundary values
+// low_order.rs:1401-1459 depth factor and incident wave; lo_frequency.rs:214-273 boundary values
+// (scattered formulation, one rigid body, rotation centre at the origin).
+__global__ void k_boundary(PanelsView pv, int F, const FreqInfo* __restrict__ fi, int H,
+                           const double* __restrict__ heads, double depth, double grav, double2* __restrict__ u,
+                           double2* __restrict__ phiI) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    int f = blockIdx.y;
+    int N = pv.N;
+    if (j >= N) return;
+    const int nrhs = 6 + H;
+    double c[3], n[3];
+    for (int d = 0; d < 3; d++) {
+        c[d] = pv.at(P_C + d, j);
+        n[d] = pv.at(P_N + d, j);
+    }
+    bool wet = pv.kind[j] == 0;
+    double2* uf = u + (size_t)f * nrhs * N;
+    double nj[6] = {n[0], n[1], n[2], c[1] * n[2] - c[2] * n[1], c[2] * n[0] - c[0] * n[2], c[0] * n[1] - c[1] * n[0]};
+    for (int m = 0; m < 6; m++) uf[(size_t)m * N + j] = make_double2(wet ? nj[m] : 0.0, 0.0);
+    double k = fi[f].k, w = fi[f].omega;
+    double Z = exp(k * c[2]), Zz = k * Z;
+    if (depth > 0.0) {
+        double b = exp(-k * (c[2] + 2.0 * depth));
+        double dd = 1.0 + exp(-2.0 * k * depth);
+        Zz = k * (Z - b) / dd;
+        Z = (Z + b) / dd;
+    }
+    for (int h = 0; h < H; h++) {
+        double sb, cb;
+        sincos(heads[h], &sb, &cb);
+        double phase = -k * (c[0] * cb + c[1] * sb);
+        double sp, cp;
+        sincos(phase, &sp, &cp);
+        // e = (i g / w) (cos + i sin)
+        double er = -(grav / w) * sp, ei = (grav / w) * cp;
+        double pr = er * Z, pi = ei * Z;
+        // grad: phi (-i k cb), phi (-i k sb), e Zz ; dphi/dn
+        double gxr = pi * k * cb, gxi = -pr * k * cb;
+        double gyr = pi * k * sb, gyi = -pr * k * sb;
+        double gzr = er * Zz, gzi = ei * Zz;
+        double dr = gxr * n[0] + gyr * n[1] + gzr * n[2];
+        double di = gxi * n[0] + gyi * n[1] + gzi * n[2];
+        phiI[((size_t)f * H + h) * N + j] = make_double2(pr, pi);
+        uf[(size_t)(6 + h) * N + j] = make_double2(wet ? -dr : 0.0, wet ? -di : 0.0);
+    }
+}
+
+void launch_boundary(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double* heads, double depth,
+                     double grav, double2* u, double2* phiI, cudaStream_t s) {
+    k_boundary<<<dim3((pv.N + 127) / 128, F), 128, 0, s>>>(pv, F, fi, H, heads, depth, grav, u, phiI);
+}
+
+// ------------------------------------------------------------------ right-hand sides -S u
+// One thread per row k holds the nrhs sums; S is read once, column by column (coalesced along k),
+// u staged in shared memory (lo_frequency.rs:875-892: the product S U with U = -u).
+template <int NR>
+__global__ void __launch_bounds__(128) k_rhs_f64(int N, int nrhs, const double2* __restrict__ S, size_t mat_stride,
+                                                 const double2* __restrict__ u, double2* __restrict__ rhs) {
+    constexpr int CH = 32;
+    __shared__ double2 su[CH][NR];
+    int f = blockIdx.y;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const double2* Sf = S + (size_t)f * mat_stride;
+    const double2* uf = u + (size_t)f * nrhs * N;
+    double2 acc[NR];
+#pragma unroll
+    for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
+    for (int n0 = 0; n0 < N; n0 += CH) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < CH * NR; t += blockDim.x) {
+            int nn = t % CH, c = t / CH;
+            su[nn][c] = (n0 + nn < N && c < nrhs) ? uf[(size_t)c * N + n0 + nn] : make_double2(0.0, 0.0);
+        }
+        __syncthreads();
+        if (k < N) {
+            int lim = min(CH, N - n0);
+            for (int nn = 0; nn < lim; nn++) {
+                double2 s = Sf[(size_t)k + (size_t)(n0 + nn) * N];
+#pragma unroll
+                for (int c = 0; c < NR; c++) {
+                    double2 v = su[nn][c];
+                    acc[c].x += s.x * v.x - s.y * v.y;
+                    acc[c].y += s.x * v.y + s.y * v.x;
+                }
+            }
+        }
+    }
+    if (k < N)
+        for (int c = 0; c < nrhs && c < NR; c++) rhs[((size_t)f * nrhs + c) * N + k] = make_double2(-acc[c].x, -acc[c].y);
+}
+
+void launch_rhs_f64(int N, int F, int nrhs, const double2* S, size_t mat_stride, const double2* u, double2* rhs,
+                    cudaStream_t s) {
+    dim3 grid((N + 127) / 128, F);
+    if (nrhs <= 8)
+        k_rhs_f64<8><<<grid, 128, 0, s>>>(N, nrhs, S, mat_stride, u, rhs);
+    else if (nrhs <= 16)
+        k_rhs_f64<16><<<grid, 128, 0, s>>>(N, nrhs, S, mat_stride, u, rhs);
+    else
+        k_rhs_f64<32><<<grid, 128, 0, s>>>(N, nrhs, S, mat_stride, u, rhs);
+}
+
+// ------------------------------------------------------------------ forces
+// lo_frequency.rs:1039-1115: z = sum_j n_i phi_c A_j over the wetted panels; A = Re(-rho z),
+// B = -w Im(-rho z); X = i w rho sum n_i (phi_S + phi_I) A_j, FK the phi_I part, SC = X - FK.
+// One block per frequency; fixed-order block reductions (deterministic).
+__global__ void __launch_bounds__(256) k_forces(PanelsView pv, const FreqInfo* __restrict__ fi, int H,
+                                                const double2* __restrict__ phi, const double2* __restrict__ phiI,
+                                                double rho, double* __restrict__ Aout, double* __restrict__ Bout,
+                                                double2* __restrict__ X, double2* __restrict__ FK,
+                                                double2* __restrict__ SC) {
+    __shared__ double red[256];
+    int f = blockIdx.x, N = pv.N;
+    int nrhs = 6 + H;
+    const double2* pf = phi + (size_t)f * nrhs * N;
+    const double2* pif = phiI + (size_t)f * H * N;
+    double w = fi[f].omega;
+    auto block_sum = [&](double v) -> double {
+        red[threadIdx.x] = v;
+        __syncthreads();
+        for (int s = 128; s > 0; s >>= 1) {
+            if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+            __syncthreads();
+        }
+        double r = red[0];
+        __syncthreads();
+        return r;
+    };
+    // columns: c < 6 radiation (phi_c), 6 <= c < 6 + H diffraction (phi_S + phi_I), then H of phi_I
+    for (int col = 0; col < 6 + 2 * H; col++) {
+        for (int i = 0; i < 6; i++) {
+            double sr = 0.0, si = 0.0;
+            for (int j = threadIdx.x; j < N; j += blockDim.x) {
+                if (pv.kind[j] != 0) continue;
+                double c[3] = {pv.at(P_C, j), pv.at(P_C + 1, j), pv.at(P_C + 2, j)};
+                double n[3] = {pv.at(P_N, j), pv.at(P_N + 1, j), pv.at(P_N + 2, j)};
+                double nj = i == 0 ? n[0] : i == 1 ? n[1] : i == 2 ? n[2]
+                          : i == 3 ? c[1] * n[2] - c[2] * n[1]
+                          : i == 4 ? c[2] * n[0] - c[0] * n[2]
+                                   : c[0] * n[1] - c[1] * n[0];
+                double wgt = nj * pv.at(P_AREA, j);
+                double2 v;
+                if (col < 6 + H) {
+                    v = pf[(size_t)col * N + j];
+                    if (col >= 6) {
+                        double2 pI = pif[(size_t)(col - 6) * N + j];
+                        v.x += pI.x;
+                        v.y += pI.y;
+                    }
+                } else {
+                    v = pif[(size_t)(col - 6 - H) * N + j];
+                }
+                sr += wgt * v.x;
+                si += wgt * v.y;
+            }
+            sr = block_sum(sr);
+            si = block_sum(si);
+            if (threadIdx.x == 0) {
+                if (col < 6) {
+                    double zr = -rho * sr, zi = -rho * si;
+                    Aout[((size_t)f * 6 + i) * 6 + col] = zr;
+                    Bout[((size_t)f * 6 + i) * 6 + col] = -w * zi;
+                } else {
+                    // i w rho (sr + i si) = (-w rho si, w rho sr)
+                    double2 val = make_double2(-w * rho * si, w * rho * sr);
+                    if (col < 6 + H)
+                        X[((size_t)f * H + (col - 6)) * 6 + i] = val;
+                    else
+                        FK[((size_t)f * H + (col - 6 - H)) * 6 + i] = val;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6 * H) {
+        size_t o = (size_t)f * H * 6 + threadIdx.x;
+        SC[o] = make_double2(X[o].x - FK[o].x, X[o].y - FK[o].y);
+    }
+}
+
+void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, const double2* phiI,
+                   double rho, double* A, double* B, double2* X, double2* FK, double2* SC, cudaStream_t s) {
+    k_forces<<<F, 256, 0, s>>>(pv, fi, H, phi, phiI, rho, A, B, X, FK, SC);
+}
+
+}  // namespace hbg

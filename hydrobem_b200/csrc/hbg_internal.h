@@ -1,0 +1,101 @@
+// hbg_internal.h -- host-side declarations shared by the translation units of libhydrobem_gpu.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "hbg_device.cuh"
+
+namespace hbg {
+
+// Kernel-family timing (off by default): CUDA events around each launch on its stream, resolved at
+// the next host synchronization, with the algorithmic work of the launch (bytes or flops).
+enum KernelFamily {
+    KF_GEOMETRY = 0, KF_STATICS, KF_STATICS_ADAPTIVE, KF_FD_TILES, KF_ASSEMBLE, KF_BOUNDARY, KF_RHS,
+    KF_LU_PANEL, KF_LU_LASWP, KF_LU_TRSM, KF_LU_GEMM, KF_LU_SOLVE, KF_FORCES, KF_MIXED_CONVERT,
+    KF_MIXED_GEMM, KF_MIXED_RESIDUAL, KF_COUNT
+};
+
+struct KernelProfiler {
+    bool on = false;
+    double ms[KF_COUNT] = {};
+    double work[KF_COUNT] = {};
+    int64_t launches[KF_COUNT] = {};
+    struct Pending {
+        int fam;
+        cudaEvent_t a, b;
+    };
+    Pending pend[4096];
+    int npend = 0;
+    void reset() {
+        for (int i = 0; i < KF_COUNT; i++) ms[i] = work[i] = 0.0, launches[i] = 0;
+    }
+    // record around a launch; call begin() before and end() after the launch on stream s
+    cudaEvent_t begin(cudaStream_t s) {
+        if (!on) return nullptr;
+        if (npend == 4096) flush();
+        cudaEventCreate(&pend[npend].a);
+        cudaEventRecord(pend[npend].a, s);
+        return pend[npend].a;
+    }
+    void end(int fam, double w, cudaStream_t s) {
+        launches[fam]++;
+        work[fam] += w;
+        if (!on) return;
+        cudaEventCreate(&pend[npend].b);
+        cudaEventRecord(pend[npend].b, s);
+        pend[npend].fam = fam;
+        npend++;
+    }
+    void flush() {
+        for (int i = 0; i < npend; i++) {
+            cudaEventSynchronize(pend[i].b);
+            float t = 0.f;
+            cudaEventElapsedTime(&t, pend[i].a, pend[i].b);
+            ms[pend[i].fam] += t;
+            cudaEventDestroy(pend[i].a);
+            cudaEventDestroy(pend[i].b);
+        }
+        npend = 0;
+    }
+};
+
+KernelProfiler& profiler();
+
+// Per-frequency data of one batch entry (one body, one omega).
+struct FreqInfo {
+    double omega, K, k;   // radian frequency, K = omega^2 / g, incident wave number
+    double logc;          // weight of the analytic log-singularity integral (0 or 1)
+};
+
+void set_constants(const double glx[17][16], const double glw[17][16], const Tables& tab);
+void launch_panel_geometry(int N, const double* verts, const int32_t* kind, double* planes, int32_t* bad,
+                           cudaStream_t s);
+void launch_statics(const PanelsView& pv, double depth, int logint, double tol, double* st, int32_t* work,
+                    int32_t* nwork, int work_cap, cudaStream_t s);
+void launch_statics_adaptive(const PanelsView& pv, const int32_t* work, int nwork, double* st, cudaStream_t s);
+
+// finite depth: per-frequency tiles [F][T1 | T2] and fin-point planes [F][FP_PLANES][N]
+void launch_fd_tiles(int F, const FdParams* fd, double* tiles, double* scratch, cudaStream_t s);
+void launch_fin_points(const PanelsView& pv, int F, const FdParams* fd, double* fpt, cudaStream_t s);
+
+// assembly of S and A (complex128, column-major N x N per frequency, stride mat_stride elements)
+void launch_assemble_f64(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
+                         const double* tiles, const double* fpt, bool finite, double2* S, double2* A,
+                         size_t mat_stride, cudaStream_t s);
+// boundary values u [F][nrhs][N] and incident wave phiI [F][H][N]
+void launch_boundary(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double* heads, double depth,
+                     double grav, double2* u, double2* phiI, cudaStream_t s);
+// rhs[F][nrhs][N] = -S u
+void launch_rhs_f64(int N, int F, int nrhs, const double2* S, size_t mat_stride, const double2* u, double2* rhs,
+                    cudaStream_t s);
+// forces: out[F][...] A, B [6][6], X, FK, SC [H][6] complex, all f64
+void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, const double2* phiI,
+                   double rho, double* A, double* B, double2* X, double2* FK, double2* SC, cudaStream_t s);
+
+// plain FP64 LU with partial pivoting, batched over F matrices (in place), and the solve
+int lu_factor_f64(int N, int F, double2* A, size_t mat_stride, int32_t* ipiv, int32_t* info, cudaStream_t s,
+                  int64_t* launches);
+int lu_solve_f64(int N, int F, const double2* LU, size_t mat_stride, const int32_t* ipiv, int nrhs, const double2* B,
+                 double2* X, cudaStream_t s);
+
+}  // namespace hbg

@@ -1,0 +1,16 @@
+// hbg_mixed.h -- the mixed-precision form (complex64 matrices, tensor-core LU, FP64 refinement).
+#pragma once
+#include <cstdint>
+
+#include "../../include/hydrobem_gpu.h"
+#include "hbg_internal.h"
+
+namespace hbg {
+
+// Solve every frequency of one body in the mixed form; statics st (FP64, [4][N*N]) already made.
+// Returns 0, or an HbStatus with the message in *msg and the frequency in *freq.
+int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgProblem& pr, const HbgOptions& opt,
+                            bool finite, double depth, cudaStream_t s, double* prof, int64_t* launches,
+                            const char** msg, int64_t* freq);
+
+}  // namespace hbg

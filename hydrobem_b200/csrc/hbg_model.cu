@@ -1,0 +1,466 @@
+// hbg_model.cu -- the model/solve/results subset of the reference's C ABI (hydrobem.h), for the
+// items of the low-order open-sea route of one rigid body.  Objects: the model (""),
+// "environment", "options", "meshes/<name>" (kind panels: vertices [P,4,3], symmetry) and
+// "bodies/<name>" (mesh, interior_surface, interior_surface_mesh).  A mesh with symmetry planes
+// is expanded to the full mesh (the stored elements, then their x, y and xy reflections,
+// geometry.rs:208-235), which solves the same discrete equations as the reference's character
+// decomposition.  Items and routes outside this subset are refused with HB_ERR_UNSUPPORTED, as the
+// reference refuses routes it lacks.
+#include <atomic>
+#include <cmath>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace hbg {
+
+struct MeshObj {
+    std::string name;
+    std::vector<double> vertices;  // [P][4][3]
+    std::string symmetry = "none";
+};
+
+struct BodyObj {
+    std::string name;
+    std::string mesh;
+    std::string interior = "detect";
+    std::string interior_mesh;
+};
+
+struct Quantity {
+    std::string name;
+    int32_t dtype;
+    std::vector<size_t> shape;
+    std::vector<unsigned char> data;
+};
+
+}  // namespace hbg
+
+struct HbResults {
+    std::vector<hbg::Quantity> q;
+};
+
+struct HbModel {
+    std::mutex lock;
+    std::atomic<int32_t> cancel{0};
+    std::atomic<bool> solving{false};
+    // environment
+    std::vector<double> omegas, periods, headings;
+    std::string frequency_input = "omegas";
+    double depth = INFINITY, gravity = 9.80665, density = 1000.0;
+    // options
+    bool logarithmic = true;
+    double log_tolerance = 1e-4;
+    std::string precision = "fp64";
+    int64_t device = 0;
+    std::vector<hbg::MeshObj> meshes;
+    std::vector<hbg::BodyObj> bodies;
+    std::unique_ptr<HbResults> results;
+};
+
+namespace hbg {
+
+constexpr uint64_t OBJ_MODEL = 0, OBJ_ENV = 1, OBJ_OPTIONS = 2, OBJ_MESH0 = 1000, OBJ_BODY0 = 2000000;
+
+static HbStatus refuse(HbStatus code, const std::string& msg) { return fail(Failure{code, msg}); }
+
+template <class F>
+static HbStatus guard(F&& f) {
+    try {
+        return f();
+    } catch (const Failure& e) {
+        return fail(e);
+    } catch (const std::exception& e) {
+        return fail(Failure{HB_ERR_INTERNAL, std::string("internal error: ") + e.what()});
+    } catch (...) {
+        return fail(Failure{HB_ERR_INTERNAL, "internal error"});
+    }
+}
+
+static bool is_mesh(const HbModel* m, uint64_t o) { return o >= OBJ_MESH0 && o < OBJ_MESH0 + m->meshes.size(); }
+static bool is_body(const HbModel* m, uint64_t o) { return o >= OBJ_BODY0 && o < OBJ_BODY0 + m->bodies.size(); }
+
+static std::vector<double> reals(const double* data, const size_t* shape, size_t ndim, size_t& count) {
+    count = 1;
+    for (size_t i = 0; i < ndim; i++) count *= shape[i];
+    return std::vector<double>(data, data + count);
+}
+
+static void add_quantity(HbResults* r, const std::string& name, int32_t dtype, std::vector<size_t> shape,
+                         const void* src, size_t bytes) {
+    Quantity q{name, dtype, std::move(shape), std::vector<unsigned char>(bytes)};
+    if (bytes) memcpy(q.data.data(), src, bytes);
+    r->q.push_back(std::move(q));
+}
+
+// The full panels of a mesh with its symmetry planes (the reflected copies, orientation restored).
+static std::vector<double> expand(const MeshObj& m) {
+    std::vector<std::pair<double, double>> refl = {{1.0, 1.0}};
+    if (m.symmetry == "yz" || m.symmetry == "xz_and_yz") refl.push_back({-1.0, 1.0});
+    if (m.symmetry == "xz" || m.symmetry == "xz_and_yz") refl.push_back({1.0, -1.0});
+    if (m.symmetry == "xz_and_yz") refl.push_back({-1.0, -1.0});
+    size_t P = m.vertices.size() / 12;
+    std::vector<double> out;
+    out.reserve(refl.size() * m.vertices.size());
+    for (auto [sx, sy] : refl)
+        for (size_t p = 0; p < P; p++) {
+            const double* v = &m.vertices[12 * p];
+            int order[4] = {0, 1, 2, 3};
+            if (sx * sy < 0) {
+                order[1] = 3;
+                order[3] = 1;
+            }
+            for (int i = 0; i < 4; i++) {
+                const double* q = v + 3 * order[i];
+                out.push_back(sx * q[0]);
+                out.push_back(sy * q[1]);
+                out.push_back(q[2]);
+            }
+        }
+    return out;
+}
+
+}  // namespace hbg
+
+using namespace hbg;
+
+extern "C" HbStatus hb_model_new(HbModel** out) {
+    return guard([&]() -> HbStatus {
+        if (!out) return refuse(HB_ERR_ARGUMENT, "null out-pointer");
+        *out = new HbModel();
+        return HB_OK;
+    });
+}
+
+extern "C" HbStatus hb_model_free(HbModel* model) {
+    if (!model) return HB_OK;
+    if (model->solving) return refuse(HB_ERR_STATE, "the model is solving");
+    delete model;
+    return HB_OK;
+}
+
+extern "C" HbStatus hb_model_cancel(HbModel* model) {
+    if (!model) return refuse(HB_ERR_ARGUMENT, "null model");
+    model->cancel = 1;
+    return HB_OK;
+}
+
+extern "C" HbStatus hb_object(HbModel* model, const char* path, uint64_t* object) {
+    return guard([&]() -> HbStatus {
+        if (!model || !path || !object) return refuse(HB_ERR_ARGUMENT, "null argument");
+        std::lock_guard<std::mutex> g(model->lock);
+        std::string p(path);
+        if (p.empty()) return *object = OBJ_MODEL, HB_OK;
+        if (p == "environment") return *object = OBJ_ENV, HB_OK;
+        if (p == "options") return *object = OBJ_OPTIONS, HB_OK;
+        for (size_t i = 0; i < model->meshes.size(); i++)
+            if (p == "meshes/" + model->meshes[i].name) return *object = OBJ_MESH0 + i, HB_OK;
+        for (size_t i = 0; i < model->bodies.size(); i++)
+            if (p == "bodies/" + model->bodies[i].name) return *object = OBJ_BODY0 + i, HB_OK;
+        return refuse(HB_ERR_VALUE, "no object at the path \"" + p + "\"");
+    });
+}
+
+extern "C" HbStatus hb_add(HbModel* model, uint64_t parent, const char* list, const char* type_name,
+                           const char* name, int64_t index, uint64_t* out) {
+    return guard([&]() -> HbStatus {
+        if (!model || !list || !out) return refuse(HB_ERR_ARGUMENT, "null argument");
+        std::lock_guard<std::mutex> g(model->lock);
+        if (parent != OBJ_MODEL) return refuse(HB_ERR_UNSUPPORTED, "only the lists of the model are on this route");
+        if (index != -1) return refuse(HB_ERR_UNSUPPORTED, "objects are added at the end of their list (index -1)");
+        std::string l(list), t(type_name ? type_name : ""), n(name ? name : "");
+        if (n.empty()) return refuse(HB_ERR_VALUE, "a mesh or body needs a name");
+        if (l == "meshes" && (t.empty() || t == "Mesh")) {
+            for (auto& m : model->meshes)
+                if (m.name == n) return refuse(HB_ERR_VALUE, "a mesh of that name exists");
+            model->meshes.push_back(MeshObj{n});
+            *out = OBJ_MESH0 + model->meshes.size() - 1;
+            return HB_OK;
+        }
+        if (l == "bodies" && (t.empty() || t == "Body")) {
+            for (auto& b : model->bodies)
+                if (b.name == n) return refuse(HB_ERR_VALUE, "a body of that name exists");
+            model->bodies.push_back(BodyObj{n});
+            *out = OBJ_BODY0 + model->bodies.size() - 1;
+            return HB_OK;
+        }
+        return refuse(HB_ERR_UNSUPPORTED, "the list \"" + l + "\" is not on this route");
+    });
+}
+
+extern "C" HbStatus hb_set_reals(HbModel* model, uint64_t object, const char* item, const double* data,
+                                 const size_t* shape, size_t ndim) {
+    return guard([&]() -> HbStatus {
+        if (!model || !item || (!data && ndim > 0) || (!shape && ndim > 0)) return refuse(HB_ERR_ARGUMENT, "null argument");
+        std::lock_guard<std::mutex> g(model->lock);
+        std::string it(item);
+        size_t count = 0;
+        std::vector<double> v = reals(data, shape, ndim, count);
+        for (double x : v)
+            if (std::isnan(x)) return refuse(HB_ERR_VALUE, "NaN in " + it);
+        if (object == OBJ_ENV) {
+            if (ndim != 1) return refuse(HB_ERR_VALUE, it + " is a 1-D array");
+            if (it == "omegas" || it == "periods") {
+                for (double x : v)
+                    if (x < 0.0) return refuse(HB_ERR_VALUE, it + " must be >= 0");
+                (it == "omegas" ? model->omegas : model->periods) = v;
+                return HB_OK;
+            }
+            if (it == "headings") {
+                for (double x : v)
+                    if (!std::isfinite(x)) return refuse(HB_ERR_VALUE, "headings must be finite");
+                model->headings = v;
+                return HB_OK;
+            }
+        }
+        if (is_mesh(model, object) && it == "vertices") {
+            if (ndim != 3 || shape[1] != 4 || shape[2] != 3) return refuse(HB_ERR_VALUE, "vertices have the shape (P, 4, 3)");
+            for (double x : v)
+                if (!std::isfinite(x)) return refuse(HB_ERR_VALUE, "non-finite vertex coordinate");
+            model->meshes[object - OBJ_MESH0].vertices = v;
+            return HB_OK;
+        }
+        return refuse(HB_ERR_UNSUPPORTED, "the item \"" + it + "\" of this object is not on this route");
+    });
+}
+
+extern "C" HbStatus hb_set_real(HbModel* model, uint64_t object, const char* item, double value) {
+    return guard([&]() -> HbStatus {
+        if (!model || !item) return refuse(HB_ERR_ARGUMENT, "null argument");
+        std::lock_guard<std::mutex> g(model->lock);
+        std::string it(item);
+        if (std::isnan(value)) return refuse(HB_ERR_VALUE, "NaN");
+        if (object == OBJ_ENV) {
+            if (it == "depth") {
+                if (!(value > 0.0)) return refuse(HB_ERR_VALUE, "depth > 0 (inf for infinite depth)");
+                model->depth = value;
+                return HB_OK;
+            }
+            if (it == "gravity" || it == "density") {
+                if (!(value > 0.0) || !std::isfinite(value)) return refuse(HB_ERR_VALUE, it + " must be positive");
+                (it == "gravity" ? model->gravity : model->density) = value;
+                return HB_OK;
+            }
+        }
+        if (object == OBJ_OPTIONS && it == "log_tolerance") {
+            if (!(value >= 0.0)) return refuse(HB_ERR_VALUE, "log_tolerance >= 0");
+            model->log_tolerance = value;
+            return HB_OK;
+        }
+        return refuse(HB_ERR_UNSUPPORTED, "the item \"" + it + "\" of this object is not on this route");
+    });
+}
+
+extern "C" HbStatus hb_set_bool(HbModel* model, uint64_t object, const char* item, int32_t value) {
+    return guard([&]() -> HbStatus {
+        if (!model || !item) return refuse(HB_ERR_ARGUMENT, "null argument");
+        std::lock_guard<std::mutex> g(model->lock);
+        std::string it(item);
+        if (object == OBJ_OPTIONS && it == "logarithmic_integration") {
+            model->logarithmic = value != 0;
+            return HB_OK;
+        }
+        return refuse(HB_ERR_UNSUPPORTED, "the item \"" + it + "\" of this object is not on this route");
+    });
+}
+
+extern "C" HbStatus hb_set_int(HbModel* model, uint64_t object, const char* item, int64_t value) {
+    return guard([&]() -> HbStatus {
+        if (!model || !item) return refuse(HB_ERR_ARGUMENT, "null argument");
+        std::lock_guard<std::mutex> g(model->lock);
+        std::string it(item);
+        if (object == OBJ_OPTIONS && it == "gpu_device") {
+            if (value < 0) return refuse(HB_ERR_VALUE, "gpu_device >= 0");
+            model->device = value;
+            return HB_OK;
+        }
+        return refuse(HB_ERR_UNSUPPORTED, "the item \"" + it + "\" of this object is not on this route");
+    });
+}
+
+extern "C" HbStatus hb_set_ints(HbModel* model, uint64_t object, const char* item, const int64_t*, const size_t*,
+                                size_t) {
+    if (!model || !item) return refuse(HB_ERR_ARGUMENT, "null argument");
+    return refuse(HB_ERR_UNSUPPORTED, std::string("the item \"") + item + "\" of this object is not on this route");
+}
+
+extern "C" HbStatus hb_set_text(HbModel* model, uint64_t object, const char* item, const char* value) {
+    return guard([&]() -> HbStatus {
+        if (!model || !item || !value) return refuse(HB_ERR_ARGUMENT, "null argument");
+        std::lock_guard<std::mutex> g(model->lock);
+        std::string it(item), v(value);
+        if (object == OBJ_ENV && it == "frequency_input") {
+            if (v != "omegas" && v != "periods") return refuse(HB_ERR_VALUE, "frequency_input is omegas or periods");
+            model->frequency_input = v;
+            return HB_OK;
+        }
+        if (object == OBJ_OPTIONS && it == "gpu_precision") {
+            if (v != "fp64" && v != "mixed") return refuse(HB_ERR_VALUE, "gpu_precision is fp64 or mixed");
+            model->precision = v;
+            return HB_OK;
+        }
+        if (is_mesh(model, object)) {
+            MeshObj& m = model->meshes[object - OBJ_MESH0];
+            if (it == "kind") return v == "panels" ? HB_OK : refuse(HB_ERR_UNSUPPORTED, "only panels meshes are on this route");
+            if (it == "symmetry") {
+                if (v != "none" && v != "yz" && v != "xz" && v != "xz_and_yz")
+                    return refuse(HB_ERR_VALUE, "symmetry is none, yz, xz or xz_and_yz");
+                m.symmetry = v;
+                return HB_OK;
+            }
+        }
+        if (is_body(model, object)) {
+            BodyObj& b = model->bodies[object - OBJ_BODY0];
+            if (it == "mesh") return b.mesh = v, HB_OK;
+            if (it == "interior_surface") {
+                if (v != "none" && v != "detect" && v != "mesh")
+                    return refuse(HB_ERR_UNSUPPORTED, "interior_surface none, detect or mesh on this route");
+                return b.interior = v, HB_OK;
+            }
+            if (it == "interior_surface_mesh") return b.interior_mesh = v, HB_OK;
+        }
+        return refuse(HB_ERR_UNSUPPORTED, "the item \"" + it + "\" of this object is not on this route");
+    });
+}
+
+extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* user, HbResults** out) {
+    return guard([&]() -> HbStatus {
+        if (!model) return refuse(HB_ERR_ARGUMENT, "null model");
+        if (model->solving.exchange(true)) return refuse(HB_ERR_STATE, "the model is solving");
+        struct Done {
+            HbModel* m;
+            ~Done() { m->solving = false; }
+        } done{model};
+        std::vector<double> verts, omegas, heads;
+        std::vector<int32_t> kinds;
+        HbgOptions opt;
+        hbg_default_options(&opt);
+        {
+            std::lock_guard<std::mutex> g(model->lock);
+            if (model->bodies.size() != 1)
+                return refuse(HB_ERR_UNSUPPORTED, "this route solves one rigid body per model (hbg_solve_batch takes many)");
+            const BodyObj& b = model->bodies[0];
+            const MeshObj* mesh = nullptr;
+            const MeshObj* lid = nullptr;
+            for (auto& m : model->meshes) {
+                if (m.name == b.mesh) mesh = &m;
+                if (m.name == b.interior_mesh) lid = &m;
+            }
+            if (!mesh || mesh->vertices.empty()) return refuse(HB_ERR_VALUE, "the body has no panels mesh");
+            verts = expand(*mesh);
+            size_t P = verts.size() / 12;
+            kinds.assign(P, HBG_WET);
+            if (b.interior == "detect")
+                for (size_t p = 0; p < P; p++) {
+                    bool z0 = true;
+                    for (int i = 0; i < 4; i++) z0 = z0 && verts[12 * p + 3 * i + 2] == 0.0;
+                    if (z0) kinds[p] = HBG_INTERIOR;
+                }
+            if (b.interior == "mesh") {
+                if (!lid) return refuse(HB_ERR_VALUE, "interior_surface_mesh names no mesh");
+                std::vector<double> lv = expand(*lid);
+                verts.insert(verts.end(), lv.begin(), lv.end());
+                kinds.resize(verts.size() / 12, HBG_INTERIOR);
+            }
+            const std::vector<double>& f = model->frequency_input == "omegas" ? model->omegas : model->periods;
+            for (double x : f) {
+                double w = model->frequency_input == "omegas" ? x : (x > 0.0 ? 2.0 * PI / x : INFINITY);
+                if (!(w > 0.0) || !std::isfinite(w))
+                    return refuse(HB_ERR_UNSUPPORTED, "the zero- and infinite-frequency limits are not on this route");
+                omegas.push_back(w);
+            }
+            heads = model->headings;
+            opt.precision = model->precision == "mixed" ? HBG_MIXED : HBG_FP64;
+            opt.logarithmic = model->logarithmic;
+            opt.log_tolerance = model->log_tolerance;
+            opt.gravity = model->gravity;
+            opt.density = model->density;
+            opt.depth = model->depth;
+            opt.device = (int32_t)model->device;
+        }
+        opt.cancel = reinterpret_cast<const volatile int32_t*>(&model->cancel);
+        if (model->cancel.exchange(0) != 0) return refuse(HB_ERR_CANCELLED, "the solve was cancelled");
+        const size_t F = omegas.size(), H = heads.size();
+        std::vector<double> A(F * 36), B(F * 36), X(F * H * 12), FK(F * H * 12), SC(F * H * 12);
+        HbgProblem pr{};
+        pr.body.n_panels = (int64_t)(verts.size() / 12);
+        pr.body.vertices = verts.data();
+        pr.body.kinds = kinds.data();
+        pr.omegas = omegas.data();
+        pr.n_omega = (int64_t)F;
+        pr.headings_deg = heads.data();
+        pr.n_heading = (int64_t)H;
+        pr.out = HbgOutputs{A.data(), B.data(), X.data(), FK.data(), SC.data()};
+        if (progress) {
+            HbProgress pg{};
+            pg.stage = 0;
+            pg.frequency = -2;
+            pg.frequencies_total = F;
+            if (progress(&pg, user) == 0) return refuse(HB_ERR_CANCELLED, "the solve was cancelled");
+        }
+        HbStatus st = hbg_solve_batch(&pr, 1, &opt);
+        if (st != HB_OK) return st;
+        if (progress) {
+            HbProgress pg{};
+            pg.stage = 0;
+            pg.frequency = -4;
+            pg.frequencies_done = F;
+            pg.frequencies_total = F;
+            pg.seconds = g_profile[5] * 1e-3;
+            progress(&pg, user);
+        }
+        auto r = std::make_unique<HbResults>();
+        add_quantity(r.get(), "omegas", HB_F64, {F}, omegas.data(), F * 8);
+        add_quantity(r.get(), "headings", HB_F64, {H}, heads.data(), H * 8);
+        std::vector<float> a32(F * 36), b32(F * 36), x32(F * H * 12), fk32(F * H * 12), sc32(F * H * 12);
+        for (size_t i = 0; i < F * 36; i++) {
+            a32[i] = (float)A[i];
+            b32[i] = (float)B[i];
+        }
+        for (size_t i = 0; i < F * H * 12; i++) {
+            x32[i] = (float)X[i];
+            fk32[i] = (float)FK[i];
+            sc32[i] = (float)SC[i];
+        }
+        add_quantity(r.get(), "added_mass", HB_F32, {F, 6, 6}, a32.data(), a32.size() * 4);
+        add_quantity(r.get(), "radiation_damping", HB_F32, {F, 6, 6}, b32.data(), b32.size() * 4);
+        add_quantity(r.get(), "excitation_diffraction", HB_C64, {F, H, 6}, x32.data(), x32.size() * 4);
+        add_quantity(r.get(), "excitation_froude_krylov", HB_C64, {F, H, 6}, fk32.data(), fk32.size() * 4);
+        add_quantity(r.get(), "excitation_scattering", HB_C64, {F, H, 6}, sc32.data(), sc32.size() * 4);
+        add_quantity(r.get(), "added_mass_f64", HB_F64, {F, 6, 6}, A.data(), A.size() * 8);
+        add_quantity(r.get(), "radiation_damping_f64", HB_F64, {F, 6, 6}, B.data(), B.size() * 8);
+        add_quantity(r.get(), "excitation_diffraction_f64", HB_C128, {F, H, 6}, X.data(), X.size() * 8);
+        add_quantity(r.get(), "excitation_froude_krylov_f64", HB_C128, {F, H, 6}, FK.data(), FK.size() * 8);
+        add_quantity(r.get(), "excitation_scattering_f64", HB_C128, {F, H, 6}, SC.data(), SC.size() * 8);
+        {
+            std::lock_guard<std::mutex> g(model->lock);
+            model->results = std::make_unique<HbResults>(*r);
+        }
+        if (out) *out = r.release();
+        return HB_OK;
+    });
+}
+
+extern "C" void hb_results_free(HbResults* results) { delete results; }
+
+extern "C" HbStatus hb_results_has(HbResults* results, const char* name, int32_t* has) {
+    if (!results || !name || !has) return refuse(HB_ERR_ARGUMENT, "null argument");
+    *has = 0;
+    for (auto& q : results->q)
+        if (q.name == name) *has = 1;
+    return HB_OK;
+}
+
+extern "C" HbStatus hb_results_quantity(HbResults* results, const char* name, HbColumn* column) {
+    if (!results || !name || !column) return refuse(HB_ERR_ARGUMENT, "null argument");
+    for (auto& q : results->q)
+        if (q.name == name) {
+            size_t count = 1;
+            for (size_t d : q.shape) count *= d;
+            *column = HbColumn{q.name.c_str(), q.dtype, q.shape.size(), q.shape.data(), count, q.data.data()};
+            return HB_OK;
+        }
+    return refuse(HB_ERR_VALUE, std::string("no quantity \"") + name + "\" in these results");
+}

@@ -1,0 +1,215 @@
+"""ctypes binding of libhydrobem_gpu.so (include/hydrobem_gpu.h).
+
+Plain pointers and sizes cross the boundary; numpy arrays own the host memory.  The library runs
+the whole path on the GPU and has no CPU fallback: without a CUDA device its solve entry returns
+HB_ERR_UNSUPPORTED, which this module raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libhydrobem_gpu.so"
+
+HB_OK = 0
+STATUS_NAMES = {1: "HB_ERR_VALUE", 2: "HB_ERR_TYPE", 3: "HB_ERR_UNSUPPORTED", 4: "HB_ERR_STATE",
+                5: "HB_ERR_CANCELLED", 6: "HB_ERR_INTERNAL", 7: "HB_ERR_ARGUMENT", 8: "HB_ERR_NUMERICAL",
+                9: "HB_ERR_IO", 10: "HB_ERR_EXISTS"}
+HBG_FP64, HBG_MIXED = 0, 1
+HBG_WET, HBG_INTERIOR = 0, 1
+
+dp = ctypes.POINTER(ctypes.c_double)
+ip = ctypes.POINTER(ctypes.c_int32)
+
+
+class HbgBody(ctypes.Structure):
+    _fields_ = [("n_panels", ctypes.c_int64), ("vertices", dp), ("kinds", ip)]
+
+
+class HbgOutputs(ctypes.Structure):
+    _fields_ = [("added_mass", dp), ("radiation_damping", dp), ("excitation", dp), ("froude_krylov", dp),
+                ("scattering", dp)]
+
+
+class HbgProblem(ctypes.Structure):
+    _fields_ = [("body", HbgBody), ("omegas", dp), ("n_omega", ctypes.c_int64), ("headings_deg", dp),
+                ("n_heading", ctypes.c_int64), ("out", HbgOutputs)]
+
+
+class HbgOptions(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int32), ("logarithmic", ctypes.c_int32), ("log_tolerance", ctypes.c_double),
+                ("gravity", ctypes.c_double), ("density", ctypes.c_double), ("depth", ctypes.c_double),
+                ("max_batch", ctypes.c_int32), ("device", ctypes.c_int32), ("cancel", ip)]
+
+
+class HbLocation(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in ("body", "mesh", "element", "field_point", "lid", "frequency")]
+
+
+class HbColumn(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char_p), ("dtype", ctypes.c_int32), ("ndim", ctypes.c_size_t),
+                ("shape", ctypes.POINTER(ctypes.c_size_t)), ("count", ctypes.c_size_t), ("data", ctypes.c_void_p)]
+
+
+# every symbol include/hydrobem_gpu.h declares
+EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_last_profile", "hbg_last_launch_count",
+           "hbg_profile_kernels", "hbg_kernel_profile", "hb_abi_version",
+           "hb_last_error_message", "hb_last_error_location", "hb_model_new", "hb_model_free", "hb_model_cancel",
+           "hb_object", "hb_add", "hb_set_bool", "hb_set_int", "hb_set_real", "hb_set_text", "hb_set_reals",
+           "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity"]
+
+_lib = None
+
+
+class HydroBEMError(RuntimeError):
+    def __init__(self, status, message, location=None):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+        self.location = location
+
+
+def lib():
+    """The loaded library (built on first use when absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        from . import build as _b
+
+        _b.build()
+    L = ctypes.CDLL(str(LIB_PATH))
+    L.hbg_default_options.argtypes = [ctypes.POINTER(HbgOptions)]
+    L.hbg_default_options.restype = None
+    L.hbg_solve_batch.argtypes = [ctypes.POINTER(HbgProblem), ctypes.c_int64, ctypes.POINTER(HbgOptions)]
+    L.hbg_solve_batch.restype = ctypes.c_int32
+    L.hbg_debug_matrices.argtypes = [ctypes.POINTER(HbgBody), ctypes.c_double, ctypes.POINTER(HbgOptions), dp, dp, dp]
+    L.hbg_debug_matrices.restype = ctypes.c_int32
+    L.hbg_last_profile.argtypes = [dp]
+    L.hbg_profile_kernels.argtypes = [ctypes.c_int32]
+    L.hbg_kernel_profile.argtypes = [ctypes.c_int32, dp, ctypes.POINTER(ctypes.c_int64), dp]
+    L.hbg_last_launch_count.argtypes = [ctypes.POINTER(ctypes.c_int64)]
+    L.hb_last_error_message.restype = ctypes.c_char_p
+    L.hb_last_error_location.argtypes = [ctypes.POINTER(HbLocation)]
+    L.hb_abi_version.restype = ctypes.c_uint32
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != HB_OK:
+        L = lib()
+        loc = HbLocation()
+        L.hb_last_error_location(ctypes.byref(loc))
+        raise HydroBEMError(status, L.hb_last_error_message().decode(errors="replace"),
+                            {f: getattr(loc, f) for f, _ in HbLocation._fields_})
+
+
+def default_options(**kw) -> HbgOptions:
+    o = HbgOptions()
+    lib().hbg_default_options(ctypes.byref(o))
+    for k, v in kw.items():
+        if k == "depth" and (v is None or not np.isfinite(v)):
+            v = float("inf")
+        setattr(o, k, v)
+    return o
+
+
+class Body:
+    """The inputs and output arrays of one body of a batch (kept alive across the call)."""
+
+    def __init__(self, vertices, omegas, headings_deg=(), kinds=None):
+        self.vertices = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 4, 3)
+        self.kinds = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
+        self.omegas = np.ascontiguousarray(omegas, dtype=np.float64).reshape(-1)
+        self.headings = np.ascontiguousarray(headings_deg, dtype=np.float64).reshape(-1)
+        F, H = self.omegas.size, self.headings.size
+        self.A = np.zeros((F, 6, 6))
+        self.B = np.zeros((F, 6, 6))
+        self.X = np.zeros((F, H, 6), dtype=np.complex128)
+        self.FK = np.zeros((F, H, 6), dtype=np.complex128)
+        self.SC = np.zeros((F, H, 6), dtype=np.complex128)
+
+    def problem(self) -> HbgProblem:
+        p = HbgProblem()
+        p.body.n_panels = self.vertices.shape[0]
+        p.body.vertices = self.vertices.ctypes.data_as(dp)
+        p.body.kinds = None if self.kinds is None else self.kinds.ctypes.data_as(ip)
+        p.omegas = self.omegas.ctypes.data_as(dp)
+        p.n_omega = self.omegas.size
+        p.headings_deg = self.headings.ctypes.data_as(dp)
+        p.n_heading = self.headings.size
+        p.out.added_mass = self.A.ctypes.data_as(dp)
+        p.out.radiation_damping = self.B.ctypes.data_as(dp)
+        p.out.excitation = self.X.ctypes.data_as(dp)
+        p.out.froude_krylov = self.FK.ctypes.data_as(dp)
+        p.out.scattering = self.SC.ctypes.data_as(dp)
+        return p
+
+    def results(self):
+        return {"A": self.A, "B": self.B, "X": self.X, "FK": self.FK, "SC": self.SC}
+
+
+def solve_batch(bodies, **options):
+    """Solve a list of Body on the GPU through hbg_solve_batch; returns the list of result dicts."""
+    arr = (HbgProblem * len(bodies))(*[b.problem() for b in bodies])
+    opt = default_options(**options)
+    check(lib().hbg_solve_batch(arr, len(bodies), ctypes.byref(opt)))
+    return [b.results() for b in bodies]
+
+
+def solve(vertices, omegas, headings_deg=(), kinds=None, **options):
+    """One body through the GPU path: dict of A, B [F][6][6], X, FK, SC [F][H][6]."""
+    return solve_batch([Body(vertices, omegas, headings_deg, kinds)], **options)[0]
+
+
+def last_profile():
+    v = (ctypes.c_double * 6)()
+    lib().hbg_last_profile(v)
+    return dict(zip(("statics", "assembly", "lu", "substitution", "forces", "total"), list(v)))
+
+
+def last_launch_count() -> int:
+    c = ctypes.c_int64()
+    lib().hbg_last_launch_count(ctypes.byref(c))
+    return c.value
+
+
+def debug_matrices(vertices, omega, kinds=None, **options):
+    """(statics [N][N][4] with entry [k][j], S, A complex128 [N][N] with entry [k][n]) of one
+    body at one frequency, FP64 form (test support)."""
+    v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 4, 3)
+    k = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
+    N = v.shape[0]
+    body = HbgBody(N, v.ctypes.data_as(dp), None if k is None else k.ctypes.data_as(ip))
+    st = np.zeros((4, N, N))       # plane, j, k  (entry (k, j) at k + j N)
+    S = np.zeros((N, N), dtype=np.complex128)   # [n][k] (column-major)
+    A = np.zeros((N, N), dtype=np.complex128)
+    opt = default_options(**options)
+    check(lib().hbg_debug_matrices(ctypes.byref(body), omega, ctypes.byref(opt), st.ctypes.data_as(dp),
+                                   S.ctypes.data_as(dp), A.ctypes.data_as(dp)))
+    return st.transpose(2, 1, 0), S.T, A.T
+
+
+KERNEL_FAMILIES = ["geometry", "statics", "statics_adaptive", "fd_tiles", "assemble", "boundary", "rhs", "lu_panel",
+                   "lu_laswp", "lu_trsm", "lu_gemm", "lu_solve", "forces", "mixed_convert", "mixed_gemm",
+                   "mixed_residual"]
+FLOP_FAMILIES = {"lu_panel", "lu_trsm", "lu_gemm", "mixed_gemm"}
+
+
+def profile_kernels(on: bool) -> None:
+    lib().hbg_profile_kernels(1 if on else 0)
+
+
+def kernel_profile():
+    """{family: (ms, launches, work)} of the last solve of this thread."""
+    out = {}
+    for i, name in enumerate(KERNEL_FAMILIES):
+        ms, n, w = ctypes.c_double(), ctypes.c_int64(), ctypes.c_double()
+        lib().hbg_kernel_profile(i, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(w))
+        out[name] = (ms.value, n.value, w.value)
+    return out

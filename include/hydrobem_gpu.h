@@ -1,0 +1,219 @@
+/*
+ * hydrobem_gpu.h -- C ABI of libhydrobem_gpu.so, the B200 implementation of HydroBEM's low-order
+ * frequency-domain hot path: per-frequency assembly of the source and dipole influence matrices,
+ * the dense complex solve for the radiation and diffraction potentials, and the pressure
+ * integration to added mass, radiation damping and exciting force.
+ *
+ * Two layers:
+ *  1. The model/solve/results subset of the reference's ABI (crates/hydrobem-c/include/hydrobem.h),
+ *     same names, status codes and conventions, for the items of the low-order open-sea route.
+ *  2. The batched entry hbg_solve_batch, which the model layer calls and which a caller with many
+ *     bodies and frequencies can use directly (it mirrors solve_frequency,
+ *     crates/hydrobem/src/lo_frequency.rs:1565-1576, run over whole frequency batches).
+ *
+ * Conventions (as docs/reference/c-api.md:49-146): every call returns an HbStatus; a failed call
+ * sets a per-thread message (hb_last_error_message); out-pointers are checked first, so a refused
+ * call changes nothing; arrays are C order, complex values (re, im) pairs; exceptions never cross
+ * the boundary.  No torch types anywhere: plain pointers and sizes.
+ */
+#ifndef HYDROBEM_GPU_H
+#define HYDROBEM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status: the codes of hydrobem.h:42-98 */
+typedef int32_t HbStatus;
+#define HB_OK 0
+#define HB_ERR_VALUE 1
+#define HB_ERR_TYPE 2
+#define HB_ERR_UNSUPPORTED 3
+#define HB_ERR_STATE 4
+#define HB_ERR_CANCELLED 5
+#define HB_ERR_INTERNAL 6
+#define HB_ERR_ARGUMENT 7
+#define HB_ERR_NUMERICAL 8
+#define HB_ERR_IO 9
+#define HB_ERR_EXISTS 10
+
+/* ---- element types of HbColumn (hydrobem.h:116-151) */
+#define HB_F64 1
+#define HB_F32 2
+#define HB_I32 3
+#define HB_I64 4
+#define HB_U64 5
+#define HB_C64 6
+#define HB_C128 7
+
+/* The version of this library's ABI (its own numbering; the reference's hb_abi_version is 8). */
+#define HBG_ABI_VERSION 1
+
+/* ==================================================================== batched entry */
+
+/* precision forms of the solve */
+#define HBG_FP64 0  /* FP64 assembly, FP64 LU: the correctness oracle form */
+#define HBG_MIXED 1 /* complex64 matrices, reduced-precision tensor-core LU, FP64 refinement */
+
+/* panel kinds (crates/hydrobem/src/low_order.rs:224-238; only these reach this route) */
+#define HBG_WET 0      /* wetted body surface */
+#define HBG_INTERIOR 1 /* interior free surface z = 0 (irregular-frequency removal) */
+
+/* One body: n_panels quadrilaterals, vertices [n_panels][4][3] (a triangle repeats its last
+ * vertex, the right-hand-rule normal into the fluid: docs/reference/inputs-meshes.md §1);
+ * kinds [n_panels] or NULL (all wet).  Rigid modes about the origin, body frame = global frame. */
+typedef struct HbgBody {
+    int64_t n_panels;
+    const double *vertices;
+    const int32_t *kinds;
+} HbgBody;
+
+/* Outputs of one body, caller-allocated host arrays (NULL: not wanted), float64:
+ *   added_mass, radiation_damping  [n_omega][6][6]   (coordinate i, radiation mode j)
+ *   excitation, froude_krylov, scattering  [n_omega][n_heading][6][2]  (re, im)          */
+typedef struct HbgOutputs {
+    double *added_mass;
+    double *radiation_damping;
+    double *excitation;
+    double *froude_krylov;
+    double *scattering;
+} HbgOutputs;
+
+typedef struct HbgProblem {
+    HbgBody body;
+    const double *omegas; /* rad/s, > 0 and finite */
+    int64_t n_omega;
+    const double *headings_deg;
+    int64_t n_heading;
+    HbgOutputs out;
+} HbgProblem;
+
+typedef struct HbgOptions {
+    int32_t precision;            /* HBG_FP64 or HBG_MIXED */
+    int32_t logarithmic;          /* analytic log-singularity integral (default 1) */
+    double log_tolerance;         /* default 1e-4 */
+    double gravity;               /* default 9.80665 */
+    double density;               /* default 1000 */
+    double depth;                 /* <= 0 or inf: infinite depth */
+    int32_t max_batch;            /* frequencies per device batch; 0: from free memory */
+    int32_t device;               /* CUDA device ordinal */
+    const volatile int32_t *cancel; /* optional: nonzero cancels between batches (HB_ERR_CANCELLED) */
+} HbgOptions;
+
+/* Defaults of the reference's schema (document_schema.rs:202-232). */
+void hbg_default_options(HbgOptions *opt);
+
+/* Solve every frequency and heading of every problem on the GPU.
+ * Replaces: SolveJob::run -> solver::solve -> run_frequencies -> solve_frequency
+ * (crates/hydrobem/src/model_solve.rs:310-370, solver.rs:265-345, lo_frequency.rs:1565-1635). */
+HbStatus hbg_solve_batch(const HbgProblem *problems, int64_t n_problems, const HbgOptions *opt);
+
+/* Timing of the phases of the last hbg_solve_batch of this thread, in milliseconds of device time
+ * (the phase times of HB_PROFILE, low_order.rs:184-208): [statics, assembly, lu, substitution,
+ * forces, total]. */
+HbStatus hbg_last_profile(double *ms6);
+
+/* Kernel-family timing of this thread's solves (the kernel-level counterpart of HB_PROFILE,
+ * low_order.rs:184-208): on != 0 records CUDA events around every launch on the solve's stream.
+ * hbg_kernel_profile: for family 0..15 (geometry, statics, statics_adaptive, fd_tiles, assemble,
+ * boundary, rhs, lu_panel, lu_laswp, lu_trsm, lu_gemm, lu_solve, forces, mixed_convert, mixed_gemm,
+ * mixed_residual) the summed device milliseconds of the last hbg_solve_batch (0 when timing is
+ * off), its launches, and its algorithmic work (bytes for the memory-bound families, real flops for
+ * lu_panel, lu_trsm, lu_gemm and mixed_gemm). */
+HbStatus hbg_profile_kernels(int32_t on);
+HbStatus hbg_kernel_profile(int32_t family, double *ms, int64_t *launches, double *work);
+
+/* The kernels launched by the last hbg_solve_batch of this thread. */
+HbStatus hbg_last_launch_count(int64_t *count);
+
+/* Test support: the static influence data (planes rs, rd, dl, dd; entry (k, j) at k + j N of each
+ * plane, N*N doubles per plane) and the matrices S and A = 2 pi I - D (column-major complex128,
+ * N*N (re, im) pairs) of one body at one frequency, FP64 form.  Any output pointer may be NULL.
+ * Replaces no reference interface (it exposes compute_static, lo_static.rs:254-308, and
+ * Frequency::matrices, lo_frequency.rs:276-312, for the parity tests). */
+HbStatus hbg_debug_matrices(const HbgBody *body, double omega, const HbgOptions *opt, double *statics, double *S,
+                            double *A);
+
+/* ==================================================================== reference ABI subset */
+
+typedef struct HbModel HbModel;
+typedef struct HbResults HbResults;
+
+typedef struct HbLocation {
+    int64_t body;
+    int64_t mesh;
+    int64_t element;
+    int64_t field_point;
+    int64_t lid;
+    int64_t frequency;
+} HbLocation;
+
+typedef struct HbColumn {
+    const char *name;
+    int32_t dtype;
+    size_t ndim;
+    const size_t *shape;
+    size_t count;
+    const void *data;
+} HbColumn;
+
+typedef struct HbProgress {
+    int32_t stage;
+    int64_t frequency;
+    uint64_t stage_done;
+    uint64_t stage_total;
+    uint64_t frequencies_done;
+    uint64_t frequencies_total;
+    double seconds;
+    int32_t worker;
+    int32_t phase;
+    int32_t step;
+    int64_t item;
+} HbProgress;
+
+typedef int32_t (*HbProgressFn)(const HbProgress *progress, void *user);
+
+#define HB_NO_OBJECT UINT64_MAX
+
+/* hydrobem.h:233 */
+uint32_t hb_abi_version(void);
+/* hydrobem.h:247, 256 */
+const char *hb_last_error_message(void);
+HbStatus hb_last_error_location(HbLocation *location);
+/* hydrobem.h:507, 557 */
+HbStatus hb_model_new(HbModel **out);
+HbStatus hb_model_free(HbModel *model);
+/* hydrobem.h:574 */
+HbStatus hb_model_cancel(HbModel *model);
+/* hydrobem.h:670: "" the model, "environment", "options", "bodies/<name>" */
+HbStatus hb_object(HbModel *model, const char *path, uint64_t *object);
+/* hydrobem.h:698: a body in the list "bodies" of the model */
+HbStatus hb_add(HbModel *model, uint64_t parent, const char *list, const char *type_name, const char *name,
+                int64_t index, uint64_t *out);
+/* hydrobem.h:764-814: the items of the route (environment: omegas, periods, headings, depth,
+ * gravity, density; body: vertices [P][4][3] (its mesh), kinds; options: logarithmic_integration,
+ * log_tolerance, precision ("fp64" | "mixed"), device) */
+HbStatus hb_set_bool(HbModel *model, uint64_t object, const char *item, int32_t value);
+HbStatus hb_set_int(HbModel *model, uint64_t object, const char *item, int64_t value);
+HbStatus hb_set_real(HbModel *model, uint64_t object, const char *item, double value);
+HbStatus hb_set_text(HbModel *model, uint64_t object, const char *item, const char *value);
+HbStatus hb_set_reals(HbModel *model, uint64_t object, const char *item, const double *data, const size_t *shape,
+                      size_t ndim);
+HbStatus hb_set_ints(HbModel *model, uint64_t object, const char *item, const int64_t *data, const size_t *shape,
+                     size_t ndim);
+/* hydrobem.h:646 */
+HbStatus hb_model_solve(HbModel *model, HbProgressFn progress, void *user, HbResults **out);
+/* hydrobem.h:1146, 1154, 1164: quantities omegas, headings, added_mass and radiation_damping
+ * (HB_F32 [F][D][K]), excitation_diffraction, excitation_froude_krylov, excitation_scattering
+ * (HB_C64 [F][H][D]); the extension quantities <name>_f64 (HB_F64 / HB_C128) keep double precision. */
+void hb_results_free(HbResults *results);
+HbStatus hb_results_has(HbResults *results, const char *name, int32_t *has);
+HbStatus hb_results_quantity(HbResults *results, const char *name, HbColumn *column);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
