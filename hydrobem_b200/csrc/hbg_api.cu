@@ -189,7 +189,7 @@ static DeviceCtx& device_ctx(int dev) {
 
 // ------------------------------------------------------------------ finite-depth scalars (host)
 // dispersion.rs:19-95
-static double dispersion_x0(double H) {
+double dispersion_x0(double H) {
     if (!(H > 0.0)) return 0.0;
     if (H >= 40.0) return H;
     double lo = std::max(H, std::sqrt(H)), hi = 0.5 * (H + std::sqrt(H * H + 4.0 * H));
@@ -231,7 +231,7 @@ static double dispersion_xn(double H, int n) {
 }
 
 // green_fin.rs:345-392 region coefficients and power table, 874-934 make_finite_depth (ordinary)
-static void make_fd_params(double h, double K, FdParams& fd) {
+void make_fd_params(double h, double K, FdParams& fd) {
     const HostTables& ht = host_tables();
     const double *meta = ht.arr[4], *Q = ht.arr[5], *L0 = ht.arr[6];
     memset(&fd, 0, sizeof fd);
@@ -308,28 +308,6 @@ struct DevBuf {
     template <class T>
     T* as() const {
         return reinterpret_cast<T*>(p);
-    }
-};
-
-struct EventTimer {
-    cudaEvent_t a{}, b{};
-    cudaStream_t s;
-    double* acc;
-    EventTimer(cudaStream_t st, double* target) : s(st), acc(target) {
-        cudaEventCreate(&a);
-        cudaEventCreate(&b);
-        cudaEventRecord(a, s);
-    }
-    void stop() {
-        cudaEventRecord(b, s);
-        cudaEventSynchronize(b);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, a, b);
-        *acc += ms;
-    }
-    ~EventTimer() {
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
     }
 };
 
@@ -525,8 +503,8 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
             double2* dSC = dFK + (size_t)H * 6 * nb;
             KernelProfiler& P = profiler();
             P.begin(s);
-            launch_forces(pv, nb, dfi.as<FreqInfo>(), H, dX.as<double2>(), dphiI.as<double2>(), opt.density, dAo, dBo,
-                          dXo, dFK, dSC, s);
+            launch_forces(pv, nb, dfi.as<FreqInfo>(), H, dX.as<double2>(), N, dphiI.as<double2>(), opt.density, dAo,
+                          dBo, dXo, dFK, dSC, s);
             P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
             g_launches += 1;
             CUDA_OK(cudaMemcpyAsync(hout.data(), dout.p, out_per * nb, cudaMemcpyDeviceToHost, s));
@@ -729,6 +707,28 @@ extern "C" HbStatus hbg_debug_matrices(const HbgBody* body, double omega, const 
     } catch (...) {
         return fail({HB_ERR_INTERNAL, "internal error"});
     }
+}
+
+extern "C" HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const float* A, const float* B, float* C) {
+    try {
+        if (!A || !B || !C) return fail({HB_ERR_ARGUMENT, "null argument"});
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            return fail({HB_ERR_UNSUPPORTED, "no CUDA device: this library runs the path on the GPU only"});
+        device_ctx(0);
+        const char* msg = "";
+        int rc = debug_gemm_tf32(M, N, K, A, B, C, &msg);
+        if (rc) return fail({rc, msg});
+        return HB_OK;
+    } catch (const Failure& f) {
+        return fail(f);
+    }
+}
+
+extern "C" HbStatus hbg_last_ir_iterations(int32_t* n) {
+    if (!n) return fail({HB_ERR_ARGUMENT, "null argument"});
+    *n = last_ir_iterations();
+    return HB_OK;
 }
 
 extern "C" const char* hb_last_error_message(void) { return g_error.c_str(); }

@@ -135,13 +135,39 @@ __device__ __forceinline__ double free_term(int kind) { return kind == 1 ? -4.0 
 // unordered pair (G(x, xi) = G(xi, x), the swapped source derivative for (n, k):
 // lo_frequency.rs:399-537), the (n, k) statics read and the (n, k) entries written through shared
 // memory transposes so that every global access is coalesced along the rows.
-template <bool FINITE>
-__global__ void __launch_bounds__(256) k_assemble_f64(PanelsView pv, const double* __restrict__ st,
-                                                      const FreqInfo* __restrict__ fi,
-                                                      const FdParams* __restrict__ fdp,
-                                                      const double* __restrict__ tiles,
-                                                      const double* __restrict__ fpt, double2* __restrict__ S,
-                                                      double2* __restrict__ A, size_t mat_stride) {
+// Output policies of the assembly: complex128 column-major N x N (the FP64 form), or two FP32 planes
+// column-major with leading dimension Np (the mixed form; entry (k, n) at n Np + k).
+struct OutF64 {
+    double2* S;
+    double2* A;
+    size_t stride;
+    int N;
+    __device__ __forceinline__ void put(int f, int k, int n, double2 s, double2 a) const {
+        size_t o = (size_t)f * stride + (size_t)k + (size_t)n * N;
+        S[o] = s;
+        A[o] = a;
+    }
+};
+
+struct OutF32 {
+    float* S;
+    float* A;
+    size_t bstride;  // per frequency: two planes of Np * Np
+    int Np;
+    __device__ __forceinline__ void put(int f, int k, int n, double2 s, double2 a) const {
+        size_t o = (size_t)f * bstride + (size_t)n * Np + k, pl = (size_t)Np * Np;
+        S[o] = (float)s.x;
+        S[o + pl] = (float)s.y;
+        A[o] = (float)a.x;
+        A[o + pl] = (float)a.y;
+    }
+};
+
+template <bool FINITE, class Out>
+__global__ void __launch_bounds__(256) k_assemble(PanelsView pv, const double* __restrict__ st,
+                                                  const FreqInfo* __restrict__ fi, const FdParams* __restrict__ fdp,
+                                                  const double* __restrict__ tiles, const double* __restrict__ fpt,
+                                                  Out out) {
     // statics (n, k) [q][k_local][n_local]; each (k_local, n_local) slot is read and then
     // overwritten with the results (S, A) of entry (n, k) by the one thread that owns it
     __shared__ double sT[4][32][33];
@@ -160,8 +186,6 @@ __global__ void __launch_bounds__(256) k_assemble_f64(PanelsView pv, const doubl
     const size_t NN = (size_t)N * N;
     const FreqInfo info = fi[f];
     const double K = info.K, logc = info.logc;
-    S += (size_t)f * mat_stride;
-    A += (size_t)f * mat_stride;
     // statics of (n, k): rows n in N0, panels k in K0
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -211,8 +235,7 @@ __global__ void __launch_bounds__(256) k_assemble_f64(PanelsView pv, const doubl
         double2 s1, d1;
         apply_kernel(__ldg(st + o1), __ldg(st + NN + o1), __ldg(st + 2 * NN + o1), __ldg(st + 3 * NN + o1), an,
                      nn3[0], nn3[1], nn3[2], kindn, xk, xn, K, logc, w, R, false, s1, d1);
-        S[o1] = s1;
-        A[o1] = make_double2((k == n ? free_term(kindk) : 0.0) - d1.x, -d1.y);
+        out.put(f, k, n, s1, make_double2((k == n ? free_term(kindk) : 0.0) - d1.x, -d1.y));
         if (n != k) {
             double2 s2, d2;
             apply_kernel(sT[0][tx][nl], sT[1][tx][nl], sT[2][tx][nl], sT[3][tx][nl], ak, nk[0], nk[1], nk[2], kindk,
@@ -228,11 +251,8 @@ __global__ void __launch_bounds__(256) k_assemble_f64(PanelsView pv, const doubl
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         int n = N0 + tx, kl = ty + 8 * i, kk = K0 + kl;
-        if (n < N && kk < N && (kb != nb || n > kk)) {
-            size_t o2 = (size_t)n + (size_t)kk * N;
-            S[o2] = make_double2(sT[0][kl][tx], sT[1][kl][tx]);
-            A[o2] = make_double2(sT[2][kl][tx], sT[3][kl][tx]);
-        }
+        if (n < N && kk < N && (kb != nb || n > kk))
+            out.put(f, n, kk, make_double2(sT[0][kl][tx], sT[1][kl][tx]), make_double2(sT[2][kl][tx], sT[3][kl][tx]));
     }
 }
 
@@ -241,10 +261,23 @@ void launch_assemble_f64(const PanelsView& pv, const double* st, int F, const Fr
                          size_t mat_stride, cudaStream_t s) {
     int nt = (pv.N + 31) / 32;
     dim3 grid(nt * (nt + 1) / 2, F);
+    OutF64 o{S, A, mat_stride, pv.N};
     if (finite)
-        k_assemble_f64<true><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, S, A, mat_stride);
+        k_assemble<true, OutF64><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
     else
-        k_assemble_f64<false><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, S, A, mat_stride);
+        k_assemble<false, OutF64><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
+}
+
+void launch_assemble_f32(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
+                         const double* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
+                         cudaStream_t s) {
+    int nt = (pv.N + 31) / 32;
+    dim3 grid(nt * (nt + 1) / 2, F);
+    OutF32 o{S, A, 2 * (size_t)Np * Np, Np};
+    if (finite)
+        k_assemble<true, OutF32><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
+    else
+        k_assemble<false, OutF32><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
 }
 
 // ------------------------------------------------------------------ boundary values
@@ -355,14 +388,15 @@ void launch_rhs_f64(int N, int F, int nrhs, const double2* S, size_t mat_stride,
 // B = -w Im(-rho z); X = i w rho sum n_i (phi_S + phi_I) A_j, FK the phi_I part, SC = X - FK.
 // One block per frequency; fixed-order block reductions (deterministic).
 __global__ void __launch_bounds__(256) k_forces(PanelsView pv, const FreqInfo* __restrict__ fi, int H,
-                                                const double2* __restrict__ phi, const double2* __restrict__ phiI,
+                                                const double2* __restrict__ phi, int ldphi,
+                                                const double2* __restrict__ phiI,
                                                 double rho, double* __restrict__ Aout, double* __restrict__ Bout,
                                                 double2* __restrict__ X, double2* __restrict__ FK,
                                                 double2* __restrict__ SC) {
     __shared__ double red[256];
     int f = blockIdx.x, N = pv.N;
     int nrhs = 6 + H;
-    const double2* pf = phi + (size_t)f * nrhs * N;
+    const double2* pf = phi + (size_t)f * nrhs * ldphi;
     const double2* pif = phiI + (size_t)f * H * N;
     double w = fi[f].omega;
     auto block_sum = [&](double v) -> double {
@@ -391,7 +425,7 @@ __global__ void __launch_bounds__(256) k_forces(PanelsView pv, const FreqInfo* _
                 double wgt = nj * pv.at(P_AREA, j);
                 double2 v;
                 if (col < 6 + H) {
-                    v = pf[(size_t)col * N + j];
+                    v = pf[(size_t)col * ldphi + j];
                     if (col >= 6) {
                         double2 pI = pif[(size_t)(col - 6) * N + j];
                         v.x += pI.x;
@@ -428,9 +462,10 @@ __global__ void __launch_bounds__(256) k_forces(PanelsView pv, const FreqInfo* _
     }
 }
 
-void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, const double2* phiI,
-                   double rho, double* A, double* B, double2* X, double2* FK, double2* SC, cudaStream_t s) {
-    k_forces<<<F, 256, 0, s>>>(pv, fi, H, phi, phiI, rho, A, B, X, FK, SC);
+void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, int ldphi,
+                   const double2* phiI, double rho, double* A, double* B, double2* X, double2* FK, double2* SC,
+                   cudaStream_t s) {
+    k_forces<<<F, 256, 0, s>>>(pv, fi, H, phi, ldphi, phiI, rho, A, B, X, FK, SC);
 }
 
 }  // namespace hbg

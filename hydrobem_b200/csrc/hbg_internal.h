@@ -61,6 +61,37 @@ struct KernelProfiler {
 
 KernelProfiler& profiler();
 
+// Refinement iterations of the last mixed-precision batch of this thread.
+inline int& last_ir_iterations() {
+    static thread_local int n = 0;
+    return n;
+}
+
+// Device time of a phase: events on the stream, added to *acc at stop().
+struct EventTimer {
+    cudaEvent_t a{}, b{};
+    cudaStream_t s;
+    double* acc;
+    EventTimer(cudaStream_t st, double* target) : s(st), acc(target) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, s);
+    }
+    void stop() {
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        *acc += ms;
+    }
+    ~EventTimer() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+};
+
+
+
 // Per-frequency data of one batch entry (one body, one omega).
 struct FreqInfo {
     double omega, K, k;   // radian frequency, K = omega^2 / g, incident wave number
@@ -82,6 +113,9 @@ void launch_fin_points(const PanelsView& pv, int F, const FdParams* fd, double* 
 void launch_assemble_f64(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
                          const double* tiles, const double* fpt, bool finite, double2* S, double2* A,
                          size_t mat_stride, cudaStream_t s);
+void launch_assemble_f32(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
+                         const double* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
+                         cudaStream_t s);
 // boundary values u [F][nrhs][N] and incident wave phiI [F][H][N]
 void launch_boundary(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double* heads, double depth,
                      double grav, double2* u, double2* phiI, cudaStream_t s);
@@ -89,8 +123,12 @@ void launch_boundary(const PanelsView& pv, int F, const FreqInfo* fi, int H, con
 void launch_rhs_f64(int N, int F, int nrhs, const double2* S, size_t mat_stride, const double2* u, double2* rhs,
                     cudaStream_t s);
 // forces: out[F][...] A, B [6][6], X, FK, SC [H][6] complex, all f64
-void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, const double2* phiI,
-                   double rho, double* A, double* B, double2* X, double2* FK, double2* SC, cudaStream_t s);
+void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, int ldphi,
+                   const double2* phiI, double rho, double* A, double* B, double2* X, double2* FK, double2* SC,
+                   cudaStream_t s);
+// host-side finite-depth scalars of one ordinary frequency (green_fin.rs:874-934)
+void make_fd_params(double h, double K, FdParams& fd);
+double dispersion_x0(double H);
 
 // plain FP64 LU with partial pivoting, batched over F matrices (in place), and the solve
 int lu_factor_f64(int N, int F, double2* A, size_t mat_stride, int32_t* ipiv, int32_t* info, cudaStream_t s,

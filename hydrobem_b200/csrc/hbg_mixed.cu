@@ -1,13 +1,398 @@
-// hbg_mixed.cu -- the mixed-precision form (placeholder until its kernels land).
+// hbg_mixed.cu -- the mixed-precision form of the frequency solve: the pair kernels in FP64 as in
+// the FP64 form, the matrices stored as complex64 (two FP32 planes), the LU on the tensor cores
+// (tcgen05 kind::tf32, FP32 accumulation, no pivoting), the right-hand sides and the residuals
+// accumulated in FP64, and iterative refinement until the correction is below 1e-12 of the solution.
+// The result is the solution of the complex64-rounded system (the reference's production path
+// stores its matrices in complex64 too, lo_frequency.rs:1-6).
+#include <cuda.h>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
 #include "hbg_mixed.h"
+#include "hbg_mixed_kernels.cuh"
 
 namespace hbg {
 
-int mixed_solve_frequencies(const PanelsView&, const double*, const HbgProblem&, const HbgOptions&, bool, double,
-                            cudaStream_t, double*, int64_t*, const char** msg, int64_t* freq) {
-    *msg = "the mixed-precision form is not built yet";
-    *freq = -1;
-    return HB_ERR_UNSUPPORTED;
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// A 4-D FP32 tensor map (x innermost) with a {32, box_rows, 1, 1} box in the 128-byte swizzle.
+static bool make_map(CUtensorMap* m, void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t d3, uint64_t s1,
+                     uint64_t s2, uint64_t s3, uint32_t box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[4] = {d0, d1, d2, d3};
+    cuuint64_t strides[3] = {s1, s2, s3};
+    cuuint32_t box[4] = {32, box_rows, 1, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
+struct MixedBuffers {
+    void* p[24] = {};
+    int n = 0;
+    ~MixedBuffers() {
+        for (int i = 0; i < n; i++)
+            if (p[i]) cudaFree(p[i]);
+    }
+    template <class T>
+    T* get(size_t count) {
+        void* q = nullptr;
+        if (cudaMalloc(&q, count * sizeof(T)) != cudaSuccess) return nullptr;
+        p[n++] = q;
+        return reinterpret_cast<T*>(q);
+    }
+};
+
+#define MIXED_FAIL(code, text, fq) \
+    do {                           \
+        *msg = text;               \
+        *freq = fq;                \
+        return code;               \
+    } while (0)
+
+int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgProblem& pr, const HbgOptions& opt,
+                            bool fin, double depth, cudaStream_t s, double* prof, int64_t* launches, const char** msg,
+                            int64_t* freq) {
+    KernelProfiler& P = profiler();
+    const int N = pv.N, F = (int)pr.n_omega, H = (int)pr.n_heading, nrhs = 6 + H;
+    const int Np = (N + NBL - 1) / NBL * NBL;
+    const size_t NP2 = (size_t)Np * Np, MB = 2 * NP2;  // floats per matrix (two planes)
+    if (nrhs > 32) MIXED_FAIL(HB_ERR_UNSUPPORTED, "more than 26 headings per solve", -1);
+    if (!encode_fn()) MIXED_FAIL(HB_ERR_UNSUPPORTED, "the driver offers no tensor-map encoder (TMA)", -1);
+    // ---- batch size from free memory
+    // GEMM operand buffers of the block row (rows 2n <= 2 (Np - NBL), 2 NBL wide), per frequency
+    const size_t prep_rows = std::max<size_t>(2 * (size_t)(Np - NBL), GBN);
+    const size_t prep = prep_rows * 2 * NBL;
+    size_t per = 3 * MB * 4 + 2 * prep * 4 + (size_t)(NBL * 2 * NBL + 4 * NBL * NBL) * 4 +
+                 (size_t)(nrhs + H) * N * 16 + 4 * (size_t)nrhs * Np * 16 + 64 +
+                 (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)FP_PLANES * N * 8 + (size_t)6912 * 3 * 8 : 0);
+    size_t freeb = 0, totalb = 0;
+    if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "cudaMemGetInfo failed", -1);
+    int B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)freeb) / per);
+    if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
+    B = std::min(B, F);
+    MixedBuffers mb;
+    float* S32 = mb.get<float>(MB * B);
+    float* A32 = mb.get<float>(MB * B);
+    float* W = mb.get<float>(MB * B);
+    float* P2 = mb.get<float>(prep * B);
+    float* P3 = mb.get<float>(prep * B);
+    float* PL = mb.get<float>((size_t)NBL * 2 * NBL * B);
+    float* PU = mb.get<float>((size_t)4 * NBL * NBL * B);
+    double2* u = mb.get<double2>((size_t)nrhs * N * B);
+    double2* phiI = mb.get<double2>((size_t)std::max(H, 1) * N * B);
+    double2* b = mb.get<double2>((size_t)nrhs * Np * B);
+    double2* x = mb.get<double2>((size_t)nrhs * Np * B);
+    double2* r = mb.get<double2>((size_t)nrhs * Np * B);
+    double* norms = mb.get<double>(2 * (size_t)B);
+    int* err = mb.get<int>(1);
+    FreqInfo* dfi = mb.get<FreqInfo>(B);
+    FdParams* dfd = mb.get<FdParams>(B);
+    double* dheads = mb.get<double>(std::max(H, 1));
+    double* tiles = fin ? mb.get<double>((size_t)(T1_SIZE + T2_SIZE) * B) : nullptr;
+    double* scr = fin ? mb.get<double>((size_t)6912 * 3 * B) : nullptr;
+    double* fpt = fin ? mb.get<double>((size_t)FP_PLANES * N * B) : nullptr;
+    double* dout = mb.get<double>((72 + 3 * (size_t)H * 12) * B);
+    if (!S32 || !A32 || !W || !P2 || !P3 || !PL || !PU || !u || !phiI || !b || !x || !r || !norms || !err || !dfi ||
+        !dfd || !dheads || !dout || (fin && (!tiles || !scr || !fpt)))
+        MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
+    // ---- tensor maps (whole batch; the batch index is the 4th coordinate)
+    CUtensorMap mapW, mapPL, mapPU, mapP2, mapP3;
+    const uint64_t fb = 4;  // bytes per float
+    bool okm = make_map(&mapW, W, Np, Np, 2, B, Np * fb, NP2 * fb, MB * fb, GBM) &&
+               make_map(&mapPL, PL, 2 * NBL, NBL, 1, B, 2 * NBL * fb, (uint64_t)NBL * 2 * NBL * fb,
+                        (uint64_t)NBL * 2 * NBL * fb, GBM) &&
+               make_map(&mapPU, PU, 2 * NBL, 2 * NBL, 1, B, 2 * NBL * fb, (uint64_t)4 * NBL * NBL * fb,
+                        (uint64_t)4 * NBL * NBL * fb, GBN) &&
+               make_map(&mapP2, P2, 2 * NBL, prep_rows, 1, B, 2 * NBL * fb, prep * fb, prep * fb, GBN) &&
+               make_map(&mapP3, P3, 2 * NBL, prep_rows, 1, B, 2 * NBL * fb, prep * fb, prep * fb, GBN);
+    if (!okm) MIXED_FAIL(HB_ERR_INTERNAL, "tensor-map encoding failed", -1);
+    const int smem = (int)gemm_smem_bytes();
+    cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int dsmem = NBL * (NBL + 1) * (int)sizeof(float2);
+    cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, dsmem);
+    std::vector<double> heads(std::max(H, 1));
+    for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
+    cudaMemcpyAsync(dheads, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(S32, 0, MB * B * 4, s);
+    cudaMemsetAsync(A32, 0, MB * B * 4, s);
+    std::vector<FreqInfo> fi(B);
+    std::vector<FdParams> fdh(B);
+    const size_t out_per = 72 + 3 * (size_t)H * 12;
+    std::vector<double> hout(out_per * B), hn(2 * (size_t)B);
+    auto gemm = [&](const CUtensorMap& mA, const CUtensorMap& mB, GemmArgs g, int nb) {
+        dim3 grid((g.M + GBM - 1) / GBM, (g.Nc + GBN - 1) / GBN, nb);
+        P.begin(s);
+        k_gemm_tf32<<<grid, 128, smem, s>>>(mA, mB, g);
+        P.end(KF_MIXED_GEMM, 2.0 * g.M * (double)g.Nc * g.Kp * nb, s);
+        (*launches)++;
+    };
+    for (int f0 = 0; f0 < F; f0 += B) {
+        if (opt.cancel && *opt.cancel) MIXED_FAIL(HB_ERR_CANCELLED, "the solve was cancelled", f0);
+        const int nb = std::min(B, F - f0);
+        for (int i = 0; i < nb; i++) {
+            double w = pr.omegas[f0 + i], K = w * w / opt.gravity;
+            fi[i].omega = w;
+            fi[i].K = K;
+            fi[i].k = fin ? dispersion_x0(K * depth) / depth : K;
+            fi[i].logc = opt.logarithmic ? 1.0 : 0.0;
+            if (fin) make_fd_params(depth, K, fdh[i]);
+        }
+        cudaMemcpyAsync(dfi, fi.data(), sizeof(FreqInfo) * nb, cudaMemcpyHostToDevice, s);
+        if (fin) cudaMemcpyAsync(dfd, fdh.data(), sizeof(FdParams) * nb, cudaMemcpyHostToDevice, s);
+        cudaMemsetAsync(err, 0, sizeof(int), s);
+        // ---- assembly, boundary values, right-hand sides
+        {
+            EventTimer t(s, &prof[1]);
+            if (fin) {
+                P.begin(s);
+                launch_fd_tiles(nb, dfd, tiles, scr, s);
+                launch_fin_points(pv, nb, dfd, fpt, s);
+                P.end(KF_FD_TILES, 0.0, s);
+                *launches += 3;
+            }
+            P.begin(s);
+            launch_assemble_f32(pv, st, nb, dfi, dfd, tiles, fpt, fin, S32, A32, Np, s);
+            // algorithmic bytes per pair: 4 FP64 statics read (32 B), S and A written as complex64 (16 B)
+            P.end(KF_ASSEMBLE, 48.0 * (double)N * N * nb, s);
+            if (Np > N) k_pad_identity<<<dim3(64, nb), 256, 0, s>>>(A32, N, Np, MB);
+            cudaMemcpyAsync(W, A32, MB * nb * 4, cudaMemcpyDeviceToDevice, s);
+            P.begin(s);
+            launch_boundary(pv, nb, dfi, H, dheads, depth, opt.gravity, u, phiI, s);
+            P.end(KF_BOUNDARY, 0.0, s);
+            cudaMemsetAsync(b, 0, sizeof(double2) * nrhs * Np * nb, s);
+            P.begin(s);
+            dim3 g((N + 127) / 128, nb);
+            if (nrhs <= 16)
+                k_cgemv_f32<16><<<g, 128, 0, s>>>(N, Np, MB, nrhs, S32, u, N, nullptr, 0, b, Np);
+            else
+                k_cgemv_f32<32><<<g, 128, 0, s>>>(N, Np, MB, nrhs, S32, u, N, nullptr, 0, b, Np);
+            P.end(KF_RHS, 8.0 * (double)N * N * nb, s);
+            *launches += 3 + (Np > N);
+            t.stop();
+        }
+        // ---- LU of M = A^T without pivoting, blocked by NBL, the products on the tensor cores
+        {
+            EventTimer t(s, &prof[2]);
+            for (int k0 = 0; k0 < Np; k0 += NBL) {
+                const int n = Np - k0 - NBL;
+                P.begin(s);
+                k_diag_factor<<<nb, 1024, dsmem, s>>>(W, Np, MB, k0, PL, PU, err);
+                P.end(KF_LU_PANEL, 8.0 * NBL * (double)NBL * NBL * nb, s);
+                (*launches)++;
+                if (n == 0) break;
+                P.begin(s);
+                k_prep_block_row<<<dim3(n / 32, NBL / 32, nb), dim3(32, 8), 0, s>>>(W, Np, MB, k0, n, P2, prep);
+                P.end(KF_MIXED_CONVERT, 2.0 * NBL * (double)n * 4 * 3 * nb, s);
+                GemmArgs g{};
+                g.err = err;
+                g.out = W;
+                g.out_bstride = MB;
+                g.plane_stride = NP2;
+                g.ld = Np;
+                // GEMM1: L21 = M21 U11^-1
+                g.M = n;
+                g.Nc = 2 * NBL;
+                g.Kp = 2 * NBL;
+                g.a_planar = 1;
+                g.a_x0 = k0;
+                g.a_kc = NBL;
+                g.a_row0 = k0 + NBL;
+                g.mode = 0;
+                g.o_row0 = k0 + NBL;
+                g.o_col0 = k0;
+                g.o_nc = NBL;
+                gemm(mapW, mapPU, g, nb);
+                // GEMM2: U12 = L11^-1 M12, and its block-real copy for GEMM3
+                GemmArgs g2 = g;
+                g2.M = NBL;
+                g2.Nc = 2 * n;
+                g2.a_planar = 0;
+                g2.a_row0 = 0;
+                g2.mode = 1;
+                g2.o_row0 = k0;
+                g2.o_col0 = k0 + NBL;
+                g2.o_nc = n;
+                g2.p3 = P3;
+                g2.p3_bstride = prep;
+                g2.p3_n = n;
+                gemm(mapPL, mapP2, g2, nb);
+                // GEMM3: M22 -= L21 U12
+                GemmArgs g3 = g;
+                g3.M = n;
+                g3.Nc = 2 * n;
+                g3.mode = 2;
+                g3.o_row0 = k0 + NBL;
+                g3.o_col0 = k0 + NBL;
+                g3.o_nc = n;
+                gemm(mapW, mapP3, g3, nb);
+                *launches += 1;
+            }
+            t.stop();
+        }
+        // ---- refinement: x_{i+1} = x_i + A^-1 (b - A x_i), A^-1 by the TF32 factors, residuals in FP64
+        int it = 0;
+        bool converged = false;
+        {
+            EventTimer t(s, &prof[3]);
+            cudaMemsetAsync(x, 0, sizeof(double2) * nrhs * Np * nb, s);
+            cudaMemcpyAsync(r, b, sizeof(double2) * nrhs * Np * nb, cudaMemcpyDeviceToDevice, s);
+            double prev = INFINITY;
+            for (it = 0; it < 30; it++) {
+                P.begin(s);
+                if (nrhs <= 16)
+                    k_trisolve_f32<16><<<nb, 1024, 0, s>>>(Np, MB, W, nrhs, r);
+                else
+                    k_trisolve_f32<32><<<nb, 1024, 0, s>>>(Np, MB, W, nrhs, r);
+                P.end(KF_LU_SOLVE, 8.0 * (double)NP2 * nb, s);
+                k_ir_update<<<nb, 256, 0, s>>>(Np, nrhs, x, r, norms);
+                cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, s);
+                P.begin(s);
+                dim3 g((N + 127) / 128, nb);
+                if (nrhs <= 16)
+                    k_cgemv_f32<16><<<g, 128, 0, s>>>(N, Np, MB, nrhs, A32, x, Np, b, Np, r, Np);
+                else
+                    k_cgemv_f32<32><<<g, 128, 0, s>>>(N, Np, MB, nrhs, A32, x, Np, b, Np, r, Np);
+                P.end(KF_MIXED_RESIDUAL, 8.0 * (double)N * N * nb, s);
+                *launches += 3;
+                cudaStreamSynchronize(s);
+                double worst = 0.0;
+                for (int i = 0; i < nb; i++) {
+                    double ratio = hn[2 * i] / std::max(hn[2 * i + 1], 1e-300);
+                    if (!std::isfinite(ratio)) ratio = INFINITY;
+                    worst = std::max(worst, ratio);
+                }
+                if (worst <= 1e-12) {
+                    converged = true;
+                    it++;
+                    break;
+                }
+                if (it >= 3 && !(worst < 0.5 * prev)) break;  // stalled or diverging
+                prev = worst;
+            }
+            t.stop();
+        }
+        int herr = 0;
+        cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        P.flush();
+        if (cudaGetLastError() != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "CUDA error in the mixed-precision solve", f0);
+        if (herr == 10) MIXED_FAIL(HB_ERR_NUMERICAL, "zero pivot in the unpivoted mixed-precision LU", f0);
+        if (herr != 0) MIXED_FAIL(HB_ERR_INTERNAL, "a tensor-core pipeline wait timed out", f0);
+        if (!converged)
+            MIXED_FAIL(HB_ERR_NUMERICAL, "iterative refinement of the mixed-precision solve did not converge", f0);
+        // ---- forces
+        {
+            EventTimer t(s, &prof[4]);
+            double* dA = dout;
+            double* dB = dout + 36 * (size_t)nb;
+            double2* dX = reinterpret_cast<double2*>(dout + 72 * (size_t)nb);
+            double2* dFK = dX + (size_t)H * 6 * nb;
+            double2* dSC = dFK + (size_t)H * 6 * nb;
+            P.begin(s);
+            launch_forces(pv, nb, dfi, H, x, Np, phiI, opt.density, dA, dB, dX, dFK, dSC, s);
+            P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
+            (*launches)++;
+            cudaMemcpyAsync(hout.data(), dout, sizeof(double) * out_per * nb, cudaMemcpyDeviceToHost, s);
+            t.stop();
+        }
+        cudaStreamSynchronize(s);
+        P.flush();
+        const double* hA = hout.data();
+        const double* hB = hA + 36 * (size_t)nb;
+        const double* hX = hA + 72 * (size_t)nb;
+        const double* hFK = hX + (size_t)H * 12 * nb;
+        const double* hSC = hFK + (size_t)H * 12 * nb;
+        for (int i = 0; i < nb; i++) {
+            const size_t fo = (size_t)(f0 + i), hx = (size_t)H * 12;
+            for (int q = 0; q < 36; q++)
+                if (!std::isfinite(hA[36 * i + q]) || !std::isfinite(hB[36 * i + q]))
+                    MIXED_FAIL(HB_ERR_NUMERICAL, "non-finite solution", f0 + i);
+            if (pr.out.added_mass) memcpy(pr.out.added_mass + fo * 36, hA + 36 * i, 36 * sizeof(double));
+            if (pr.out.radiation_damping) memcpy(pr.out.radiation_damping + fo * 36, hB + 36 * i, 36 * sizeof(double));
+            if (pr.out.excitation) memcpy(pr.out.excitation + fo * hx, hX + hx * i, hx * sizeof(double));
+            if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
+            if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
+        }
+        last_ir_iterations() = it;
+    }
+    return 0;
+}
+
+// Test support: C (M x N, row-major FP32) = A (M x K, row-major) B^T where B is given N x K
+// (K-major), on the tcgen05 TF32 path of the mixed LU.  M, N, K multiples of 128, 256, 32.
+int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* C, const char** msg) {
+    if (M % 128 || N % 256 || K % 32 || M <= 0 || N <= 0 || K <= 0) {
+        *msg = "debug GEMM shape: M % 128, N % 256, K % 32";
+        return HB_ERR_VALUE;
+    }
+    if (!encode_fn()) {
+        *msg = "no tensor-map encoder";
+        return HB_ERR_UNSUPPORTED;
+    }
+    MixedBuffers mb;
+    float* dA = mb.get<float>((size_t)M * K);
+    float* dB = mb.get<float>((size_t)N * K);
+    float* dC = mb.get<float>((size_t)M * N);
+    int* err = mb.get<int>(1);
+    if (!dA || !dB || !dC || !err) {
+        *msg = "allocation failed";
+        return HB_ERR_INTERNAL;
+    }
+    cudaMemcpy(dA, A, sizeof(float) * M * K, cudaMemcpyHostToDevice);
+    cudaMemcpy(dB, B, sizeof(float) * N * K, cudaMemcpyHostToDevice);
+    cudaMemset(err, 0, sizeof(int));
+    CUtensorMap mA, mB;
+    if (!make_map(&mA, dA, K, M, 1, 1, (uint64_t)K * 4, (uint64_t)M * K * 4, (uint64_t)M * K * 4, GBM) ||
+        !make_map(&mB, dB, K, N, 1, 1, (uint64_t)K * 4, (uint64_t)N * K * 4, (uint64_t)N * K * 4, GBN)) {
+        *msg = "tensor-map encoding failed";
+        return HB_ERR_INTERNAL;
+    }
+    GemmArgs g{};
+    g.M = M;
+    g.Nc = N;
+    g.Kp = K;
+    g.a_planar = 0;
+    g.mode = 0;
+    g.out = dC;
+    g.out_bstride = (size_t)M * N;
+    g.plane_stride = 0;
+    g.ld = N;
+    g.o_nc = N;
+    g.err = err;
+    const int smem = (int)gemm_smem_bytes();
+    cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    k_gemm_tf32<<<dim3(M / GBM, N / GBN, 1), 128, smem>>>(mA, mB, g);
+    int herr = 0;
+    cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(C, dC, sizeof(float) * M * N, cudaMemcpyDeviceToHost);
+    if (cudaGetLastError() != cudaSuccess) {
+        *msg = "CUDA error";
+        return HB_ERR_INTERNAL;
+    }
+    if (herr) {
+        *msg = "pipeline wait timed out";
+        return HB_ERR_INTERNAL;
+    }
+    return 0;
 }
 
 }  // namespace hbg

@@ -56,7 +56,8 @@ class HbColumn(ctypes.Structure):
 
 
 # every symbol include/hydrobem_gpu.h declares
-EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_last_profile", "hbg_last_launch_count",
+EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_debug_gemm_tf32",
+           "hbg_last_ir_iterations", "hbg_last_profile", "hbg_last_launch_count",
            "hbg_profile_kernels", "hbg_kernel_profile", "hb_abi_version",
            "hb_last_error_message", "hb_last_error_location", "hb_model_new", "hb_model_free", "hb_model_cancel",
            "hb_object", "hb_add", "hb_set_bool", "hb_set_int", "hb_set_real", "hb_set_text", "hb_set_reals",
@@ -89,6 +90,9 @@ def lib():
     L.hbg_solve_batch.restype = ctypes.c_int32
     L.hbg_debug_matrices.argtypes = [ctypes.POINTER(HbgBody), ctypes.c_double, ctypes.POINTER(HbgOptions), dp, dp, dp]
     L.hbg_debug_matrices.restype = ctypes.c_int32
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.hbg_debug_gemm_tf32.argtypes = [ctypes.c_int32] * 3 + [fp, fp, fp]
+    L.hbg_last_ir_iterations.argtypes = [ctypes.POINTER(ctypes.c_int32)]
     L.hbg_last_profile.argtypes = [dp]
     L.hbg_profile_kernels.argtypes = [ctypes.c_int32]
     L.hbg_kernel_profile.argtypes = [ctypes.c_int32, dp, ctypes.POINTER(ctypes.c_int64), dp]
@@ -213,3 +217,21 @@ def kernel_profile():
         lib().hbg_kernel_profile(i, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(w))
         out[name] = (ms.value, n.value, w.value)
     return out
+
+
+def debug_gemm_tf32(A, B):
+    """C = A B^T through the tcgen05 TF32 kernel (test support); A [M][K], B [N][K] float32."""
+    A = np.ascontiguousarray(A, dtype=np.float32)
+    B = np.ascontiguousarray(B, dtype=np.float32)
+    M, K = A.shape
+    N = B.shape[0]
+    C = np.zeros((M, N), dtype=np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    check(lib().hbg_debug_gemm_tf32(M, N, K, A.ctypes.data_as(fp), B.ctypes.data_as(fp), C.ctypes.data_as(fp)))
+    return C
+
+
+def last_ir_iterations() -> int:
+    n = ctypes.c_int32()
+    lib().hbg_last_ir_iterations(ctypes.byref(n))
+    return n.value

@@ -1,0 +1,91 @@
+"""The mixed-precision form: the tcgen05 TF32 product kernel against exact and FP64 products, and the
+whole mixed solve against the CPU oracle at the bar of the benchmark metric (A, B, X within 1e-5 of
+each entry's scale -- the regression measure, floor 1e-3 of the peak)."""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from hydrobem_b200 import meshes
+from hydrobem_b200 import native as nv
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MIXED_TOL = 1e-5
+
+
+def scaled_error(got, ref, floor=1e-3):
+    ref = np.asarray(ref)
+    peak = np.abs(ref).max()
+    scale = np.maximum(np.abs(ref).max(axis=0, keepdims=True), floor * peak)
+    return float((np.abs(np.asarray(got) - ref) / scale).max())
+
+
+def test_tf32_gemm_exact_on_small_integers():
+    """Small integers are exact in TF32 and their sums exact in FP32: any layout, swizzle or
+    descriptor mistake shows as a mismatch."""
+    rng = np.random.default_rng(1)
+    for M, N, K in ((128, 256, 32), (256, 512, 256), (384, 256, 96)):
+        A = rng.integers(-3, 4, size=(M, K)).astype(np.float32)
+        B = rng.integers(-3, 4, size=(N, K)).astype(np.float32)
+        C = nv.debug_gemm_tf32(A, B)
+        assert np.array_equal(C, A @ B.T), (M, N, K)
+
+
+def test_tf32_gemm_against_fp64():
+    rng = np.random.default_rng(2)
+    A = rng.standard_normal((256, 256)).astype(np.float32)
+    B = rng.standard_normal((512, 256)).astype(np.float32)
+    C = nv.debug_gemm_tf32(A, B)
+    ref = A.astype(np.float64) @ B.astype(np.float64).T
+    # TF32 keeps 10 mantissa bits: products to ~5e-4, sums of 256 random terms to ~1e-2 absolute
+    err = np.abs(C - ref).max() / np.abs(ref).max()
+    assert err < 5e-3, err
+    assert err > 1e-7  # the operands were rounded to TF32 (not an FP32 path in disguise)
+
+
+def test_mixed_config1_cylinder():
+    v = meshes.cylinder(1.0, 0.5, 32, 8, 8)
+    omegas = 2.0 * math.pi / np.arange(2.0, 12.0)
+    gpu = nv.solve(v, omegas, [0.0], precision=nv.HBG_MIXED)
+    its = nv.last_ir_iterations()
+    ref = O.solve_body(v, omegas, [0.0], depth=math.inf)
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    assert max(errs.values()) <= MIXED_TOL, (errs, its)
+    assert 1 <= its <= 12
+
+
+def test_mixed_finite_depth_four_headings():
+    v = meshes.cylinder(1.0, 0.5, 32, 8, 8)
+    omegas = 2.0 * math.pi / np.array([1.5, 3.0, 7.0, 20.0])
+    heads = [0.0, 30.0, 60.0, 90.0]
+    gpu = nv.solve(v, omegas, heads, depth=5.0, precision=nv.HBG_MIXED)
+    ref = O.solve_body(v, omegas, heads, depth=5.0)
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    assert max(errs.values()) <= MIXED_TOL, errs
+
+
+def test_mixed_padding_and_uneven_bodies():
+    """Panel counts that are not multiples of the 128-column LU block (identity padding)."""
+    bodies = [nv.Body(meshes.hemisphere(1.3, 6, 12), [1.1, 2.0], [0.0, 90.0]),
+              nv.Body(meshes.cylinder(2.0, 1.0, 24, 6, 6), [0.5, 1.0], [30.0])]
+    out = nv.solve_batch(bodies, precision=nv.HBG_MIXED)
+    for b, g in zip(bodies, out):
+        ref = O.solve_body(b.vertices, b.omegas, b.headings, depth=math.inf)
+        errs = {k: scaled_error(g[k], ref[k]) for k in ("A", "B", "X")}
+        assert max(errs.values()) <= MIXED_TOL, errs
+
+
+def test_mixed_interior_lid():
+    v = meshes.box(1.0, 0.5, 0.5, n=(8, 4, 4), lid=True)
+    kinds = np.zeros(len(v), np.int32)
+    kinds[-32:] = 1
+    omegas = np.array([1.0, 2.0, 3.5])
+    gpu = nv.solve(v, omegas, [0.0, 45.0], kinds=kinds, precision=nv.HBG_MIXED)
+    ref = O.solve_body(v, omegas, [0.0, 45.0], depth=math.inf, kinds=kinds)
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    assert max(errs.values()) <= MIXED_TOL, errs
