@@ -1,6 +1,5 @@
-// hbg_all.cu -- the single translation unit of libhydrobem_gpu.so (the __constant__ tables and
-// Gauss nodes are defined once and seen by every kernel).
-#include "hbg_statics.cu"
+// hbg_all.cu -- the main translation unit of libhydrobem_gpu.so (hbg_statics.cu is the other one,
+// compiled without floating-point contraction).
 #include "hbg_freq.cu"
 #include "hbg_lu.cu"
 #include "hbg_mixed.cu"

@@ -182,6 +182,7 @@ static DeviceCtx& device_ctx(int dev) {
     memset(glw, 0, sizeof glw);
     for (int n = 1; n <= 16; n++) gauss_legendre(n, glx[n], glw[n]);
     set_constants(glx, glw, d.tab);
+    set_constants_statics(glx, glw);
     CUDA_OK(cudaGetLastError());
     d.ready = true;
     return d;

@@ -72,11 +72,11 @@ struct FdParams {
 // the fin_point data of one panel depth (green_fin.rs:119-130), stored as planes per frequency
 constexpr int FP_PLANES = 4 + 2 * FIN_ROOTS;
 
-// Gauss-Legendre rules of orders 1..16 and the table pointers (one definition: the library is a
-// single translation unit, hbg_all.cu)
-__constant__ double c_glx[17][16];
-__constant__ double c_glw[17][16];
-__constant__ Tables c_tab;
+// Gauss-Legendre rules of orders 1..16 and the table pointers: one copy per translation unit
+// (hbg_statics.cu and hbg_all.cu), each set by its own set_constants function.
+static __constant__ double c_glx[17][16];
+static __constant__ double c_glw[17][16];
+static __constant__ Tables c_tab;
 
 // ------------------------------------------------------------------ small helpers
 __device__ __forceinline__ double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }

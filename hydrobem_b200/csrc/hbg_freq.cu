@@ -5,6 +5,12 @@
 
 namespace hbg {
 
+void set_constants(const double glx[17][16], const double glw[17][16], const Tables& tab) {
+    cudaMemcpyToSymbol(c_glx, glx, sizeof(double) * 17 * 16);
+    cudaMemcpyToSymbol(c_glw, glw, sizeof(double) * 17 * 16);
+    cudaMemcpyToSymbol(c_tab, &tab, sizeof(Tables));
+}
+
 // ------------------------------------------------------------------ finite-depth tiles
 // green_fin.rs:493-564 build_tiles: the values and both derivatives of Phi1, Phi2 at the
 // first-kind Chebyshev nodes of each tile (one thread per node), then per tile and quantity the
@@ -222,8 +228,9 @@ __global__ void __launch_bounds__(256) k_assemble(PanelsView pv, const double* _
         }
         double an = pv.at(P_AREA, n);
         int kindn = pv.kind[n];
+        // R without contraction: the finite-depth kernel switches form at R = h/2 exactly
         double dx = xk[0] - xn[0], dy = xk[1] - xn[1];
-        double R = sqrt(dx * dx + dy * dy);
+        double R = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
         Kern w;
         if (FINITE) {
             w = finite_kernel(*fd, T1, T2, R, xk[2], xn[2], fp + k, fp + n, N);

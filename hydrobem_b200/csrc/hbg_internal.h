@@ -99,6 +99,7 @@ struct FreqInfo {
 };
 
 void set_constants(const double glx[17][16], const double glw[17][16], const Tables& tab);
+void set_constants_statics(const double glx[17][16], const double glw[17][16]);
 void launch_panel_geometry(int N, const double* verts, const int32_t* kind, double* planes, int32_t* bad,
                            cudaStream_t s);
 void launch_statics(const PanelsView& pv, double depth, int logint, double tol, double* st, int32_t* work,

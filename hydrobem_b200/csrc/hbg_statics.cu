@@ -10,6 +10,12 @@
 //
 // Layout: statics planes [4][N*N] (rs, rd, dl, dd), entry (k, j) at k + j*N (column-major, the
 // layout of the matrices the assembly writes), so a warp of consecutive rows k writes coalesced.
+//
+// This file is its own translation unit, compiled without floating-point contraction (-fmad=false):
+// the reference picks closed forms, Gauss orders and the adaptive rule by thresholds on geometric
+// ratios (distance over panel radius, clearance, log_pair), which regular meshes put exactly on
+// the thresholds; with the same IEEE operations in the same order as the reference, every such
+// decision (and every geometric quantity) is the reference's to the bit.
 #include "hbg_device.cuh"
 #include "hbg_internal.h"
 
@@ -402,15 +408,36 @@ __device__ inline void log_cell(const double m[4][3], const double* image, const
         }
 }
 
-// The adaptive pairs: quadrisection to 1e-13 of the integrals' scale, at most 14 levels, summed in
-// the depth-first order of panel_integrals.rs:100-120 (an explicit stack, children pushed last
-// first).  One thread per pair.
-__global__ void __launch_bounds__(128) k_statics_adaptive(PanelsView pv, const int32_t* __restrict__ work, int nwork,
-                                                          double* __restrict__ st) {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
+// The adaptive pairs: quadrisection to 1e-13 of the integrals' scale, at most 14 levels, cells
+// taken in the depth-first order of panel_integrals.rs:100-120.  One warp per pair: at each level
+// the 32 lanes evaluate the 4 sub-cells x 16 Gauss points (two points a lane), reduce them per
+// sub-cell by shuffles, and lane 0 keeps the depth-first stack in shared memory.
+constexpr int AD_WARPS = 4, AD_STACK = 48;
+
+struct AdCell {
+    double u0, u1, v0, v1, p0, p1;
+    int depth;
+};
+
+__device__ __forceinline__ void log_point(const double m[4][3], const double* image, const double* n, double u0,
+                                          double u1, double v0, double v1, int i, int j, double& a, double& b) {
+    double hu = 0.5 * (u1 - u0), hv = 0.5 * (v1 - v0);
+    double xi[3], jac, psi, dpsi;
+    bilinear(m, u0 + hu * (c_glx[4][i] + 1.0), v0 + hv * (c_glx[4][j] + 1.0), xi, jac);
+    double ww = c_glw[4][i] * c_glw[4][j] * hu * hv * jac;
+    psi_terms(xi, image, n, psi, dpsi);
+    a = ww * psi;
+    b = ww * dpsi;
+}
+
+__global__ void __launch_bounds__(AD_WARPS * 32) k_statics_adaptive(PanelsView pv, const int32_t* __restrict__ work,
+                                                                    int nwork, double* __restrict__ st) {
+    __shared__ AdCell stack[AD_WARPS][AD_STACK];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * AD_WARPS + warp;
     if (t >= nwork) return;
-    int N = pv.N;
-    int k = work[2 * t], j = work[2 * t + 1];
+    const int N = pv.N;
+    const int k = work[2 * t], j = work[2 * t + 1];
     PanelRegs p;
     load_panel(pv, j, p);
     double xb[3] = {pv.at(P_C + 0, k), pv.at(P_C + 1, k), -pv.at(P_C + 2, k)};
@@ -421,38 +448,66 @@ __global__ void __launch_bounds__(128) k_statics_adaptive(PanelsView pv, const i
     double dmin = fmax(dist - p.radius, 1e-3 * p.radius);
     double scale = fabs(log(dist + p.radius)) + 1.0;
     double tol_l = 1e-13 * p.area * scale, tol_d = 1e-13 * p.area / dmin;
-    struct Cell {
-        double u0, u1, v0, v1, p0, p1;
-        int depth;
-    };
-    constexpr int STACK = 48;
-    Cell stack[STACK];
+    // the whole square by one 4 x 4 cell (lanes 0..15 one point each)
+    double wa = 0.0, wb = 0.0;
+    if (lane < 16) log_point(m, xb, p.n, -1.0, 1.0, -1.0, 1.0, lane / 4, lane % 4, wa, wb);
+    for (int o = 16; o > 0; o >>= 1) {
+        wa += __shfl_xor_sync(0xffffffffu, wa, o);
+        wb += __shfl_xor_sync(0xffffffffu, wb, o);
+    }
+    AdCell* stk = stack[warp];
     int sp = 0;
-    double whole[2];
-    log_cell(m, xb, p.n, -1.0, 1.0, -1.0, 1.0, whole);
-    stack[sp++] = Cell{-1.0, 1.0, -1.0, 1.0, whole[0], whole[1], 0};
+    if (lane == 0) stk[0] = AdCell{-1.0, 1.0, -1.0, 1.0, wa, wb, 0};
+    sp = 1;
+    __syncwarp();
     double acc0 = 0.0, acc1 = 0.0;
     while (sp > 0) {
-        Cell c = stack[--sp];
-        double um = 0.5 * (c.u0 + c.u1), vm = 0.5 * (c.v0 + c.v1);
-        double us[4][2] = {{c.u0, um}, {um, c.u1}, {um, c.u1}, {c.u0, um}};
-        double vs[4][2] = {{c.v0, vm}, {c.v0, vm}, {vm, c.v1}, {vm, c.v1}};
+        AdCell c = stk[sp - 1];
+        sp--;
+        __syncwarp();
+        const double um = 0.5 * (c.u0 + c.u1), vm = 0.5 * (c.v0 + c.v1);
+        const double us0[4] = {c.u0, um, um, c.u0}, us1[4] = {um, c.u1, c.u1, um};
+        const double vs0[4] = {c.v0, c.v0, vm, vm}, vs1[4] = {vm, vm, c.v1, c.v1};
+        // lane l: point l of sub-cells (l / 16) and (l / 16) + 2
+        const int sa = lane >> 4, q = lane & 15;
+        double a0, b0, a1, b1;
+        log_point(m, xb, p.n, us0[sa], us1[sa], vs0[sa], vs1[sa], q / 4, q % 4, a0, b0);
+        log_point(m, xb, p.n, us0[sa + 2], us1[sa + 2], vs0[sa + 2], vs1[sa + 2], q / 4, q % 4, a1, b1);
+        for (int o = 8; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            b0 += __shfl_xor_sync(0xffffffffu, b0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            b1 += __shfl_xor_sync(0xffffffffu, b1, o);
+        }
         double cc[4][2];
-        for (int q = 0; q < 4; q++) log_cell(m, xb, p.n, us[q][0], us[q][1], vs[q][0], vs[q][1], cc[q]);
-        double s0 = cc[0][0] + cc[1][0] + cc[2][0] + cc[3][0];
-        double s1 = cc[0][1] + cc[1][1] + cc[2][1] + cc[3][1];
-        if (c.depth >= 14 || (fabs(s0 - c.p0) <= tol_l && fabs(s1 - c.p1) <= tol_d) || sp + 4 > STACK) {
+        cc[0][0] = __shfl_sync(0xffffffffu, a0, 0);
+        cc[0][1] = __shfl_sync(0xffffffffu, b0, 0);
+        cc[1][0] = __shfl_sync(0xffffffffu, a0, 16);
+        cc[1][1] = __shfl_sync(0xffffffffu, b0, 16);
+        cc[2][0] = __shfl_sync(0xffffffffu, a1, 0);
+        cc[2][1] = __shfl_sync(0xffffffffu, b1, 0);
+        cc[3][0] = __shfl_sync(0xffffffffu, a1, 16);
+        cc[3][1] = __shfl_sync(0xffffffffu, b1, 16);
+        const double s0 = cc[0][0] + cc[1][0] + cc[2][0] + cc[3][0];
+        const double s1 = cc[0][1] + cc[1][1] + cc[2][1] + cc[3][1];
+        if (c.depth >= 14 || (fabs(s0 - c.p0) <= tol_l && fabs(s1 - c.p1) <= tol_d) || sp + 4 > AD_STACK) {
             acc0 += s0;
             acc1 += s1;
             continue;
         }
-        for (int q = 3; q >= 0; q--) stack[sp++] = Cell{us[q][0], us[q][1], vs[q][0], vs[q][1], cc[q][0], cc[q][1], c.depth + 1};
+        if (lane == 0)
+            for (int qq = 3; qq >= 0; qq--)
+                stk[sp + 3 - qq] = AdCell{us0[qq], us1[qq], vs0[qq], vs1[qq], cc[qq][0], cc[qq][1], c.depth + 1};
+        sp += 4;
+        __syncwarp();
     }
-    double psi, dpsi;
-    psi_terms(p.c, xb, p.n, psi, dpsi);
-    size_t NN = (size_t)N * N, o = (size_t)k + (size_t)j * N;
-    st[2 * NN + o] = acc0 - p.area * psi;
-    st[3 * NN + o] = acc1 - p.area * dpsi;
+    if (lane == 0) {
+        double psi, dpsi;
+        psi_terms(p.c, xb, p.n, psi, dpsi);
+        size_t NN = (size_t)N * N, o = (size_t)k + (size_t)j * N;
+        st[2 * NN + o] = acc0 - p.area * psi;
+        st[3 * NN + o] = acc1 - p.area * dpsi;
+    }
 }
 
 // ------------------------------------------------------------------ host launchers
@@ -468,13 +523,12 @@ void launch_statics(const PanelsView& pv, double depth, int logint, double tol, 
 }
 
 void launch_statics_adaptive(const PanelsView& pv, const int32_t* work, int nwork, double* st, cudaStream_t s) {
-    if (nwork > 0) k_statics_adaptive<<<(nwork + 127) / 128, 128, 0, s>>>(pv, work, nwork, st);
+    if (nwork > 0) k_statics_adaptive<<<(nwork + AD_WARPS - 1) / AD_WARPS, AD_WARPS * 32, 0, s>>>(pv, work, nwork, st);
 }
 
-void set_constants(const double glx[17][16], const double glw[17][16], const Tables& tab) {
+void set_constants_statics(const double glx[17][16], const double glw[17][16]) {
     cudaMemcpyToSymbol(c_glx, glx, sizeof(double) * 17 * 16);
     cudaMemcpyToSymbol(c_glw, glw, sizeof(double) * 17 * 16);
-    cudaMemcpyToSymbol(c_tab, &tab, sizeof(Tables));
 }
 
 }  // namespace hbg
