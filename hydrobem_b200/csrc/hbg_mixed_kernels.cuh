@@ -207,50 +207,67 @@ __global__ void __launch_bounds__(1024) k_diag_factor(float* __restrict__ W, int
         Wr[o] = blk[r * LD + c].x;
         Wi[o] = blk[r * LD + c].y;
     }
+    __syncthreads();
+    // In-place inversion of U11 (upper) and L11 (unit lower), column by column: for column j of
+    // U^-1 the leading block is already inverted, U^-1(0:j, j) = -U^-1(0:j, 0:j) U(0:j, j) / U(j, j);
+    // for L^-1 from the last column, L^-1(j+1:, j) = -L^-1(j+1:, j+1:) L(j+1:, j).  Eight threads
+    // per row share each dot product (shuffle reduction).
+    const int row = threadIdx.x >> 3, part = threadIdx.x & 7;
+    for (int j = 0; j < NBL; j++) {
+        float2 d = blk[j * LD + j];
+        float dd = d.x * d.x + d.y * d.y;
+        float2 inv = make_float2(d.x / dd, -d.y / dd);
+        float2 acc = make_float2(0.f, 0.f);
+        if (row < j)
+            for (int p = row + part; p < j; p += 8) {
+                float2 t = blk[row * LD + p], v = blk[p * LD + j];
+                acc.x += t.x * v.x - t.y * v.y;
+                acc.y += t.x * v.y + t.y * v.x;
+            }
+        for (int o = 4; o > 0; o >>= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+        }
+        __syncthreads();
+        if (row < j && part == 0)  // -acc / U(j, j) = -acc * inv
+            blk[row * LD + j] = make_float2(-(acc.x * inv.x - acc.y * inv.y), -(acc.x * inv.y + acc.y * inv.x));
+        if (row == j && part == 0) blk[j * LD + j] = inv;
+        __syncthreads();
+    }
+    for (int j = NBL - 2; j >= 0; j--) {
+        float2 acc = make_float2(0.f, 0.f);
+        if (row > j) {
+            // L^-1(row, j) = -(L(row, j) + sum_{j < p < row} L^-1(row, p) L(p, j))
+            if (part == 0) acc = blk[row * LD + j];
+            for (int p = j + 1 + part; p < row; p += 8) {
+                float2 t = blk[row * LD + p], v = blk[p * LD + j];
+                acc.x += t.x * v.x - t.y * v.y;
+                acc.y += t.x * v.y + t.y * v.x;
+            }
+        }
+        for (int o = 4; o > 0; o >>= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+        }
+        __syncthreads();
+        if (row > j && part == 0) blk[row * LD + j] = make_float2(-acc.x, -acc.y);
+        __syncthreads();
+    }
+    // blk now holds L^-1 (strictly below the diagonal, unit diagonal) and U^-1 (upper)
     float* PLf = PL + (size_t)f * NBL * 2 * NBL;
     float* PUf = PU + (size_t)f * 2 * NBL * 2 * NBL;
-    const int c = threadIdx.x;
-    if (c < NBL) {
-        // column c of U11^-1 by back substitution
-        float2 x[NBL];
-        for (int i = 0; i < NBL; i++) x[i] = make_float2(0.f, 0.f);
-        for (int i = c; i >= 0; i--) {
-            float sr = (i == c) ? 1.f : 0.f, si = 0.f;
-            for (int p = i + 1; p <= c; p++) {
-                float2 u = blk[i * LD + p];
-                sr -= u.x * x[p].x - u.y * x[p].y;
-                si -= u.x * x[p].y + u.y * x[p].x;
-            }
-            float2 d = blk[i * LD + i];
-            float dd = d.x * d.x + d.y * d.y;
-            x[i] = make_float2((sr * d.x + si * d.y) / dd, (si * d.x - sr * d.y) / dd);
-        }
-        // block-real K-major rows: row c: [Ur(:,c); -Ui(:,c)], row NBL + c: [Ui(:,c); Ur(:,c)]
-        for (int k = 0; k < NBL; k++) {
-            PUf[(size_t)c * 2 * NBL + k] = x[k].x;
-            PUf[(size_t)c * 2 * NBL + NBL + k] = -x[k].y;
-            PUf[(size_t)(NBL + c) * 2 * NBL + k] = x[k].y;
-            PUf[(size_t)(NBL + c) * 2 * NBL + NBL + k] = x[k].x;
-        }
-    } else if (c < 2 * NBL) {
-        // column cc of L11^-1 (unit lower) by forward substitution; written as rows [Lr | Li]
-        const int cc = c - NBL;
-        float2 x[NBL];
-        for (int i = 0; i < NBL; i++) x[i] = make_float2(0.f, 0.f);
-        x[cc] = make_float2(1.f, 0.f);
-        for (int i = cc + 1; i < NBL; i++) {
-            float sr = 0.f, si = 0.f;
-            for (int p = cc; p < i; p++) {
-                float2 l = blk[i * LD + p];
-                sr -= l.x * x[p].x - l.y * x[p].y;
-                si -= l.x * x[p].y + l.y * x[p].x;
-            }
-            x[i] = make_float2(sr, si);
-        }
-        for (int i = 0; i < NBL; i++) {
-            PLf[(size_t)i * 2 * NBL + cc] = x[i].x;
-            PLf[(size_t)i * 2 * NBL + NBL + cc] = x[i].y;
-        }
+    for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) {
+        const int i = t / NBL, c = t % NBL;
+        // [Lr | Li] rows of L^-1
+        float2 l = i > c ? blk[i * LD + c] : make_float2(i == c ? 1.f : 0.f, 0.f);
+        PLf[(size_t)i * 2 * NBL + c] = l.x;
+        PLf[(size_t)i * 2 * NBL + NBL + c] = l.y;
+        // U^-1 block-real K-major: row c: [Ur(:, c); -Ui(:, c)], row NBL + c: [Ui(:, c); Ur(:, c)]
+        float2 u = i <= c ? blk[i * LD + c] : make_float2(0.f, 0.f);  // U^-1(i, c)
+        PUf[(size_t)c * 2 * NBL + i] = u.x;
+        PUf[(size_t)c * 2 * NBL + NBL + i] = -u.y;
+        PUf[(size_t)(NBL + c) * 2 * NBL + i] = u.y;
+        PUf[(size_t)(NBL + c) * 2 * NBL + NBL + i] = u.x;
     }
 }
 
@@ -282,33 +299,36 @@ __global__ void k_prep_block_row(const float* __restrict__ W, int Np, size_t bst
     }
 }
 
-// out[f][c][k] = bias[f][c][k] - sum_n M(k, n) x[f][c][n], M column-major planar FP32 (entry (k, n)
-// at n Np + k), x and out FP64 complex [F][nrhs][ld]; one thread per row, M read once (coalesced
-// along k), x staged in shared memory.  bias may be null (zero).
+// Partial products of y = M x over column chunks: part[z][f][c][k] = sum_{n in chunk z} M(k, n) x[f][c][n],
+// M column-major planar FP32 (entry (k, n) at n Np + k), x FP64 complex [F][nrhs][ldx]; one thread
+// per row (M read once, coalesced along k), FP64 accumulation.  k_gemv_reduce then forms
+// out = bias - sum_z part[z] in a fixed order (deterministic).
+constexpr int GEMV_CHUNK = 512;
 template <int NR>
-__global__ void __launch_bounds__(128) k_cgemv_f32(int N, int Np, size_t bstride, int nrhs,
-                                                   const float* __restrict__ Mall, const double2* __restrict__ xall,
-                                                   int ldx, const double2* __restrict__ bias, int ldb,
-                                                   double2* __restrict__ out, int ldo) {
+__global__ void __launch_bounds__(128) k_cgemv_part(int N, int Np, size_t bstride, int nrhs,
+                                                    const float* __restrict__ Mall, const double2* __restrict__ xall,
+                                                    int ldx, double2* __restrict__ part, int F) {
     constexpr int CH = 32;
     __shared__ double2 sx[CH][NR];
-    const int f = blockIdx.y;
+    const int f = blockIdx.y, z = blockIdx.z;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const float* Mr = Mall + (size_t)f * bstride;
     const float* Mi = Mr + (size_t)Np * Np;
     const double2* x = xall + (size_t)f * nrhs * ldx;
+    const int nbeg = z * GEMV_CHUNK, nend = min(N, nbeg + GEMV_CHUNK);
     double2 acc[NR];
 #pragma unroll
     for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
-    for (int n0 = 0; n0 < N; n0 += CH) {
+    for (int n0 = nbeg; n0 < nend; n0 += CH) {
         __syncthreads();
         for (int t = threadIdx.x; t < CH * NR; t += blockDim.x) {
             int nn = t % CH, c = t / CH;
-            sx[nn][c] = (n0 + nn < N && c < nrhs) ? x[(size_t)c * ldx + n0 + nn] : make_double2(0.0, 0.0);
+            sx[nn][c] = (n0 + nn < nend && c < nrhs) ? x[(size_t)c * ldx + n0 + nn] : make_double2(0.0, 0.0);
         }
         __syncthreads();
         if (k < N) {
-            const int lim = min(CH, N - n0);
+            const int lim = min(CH, nend - n0);
+#pragma unroll 4
             for (int nn = 0; nn < lim; nn++) {
                 const size_t o = (size_t)(n0 + nn) * Np + k;
                 const double mr = Mr[o], mi = Mi[o];
@@ -322,100 +342,158 @@ __global__ void __launch_bounds__(128) k_cgemv_f32(int N, int Np, size_t bstride
         }
     }
     if (k < N)
-        for (int c = 0; c < nrhs && c < NR; c++) {
-            double2 b = bias ? bias[((size_t)f * nrhs + c) * ldb + k] : make_double2(0.0, 0.0);
-            out[((size_t)f * nrhs + c) * ldo + k] = make_double2(b.x - acc[c].x, b.y - acc[c].y);
-        }
+        for (int c = 0; c < nrhs && c < NR; c++) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
+}
+
+__global__ void k_gemv_reduce(int N, int nrhs, int F, int nz, const double2* __restrict__ part,
+                              const double2* __restrict__ bias, int ldb, double2* __restrict__ out, int ldo) {
+    const int f = blockIdx.y;
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)nrhs * N) return;
+    const int c = (int)(t / N), k = (int)(t % N);
+    double sr = 0.0, si = 0.0;
+    for (int z = 0; z < nz; z++) {
+        double2 v = part[(((size_t)z * F + f) * nrhs + c) * N + k];
+        sr += v.x;
+        si += v.y;
+    }
+    double2 b = bias ? bias[((size_t)f * nrhs + c) * ldb + k] : make_double2(0.0, 0.0);
+    out[((size_t)f * nrhs + c) * ldo + k] = make_double2(b.x - sr, b.y - si);
 }
 
 // x = A^-1 r with the factors of M = A^T = L U (FP32 planar, row-major in W): U^T y = r, then
-// L^T x = y; FP64 vectors [F][nrhs][Np], in place.  One block per matrix, 32-row blocks: a warp per
-// right-hand side solves the triangle, then every thread updates its rows with the block's values
-// (row b0 + p of W read along the updated rows: coalesced).
+// L^T x = y, FP64 vectors [F][nrhs][Np] in place, in blocks of TB = 128 rows.  One launch per
+// block step: every CTA of the step owns 128 rows, subtracts the contribution of the block solved
+// by the previous step (row b0 + p of W read along its rows: coalesced), and the CTA that owns the
+// next diagonal block then solves it (a warp per right-hand side, 32-row sub-blocks).
+constexpr int TB = 128;
+
 template <int NR>
-__global__ void __launch_bounds__(1024) k_trisolve_f32(int Np, size_t bstride, const float* __restrict__ W, int nrhs,
-                                                       double2* __restrict__ Xall) {
-    __shared__ double2 xs[32][NR];
-    const int f = blockIdx.x;
+__device__ __forceinline__ void tri_block(const float* Mr, const float* Mi, int Np, double2* X, int nrhs, int b0,
+                                          bool upper_t, double2 (*xs)[NR]) {
+    // solve the TB x TB diagonal block of U^T (upper_t) or L^T in place in X rows b0..b0+TB
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    auto m = [&](int r, int c) { size_t o = (size_t)r * Np + c; return make_double2(Mr[o], Mi[o]); };
+    if (upper_t) {
+        for (int s0 = 0; s0 < TB; s0 += 32) {
+            if (warp < nrhs) {
+                double2 y = X[(size_t)warp * Np + b0 + s0 + lane];
+                for (int p = 0; p < 32; p++) {
+                    if (lane == p) {
+                        double2 d = m(b0 + s0 + p, b0 + s0 + p);
+                        double dd = d.x * d.x + d.y * d.y;
+                        y = make_double2((y.x * d.x + y.y * d.y) / dd, (y.y * d.x - y.x * d.y) / dd);
+                    }
+                    double2 yp = make_double2(__shfl_sync(0xffffffffu, y.x, p), __shfl_sync(0xffffffffu, y.y, p));
+                    if (lane > p) {
+                        double2 u = m(b0 + s0 + p, b0 + s0 + lane);
+                        y.x -= u.x * yp.x - u.y * yp.y;
+                        y.y -= u.x * yp.y + u.y * yp.x;
+                    }
+                }
+                X[(size_t)warp * Np + b0 + s0 + lane] = y;
+                xs[lane][warp] = y;
+            }
+            __syncthreads();
+            for (int i = b0 + s0 + 32 + threadIdx.x; i < b0 + TB; i += blockDim.x)
+                for (int c = 0; c < nrhs; c++) {
+                    double2 acc = X[(size_t)c * Np + i];
+                    for (int p = 0; p < 32; p++) {
+                        double2 u = m(b0 + s0 + p, i), v = xs[p][c];
+                        acc.x -= u.x * v.x - u.y * v.y;
+                        acc.y -= u.x * v.y + u.y * v.x;
+                    }
+                    X[(size_t)c * Np + i] = acc;
+                }
+            __syncthreads();
+        }
+    } else {
+        for (int s0 = TB - 32; s0 >= 0; s0 -= 32) {
+            if (warp < nrhs) {
+                double2 x = X[(size_t)warp * Np + b0 + s0 + lane];
+                for (int p = 31; p >= 0; p--) {
+                    double2 xp = make_double2(__shfl_sync(0xffffffffu, x.x, p), __shfl_sync(0xffffffffu, x.y, p));
+                    if (lane < p) {
+                        double2 l = m(b0 + s0 + p, b0 + s0 + lane);
+                        x.x -= l.x * xp.x - l.y * xp.y;
+                        x.y -= l.x * xp.y + l.y * xp.x;
+                    }
+                }
+                X[(size_t)warp * Np + b0 + s0 + lane] = x;
+                xs[lane][warp] = x;
+            }
+            __syncthreads();
+            for (int i = b0 + threadIdx.x; i < b0 + s0; i += blockDim.x)
+                for (int c = 0; c < nrhs; c++) {
+                    double2 acc = X[(size_t)c * Np + i];
+                    for (int p = 0; p < 32; p++) {
+                        double2 l = m(b0 + s0 + p, i), v = xs[p][c];
+                        acc.x -= l.x * v.x - l.y * v.y;
+                        acc.y -= l.x * v.y + l.y * v.x;
+                    }
+                    X[(size_t)c * Np + i] = acc;
+                }
+            __syncthreads();
+        }
+    }
+}
+
+// One block step of the forward (upper_t) or backward solve.  step = index of the block solved by
+// the previous launch (-1: none, only the first diagonal block is solved).
+template <int NR>
+__global__ void __launch_bounds__(256) k_tri_step(int Np, size_t bstride, const float* __restrict__ W, int nrhs,
+                                                  double2* __restrict__ Xall, int step, int upper_t) {
+    extern __shared__ double2 tri_smem[];  // ys [TB][NR], then xs [32][NR]
+    double2(*ys)[NR] = reinterpret_cast<double2(*)[NR]>(tri_smem);
+    double2(*xs)[NR] = reinterpret_cast<double2(*)[NR]>(tri_smem + TB * NR);
+    const int f = blockIdx.y;
     const float* Mr = W + (size_t)f * bstride;
     const float* Mi = Mr + (size_t)Np * Np;
     double2* X = Xall + (size_t)f * nrhs * Np;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    auto m = [&](int r, int c) { size_t o = (size_t)r * Np + c; return make_double2(Mr[o], Mi[o]); };
-    // forward: U^T y = r  (U^T(i, j) = M(j, i), j <= i)
-    for (int b0 = 0; b0 < Np; b0 += 32) {
-        if (warp < nrhs) {
-            double2 y = X[(size_t)warp * Np + b0 + lane];
-            for (int p = 0; p < 32; p++) {
-                if (lane == p) {
-                    double2 d = m(b0 + p, b0 + p);
-                    double dd = d.x * d.x + d.y * d.y;
-                    y = make_double2((y.x * d.x + y.y * d.y) / dd, (y.y * d.x - y.x * d.y) / dd);
-                }
-                double2 yp = make_double2(__shfl_sync(0xffffffffu, y.x, p), __shfl_sync(0xffffffffu, y.y, p));
-                if (lane > p) {
-                    double2 u = m(b0 + p, b0 + lane);
-                    y.x -= u.x * yp.x - u.y * yp.y;
-                    y.y -= u.x * yp.y + u.y * yp.x;
-                }
-            }
-            X[(size_t)warp * Np + b0 + lane] = y;
-            xs[lane][warp] = y;
-        }
-        __syncthreads();
-        for (int i = b0 + 32 + threadIdx.x; i < Np; i += blockDim.x) {
-            double2 acc[NR];
-#pragma unroll
-            for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
-            for (int p = 0; p < 32; p++) {
-                double2 u = m(b0 + p, i);
-#pragma unroll
-                for (int c = 0; c < NR; c++) {
-                    acc[c].x += u.x * xs[p][c].x - u.y * xs[p][c].y;
-                    acc[c].y += u.x * xs[p][c].y + u.y * xs[p][c].x;
-                }
-            }
-            for (int c = 0; c < nrhs; c++) {
-                double2 v = X[(size_t)c * Np + i];
-                X[(size_t)c * Np + i] = make_double2(v.x - acc[c].x, v.y - acc[c].y);
-            }
-        }
-        __syncthreads();
+    const int nblk = Np / TB;
+    if (step < 0) {
+        const int first = upper_t ? 0 : nblk - 1;
+        tri_block<NR>(Mr, Mi, Np, X, nrhs, first * TB, upper_t, xs);
+        return;
     }
-    // backward: L^T x = y  (L^T(i, j) = M(j, i), j > i, unit diagonal)
-    for (int b0 = Np - 32; b0 >= 0; b0 -= 32) {
-        if (warp < nrhs) {
-            double2 x = X[(size_t)warp * Np + b0 + lane];
-            for (int p = 31; p >= 0; p--) {
-                double2 xp = make_double2(__shfl_sync(0xffffffffu, x.x, p), __shfl_sync(0xffffffffu, x.y, p));
-                if (lane < p) {
-                    double2 l = m(b0 + p, b0 + lane);
-                    x.x -= l.x * xp.x - l.y * xp.y;
-                    x.y -= l.x * xp.y + l.y * xp.x;
-                }
-            }
-            X[(size_t)warp * Np + b0 + lane] = x;
-            xs[lane][warp] = x;
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < b0; i += blockDim.x) {
-            double2 acc[NR];
+    // block solved last: rows s0 = step TB; this CTA's rows: the c-th block after it (forward) or
+    // before it (backward)
+    const int s0 = step * TB;
+    const int cb = upper_t ? step + 1 + blockIdx.x : step - 1 - blockIdx.x;
+    const int r0 = cb * TB;
+    for (int t = threadIdx.x; t < TB * nrhs; t += blockDim.x) {
+        int p = t % TB, c = t / TB;
+        ys[p][c] = X[(size_t)c * Np + s0 + p];
+    }
+    __syncthreads();
+    // rows r0 .. r0 + TB: two threads a row, each a half of the block's 128 terms
+    const int i = r0 + (threadIdx.x >> 1), half = threadIdx.x & 1;
+    double2 acc[NR];
 #pragma unroll
-            for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
-            for (int p = 0; p < 32; p++) {
-                double2 l = m(b0 + p, i);
+    for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
+    for (int p = half * (TB / 2); p < (half + 1) * (TB / 2); p++) {
+        const size_t o = (size_t)(s0 + p) * Np + i;
+        const double mr = Mr[o], mi = Mi[o];
 #pragma unroll
-                for (int c = 0; c < NR; c++) {
-                    acc[c].x += l.x * xs[p][c].x - l.y * xs[p][c].y;
-                    acc[c].y += l.x * xs[p][c].y + l.y * xs[p][c].x;
-                }
-            }
-            for (int c = 0; c < nrhs; c++) {
-                double2 v = X[(size_t)c * Np + i];
-                X[(size_t)c * Np + i] = make_double2(v.x - acc[c].x, v.y - acc[c].y);
-            }
+        for (int c = 0; c < NR; c++) {
+            double2 v = ys[p][c];
+            acc[c].x += mr * v.x - mi * v.y;
+            acc[c].y += mr * v.y + mi * v.x;
         }
+    }
+#pragma unroll
+    for (int c = 0; c < NR; c++) {
+        acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, 1);
+        acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, 1);
+    }
+    if (half == 0)
+        for (int c = 0; c < nrhs; c++) {
+            double2 v = X[(size_t)c * Np + i];
+            X[(size_t)c * Np + i] = make_double2(v.x - acc[c].x, v.y - acc[c].y);
+        }
+    if (blockIdx.x == 0) {
         __syncthreads();
+        tri_block<NR>(Mr, Mi, Np, X, nrhs, r0, upper_t, xs);
     }
 }
 
