@@ -254,7 +254,7 @@ def ours(args, world, rank, local, pg):
     clocks = clk.summary()
     line = {"metric": "freq solves/s at N=4096", "value": value, "unit": "freq solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == nv.HBG_FP64 else "c64+tf32/bf16",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == nv.HBG_FP64 else "c64+tf32",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "form": args.precision, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}"},
@@ -267,9 +267,40 @@ def ours(args, world, rank, local, pg):
             "phases_ms": {k: round(x, 3) for k, x in phases.items()},
             "kernels_ms": {k: round(x[0], 3) for k, x in prof.items() if x[1]},
             "clocks": clocks}
+    if precision == nv.HBG_MIXED and not args.no_plain:
+        line["plain_fp64"] = plain_comparison(nv, v, omegas, device, body)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_quick()
     return line
+
+
+def plain_comparison(nv, v, omegas, device, mixed_body):
+    """The plain FP64 form of the same job (the correctness oracle of the mixed form): its throughput,
+    the speed-up of the mixed form, and the error of the mixed A, B, X against it (per entry, over the
+    entry's largest modulus across frequencies, floor 1e-3 of the quantity's peak)."""
+    import ctypes
+
+    body = nv.Body(v, omegas, HEADINGS)
+    arr = (nv.HbgProblem * 1)(body.problem())
+    opt = nv.default_options(precision=nv.HBG_FP64, depth=DEPTH, device=device)
+    L = nv.lib()
+    nv.check(L.hbg_solve_batch(arr, 1, ctypes.byref(opt)))  # warm-up
+    ms = []
+    for _ in range(2):
+        nv.check(L.hbg_solve_batch(arr, 1, ctypes.byref(opt)))
+        ms.append(nv.last_profile()["total"])
+    step = float(np.mean(ms))
+
+    def err(got, ref):
+        ref = np.asarray(ref)
+        peak = np.abs(ref).max()
+        scale = np.maximum(np.abs(ref).max(axis=0, keepdims=True), 1e-3 * peak)
+        return float((np.abs(np.asarray(got) - ref) / scale).max())
+
+    mixed = mixed_body.results()
+    plain = body.results()
+    return {"value": len(omegas) / (step * 1e-3), "ms_per_step": step,
+            "err_vs_fp64": {k: err(mixed[k], plain[k]) for k in ("A", "B", "X")}}
 
 
 def cpu_baseline_quick():
@@ -297,7 +328,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison of the mixed form")
     ap.add_argument("--fp64-peak", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--case", default="c2", choices=["c2", "small"])

@@ -372,12 +372,12 @@ template <int NR>
 __device__ __forceinline__ void tri_block(const float* Mr, const float* Mi, int Np, double2* X, int nrhs, int b0,
                                           bool upper_t, double2 (*xs)[NR]) {
     // solve the TB x TB diagonal block of U^T (upper_t) or L^T in place in X rows b0..b0+TB
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     auto m = [&](int r, int c) { size_t o = (size_t)r * Np + c; return make_double2(Mr[o], Mi[o]); };
     if (upper_t) {
         for (int s0 = 0; s0 < TB; s0 += 32) {
-            if (warp < nrhs) {
-                double2 y = X[(size_t)warp * Np + b0 + s0 + lane];
+            for (int c = warp; c < nrhs; c += nwarps) {  // a warp per right-hand side
+                double2 y = X[(size_t)c * Np + b0 + s0 + lane];
                 for (int p = 0; p < 32; p++) {
                     if (lane == p) {
                         double2 d = m(b0 + s0 + p, b0 + s0 + p);
@@ -391,8 +391,8 @@ __device__ __forceinline__ void tri_block(const float* Mr, const float* Mi, int 
                         y.y -= u.x * yp.y + u.y * yp.x;
                     }
                 }
-                X[(size_t)warp * Np + b0 + s0 + lane] = y;
-                xs[lane][warp] = y;
+                X[(size_t)c * Np + b0 + s0 + lane] = y;
+                xs[lane][c] = y;
             }
             __syncthreads();
             for (int i = b0 + s0 + 32 + threadIdx.x; i < b0 + TB; i += blockDim.x)
@@ -409,8 +409,8 @@ __device__ __forceinline__ void tri_block(const float* Mr, const float* Mi, int 
         }
     } else {
         for (int s0 = TB - 32; s0 >= 0; s0 -= 32) {
-            if (warp < nrhs) {
-                double2 x = X[(size_t)warp * Np + b0 + s0 + lane];
+            for (int c = warp; c < nrhs; c += nwarps) {
+                double2 x = X[(size_t)c * Np + b0 + s0 + lane];
                 for (int p = 31; p >= 0; p--) {
                     double2 xp = make_double2(__shfl_sync(0xffffffffu, x.x, p), __shfl_sync(0xffffffffu, x.y, p));
                     if (lane < p) {
@@ -419,8 +419,8 @@ __device__ __forceinline__ void tri_block(const float* Mr, const float* Mi, int 
                         x.y -= l.x * xp.y + l.y * xp.x;
                     }
                 }
-                X[(size_t)warp * Np + b0 + s0 + lane] = x;
-                xs[lane][warp] = x;
+                X[(size_t)c * Np + b0 + s0 + lane] = x;
+                xs[lane][c] = x;
             }
             __syncthreads();
             for (int i = b0 + threadIdx.x; i < b0 + s0; i += blockDim.x)

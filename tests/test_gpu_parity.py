@@ -78,6 +78,16 @@ def test_finite_depth_cylinder(depth):
     compare(gpu, ref)
 
 
+def test_many_headings():
+    """12 headings: 18 right-hand sides (the wide substitution variant)."""
+    v = meshes.cylinder(1.0, 0.5, 16, 4, 4)
+    heads = list(np.linspace(0.0, 330.0, 12))
+    omegas = np.array([0.9, 2.2])
+    gpu = nv.solve(v, omegas, heads, depth=3.0)
+    ref = O.solve_body(v, omegas, heads, depth=3.0)
+    compare(gpu, ref)
+
+
 def test_interior_lid_box():
     """A box with an interior free-surface lid (kind interior: column K S, free term -4 pi, the
     in-plane log integral for pairs both in z = 0)."""

@@ -89,3 +89,14 @@ def test_mixed_interior_lid():
     ref = O.solve_body(v, omegas, [0.0, 45.0], depth=math.inf, kinds=kinds)
     errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
     assert max(errs.values()) <= MIXED_TOL, errs
+
+
+def test_mixed_many_headings():
+    """12 headings (18 right-hand sides: the wide refinement and triangular-solve variants)."""
+    v = meshes.cylinder(1.0, 0.5, 16, 4, 4)
+    heads = list(np.linspace(0.0, 330.0, 12))
+    omegas = np.array([0.9, 2.2])
+    gpu = nv.solve(v, omegas, heads, depth=3.0, precision=nv.HBG_MIXED)
+    ref = O.solve_body(v, omegas, heads, depth=3.0)
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    assert max(errs.values()) <= MIXED_TOL, errs
