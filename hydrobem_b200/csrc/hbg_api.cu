@@ -28,6 +28,15 @@ static thread_local double g_profile[6];
 static thread_local int64_t g_launches;
 
 static thread_local KernelProfiler* g_prof = nullptr;
+static thread_local Workspace* g_ws[16] = {};
+
+Workspace& workspace() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 16) dev = 0;
+    if (!g_ws[dev]) g_ws[dev] = new Workspace();
+    return *g_ws[dev];
+}
 KernelProfiler& profiler() {
     if (!g_prof) g_prof = new KernelProfiler();
     return *g_prof;
@@ -292,6 +301,24 @@ void make_fd_params(double h, double K, FdParams& fd) {
 }
 
 // ------------------------------------------------------------------ device buffers
+// A slot of the per-thread workspace (kept across calls).
+struct WsBuf {
+    Workspace& ws;
+    int slot;
+    void* p = nullptr;
+    size_t bytes = 0;
+    WsBuf(Workspace& w, int s) : ws(w), slot(s) {}
+    void alloc(size_t b) {
+        p = ws.get(slot, b);
+        if (!p) throw Failure{HB_ERR_INTERNAL, "device memory allocation failed"};
+        bytes = b;
+    }
+    template <class T>
+    T* as() const {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -334,7 +361,9 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
                 throw Failure{HB_ERR_VALUE, "a vertex lies below the sea bottom", body_index};
     }
     // ---- geometry and statics
-    DevBuf dverts, dkind, dplanes, dbad, dst, dwork, dnwork;
+    Workspace& ws = workspace();
+    WsBuf dverts(ws, WS_VERTS), dkind(ws, WS_KIND), dplanes(ws, WS_PLANES), dbad(ws, WS_BAD), dst(ws, WS_ST),
+        dwork(ws, WS_WORK), dnwork(ws, WS_NWORK);
     dverts.alloc(sizeof(double) * 12 * N);
     dkind.alloc(sizeof(int32_t) * N);
     dplanes.alloc(sizeof(double) * P_PLANES * N);
@@ -406,10 +435,13 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
                                                         : 0);
     size_t freeb = 0, totalb = 0;
     CUDA_OK(cudaMemGetInfo(&freeb, &totalb));
-    int B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)freeb) / per_freq);
+    const size_t reusable = ws.bytes[WS_S] + ws.bytes[WS_A];
+    int B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)(freeb + reusable)) / per_freq);
     if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
     B = std::min(B, F);
-    DevBuf dS, dA, du, drhs, dX, dphiI, dipiv, dinfo, dfi, dfd, dtiles, dscr, dfpt, dheads, dout;
+    WsBuf dS(ws, WS_S), dA(ws, WS_A), du(ws, WS_U), drhs(ws, WS_RHS), dX(ws, WS_X), dphiI(ws, WS_PHII),
+        dipiv(ws, WS_IPIV), dinfo(ws, WS_INFO), dfi(ws, WS_FI), dfd(ws, WS_FD), dtiles(ws, WS_TILES),
+        dscr(ws, WS_SCR), dfpt(ws, WS_FPT), dheads(ws, WS_HEADS), dout(ws, WS_OUT);
     dS.alloc(sizeof(double2) * NN * B);
     dA.alloc(sizeof(double2) * NN * B);
     du.alloc(sizeof(double2) * (size_t)nrhs * N * B);
@@ -630,6 +662,18 @@ extern "C" HbStatus hbg_kernel_profile(int32_t family, double* ms, int64_t* laun
     *ms = P.ms[family];
     *launches = P.launches[family];
     *work = P.work[family];
+    return HB_OK;
+}
+
+extern "C" HbStatus hbg_release_workspace(void) {
+    for (int d = 0; d < 16; d++)
+        if (g_ws[d]) {
+            int cur = 0;
+            cudaGetDevice(&cur);
+            cudaSetDevice(d);
+            g_ws[d]->release();
+            cudaSetDevice(cur);
+        }
     return HB_OK;
 }
 

@@ -369,6 +369,7 @@ __device__ inline void phi_direct(const FdParams& fd, int which, double xb, doub
 // Phi and its two derivatives from the per-frequency tiles (green_fin.rs:566-600)
 __device__ __forceinline__ void phi_tiles(const double* T, int which, double xb, double vb, double* v) {
     constexpr int N = TN;
+    static_assert(TN == 6, "the vectorized Horner chain below is written for degree-5 tiles");
     int ny = which == 1 ? TW : TV;
     double ymax = which == 1 ? 1.0 : 2.0;
     double ux = xb * (TS / XMAX), uy = vb * (ny / ymax);
@@ -378,15 +379,20 @@ __device__ __forceinline__ void phi_tiles(const double* T, int which, double xb,
     double tx = 2.0 * (ux - ix) - 1.0, ty = 2.0 * (uy - iy) - 1.0;
     const double* c = T + (size_t)(ix * ny + iy) * 3 * N * N;
     double v0 = 0, v1 = 0, v2 = 0;
+    // rows of N = 6 coefficients, 16-byte aligned: three double2 loads a row
 #pragma unroll
     for (int i = N - 1; i >= 0; i--) {
         double pq[3];
 #pragma unroll
         for (int q = 0; q < 3; q++) {
-            const double* r = c + q * N * N + i * N;
-            double p = __ldg(r + N - 1);
-#pragma unroll
-            for (int j = N - 2; j >= 0; j--) p = p * ty + __ldg(r + j);
+            const double2* r = reinterpret_cast<const double2*>(c + q * N * N + i * N);
+            double2 a = __ldg(r), b = __ldg(r + 1), d = __ldg(r + 2);
+            double p = d.y;
+            p = p * ty + d.x;
+            p = p * ty + b.y;
+            p = p * ty + b.x;
+            p = p * ty + a.y;
+            p = p * ty + a.x;
             pq[q] = p;
         }
         v0 = v0 * tx + pq[0];

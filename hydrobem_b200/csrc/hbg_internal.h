@@ -61,6 +61,45 @@ struct KernelProfiler {
 
 KernelProfiler& profiler();
 
+// Device buffers kept across calls (per host thread and device), by role: a solve reuses the
+// buffers of the previous one when they are large enough, so repeated solves allocate nothing.
+// hbg_release_workspace frees them.
+enum WsSlot {
+    WS_VERTS = 0, WS_KIND, WS_PLANES, WS_BAD, WS_ST, WS_WORK, WS_NWORK, WS_S, WS_A, WS_U, WS_RHS, WS_X, WS_PHII,
+    WS_IPIV, WS_INFO, WS_FI, WS_FD, WS_TILES, WS_SCR, WS_FPT, WS_HEADS, WS_OUT, WS_S32, WS_A32, WS_W, WS_P2,
+    WS_P3, WS_PL, WS_PU, WS_B, WS_XM, WS_R, WS_NORMS, WS_ERR, WS_PART, WS_DINV, WS_COUNT
+};
+
+struct Workspace {
+    void* p[WS_COUNT] = {};
+    size_t bytes[WS_COUNT] = {};
+    // a buffer of at least b bytes for the slot (nullptr when the allocation fails)
+    void* get(int slot, size_t b) {
+        if (b == 0) b = 16;
+        if (bytes[slot] >= b) return p[slot];
+        if (p[slot]) cudaFree(p[slot]);
+        p[slot] = nullptr;
+        bytes[slot] = 0;
+        if (cudaMalloc(&p[slot], b) != cudaSuccess) return nullptr;
+        bytes[slot] = b;
+        return p[slot];
+    }
+    size_t held() const {
+        size_t t = 0;
+        for (int i = 0; i < WS_COUNT; i++) t += bytes[i];
+        return t;
+    }
+    void release() {
+        for (int i = 0; i < WS_COUNT; i++) {
+            if (p[i]) cudaFree(p[i]);
+            p[i] = nullptr;
+            bytes[i] = 0;
+        }
+    }
+};
+
+Workspace& workspace();  // of the current device, this host thread
+
 // Refinement iterations of the last mixed-precision batch of this thread.
 inline int& last_ir_iterations() {
     static thread_local int n = 0;

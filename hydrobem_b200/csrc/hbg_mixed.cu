@@ -62,9 +62,9 @@ struct MixedBuffers {
 };
 
 // Refinement stops when the largest correction is below IR_TOL of the largest solution entry: the
-// solution is then that of the complex64 system to ~1e-10, far inside its ~1e-7 distance from the
+// solution is then that of the complex64 system to ~1e-9, far inside its ~1e-7 distance from the
 // FP64 system's solution (the rounding of the stored matrix).
-constexpr double IR_TOL = 1e-10;
+constexpr double IR_TOL = 1e-9;
 
 #define MIXED_FAIL(code, text, fq) \
     do {                           \
@@ -89,36 +89,47 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     size_t per = 3 * MB * 4 + 2 * prep * 4 + (size_t)(NBL * 2 * NBL + 4 * NBL * NBL) * 4 +
                  (size_t)(nrhs + H) * N * 16 + 4 * (size_t)nrhs * Np * 16 + 64 +
                  (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)FP_PLANES * N * 8 + (size_t)6912 * 3 * 8 : 0);
+    per += (size_t)(Np / NBL) * NBL * NBL * 8;  // the diagonal-block inverses
     size_t freeb = 0, totalb = 0;
     if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "cudaMemGetInfo failed", -1);
+    {
+        Workspace& w0 = workspace();
+        freeb += w0.bytes[WS_S32] + w0.bytes[WS_A32] + w0.bytes[WS_W] + w0.bytes[WS_DINV];
+    }
     int B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)freeb) / per);
     if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
     B = std::min(B, F);
-    MixedBuffers mb;
-    float* S32 = mb.get<float>(MB * B);
-    float* A32 = mb.get<float>(MB * B);
-    float* W = mb.get<float>(MB * B);
-    float* P2 = mb.get<float>(prep * B);
-    float* P3 = mb.get<float>(prep * B);
-    float* PL = mb.get<float>((size_t)NBL * 2 * NBL * B);
-    float* PU = mb.get<float>((size_t)4 * NBL * NBL * B);
-    double2* u = mb.get<double2>((size_t)nrhs * N * B);
-    double2* phiI = mb.get<double2>((size_t)std::max(H, 1) * N * B);
-    double2* b = mb.get<double2>((size_t)nrhs * Np * B);
-    double2* x = mb.get<double2>((size_t)nrhs * Np * B);
-    double2* r = mb.get<double2>((size_t)nrhs * Np * B);
-    double* norms = mb.get<double>(2 * (size_t)B);
-    int* err = mb.get<int>(1);
-    FreqInfo* dfi = mb.get<FreqInfo>(B);
-    FdParams* dfd = mb.get<FdParams>(B);
-    double* dheads = mb.get<double>(std::max(H, 1));
-    double* tiles = fin ? mb.get<double>((size_t)(T1_SIZE + T2_SIZE) * B) : nullptr;
-    double* scr = fin ? mb.get<double>((size_t)6912 * 3 * B) : nullptr;
-    double* fpt = fin ? mb.get<double>((size_t)FP_PLANES * N * B) : nullptr;
-    double* dout = mb.get<double>((72 + 3 * (size_t)H * 12) * B);
-    if (!S32 || !A32 || !W || !P2 || !P3 || !PL || !PU || !u || !phiI || !b || !x || !r || !norms || !err || !dfi ||
-        !dfd || !dheads || !dout || (fin && (!tiles || !scr || !fpt)))
-        MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
+    Workspace& ws = workspace();
+    const size_t nblk = (size_t)Np / NBL;
+    bool okb = true;
+    auto get = [&](int slot, size_t bytes) -> void* {
+        void* q = ws.get(slot, bytes);
+        okb = okb && q != nullptr;
+        return q;
+    };
+    float* S32 = (float*)get(WS_S32, MB * B * 4);
+    float* A32 = (float*)get(WS_A32, MB * B * 4);
+    float* W = (float*)get(WS_W, MB * B * 4);
+    float* P2 = (float*)get(WS_P2, prep * B * 4);
+    float* P3 = (float*)get(WS_P3, prep * B * 4);
+    float* PL = (float*)get(WS_PL, (size_t)NBL * 2 * NBL * B * 4);
+    float* PU = (float*)get(WS_PU, (size_t)4 * NBL * NBL * B * 4);
+    float2* DINV = (float2*)get(WS_DINV, nblk * NBL * NBL * B * sizeof(float2));
+    double2* u = (double2*)get(WS_U, (size_t)nrhs * N * B * 16);
+    double2* phiI = (double2*)get(WS_PHII, (size_t)std::max(H, 1) * N * B * 16);
+    double2* b = (double2*)get(WS_B, (size_t)nrhs * Np * B * 16);
+    double2* x = (double2*)get(WS_XM, (size_t)nrhs * Np * B * 16);
+    double2* r = (double2*)get(WS_R, (size_t)nrhs * Np * B * 16);
+    double* norms = (double*)get(WS_NORMS, 2 * (size_t)B * 8);
+    int* err = (int*)get(WS_ERR, sizeof(int));
+    FreqInfo* dfi = (FreqInfo*)get(WS_FI, sizeof(FreqInfo) * B);
+    FdParams* dfd = (FdParams*)get(WS_FD, sizeof(FdParams) * B);
+    double* dheads = (double*)get(WS_HEADS, sizeof(double) * std::max(H, 1));
+    double* tiles = fin ? (double*)get(WS_TILES, sizeof(double) * (T1_SIZE + T2_SIZE) * B) : nullptr;
+    double* scr = fin ? (double*)get(WS_SCR, sizeof(double) * 6912 * 3 * B) : nullptr;
+    double* fpt = fin ? (double*)get(WS_FPT, sizeof(double) * FP_PLANES * N * B) : nullptr;
+    double* dout = (double*)get(WS_OUT, sizeof(double) * (72 + 3 * (size_t)H * 12) * B);
+    if (!okb) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
     // ---- tensor maps (whole batch; the batch index is the 4th coordinate)
     CUtensorMap mapW, mapPL, mapPU, mapP2, mapP3;
     const uint64_t fb = 4;  // bytes per float
@@ -139,15 +150,13 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     std::vector<double> heads(std::max(H, 1));
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
     cudaMemcpyAsync(dheads, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(S32, 0, MB * B * 4, s);
-    cudaMemsetAsync(A32, 0, MB * B * 4, s);
     std::vector<FreqInfo> fi(B);
     std::vector<FdParams> fdh(B);
     const size_t out_per = 72 + 3 * (size_t)H * 12;
     std::vector<double> hout(out_per * B), hn(2 * (size_t)B);
     // out = bias - M x over the batch (M column-major planar FP32), FP64 accumulation
     const int nz = (N + GEMV_CHUNK - 1) / GEMV_CHUNK;
-    double2* part = mb.get<double2>((size_t)nz * B * nrhs * N);
+    double2* part = (double2*)ws.get(WS_PART, (size_t)nz * B * nrhs * N * 16);
     if (!part) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
     auto gemv = [&](const float* Mm, const double2* xv, int ldx, const double2* bias, double2* out, int nb, int fam) {
         P.begin(s);
@@ -165,24 +174,25 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         P.end(fam, 8.0 * (double)N * N * nb, s);
         *launches += 2;
     };
-    // x = A^-1 x in place with the FP32 factors in W: U^T y = x, then L^T x = y
+    // x = A^-1 x in place with the FP32 factors in W: U^T y = x, then L^T x = y, the diagonal blocks
+    // by the products with their inverses (stored by the LU)
     auto trisolve = [&](double2* xv, int nb) {
-        const int nblk = Np / TB;
+        const int nblk_i = Np / TB;
         P.begin(s);
         for (int dir = 0; dir < 2; dir++) {
             const int up = dir == 0;
-            for (int st = -1; st < nblk - 1; st++) {
-                const int cnt = st < 0 ? 1 : nblk - 1 - st;
-                const int stepi = st < 0 ? -1 : (up ? st : nblk - 1 - st);
+            for (int st = -1; st < nblk_i - 1; st++) {
+                const int cnt = st < 0 ? 1 : nblk_i - 1 - st;
+                const int stepi = st < 0 ? -1 : (up ? st : nblk_i - 1 - st);
                 dim3 g(cnt, nb);
                 if (nrhs <= 8)
-                    k_tri_step<8><<<g, 256, (TB + 32) * 8 * 16, s>>>(Np, MB, W, nrhs, xv, stepi, up);
+                    k_tri_step<8><<<g, 256, (TB + 32) * 8 * 16, s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
                 else if (nrhs <= 12)
-                    k_tri_step<12><<<g, 256, (TB + 32) * 12 * 16, s>>>(Np, MB, W, nrhs, xv, stepi, up);
+                    k_tri_step<12><<<g, 256, (TB + 32) * 12 * 16, s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
                 else if (nrhs <= 16)
-                    k_tri_step<16><<<g, 256, (TB + 32) * 16 * 16, s>>>(Np, MB, W, nrhs, xv, stepi, up);
+                    k_tri_step<16><<<g, 256, (TB + 32) * 16 * 16, s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
                 else
-                    k_tri_step<32><<<g, 256, (TB + 32) * 32 * 16, s>>>(Np, MB, W, nrhs, xv, stepi, up);
+                    k_tri_step<32><<<g, 256, (TB + 32) * 32 * 16, s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
                 (*launches)++;
             }
         }
@@ -240,7 +250,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             for (int k0 = 0; k0 < Np; k0 += NBL) {
                 const int n = Np - k0 - NBL;
                 P.begin(s);
-                k_diag_factor<<<nb, 1024, dsmem, s>>>(W, Np, MB, k0, PL, PU, err);
+                k_diag_factor<<<nb, 1024, dsmem, s>>>(W, Np, MB, k0, PL, PU, DINV, err);
                 P.end(KF_LU_PANEL, 8.0 * NBL * (double)NBL * NBL * nb, s);
                 (*launches)++;
                 if (n == 0) break;

@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_tf32(const __grid_constant__ CU
 // mixed form then reports the frequency; the FP64 form pivots).
 __global__ void __launch_bounds__(1024) k_diag_factor(float* __restrict__ W, int Np, size_t bstride, int k0,
                                                       float* __restrict__ PL, float* __restrict__ PU,
-                                                      int* __restrict__ err) {
+                                                      float2* __restrict__ DINV, int* __restrict__ err) {
     extern __shared__ float2 blk[];  // [NBL][NBL + 1]
     const int f = blockIdx.x;
     float* Wr = W + (size_t)f * bstride;
@@ -253,7 +253,12 @@ __global__ void __launch_bounds__(1024) k_diag_factor(float* __restrict__ W, int
         if (row > j && part == 0) blk[row * LD + j] = make_float2(-acc.x, -acc.y);
         __syncthreads();
     }
-    // blk now holds L^-1 (strictly below the diagonal, unit diagonal) and U^-1 (upper)
+    // blk now holds L^-1 (strictly below the diagonal, unit diagonal) and U^-1 (upper); kept per
+    // block for the triangular solves ([F][Np / NBL][NBL][NBL], row-major)
+    {
+        float2* D = DINV + ((size_t)f * (Np / NBL) + k0 / NBL) * NBL * NBL;
+        for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) D[t] = blk[(t / NBL) * LD + t % NBL];
+    }
     float* PLf = PL + (size_t)f * NBL * 2 * NBL;
     float* PUf = PU + (size_t)f * 2 * NBL * 2 * NBL;
     for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) {
@@ -368,92 +373,58 @@ __global__ void k_gemv_reduce(int N, int nrhs, int F, int nz, const double2* __r
 // next diagonal block then solves it (a warp per right-hand side, 32-row sub-blocks).
 constexpr int TB = 128;
 
+// The diagonal block b of U^T (upper_t) or L^T, solved by its stored inverse: y_b = D^T r_b with
+// D = U_bb^-1 (upper part of the stored block, with the diagonal) or L_bb^-1 (lower part, unit
+// diagonal).  Rows b0..b0+TB of X in place; thread t computes column t % TB for a set of right-hand sides.
 template <int NR>
-__device__ __forceinline__ void tri_block(const float* Mr, const float* Mi, int Np, double2* X, int nrhs, int b0,
-                                          bool upper_t, double2 (*xs)[NR]) {
-    // solve the TB x TB diagonal block of U^T (upper_t) or L^T in place in X rows b0..b0+TB
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    auto m = [&](int r, int c) { size_t o = (size_t)r * Np + c; return make_double2(Mr[o], Mi[o]); };
-    if (upper_t) {
-        for (int s0 = 0; s0 < TB; s0 += 32) {
-            for (int c = warp; c < nrhs; c += nwarps) {  // a warp per right-hand side
-                double2 y = X[(size_t)c * Np + b0 + s0 + lane];
-                for (int p = 0; p < 32; p++) {
-                    if (lane == p) {
-                        double2 d = m(b0 + s0 + p, b0 + s0 + p);
-                        double dd = d.x * d.x + d.y * d.y;
-                        y = make_double2((y.x * d.x + y.y * d.y) / dd, (y.y * d.x - y.x * d.y) / dd);
-                    }
-                    double2 yp = make_double2(__shfl_sync(0xffffffffu, y.x, p), __shfl_sync(0xffffffffu, y.y, p));
-                    if (lane > p) {
-                        double2 u = m(b0 + s0 + p, b0 + s0 + lane);
-                        y.x -= u.x * yp.x - u.y * yp.y;
-                        y.y -= u.x * yp.y + u.y * yp.x;
-                    }
-                }
-                X[(size_t)c * Np + b0 + s0 + lane] = y;
-                xs[lane][c] = y;
-            }
-            __syncthreads();
-            for (int i = b0 + s0 + 32 + threadIdx.x; i < b0 + TB; i += blockDim.x)
-                for (int c = 0; c < nrhs; c++) {
-                    double2 acc = X[(size_t)c * Np + i];
-                    for (int p = 0; p < 32; p++) {
-                        double2 u = m(b0 + s0 + p, i), v = xs[p][c];
-                        acc.x -= u.x * v.x - u.y * v.y;
-                        acc.y -= u.x * v.y + u.y * v.x;
-                    }
-                    X[(size_t)c * Np + i] = acc;
-                }
-            __syncthreads();
-        }
-    } else {
-        for (int s0 = TB - 32; s0 >= 0; s0 -= 32) {
-            for (int c = warp; c < nrhs; c += nwarps) {
-                double2 x = X[(size_t)c * Np + b0 + s0 + lane];
-                for (int p = 31; p >= 0; p--) {
-                    double2 xp = make_double2(__shfl_sync(0xffffffffu, x.x, p), __shfl_sync(0xffffffffu, x.y, p));
-                    if (lane < p) {
-                        double2 l = m(b0 + s0 + p, b0 + s0 + lane);
-                        x.x -= l.x * xp.x - l.y * xp.y;
-                        x.y -= l.x * xp.y + l.y * xp.x;
-                    }
-                }
-                X[(size_t)c * Np + b0 + s0 + lane] = x;
-                xs[lane][c] = x;
-            }
-            __syncthreads();
-            for (int i = b0 + threadIdx.x; i < b0 + s0; i += blockDim.x)
-                for (int c = 0; c < nrhs; c++) {
-                    double2 acc = X[(size_t)c * Np + i];
-                    for (int p = 0; p < 32; p++) {
-                        double2 l = m(b0 + s0 + p, i), v = xs[p][c];
-                        acc.x -= l.x * v.x - l.y * v.y;
-                        acc.y -= l.x * v.y + l.y * v.x;
-                    }
-                    X[(size_t)c * Np + i] = acc;
-                }
-            __syncthreads();
-        }
+__device__ __forceinline__ void tri_block_inv(const float2* __restrict__ D, double2* X, int Np, int nrhs, int b0,
+                                              bool upper_t, double2 (*rs)[NR]) {
+    for (int t = threadIdx.x; t < TB * nrhs; t += blockDim.x) {
+        int p = t % TB, c = t / TB;
+        rs[p][c] = X[(size_t)c * Np + b0 + p];
     }
+    __syncthreads();
+    const int i = threadIdx.x % TB, c0 = threadIdx.x / TB, cs = blockDim.x / TB;
+    double2 acc[NR];
+#pragma unroll
+    for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
+    const int pbeg = upper_t ? 0 : i, pend = upper_t ? i + 1 : TB;
+    for (int p = pbeg; p < pend; p++) {
+        float2 dv = D[p * TB + i];
+        double dr = dv.x, di = dv.y;
+        if (!upper_t && p == i) {  // the unit diagonal of L^-1
+            dr = 1.0;
+            di = 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c < NR; c++)
+            if ((c % cs) == c0) {
+                double2 v = rs[p][c];
+                acc[c].x += dr * v.x - di * v.y;
+                acc[c].y += dr * v.y + di * v.x;
+            }
+    }
+    __syncthreads();
+    for (int c = c0; c < nrhs; c += cs) X[(size_t)c * Np + b0 + i] = acc[c];
 }
 
 // One block step of the forward (upper_t) or backward solve.  step = index of the block solved by
 // the previous launch (-1: none, only the first diagonal block is solved).
 template <int NR>
-__global__ void __launch_bounds__(256) k_tri_step(int Np, size_t bstride, const float* __restrict__ W, int nrhs,
+__global__ void __launch_bounds__(256) k_tri_step(int Np, size_t bstride, const float* __restrict__ W,
+                                                  const float2* __restrict__ DINV, int nrhs,
                                                   double2* __restrict__ Xall, int step, int upper_t) {
-    extern __shared__ double2 tri_smem[];  // ys [TB][NR], then xs [32][NR]
+    extern __shared__ double2 tri_smem[];  // ys [TB][NR]
     double2(*ys)[NR] = reinterpret_cast<double2(*)[NR]>(tri_smem);
-    double2(*xs)[NR] = reinterpret_cast<double2(*)[NR]>(tri_smem + TB * NR);
     const int f = blockIdx.y;
     const float* Mr = W + (size_t)f * bstride;
     const float* Mi = Mr + (size_t)Np * Np;
     double2* X = Xall + (size_t)f * nrhs * Np;
     const int nblk = Np / TB;
+    const float2* Df = DINV + (size_t)f * nblk * TB * TB;
     if (step < 0) {
         const int first = upper_t ? 0 : nblk - 1;
-        tri_block<NR>(Mr, Mi, Np, X, nrhs, first * TB, upper_t, xs);
+        tri_block_inv<NR>(Df + (size_t)first * TB * TB, X, Np, nrhs, first * TB, upper_t, ys);
         return;
     }
     // block solved last: rows s0 = step TB; this CTA's rows: the c-th block after it (forward) or
@@ -487,13 +458,15 @@ __global__ void __launch_bounds__(256) k_tri_step(int Np, size_t bstride, const 
         acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, 1);
     }
     if (half == 0)
-        for (int c = 0; c < nrhs; c++) {
-            double2 v = X[(size_t)c * Np + i];
-            X[(size_t)c * Np + i] = make_double2(v.x - acc[c].x, v.y - acc[c].y);
-        }
+#pragma unroll
+        for (int c = 0; c < NR; c++)
+            if (c < nrhs) {
+                double2 v = X[(size_t)c * Np + i];
+                X[(size_t)c * Np + i] = make_double2(v.x - acc[c].x, v.y - acc[c].y);
+            }
     if (blockIdx.x == 0) {
         __syncthreads();
-        tri_block<NR>(Mr, Mi, Np, X, nrhs, r0, upper_t, xs);
+        tri_block_inv<NR>(Df + (size_t)cb * TB * TB, X, Np, nrhs, r0, upper_t, ys);
     }
 }
 

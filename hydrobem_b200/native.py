@@ -58,7 +58,7 @@ class HbColumn(ctypes.Structure):
 # every symbol include/hydrobem_gpu.h declares
 EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_debug_gemm_tf32",
            "hbg_last_ir_iterations", "hbg_last_profile", "hbg_last_launch_count",
-           "hbg_profile_kernels", "hbg_kernel_profile", "hb_abi_version",
+           "hbg_profile_kernels", "hbg_kernel_profile", "hbg_release_workspace", "hb_abi_version",
            "hb_last_error_message", "hb_last_error_location", "hb_model_new", "hb_model_free", "hb_model_cancel",
            "hb_object", "hb_add", "hb_set_bool", "hb_set_int", "hb_set_real", "hb_set_text", "hb_set_reals",
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity"]

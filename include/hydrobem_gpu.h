@@ -126,6 +126,10 @@ HbStatus hbg_last_profile(double *ms6);
 HbStatus hbg_profile_kernels(int32_t on);
 HbStatus hbg_kernel_profile(int32_t family, double *ms, int64_t *launches, double *work);
 
+/* Device buffers are kept across solves of the same host thread (a repeated solve allocates
+ * nothing); this frees them.  No counterpart in the reference (its buffers are per solve). */
+HbStatus hbg_release_workspace(void);
+
 /* The kernels launched by the last hbg_solve_batch of this thread. */
 HbStatus hbg_last_launch_count(int64_t *count);
 
