@@ -754,7 +754,8 @@ extern "C" HbStatus hbg_debug_matrices(const HbgBody* body, double omega, const 
     }
 }
 
-extern "C" HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const float* A, const float* B, float* C) {
+extern "C" HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const float* A, const float* B, float* C,
+                                        int32_t subtract) {
     try {
         if (!A || !B || !C) return fail({HB_ERR_ARGUMENT, "null argument"});
         int ndev = 0;
@@ -762,7 +763,7 @@ extern "C" HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const f
             return fail({HB_ERR_UNSUPPORTED, "no CUDA device: this library runs the path on the GPU only"});
         device_ctx(0);
         const char* msg = "";
-        int rc = debug_gemm_tf32(M, N, K, A, B, C, &msg);
+        int rc = debug_gemm_tf32(M, N, K, A, B, C, subtract != 0, &msg);
         if (rc) return fail({rc, msg});
         return HB_OK;
     } catch (const Failure& f) {

@@ -6,6 +6,7 @@
 // stores its matrices in complex64 too, lo_frequency.rs:1-6).
 #include <cuda.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -119,7 +120,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     double2* phiI = (double2*)get(WS_PHII, (size_t)std::max(H, 1) * N * B * 16);
     double2* b = (double2*)get(WS_B, (size_t)nrhs * Np * B * 16);
     double2* x = (double2*)get(WS_XM, (size_t)nrhs * Np * B * 16);
-    double2* r = (double2*)get(WS_R, (size_t)nrhs * Np * B * 16);
+    float2* r = (float2*)get(WS_R, (size_t)nrhs * Np * B * 8);
     double* norms = (double*)get(WS_NORMS, 2 * (size_t)B * 8);
     int* err = (int*)get(WS_ERR, sizeof(int));
     FreqInfo* dfi = (FreqInfo*)get(WS_FI, sizeof(FreqInfo) * B);
@@ -143,10 +144,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     if (!okm) MIXED_FAIL(HB_ERR_INTERNAL, "tensor-map encoding failed", -1);
     const int smem = (int)gemm_smem_bytes();
     cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int dev = 0, n_sm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     const int dsmem = NBL * (NBL + 1) * (int)sizeof(float2);
     cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, dsmem);
-    cudaFuncSetAttribute(k_tri_step<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (TB + 32) * 16 * 16);
-    cudaFuncSetAttribute(k_tri_step<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (TB + 32) * 32 * 16);
     std::vector<double> heads(std::max(H, 1));
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
     cudaMemcpyAsync(dheads, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s);
@@ -158,11 +160,13 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     const int nz = (N + GEMV_CHUNK - 1) / GEMV_CHUNK;
     double2* part = (double2*)ws.get(WS_PART, (size_t)nz * B * nrhs * N * 16);
     if (!part) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
-    auto gemv = [&](const float* Mm, const double2* xv, int ldx, const double2* bias, double2* out, int nb, int fam) {
+    auto gemv = [&](const float* Mm, const double2* xv, int ldx, const double2* bias, auto* out, int nb, int fam) {
         P.begin(s);
         dim3 g((N + 127) / 128, nb, nz);
         if (nrhs <= 8)
             k_cgemv_part<8><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
+        else if (nrhs <= 10)
+            k_cgemv_part<10><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
         else if (nrhs <= 12)
             k_cgemv_part<12><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
         else if (nrhs <= 16)
@@ -174,9 +178,9 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         P.end(fam, 8.0 * (double)N * N * nb, s);
         *launches += 2;
     };
-    // x = A^-1 x in place with the FP32 factors in W: U^T y = x, then L^T x = y, the diagonal blocks
-    // by the products with their inverses (stored by the LU)
-    auto trisolve = [&](double2* xv, int nb) {
+    // d = A^-1 d in place (complex64) with the FP32 factors in W: U^T y = d, then L^T d = y, the
+    // diagonal blocks by the products with their inverses (stored by the LU)
+    auto trisolve = [&](float2* xv, int nb) {
         const int nblk_i = Np / TB;
         P.begin(s);
         for (int dir = 0; dir < 2; dir++) {
@@ -186,13 +190,13 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 const int stepi = st < 0 ? -1 : (up ? st : nblk_i - 1 - st);
                 dim3 g(cnt, nb);
                 if (nrhs <= 8)
-                    k_tri_step<8><<<g, 256, (TB + 32) * 8 * 16, s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
+                    k_tri_step<8><<<g, TRI_THREADS, tri_smem_bytes(8), s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
+                else if (nrhs <= 10)
+                    k_tri_step<10><<<g, TRI_THREADS, tri_smem_bytes(10), s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
                 else if (nrhs <= 12)
-                    k_tri_step<12><<<g, 256, (TB + 32) * 12 * 16, s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
-                else if (nrhs <= 16)
-                    k_tri_step<16><<<g, 256, (TB + 32) * 16 * 16, s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
+                    k_tri_step<12><<<g, TRI_THREADS, tri_smem_bytes(12), s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
                 else
-                    k_tri_step<32><<<g, 256, (TB + 32) * 32 * 16, s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
+                    k_tri_step<16><<<g, TRI_THREADS, tri_smem_bytes(16), s>>>(Np, MB, W, DINV, nrhs, xv, stepi, up);
                 (*launches)++;
             }
         }
@@ -200,9 +204,10 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         P.end(KF_LU_SOLVE, 8.0 * (double)NP2 * nb, s);
     };
     auto gemm = [&](const CUtensorMap& mA, const CUtensorMap& mB, GemmArgs g, int nb) {
-        dim3 grid((g.M + GBM - 1) / GBM, (g.Nc + GBN - 1) / GBN, nb);
+        g.batch = nb;
+        const int tiles = ((g.M + GBM - 1) / GBM) * ((g.Nc + GBN - 1) / GBN) * nb;
         P.begin(s);
-        k_gemm_tf32<<<grid, 128, smem, s>>>(mA, mB, g);
+        k_gemm_tf32<<<std::min(tiles, n_sm), GEMM_THREADS, smem, s>>>(mA, mB, mapW, g);
         P.end(KF_MIXED_GEMM, 2.0 * g.M * (double)g.Nc * g.Kp * nb, s);
         (*launches)++;
     };
@@ -259,10 +264,6 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 P.end(KF_MIXED_CONVERT, 2.0 * NBL * (double)n * 4 * 3 * nb, s);
                 GemmArgs g{};
                 g.err = err;
-                g.out = W;
-                g.out_bstride = MB;
-                g.plane_stride = NP2;
-                g.ld = Np;
                 // GEMM1: L21 = M21 U11^-1
                 g.M = n;
                 g.Nc = 2 * NBL;
@@ -309,13 +310,13 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         {
             EventTimer t(s, &prof[3]);
             cudaMemsetAsync(x, 0, sizeof(double2) * nrhs * Np * nb, s);
-            cudaMemcpyAsync(r, b, sizeof(double2) * nrhs * Np * nb, cudaMemcpyDeviceToDevice, s);
+            k_to_c64<<<592, 256, 0, s>>>((size_t)nrhs * Np * nb, b, r);
+            (*launches)++;
             double prev = INFINITY;
             for (it = 0; it < 30; it++) {
                 trisolve(r, nb);
                 k_ir_update<<<nb, 256, 0, s>>>(Np, nrhs, x, r, norms);
                 cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, s);
-                gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL);
                 *launches += 1;
                 cudaStreamSynchronize(s);
                 double worst = 0.0;
@@ -324,13 +325,14 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                     if (!std::isfinite(ratio)) ratio = INFINITY;
                     worst = std::max(worst, ratio);
                 }
-                if (worst <= IR_TOL) {
+                if (worst <= IR_TOL) {  // the last correction was small: no residual needed
                     converged = true;
                     it++;
                     break;
                 }
                 if (it >= 3 && !(worst < 0.5 * prev)) break;  // stalled or diverging
                 prev = worst;
+                gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL);
             }
             t.stop();
         }
@@ -382,10 +384,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
 }
 
 // Test support: C (M x N, row-major FP32) = A (M x K, row-major) B^T where B is given N x K
-// (K-major), on the tcgen05 TF32 path of the mixed LU.  M, N, K multiples of 128, 256, 32.
-int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* C, const char** msg) {
-    if (M % 128 || N % 256 || K % 32 || M <= 0 || N <= 0 || K <= 0) {
-        *msg = "debug GEMM shape: M % 128, N % 256, K % 32";
+// (K-major), or C -= A B^T, on the tcgen05 TF32 path of the mixed LU.  M, N, K multiples of 128,
+// 128, 32.
+int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* C, bool subtract, const char** msg) {
+    if (M % GBM || N % GBN || K % GBK || M <= 0 || N <= 0 || K <= 0) {
+        *msg = "debug GEMM shape: M % 128, N % 128, K % 32";
         return HB_ERR_VALUE;
     }
     if (!encode_fn()) {
@@ -403,10 +406,12 @@ int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* 
     }
     cudaMemcpy(dA, A, sizeof(float) * M * K, cudaMemcpyHostToDevice);
     cudaMemcpy(dB, B, sizeof(float) * N * K, cudaMemcpyHostToDevice);
+    if (subtract) cudaMemcpy(dC, C, sizeof(float) * M * N, cudaMemcpyHostToDevice);
     cudaMemset(err, 0, sizeof(int));
-    CUtensorMap mA, mB;
+    CUtensorMap mA, mB, mC;
     if (!make_map(&mA, dA, K, M, 1, 1, (uint64_t)K * 4, (uint64_t)M * K * 4, (uint64_t)M * K * 4, GBM) ||
-        !make_map(&mB, dB, K, N, 1, 1, (uint64_t)K * 4, (uint64_t)N * K * 4, (uint64_t)N * K * 4, GBN)) {
+        !make_map(&mB, dB, K, N, 1, 1, (uint64_t)K * 4, (uint64_t)N * K * 4, (uint64_t)N * K * 4, GBN) ||
+        !make_map(&mC, dC, N, M, 1, 1, (uint64_t)N * 4, (uint64_t)M * N * 4, (uint64_t)M * N * 4, GBM)) {
         *msg = "tensor-map encoding failed";
         return HB_ERR_INTERNAL;
     }
@@ -415,16 +420,18 @@ int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* 
     g.Nc = N;
     g.Kp = K;
     g.a_planar = 0;
-    g.mode = 0;
-    g.out = dC;
-    g.out_bstride = (size_t)M * N;
-    g.plane_stride = 0;
-    g.ld = N;
+    g.mode = subtract ? 2 : 0;
     g.o_nc = N;
+    g.batch = 1;
     g.err = err;
     const int smem = (int)gemm_smem_bytes();
     cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    k_gemm_tf32<<<dim3(M / GBM, N / GBN, 1), 128, smem>>>(mA, mB, g);
+    int dev = 0, n_sm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    // fewer CTAs than tiles, so that the persistent loop and both accumulator buffers are exercised
+    const int tiles = (M / GBM) * (N / GBN);
+    k_gemm_tf32<<<std::max(1, std::min(tiles / 3, n_sm)), GEMM_THREADS, smem>>>(mA, mB, mC, g);
     int herr = 0;
     cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost);
     cudaMemcpy(C, dC, sizeof(float) * M * N, cudaMemcpyDeviceToHost);

@@ -13,6 +13,6 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                             bool finite, double depth, cudaStream_t s, double* prof, int64_t* launches,
                             const char** msg, int64_t* freq);
 
-int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* C, const char** msg);
+int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* C, bool subtract, const char** msg);
 
 }  // namespace hbg

@@ -19,16 +19,15 @@
 namespace hbg {
 
 constexpr int NBL = 128;  // LU block width (complex columns)
-constexpr int GBM = 128, GBK = 32, GSTAGES = 4, GBN = 256;
+constexpr int GBM = 128, GBK = 32, GSTAGES = 4, GBN = 128;
 
 struct GemmArgs {
     int M, Nc, Kp;         // rows, real output columns, real inner dimension
     int a_planar;          // A from the planar matrix (x = a_x0 + kk % a_kc, plane = kk / a_kc) or a packed buffer
     int a_x0, a_kc, a_row0;
     int mode;              // 0 store, 1 store and scatter into the GEMM3 operand, 2 subtract
-    float* out;            // planar matrices [F][2][Np][Np] (row-major view)
-    size_t out_bstride, plane_stride;
-    int ld, o_row0, o_col0, o_nc;
+    int o_row0, o_col0, o_nc;  // output placement in the planar matrix: column j' -> plane j' / o_nc
+    int batch;             // matrices in the launch
     float* p3;             // GEMM3's B operand [F][2n][2 NBL] (mode 1)
     size_t p3_bstride;
     int p3_n;
@@ -39,127 +38,213 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
     return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
 }
 
-constexpr size_t gemm_smem_bytes() {
-    return 1024 + (size_t)GSTAGES * (GBM + GBN) * GBK * 4 + 256;
-}
+constexpr int GEMM_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
+constexpr size_t GEMM_STAGE_BYTES = (size_t)(GBM + GBN) * GBK * 4;
+constexpr size_t GEMM_C_BYTES = (size_t)GBM * GBN * 4;  // the output tile, four 32-column boxes
+constexpr size_t gemm_smem_bytes() { return 1024 + GSTAGES * GEMM_STAGE_BYTES + GEMM_C_BYTES + 256; }
 
-// One 128 x 256 output tile per block: warp 0 lane 0 issues the TMA loads (4-stage ring), warp 1
-// lane 0 the tcgen05.mma chain, then all four warps read the accumulator from TMEM (warp w owns
-// rows 32w..32w+31) and apply the epilogue.
-__global__ void __launch_bounds__(128, 1) k_gemm_tf32(const __grid_constant__ CUtensorMap mapA,
-                                                      const __grid_constant__ CUtensorMap mapB, GemmArgs g) {
+// Persistent, warp-specialized TF32 GEMM of the mixed LU: tiles of 128 x 128 (real columns) taken
+// round-robin over (row tile, column tile, matrix).  Warp 0 lane 0 streams the A/B k-chunks through a
+// 4-stage TMA ring and prefetches the tile's C block (mode 2) into shared memory; warp 1 lane 0
+// issues tcgen05.mma into one of two TMEM accumulators; warps 2..5 read the accumulator
+// (tcgen05.ld), combine it with the C block in shared memory, and write the tile back with TMA
+// stores -- so the epilogue of a tile overlaps the main loop of the next.  C / D tiles live in
+// shared memory in the 128-byte swizzle of four 32-column boxes (conflict-free 16-byte accesses).
+__global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_constant__ CUtensorMap mapA,
+                                                               const __grid_constant__ CUtensorMap mapB,
+                                                               const __grid_constant__ CUtensorMap mapC,
+                                                               GemmArgs g) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* base = align1024(smem_raw);
     float* sA = reinterpret_cast<float*>(base);
     float* sB = sA + GSTAGES * GBM * GBK;
-    uint64_t* full = reinterpret_cast<uint64_t*>(sB + GSTAGES * GBN * GBK);
+    float* sC = sB + GSTAGES * GBN * GBK;  // [4 boxes][128 rows][32]
+    uint64_t* full = reinterpret_cast<uint64_t*>(sC + GBM * GBN);
     uint64_t* empty = full + GSTAGES;
-    uint64_t* done = empty + GSTAGES;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+    uint64_t* tfull = empty + GSTAGES;  // [2]
+    uint64_t* tempty = tfull + 2;       // [2]
+    uint64_t* cfull = tempty + 2;
+    uint64_t* cempty = cfull + 1;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(cempty + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * GBM, n0 = blockIdx.y * GBN, f = blockIdx.z;
+    const int mt = (g.M + GBM - 1) / GBM, nt = (g.Nc + GBN - 1) / GBN;
+    const int ntiles = mt * nt * g.batch;
     const int nk = g.Kp / GBK;
     if (threadIdx.x == 0) {
         for (int s = 0; s < GSTAGES; s++) {
             tc::mbar_init(&full[s], 1);
             tc::mbar_init(&empty[s], 1);
         }
-        tc::mbar_init(done, 1);
+        for (int b = 0; b < 2; b++) {
+            tc::mbar_init(&tfull[b], 1);
+            tc::mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
+        }
+        tc::mbar_init(cfull, 1);
+        tc::mbar_init(cempty, 1);
         tc::fence_barrier_init();
         tc::prefetch_tensormap(&mapA);
         tc::prefetch_tensormap(&mapB);
+        tc::prefetch_tensormap(&mapC);
     }
-    if (warp == 0) tc::tmem_alloc(tslot, GBN);
+    if (warp == 0) tc::tmem_alloc(tslot, 2 * GBN);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *tslot;
-    if (warp == 0 && lane == 0) {
-        const uint32_t bytes = (GBM + GBN) * GBK * 4;
-        for (int kc = 0; kc < nk; kc++) {
-            const int s = kc % GSTAGES;
-            if (kc >= GSTAGES && !tc::mbar_wait(&empty[s], ((kc / GSTAGES) - 1) & 1)) {
-                atomicExch(g.err, 1);
-                break;
-            }
-            tc::mbar_arrive_expect_tx(&full[s], bytes);
-            const int kk = kc * GBK;
-            int ax = kk, plane = 0;
-            if (g.a_planar) {
-                ax = g.a_x0 + kk % g.a_kc;
-                plane = kk / g.a_kc;
-            }
-            tc::tma_load_4d(sA + s * GBM * GBK, &mapA, &full[s], ax, g.a_row0 + m0, plane, f);
-            tc::tma_load_4d(sB + s * GBN * GBK, &mapB, &full[s], kk, n0, 0, f);
-        }
-    } else if (warp == 1 && lane == 0) {
-        const uint32_t idesc = tc::idesc_tf32(GBM, GBN);
-        for (int kc = 0; kc < nk; kc++) {
-            const int s = kc % GSTAGES;
-            if (!tc::mbar_wait(&full[s], (kc / GSTAGES) & 1)) {
-                atomicExch(g.err, 2);
-                break;
-            }
-            tc::tc_fence_after();
-            const uint32_t a0 = tc::smem_u32(sA + s * GBM * GBK), b0 = tc::smem_u32(sB + s * GBN * GBK);
-#pragma unroll
-            for (int k8 = 0; k8 < GBK / 8; k8++)
-                tc::mma_tf32(tmem, tc::desc_kmajor_sw128(a0 + 32 * k8), tc::desc_kmajor_sw128(b0 + 32 * k8), idesc,
-                             (kc | k8) != 0);
-            tc::mma_commit(&empty[s]);
-        }
-        tc::mma_commit(done);
-    }
-    __syncwarp();
-    const bool ok = tc::mbar_wait(done, 0);
-    if (!ok) atomicExch(g.err, 3);
-    __syncwarp();
-    tc::tc_fence_after();
-    const int row = m0 + warp * 32 + lane;
-    float* outf = g.out + (size_t)f * g.out_bstride;
-    float* p3f = g.p3 ? g.p3 + (size_t)f * g.p3_bstride : nullptr;
-    for (int c = 0; c < GBN / 32; c++) {
-        float v[32];
-        tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + c * 32, v);
-        const int jg0 = n0 + c * 32;
-        if (!ok || row >= g.M || jg0 >= g.Nc) continue;
-        const int plane = jg0 >= g.o_nc ? 1 : 0;
-        const int col0 = jg0 - plane * g.o_nc;
-        float* p = outf + plane * g.plane_stride + (size_t)(g.o_row0 + row) * g.ld + g.o_col0 + col0;
-        float4* p4 = reinterpret_cast<float4*>(p);
-        if (g.mode == 2) {
-#pragma unroll
-            for (int q = 0; q < 8; q++) {
-                float4 o = p4[q];
-                o.x -= v[4 * q];
-                o.y -= v[4 * q + 1];
-                o.z -= v[4 * q + 2];
-                o.w -= v[4 * q + 3];
-                p4[q] = o;
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < 8; q++) p4[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-            if (g.mode == 1) {
-                // U12(kk = row, j) into the block-real K-major operand of GEMM3 (rows 2n, 2 NBL wide)
-                const int n = g.p3_n;
-#pragma unroll 4
-                for (int i = 0; i < 32; i++) {
-                    const int j = col0 + i;
-                    if (plane == 0) {
-                        p3f[(size_t)j * (2 * NBL) + row] = v[i];
-                        p3f[(size_t)(n + j) * (2 * NBL) + NBL + row] = v[i];
-                    } else {
-                        p3f[(size_t)j * (2 * NBL) + NBL + row] = -v[i];
-                        p3f[(size_t)(n + j) * (2 * NBL) + row] = v[i];
+    auto tile_coords = [&](int t, int& m0, int& n0, int& f) {
+        f = t / (mt * nt);
+        int r = t % (mt * nt);
+        n0 = (r / mt) * GBN;  // row tiles fastest: consecutive CTAs share the B block
+        m0 = (r % mt) * GBM;
+    };
+    if (warp == 0) {
+        if (lane == 0) {
+            int kc_global = 0, it = 0;
+            bool bad = false;
+            for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x, it++) {
+                int m0, n0, f;
+                tile_coords(t, m0, n0, f);
+                for (int kc = 0; kc < nk; kc++, kc_global++) {
+                    const int s = kc_global % GSTAGES;
+                    if (kc_global >= GSTAGES && !tc::mbar_wait(&empty[s], ((kc_global / GSTAGES) - 1) & 1)) {
+                        atomicExch(g.err, 1);
+                        bad = true;
+                        break;
                     }
+                    tc::mbar_arrive_expect_tx(&full[s], (uint32_t)GEMM_STAGE_BYTES);
+                    const int kk = kc * GBK;
+                    int ax = kk, plane = 0;
+                    if (g.a_planar) {
+                        ax = g.a_x0 + kk % g.a_kc;
+                        plane = kk / g.a_kc;
+                    }
+                    tc::tma_load_4d(sA + s * GBM * GBK, &mapA, &full[s], ax, g.a_row0 + m0, plane, f);
+                    tc::tma_load_4d(sB + s * GBN * GBK, &mapB, &full[s], kk, n0, 0, f);
+                }
+                if (!bad && g.mode == 2) {
+                    // the C block of this tile, once the previous tile's store has read the buffer (the
+                    // k-chunks above are already queued, so the main loop runs on meanwhile)
+                    if (it > 0 && !tc::mbar_wait(cempty, (it - 1) & 1)) {
+                        atomicExch(g.err, 4);
+                        break;
+                    }
+                    const int plane = n0 >= g.o_nc ? 1 : 0, col0 = n0 - plane * g.o_nc;
+                    tc::mbar_arrive_expect_tx(cfull, (uint32_t)GEMM_C_BYTES);
+                    for (int q = 0; q < GBN / 32; q++)
+                        tc::tma_load_4d(sC + q * GBM * 32, &mapC, cfull, g.o_col0 + col0 + 32 * q, g.o_row0 + m0, plane,
+                                        f);
                 }
             }
         }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_tf32(GBM, GBN);
+            int kc_global = 0, it = 0;
+            for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+                const int b = it & 1;
+                // the accumulator buffer must have been drained by the epilogue of tile it - 2
+                if (it >= 2 && !tc::mbar_wait(&tempty[b], ((it >> 1) - 1) & 1)) {
+                    atomicExch(g.err, 5);
+                    break;
+                }
+                tc::tc_fence_after();
+                const uint32_t d = tmem + b * GBN;
+                bool bad = false;
+                for (int kc = 0; kc < nk; kc++, kc_global++) {
+                    const int s = kc_global % GSTAGES;
+                    if (!tc::mbar_wait(&full[s], (kc_global / GSTAGES) & 1)) {
+                        atomicExch(g.err, 2);
+                        bad = true;
+                        break;
+                    }
+                    tc::tc_fence_after();
+                    const uint32_t a0 = tc::smem_u32(sA + s * GBM * GBK), b0 = tc::smem_u32(sB + s * GBN * GBK);
+#pragma unroll
+                    for (int k8 = 0; k8 < GBK / 8; k8++)
+                        tc::mma_tf32(d, tc::desc_kmajor_sw128(a0 + 32 * k8), tc::desc_kmajor_sw128(b0 + 32 * k8), idesc,
+                                     (kc | k8) != 0);
+                    tc::mma_commit(&empty[s]);
+                }
+                tc::mma_commit(&tfull[b]);
+                if (bad) break;
+            }
+        }
+    } else {
+        // epilogue warps 2..5: TMEM lane quadrant (warp % 4), rows 32 (warp % 4) .. + 32 of the tile
+        const int quad = warp & 3;
+        const int r = quad * 32 + lane;  // row within the tile
+        int it = 0;
+        for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
+            int m0, n0, f;
+            tile_coords(t, m0, n0, f);
+            const int b = it & 1;
+            bool ok = tc::mbar_wait(&tfull[b], (it >> 1) & 1);
+            if (ok && g.mode == 2) ok = tc::mbar_wait(cfull, it & 1);
+            if (ok && g.mode != 2 && it > 0) ok = tc::mbar_wait(cempty, (it - 1) & 1);  // the store buffer is free
+            // one decision for the four epilogue warps, so none waits at a barrier the others left
+            __syncwarp();
+            if (!tc::bar_and(ok, 1, 128)) {
+                if (threadIdx.x == 64) atomicExch(g.err, 3);
+                break;
+            }
+            tc::tc_fence_after();
+            const int plane = n0 >= g.o_nc ? 1 : 0, col0 = n0 - plane * g.o_nc;
+            for (int q = 0; q < GBN / 32; q++) {
+                float v[32];
+                tc::tmem_ld32(tmem + b * GBN + ((uint32_t)(quad * 32) << 16) + q * 32, v);
+                float* row = sC + q * GBM * 32 + r * 32;  // 128 B, 16-byte chunks swizzled by r % 8
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    float4* c4 = reinterpret_cast<float4*>(row + 4 * (j ^ (r & 7)));
+                    float4 o;
+                    if (g.mode == 2) {
+                        o = *c4;
+                        o.x -= v[4 * j];
+                        o.y -= v[4 * j + 1];
+                        o.z -= v[4 * j + 2];
+                        o.w -= v[4 * j + 3];
+                    } else {
+                        o = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+                    }
+                    *c4 = o;
+                }
+                if (g.mode == 1 && m0 + r < g.M) {
+                    // U12(kk = row, j) into the block-real K-major operand of GEMM3 (rows 2n, 2 NBL wide)
+                    float* p3f = g.p3 + (size_t)f * g.p3_bstride;
+                    const int n = g.p3_n, kk = m0 + r;
+#pragma unroll
+                    for (int i = 0; i < 32; i++) {
+                        const int j = col0 + 32 * q + i;
+                        if (plane == 0) {
+                            p3f[(size_t)j * (2 * NBL) + kk] = v[i];
+                            p3f[(size_t)(n + j) * (2 * NBL) + NBL + kk] = v[i];
+                        } else {
+                            p3f[(size_t)j * (2 * NBL) + NBL + kk] = -v[i];
+                            p3f[(size_t)(n + j) * (2 * NBL) + kk] = v[i];
+                        }
+                    }
+                }
+            }
+            // the accumulator buffer is free for the MMA of tile it + 2
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&tempty[b]);
+            // all four epilogue warps have written the tile: one thread stores it
+            tc::fence_proxy_async_smem();
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+            if (warp == 2 && lane == 0) {
+                for (int q = 0; q < GBN / 32; q++)
+                    tc::tma_store_4d(&mapC, sC + q * GBM * 32, g.o_col0 + col0 + 32 * q, g.o_row0 + m0, plane, f);
+                tc::bulk_commit();
+                tc::bulk_wait_read();  // the buffer may be refilled once the store has read it
+                tc::mbar_arrive(cempty);
+            }
+        }
+        if (warp == 2 && lane == 0) tc::bulk_wait_all();
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 0) tc::tmem_dealloc(tmem, GBN);
+    if (warp == 0) tc::tmem_dealloc(tmem, 2 * GBN);
 }
 
 // ---- diagonal block: M11 = L11 U11 (no pivoting) in shared memory, then L11^-1 and U11^-1.
@@ -333,25 +418,62 @@ __global__ void __launch_bounds__(128) k_cgemv_part(int N, int Np, size_t bstrid
         __syncthreads();
         if (k < N) {
             const int lim = min(CH, nend - n0);
-#pragma unroll 4
-            for (int nn = 0; nn < lim; nn++) {
-                const size_t o = (size_t)(n0 + nn) * Np + k;
-                const double mr = Mr[o], mi = Mi[o];
+            if (lim == CH) {
+                // a full chunk: the matrix entries of 8 columns loaded ahead of their products
 #pragma unroll
-                for (int c = 0; c < NR; c++) {
-                    double2 v = sx[nn][c];
-                    acc[c].x += mr * v.x - mi * v.y;
-                    acc[c].y += mr * v.y + mi * v.x;
+                for (int q = 0; q < CH; q += 8) {
+                    float mr[8], mi[8];
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        const size_t o = (size_t)(n0 + q + j) * Np + k;
+                        mr[j] = Mr[o];
+                        mi[j] = Mi[o];
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; j++) {
+                        const double dr = mr[j], di = mi[j];
+#pragma unroll
+                        for (int c = 0; c < NR; c++) {
+                            const double2 v = sx[q + j][c];
+                            acc[c].x += dr * v.x - di * v.y;
+                            acc[c].y += dr * v.y + di * v.x;
+                        }
+                    }
+                }
+            } else {
+                for (int nn = 0; nn < lim; nn++) {
+                    const size_t o = (size_t)(n0 + nn) * Np + k;
+                    const double mr = Mr[o], mi = Mi[o];
+#pragma unroll
+                    for (int c = 0; c < NR; c++) {
+                        const double2 v = sx[nn][c];
+                        acc[c].x += mr * v.x - mi * v.y;
+                        acc[c].y += mr * v.y + mi * v.x;
+                    }
                 }
             }
         }
     }
     if (k < N)
-        for (int c = 0; c < nrhs && c < NR; c++) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
+#pragma unroll
+        for (int c = 0; c < NR; c++)
+            if (c < nrhs) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
 }
 
+template <class T>
+__device__ __forceinline__ T make_out(double x, double y);
+template <>
+__device__ __forceinline__ double2 make_out<double2>(double x, double y) {
+    return make_double2(x, y);
+}
+template <>
+__device__ __forceinline__ float2 make_out<float2>(double x, double y) {
+    return make_float2((float)x, (float)y);
+}
+
+template <class T>
 __global__ void k_gemv_reduce(int N, int nrhs, int F, int nz, const double2* __restrict__ part,
-                              const double2* __restrict__ bias, int ldb, double2* __restrict__ out, int ldo) {
+                              const double2* __restrict__ bias, int ldb, T* __restrict__ out, int ldo) {
     const int f = blockIdx.y;
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (size_t)nrhs * N) return;
@@ -363,115 +485,139 @@ __global__ void k_gemv_reduce(int N, int nrhs, int F, int nz, const double2* __r
         si += v.y;
     }
     double2 b = bias ? bias[((size_t)f * nrhs + c) * ldb + k] : make_double2(0.0, 0.0);
-    out[((size_t)f * nrhs + c) * ldo + k] = make_double2(b.x - sr, b.y - si);
+    out[((size_t)f * nrhs + c) * ldo + k] = make_out<T>(b.x - sr, b.y - si);
 }
 
-// x = A^-1 r with the factors of M = A^T = L U (FP32 planar, row-major in W): U^T y = r, then
-// L^T x = y, FP64 vectors [F][nrhs][Np] in place, in blocks of TB = 128 rows.  One launch per
-// block step: every CTA of the step owns 128 rows, subtracts the contribution of the block solved
-// by the previous step (row b0 + p of W read along its rows: coalesced), and the CTA that owns the
-// next diagonal block then solves it (a warp per right-hand side, 32-row sub-blocks).
+// d = A^-1 r with the factors of M = A^T = L U (FP32 planar, row-major in W): U^T y = r, then
+// L^T d = y, in FP32 (the correction only needs the accuracy of the TF32 factors; the residual that
+// sets the attainable accuracy is formed in FP64), vectors [F][nrhs][Np] complex64 in place, in
+// blocks of TB = 128 rows.  One launch per block step: every CTA of the step owns 128 rows and
+// subtracts the contribution of the block solved by the previous step (row s0 + p of W read along
+// its rows: coalesced); the CTA that owns the next diagonal block then solves it by the stored
+// inverse of that block.
 constexpr int TB = 128;
+constexpr int TRI_THREADS = 128;
 
-// The diagonal block b of U^T (upper_t) or L^T, solved by its stored inverse: y_b = D^T r_b with
+// The diagonal block of U^T (upper_t) or L^T, solved by its stored inverse: y_b = D^T r_b with
 // D = U_bb^-1 (upper part of the stored block, with the diagonal) or L_bb^-1 (lower part, unit
-// diagonal).  Rows b0..b0+TB of X in place; thread t computes column t % TB for a set of right-hand sides.
+// diagonal).  Rows b0..b0+TB of X in place, right-hand sides in chunks of NR; thread t owns column t.
 template <int NR>
-__device__ __forceinline__ void tri_block_inv(const float2* __restrict__ D, double2* X, int Np, int nrhs, int b0,
-                                              bool upper_t, double2 (*rs)[NR]) {
-    for (int t = threadIdx.x; t < TB * nrhs; t += blockDim.x) {
-        int p = t % TB, c = t / TB;
-        rs[p][c] = X[(size_t)c * Np + b0 + p];
-    }
-    __syncthreads();
-    const int i = threadIdx.x % TB, c0 = threadIdx.x / TB, cs = blockDim.x / TB;
-    double2 acc[NR];
+__device__ __forceinline__ void tri_diag_f32(const float2* __restrict__ D, float2* X, int Np, int nrhs, int b0,
+                                             bool upper_t, float2 (*rs)[NR]) {
+    const int i = threadIdx.x;
+    const int pbeg = upper_t ? 0 : i + 1, pend = upper_t ? i + 1 : TB;
+    for (int c0 = 0; c0 < nrhs; c0 += NR) {
+        const int nc = min(NR, nrhs - c0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < TB * NR; t += blockDim.x) {
+            const int p = t % TB, c = t / TB;
+            rs[p][c] = c < nc ? X[(size_t)(c0 + c) * Np + b0 + p] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        float2 acc[NR];
 #pragma unroll
-    for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
-    const int pbeg = upper_t ? 0 : i, pend = upper_t ? i + 1 : TB;
-    for (int p = pbeg; p < pend; p++) {
-        float2 dv = D[p * TB + i];
-        double dr = dv.x, di = dv.y;
-        if (!upper_t && p == i) {  // the unit diagonal of L^-1
-            dr = 1.0;
-            di = 0.0;
+        for (int c = 0; c < NR; c++) acc[c] = upper_t ? make_float2(0.f, 0.f) : rs[i][c];  // unit diagonal of L^-1
+#pragma unroll 4
+        for (int p = pbeg; p < pend; p++) {
+            const float2 dv = D[p * TB + i];
+#pragma unroll
+            for (int c = 0; c < NR; c++) {
+                const float2 v = rs[p][c];
+                acc[c].x += dv.x * v.x - dv.y * v.y;
+                acc[c].y += dv.x * v.y + dv.y * v.x;
+            }
         }
 #pragma unroll
         for (int c = 0; c < NR; c++)
-            if ((c % cs) == c0) {
-                double2 v = rs[p][c];
-                acc[c].x += dr * v.x - di * v.y;
-                acc[c].y += dr * v.y + di * v.x;
-            }
+            if (c < nc) X[(size_t)(c0 + c) * Np + b0 + i] = acc[c];
     }
-    __syncthreads();
-    for (int c = c0; c < nrhs; c += cs) X[(size_t)c * Np + b0 + i] = acc[c];
 }
 
 // One block step of the forward (upper_t) or backward solve.  step = index of the block solved by
-// the previous launch (-1: none, only the first diagonal block is solved).
+// the previous launch (-1: none, only the first diagonal block is solved).  Thread layout: warp w
+// owns rows 32 (w % 2) + lane and 64 more, and the half w / 2 of the solved block's 128 entries;
+// every lane of a warp reads the same solved entry (a shared-memory broadcast).
 template <int NR>
-__global__ void __launch_bounds__(256) k_tri_step(int Np, size_t bstride, const float* __restrict__ W,
-                                                  const float2* __restrict__ DINV, int nrhs,
-                                                  double2* __restrict__ Xall, int step, int upper_t) {
-    extern __shared__ double2 tri_smem[];  // ys [TB][NR]
-    double2(*ys)[NR] = reinterpret_cast<double2(*)[NR]>(tri_smem);
+__global__ void __launch_bounds__(TRI_THREADS) k_tri_step(int Np, size_t bstride, const float* __restrict__ W,
+                                                          const float2* __restrict__ DINV, int nrhs,
+                                                          float2* __restrict__ Xall, int step, int upper_t) {
+    extern __shared__ float2 tri_smem[];  // ys [TB][NR], partial sums [TB][NR]
+    float2(*ys)[NR] = reinterpret_cast<float2(*)[NR]>(tri_smem);
+    float2(*pt)[NR] = reinterpret_cast<float2(*)[NR]>(tri_smem + TB * NR);
     const int f = blockIdx.y;
     const float* Mr = W + (size_t)f * bstride;
     const float* Mi = Mr + (size_t)Np * Np;
-    double2* X = Xall + (size_t)f * nrhs * Np;
+    float2* X = Xall + (size_t)f * nrhs * Np;
     const int nblk = Np / TB;
     const float2* Df = DINV + (size_t)f * nblk * TB * TB;
     if (step < 0) {
         const int first = upper_t ? 0 : nblk - 1;
-        tri_block_inv<NR>(Df + (size_t)first * TB * TB, X, Np, nrhs, first * TB, upper_t, ys);
+        tri_diag_f32<NR>(Df + (size_t)first * TB * TB, X, Np, nrhs, first * TB, upper_t, ys);
         return;
     }
-    // block solved last: rows s0 = step TB; this CTA's rows: the c-th block after it (forward) or
-    // before it (backward)
     const int s0 = step * TB;
     const int cb = upper_t ? step + 1 + blockIdx.x : step - 1 - blockIdx.x;
     const int r0 = cb * TB;
-    for (int t = threadIdx.x; t < TB * nrhs; t += blockDim.x) {
-        int p = t % TB, c = t / TB;
-        ys[p][c] = X[(size_t)c * Np + s0 + p];
-    }
-    __syncthreads();
-    // rows r0 .. r0 + TB: two threads a row, each a half of the block's 128 terms
-    const int i = r0 + (threadIdx.x >> 1), half = threadIdx.x & 1;
-    double2 acc[NR];
-#pragma unroll
-    for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
-    for (int p = half * (TB / 2); p < (half + 1) * (TB / 2); p++) {
-        const size_t o = (size_t)(s0 + p) * Np + i;
-        const double mr = Mr[o], mi = Mi[o];
-#pragma unroll
-        for (int c = 0; c < NR; c++) {
-            double2 v = ys[p][c];
-            acc[c].x += mr * v.x - mi * v.y;
-            acc[c].y += mr * v.y + mi * v.x;
-        }
-    }
-#pragma unroll
-    for (int c = 0; c < NR; c++) {
-        acc[c].x += __shfl_xor_sync(0xffffffffu, acc[c].x, 1);
-        acc[c].y += __shfl_xor_sync(0xffffffffu, acc[c].y, 1);
-    }
-    if (half == 0)
-#pragma unroll
-        for (int c = 0; c < NR; c++)
-            if (c < nrhs) {
-                double2 v = X[(size_t)c * Np + i];
-                X[(size_t)c * Np + i] = make_double2(v.x - acc[c].x, v.y - acc[c].y);
-            }
-    if (blockIdx.x == 0) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int li = 32 * (warp & 1) + lane;  // local rows li and li + 64
+    const int ph = warp >> 1;
+    const float* pr = Mr + (size_t)(s0 + ph * 64) * Np + r0 + li;
+    const float* pi = Mi + (size_t)(s0 + ph * 64) * Np + r0 + li;
+    for (int c0 = 0; c0 < nrhs; c0 += NR) {
+        const int nc = min(NR, nrhs - c0);
         __syncthreads();
-        tri_block_inv<NR>(Df + (size_t)cb * TB * TB, X, Np, nrhs, r0, upper_t, ys);
+        for (int t = threadIdx.x; t < TB * NR; t += blockDim.x) {
+            const int p = t % TB, c = t / TB;
+            ys[p][c] = c < nc ? X[(size_t)(c0 + c) * Np + s0 + p] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        float2 a0[NR], a1[NR];
+#pragma unroll
+        for (int c = 0; c < NR; c++) a0[c] = a1[c] = make_float2(0.f, 0.f);
+#pragma unroll 8
+        for (int p = 0; p < 64; p++) {
+            const size_t o = (size_t)p * Np;
+            const float r0v = pr[o], i0v = pi[o], r1v = pr[o + 64], i1v = pi[o + 64];
+#pragma unroll
+            for (int c = 0; c < NR; c++) {
+                const float2 v = ys[ph * 64 + p][c];
+                a0[c].x += r0v * v.x - i0v * v.y;
+                a0[c].y += r0v * v.y + i0v * v.x;
+                a1[c].x += r1v * v.x - i1v * v.y;
+                a1[c].y += r1v * v.y + i1v * v.x;
+            }
+        }
+        if (ph == 1)
+#pragma unroll
+            for (int c = 0; c < NR; c++) {
+                pt[li][c] = a0[c];
+                pt[li + 64][c] = a1[c];
+            }
+        __syncthreads();
+        if (ph == 0)
+#pragma unroll
+            for (int c = 0; c < NR; c++)
+                if (c < nc) {
+                    float2* x0 = X + (size_t)(c0 + c) * Np + r0 + li;
+                    float2 v0 = x0[0], v1 = x0[64];
+                    const float2 q0 = pt[li][c], q1 = pt[li + 64][c];
+                    x0[0] = make_float2(v0.x - (a0[c].x + q0.x), v0.y - (a0[c].y + q0.y));
+                    x0[64] = make_float2(v1.x - (a1[c].x + q1.x), v1.y - (a1[c].y + q1.y));
+                }
     }
+    if (blockIdx.x == 0) tri_diag_f32<NR>(Df + (size_t)cb * TB * TB, X, Np, nrhs, r0, upper_t, ys);
+}
+
+constexpr size_t tri_smem_bytes(int nr) { return (size_t)2 * TB * nr * sizeof(float2); }
+
+// FP64 vectors to complex64 (the right-hand sides entering the first correction).
+__global__ void k_to_c64(size_t n, const double2* __restrict__ a, float2* __restrict__ b) {
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        b[t] = make_float2((float)a[t].x, (float)a[t].y);
 }
 
 // x += d; per matrix the largest |d| and |x| (for the refinement's stopping test), [F][2].
-__global__ void k_ir_update(int Np, int nrhs, double2* __restrict__ x, const double2* __restrict__ d,
+__global__ void k_ir_update(int Np, int nrhs, double2* __restrict__ x, const float2* __restrict__ d,
                             double* __restrict__ norms) {
     __shared__ double sd[256], sx[256];
     const int f = blockIdx.x;
@@ -479,11 +625,12 @@ __global__ void k_ir_update(int Np, int nrhs, double2* __restrict__ x, const dou
     double md = 0.0, mx = 0.0;
     for (size_t t = threadIdx.x; t < n; t += blockDim.x) {
         size_t o = (size_t)f * n + t;
-        double2 a = x[o], b = d[o];
-        a.x += b.x;
-        a.y += b.y;
+        double2 a = x[o];
+        const float2 b = d[o];
+        a.x += (double)b.x;
+        a.y += (double)b.y;
         x[o] = a;
-        md = fmax(md, fmax(fabs(b.x), fabs(b.y)));
+        md = fmax(md, fmax(fabs((double)b.x), fabs((double)b.y)));
         mx = fmax(mx, fmax(fabs(a.x), fabs(a.y)));
     }
     sd[threadIdx.x] = md;

@@ -91,7 +91,7 @@ def lib():
     L.hbg_debug_matrices.argtypes = [ctypes.POINTER(HbgBody), ctypes.c_double, ctypes.POINTER(HbgOptions), dp, dp, dp]
     L.hbg_debug_matrices.restype = ctypes.c_int32
     fp = ctypes.POINTER(ctypes.c_float)
-    L.hbg_debug_gemm_tf32.argtypes = [ctypes.c_int32] * 3 + [fp, fp, fp]
+    L.hbg_debug_gemm_tf32.argtypes = [ctypes.c_int32] * 3 + [fp, fp, fp, ctypes.c_int32]
     L.hbg_last_ir_iterations.argtypes = [ctypes.POINTER(ctypes.c_int32)]
     L.hbg_last_profile.argtypes = [dp]
     L.hbg_profile_kernels.argtypes = [ctypes.c_int32]
@@ -219,15 +219,18 @@ def kernel_profile():
     return out
 
 
-def debug_gemm_tf32(A, B):
-    """C = A B^T through the tcgen05 TF32 kernel (test support); A [M][K], B [N][K] float32."""
+def debug_gemm_tf32(A, B, C=None):
+    """C = A B^T, or C - A B^T when C is given, through the tcgen05 TF32 kernel (test support);
+    A [M][K], B [N][K], C [M][N] float32."""
     A = np.ascontiguousarray(A, dtype=np.float32)
     B = np.ascontiguousarray(B, dtype=np.float32)
     M, K = A.shape
     N = B.shape[0]
-    C = np.zeros((M, N), dtype=np.float32)
+    sub = C is not None
+    C = np.array(C, dtype=np.float32, order="C", copy=True) if sub else np.zeros((M, N), dtype=np.float32)
     fp = ctypes.POINTER(ctypes.c_float)
-    check(lib().hbg_debug_gemm_tf32(M, N, K, A.ctypes.data_as(fp), B.ctypes.data_as(fp), C.ctypes.data_as(fp)))
+    check(lib().hbg_debug_gemm_tf32(M, N, K, A.ctypes.data_as(fp), B.ctypes.data_as(fp), C.ctypes.data_as(fp),
+                                    int(sub)))
     return C
 
 

@@ -141,11 +141,13 @@ HbStatus hbg_last_launch_count(int64_t *count);
 HbStatus hbg_debug_matrices(const HbgBody *body, double omega, const HbgOptions *opt, double *statics, double *S,
                             double *A);
 
-/* Test support: C = A B^T on the tensor-core path of the mixed LU (tcgen05 kind::tf32, FP32
- * accumulation): A [M][K], B [N][K], C [M][N], row-major FP32 host arrays; M % 128 == 0,
- * N % 256 == 0, K % 32 == 0.  Replaces no reference interface (the product kernel of the
- * trailing update, linalg.rs:114-125, exposed for its numerics test). */
-HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const float *A, const float *B, float *C);
+/* Test support: C = A B^T (subtract == 0) or C -= A B^T (subtract != 0, C read first) on the
+ * tensor-core path of the mixed LU (tcgen05 kind::tf32, FP32 accumulation): A [M][K], B [N][K],
+ * C [M][N], row-major FP32 host arrays; M % 128 == 0, N % 128 == 0, K % 32 == 0.  Replaces no
+ * reference interface (the product kernel of the trailing update, linalg.rs:114-125, exposed for
+ * its numerics test). */
+HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const float *A, const float *B, float *C,
+                             int32_t subtract);
 
 /* Refinement iterations of the last mixed-precision frequency batch of this thread. */
 HbStatus hbg_last_ir_iterations(int32_t *n);

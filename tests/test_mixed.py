@@ -29,11 +29,22 @@ def test_tf32_gemm_exact_on_small_integers():
     """Small integers are exact in TF32 and their sums exact in FP32: any layout, swizzle or
     descriptor mistake shows as a mismatch."""
     rng = np.random.default_rng(1)
-    for M, N, K in ((128, 256, 32), (256, 512, 256), (384, 256, 96)):
+    for M, N, K in ((128, 128, 32), (128, 256, 32), (256, 512, 256), (384, 256, 96), (1152, 1408, 64)):
         A = rng.integers(-3, 4, size=(M, K)).astype(np.float32)
         B = rng.integers(-3, 4, size=(N, K)).astype(np.float32)
         C = nv.debug_gemm_tf32(A, B)
         assert np.array_equal(C, A @ B.T), (M, N, K)
+
+
+def test_tf32_gemm_subtract_exact_on_small_integers():
+    """The trailing-update form C -= A B^T: C tiles prefetched by TMA, updated, stored by TMA."""
+    rng = np.random.default_rng(3)
+    for M, N, K in ((128, 128, 32), (640, 896, 256)):
+        A = rng.integers(-3, 4, size=(M, K)).astype(np.float32)
+        B = rng.integers(-3, 4, size=(N, K)).astype(np.float32)
+        C0 = rng.integers(-100, 100, size=(M, N)).astype(np.float32)
+        C = nv.debug_gemm_tf32(A, B, C0)
+        assert np.array_equal(C, C0 - A @ B.T), (M, N, K)
 
 
 def test_tf32_gemm_against_fp64():
