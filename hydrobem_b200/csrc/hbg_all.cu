@@ -5,3 +5,4 @@
 #include "hbg_mixed.cu"
 #include "hbg_api.cu"
 #include "hbg_model.cu"
+#include "hbg_noalloc.cu"

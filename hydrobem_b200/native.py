@@ -8,6 +8,7 @@ HB_ERR_UNSUPPORTED, which this module raises.
 from __future__ import annotations
 
 import ctypes
+import math
 from pathlib import Path
 
 import numpy as np
@@ -61,7 +62,8 @@ EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_
            "hbg_profile_kernels", "hbg_kernel_profile", "hbg_release_workspace", "hb_abi_version",
            "hb_last_error_message", "hb_last_error_location", "hb_model_new", "hb_model_free", "hb_model_cancel",
            "hb_object", "hb_add", "hb_set_bool", "hb_set_int", "hb_set_real", "hb_set_text", "hb_set_reals",
-           "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity"]
+           "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
+           "hbg_statics_noalloc"]
 
 _lib = None
 
@@ -93,6 +95,9 @@ def lib():
     fp = ctypes.POINTER(ctypes.c_float)
     L.hbg_debug_gemm_tf32.argtypes = [ctypes.c_int32] * 3 + [fp, fp, fp, ctypes.c_int32]
     L.hbg_last_ir_iterations.argtypes = [ctypes.POINTER(ctypes.c_int32)]
+    L.hbg_statics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
+                                      ctypes.c_int32, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+    L.hbg_statics_noalloc.restype = ctypes.c_int32
     L.hbg_last_profile.argtypes = [dp]
     L.hbg_profile_kernels.argtypes = [ctypes.c_int32]
     L.hbg_kernel_profile.argtypes = [ctypes.c_int32, dp, ctypes.POINTER(ctypes.c_int64), dp]
@@ -232,6 +237,16 @@ def debug_gemm_tf32(A, B, C=None):
     check(lib().hbg_debug_gemm_tf32(M, N, K, A.ctypes.data_as(fp), B.ctypes.data_as(fp), C.ctypes.data_as(fp),
                                     int(sub)))
     return C
+
+
+def statics_noalloc(d_vertices: int, d_kinds: int | None, n_panels: int, d_statics: int, depth: float = math.inf,
+                    logarithmic: bool = True, log_tolerance: float = 1e-4, stream: int | None = None) -> None:
+    """The statics of a panel set into caller-owned device memory, with no device allocation by the
+    library (its scratch is a fixed array for at most 2048 panels).  Arguments are raw device
+    addresses on the current device: vertices [N][4][3] FP64, kinds [N] int32 or None, statics
+    [4][N][N] FP64 with entry (k, j) of plane q at q N^2 + k + j N."""
+    check(lib().hbg_statics_noalloc(d_vertices, d_kinds, n_panels, depth, 1 if logarithmic else 0, log_tolerance,
+                                    d_statics, stream))
 
 
 def last_ir_iterations() -> int:

@@ -152,6 +152,27 @@ HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const float *A, co
 /* Refinement iterations of the last mixed-precision frequency batch of this thread. */
 HbStatus hbg_last_ir_iterations(int32_t *n);
 
+/* The statics of one panel set -- the frequency-independent Rankine source and dipole integrals
+ * with their logarithmic-singularity corrections, FP64 [4][N][N] with entry (k, j) of plane q at
+ * q N^2 + k + j N -- written into caller-owned device memory, with NO device allocation by the
+ * library.  No counterpart in the reference (its statics are allocated inside the solve).
+ *
+ * For callers that own all device memory themselves (a pool allocator, a process that must not
+ * grow its device footprint once running): the kernels' scratch (panel planes, adaptive-pair
+ * worklist, flags) is one fixed __device__ array of 1.73 MB inside the library, so n_panels is at
+ * most 2048; larger sets are rejected with HB_ERR_VALUE.  Every argument pointer is device memory
+ * of the CURRENT device: d_vertices [N][4][3] (normals into the fluid), d_kinds [N] (HBG_WET /
+ * HBG_INTERIOR, or NULL for all wetted), d_statics [4 N^2].  depth <= 0 or non-finite = infinite
+ * depth.  The call runs on `stream` (a cudaStream_t; NULL = the legacy default stream), resets the
+ * scratch's flags and worklist count itself, and synchronizes that stream before it returns, so
+ * it cannot be captured into a CUDA graph.  The first call on each device resolves the scratch
+ * address (cudaGetSymbolAddress) and writes the quadrature constants: make it before any stream
+ * capture on that device begins.  All calls on one device share the one scratch array: calls
+ * that overlap in time (from several host threads, or on several streams) race on it and must be
+ * serialized by the caller. */
+HbStatus hbg_statics_noalloc(const double *d_vertices, const int32_t *d_kinds, int64_t n_panels, double depth,
+                             int32_t logarithmic, double log_tolerance, double *d_statics, void *stream);
+
 /* ==================================================================== reference ABI subset */
 
 typedef struct HbModel HbModel;
