@@ -41,6 +41,12 @@ N_PERIODS = 40
 HEADINGS = [0.0, 30.0, 60.0, 90.0]
 DEPTH = 5.0
 WORKLOAD = "cylinder r=1 m d=0.5 m, 4096 panels (64x32 side + 64x32 bottom), h=5 m, 40 periods 1.5-20 s, 4 headings"
+CASE_LABELS = {
+    "c2": WORKLOAD,
+    "medium": "cylinder r=1 m d=0.5 m, 4096 panels, h=5 m, 8 periods 1.5-20 s, 4 headings (profiling cut)",
+    "small": "cylinder r=1 m d=0.5 m, 2048 panels (32x16 side + 32x16 bottom), h=5 m, 4 periods 1.5-20 s, "
+             "4 headings (profiling cut)",
+}
 
 
 CASE = "c2"
@@ -48,11 +54,14 @@ CASE = "c2"
 
 def workload():
     """The benchmark body and frequencies; --case small is a 2048-panel, 4-frequency cut of the same
-    family for profiler captures (each matrix 67 MB, the batch still larger than L2)."""
+    family for profiler captures (each matrix 67 MB, the batch still larger than L2); --case medium
+    the 4096-panel body at 8 of the periods (the benchmark's matrix shapes, a fifth of its batch)."""
     from hydrobem_b200 import meshes
 
     if CASE == "small":
         return meshes.cylinder(1.0, 0.5, 32, 16, 16), 2.0 * math.pi / np.linspace(1.5, 20.0, 4)
+    if CASE == "medium":
+        return meshes.cylinder(1.0, 0.5, 64, 32, 32), 2.0 * math.pi / np.linspace(1.5, 20.0, 8)
     v = meshes.cylinder(1.0, 0.5, 64, 32, 32)
     periods = np.linspace(1.5, 20.0, N_PERIODS)
     return v, 2.0 * math.pi / periods
@@ -166,7 +175,7 @@ def cpu_reference(args, world, rank, pg):
     line = {"metric": "freq solves/s at N=4096", "value": value, "unit": "freq solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": job * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "form": "FP64 (the reference's diagnostic double path)",
+            "config": {"workload": CASE_LABELS[CASE], "form": "FP64 (the reference's diagnostic double path)",
                        "l2": "inputs larger than L2"},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "freq solves/s", "cores": cores, "kind": "port",
@@ -256,7 +265,7 @@ def ours(args, world, rank, local, pg):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == nv.HBG_FP64 else "c64+tf32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "form": args.precision, "l2": "inputs larger than L2 (no flush)",
+            "config": {"workload": CASE_LABELS[CASE], "form": args.precision, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}"},
             "e2e": {"value": e2e, "unit": "freq solves/s", "h2d_bytes_per_step": int(v.nbytes + omegas.nbytes + 32),
                     "d2h_bytes_per_step": int(F * (72 + 3 * len(HEADINGS) * 12) * 8)},
@@ -332,7 +341,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison of the mixed form")
     ap.add_argument("--fp64-peak", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", default="c2", choices=["c2", "small"])
+    ap.add_argument("--case", default="c2", choices=["c2", "medium", "small"])
     args = ap.parse_args()
     global CASE
     CASE = args.case

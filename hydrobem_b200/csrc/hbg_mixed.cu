@@ -149,6 +149,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     const int dsmem = NBL * (NBL + 1) * (int)sizeof(float2);
     cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, dsmem);
+    cudaFuncSetAttribute(k_tri_step<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(12));
+    cudaFuncSetAttribute(k_tri_step<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(16));
     std::vector<double> heads(std::max(H, 1));
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
     cudaMemcpyAsync(dheads, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s);

@@ -496,16 +496,17 @@ __global__ void k_gemv_reduce(int N, int nrhs, int F, int nz, const double2* __r
 // its rows: coalesced); the CTA that owns the next diagonal block then solves it by the stored
 // inverse of that block.
 constexpr int TB = 128;
-constexpr int TRI_THREADS = 128;
+constexpr int TRI_THREADS = 256;
 
 // The diagonal block of U^T (upper_t) or L^T, solved by its stored inverse: y_b = D^T r_b with
 // D = U_bb^-1 (upper part of the stored block, with the diagonal) or L_bb^-1 (lower part, unit
-// diagonal).  Rows b0..b0+TB of X in place, right-hand sides in chunks of NR; thread t owns column t.
+// diagonal).  Rows b0..b0+TB of X in place, right-hand sides in chunks of NR.  Thread t < TB owns
+// column t for the first half of the block's rows, thread t + TB the same column for the second
+// half; each loads the 16 entries of a chunk before using them (one memory latency per chunk).
 template <int NR>
 __device__ __forceinline__ void tri_diag_f32(const float2* __restrict__ D, float2* X, int Np, int nrhs, int b0,
-                                             bool upper_t, float2 (*rs)[NR]) {
-    const int i = threadIdx.x;
-    const int pbeg = upper_t ? 0 : i + 1, pend = upper_t ? i + 1 : TB;
+                                             bool upper_t, float2 (*rs)[NR], float2 (*pt)[NR]) {
+    const int i = threadIdx.x % TB, half = threadIdx.x / TB;
     for (int c0 = 0; c0 < nrhs; c0 += NR) {
         const int nc = min(NR, nrhs - c0);
         __syncthreads();
@@ -516,32 +517,51 @@ __device__ __forceinline__ void tri_diag_f32(const float2* __restrict__ D, float
         __syncthreads();
         float2 acc[NR];
 #pragma unroll
-        for (int c = 0; c < NR; c++) acc[c] = upper_t ? make_float2(0.f, 0.f) : rs[i][c];  // unit diagonal of L^-1
-#pragma unroll 4
-        for (int p = pbeg; p < pend; p++) {
-            const float2 dv = D[p * TB + i];
+        for (int c = 0; c < NR; c++)  // the unit diagonal of L^-1
+            acc[c] = (!upper_t && half == (i >= TB / 2 ? 1 : 0)) ? rs[i][c] : make_float2(0.f, 0.f);
+        const int pb = half * (TB / 2);
+#pragma unroll 1
+        for (int pc = 0; pc < TB / 2; pc += 16) {
+            float2 dv[16];
 #pragma unroll
-            for (int c = 0; c < NR; c++) {
-                const float2 v = rs[p][c];
-                acc[c].x += dv.x * v.x - dv.y * v.y;
-                acc[c].y += dv.x * v.y + dv.y * v.x;
+            for (int q = 0; q < 16; q++) dv[q] = D[(pb + pc + q) * TB + i];
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+                const int p = pb + pc + q;
+                if (upper_t ? p <= i : p > i) {
+#pragma unroll
+                    for (int c = 0; c < NR; c++) {
+                        const float2 v = rs[p][c];
+                        acc[c].x += dv[q].x * v.x - dv[q].y * v.y;
+                        acc[c].y += dv[q].x * v.y + dv[q].y * v.x;
+                    }
+                }
             }
         }
+        if (half == 1)
 #pragma unroll
-        for (int c = 0; c < NR; c++)
-            if (c < nc) X[(size_t)(c0 + c) * Np + b0 + i] = acc[c];
+            for (int c = 0; c < NR; c++) pt[i][c] = acc[c];
+        __syncthreads();
+        if (half == 0)
+#pragma unroll
+            for (int c = 0; c < NR; c++)
+                if (c < nc) {
+                    const float2 q2 = pt[i][c];
+                    X[(size_t)(c0 + c) * Np + b0 + i] = make_float2(acc[c].x + q2.x, acc[c].y + q2.y);
+                }
     }
 }
 
 // One block step of the forward (upper_t) or backward solve.  step = index of the block solved by
 // the previous launch (-1: none, only the first diagonal block is solved).  Thread layout: warp w
-// owns rows 32 (w % 2) + lane and 64 more, and the half w / 2 of the solved block's 128 entries;
-// every lane of a warp reads the same solved entry (a shared-memory broadcast).
+// owns rows 32 (w % 2) + lane and 64 more, and the quarter w / 2 of the solved block's 128
+// entries, loaded 16 at a time before use; every lane of a warp reads the same solved entry (a
+// shared-memory broadcast).
 template <int NR>
-__global__ void __launch_bounds__(TRI_THREADS) k_tri_step(int Np, size_t bstride, const float* __restrict__ W,
+__global__ void __launch_bounds__(TRI_THREADS, 2) k_tri_step(int Np, size_t bstride, const float* __restrict__ W,
                                                           const float2* __restrict__ DINV, int nrhs,
                                                           float2* __restrict__ Xall, int step, int upper_t) {
-    extern __shared__ float2 tri_smem[];  // ys [TB][NR], partial sums [TB][NR]
+    extern __shared__ float2 tri_smem[];  // ys [TB][NR], partial sums [3][TB][NR]
     float2(*ys)[NR] = reinterpret_cast<float2(*)[NR]>(tri_smem);
     float2(*pt)[NR] = reinterpret_cast<float2(*)[NR]>(tri_smem + TB * NR);
     const int f = blockIdx.y;
@@ -552,7 +572,7 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tri_step(int Np, size_t bstride
     const float2* Df = DINV + (size_t)f * nblk * TB * TB;
     if (step < 0) {
         const int first = upper_t ? 0 : nblk - 1;
-        tri_diag_f32<NR>(Df + (size_t)first * TB * TB, X, Np, nrhs, first * TB, upper_t, ys);
+        tri_diag_f32<NR>(Df + (size_t)first * TB * TB, X, Np, nrhs, first * TB, upper_t, ys, pt);
         return;
     }
     const int s0 = step * TB;
@@ -560,9 +580,9 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tri_step(int Np, size_t bstride
     const int r0 = cb * TB;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int li = 32 * (warp & 1) + lane;  // local rows li and li + 64
-    const int ph = warp >> 1;
-    const float* pr = Mr + (size_t)(s0 + ph * 64) * Np + r0 + li;
-    const float* pi = Mi + (size_t)(s0 + ph * 64) * Np + r0 + li;
+    const int pq = warp >> 1;               // quarter of the solved block
+    const float* pr = Mr + (size_t)(s0 + pq * 32) * Np + r0 + li;
+    const float* pi = Mi + (size_t)(s0 + pq * 32) * Np + r0 + li;
     for (int c0 = 0; c0 < nrhs; c0 += NR) {
         const int nc = min(NR, nrhs - c0);
         __syncthreads();
@@ -574,41 +594,59 @@ __global__ void __launch_bounds__(TRI_THREADS) k_tri_step(int Np, size_t bstride
         float2 a0[NR], a1[NR];
 #pragma unroll
         for (int c = 0; c < NR; c++) a0[c] = a1[c] = make_float2(0.f, 0.f);
-#pragma unroll 8
-        for (int p = 0; p < 64; p++) {
-            const size_t o = (size_t)p * Np;
-            const float r0v = pr[o], i0v = pi[o], r1v = pr[o + 64], i1v = pi[o + 64];
+#pragma unroll 1
+        for (int pc = 0; pc < 32; pc += 16) {
+            float r0v[16], i0v[16], r1v[16], i1v[16];
 #pragma unroll
-            for (int c = 0; c < NR; c++) {
-                const float2 v = ys[ph * 64 + p][c];
-                a0[c].x += r0v * v.x - i0v * v.y;
-                a0[c].y += r0v * v.y + i0v * v.x;
-                a1[c].x += r1v * v.x - i1v * v.y;
-                a1[c].y += r1v * v.y + i1v * v.x;
+            for (int q = 0; q < 16; q++) {
+                const size_t o = (size_t)(pc + q) * Np;
+                r0v[q] = pr[o];
+                i0v[q] = pi[o];
+                r1v[q] = pr[o + 64];
+                i1v[q] = pi[o + 64];
+            }
+#pragma unroll
+            for (int q = 0; q < 16; q++) {
+#pragma unroll
+                for (int c = 0; c < NR; c++) {
+                    const float2 v = ys[pq * 32 + pc + q][c];
+                    a0[c].x += r0v[q] * v.x - i0v[q] * v.y;
+                    a0[c].y += r0v[q] * v.y + i0v[q] * v.x;
+                    a1[c].x += r1v[q] * v.x - i1v[q] * v.y;
+                    a1[c].y += r1v[q] * v.y + i1v[q] * v.x;
+                }
             }
         }
-        if (ph == 1)
+        if (pq > 0)
 #pragma unroll
             for (int c = 0; c < NR; c++) {
-                pt[li][c] = a0[c];
-                pt[li + 64][c] = a1[c];
+                pt[(pq - 1) * TB + li][c] = a0[c];
+                pt[(pq - 1) * TB + li + 64][c] = a1[c];
             }
         __syncthreads();
-        if (ph == 0)
+        if (pq == 0)
 #pragma unroll
             for (int c = 0; c < NR; c++)
                 if (c < nc) {
+                    float2 s0v = a0[c], s1v = a1[c];
+#pragma unroll
+                    for (int h = 0; h < 3; h++) {
+                        const float2 q0 = pt[h * TB + li][c], q1 = pt[h * TB + li + 64][c];
+                        s0v.x += q0.x;
+                        s0v.y += q0.y;
+                        s1v.x += q1.x;
+                        s1v.y += q1.y;
+                    }
                     float2* x0 = X + (size_t)(c0 + c) * Np + r0 + li;
-                    float2 v0 = x0[0], v1 = x0[64];
-                    const float2 q0 = pt[li][c], q1 = pt[li + 64][c];
-                    x0[0] = make_float2(v0.x - (a0[c].x + q0.x), v0.y - (a0[c].y + q0.y));
-                    x0[64] = make_float2(v1.x - (a1[c].x + q1.x), v1.y - (a1[c].y + q1.y));
+                    const float2 v0 = x0[0], v1 = x0[64];
+                    x0[0] = make_float2(v0.x - s0v.x, v0.y - s0v.y);
+                    x0[64] = make_float2(v1.x - s1v.x, v1.y - s1v.y);
                 }
     }
-    if (blockIdx.x == 0) tri_diag_f32<NR>(Df + (size_t)cb * TB * TB, X, Np, nrhs, r0, upper_t, ys);
+    if (blockIdx.x == 0) tri_diag_f32<NR>(Df + (size_t)cb * TB * TB, X, Np, nrhs, r0, upper_t, ys, pt);
 }
 
-constexpr size_t tri_smem_bytes(int nr) { return (size_t)2 * TB * nr * sizeof(float2); }
+constexpr size_t tri_smem_bytes(int nr) { return (size_t)4 * TB * nr * sizeof(float2); }
 
 // FP64 vectors to complex64 (the right-hand sides entering the first correction).
 __global__ void k_to_c64(size_t n, const double2* __restrict__ a, float2* __restrict__ b) {
