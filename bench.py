@@ -46,6 +46,7 @@ CASE_LABELS = {
     "medium": "cylinder r=1 m d=0.5 m, 4096 panels, h=5 m, 8 periods 1.5-20 s, 4 headings (profiling cut)",
     "small": "cylinder r=1 m d=0.5 m, 2048 panels (32x16 side + 32x16 bottom), h=5 m, 4 periods 1.5-20 s, "
              "4 headings (profiling cut)",
+    "tiny": "cylinder r=1 m d=0.5 m, 32 panels, h=5 m, 3 periods 1.5-20 s, 4 headings (host-logic tests)",
 }
 
 
@@ -62,6 +63,8 @@ def workload():
         return meshes.cylinder(1.0, 0.5, 32, 16, 16), 2.0 * math.pi / np.linspace(1.5, 20.0, 4)
     if CASE == "medium":
         return meshes.cylinder(1.0, 0.5, 64, 32, 32), 2.0 * math.pi / np.linspace(1.5, 20.0, 8)
+    if CASE == "tiny":
+        return meshes.cylinder(1.0, 0.5, 8, 2, 2), 2.0 * math.pi / np.linspace(1.5, 20.0, 3)
     v = meshes.cylinder(1.0, 0.5, 64, 32, 32)
     periods = np.linspace(1.5, 20.0, N_PERIODS)
     return v, 2.0 * math.pi / periods
@@ -139,6 +142,17 @@ def dist_setup():
         dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         pg = dist
     return world, rank, local, pg
+
+
+def reduce_max(pg, values, device="cpu"):
+    """The element-wise maximum over ranks (the job's time is that of its slowest rank)."""
+    if pg is None:
+        return [float(x) for x in values]
+    import torch
+
+    t = torch.tensor([float(x) for x in values], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
 
 
 def cpu_reference(args, world, rank, pg):
@@ -226,10 +240,7 @@ def ours(args, world, rank, local, pg):
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
     step_ms = float(np.mean(dev_ms))
-    if pg is not None:
-        t = torch.tensor([step_ms, e2e_ms], device=f"cuda:{device}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        step_ms, e2e_ms = float(t[0]), float(t[1])
+    step_ms, e2e_ms = reduce_max(pg, [step_ms, e2e_ms], f"cuda:{device}")
     launches = nv.last_launch_count()
     # one more step with kernel-family timing for the roofline (outside the timed region)
     nv.profile_kernels(True)
@@ -237,6 +248,9 @@ def ours(args, world, rank, local, pg):
     prof = nv.kernel_profile()
     nv.profile_kernels(False)
     phases = nv.last_profile()
+    ir = {"iterations": nv.last_ir_iterations(), "history": [float(f"{x:.3g}") for x in nv.last_ir_history()]} \
+        if precision == nv.HBG_MIXED else None
+    pipe_peaks = nv.measure_peaks()  # FP64 FMA / FP64 MMA / TF32 tcgen05 of this device, measured here
     if rank != 0:
         return None
     F = len(omegas)
@@ -248,11 +262,11 @@ def ours(args, world, rank, local, pg):
     achieved = work / (ms * 1e-3) / (1e12 if flops else 1e9) if ms > 0 else None
     if flops:
         if fam == "mixed_gemm":
-            peak = peaks.get("bf16_tflops_sustained", peaks.get("bf16_tflops"))
-            pk = f"bf16 dense sustained ({peak_kind})"
+            peak = pipe_peaks["tf32_tcgen05"]
+            pk = "tf32 tcgen05 dense (measured in this run by hbg_measure_peaks)"
         else:
-            peak = args.fp64_peak
-            pk = "fp64 (datasheet 40 TFLOP/s; no measured FP64 peak on this pool)"
+            peak = pipe_peaks["fp64_fma"]
+            pk = "fp64 FMA (measured in this run by hbg_measure_peaks)"
         bound, unit = "tensor", "TFLOP/s"
     else:
         peak, bound, unit, pk = peaks["hbm_gbs"], "hbm", "GB/s", f"hbm copy ({peak_kind})"
@@ -275,7 +289,10 @@ def ours(args, world, rank, local, pg):
                          "peak_kind": pk, "launches": n, "ms": ms},
             "phases_ms": {k: round(x, 3) for k, x in phases.items()},
             "kernels_ms": {k: round(x[0], 3) for k, x in prof.items() if x[1]},
+            "measured_peaks_tflops": {k: round(x, 1) for k, x in pipe_peaks.items()},
             "clocks": clocks}
+    if ir is not None:
+        line["refinement"] = ir
     if precision == nv.HBG_MIXED and not args.no_plain:
         line["plain_fp64"] = plain_comparison(nv, v, omegas, device, body)
     if world == 1 and not args.no_cpu_baseline:
@@ -339,9 +356,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison of the mixed form")
-    ap.add_argument("--fp64-peak", type=float, default=40.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--case", default="c2", choices=["c2", "medium", "small"])
+    ap.add_argument("--case", default="c2", choices=["c2", "medium", "small", "tiny"])
     args = ap.parse_args()
     global CASE
     CASE = args.case

@@ -160,6 +160,7 @@ static void gauss_legendre(int n, double* x, double* w) {
 struct DeviceCtx {
     bool ready = false;
     double* tables = nullptr;
+    float* t2d_f = nullptr;
     Tables tab{};
 };
 
@@ -185,7 +186,12 @@ static DeviceCtx& device_ctx(int dev) {
         dp[i] = d.tables + off;
         off += padded(ht.len[i]);
     }
-    d.tab = Tables{dp[0], dp[1], dp[2], dp[3], dp[4], dp[5], dp[6], dp[7]};
+    // TABLE_2D rounded to FP32 for the mixed form's coefficient reads
+    std::vector<float> t2f(ht.len[1]);
+    for (size_t i = 0; i < ht.len[1]; i++) t2f[i] = (float)ht.arr[1][i];
+    CUDA_OK(cudaMalloc(&d.t2d_f, t2f.size() * sizeof(float)));
+    CUDA_OK(cudaMemcpy(d.t2d_f, t2f.data(), t2f.size() * sizeof(float), cudaMemcpyHostToDevice));
+    d.tab = Tables{dp[0], dp[1], dp[2], dp[3], dp[4], dp[5], dp[6], dp[7], d.t2d_f};
     static double glx[17][16], glw[17][16];
     memset(glx, 0, sizeof glx);
     memset(glw, 0, sizeof glw);
@@ -769,6 +775,29 @@ extern "C" HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const f
     } catch (const Failure& f) {
         return fail(f);
     }
+}
+
+extern "C" HbStatus hbg_measure_peaks(double* out3) {
+    try {
+        if (!out3) return fail({HB_ERR_ARGUMENT, "null argument"});
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            return fail({HB_ERR_UNSUPPORTED, "no CUDA device: this library runs the path on the GPU only"});
+        const char* msg = "";
+        int rc = measure_peaks(out3, &msg);
+        if (rc) return fail({rc, msg});
+        return HB_OK;
+    } catch (const Failure& f) {
+        return fail(f);
+    }
+}
+
+extern "C" HbStatus hbg_last_ir_history(double* ratios32, int32_t* n) {
+    if (!ratios32 || !n) return fail({HB_ERR_ARGUMENT, "null argument"});
+    const IrHistory& h = last_ir_history();
+    for (int i = 0; i < h.n; i++) ratios32[i] = h.ratio[i];
+    *n = h.n;
+    return HB_OK;
 }
 
 extern "C" HbStatus hbg_last_ir_iterations(int32_t* n) {

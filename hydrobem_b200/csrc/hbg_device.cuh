@@ -34,6 +34,7 @@ struct Tables {
     const double* q;     // Q_m Chebyshev coefficients
     const double* l0;
     const double* bk;    // scaled K0, K1 tiles
+    const float* t2d_f;  // t2d rounded to FP32 (the mixed form's coefficient reads)
 };
 
 // Panels in structure-of-arrays planes (each plane N doubles, plane p at base + p N).
@@ -132,6 +133,44 @@ __device__ __forceinline__ void table2d(double X, double Y, double& v, double& v
             }
         }
         double acc = 0.0;
+#pragma unroll
+        for (int a = M - 1; a >= 0; a--) acc = acc * ty + r[a];
+        s[q] = acc;
+    }
+    v = s[0];
+    vx = s[1];
+}
+
+// table2d from the FP32 copy of the coefficients, FP32 Horner chains (the mixed form: half the
+// coefficient bytes per evaluation; its matrices are stored in complex64).
+__device__ __forceinline__ void table2d_f32(double X, double Y, double& v, double& vx) {
+    int ix = (int)X, iy = (int)Y;
+    if (ix >= XT) ix = XT - 1;
+    if (iy >= YT) iy = YT - 1;
+    const float tx = (float)(2.0 * (X - ix) - 1.0), ty = (float)(2.0 * (Y - iy) - 1.0);
+    constexpr int M = N2 + 1;
+    static_assert(M == 8, "rows of 8 FP32 coefficients: two float4 loads a row");
+    const float* c = c_tab.t2d_f + ((size_t)iy * XT + ix) * 2 * M * M;
+    float s[2];
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const float4* cq = reinterpret_cast<const float4*>(c + q * M * M);
+        float r[M];
+#pragma unroll
+        for (int a = 0; a < M; a++) r[a] = 0.f;
+#pragma unroll
+        for (int j = M - 1; j >= 0; j--) {
+            const float4 c0 = __ldg(cq + 2 * j), c1 = __ldg(cq + 2 * j + 1);
+            r[0] = r[0] * tx + c0.x;
+            r[1] = r[1] * tx + c0.y;
+            r[2] = r[2] * tx + c0.z;
+            r[3] = r[3] * tx + c0.w;
+            r[4] = r[4] * tx + c1.x;
+            r[5] = r[5] * tx + c1.y;
+            r[6] = r[6] * tx + c1.z;
+            r[7] = r[7] * tx + c1.w;
+        }
+        float acc = 0.f;
 #pragma unroll
         for (int a = M - 1; a >= 0; a--) acc = acc * ty + r[a];
         s[q] = acc;
@@ -242,6 +281,7 @@ struct Wave {
     double F, FX, FY, I, IX, IY, c;
 };
 
+template <bool F32 = false>
 __device__ inline Wave wave_kernel(double X, double Y) {
     Wave o;
     double R0 = sqrt(X * X + Y * Y);
@@ -251,7 +291,10 @@ __device__ inline Wave wave_kernel(double X, double Y) {
         table1d(X, f);
         j0 = f[0];
         j1 = f[1];
-        table2d(X, Y, v, vx);
+        if constexpr (F32)
+            table2d_f32(X, Y, v, vx);
+        else
+            table2d(X, Y, v, vx);
         double lg = log(Y + R0) + (GAMMA - LOG2);
         F = -2.0 * eY * j0 * lg - PI * eY * f[2] - 2.0 * R0 * v;
         FX = 2.0 * eY * j1 * lg - 2.0 * eY * j0 * X / (R0 * (Y + R0)) - PI * eY * f[3] - 2.0 * (X / R0) * v -
@@ -283,6 +326,7 @@ __device__ inline Wave wave_kernel(double X, double Y) {
 }
 
 // real part only (green_inf.rs:647-675)
+template <bool F32 = false>
 __device__ inline void wave_real(double X, double Y, double& F, double& FX, double& FY) {
     double R0 = sqrt(X * X + Y * Y);
     if (Y >= YT) {
@@ -291,7 +335,7 @@ __device__ inline void wave_real(double X, double Y, double& F, double& FX, doub
         F = -2.0 * P;
         FX = -2.0 * PX;
     } else {
-        Wave w = wave_kernel(X, Y);
+        Wave w = wave_kernel<F32>(X, Y);
         F = w.F;
         FX = w.FX;
     }
@@ -402,6 +446,42 @@ __device__ __forceinline__ void phi_tiles(const double* T, int which, double xb,
     v[0] = v0; v[1] = v1; v[2] = v2;
 }
 
+// phi_tiles from FP32 tiles (the mixed form): per tile 3 blocks of 36 coefficients, 432 bytes
+// (27 float4 loads), FP32 Horner chains.
+__device__ __forceinline__ void phi_tiles_f32(const float* T, int which, double xb, double vb, double* v) {
+    constexpr int N = TN;
+    static_assert(TN == 6, "blocks of 36 FP32 coefficients: nine float4 loads a block");
+    int ny = which == 1 ? TW : TV;
+    double ymax = which == 1 ? 1.0 : 2.0;
+    double ux = xb * (TS / XMAX), uy = vb * (ny / ymax);
+    int ix = (int)ux, iy = (int)uy;
+    if (ix > TS - 1) ix = TS - 1;
+    if (iy > ny - 1) iy = ny - 1;
+    const float tx = (float)(2.0 * (ux - ix) - 1.0), ty = (float)(2.0 * (uy - iy) - 1.0);
+    const float4* c = reinterpret_cast<const float4*>(T + (size_t)(ix * ny + iy) * 3 * N * N);
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+        float cf[N * N];
+#pragma unroll
+        for (int u = 0; u < N * N / 4; u++) {
+            const float4 a = __ldg(c + q * (N * N / 4) + u);
+            cf[4 * u] = a.x;
+            cf[4 * u + 1] = a.y;
+            cf[4 * u + 2] = a.z;
+            cf[4 * u + 3] = a.w;
+        }
+        float vq = 0.f;
+#pragma unroll
+        for (int i = N - 1; i >= 0; i--) {
+            float p = cf[i * N + N - 1];
+#pragma unroll
+            for (int j = N - 2; j >= 0; j--) p = p * ty + cf[i * N + j];
+            vq = vq * tx + p;
+        }
+        v[q] = vq;
+    }
+}
+
 // Regular part of the kernel: Wr WrR WrZ Wrz Wi WiR WiZ Wiz (green_fin.rs:48-60 Kern)
 struct Kern {
     double Wr, WrR, WrZ, Wrz, Wi, WiR, WiZ, Wiz;
@@ -423,6 +503,7 @@ __device__ __forceinline__ Kern wave_kern(double K, const Wave& w) {
 }
 
 // low_order.rs:627-648 pair_kernel, infinite depth
+template <bool F32 = false>
 __device__ inline Kern pair_kernel_inf(double K, double R, double z, double zeta) {
     if (R == 0.0 && z == 0.0 && zeta == 0.0) {
         Kern k = {};
@@ -430,12 +511,13 @@ __device__ inline Kern pair_kernel_inf(double K, double R, double z, double zeta
         k.Wi = -2.0 * PI * K;
         return k;
     }
-    return wave_kern(K, wave_kernel(K * R, -K * (z + zeta)));
+    return wave_kern(K, wave_kernel<F32>(K * R, -K * (z + zeta)));
 }
 
 // green_fin.rs:1007-1095 finite_kernel with the fin_point data of both points.
 // fz / fzeta: pointers to the plane-0 entry of the point in the fin_point planes (stride N).
-__device__ inline Kern finite_kernel(const FdParams& fd, const double* T1, const double* T2, double R, double z,
+template <bool F32 = false, class TT = double>
+__device__ inline Kern finite_kernel(const FdParams& fd, const TT* T1, const TT* T2, double R, double z,
                                      double zeta, const double* fz, const double* fzeta, int stride) {
     double h = fd.h;
     double d1 = z - zeta;
@@ -503,8 +585,13 @@ __device__ inline Kern finite_kernel(const FdParams& fd, const double* T1, const
         return o;
     }
     double ih = 1.0 / h, ih2 = ih * ih, f1[3], f2[3];
-    phi_tiles(T1, 1, R * ih, v[0] * ih, f1);
-    phi_tiles(T2, 2, R * ih, v[1] * ih, f2);
+    if constexpr (F32) {
+        phi_tiles_f32(T1, 1, R * ih, v[0] * ih, f1);
+        phi_tiles_f32(T2, 2, R * ih, v[1] * ih, f2);
+    } else {
+        phi_tiles(T1, 1, R * ih, v[0] * ih, f1);
+        phi_tiles(T2, 2, R * ih, v[1] * ih, f2);
+    }
     o.Wr = ih * (f1[0] + f2[0]);
     o.WrR = ih2 * (f1[1] + f2[1]);
     double A1z = -sg * ih2 * f1[2], Bz = ih2 * f2[2];
@@ -515,7 +602,7 @@ __device__ inline Kern finite_kernel(const FdParams& fd, const double* T1, const
             F3X = 0.0;
             F3Y = 0.0;
         } else {
-            wave_real(K * R, K * v[2], F3, F3X, F3Y);
+            wave_real<F32>(K * R, K * v[2], F3, F3X, F3Y);
         }
         o.Wr += K * F3;
         o.WrR += K * K * F3X;

@@ -144,6 +144,8 @@ __device__ __forceinline__ double free_term(int kind) { return kind == 1 ? -4.0 
 // Output policies of the assembly: complex128 column-major N x N (the FP64 form), or two FP32 planes
 // column-major with leading dimension Np (the mixed form; entry (k, n) at n Np + k).
 struct OutF64 {
+    static constexpr bool kF32 = false;  // FP64 coefficient tables
+    using Tile = double;
     double2* S;
     double2* A;
     size_t stride;
@@ -156,6 +158,8 @@ struct OutF64 {
 };
 
 struct OutF32 {
+    static constexpr bool kF32 = true;  // FP32 coefficient tables and tiles
+    using Tile = float;
     float* S;
     float* A;
     size_t bstride;  // per frequency: two planes of Np * Np
@@ -172,8 +176,8 @@ struct OutF32 {
 template <bool FINITE, class Out>
 __global__ void __launch_bounds__(256, 2) k_assemble(PanelsView pv, const double* __restrict__ st,
                                                   const FreqInfo* __restrict__ fi, const FdParams* __restrict__ fdp,
-                                                  const double* __restrict__ tiles, const double* __restrict__ fpt,
-                                                  Out out) {
+                                                  const typename Out::Tile* __restrict__ tiles,
+                                                  const double* __restrict__ fpt, Out out) {
     // statics (n, k) [q][k_local][n_local]; each (k_local, n_local) slot is read and then
     // overwritten with the results (S, A) of entry (n, k) by the one thread that owns it
     __shared__ double sT[4][32][33];
@@ -213,8 +217,8 @@ __global__ void __launch_bounds__(256, 2) k_assemble(PanelsView pv, const double
         kindk = pv.kind[k];
     }
     const FdParams* fd = FINITE ? fdp + f : nullptr;
-    const double* T1 = FINITE ? tiles + (size_t)f * (T1_SIZE + T2_SIZE) : nullptr;
-    const double* T2 = FINITE ? T1 + T1_SIZE : nullptr;
+    const typename Out::Tile* T1 = FINITE ? tiles + (size_t)f * (T1_SIZE + T2_SIZE) : nullptr;
+    const typename Out::Tile* T2 = FINITE ? T1 + T1_SIZE : nullptr;
     const double* fp = FINITE ? fpt + (size_t)f * FP_PLANES * N : nullptr;
 #pragma unroll 1
     for (int i = 0; i < 4; i++) {
@@ -233,9 +237,9 @@ __global__ void __launch_bounds__(256, 2) k_assemble(PanelsView pv, const double
         double R = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
         Kern w;
         if (FINITE) {
-            w = finite_kernel(*fd, T1, T2, R, xk[2], xn[2], fp + k, fp + n, N);
+            w = finite_kernel<Out::kF32>(*fd, T1, T2, R, xk[2], xn[2], fp + k, fp + n, N);
         } else {
-            w = pair_kernel_inf(K, R, xk[2], xn[2]);
+            w = pair_kernel_inf<Out::kF32>(K, R, xk[2], xn[2]);
         }
         // entry (k, n): the field point x_k against panel n
         size_t o1 = (size_t)k + (size_t)n * N;
@@ -275,8 +279,18 @@ void launch_assemble_f64(const PanelsView& pv, const double* st, int F, const Fr
         k_assemble<false, OutF64><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
 }
 
+// The finite-depth tiles of a batch rounded to FP32 (same layout: blocks of 36 coefficients).
+__global__ void k_tiles_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+        b[t] = (float)a[t];
+}
+
+void launch_tiles_f32(int F, const double* tiles, float* tiles_f, cudaStream_t s) {
+    k_tiles_f32<<<148, 256, 0, s>>>((size_t)F * (T1_SIZE + T2_SIZE), tiles, tiles_f);
+}
+
 void launch_assemble_f32(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
-                         const double* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
+                         const float* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
                          cudaStream_t s) {
     int nt = (pv.N + 31) / 32;
     dim3 grid(nt * (nt + 1) / 2, F);

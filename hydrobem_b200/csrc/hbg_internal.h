@@ -67,7 +67,7 @@ KernelProfiler& profiler();
 enum WsSlot {
     WS_VERTS = 0, WS_KIND, WS_PLANES, WS_BAD, WS_ST, WS_WORK, WS_NWORK, WS_S, WS_A, WS_U, WS_RHS, WS_X, WS_PHII,
     WS_IPIV, WS_INFO, WS_FI, WS_FD, WS_TILES, WS_SCR, WS_FPT, WS_HEADS, WS_OUT, WS_S32, WS_A32, WS_W, WS_P2,
-    WS_P3, WS_PL, WS_PU, WS_B, WS_XM, WS_R, WS_NORMS, WS_ERR, WS_PART, WS_DINV, WS_COUNT
+    WS_P3, WS_PL, WS_PU, WS_B, WS_XM, WS_R, WS_NORMS, WS_ERR, WS_PART, WS_DINV, WS_TILES_F, WS_COUNT
 };
 
 struct Workspace {
@@ -104,6 +104,17 @@ Workspace& workspace();  // of the current device, this host thread
 inline int& last_ir_iterations() {
     static thread_local int n = 0;
     return n;
+}
+
+// The largest relative correction max|d| / max|x| over the batch, per refinement iteration, of
+// the last mixed-precision batch of this thread.
+struct IrHistory {
+    double ratio[32];
+    int n = 0;
+};
+inline IrHistory& last_ir_history() {
+    static thread_local IrHistory h;
+    return h;
 }
 
 // Device time of a phase: events on the stream, added to *acc at stop().
@@ -154,8 +165,9 @@ void launch_assemble_f64(const PanelsView& pv, const double* st, int F, const Fr
                          const double* tiles, const double* fpt, bool finite, double2* S, double2* A,
                          size_t mat_stride, cudaStream_t s);
 void launch_assemble_f32(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
-                         const double* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
+                         const float* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
                          cudaStream_t s);
+void launch_tiles_f32(int F, const double* tiles, float* tiles_f, cudaStream_t s);
 // boundary values u [F][nrhs][N] and incident wave phiI [F][H][N]
 void launch_boundary(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double* heads, double depth,
                      double grav, double2* u, double2* phiI, cudaStream_t s);

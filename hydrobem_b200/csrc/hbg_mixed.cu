@@ -46,6 +46,19 @@ static bool make_map(CUtensorMap* m, void* base, uint64_t d0, uint64_t d1, uint6
            CUDA_SUCCESS;
 }
 
+// A 4-D tensor map with an arbitrary box, no swizzle (plain row-major tiles in shared memory).
+static bool make_map_box(CUtensorMap* m, CUtensorMapDataType dt, void* base, const uint64_t dims[4],
+                         const uint64_t strides[3], const uint32_t box[4]) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t d[4] = {dims[0], dims[1], dims[2], dims[3]};
+    cuuint64_t st[3] = {strides[0], strides[1], strides[2]};
+    cuuint32_t bx[4] = {box[0], box[1], box[2], box[3]};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    return fn(m, dt, 4, base, d, st, bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 struct MixedBuffers {
     void* p[24] = {};
     int n = 0;
@@ -62,9 +75,11 @@ struct MixedBuffers {
     }
 };
 
-// Refinement stops when the largest correction is below IR_TOL of the largest solution entry: the
-// solution is then that of the complex64 system to ~1e-9, far inside its ~1e-7 distance from the
-// FP64 system's solution (the rounding of the stored matrix).
+// Refinement stops when the error left after the last correction d_k is predicted below IR_TOL of
+// the largest solution entry: that error is about rho |d_k|, rho = |d_k| / |d_{k-1}| being the
+// observed contraction (about 1e-3 with the TF32 factors), and at most |d_k| itself.  The solution
+// is then that of the complex64 system to ~1e-9, far inside its ~1e-7 distance from the FP64
+// system's solution (the rounding of the stored matrix).
 constexpr double IR_TOL = 1e-9;
 
 #define MIXED_FAIL(code, text, fq) \
@@ -89,7 +104,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     const size_t prep = prep_rows * 2 * NBL;
     size_t per = 3 * MB * 4 + 2 * prep * 4 + (size_t)(NBL * 2 * NBL + 4 * NBL * NBL) * 4 +
                  (size_t)(nrhs + H) * N * 16 + 4 * (size_t)nrhs * Np * 16 + 64 +
-                 (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)FP_PLANES * N * 8 + (size_t)6912 * 3 * 8 : 0);
+                 (fin ? (size_t)(T1_SIZE + T2_SIZE) * 12 + (size_t)FP_PLANES * N * 8 + (size_t)6912 * 3 * 8 : 0);
     per += (size_t)(Np / NBL) * NBL * NBL * 8;  // the diagonal-block inverses
     size_t freeb = 0, totalb = 0;
     if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "cudaMemGetInfo failed", -1);
@@ -127,6 +142,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     FdParams* dfd = (FdParams*)get(WS_FD, sizeof(FdParams) * B);
     double* dheads = (double*)get(WS_HEADS, sizeof(double) * std::max(H, 1));
     double* tiles = fin ? (double*)get(WS_TILES, sizeof(double) * (T1_SIZE + T2_SIZE) * B) : nullptr;
+    float* tiles_f = fin ? (float*)get(WS_TILES_F, sizeof(float) * (T1_SIZE + T2_SIZE) * B) : nullptr;
     double* scr = fin ? (double*)get(WS_SCR, sizeof(double) * 6912 * 3 * B) : nullptr;
     double* fpt = fin ? (double*)get(WS_FPT, sizeof(double) * FP_PLANES * N * B) : nullptr;
     double* dout = (double*)get(WS_OUT, sizeof(double) * (72 + 3 * (size_t)H * 12) * B);
@@ -162,10 +178,43 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     const int nz = (N + GEMV_CHUNK - 1) / GEMV_CHUNK;
     double2* part = (double2*)ws.get(WS_PART, (size_t)nz * B * nrhs * N * 16);
     if (!part) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
+    for (auto fn : {(const void*)k_cgemv_tma<8>, (const void*)k_cgemv_tma<10>, (const void*)k_cgemv_tma<12>,
+                    (const void*)k_cgemv_tma<16>})
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gv_smem_bytes<16>());
+    // the TMA form for up to 16 right-hand sides (its maps cover exactly the matrices and vectors
+    // of the batch); the register form otherwise
+    auto gemv_tma = [&](const float* Mm, const double2* xv, int ldx, int nb, int nzt) -> bool {
+        if (nrhs > 16) return false;
+        CUtensorMap mM, mX;
+        const uint64_t dm[4] = {(uint64_t)Np, (uint64_t)Np, 2, (uint64_t)nb};
+        const uint64_t sm[3] = {(uint64_t)Np * 4, NP2 * 4, MB * 4};
+        const uint32_t bm[4] = {GV_ROWS, GV_COLS, 1, 1};
+        const int nr = nrhs <= 8 ? 8 : nrhs <= 10 ? 10 : nrhs <= 12 ? 12 : 16;
+        const uint64_t dx[4] = {2 * (uint64_t)ldx, (uint64_t)nrhs, (uint64_t)nb, 1};
+        const uint64_t sx[3] = {(uint64_t)ldx * 16, (uint64_t)nrhs * ldx * 16, (uint64_t)nb * nrhs * ldx * 16};
+        const uint32_t bx[4] = {2 * GV_COLS, (uint32_t)nr, 1, 1};
+        if (!make_map_box(&mM, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)Mm, dm, sm, bm) ||
+            !make_map_box(&mX, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void*)xv, dx, sx, bx))
+            return false;
+        dim3 g((N + GV_ROWS - 1) / GV_ROWS, nb, nzt);
+        if (nr == 8)
+            k_cgemv_tma<8><<<g, GV_THREADS, gv_smem_bytes<8>(), s>>>(mM, mX, N, nrhs, part, nb, err);
+        else if (nr == 10)
+            k_cgemv_tma<10><<<g, GV_THREADS, gv_smem_bytes<10>(), s>>>(mM, mX, N, nrhs, part, nb, err);
+        else if (nr == 12)
+            k_cgemv_tma<12><<<g, GV_THREADS, gv_smem_bytes<12>(), s>>>(mM, mX, N, nrhs, part, nb, err);
+        else
+            k_cgemv_tma<16><<<g, GV_THREADS, gv_smem_bytes<16>(), s>>>(mM, mX, N, nrhs, part, nb, err);
+        return true;
+    };
+    const int nz_tma = (N + GV_CHUNK - 1) / GV_CHUNK;
     auto gemv = [&](const float* Mm, const double2* xv, int ldx, const double2* bias, auto* out, int nb, int fam) {
         P.begin(s);
         dim3 g((N + 127) / 128, nb, nz);
-        if (nrhs <= 8)
+        int nzr = nz;
+        if (gemv_tma(Mm, xv, ldx, nb, nz_tma))
+            nzr = nz_tma;
+        else if (nrhs <= 8)
             k_cgemv_part<8><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
         else if (nrhs <= 10)
             k_cgemv_part<10><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
@@ -175,8 +224,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             k_cgemv_part<16><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
         else
             k_cgemv_part<32><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
-        k_gemv_reduce<<<dim3((unsigned)(((size_t)nrhs * N + 255) / 256), nb), 256, 0, s>>>(N, nrhs, nb, nz, part, bias,
-                                                                                          Np, out, Np);
+        k_gemv_reduce<<<dim3((unsigned)(((size_t)nrhs * N + 255) / 256), nb), 256, 0, s>>>(N, nrhs, nb, nzr, part,
+                                                                                          bias, Np, out, Np);
         P.end(fam, 8.0 * (double)N * N * nb, s);
         *launches += 2;
     };
@@ -233,12 +282,13 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             if (fin) {
                 P.begin(s);
                 launch_fd_tiles(nb, dfd, tiles, scr, s);
+                launch_tiles_f32(nb, tiles, tiles_f, s);
                 launch_fin_points(pv, nb, dfd, fpt, s);
                 P.end(KF_FD_TILES, 0.0, s);
-                *launches += 3;
+                *launches += 4;
             }
             P.begin(s);
-            launch_assemble_f32(pv, st, nb, dfi, dfd, tiles, fpt, fin, S32, A32, Np, s);
+            launch_assemble_f32(pv, st, nb, dfi, dfd, tiles_f, fpt, fin, S32, A32, Np, s);
             // algorithmic bytes per pair: 4 FP64 statics read (32 B), S and A written as complex64 (16 B)
             P.end(KF_ASSEMBLE, 48.0 * (double)N * N * nb, s);
             if (Np > N) k_pad_identity<<<dim3(64, nb), 256, 0, s>>>(A32, N, Np, MB);
@@ -315,6 +365,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             k_to_c64<<<592, 256, 0, s>>>((size_t)nrhs * Np * nb, b, r);
             (*launches)++;
             double prev = INFINITY;
+            IrHistory& hist = last_ir_history();
+            hist.n = 0;
             for (it = 0; it < 30; it++) {
                 trisolve(r, nb);
                 k_ir_update<<<nb, 256, 0, s>>>(Np, nrhs, x, r, norms);
@@ -327,7 +379,9 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                     if (!std::isfinite(ratio)) ratio = INFINITY;
                     worst = std::max(worst, ratio);
                 }
-                if (worst <= IR_TOL) {  // the last correction was small: no residual needed
+                hist.ratio[hist.n++] = worst;
+                const double rho = it > 0 ? std::min(1.0, worst / prev) : 1.0;
+                if (worst * rho <= IR_TOL) {  // the error left is negligible: no residual needed
                     converged = true;
                     it++;
                     break;

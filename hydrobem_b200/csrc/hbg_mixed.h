@@ -14,5 +14,6 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                             const char** msg, int64_t* freq);
 
 int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* C, bool subtract, const char** msg);
+int measure_peaks(double* out, const char** msg);
 
 }  // namespace hbg

@@ -460,6 +460,114 @@ __global__ void __launch_bounds__(128) k_cgemv_part(int N, int Np, size_t bstrid
             if (c < nrhs) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
 }
 
+// The same partial products with the matrix and vector tiles streamed by TMA: CTA of 128 rows k
+// (one thread each) over a chunk of columns n, 16 columns per stage (both FP32 planes, 16 KB, and
+// the 16 complex entries of every right-hand side), GV_STAGES stages in flight from a producer
+// warp, so the bytes in flight do not depend on registers; FP64 accumulation as above.
+constexpr int GV_ROWS = 128, GV_COLS = 16, GV_STAGES = 3, GV_CHUNK = 1024;
+constexpr int GV_THREADS = GV_ROWS + 32;
+template <int NR>
+__host__ __device__ constexpr size_t gv_tx_bytes() {  // bytes one stage receives
+    return (size_t)2 * GV_COLS * GV_ROWS * 4 + (size_t)NR * GV_COLS * 16;
+}
+template <int NR>
+__host__ __device__ constexpr size_t gv_stage_bytes() {  // stage stride in shared memory (1024-byte aligned)
+    return (gv_tx_bytes<NR>() + 1023) / 1024 * 1024;
+}
+template <int NR>
+__host__ __device__ constexpr size_t gv_smem_bytes() {
+    return 1024 + GV_STAGES * gv_stage_bytes<NR>() + 128;
+}
+
+template <int NR>
+__global__ void __launch_bounds__(GV_THREADS) k_cgemv_tma(const __grid_constant__ CUtensorMap mapM,
+                                                             const __grid_constant__ CUtensorMap mapX, int N,
+                                                             int nrhs, double2* __restrict__ part, int F,
+                                                             int* __restrict__ err) {
+    extern __shared__ uint8_t gv_raw[];
+    uint8_t* base = align1024(gv_raw);
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + GV_STAGES * gv_stage_bytes<NR>());
+    uint64_t* empty = full + GV_STAGES;
+    const int f = blockIdx.y, z = blockIdx.z;
+    const int k0 = blockIdx.x * GV_ROWS;
+    const int nbeg = z * GV_CHUNK, nend = min(N, nbeg + GV_CHUNK);
+    const int nst = (nend - nbeg + GV_COLS - 1) / GV_COLS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < GV_STAGES; s++) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], GV_ROWS / 32);
+        }
+        tc::fence_barrier_init();
+    }
+    __syncthreads();
+    if (warp == GV_ROWS / 32) {
+        if (lane == 0) {
+            tc::prefetch_tensormap(&mapM);
+            tc::prefetch_tensormap(&mapX);
+            for (int si = 0; si < nst; si++) {
+                const int s = si % GV_STAGES;
+                if (si >= GV_STAGES && !tc::mbar_wait(&empty[s], ((si / GV_STAGES) - 1) & 1)) {
+                    atomicExch(err, 6);
+                    break;
+                }
+                uint8_t* st = base + s * gv_stage_bytes<NR>();
+                const int n0 = nbeg + si * GV_COLS;
+                tc::mbar_arrive_expect_tx(&full[s], (uint32_t)gv_tx_bytes<NR>());
+                tc::tma_load_4d(st, &mapM, &full[s], k0, n0, 0, f);
+                tc::tma_load_4d(st + GV_COLS * GV_ROWS * 4, &mapM, &full[s], k0, n0, 1, f);
+                tc::tma_load_4d(st + 2 * GV_COLS * GV_ROWS * 4, &mapX, &full[s], 2 * n0, 0, f, 0);
+            }
+        }
+        return;
+    }
+    double2 acc[NR];
+#pragma unroll
+    for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
+    const int t = threadIdx.x;
+    for (int si = 0; si < nst; si++) {
+        const int s = si % GV_STAGES;
+        if (!tc::mbar_wait(&full[s], (si / GV_STAGES) & 1)) {
+            atomicExch(err, 7);
+            break;
+        }
+        const uint8_t* st = base + s * gv_stage_bytes<NR>();
+        const float* sMr = reinterpret_cast<const float*>(st);
+        const float* sMi = sMr + GV_COLS * GV_ROWS;
+        const double2* sx = reinterpret_cast<const double2*>(st + 2 * GV_COLS * GV_ROWS * 4);  // [NR][GV_COLS]
+        const int lim = min(GV_COLS, nend - (nbeg + si * GV_COLS));
+        if (lim == GV_COLS) {
+#pragma unroll 4
+            for (int j = 0; j < GV_COLS; j++) {
+                const double mr = sMr[j * GV_ROWS + t], mi = sMi[j * GV_ROWS + t];
+#pragma unroll
+                for (int c = 0; c < NR; c++) {
+                    const double2 v = sx[c * GV_COLS + j];
+                    acc[c].x += mr * v.x - mi * v.y;
+                    acc[c].y += mr * v.y + mi * v.x;
+                }
+            }
+        } else {
+            for (int j = 0; j < lim; j++) {  // columns beyond N are never read (padding may hold anything)
+                const double mr = sMr[j * GV_ROWS + t], mi = sMi[j * GV_ROWS + t];
+#pragma unroll
+                for (int c = 0; c < NR; c++) {
+                    const double2 v = sx[c * GV_COLS + j];
+                    acc[c].x += mr * v.x - mi * v.y;
+                    acc[c].y += mr * v.y + mi * v.x;
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[s]);
+    }
+    const int k = k0 + t;
+    if (k < N)
+#pragma unroll
+        for (int c = 0; c < NR; c++)
+            if (c < nrhs) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
+}
+
 template <class T>
 __device__ __forceinline__ T make_out(double x, double y);
 template <>

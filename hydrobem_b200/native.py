@@ -63,7 +63,7 @@ EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_
            "hb_last_error_message", "hb_last_error_location", "hb_model_new", "hb_model_free", "hb_model_cancel",
            "hb_object", "hb_add", "hb_set_bool", "hb_set_int", "hb_set_real", "hb_set_text", "hb_set_reals",
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
-           "hbg_statics_noalloc"]
+           "hbg_statics_noalloc", "hbg_measure_peaks", "hbg_last_ir_history"]
 
 _lib = None
 
@@ -95,6 +95,8 @@ def lib():
     fp = ctypes.POINTER(ctypes.c_float)
     L.hbg_debug_gemm_tf32.argtypes = [ctypes.c_int32] * 3 + [fp, fp, fp, ctypes.c_int32]
     L.hbg_last_ir_iterations.argtypes = [ctypes.POINTER(ctypes.c_int32)]
+    L.hbg_measure_peaks.argtypes = [dp]
+    L.hbg_last_ir_history.argtypes = [dp, ctypes.POINTER(ctypes.c_int32)]
     L.hbg_statics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
                                       ctypes.c_int32, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
     L.hbg_statics_noalloc.restype = ctypes.c_int32
@@ -247,6 +249,21 @@ def statics_noalloc(d_vertices: int, d_kinds: int | None, n_panels: int, d_stati
     [4][N][N] FP64 with entry (k, j) of plane q at q N^2 + k + j N."""
     check(lib().hbg_statics_noalloc(d_vertices, d_kinds, n_panels, depth, 1 if logarithmic else 0, log_tolerance,
                                     d_statics, stream))
+
+
+def measure_peaks() -> dict:
+    """Measured dense peaks of the current device in TFLOP/s: fp64_fma, fp64_mma, tf32_tcgen05."""
+    out = np.zeros(3)
+    check(lib().hbg_measure_peaks(out.ctypes.data_as(dp)))
+    return {"fp64_fma": float(out[0]), "fp64_mma": float(out[1]), "tf32_tcgen05": float(out[2])}
+
+
+def last_ir_history() -> list:
+    """Largest relative correction per refinement iteration of the last mixed-precision batch."""
+    out = np.zeros(32)
+    n = ctypes.c_int32()
+    check(lib().hbg_last_ir_history(out.ctypes.data_as(dp), ctypes.byref(n)))
+    return [float(v) for v in out[: n.value]]
 
 
 def last_ir_iterations() -> int:

@@ -149,8 +149,18 @@ HbStatus hbg_debug_matrices(const HbgBody *body, double omega, const HbgOptions 
 HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const float *A, const float *B, float *C,
                              int32_t subtract);
 
+/* Measured compute peaks of the current device, for the benchmark's rooflines: out3[0] FP64 FMA,
+ * out3[1] FP64 warp MMA (mma.sync m8n8k4), out3[2] TF32 tcgen05 MMA, all dense TFLOP/s, each from
+ * a kernel that keeps its pipe busy from registers or shared memory.  Replaces no reference
+ * interface. */
+HbStatus hbg_measure_peaks(double *out3);
+
 /* Refinement iterations of the last mixed-precision frequency batch of this thread. */
 HbStatus hbg_last_ir_iterations(int32_t *n);
+
+/* The refinement history of that batch: per iteration the largest relative correction
+ * max|d| / max|x| over its frequencies (*n <= 32 values into ratios32[32]). */
+HbStatus hbg_last_ir_history(double *ratios32, int32_t *n);
 
 /* The statics of one panel set -- the frequency-independent Rankine source and dipole integrals
  * with their logarithmic-singularity corrections, FP64 [4][N][N] with entry (k, j) of plane q at
