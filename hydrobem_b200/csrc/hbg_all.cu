@@ -4,6 +4,7 @@
 #include "hbg_lu.cu"
 #include "hbg_mixed.cu"
 #include "hbg_peaks.cu"
+#include "hbg_surrogate.cu"
 #include "hbg_api.cu"
 #include "hbg_model.cu"
 #include "hbg_noalloc.cu"

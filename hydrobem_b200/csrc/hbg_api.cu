@@ -777,6 +777,61 @@ extern "C" HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const f
     }
 }
 
+static int current_device_ready() {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        throw Failure{HB_ERR_UNSUPPORTED, "no CUDA device: this library runs the path on the GPU only"};
+    int dev = 0;
+    CUDA_OK(cudaGetDevice(&dev));
+    device_ctx(dev);
+    return dev;
+}
+
+extern "C" HbStatus hbg_surrogate_train(int64_t n_train, int32_t batch, int32_t steps, double lr, uint64_t seed,
+                                        int64_t n_val, float* params, float* norm, double* report) {
+    try {
+        if (!params || !norm || !report) return fail({HB_ERR_ARGUMENT, "null argument"});
+        current_device_ready();
+        const char* msg = "";
+        int rc = surrogate_train(n_train, batch, steps, lr, seed, n_val, params, norm, report, &msg);
+        if (rc) return fail({rc, msg});
+        return HB_OK;
+    } catch (const Failure& f) {
+        return fail(f);
+    }
+}
+
+extern "C" HbStatus hbg_surrogate_grad(const float* params, int32_t n, const float* inputs, const float* targets,
+                                       float* grads, double* loss) {
+    try {
+        if (!params || !inputs || !targets || !grads || !loss) return fail({HB_ERR_ARGUMENT, "null argument"});
+        current_device_ready();
+        const char* msg = "";
+        int rc = surrogate_grad(params, n, inputs, targets, grads, loss, &msg);
+        if (rc) return fail({rc, msg});
+        return HB_OK;
+    } catch (const Failure& f) {
+        return fail(f);
+    }
+}
+
+extern "C" HbStatus hbg_surrogate_eval(const float* params, const float* norm, int32_t n, const double* xy,
+                                       double* out_net, double* out_table, double* ms2) {
+    try {
+        if (!params || !norm || !xy || !ms2) return fail({HB_ERR_ARGUMENT, "null argument"});
+        if (n < 1) return fail({HB_ERR_VALUE, "n must be positive"});
+        for (int32_t i = 0; i < 2 * n; i++)
+            if (!(xy[i] >= 0.0 && xy[i] < 30.0)) return fail({HB_ERR_VALUE, "points must lie in the trained domain [0, 30)^2"});
+        current_device_ready();
+        const char* msg = "";
+        int rc = surrogate_eval(params, norm, n, xy, out_net, out_table, ms2, &msg);
+        if (rc) return fail({rc, msg});
+        return HB_OK;
+    } catch (const Failure& f) {
+        return fail(f);
+    }
+}
+
 extern "C" HbStatus hbg_measure_peaks(double* out3) {
     try {
         if (!out3) return fail({HB_ERR_ARGUMENT, "null argument"});

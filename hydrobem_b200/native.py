@@ -63,7 +63,8 @@ EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_
            "hb_last_error_message", "hb_last_error_location", "hb_model_new", "hb_model_free", "hb_model_cancel",
            "hb_object", "hb_add", "hb_set_bool", "hb_set_int", "hb_set_real", "hb_set_text", "hb_set_reals",
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
-           "hbg_statics_noalloc", "hbg_measure_peaks", "hbg_last_ir_history"]
+           "hbg_statics_noalloc", "hbg_measure_peaks", "hbg_last_ir_history", "hbg_surrogate_train",
+           "hbg_surrogate_grad", "hbg_surrogate_eval"]
 
 _lib = None
 
@@ -97,6 +98,10 @@ def lib():
     L.hbg_last_ir_iterations.argtypes = [ctypes.POINTER(ctypes.c_int32)]
     L.hbg_measure_peaks.argtypes = [dp]
     L.hbg_last_ir_history.argtypes = [dp, ctypes.POINTER(ctypes.c_int32)]
+    L.hbg_surrogate_train.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                      ctypes.c_uint64, ctypes.c_int64, fp, fp, dp]
+    L.hbg_surrogate_grad.argtypes = [fp, ctypes.c_int32, fp, fp, fp, dp]
+    L.hbg_surrogate_eval.argtypes = [fp, fp, ctypes.c_int32, dp, dp, dp, dp]
     L.hbg_statics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
                                       ctypes.c_int32, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
     L.hbg_statics_noalloc.restype = ctypes.c_int32
@@ -264,6 +269,52 @@ def last_ir_history() -> list:
     n = ctypes.c_int32()
     check(lib().hbg_last_ir_history(out.ctypes.data_as(dp), ctypes.byref(n)))
     return [float(v) for v in out[: n.value]]
+
+
+SURROGATE_PARAMS = 50822
+SURROGATE_OUTPUTS = ["g", "g_X", "g_Y", "I", "I_X", "I_Y"]
+
+
+def surrogate_train(n_train=1 << 22, batch=8192, steps=3000, lr=2e-3, seed=1, n_val=1 << 16):
+    """Train the wave-term surrogate on the current device; returns (params, norm, report dict)."""
+    p = np.zeros(SURROGATE_PARAMS, np.float32)
+    nm = np.zeros(12, np.float32)
+    rep = np.zeros(15)
+    fpp = ctypes.POINTER(ctypes.c_float)
+    check(lib().hbg_surrogate_train(n_train, batch, steps, lr, seed, n_val, p.ctypes.data_as(fpp),
+                                    nm.ctypes.data_as(fpp), rep.ctypes.data_as(dp)))
+    report = {"loss_first": rep[0], "loss_last": rep[1], "train_ms": rep[2],
+              "val_rms_over_spread": dict(zip(SURROGATE_OUTPUTS, rep[3:9].tolist())),
+              "val_max_over_max": dict(zip(SURROGATE_OUTPUTS, rep[9:15].tolist()))}
+    return p, nm, report
+
+
+def surrogate_grad(params, inputs, targets):
+    """(loss, grads) of the training loss from the device training kernels (test support)."""
+    fpp = ctypes.POINTER(ctypes.c_float)
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(inputs, np.float32)
+    t = np.ascontiguousarray(targets, np.float32)
+    g = np.zeros(SURROGATE_PARAMS, np.float32)
+    loss = ctypes.c_double()
+    check(lib().hbg_surrogate_grad(p.ctypes.data_as(fpp), len(x), x.ctypes.data_as(fpp), t.ctypes.data_as(fpp),
+                                   g.ctypes.data_as(fpp), ctypes.byref(loss)))
+    return loss.value, g
+
+
+def surrogate_eval(params, norm, xy):
+    """(network [n][6], table [n][6], (ms network, ms table)) at points xy [n][2] in [0, 30)^2."""
+    fpp = ctypes.POINTER(ctypes.c_float)
+    p = np.ascontiguousarray(params, np.float32)
+    nm = np.ascontiguousarray(norm, np.float32)
+    x = np.ascontiguousarray(xy, np.float64)
+    n = len(x)
+    on = np.zeros((n, 6))
+    ot = np.zeros((n, 6))
+    ms = np.zeros(2)
+    check(lib().hbg_surrogate_eval(p.ctypes.data_as(fpp), nm.ctypes.data_as(fpp), n, x.ctypes.data_as(dp),
+                                   on.ctypes.data_as(dp), ot.ctypes.data_as(dp), ms.ctypes.data_as(dp)))
+    return on, ot, (float(ms[0]), float(ms[1]))
 
 
 def last_ir_iterations() -> int:

@@ -155,6 +155,32 @@ HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const float *A, co
  * interface. */
 HbStatus hbg_measure_peaks(double *out3);
 
+/* ---- the learned part: an MLP surrogate of the regular part of the infinite-depth wave term
+ * (inputs X = K R, Y = -K (z + zeta) in [0, 30)^2, log-scaled, and 1 / (K h) = 0; outputs g, g_X, g_Y
+ * with g = F + 2 e^-Y J0(X) (log(Y + R0) + gamma - log 2), and I, I_X, I_Y), 3 -> 128 x 4 -> 6,
+ * SiLU, BF16 weights, FP32 accumulation.  No counterpart in the reference (it replaces the table
+ * evaluation of green_inf.rs:316-368 inside its domain, the table remaining the fallback and the
+ * judge of its error).  params: 50822 floats; norm: 12 floats (means, spreads of the outputs). */
+
+/* Train on the current device: n_train samples of the library's own table evaluation (2-D Halton,
+ * log-spaced), `steps` Adam steps of `batch` samples (cosine learning-rate decay from lr), then
+ * validate on n_val further samples through the tensor-core inference kernel.  report[15]: loss of
+ * the first and last step, training device ms, validation rms error / spread per output [3..8],
+ * max |error| / max |target| per output [9..14]. */
+HbStatus hbg_surrogate_train(int64_t n_train, int32_t batch, int32_t steps, double lr, uint64_t seed, int64_t n_val,
+                             float *params, float *norm, double *report);
+
+/* Test support: the gradient of the mean squared error over n standardized samples (inputs [n][3],
+ * targets [n][6]) at params, computed by the training kernels; grads [50822]. */
+HbStatus hbg_surrogate_grad(const float *params, int32_t n, const float *inputs, const float *targets, float *grads,
+                            double *loss);
+
+/* The network (tensor cores) and the table evaluation at the same n points xy [n][2] = (X, Y) in
+ * [0, 30)^2: out_net, out_table [n][6] (either may be NULL); ms2 = device milliseconds of each over
+ * the n points (points resident on the device). */
+HbStatus hbg_surrogate_eval(const float *params, const float *norm, int32_t n, const double *xy, double *out_net,
+                            double *out_table, double *ms2);
+
 /* Refinement iterations of the last mixed-precision frequency batch of this thread. */
 HbStatus hbg_last_ir_iterations(int32_t *n);
 

@@ -1,0 +1,129 @@
+"""The learned part: the wave-term surrogate's training kernels against a CPU computation of the same
+network (gradients), its training on the library's own table evaluation, and what the trained network
+gains, or loses, against the table evaluation it would replace (device time per evaluation, error)."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from hydrobem_b200 import native as nv
+
+pytestmark = pytest.mark.gpu
+
+IN, H, OUT = 3, 128, 6
+
+
+def bf16(x):
+    """Round float32 values to bfloat16 (nearest, ties to even), returned as float32."""
+    b = np.asarray(x, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((b + 0x7FFF + ((b >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32)
+
+
+def layout():
+    """(weight offset, bias offset, fan-in, fan-out) of the five layers in the parameter vector."""
+    out, off = [], 0
+    for l in range(5):
+        fi, fo = (IN if l == 0 else H), (OUT if l == 4 else H)
+        out.append((off, off + fo * fi, fi, fo))
+        off += fo * fi + fo
+    assert off == nv.SURROGATE_PARAMS
+    return out
+
+
+def silu(z):
+    return z / (1.0 + np.exp(-z))
+
+
+def silu_d(z):
+    s = 1.0 / (1.0 + np.exp(-z))
+    return s * (1.0 + z * (1.0 - s))
+
+
+def cpu_loss_grad(p, X, T):
+    """Mean squared error and its gradient, FP64, with the device's BF16 rounding of the weights,
+    biases, inputs and hidden activations (the rounding itself passed straight through)."""
+    pr = bf16(p).astype(np.float64)
+    h = bf16(X).astype(np.float64)
+    hs, zs = [h], []
+    lay = layout()
+    for l, (ow, ob, fi, fo) in enumerate(lay):
+        W = pr[ow:ow + fo * fi].reshape(fo, fi)
+        z = h @ W.T + pr[ob:ob + fo]
+        zs.append(z)
+        h = bf16(silu(z).astype(np.float32)).astype(np.float64) if l < 4 else z
+        hs.append(h)
+    n = len(X)
+    d = 2.0 * (h - T) / (n * OUT)
+    loss = float(((h - T) ** 2).mean())
+    g = np.zeros(nv.SURROGATE_PARAMS)
+    for l in range(4, -1, -1):
+        ow, ob, fi, fo = lay[l]
+        g[ow:ow + fo * fi] = (d.T @ hs[l]).ravel()
+        g[ob:ob + fo] = d.sum(0)
+        if l > 0:
+            W = pr[ow:ow + fo * fi].reshape(fo, fi)
+            d = (d @ W) * silu_d(zs[l - 1])
+    return loss, g
+
+
+def test_training_gradients_match_cpu():
+    rng = np.random.default_rng(7)
+    p = np.zeros(nv.SURROGATE_PARAMS, np.float32)
+    for ow, ob, fi, fo in layout():
+        p[ow:ow + fo * fi] = rng.uniform(-1, 1, fo * fi) * np.sqrt(3.0 / fi)
+        p[ob:ob + fo] = rng.uniform(-0.1, 0.1, fo)
+    n = 300
+    X = np.column_stack([rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), np.zeros(n)]).astype(np.float32)
+    T = rng.standard_normal((n, OUT)).astype(np.float32)
+    loss_gpu, g_gpu = nv.surrogate_grad(p, X, T)
+    loss_cpu, g_cpu = cpu_loss_grad(p, X, T)
+    assert abs(loss_gpu - loss_cpu) <= 1e-5 * abs(loss_cpu)
+    for l, (ow, ob, fi, fo) in enumerate(layout()):
+        for a, b in ((ow, ow + fo * fi), (ob, ob + fo)):
+            ref = g_cpu[a:b]
+            err = np.linalg.norm(g_gpu[a:b] - ref) / np.linalg.norm(ref)
+            assert err < 2e-3, (l, a, err)
+
+
+@pytest.fixture(scope="module")
+def trained():
+    return nv.surrogate_train(n_train=1 << 18, batch=4096, steps=1500, lr=2e-3, seed=3, n_val=1 << 14)
+
+
+def test_training_fits_the_table(trained):
+    p, nm, rep = trained
+    assert np.isfinite(p).all()
+    assert rep["loss_last"] < 0.02 * rep["loss_first"], rep
+    # a BF16 network: percent-level agreement with the table, far from the 1e-5 of the solve
+    for k, v in rep["val_rms_over_spread"].items():
+        assert v < 0.2, (k, rep)
+
+
+def test_network_against_the_table_it_would_replace(trained):
+    """Same points, both on the device: the network's device time per evaluation and its error, next
+    to the table evaluation's.  The table stays the default and the judge of the network's error."""
+    p, nm, rep = trained
+    rng = np.random.default_rng(11)
+    n = 1 << 20
+    xy = np.expm1(rng.uniform(0.0, 1.0, (n, 2)) * np.log(31.0))
+    net, tab, (ms_net, ms_tab) = nv.surrogate_eval(p, nm, xy)
+    assert np.isfinite(net).all() and np.isfinite(tab).all()
+    assert ms_net > 0 and ms_tab > 0
+    # the error on fresh points is the validation error of the training run (same network, same
+    # kernel): rms / spread within a factor of 3 of it, per output
+    spread = nm[6:12].astype(np.float64)
+    rms = np.sqrt(((net - tab) ** 2).mean(axis=0)) / spread
+    val = np.array([rep["val_rms_over_spread"][k] for k in nv.SURROGATE_OUTPUTS])
+    assert (rms < 3.0 * val + 1e-3).all() and (val < 3.0 * rms + 1e-3).all(), (rms, val)
+    err = np.abs(net - tab).max(axis=0) / np.abs(tab).max(axis=0)
+    print(f"\nsurrogate vs table, {n} points: network {ms_net:.3f} ms, table {ms_tab:.3f} ms "
+          f"(network/table time {ms_net / ms_tab:.2f}); rms error / spread {np.round(rms, 4).tolist()}; "
+          f"max error / max |value| {np.round(err, 4).tolist()}")
+
+
+def test_points_outside_the_trained_domain_are_refused(trained):
+    p, nm, _ = trained
+    with pytest.raises(nv.HydroBEMError):
+        nv.surrogate_eval(p, nm, np.array([[31.0, 1.0]]))
