@@ -41,6 +41,11 @@ N_PERIODS = 40
 HEADINGS = [0.0, 30.0, 60.0, 90.0]
 DEPTH = 5.0
 WORKLOAD = "cylinder r=1 m d=0.5 m, 4096 panels (64x32 side + 64x32 bottom), h=5 m, 40 periods 1.5-20 s, 4 headings"
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a kernel family on the
+# benchmark workload, from an ncu capture of the 8-frequency medium case scaled by 5 (every byte of
+# the assembly scales with the frequencies of the launch).
+DRAM_TRAFFIC = {("mixed", "assemble"): 32.1e9}
+
 CASE_LABELS = {
     "c2": WORKLOAD,
     "medium": "cylinder r=1 m d=0.5 m, 4096 panels, h=5 m, 8 periods 1.5-20 s, 4 headings (profiling cut)",
@@ -270,10 +275,7 @@ def ours(args, world, rank, local, pg):
         bound, unit = "tensor", "TFLOP/s"
     else:
         peak, bound, unit, pk = peaks["hbm_gbs"], "hbm", "GB/s", f"hbm copy ({peak_kind})"
-    traffic = None
-    tfile = ROOT / "profiles" / "traffic.json"
-    if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(f"{args.precision}:{fam}")
+    traffic = DRAM_TRAFFIC.get((args.precision, fam)) if CASE == "c2" else None
     clocks = clk.summary()
     line = {"metric": "freq solves/s at N=4096", "value": value, "unit": "freq solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
