@@ -289,6 +289,7 @@ def ours(args, world, rank, local, pg):
             "roofline": {"bound": bound, "kernel": fam, "achieved": achieved, "peak": peak, "unit": unit,
                          "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
                          "peak_kind": pk, "launches": n, "ms": ms},
+            "step_ms": [round(x, 2) for x in dev_ms],
             "phases_ms": {k: round(x, 3) for k, x in phases.items()},
             "kernels_ms": {k: round(x[0], 3) for k, x in prof.items() if x[1]},
             "measured_peaks_tflops": {k: round(x, 1) for k, x in pipe_peaks.items()},

@@ -623,10 +623,12 @@ extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_proble
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);
+        phase_timers().flush();
         try {
             for (int64_t p = 0; p < n_problems; p++) solve_problem(problems[p], *opt, p, s);
         } catch (...) {
             cudaStreamSynchronize(s);
+            phase_timers().flush();
             cudaStreamDestroy(s);
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
@@ -634,6 +636,7 @@ extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_proble
         }
         cudaEventRecord(e1, s);
         cudaEventSynchronize(e1);
+        phase_timers().flush();
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         g_profile[5] = ms;

@@ -1,5 +1,6 @@
 // hbg_internal.h -- host-side declarations shared by the translation units of libhydrobem_gpu.
 #pragma once
+#include <vector>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -117,11 +118,37 @@ inline IrHistory& last_ir_history() {
     return h;
 }
 
-// Device time of a phase: events on the stream, added to *acc at stop().
+// Phase timings recorded without waiting: the event pairs are kept until flush(), which the solve
+// calls once its stream has finished, so a phase boundary never stalls the host.
+struct PhaseTimers {
+    struct Pending {
+        cudaEvent_t a, b;
+        double* acc;
+    };
+    std::vector<Pending> pend;
+    void flush() {
+        for (auto& p : pend) {
+            cudaEventSynchronize(p.b);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, p.a, p.b);
+            *p.acc += ms;
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+        pend.clear();
+    }
+};
+inline PhaseTimers& phase_timers() {
+    static thread_local PhaseTimers t;
+    return t;
+}
+
+// Device time of a phase: events on the stream, added to *acc at the next PhaseTimers::flush().
 struct EventTimer {
     cudaEvent_t a{}, b{};
     cudaStream_t s;
     double* acc;
+    bool stopped = false;
     EventTimer(cudaStream_t st, double* target) : s(st), acc(target) {
         cudaEventCreate(&a);
         cudaEventCreate(&b);
@@ -129,14 +156,14 @@ struct EventTimer {
     }
     void stop() {
         cudaEventRecord(b, s);
-        cudaEventSynchronize(b);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, a, b);
-        *acc += ms;
+        phase_timers().pend.push_back({a, b, acc});
+        stopped = true;
     }
     ~EventTimer() {
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
+        if (!stopped) {
+            cudaEventDestroy(a);
+            cudaEventDestroy(b);
+        }
     }
 };
 

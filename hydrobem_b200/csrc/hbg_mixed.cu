@@ -163,7 +163,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     int dev = 0, n_sm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    const int dsmem = NBL * (NBL + 1) * (int)sizeof(float2);
+    const int dsmem = (int)df_smem_bytes();
     cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, dsmem);
     cudaFuncSetAttribute(k_tri_step<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(12));
     cudaFuncSetAttribute(k_tri_step<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(16));
@@ -307,7 +307,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             for (int k0 = 0; k0 < Np; k0 += NBL) {
                 const int n = Np - k0 - NBL;
                 P.begin(s);
-                k_diag_factor<<<nb, 1024, dsmem, s>>>(W, Np, MB, k0, PL, PU, DINV, err);
+                k_diag_factor<<<nb, DF_THREADS, dsmem, s>>>(W, Np, MB, k0, PL, PU, DINV, err);
                 P.end(KF_LU_PANEL, 8.0 * NBL * (double)NBL * NBL * nb, s);
                 (*launches)++;
                 if (n == 0) break;
@@ -370,8 +370,14 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             for (it = 0; it < 30; it++) {
                 trisolve(r, nb);
                 k_ir_update<<<nb, 256, 0, s>>>(Np, nrhs, x, r, norms);
-                cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, s);
                 *launches += 1;
+                if (it == 0) {  // x = d: the first correction is the whole iterate (relative size 1)
+                    hist.ratio[hist.n++] = 1.0;
+                    prev = 1.0;
+                    gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL);
+                    continue;
+                }
+                cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, s);
                 cudaStreamSynchronize(s);
                 double worst = 0.0;
                 for (int i = 0; i < nb; i++) {
@@ -392,16 +398,9 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             }
             t.stop();
         }
+        // ---- forces (read back with the error flag: one wait for both)
         int herr = 0;
         cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
-        cudaStreamSynchronize(s);
-        P.flush();
-        if (cudaGetLastError() != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "CUDA error in the mixed-precision solve", f0);
-        if (herr == 10) MIXED_FAIL(HB_ERR_NUMERICAL, "zero pivot in the unpivoted mixed-precision LU", f0);
-        if (herr != 0) MIXED_FAIL(HB_ERR_INTERNAL, "a tensor-core pipeline wait timed out", f0);
-        if (!converged)
-            MIXED_FAIL(HB_ERR_NUMERICAL, "iterative refinement of the mixed-precision solve did not converge", f0);
-        // ---- forces
         {
             EventTimer t(s, &prof[4]);
             double* dA = dout;
@@ -418,6 +417,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         }
         cudaStreamSynchronize(s);
         P.flush();
+        if (cudaGetLastError() != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "CUDA error in the mixed-precision solve", f0);
+        if (herr == 10) MIXED_FAIL(HB_ERR_NUMERICAL, "zero pivot in the unpivoted mixed-precision LU", f0);
+        if (herr != 0) MIXED_FAIL(HB_ERR_INTERNAL, "a tensor-core pipeline wait timed out", f0);
+        if (!converged)
+            MIXED_FAIL(HB_ERR_NUMERICAL, "iterative refinement of the mixed-precision solve did not converge", f0);
         const double* hA = hout.data();
         const double* hB = hA + 36 * (size_t)nb;
         const double* hX = hA + 72 * (size_t)nb;

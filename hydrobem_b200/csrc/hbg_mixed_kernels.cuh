@@ -248,116 +248,255 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
 }
 
 // ---- diagonal block: M11 = L11 U11 (no pivoting) in shared memory, then L11^-1 and U11^-1.
-// One block per matrix.  Writes the factors back, L11^-1 as [Lr | Li] rows (the A operand of
-// GEMM2, [F][NBL][2 NBL]) and U11^-1 in the block-real K-major form (the B operand of GEMM1,
-// [F][2 NBL][2 NBL]).  A pivot of modulus below 1e-30 of the block's largest sets err (the
-// mixed form then reports the frequency; the FP64 form pivots).
-__global__ void __launch_bounds__(1024) k_diag_factor(float* __restrict__ W, int Np, size_t bstride, int k0,
-                                                      float* __restrict__ PL, float* __restrict__ PU,
-                                                      float2* __restrict__ DINV, int* __restrict__ err) {
-    extern __shared__ float2 blk[];  // [NBL][NBL + 1]
+// One CTA of DF_THREADS per matrix.  Writes the factors back, L11^-1 as [Lr | Li] rows (the A operand
+// of GEMM2, [F][NBL][2 NBL]), U11^-1 in the block-real K-major form (the B operand of GEMM1,
+// [F][2 NBL][2 NBL]) and both inverses per block for the triangular solves.  A pivot of modulus
+// below 1e-30 sets err (the mixed form then reports the frequency; the FP64 form pivots).
+//
+// Blocked by 32 columns: per panel, four warps factor the 32 columns (a lane per column, rows
+// shared round-robin, one named barrier per pivot), one warp each inverts the panel's 32 x 32 unit
+// lower and upper diagonal blocks (warp-synchronous, into a scratch), then all threads form
+// U12 = L_pp^-1 A12 and the trailing update A22 -= L21 U12.  The inverses of the whole 128 x 128
+// factors are then assembled from the diagonal-block inverses in three block-column stages.
+constexpr int DF_THREADS = 512, DF_LD = NBL + 1, DF_BLK = 32, DF_NB = NBL / DF_BLK, DF_SLD = DF_BLK + 1;
+constexpr size_t df_smem_bytes() { return (size_t)(NBL * DF_LD + 2 * DF_NB * DF_BLK * DF_SLD) * sizeof(float2); }
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ void cfma_sub(float2& x, float2 a, float2 b) {  // x -= a b
+    x.x -= a.x * b.x - a.y * b.y;
+    x.y -= a.x * b.y + a.y * b.x;
+}
+__device__ __forceinline__ void cfma_add(float2& x, float2 a, float2 b) {  // x += a b
+    x.x += a.x * b.x - a.y * b.y;
+    x.y += a.x * b.y + a.y * b.x;
+}
+
+// Warp-synchronous inverse of the 32 x 32 upper block U (diagonal included) at A (leading
+// dimension DF_LD) into X (leading dimension DF_SLD): X U = I, column by column, lane i owns row i.
+__device__ __forceinline__ void df_inv_upper32(const float2* A, float2* X) {
+    const int i = threadIdx.x & 31;
+    for (int j = 0; j < DF_BLK; j++) {
+        const float2 d = A[j * DF_LD + j];
+        const float dd = d.x * d.x + d.y * d.y;
+        const float2 inv = make_float2(d.x / dd, -d.y / dd);
+        float2 t = make_float2(0.f, 0.f);
+        if (i < j)  // X(i, j) = -(sum_{i <= k < j} X(i, k) U(k, j)) / U(j, j)
+            for (int k = i; k < j; k++) cfma_add(t, X[i * DF_SLD + k], A[k * DF_LD + j]);
+        __syncwarp();
+        if (i < j) X[i * DF_SLD + j] = make_float2(-(t.x * inv.x - t.y * inv.y), -(t.x * inv.y + t.y * inv.x));
+        if (i == j) X[j * DF_SLD + j] = inv;
+        if (i > j) X[i * DF_SLD + j] = make_float2(0.f, 0.f);
+        __syncwarp();
+    }
+}
+
+// Warp-synchronous inverse of the 32 x 32 unit lower block L at A into X: Y L = I from the last
+// column, Y(i, j) = -sum_{j < k <= i} Y(i, k) L(k, j) for i > j.
+__device__ __forceinline__ void df_inv_lower32(const float2* A, float2* X) {
+    const int i = threadIdx.x & 31;
+    for (int j = DF_BLK - 1; j >= 0; j--) {
+        float2 t = make_float2(0.f, 0.f);
+        if (i > j) {
+            t = A[i * DF_LD + j];  // k = i: Y(i, i) = 1
+            for (int k = j + 1; k < i; k++) cfma_add(t, X[i * DF_SLD + k], A[k * DF_LD + j]);
+        }
+        __syncwarp();
+        if (i > j) X[i * DF_SLD + j] = make_float2(-t.x, -t.y);
+        if (i == j) X[j * DF_SLD + j] = make_float2(1.f, 0.f);
+        if (i < j) X[i * DF_SLD + j] = make_float2(0.f, 0.f);
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ W, int Np, size_t bstride, int k0,
+                                                            float* __restrict__ PL, float* __restrict__ PU,
+                                                            float2* __restrict__ DINV, int* __restrict__ err) {
+    extern __shared__ float2 df_smem[];
+    float2* blk = df_smem;                    // [NBL][DF_LD]
+    float2* Li = blk + NBL * DF_LD;           // [DF_NB][DF_BLK][DF_SLD]: inverses of the diagonal L blocks
+    float2* Ui = Li + DF_NB * DF_BLK * DF_SLD;  // the same for U
     const int f = blockIdx.x;
     float* Wr = W + (size_t)f * bstride;
     float* Wi = Wr + (size_t)Np * Np;
-    constexpr int LD = NBL + 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) {
-        int r = t / NBL, c = t % NBL;
-        size_t o = (size_t)(k0 + r) * Np + k0 + c;
-        blk[r * LD + c] = make_float2(Wr[o], Wi[o]);
+        const int r = t / NBL, c = t % NBL;
+        const size_t o = (size_t)(k0 + r) * Np + k0 + c;
+        blk[r * DF_LD + c] = make_float2(Wr[o], Wi[o]);
     }
     __syncthreads();
-    for (int j = 0; j < NBL; j++) {
-        float2 d = blk[j * LD + j];
-        float dd = d.x * d.x + d.y * d.y;
-        if (threadIdx.x == 0 && !(dd > 1e-30f)) atomicExch(err, 10);
-        float2 inv = make_float2(d.x / dd, -d.y / dd);
-        for (int i = j + 1 + threadIdx.x; i < NBL; i += blockDim.x) {
-            float2 a = blk[i * LD + j];
-            blk[i * LD + j] = make_float2(a.x * inv.x - a.y * inv.y, a.x * inv.y + a.y * inv.x);
+    for (int pb = 0; pb < DF_NB; pb++) {
+        const int c0 = pb * DF_BLK;
+        // ---- panel: columns c0 .. c0 + 31, rows c0 .. NBL - 1; warp w < 4 owns rows c0 + w + 4 q
+        if (warp < 4) {
+            for (int j = 0; j < DF_BLK; j++) {
+                const int c = c0 + j;
+                asm volatile("bar.sync 1, 128;" ::: "memory");  // row c is final
+                const float2 d = blk[c * DF_LD + c];
+                const float dd = d.x * d.x + d.y * d.y;
+                if (threadIdx.x == 0 && !(dd > 1e-30f)) atomicExch(err, 10);
+                const float2 inv = make_float2(d.x / dd, -d.y / dd);
+                const float2 u = blk[c * DF_LD + c0 + lane];
+                int r = c + 1 + (((c0 + warp - (c + 1)) % 4) + 4) % 4;
+                for (; r < NBL; r += 4) {
+                    const float2 l = cmulf(blk[r * DF_LD + c], inv);
+                    if (lane > j) cfma_sub(blk[r * DF_LD + c0 + lane], l, u);
+                    __syncwarp();
+                    if (lane == j) blk[r * DF_LD + c] = l;
+                }
+            }
         }
         __syncthreads();
-        const int rem = NBL - 1 - j;
-        for (int t = threadIdx.x; t < rem * rem; t += blockDim.x) {
-            int i = j + 1 + t / rem, c = j + 1 + t % rem;
-            float2 l = blk[i * LD + j], u = blk[j * LD + c], a = blk[i * LD + c];
-            a.x -= l.x * u.x - l.y * u.y;
-            a.y -= l.x * u.y + l.y * u.x;
-            blk[i * LD + c] = a;
+        // ---- inverses of the panel's diagonal blocks (warps 0 and 1)
+        if (warp == 0) df_inv_lower32(blk + c0 * DF_LD + c0, Li + pb * DF_BLK * DF_SLD);
+        if (warp == 1) df_inv_upper32(blk + c0 * DF_LD + c0, Ui + pb * DF_BLK * DF_SLD);
+        __syncthreads();
+        const int n2 = NBL - c0 - DF_BLK;
+        if (n2 == 0) break;
+        // ---- U12 = L_pp^-1 A12 (rows c0 .. c0 + 31, columns c0 + 32 ..): into registers, then back
+        {
+            const float2* Y = Li + pb * DF_BLK * DF_SLD;
+            constexpr int MAXE = (DF_BLK * (NBL - DF_BLK) + DF_THREADS - 1) / DF_THREADS;  // 6
+            float2 v[MAXE];
+#pragma unroll
+            for (int e = 0; e < MAXE; e++) {
+                const int t = threadIdx.x + e * DF_THREADS;
+                v[e] = make_float2(0.f, 0.f);
+                if (t < DF_BLK * n2) {
+                    const int i = t / n2, cc = c0 + DF_BLK + t % n2;
+                    float2 a = make_float2(0.f, 0.f);
+                    for (int k = 0; k <= i; k++) cfma_add(a, Y[i * DF_SLD + k], blk[(c0 + k) * DF_LD + cc]);
+                    v[e] = a;
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < MAXE; e++) {
+                const int t = threadIdx.x + e * DF_THREADS;
+                if (t < DF_BLK * n2) blk[(c0 + t / n2) * DF_LD + c0 + DF_BLK + t % n2] = v[e];
+            }
+            __syncthreads();
+        }
+        // ---- trailing update A22 -= L21 U12
+        for (int t = threadIdx.x; t < n2 * n2; t += DF_THREADS) {
+            const int r = c0 + DF_BLK + t / n2, cc = c0 + DF_BLK + t % n2;
+            float2 a = blk[r * DF_LD + cc];
+#pragma unroll 8
+            for (int k = 0; k < DF_BLK; k++) cfma_sub(a, blk[r * DF_LD + c0 + k], blk[(c0 + k) * DF_LD + cc]);
+            blk[r * DF_LD + cc] = a;
         }
         __syncthreads();
     }
+    // the factors back to W
     for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) {
-        int r = t / NBL, c = t % NBL;
-        size_t o = (size_t)(k0 + r) * Np + k0 + c;
-        Wr[o] = blk[r * LD + c].x;
-        Wi[o] = blk[r * LD + c].y;
+        const int r = t / NBL, c = t % NBL;
+        const size_t o = (size_t)(k0 + r) * Np + k0 + c;
+        Wr[o] = blk[r * DF_LD + c].x;
+        Wi[o] = blk[r * DF_LD + c].y;
     }
     __syncthreads();
-    // In-place inversion of U11 (upper) and L11 (unit lower), column by column: for column j of
-    // U^-1 the leading block is already inverted, U^-1(0:j, j) = -U^-1(0:j, 0:j) U(0:j, j) / U(j, j);
-    // for L^-1 from the last column, L^-1(j+1:, j) = -L^-1(j+1:, j+1:) L(j+1:, j).  Eight threads
-    // per row share each dot product (shuffle reduction).
-    const int row = threadIdx.x >> 3, part = threadIdx.x & 7;
-    for (int j = 0; j < NBL; j++) {
-        float2 d = blk[j * LD + j];
-        float dd = d.x * d.x + d.y * d.y;
-        float2 inv = make_float2(d.x / dd, -d.y / dd);
-        float2 acc = make_float2(0.f, 0.f);
-        if (row < j)
-            for (int p = row + part; p < j; p += 8) {
-                float2 t = blk[row * LD + p], v = blk[p * LD + j];
-                acc.x += t.x * v.x - t.y * v.y;
-                acc.y += t.x * v.y + t.y * v.x;
-            }
-        for (int o = 4; o > 0; o >>= 1) {
-            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
-            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
-        }
-        __syncthreads();
-        if (row < j && part == 0)  // -acc / U(j, j) = -acc * inv
-            blk[row * LD + j] = make_float2(-(acc.x * inv.x - acc.y * inv.y), -(acc.x * inv.y + acc.y * inv.x));
-        if (row == j && part == 0) blk[j * LD + j] = inv;
-        __syncthreads();
-    }
-    for (int j = NBL - 2; j >= 0; j--) {
-        float2 acc = make_float2(0.f, 0.f);
-        if (row > j) {
-            // L^-1(row, j) = -(L(row, j) + sum_{j < p < row} L^-1(row, p) L(p, j))
-            if (part == 0) acc = blk[row * LD + j];
-            for (int p = j + 1 + part; p < row; p += 8) {
-                float2 t = blk[row * LD + p], v = blk[p * LD + j];
-                acc.x += t.x * v.x - t.y * v.y;
-                acc.y += t.x * v.y + t.y * v.x;
+    // ---- the off-diagonal blocks of U^-1 (threads 0..255) and L^-1 (threads 256..511), in place in
+    // blk, one block column per stage: U^-1(I, J) = -(sum_{I <= K < J} X(I, K) U(K, J)) X(J, J) for
+    // J = 1, 2, 3; L^-1(I, J) = -(sum_{J < K <= I} Y(I, K) L(K, J)) Y(J, J) for J = 2, 1, 0.
+    // X(I, K) / Y(I, K) are diagonal-block inverses (scratch) or blocks of earlier stages (blk).
+    const bool upper = threadIdx.x < DF_THREADS / 2;
+    const int tu = threadIdx.x % (DF_THREADS / 2);
+    for (int st = 1; st < DF_NB; st++) {
+        const int J = upper ? st : DF_NB - 1 - st;
+        const int nI = st;  // blocks I of this column: I < J (upper) or I > J (lower)
+        constexpr int MAXE = (DF_NB - 1) * DF_BLK * DF_BLK / (DF_THREADS / 2);  // 12
+        float2 v[MAXE];
+        // T(I, J) = sum_K X(I, K) U(K, J)
+#pragma unroll
+        for (int e = 0; e < MAXE; e++) {
+            const int t = tu + e * (DF_THREADS / 2);
+            v[e] = make_float2(0.f, 0.f);
+            if (t < nI * DF_BLK * DF_BLK) {
+                const int bi = t / (DF_BLK * DF_BLK), i = (t / DF_BLK) % DF_BLK, j = t % DF_BLK;
+                const int I = upper ? bi : J + 1 + bi;
+                const int row = I * DF_BLK + i, col = J * DF_BLK + j;
+                float2 a = make_float2(0.f, 0.f);
+                const int Kb = upper ? I : J + 1, Ke = upper ? J - 1 : I;
+                for (int K = Kb; K <= Ke; K++) {
+                    const float2* Xd = (upper ? Ui : Li) + K * DF_BLK * DF_SLD;  // X(K, K) when K == I
+                    for (int k = 0; k < DF_BLK; k++) {
+                        const int kk = K * DF_BLK + k;
+                        const float2 x = (K == I) ? Xd[i * DF_SLD + k] : blk[row * DF_LD + kk];
+                        cfma_add(a, x, blk[kk * DF_LD + col]);
+                    }
+                }
+                v[e] = a;
             }
         }
-        for (int o = 4; o > 0; o >>= 1) {
-            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
-            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+        __syncthreads();
+        // X(I, J) = -T(I, J) X(J, J): T staged in blk (block (I, J)), then the product back
+#pragma unroll
+        for (int e = 0; e < MAXE; e++) {
+            const int t = tu + e * (DF_THREADS / 2);
+            if (t < nI * DF_BLK * DF_BLK) {
+                const int bi = t / (DF_BLK * DF_BLK), i = (t / DF_BLK) % DF_BLK, j = t % DF_BLK;
+                const int I = upper ? bi : J + 1 + bi;
+                blk[(I * DF_BLK + i) * DF_LD + J * DF_BLK + j] = v[e];
+            }
         }
         __syncthreads();
-        if (row > j && part == 0) blk[row * LD + j] = make_float2(-acc.x, -acc.y);
+#pragma unroll
+        for (int e = 0; e < MAXE; e++) {
+            const int t = tu + e * (DF_THREADS / 2);
+            if (t < nI * DF_BLK * DF_BLK) {
+                const int bi = t / (DF_BLK * DF_BLK), i = (t / DF_BLK) % DF_BLK, j = t % DF_BLK;
+                const int I = upper ? bi : J + 1 + bi;
+                const float2* Xj = (upper ? Ui : Li) + J * DF_BLK * DF_SLD;
+                float2 a = make_float2(0.f, 0.f);
+                for (int k = 0; k < DF_BLK; k++)
+                    cfma_add(a, blk[(I * DF_BLK + i) * DF_LD + J * DF_BLK + k], Xj[k * DF_SLD + j]);
+                v[e] = make_float2(-a.x, -a.y);
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < MAXE; e++) {
+            const int t = tu + e * (DF_THREADS / 2);
+            if (t < nI * DF_BLK * DF_BLK) {
+                const int bi = t / (DF_BLK * DF_BLK), i = (t / DF_BLK) % DF_BLK, j = t % DF_BLK;
+                const int I = upper ? bi : J + 1 + bi;
+                blk[(I * DF_BLK + i) * DF_LD + J * DF_BLK + j] = v[e];
+            }
+        }
         __syncthreads();
     }
-    // blk now holds L^-1 (strictly below the diagonal, unit diagonal) and U^-1 (upper); kept per
-    // block for the triangular solves ([F][Np / NBL][NBL][NBL], row-major)
+    // inverse entry (i, c): U^-1 for i <= c, L^-1 (unit diagonal) for i > c
+    auto inv_at = [&](int i, int c) -> float2 {
+        const int bi = i / DF_BLK, bc = c / DF_BLK;
+        if (bi == bc) {
+            const float2* X = (i <= c ? Ui : Li) + bi * DF_BLK * DF_SLD;
+            return X[(i % DF_BLK) * DF_SLD + c % DF_BLK];
+        }
+        return blk[i * DF_LD + c];
+    };
     {
         float2* D = DINV + ((size_t)f * (Np / NBL) + k0 / NBL) * NBL * NBL;
-        for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) D[t] = blk[(t / NBL) * LD + t % NBL];
+        for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) D[t] = inv_at(t / NBL, t % NBL);
     }
     float* PLf = PL + (size_t)f * NBL * 2 * NBL;
     float* PUf = PU + (size_t)f * 2 * NBL * 2 * NBL;
     for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) {
-        const int i = t / NBL, c = t % NBL;
-        // [Lr | Li] rows of L^-1
-        float2 l = i > c ? blk[i * LD + c] : make_float2(i == c ? 1.f : 0.f, 0.f);
-        PLf[(size_t)i * 2 * NBL + c] = l.x;
-        PLf[(size_t)i * 2 * NBL + NBL + c] = l.y;
-        // U^-1 block-real K-major: row c: [Ur(:, c); -Ui(:, c)], row NBL + c: [Ui(:, c); Ur(:, c)]
-        float2 u = i <= c ? blk[i * LD + c] : make_float2(0.f, 0.f);  // U^-1(i, c)
-        PUf[(size_t)c * 2 * NBL + i] = u.x;
-        PUf[(size_t)c * 2 * NBL + NBL + i] = -u.y;
-        PUf[(size_t)(NBL + c) * 2 * NBL + i] = u.y;
-        PUf[(size_t)(NBL + c) * 2 * NBL + NBL + i] = u.x;
+        {  // [Lr | Li] rows of L^-1 (c fastest: coalesced)
+            const int i = t / NBL, c = t % NBL;
+            const float2 l = i > c ? inv_at(i, c) : make_float2(i == c ? 1.f : 0.f, 0.f);
+            PLf[(size_t)i * 2 * NBL + c] = l.x;
+            PLf[(size_t)i * 2 * NBL + NBL + c] = l.y;
+        }
+        {  // U^-1 block-real K-major (i fastest: coalesced): row c: [Ur(:, c); -Ui(:, c)], row NBL + c: [Ui(:, c); Ur(:, c)]
+            const int c = t / NBL, i = t % NBL;
+            const float2 u = i <= c ? inv_at(i, c) : make_float2(0.f, 0.f);  // U^-1(i, c)
+            PUf[(size_t)c * 2 * NBL + i] = u.x;
+            PUf[(size_t)c * 2 * NBL + NBL + i] = -u.y;
+            PUf[(size_t)(NBL + c) * 2 * NBL + i] = u.y;
+            PUf[(size_t)(NBL + c) * 2 * NBL + NBL + i] = u.x;
+        }
     }
 }
 
