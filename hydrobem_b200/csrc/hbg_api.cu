@@ -393,13 +393,6 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
         launch_panel_geometry(N, dverts.as<double>(), dkind.as<int32_t>(), dplanes.as<double>(), dbad.as<int32_t>(), s);
         P.end(KF_GEOMETRY, 0.0, s);
         g_launches++;
-        int32_t bad = 0;
-        CUDA_OK(cudaMemcpyAsync(&bad, dbad.p, sizeof bad, cudaMemcpyDeviceToHost, s));
-        CUDA_OK(cudaStreamSynchronize(s));
-        if (bad != big) {
-            Failure f{HB_ERR_VALUE, "invalid panel " + std::to_string(bad + 1) + " (degenerate, non-convex or non-finite)", body_index};
-            throw f;
-        }
         PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
         const size_t NN = (size_t)N * N;
         dst.alloc(sizeof(double) * 4 * NN);
@@ -412,9 +405,16 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
                        dnwork.as<int32_t>(), work_cap, s);
         // algorithmic bytes: the four FP64 planes written
         P.end(KF_STATICS, 32.0 * (double)NN, s);
-        int32_t nwork = 0;
+        // one wait for both: the first invalid panel (geometry) and the adaptive worklist size (statics;
+        // on invalid panels the statics are discarded, their kernels only see non-finite values)
+        int32_t bad = 0, nwork = 0;
+        CUDA_OK(cudaMemcpyAsync(&bad, dbad.p, sizeof bad, cudaMemcpyDeviceToHost, s));
         CUDA_OK(cudaMemcpyAsync(&nwork, dnwork.p, sizeof nwork, cudaMemcpyDeviceToHost, s));
         CUDA_OK(cudaStreamSynchronize(s));
+        if (bad != big) {
+            Failure f{HB_ERR_VALUE, "invalid panel " + std::to_string(bad + 1) + " (degenerate, non-convex or non-finite)", body_index};
+            throw f;
+        }
         if (nwork > work_cap) throw Failure{HB_ERR_INTERNAL, "adaptive log-integral worklist overflow", body_index};
         P.begin(s);
         launch_statics_adaptive(pv, dwork.as<int32_t>(), nwork, dst.as<double>(), s);

@@ -19,7 +19,7 @@
 namespace hbg {
 
 constexpr int NBL = 128;  // LU block width (complex columns)
-constexpr int GBM = 128, GBK = 32, GSTAGES = 4, GBN = 128;
+constexpr int GBM = 128, GBK = 32, GSTAGES = 3, GBN = 128;
 
 struct GemmArgs {
     int M, Nc, Kp;         // rows, real output columns, real inner dimension
@@ -28,9 +28,11 @@ struct GemmArgs {
     int mode;              // 0 store, 1 store and scatter into the GEMM3 operand, 2 subtract
     int o_row0, o_col0, o_nc;  // output placement in the planar matrix: column j' -> plane j' / o_nc
     int batch;             // matrices in the launch
-    float* p3;             // GEMM3's B operand [F][2n][2 NBL] (mode 1)
+    int b_split;           // 0: B coordinates (kk, row); > 0: B viewed as [row][2][.]: (kk % b_split, kk / b_split, row)
+    float* p3;             // a later update's B operand [F][2 p3_n][p3_ld] (mode 1)
     size_t p3_bstride;
     int p3_n;
+    int p3_ld, p3_kh, p3_koff;  // row length, offset of the second (imaginary-weight) half, first row of this block
     int* err;
 };
 
@@ -41,7 +43,7 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
 constexpr int GEMM_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
 constexpr size_t GEMM_STAGE_BYTES = (size_t)(GBM + GBN) * GBK * 4;
 constexpr size_t GEMM_C_BYTES = (size_t)GBM * GBN * 4;  // the output tile, four 32-column boxes
-constexpr size_t gemm_smem_bytes() { return 1024 + GSTAGES * GEMM_STAGE_BYTES + GEMM_C_BYTES + 256; }
+constexpr size_t gemm_smem_bytes() { return 1024 + GSTAGES * GEMM_STAGE_BYTES + 2 * GEMM_C_BYTES + 256; }
 
 // Persistent, warp-specialized TF32 GEMM of the mixed LU: tiles of 128 x 128 (real columns) taken
 // round-robin over (row tile, column tile, matrix).  Warp 0 lane 0 streams the A/B k-chunks through a
@@ -58,14 +60,14 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
     uint8_t* base = align1024(smem_raw);
     float* sA = reinterpret_cast<float*>(base);
     float* sB = sA + GSTAGES * GBM * GBK;
-    float* sC = sB + GSTAGES * GBN * GBK;  // [4 boxes][128 rows][32]
-    uint64_t* full = reinterpret_cast<uint64_t*>(sC + GBM * GBN);
+    float* sCb = sB + GSTAGES * GBN * GBK;  // two output-tile buffers, each [4 boxes][128 rows][32]
+    uint64_t* full = reinterpret_cast<uint64_t*>(sCb + 2 * GBM * GBN);
     uint64_t* empty = full + GSTAGES;
     uint64_t* tfull = empty + GSTAGES;  // [2]
     uint64_t* tempty = tfull + 2;       // [2]
-    uint64_t* cfull = tempty + 2;
-    uint64_t* cempty = cfull + 1;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(cempty + 1);
+    uint64_t* cfull = tempty + 2;   // [2]
+    uint64_t* cempty = cfull + 2;  // [2]
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(cempty + 2);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = (g.M + GBM - 1) / GBM, nt = (g.Nc + GBN - 1) / GBN;
     const int ntiles = mt * nt * g.batch;
@@ -79,8 +81,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
             tc::mbar_init(&tfull[b], 1);
             tc::mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
         }
-        tc::mbar_init(cfull, 1);
-        tc::mbar_init(cempty, 1);
+        for (int b = 0; b < 2; b++) {
+            tc::mbar_init(&cfull[b], 1);
+            tc::mbar_init(&cempty[b], 1);
+        }
         tc::fence_barrier_init();
         tc::prefetch_tensormap(&mapA);
         tc::prefetch_tensormap(&mapB);
@@ -104,6 +108,20 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
             for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x, it++) {
                 int m0, n0, f;
                 tile_coords(t, m0, n0, f);
+                if (g.mode == 2) {
+                    // the C block of this tile into buffer it % 2, once the store of tile it - 2 has read it
+                    const int cb = it & 1;
+                    if (it >= 2 && !tc::mbar_wait(&cempty[cb], ((it >> 1) - 1) & 1)) {
+                        atomicExch(g.err, 4);
+                        break;
+                    }
+                    const int plane = n0 >= g.o_nc ? 1 : 0, col0 = n0 - plane * g.o_nc;
+                    float* sC = sCb + cb * GBM * GBN;
+                    tc::mbar_arrive_expect_tx(&cfull[cb], (uint32_t)GEMM_C_BYTES);
+                    for (int q = 0; q < GBN / 32; q++)
+                        tc::tma_load_4d(sC + q * GBM * 32, &mapC, &cfull[cb], g.o_col0 + col0 + 32 * q, g.o_row0 + m0,
+                                        plane, f);
+                }
                 for (int kc = 0; kc < nk; kc++, kc_global++) {
                     const int s = kc_global % GSTAGES;
                     if (kc_global >= GSTAGES && !tc::mbar_wait(&empty[s], ((kc_global / GSTAGES) - 1) & 1)) {
@@ -119,20 +137,10 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
                         plane = kk / g.a_kc;
                     }
                     tc::tma_load_4d(sA + s * GBM * GBK, &mapA, &full[s], ax, g.a_row0 + m0, plane, f);
-                    tc::tma_load_4d(sB + s * GBN * GBK, &mapB, &full[s], kk, n0, 0, f);
-                }
-                if (!bad && g.mode == 2) {
-                    // the C block of this tile, once the previous tile's store has read the buffer (the
-                    // k-chunks above are already queued, so the main loop runs on meanwhile)
-                    if (it > 0 && !tc::mbar_wait(cempty, (it - 1) & 1)) {
-                        atomicExch(g.err, 4);
-                        break;
-                    }
-                    const int plane = n0 >= g.o_nc ? 1 : 0, col0 = n0 - plane * g.o_nc;
-                    tc::mbar_arrive_expect_tx(cfull, (uint32_t)GEMM_C_BYTES);
-                    for (int q = 0; q < GBN / 32; q++)
-                        tc::tma_load_4d(sC + q * GBM * 32, &mapC, cfull, g.o_col0 + col0 + 32 * q, g.o_row0 + m0, plane,
-                                        f);
+                    if (g.b_split)
+                        tc::tma_load_4d(sB + s * GBN * GBK, &mapB, &full[s], kk % g.b_split, kk / g.b_split, n0, f);
+                    else
+                        tc::tma_load_4d(sB + s * GBN * GBK, &mapB, &full[s], kk, n0, 0, f);
                 }
             }
         }
@@ -179,8 +187,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
             tile_coords(t, m0, n0, f);
             const int b = it & 1;
             bool ok = tc::mbar_wait(&tfull[b], (it >> 1) & 1);
-            if (ok && g.mode == 2) ok = tc::mbar_wait(cfull, it & 1);
-            if (ok && g.mode != 2 && it > 0) ok = tc::mbar_wait(cempty, (it - 1) & 1);  // the store buffer is free
+            float* sC = sCb + b * GBM * GBN;  // output buffer it % 2
+            if (ok && g.mode == 2) ok = tc::mbar_wait(&cfull[b], (it >> 1) & 1);
+            if (ok && g.mode != 2 && it >= 2) ok = tc::mbar_wait(&cempty[b], ((it >> 1) - 1) & 1);  // buffer free
             // one decision for the four epilogue warps, so none waits at a barrier the others left
             __syncwarp();
             if (!tc::bar_and(ok, 1, 128)) {
@@ -209,18 +218,19 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
                     *c4 = o;
                 }
                 if (g.mode == 1 && m0 + r < g.M) {
-                    // U12(kk = row, j) into the block-real K-major operand of GEMM3 (rows 2n, 2 NBL wide)
+                    // U(kk = row, j) into the block-real K-major operand of a later update (rows 2n,
+                    // p3_ld wide): row j [Ur(:, j) | -Ui(:, j)], row n + j [Ui(:, j) | Ur(:, j)]
                     float* p3f = g.p3 + (size_t)f * g.p3_bstride;
-                    const int n = g.p3_n, kk = m0 + r;
+                    const int n = g.p3_n, kk = g.p3_koff + m0 + r, ld = g.p3_ld, kh = g.p3_kh;
 #pragma unroll
                     for (int i = 0; i < 32; i++) {
                         const int j = col0 + 32 * q + i;
                         if (plane == 0) {
-                            p3f[(size_t)j * (2 * NBL) + kk] = v[i];
-                            p3f[(size_t)(n + j) * (2 * NBL) + NBL + kk] = v[i];
+                            p3f[(size_t)j * ld + kk] = v[i];
+                            p3f[(size_t)(n + j) * ld + kh + kk] = v[i];
                         } else {
-                            p3f[(size_t)j * (2 * NBL) + NBL + kk] = -v[i];
-                            p3f[(size_t)(n + j) * (2 * NBL) + kk] = v[i];
+                            p3f[(size_t)j * ld + kh + kk] = -v[i];
+                            p3f[(size_t)(n + j) * ld + kk] = v[i];
                         }
                     }
                 }
@@ -237,7 +247,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
                     tc::tma_store_4d(&mapC, sC + q * GBM * 32, g.o_col0 + col0 + 32 * q, g.o_row0 + m0, plane, f);
                 tc::bulk_commit();
                 tc::bulk_wait_read();  // the buffer may be refilled once the store has read it
-                tc::mbar_arrive(cempty);
+                tc::mbar_arrive(&cempty[b]);
             }
         }
         if (warp == 2 && lane == 0) tc::bulk_wait_all();
@@ -500,10 +510,10 @@ __global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ 
     }
 }
 
-// The block row M12 = rows k0..k0+NBL, columns k0+NBL..k0+NBL+n in the block-real K-major form
+// The block row B = rows k0..k0+NBL, columns c0..c0+n in the block-real K-major form
 // [F][2n][2 NBL]: row j: [Br(:, j); -Bi(:, j)], row n + j: [Bi(:, j); Br(:, j)] (32 x 32 tiles
 // transposed through shared memory).
-__global__ void k_prep_block_row(const float* __restrict__ W, int Np, size_t bstride, int k0, int n,
+__global__ void k_prep_block_row(const float* __restrict__ W, int Np, size_t bstride, int k0, int c0, int n,
                                  float* __restrict__ P2, size_t p2_bstride) {
     __shared__ float tr[32][33], ti[32][33];
     const int f = blockIdx.z;
@@ -512,7 +522,7 @@ __global__ void k_prep_block_row(const float* __restrict__ W, int Np, size_t bst
     const float* Wi = Wr + (size_t)Np * Np;
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int r = ty; r < 32; r += blockDim.y) {
-        size_t o = (size_t)(k0 + kk0 + r) * Np + k0 + NBL + j0 + tx;
+        size_t o = (size_t)(k0 + kk0 + r) * Np + c0 + j0 + tx;
         tr[r][tx] = Wr[o];
         ti[r][tx] = Wi[o];
     }
