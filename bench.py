@@ -297,7 +297,9 @@ def ours(args, world, rank, local, pg):
     if ir is not None:
         line["refinement"] = ir
     if precision == nv.HBG_MIXED and not args.no_plain:
-        line["plain_fp64"] = plain_comparison(nv, v, omegas, device, body)
+        line["plain_fp64"], plain = plain_comparison(nv, v, omegas, device, body)
+        if args.surrogate_steps > 0:
+            line["surrogate"] = surrogate_comparison(nv, v, omegas, device, plain, args.surrogate_steps)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_quick()
     return line
@@ -320,16 +322,51 @@ def plain_comparison(nv, v, omegas, device, mixed_body):
         ms.append(nv.last_profile()["total"])
     step = float(np.mean(ms))
 
-    def err(got, ref):
-        ref = np.asarray(ref)
-        peak = np.abs(ref).max()
-        scale = np.maximum(np.abs(ref).max(axis=0, keepdims=True), 1e-3 * peak)
-        return float((np.abs(np.asarray(got) - ref) / scale).max())
-
     mixed = mixed_body.results()
     plain = body.results()
     return {"value": len(omegas) / (step * 1e-3), "ms_per_step": step,
-            "err_vs_fp64": {k: err(mixed[k], plain[k]) for k in ("A", "B", "X")}}
+            "err_vs_fp64": {k: scaled_error(mixed[k], plain[k]) for k in ("A", "B", "X")}}, plain
+
+
+def scaled_error(got, ref):
+    """Per entry |got - ref| over the entry's largest modulus across frequencies (floor 1e-3 of the
+    quantity's peak), the largest over all entries."""
+    ref = np.asarray(ref)
+    peak = np.abs(ref).max()
+    scale = np.maximum(np.abs(ref).max(axis=0, keepdims=True), 1e-3 * peak)
+    return float((np.abs(np.asarray(got) - ref) / scale).max())
+
+
+def surrogate_comparison(nv, v, omegas, device, plain, train_steps):
+    """The learned part measured on the same job: train the wave-term network on the device (its own
+    kernels, samples of the table evaluation), solve the job with it as the wave term of the mixed
+    assembly, and report its throughput and its A, B, X error against the FP64 form, plus the device
+    time of one million network and table evaluations."""
+    import ctypes
+
+    p, nm, rep = nv.surrogate_train(n_train=1 << 20, batch=8192, steps=train_steps, lr=2e-3, seed=1,
+                                    n_val=1 << 16)
+    body = nv.Body(v, omegas, HEADINGS)
+    arr = (nv.HbgProblem * 1)(body.problem())
+    opt = nv.default_options(precision=nv.HBG_MIXED, depth=DEPTH, device=device, surrogate=nv.surrogate_blob(p, nm))
+    L = nv.lib()
+    nv.check(L.hbg_solve_batch(arr, 1, ctypes.byref(opt)))  # warm-up
+    ms = []
+    for _ in range(2):
+        nv.check(L.hbg_solve_batch(arr, 1, ctypes.byref(opt)))
+        ms.append(nv.last_profile()["total"])
+    pairs = nv.last_surrogate_pairs()
+    got = body.results()
+    rng = np.random.default_rng(5)
+    xy = np.expm1(rng.uniform(0.0, 1.0, (1 << 20, 2)) * np.log(31.0))
+    _, _, (ms_net, ms_tab) = nv.surrogate_eval(p, nm, xy)
+    err = {k: scaled_error(got[k], plain[k]) for k in ("A", "B", "X")}
+    step = float(np.mean(ms))
+    return {"value": len(omegas) / (step * 1e-3), "ms_per_step": step, "pairs_from_network": int(pairs),
+            "err_vs_fp64": err, "meets_1e-5": bool(max(err.values()) <= 1e-5),
+            "train": {"steps": train_steps, "samples": 1 << 20, "device_ms": round(rep["train_ms"], 1),
+                      "val_rms_over_spread": {k: round(x, 5) for k, x in rep["val_rms_over_spread"].items()}},
+            "eval_ms_per_1M_points": {"network": round(ms_net, 3), "table": round(ms_tab, 3)}}
 
 
 def cpu_baseline_quick():
@@ -360,6 +397,8 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison of the mixed form")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--surrogate-steps", type=int, default=4000,
+                    help="training steps of the wave-term network measured beside the mixed form (0: skip)")
     ap.add_argument("--case", default="c2", choices=["c2", "medium", "small", "tiny"])
     args = ap.parse_args()
     global CASE

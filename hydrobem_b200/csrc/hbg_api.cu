@@ -593,6 +593,7 @@ extern "C" void hbg_default_options(HbgOptions* opt) {
     opt->max_batch = 0;
     opt->device = 0;
     opt->cancel = nullptr;
+    opt->surrogate = nullptr;
 }
 
 extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_problems, const HbgOptions* opt) {
@@ -609,6 +610,8 @@ extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_proble
         }
         if (opt->precision != HBG_FP64 && opt->precision != HBG_MIXED)
             return fail({HB_ERR_VALUE, "unknown precision form"});
+        if (opt->surrogate && opt->precision != HBG_MIXED)
+            return fail({HB_ERR_VALUE, "the wave-term network is an option of the mixed form only"});
         if (!(opt->gravity > 0.0) || !(opt->density > 0.0) || opt->log_tolerance < 0.0)
             return fail({HB_ERR_VALUE, "gravity and density must be positive, log_tolerance nonnegative"});
         int ndev = 0;
@@ -833,6 +836,12 @@ extern "C" HbStatus hbg_surrogate_eval(const float* params, const float* norm, i
     } catch (const Failure& f) {
         return fail(f);
     }
+}
+
+extern "C" HbStatus hbg_last_surrogate_pairs(int64_t* n) {
+    if (!n) return fail({HB_ERR_ARGUMENT, "null argument"});
+    *n = last_surrogate_pairs();
+    return HB_OK;
 }
 
 extern "C" HbStatus hbg_measure_peaks(double* out3) {

@@ -516,9 +516,11 @@ __device__ inline Kern pair_kernel_inf(double K, double R, double z, double zeta
 
 // green_fin.rs:1007-1095 finite_kernel with the fin_point data of both points.
 // fz / fzeta: pointers to the plane-0 entry of the point in the fin_point planes (stride N).
-template <bool F32 = false, class TT = double>
+// SW: the infinite-depth wave term F3 at (K R, K v3) is supplied by the caller (*sw, when not null).
+template <bool F32 = false, class TT = double, bool SW = false>
 __device__ inline Kern finite_kernel(const FdParams& fd, const TT* T1, const TT* T2, double R, double z,
-                                     double zeta, const double* fz, const double* fzeta, int stride) {
+                                     double zeta, const double* fz, const double* fzeta, int stride,
+                                     const Wave* sw = nullptr) {
     double h = fd.h;
     double d1 = z - zeta;
     double sg = d1 > 0.0 ? 1.0 : d1 < 0.0 ? -1.0 : 0.0;
@@ -602,7 +604,17 @@ __device__ inline Kern finite_kernel(const FdParams& fd, const TT* T1, const TT*
             F3X = 0.0;
             F3Y = 0.0;
         } else {
-            wave_real<F32>(K * R, K * v[2], F3, F3X, F3Y);
+            if constexpr (SW) {
+                if (sw) {
+                    F3 = sw->F;
+                    F3X = sw->FX;
+                    F3Y = sw->FY;
+                } else {
+                    wave_real<F32>(K * R, K * v[2], F3, F3X, F3Y);
+                }
+            } else {
+                wave_real<F32>(K * R, K * v[2], F3, F3X, F3Y);
+            }
         }
         o.Wr += K * F3;
         o.WrR += K * K * F3X;

@@ -68,7 +68,8 @@ KernelProfiler& profiler();
 enum WsSlot {
     WS_VERTS = 0, WS_KIND, WS_PLANES, WS_BAD, WS_ST, WS_WORK, WS_NWORK, WS_S, WS_A, WS_U, WS_RHS, WS_X, WS_PHII,
     WS_IPIV, WS_INFO, WS_FI, WS_FD, WS_TILES, WS_SCR, WS_FPT, WS_HEADS, WS_OUT, WS_S32, WS_A32, WS_W, WS_P2,
-    WS_P3, WS_PL, WS_PU, WS_B, WS_XM, WS_R, WS_NORMS, WS_ERR, WS_PART, WS_DINV, WS_TILES_F, WS_COUNT
+    WS_P3, WS_PL, WS_PU, WS_B, WS_XM, WS_R, WS_NORMS, WS_ERR, WS_PART, WS_DINV, WS_TILES_F, WS_SG_PARAMS,
+    WS_SG_IMG, WS_SG_COUNT, WS_COUNT
 };
 
 struct Workspace {
@@ -195,6 +196,19 @@ void launch_assemble_f32(const PanelsView& pv, const double* st, int F, const Fr
                          const float* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
                          cudaStream_t s);
 void launch_tiles_f32(int F, const double* tiles, float* tiles_f, cudaStream_t s);
+// the wave-term network inside the mixed assembly: its parameters followed by the outputs' means and
+// spreads
+constexpr int SURROGATE_FLOATS = 50822 + 12;
+void launch_sg_pack(const float* params_norm, uint8_t* img, cudaStream_t s);
+size_t sg_image_bytes();
+void launch_assemble_f32_sg(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
+                            const float* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
+                            const uint8_t* img, unsigned long long* counts, cudaStream_t s);
+// pairs (unordered, over all frequencies) whose wave term came from the network in the last mixed solve
+inline long long& last_surrogate_pairs() {
+    static thread_local long long n = 0;
+    return n;
+}
 // boundary values u [F][nrhs][N] and incident wave phiI [F][H][N]
 void launch_boundary(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double* heads, double depth,
                      double grav, double2* u, double2* phiI, cudaStream_t s);

@@ -168,10 +168,23 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     double* dheads = (double*)get(WS_HEADS, sizeof(double) * std::max(H, 1));
     double* tiles = fin ? (double*)get(WS_TILES, sizeof(double) * (T1_SIZE + T2_SIZE) * B) : nullptr;
     float* tiles_f = fin ? (float*)get(WS_TILES_F, sizeof(float) * (T1_SIZE + T2_SIZE) * B) : nullptr;
+    // the wave-term network (optional): its parameters, the packed BF16 image the assembly loads, and
+    // the count of pairs it served
+    const bool sg = opt.surrogate != nullptr;
+    float* sg_params = sg ? (float*)get(WS_SG_PARAMS, sizeof(float) * SURROGATE_FLOATS) : nullptr;
+    uint8_t* sg_img = sg ? (uint8_t*)get(WS_SG_IMG, sg_image_bytes()) : nullptr;
+    unsigned long long* sg_count = sg ? (unsigned long long*)get(WS_SG_COUNT, sizeof(unsigned long long)) : nullptr;
     double* scr = fin ? (double*)get(WS_SCR, sizeof(double) * 6912 * 3 * B) : nullptr;
     double* fpt = fin ? (double*)get(WS_FPT, sizeof(double) * FP_PLANES * N * B) : nullptr;
     double* dout = (double*)get(WS_OUT, sizeof(double) * (72 + 3 * (size_t)H * 12) * B);
     if (!okb) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
+    last_surrogate_pairs() = 0;
+    if (sg) {
+        cudaMemcpyAsync(sg_params, opt.surrogate, sizeof(float) * SURROGATE_FLOATS, cudaMemcpyHostToDevice, s);
+        launch_sg_pack(sg_params, sg_img, s);
+        cudaMemsetAsync(sg_count, 0, sizeof(unsigned long long), s);
+        (*launches)++;
+    }
     // ---- tensor maps (whole batch; the batch index is the 4th coordinate)
     CUtensorMap mapW, mapPL, mapPU, mapP2, mapP3, mapP3w, mapP3h;
     const uint64_t fb = 4;  // bytes per float
@@ -317,7 +330,10 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 *launches += 4;
             }
             P.begin(s);
-            launch_assemble_f32(pv, st, nb, dfi, dfd, tiles_f, fpt, fin, S32, A32, Np, s);
+            if (sg)
+                launch_assemble_f32_sg(pv, st, nb, dfi, dfd, tiles_f, fpt, fin, S32, A32, Np, sg_img, sg_count, s);
+            else
+                launch_assemble_f32(pv, st, nb, dfi, dfd, tiles_f, fpt, fin, S32, A32, Np, s);
             // algorithmic bytes per pair: 4 FP64 statics read (32 B), S and A written as complex64 (16 B)
             P.end(KF_ASSEMBLE, 48.0 * (double)N * N * nb, s);
             if (Np > N) k_pad_identity<<<dim3(64, nb), 256, 0, s>>>(A32, N, Np, MB);
@@ -544,6 +560,12 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
         }
         last_ir_iterations() = it;
+    }
+    if (sg) {
+        unsigned long long used = 0;
+        cudaMemcpyAsync(&used, sg_count, sizeof used, cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        last_surrogate_pairs() = (long long)used;
     }
     return 0;
 }

@@ -30,6 +30,7 @@ constexpr int SG_LAYER_HH = SG_H * SG_H + SG_H;  // W and b of a hidden layer
 constexpr int SG_OFF_W4 = SG_OFF_W1 + 3 * SG_LAYER_HH, SG_OFF_B4 = SG_OFF_W4 + SG_OUT * SG_H;
 constexpr int SG_PARAMS = SG_OFF_B4 + SG_OUT;  // 50,822
 constexpr double SG_XMAX = 30.0;
+static_assert(SURROGATE_FLOATS == SG_PARAMS + 2 * SG_OUT, "parameters then means and spreads");
 
 __host__ __device__ inline int sg_off_w(int l) { return l == 0 ? SG_OFF_W0 : l < 4 ? SG_OFF_W1 + (l - 1) * SG_LAYER_HH : SG_OFF_W4; }
 __host__ __device__ inline int sg_off_b(int l) {
@@ -413,6 +414,275 @@ __global__ void __launch_bounds__(256) k_sg_infer(int n, const float* __restrict
             const int r = s0 + g + (q >= 2 ? 8 : 0), c = 2 * tq + (q & 1);
             if (r < n && c < SG_OUT) out[(size_t)r * SG_OUT + c] = norm[c] + norm[SG_OUT + c] * (o[q] + b4[c]);
         }
+    }
+}
+
+// ---------------------------------------------------------------- the network inside the assembly
+// The packed weight image (global memory, copied whole into each persistent CTA's shared memory):
+// w0 [H][16] BF16 (k padded), w1..w3 [H][SG_LD] BF16, w4 [8][SG_LD] BF16 (rows 6, 7 zero), biases
+// FP32 [4 H + 8] (BF16-rounded values), output means and spreads FP32 [12].
+constexpr size_t SG_IMG_WH = (size_t)SG_H * 16 * 2;
+constexpr size_t SG_IMG_W4 = SG_IMG_WH + (size_t)3 * SG_H * SG_LD * 2;
+constexpr size_t SG_IMG_B = SG_IMG_W4 + (size_t)8 * SG_LD * 2;
+constexpr size_t SG_IMG_N = SG_IMG_B + (size_t)(4 * SG_H + 8) * 4;
+constexpr size_t SG_IMG_BYTES = (SG_IMG_N + 2 * SG_OUT * 4 + 15) / 16 * 16;
+static_assert(SG_IMG_B % 16 == 0, "biases at a 16-byte boundary");
+
+__global__ void k_sg_pack(const float* __restrict__ params, const float* __restrict__ norm, uint8_t* __restrict__ img) {
+    __nv_bfloat16* w0 = reinterpret_cast<__nv_bfloat16*>(img);
+    __nv_bfloat16* wh = reinterpret_cast<__nv_bfloat16*>(img + SG_IMG_WH);
+    __nv_bfloat16* w4 = reinterpret_cast<__nv_bfloat16*>(img + SG_IMG_W4);
+    float* bias = reinterpret_cast<float*>(img + SG_IMG_B);
+    float* nm = reinterpret_cast<float*>(img + SG_IMG_N);
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
+    for (int t = t0; t < SG_H * 16; t += st) {
+        const int j = t / 16, k = t % 16;
+        w0[t] = __float2bfloat16_rn(k < SG_IN ? params[SG_OFF_W0 + j * SG_IN + k] : 0.f);
+    }
+    for (int t = t0; t < 3 * SG_H * SG_LD; t += st) {
+        const int l = t / (SG_H * SG_LD), r = t % (SG_H * SG_LD), j = r / SG_LD, k = r % SG_LD;
+        wh[t] = __float2bfloat16_rn(k < SG_H ? params[sg_off_w(l + 1) + j * SG_H + k] : 0.f);
+    }
+    for (int t = t0; t < 8 * SG_LD; t += st) {
+        const int j = t / SG_LD, k = t % SG_LD;
+        w4[t] = __float2bfloat16_rn(j < SG_OUT && k < SG_H ? params[SG_OFF_W4 + j * SG_H + k] : 0.f);
+    }
+    for (int t = t0; t < 4 * SG_H + 8; t += st)
+        bias[t] = bf16r(t < 4 * SG_H ? params[sg_off_b(t / SG_H) + t % SG_H]
+                                     : (t - 4 * SG_H < SG_OUT ? params[SG_OFF_B4 + t - 4 * SG_H] : 0.f));
+    for (int t = t0; t < 2 * SG_OUT; t += st) nm[t] = norm[t];
+}
+
+// One forward pass for the 32 lanes of a warp (each lane's inputs u, v; w = 0), lanes 0-15 and
+// 16-31 as two m16 tiles of mma.sync m16n8k16 BF16; out6 = the de-standardized outputs of the
+// lane's own sample.  Every lane of the warp must call it.
+__device__ __forceinline__ void sg_warp_mlp(const uint8_t* img, float u, float v, float* out6) {
+    const uint32_t* w0u = reinterpret_cast<const uint32_t*>(img);
+    const uint32_t* whu = reinterpret_cast<const uint32_t*>(img + SG_IMG_WH);
+    const uint32_t* w4u = reinterpret_cast<const uint32_t*>(img + SG_IMG_W4);
+    const float* bias = reinterpret_cast<const float*>(img + SG_IMG_B);
+    const float* nm = reinterpret_cast<const float*>(img + SG_IMG_N);
+    const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+#pragma unroll 1
+    for (int mt = 0; mt < 2; mt++) {
+        const float u0 = __shfl_sync(0xffffffffu, u, mt * 16 + g), v0 = __shfl_sync(0xffffffffu, v, mt * 16 + g);
+        const float u1 = __shfl_sync(0xffffffffu, u, mt * 16 + g + 8), v1 = __shfl_sync(0xffffffffu, v, mt * 16 + g + 8);
+        uint32_t a[8][4];
+        {
+            const uint32_t a0[4] = {tq == 0 ? pack_bf16(u0, v0) : 0u, tq == 0 ? pack_bf16(u1, v1) : 0u, 0u, 0u};
+            float acc[16][4];
+#pragma unroll
+            for (int nt = 0; nt < 16; nt++) {
+                acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+                const int j = nt * 8 + g;
+                mma_bf16_16816(acc[nt], a0, w0u[(j * 16 + 2 * tq) / 2], w0u[(j * 16 + 2 * tq + 8) / 2]);
+            }
+#pragma unroll
+            for (int kt = 0; kt < 8; kt++) {
+                const int c0 = (2 * kt) * 8 + 2 * tq, c1 = (2 * kt + 1) * 8 + 2 * tq;
+                a[kt][0] = pack_bf16(silu(acc[2 * kt][0] + bias[c0]), silu(acc[2 * kt][1] + bias[c0 + 1]));
+                a[kt][1] = pack_bf16(silu(acc[2 * kt][2] + bias[c0]), silu(acc[2 * kt][3] + bias[c0 + 1]));
+                a[kt][2] = pack_bf16(silu(acc[2 * kt + 1][0] + bias[c1]), silu(acc[2 * kt + 1][1] + bias[c1 + 1]));
+                a[kt][3] = pack_bf16(silu(acc[2 * kt + 1][2] + bias[c1]), silu(acc[2 * kt + 1][3] + bias[c1 + 1]));
+            }
+        }
+#pragma unroll 1
+        for (int l = 0; l < 3; l++) {
+            const uint32_t* W = whu + (size_t)l * SG_H * SG_LD / 2;
+            float acc[16][4];
+#pragma unroll
+            for (int nt = 0; nt < 16; nt++) {
+                acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+                const int j = nt * 8 + g;
+#pragma unroll
+                for (int kt = 0; kt < 8; kt++)
+                    mma_bf16_16816(acc[nt], a[kt], W[(j * SG_LD + kt * 16 + 2 * tq) / 2],
+                                   W[(j * SG_LD + kt * 16 + 2 * tq + 8) / 2]);
+            }
+            const float* b = bias + (l + 1) * SG_H;
+#pragma unroll
+            for (int kt = 0; kt < 8; kt++) {
+                const int c0 = (2 * kt) * 8 + 2 * tq, c1 = (2 * kt + 1) * 8 + 2 * tq;
+                a[kt][0] = pack_bf16(silu(acc[2 * kt][0] + b[c0]), silu(acc[2 * kt][1] + b[c0 + 1]));
+                a[kt][1] = pack_bf16(silu(acc[2 * kt][2] + b[c0]), silu(acc[2 * kt][3] + b[c0 + 1]));
+                a[kt][2] = pack_bf16(silu(acc[2 * kt + 1][0] + b[c1]), silu(acc[2 * kt + 1][1] + b[c1 + 1]));
+                a[kt][3] = pack_bf16(silu(acc[2 * kt + 1][2] + b[c1]), silu(acc[2 * kt + 1][3] + b[c1 + 1]));
+            }
+        }
+        float o[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kt = 0; kt < 8; kt++)
+            mma_bf16_16816(o, a[kt], w4u[(g * SG_LD + kt * 16 + 2 * tq) / 2], w4u[(g * SG_LD + kt * 16 + 2 * tq + 8) / 2]);
+        // row r of the tile (lane mt * 16 + r) holds column c at lane 4 (r % 8) + c / 2, register
+        // (c % 2) + 2 (r / 8)
+        const int r = lane - mt * 16;
+#pragma unroll
+        for (int c = 0; c < SG_OUT; c++) {
+            const int src = 4 * (r & 7) + c / 2;
+            const float lo = __shfl_sync(0xffffffffu, o[c & 1], src & 31);
+            const float hi = __shfl_sync(0xffffffffu, o[2 + (c & 1)], src & 31);
+            if (r >= 0 && r < 16) out6[c] = nm[c] + nm[SG_OUT + c] * ((r < 8 ? lo : hi) + bias[4 * SG_H + c]);
+        }
+    }
+}
+
+// The wave term from the network's outputs: the logarithmic part in closed form (J0, J1 from the
+// 1-D table), the regular part and the imaginary part from the network, FY by the identity
+// FY = -F - 2 / R0.
+__device__ inline Wave sg_wave(double X, double Y, const float* o) {
+    double f[4];
+    table1d(X, f);
+    const double j0 = f[0], j1 = f[1], eY = exp(-Y), R0 = sqrt(X * X + Y * Y);
+    const double lg = log(Y + R0) + (GAMMA - LOG2);
+    Wave w;
+    w.F = -2.0 * eY * j0 * lg + (double)o[0];
+    w.FX = 2.0 * eY * j1 * lg - 2.0 * eY * j0 * X / (R0 * (Y + R0)) + (double)o[1];
+    w.FY = -w.F - 2.0 / R0;
+    w.I = o[3];
+    w.IX = o[4];
+    w.IY = o[5];
+    w.c = eY * j0;
+    return w;
+}
+
+// The mixed-form assembly with the network as the wave term inside its domain (X, Y < 30, R0 > 0;
+// the tables outside): persistent CTAs (the weight image is loaded once per CTA), work items
+// (tile pair, frequency) taken round-robin; the per-item work is k_assemble's.
+template <bool FINITE>
+__global__ void __launch_bounds__(256, 1) k_assemble_sg(PanelsView pv, const double* __restrict__ st,
+                                                       const FreqInfo* __restrict__ fi, const FdParams* __restrict__ fdp,
+                                                       const float* __restrict__ tiles, const double* __restrict__ fpt,
+                                                       OutF32 out, int F, const uint8_t* __restrict__ img_g,
+                                                       unsigned long long* __restrict__ counts) {
+    extern __shared__ __align__(16) uint8_t img[];
+    __shared__ double sT[4][32][33];
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(img_g);
+        uint4* dst = reinterpret_cast<uint4*>(img);
+        for (int t = threadIdx.y * 32 + threadIdx.x; t < (int)(SG_IMG_BYTES / 16); t += 256) dst[t] = src[t];
+    }
+    __syncthreads();
+    const int N = pv.N;
+    const int nt = (N + 31) / 32, ntp = nt * (nt + 1) / 2;
+    const size_t NN = (size_t)N * N;
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    unsigned long long used = 0;
+    for (int item = blockIdx.x; item < ntp * F; item += gridDim.x) {
+        const int f = item / ntp;
+        int idx = item % ntp, kb = 0;
+        while (idx >= nt - kb) {
+            idx -= nt - kb;
+            kb++;
+        }
+        const int nb = kb + idx;
+        const int K0 = kb * 32, N0 = nb * 32;
+        const FreqInfo info = fi[f];
+        const double K = info.K, logc = info.logc;
+        __syncthreads();  // sT of the previous item written out
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int n = N0 + tx, k = K0 + ty + 8 * i;
+            if (n < N && k < N)
+#pragma unroll
+                for (int q = 0; q < 4; q++) sT[q][ty + 8 * i][tx] = __ldg(st + q * NN + (size_t)n + (size_t)k * N);
+        }
+        __syncthreads();
+        const int k = K0 + tx;
+        const int kc = min(k, N - 1);
+        double xk[3], nk[3], ak;
+        for (int d = 0; d < 3; d++) {
+            xk[d] = pv.at(P_C + d, kc);
+            nk[d] = pv.at(P_N + d, kc);
+        }
+        ak = pv.at(P_AREA, kc);
+        const int kindk = pv.kind[kc];
+        const FdParams* fd = FINITE ? fdp + f : nullptr;
+        const float* T1 = FINITE ? tiles + (size_t)f * (T1_SIZE + T2_SIZE) : nullptr;
+        const float* T2 = FINITE ? T1 + T1_SIZE : nullptr;
+        const double* fp = FINITE ? fpt + (size_t)f * FP_PLANES * N : nullptr;
+#pragma unroll 1
+        for (int i = 0; i < 4; i++) {
+            const int nl = ty + 8 * i, n = N0 + nl;
+            const bool live = k < N && n < N && (kb != nb || k <= n);
+            const int ncl = min(n, N - 1);
+            double xn[3], nn3[3];
+            for (int d = 0; d < 3; d++) {
+                xn[d] = pv.at(P_C + d, ncl);
+                nn3[d] = pv.at(P_N + d, ncl);
+            }
+            const double an = pv.at(P_AREA, ncl);
+            const int kindn = pv.kind[ncl];
+            double dx = xk[0] - xn[0], dy = xk[1] - xn[1];
+            double R = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+            const double X = K * R, Y = -K * (xk[2] + xn[2]);
+            const bool inb = live && X < SG_XMAX && Y < SG_XMAX && (X > 0.0 || Y > 0.0);
+            float o6[SG_OUT] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            __syncwarp();
+            if (__any_sync(0xffffffffu, inb)) {
+                float in3[3];
+                sg_inputs(X, Y, in3);
+                sg_warp_mlp(img, in3[0], in3[1], o6);
+            }
+            if (!live) continue;
+            used += inb;
+            Kern w;
+            if (FINITE) {
+                if (inb) {
+                    const Wave sw = sg_wave(X, Y, o6);
+                    w = finite_kernel<true, float, true>(*fd, T1, T2, R, xk[2], xn[2], fp + k, fp + n, N, &sw);
+                } else {
+                    w = finite_kernel<true>(*fd, T1, T2, R, xk[2], xn[2], fp + k, fp + n, N);
+                }
+            } else {
+                w = inb ? wave_kern(K, sg_wave(X, Y, o6)) : pair_kernel_inf<true>(K, R, xk[2], xn[2]);
+            }
+            size_t o1 = (size_t)k + (size_t)n * N;
+            double2 s1, d1;
+            apply_kernel(__ldg(st + o1), __ldg(st + NN + o1), __ldg(st + 2 * NN + o1), __ldg(st + 3 * NN + o1), an,
+                         nn3[0], nn3[1], nn3[2], kindn, xk, xn, K, logc, w, R, false, s1, d1);
+            out.put(f, k, n, s1, make_double2((k == n ? free_term(kindk) : 0.0) - d1.x, -d1.y));
+            if (n != k) {
+                double2 s2, d2;
+                apply_kernel(sT[0][tx][nl], sT[1][tx][nl], sT[2][tx][nl], sT[3][tx][nl], ak, nk[0], nk[1], nk[2],
+                             kindk, xn, xk, K, logc, w, R, true, s2, d2);
+                sT[0][tx][nl] = s2.x;
+                sT[1][tx][nl] = s2.y;
+                sT[2][tx][nl] = -d2.x;
+                sT[3][tx][nl] = -d2.y;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int n = N0 + tx, kl = ty + 8 * i, kk = K0 + kl;
+            if (n < N && kk < N && (kb != nb || n > kk))
+                out.put(f, n, kk, make_double2(sT[0][kl][tx], sT[1][kl][tx]), make_double2(sT[2][kl][tx], sT[3][kl][tx]));
+        }
+    }
+    // pairs whose wave term came from the network
+    for (int o = 16; o > 0; o >>= 1) used += __shfl_xor_sync(0xffffffffu, used, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(counts, used);
+}
+
+void launch_sg_pack(const float* params_norm, uint8_t* img, cudaStream_t s) {
+    k_sg_pack<<<64, 256, 0, s>>>(params_norm, params_norm + SG_PARAMS, img);
+}
+
+size_t sg_image_bytes() { return SG_IMG_BYTES; }
+
+void launch_assemble_f32_sg(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
+                            const float* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
+                            const uint8_t* img, unsigned long long* counts, cudaStream_t s) {
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    OutF32 o{S, A, 2 * (size_t)Np * Np, Np};
+    if (finite) {
+        cudaFuncSetAttribute(k_assemble_sg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG_IMG_BYTES);
+        k_assemble_sg<true><<<nsm, dim3(32, 8), SG_IMG_BYTES, s>>>(pv, st, fi, fd, tiles, fpt, o, F, img, counts);
+    } else {
+        cudaFuncSetAttribute(k_assemble_sg<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG_IMG_BYTES);
+        k_assemble_sg<false><<<nsm, dim3(32, 8), SG_IMG_BYTES, s>>>(pv, st, fi, fd, tiles, fpt, o, F, img, counts);
     }
 }
 

@@ -44,7 +44,8 @@ class HbgProblem(ctypes.Structure):
 class HbgOptions(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("logarithmic", ctypes.c_int32), ("log_tolerance", ctypes.c_double),
                 ("gravity", ctypes.c_double), ("density", ctypes.c_double), ("depth", ctypes.c_double),
-                ("max_batch", ctypes.c_int32), ("device", ctypes.c_int32), ("cancel", ip)]
+                ("max_batch", ctypes.c_int32), ("device", ctypes.c_int32), ("cancel", ip),
+                ("surrogate", ctypes.POINTER(ctypes.c_float))]
 
 
 class HbLocation(ctypes.Structure):
@@ -64,7 +65,7 @@ EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_
            "hb_object", "hb_add", "hb_set_bool", "hb_set_int", "hb_set_real", "hb_set_text", "hb_set_reals",
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
            "hbg_statics_noalloc", "hbg_measure_peaks", "hbg_last_ir_history", "hbg_surrogate_train",
-           "hbg_surrogate_grad", "hbg_surrogate_eval"]
+           "hbg_surrogate_grad", "hbg_surrogate_eval", "hbg_last_surrogate_pairs"]
 
 _lib = None
 
@@ -102,6 +103,7 @@ def lib():
                                       ctypes.c_uint64, ctypes.c_int64, fp, fp, dp]
     L.hbg_surrogate_grad.argtypes = [fp, ctypes.c_int32, fp, fp, fp, dp]
     L.hbg_surrogate_eval.argtypes = [fp, fp, ctypes.c_int32, dp, dp, dp, dp]
+    L.hbg_last_surrogate_pairs.argtypes = [ctypes.POINTER(ctypes.c_int64)]
     L.hbg_statics_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
                                       ctypes.c_int32, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
     L.hbg_statics_noalloc.restype = ctypes.c_int32
@@ -131,6 +133,11 @@ def default_options(**kw) -> HbgOptions:
     for k, v in kw.items():
         if k == "depth" and (v is None or not np.isfinite(v)):
             v = float("inf")
+        if k == "surrogate":
+            if v is None:
+                continue
+            o._surrogate_keep = np.ascontiguousarray(v, np.float32)  # alive as long as the options
+            v = o._surrogate_keep.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
         setattr(o, k, v)
     return o
 
@@ -315,6 +322,18 @@ def surrogate_eval(params, norm, xy):
     check(lib().hbg_surrogate_eval(p.ctypes.data_as(fpp), nm.ctypes.data_as(fpp), n, x.ctypes.data_as(dp),
                                    on.ctypes.data_as(dp), ot.ctypes.data_as(dp), ms.ctypes.data_as(dp)))
     return on, ot, (float(ms[0]), float(ms[1]))
+
+
+def last_surrogate_pairs() -> int:
+    """Pairs whose wave term came from the network in the last mixed solve with a surrogate."""
+    n = ctypes.c_int64()
+    check(lib().hbg_last_surrogate_pairs(ctypes.byref(n)))
+    return n.value
+
+
+def surrogate_blob(params, norm):
+    """The HbgOptions.surrogate array: parameters then the outputs' means and spreads (float32)."""
+    return np.ascontiguousarray(np.concatenate([np.asarray(params, np.float32), np.asarray(norm, np.float32)]))
 
 
 def last_ir_iterations() -> int:

@@ -50,7 +50,7 @@ typedef int32_t HbStatus;
 #define HB_C128 7
 
 /* The version of this library's ABI (its own numbering; the reference's hb_abi_version is 8). */
-#define HBG_ABI_VERSION 1
+#define HBG_ABI_VERSION 2
 
 /* ==================================================================== batched entry */
 
@@ -101,6 +101,9 @@ typedef struct HbgOptions {
     int32_t max_batch;            /* frequencies per device batch; 0: from free memory */
     int32_t device;               /* CUDA device ordinal */
     const volatile int32_t *cancel; /* optional: nonzero cancels between batches (HB_ERR_CANCELLED) */
+    const float *surrogate;       /* optional, mixed form only: a trained wave-term network (50822
+                                   * parameters then 12 output means/spreads, as hbg_surrogate_train
+                                   * returns them) used in the assembly inside its domain; NULL: tables */
 } HbgOptions;
 
 /* Defaults of the reference's schema (document_schema.rs:202-232). */
@@ -180,6 +183,10 @@ HbStatus hbg_surrogate_grad(const float *params, int32_t n, const float *inputs,
  * the n points (points resident on the device). */
 HbStatus hbg_surrogate_eval(const float *params, const float *norm, int32_t n, const double *xy, double *out_net,
                             double *out_table, double *ms2);
+
+/* Pairs (unordered, summed over frequencies) whose wave term came from the network in the last
+ * mixed solve of this thread with HbgOptions.surrogate set (0 otherwise). */
+HbStatus hbg_last_surrogate_pairs(int64_t *n);
 
 /* Refinement iterations of the last mixed-precision frequency batch of this thread. */
 HbStatus hbg_last_ir_iterations(int32_t *n);

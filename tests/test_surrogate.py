@@ -4,9 +4,12 @@ gains, or loses, against the table evaluation it would replace (device time per 
 
 from __future__ import annotations
 
+import math
+
 import numpy as np
 import pytest
 
+from hydrobem_b200 import meshes
 from hydrobem_b200 import native as nv
 
 pytestmark = pytest.mark.gpu
@@ -127,3 +130,36 @@ def test_points_outside_the_trained_domain_are_refused(trained):
     p, nm, _ = trained
     with pytest.raises(nv.HydroBEMError):
         nv.surrogate_eval(p, nm, np.array([[31.0, 1.0]]))
+
+
+def _scaled_error(got, ref, floor=1e-3):
+    ref = np.asarray(ref)
+    scale = np.maximum(np.abs(ref).max(axis=0, keepdims=True), floor * np.abs(ref).max())
+    return float((np.abs(np.asarray(got) - ref) / scale).max())
+
+
+@pytest.mark.parametrize("depth", [math.inf, 3.0])
+def test_network_as_the_wave_term_of_the_mixed_assembly(trained, depth):
+    """The mixed solve with the network inside the assembly: it serves the pairs of its domain, the
+    solve stays finite, and A, B, X move from the table solve by the network's own error, far above
+    the 1e-5 of the solve -- which is why the tables stay the default."""
+    p, nm, _ = trained
+    v = meshes.cylinder(1.0, 0.5, 32, 8, 8)
+    omegas = 2.0 * math.pi / np.array([2.0, 4.0, 8.0])
+    ref = nv.solve(v, omegas, [0.0], depth=depth, precision=nv.HBG_MIXED)
+    assert nv.last_surrogate_pairs() == 0
+    got = nv.solve(v, omegas, [0.0], depth=depth, precision=nv.HBG_MIXED, surrogate=nv.surrogate_blob(p, nm))
+    used = nv.last_surrogate_pairs()
+    N = len(v)
+    assert 0 < used <= len(omegas) * N * (N + 1) // 2
+    errs = {k: _scaled_error(got[k], ref[k]) for k in ("A", "B", "X")}
+    assert all(np.isfinite(got[k]).all() for k in ("A", "B", "X"))
+    assert max(errs.values()) < 1.0, errs
+    print(f"\nnetwork in the assembly (depth {depth}): {used} pairs; error vs the table solve {errs}")
+
+
+def test_network_refused_in_the_fp64_form(trained):
+    p, nm, _ = trained
+    v = meshes.cylinder(1.0, 0.5, 16, 4, 4)
+    with pytest.raises(nv.HydroBEMError):
+        nv.solve(v, [1.0], [0.0], precision=nv.HBG_FP64, surrogate=nv.surrogate_blob(p, nm))
