@@ -207,6 +207,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     const int dsmem = (int)df_smem_bytes();
     cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, dsmem);
+    cudaFuncSetAttribute(k_tri_step<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(8));
+    cudaFuncSetAttribute(k_tri_step<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(10));
     cudaFuncSetAttribute(k_tri_step<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(12));
     cudaFuncSetAttribute(k_tri_step<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(16));
     std::vector<double> heads(std::max(H, 1));

@@ -755,6 +755,28 @@ __global__ void k_gemv_reduce(int N, int nrhs, int F, int nz, const double2* __r
 constexpr int TB = 128;
 constexpr int TRI_THREADS = 256;
 
+// Packed FP32 pairs (fma.rn.f32x2: two FP32 FMAs per instruction).  A complex multiply-add
+// acc += m v is two packed FMAs: acc += (m.re, m.re) (v.re, v.im), then acc += (-m.im, m.im) (v.im, v.re);
+// the right-hand sides are kept in shared memory as {re, im, im, re} so one 16-byte load gives both
+// orders.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2pack(float a, float b) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 f2unpack(f32x2 r) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ f32x2 ffma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ float4 dup_swap(float2 v) { return make_float4(v.x, v.y, v.y, v.x); }
+
 // The diagonal block of U^T (upper_t) or L^T, solved by its stored inverse: y_b = D^T r_b with
 // D = U_bb^-1 (upper part of the stored block, with the diagonal) or L_bb^-1 (lower part, unit
 // diagonal).  Rows b0..b0+TB of X in place, right-hand sides in chunks of NR.  Thread t < TB owns
@@ -762,20 +784,20 @@ constexpr int TRI_THREADS = 256;
 // half; each loads the 16 entries of a chunk before using them (one memory latency per chunk).
 template <int NR>
 __device__ __forceinline__ void tri_diag_f32(const float2* __restrict__ D, float2* X, int Np, int nrhs, int b0,
-                                             bool upper_t, float2 (*rs)[NR], float2 (*pt)[NR]) {
+                                             bool upper_t, float4 (*rs)[NR], float2 (*pt)[NR]) {
     const int i = threadIdx.x % TB, half = threadIdx.x / TB;
     for (int c0 = 0; c0 < nrhs; c0 += NR) {
         const int nc = min(NR, nrhs - c0);
         __syncthreads();
         for (int t = threadIdx.x; t < TB * NR; t += blockDim.x) {
             const int p = t % TB, c = t / TB;
-            rs[p][c] = c < nc ? X[(size_t)(c0 + c) * Np + b0 + p] : make_float2(0.f, 0.f);
+            rs[p][c] = dup_swap(c < nc ? X[(size_t)(c0 + c) * Np + b0 + p] : make_float2(0.f, 0.f));
         }
         __syncthreads();
-        float2 acc[NR];
+        f32x2 acc[NR];
 #pragma unroll
         for (int c = 0; c < NR; c++)  // the unit diagonal of L^-1
-            acc[c] = (!upper_t && half == (i >= TB / 2 ? 1 : 0)) ? rs[i][c] : make_float2(0.f, 0.f);
+            acc[c] = (!upper_t && half == (i >= TB / 2 ? 1 : 0)) ? f2pack(rs[i][c].x, rs[i][c].y) : f2pack(0.f, 0.f);
         const int pb = half * (TB / 2);
 #pragma unroll 1
         for (int pc = 0; pc < TB / 2; pc += 16) {
@@ -786,25 +808,26 @@ __device__ __forceinline__ void tri_diag_f32(const float2* __restrict__ D, float
             for (int q = 0; q < 16; q++) {
                 const int p = pb + pc + q;
                 if (upper_t ? p <= i : p > i) {
+                    const f32x2 m = f2pack(dv[q].x, dv[q].x), mn = f2pack(-dv[q].y, dv[q].y);
 #pragma unroll
                     for (int c = 0; c < NR; c++) {
-                        const float2 v = rs[p][c];
-                        acc[c].x += dv[q].x * v.x - dv[q].y * v.y;
-                        acc[c].y += dv[q].x * v.y + dv[q].y * v.x;
+                        const float4 v = rs[p][c];
+                        acc[c] = ffma2(m, f2pack(v.x, v.y), acc[c]);
+                        acc[c] = ffma2(mn, f2pack(v.z, v.w), acc[c]);
                     }
                 }
             }
         }
         if (half == 1)
 #pragma unroll
-            for (int c = 0; c < NR; c++) pt[i][c] = acc[c];
+            for (int c = 0; c < NR; c++) pt[i][c] = f2unpack(acc[c]);
         __syncthreads();
         if (half == 0)
 #pragma unroll
             for (int c = 0; c < NR; c++)
                 if (c < nc) {
-                    const float2 q2 = pt[i][c];
-                    X[(size_t)(c0 + c) * Np + b0 + i] = make_float2(acc[c].x + q2.x, acc[c].y + q2.y);
+                    const float2 q2 = pt[i][c], a = f2unpack(acc[c]);
+                    X[(size_t)(c0 + c) * Np + b0 + i] = make_float2(a.x + q2.x, a.y + q2.y);
                 }
     }
 }
@@ -818,9 +841,9 @@ template <int NR>
 __global__ void __launch_bounds__(TRI_THREADS, 2) k_tri_step(int Np, size_t bstride, const float* __restrict__ W,
                                                           const float2* __restrict__ DINV, int nrhs,
                                                           float2* __restrict__ Xall, int step, int upper_t) {
-    extern __shared__ float2 tri_smem[];  // ys [TB][NR], partial sums [3][TB][NR]
-    float2(*ys)[NR] = reinterpret_cast<float2(*)[NR]>(tri_smem);
-    float2(*pt)[NR] = reinterpret_cast<float2(*)[NR]>(tri_smem + TB * NR);
+    extern __shared__ float4 tri_smem4[];  // ys [TB][NR] as {re, im, im, re}, partial sums [3][TB][NR]
+    float4(*ys)[NR] = reinterpret_cast<float4(*)[NR]>(tri_smem4);
+    float2(*pt)[NR] = reinterpret_cast<float2(*)[NR]>(tri_smem4 + TB * NR);
     const int f = blockIdx.y;
     const float* Mr = W + (size_t)f * bstride;
     const float* Mi = Mr + (size_t)Np * Np;
@@ -845,12 +868,12 @@ __global__ void __launch_bounds__(TRI_THREADS, 2) k_tri_step(int Np, size_t bstr
         __syncthreads();
         for (int t = threadIdx.x; t < TB * NR; t += blockDim.x) {
             const int p = t % TB, c = t / TB;
-            ys[p][c] = c < nc ? X[(size_t)(c0 + c) * Np + s0 + p] : make_float2(0.f, 0.f);
+            ys[p][c] = dup_swap(c < nc ? X[(size_t)(c0 + c) * Np + s0 + p] : make_float2(0.f, 0.f));
         }
         __syncthreads();
-        float2 a0[NR], a1[NR];
+        f32x2 a0[NR], a1[NR];
 #pragma unroll
-        for (int c = 0; c < NR; c++) a0[c] = a1[c] = make_float2(0.f, 0.f);
+        for (int c = 0; c < NR; c++) a0[c] = a1[c] = f2pack(0.f, 0.f);
 #pragma unroll 1
         for (int pc = 0; pc < 32; pc += 16) {
             float r0v[16], i0v[16], r1v[16], i1v[16];
@@ -864,28 +887,31 @@ __global__ void __launch_bounds__(TRI_THREADS, 2) k_tri_step(int Np, size_t bstr
             }
 #pragma unroll
             for (int q = 0; q < 16; q++) {
+                const f32x2 m0 = f2pack(r0v[q], r0v[q]), n0 = f2pack(-i0v[q], i0v[q]);
+                const f32x2 m1 = f2pack(r1v[q], r1v[q]), n1 = f2pack(-i1v[q], i1v[q]);
 #pragma unroll
                 for (int c = 0; c < NR; c++) {
-                    const float2 v = ys[pq * 32 + pc + q][c];
-                    a0[c].x += r0v[q] * v.x - i0v[q] * v.y;
-                    a0[c].y += r0v[q] * v.y + i0v[q] * v.x;
-                    a1[c].x += r1v[q] * v.x - i1v[q] * v.y;
-                    a1[c].y += r1v[q] * v.y + i1v[q] * v.x;
+                    const float4 v4 = ys[pq * 32 + pc + q][c];
+                    const f32x2 v = f2pack(v4.x, v4.y), vs = f2pack(v4.z, v4.w);
+                    a0[c] = ffma2(m0, v, a0[c]);
+                    a0[c] = ffma2(n0, vs, a0[c]);
+                    a1[c] = ffma2(m1, v, a1[c]);
+                    a1[c] = ffma2(n1, vs, a1[c]);
                 }
             }
         }
         if (pq > 0)
 #pragma unroll
             for (int c = 0; c < NR; c++) {
-                pt[(pq - 1) * TB + li][c] = a0[c];
-                pt[(pq - 1) * TB + li + 64][c] = a1[c];
+                pt[(pq - 1) * TB + li][c] = f2unpack(a0[c]);
+                pt[(pq - 1) * TB + li + 64][c] = f2unpack(a1[c]);
             }
         __syncthreads();
         if (pq == 0)
 #pragma unroll
             for (int c = 0; c < NR; c++)
                 if (c < nc) {
-                    float2 s0v = a0[c], s1v = a1[c];
+                    float2 s0v = f2unpack(a0[c]), s1v = f2unpack(a1[c]);
 #pragma unroll
                     for (int h = 0; h < 3; h++) {
                         const float2 q0 = pt[h * TB + li][c], q1 = pt[h * TB + li + 64][c];
@@ -903,7 +929,7 @@ __global__ void __launch_bounds__(TRI_THREADS, 2) k_tri_step(int Np, size_t bstr
     if (blockIdx.x == 0) tri_diag_f32<NR>(Df + (size_t)cb * TB * TB, X, Np, nrhs, r0, upper_t, ys, pt);
 }
 
-constexpr size_t tri_smem_bytes(int nr) { return (size_t)4 * TB * nr * sizeof(float2); }
+constexpr size_t tri_smem_bytes(int nr) { return (size_t)TB * nr * (sizeof(float4) + 3 * sizeof(float2)); }
 
 // FP64 vectors to complex64 (the right-hand sides entering the first correction).
 __global__ void k_to_c64(size_t n, const double2* __restrict__ a, float2* __restrict__ b) {
