@@ -609,12 +609,14 @@ __global__ void __launch_bounds__(128) k_cgemv_part(int N, int Np, size_t bstrid
             if (c < nrhs) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
 }
 
-// The same partial products with the matrix and vector tiles streamed by TMA: CTA of 128 rows k
-// (one thread each) over a chunk of columns n, 16 columns per stage (both FP32 planes, 16 KB, and
-// the 16 complex entries of every right-hand side), GV_STAGES stages in flight from a producer
-// warp, so the bytes in flight do not depend on registers; FP64 accumulation as above.
-constexpr int GV_ROWS = 128, GV_COLS = 16, GV_STAGES = 3, GV_CHUNK = 1024;
-constexpr int GV_THREADS = GV_ROWS + 32;
+// The same partial products with the matrix and vector tiles streamed by TMA: CTA of 256 rows k
+// (two a thread: t and t + 128, so each vector entry read from shared memory feeds both) over a
+// chunk of columns n, 16 columns per stage (both FP32 planes, 32 KB, and the 16 complex entries of
+// every right-hand side), GV_STAGES stages in flight from a producer warp, so the bytes in flight do
+// not depend on registers; FP64 accumulation as above.
+constexpr int GV_ROWS = 256, GV_COLS = 16, GV_STAGES = 3, GV_CHUNK = 1024;
+constexpr int GV_WORKERS = GV_ROWS / 2;
+constexpr int GV_THREADS = GV_WORKERS + 32;
 template <int NR>
 __host__ __device__ constexpr size_t gv_tx_bytes() {  // bytes one stage receives
     return (size_t)2 * GV_COLS * GV_ROWS * 4 + (size_t)NR * GV_COLS * 16;
@@ -645,12 +647,12 @@ __global__ void __launch_bounds__(GV_THREADS) k_cgemv_tma(const __grid_constant_
     if (threadIdx.x == 0) {
         for (int s = 0; s < GV_STAGES; s++) {
             tc::mbar_init(&full[s], 1);
-            tc::mbar_init(&empty[s], GV_ROWS / 32);
+            tc::mbar_init(&empty[s], GV_WORKERS / 32);
         }
         tc::fence_barrier_init();
     }
     __syncthreads();
-    if (warp == GV_ROWS / 32) {
+    if (warp == GV_WORKERS / 32) {
         if (lane == 0) {
             tc::prefetch_tensormap(&mapM);
             tc::prefetch_tensormap(&mapX);
@@ -670,9 +672,9 @@ __global__ void __launch_bounds__(GV_THREADS) k_cgemv_tma(const __grid_constant_
         }
         return;
     }
-    double2 acc[NR];
+    double2 acc[NR], acd[NR];  // rows k0 + t and k0 + t + GV_WORKERS
 #pragma unroll
-    for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
+    for (int c = 0; c < NR; c++) acc[c] = acd[c] = make_double2(0.0, 0.0);
     const int t = threadIdx.x;
     for (int si = 0; si < nst; si++) {
         const int s = si % GV_STAGES;
@@ -684,37 +686,31 @@ __global__ void __launch_bounds__(GV_THREADS) k_cgemv_tma(const __grid_constant_
         const float* sMr = reinterpret_cast<const float*>(st);
         const float* sMi = sMr + GV_COLS * GV_ROWS;
         const double2* sx = reinterpret_cast<const double2*>(st + 2 * GV_COLS * GV_ROWS * 4);  // [NR][GV_COLS]
+        // columns beyond N are never read (the padding may hold anything)
         const int lim = min(GV_COLS, nend - (nbeg + si * GV_COLS));
-        if (lim == GV_COLS) {
-#pragma unroll 4
-            for (int j = 0; j < GV_COLS; j++) {
-                const double mr = sMr[j * GV_ROWS + t], mi = sMi[j * GV_ROWS + t];
+#pragma unroll 2
+        for (int j = 0; j < lim; j++) {
+            const double mr = sMr[j * GV_ROWS + t], mi = sMi[j * GV_ROWS + t];
+            const double nr = sMr[j * GV_ROWS + t + GV_WORKERS], ni = sMi[j * GV_ROWS + t + GV_WORKERS];
 #pragma unroll
-                for (int c = 0; c < NR; c++) {
-                    const double2 v = sx[c * GV_COLS + j];
-                    acc[c].x += mr * v.x - mi * v.y;
-                    acc[c].y += mr * v.y + mi * v.x;
-                }
-            }
-        } else {
-            for (int j = 0; j < lim; j++) {  // columns beyond N are never read (padding may hold anything)
-                const double mr = sMr[j * GV_ROWS + t], mi = sMi[j * GV_ROWS + t];
-#pragma unroll
-                for (int c = 0; c < NR; c++) {
-                    const double2 v = sx[c * GV_COLS + j];
-                    acc[c].x += mr * v.x - mi * v.y;
-                    acc[c].y += mr * v.y + mi * v.x;
-                }
+            for (int c = 0; c < NR; c++) {
+                const double2 v = sx[c * GV_COLS + j];
+                acc[c].x += mr * v.x - mi * v.y;
+                acc[c].y += mr * v.y + mi * v.x;
+                acd[c].x += nr * v.x - ni * v.y;
+                acd[c].y += nr * v.y + ni * v.x;
             }
         }
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&empty[s]);
     }
-    const int k = k0 + t;
-    if (k < N)
+    const int k = k0 + t, kd = k + GV_WORKERS;
 #pragma unroll
-        for (int c = 0; c < NR; c++)
-            if (c < nrhs) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
+    for (int c = 0; c < NR; c++)
+        if (c < nrhs) {
+            if (k < N) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
+            if (kd < N) part[(((size_t)z * F + f) * nrhs + c) * N + kd] = acd[c];
+        }
 }
 
 template <class T>
