@@ -576,7 +576,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
 // (K-major), or C -= A B^T, on the tcgen05 TF32 path of the mixed LU.  M, N, K multiples of 128,
 // 128, 32.
 int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* C, bool subtract, const char** msg) {
-    if (M % GBM || N % GBN || K % GBK || M <= 0 || N <= 0 || K <= 0) {
+    if (M % GBM || N % 128 || K % GBK || M <= 0 || N <= 0 || K <= 0) {
         *msg = "debug GEMM shape: M % 128, N % 128, K % 32";
         return HB_ERR_VALUE;
     }
@@ -619,7 +619,7 @@ int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     // fewer CTAs than tiles, so that the persistent loop and both accumulator buffers are exercised
-    const int tiles = (M / GBM) * (N / GBN);
+    const int tiles = (M / GBM) * ((N + GBN - 1) / GBN);
     k_gemm_tf32<<<std::max(1, std::min(tiles / 3, n_sm)), GEMM_THREADS, smem>>>(mA, mB, mC, g);
     int herr = 0;
     cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost);

@@ -19,7 +19,8 @@
 namespace hbg {
 
 constexpr int NBL = 128;  // LU block width (complex columns)
-constexpr int GBM = 128, GBK = 32, GSTAGES = 3, GBN = 128;
+constexpr int GBM = 128, GBK = 32, GSTAGES = 3, GBN = 256;
+constexpr int GNBOX = 4;  // ring of 32-column output boxes in shared memory
 
 struct GemmArgs {
     int M, Nc, Kp;         // rows, real output columns, real inner dimension
@@ -42,16 +43,16 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
 
 constexpr int GEMM_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2..5 epilogue
 constexpr size_t GEMM_STAGE_BYTES = (size_t)(GBM + GBN) * GBK * 4;
-constexpr size_t GEMM_C_BYTES = (size_t)GBM * GBN * 4;  // the output tile, four 32-column boxes
-constexpr size_t gemm_smem_bytes() { return 1024 + GSTAGES * GEMM_STAGE_BYTES + 2 * GEMM_C_BYTES + 256; }
+constexpr size_t GEMM_BOX_BYTES = (size_t)GBM * 32 * 4;  // one 32-column box of the output tile
+constexpr size_t gemm_smem_bytes() { return 1024 + GSTAGES * GEMM_STAGE_BYTES + GNBOX * GEMM_BOX_BYTES + 256; }
 
-// Persistent, warp-specialized TF32 GEMM of the mixed LU: tiles of 128 x 128 (real columns) taken
+// Persistent, warp-specialized TF32 GEMM of the mixed LU: tiles of 128 x 256 (real columns) taken
 // round-robin over (row tile, column tile, matrix).  Warp 0 lane 0 streams the A/B k-chunks through a
-// 4-stage TMA ring and prefetches the tile's C block (mode 2) into shared memory; warp 1 lane 0
-// issues tcgen05.mma into one of two TMEM accumulators; warps 2..5 read the accumulator
-// (tcgen05.ld), combine it with the C block in shared memory, and write the tile back with TMA
-// stores -- so the epilogue of a tile overlaps the main loop of the next.  C / D tiles live in
-// shared memory in the 128-byte swizzle of four 32-column boxes (conflict-free 16-byte accesses).
+// 3-stage TMA ring; warp 1 lane 0 issues tcgen05.mma (M 128, N 256) into one of two TMEM
+// accumulators; warps 2..5 read the accumulator (tcgen05.ld) in 32-column chunks, place each chunk in
+// a ring of four shared-memory boxes (128-byte swizzle, conflict-free 16-byte accesses) and write it
+// out by TMA: a store, or for the trailing update a TMA reduction that adds -acc to C in L2 (so C
+// never passes through the SM).  The epilogue of one tile overlaps the main loop of the next.
 __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_constant__ CUtensorMap mapA,
                                                                const __grid_constant__ CUtensorMap mapB,
                                                                const __grid_constant__ CUtensorMap mapC,
@@ -60,14 +61,12 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
     uint8_t* base = align1024(smem_raw);
     float* sA = reinterpret_cast<float*>(base);
     float* sB = sA + GSTAGES * GBM * GBK;
-    float* sCb = sB + GSTAGES * GBN * GBK;  // two output-tile buffers, each [4 boxes][128 rows][32]
-    uint64_t* full = reinterpret_cast<uint64_t*>(sCb + 2 * GBM * GBN);
+    float* sBox = sB + GSTAGES * GBN * GBK;  // [GNBOX][128 rows][32]
+    uint64_t* full = reinterpret_cast<uint64_t*>(sBox + GNBOX * GBM * 32);
     uint64_t* empty = full + GSTAGES;
     uint64_t* tfull = empty + GSTAGES;  // [2]
     uint64_t* tempty = tfull + 2;       // [2]
-    uint64_t* cfull = tempty + 2;   // [2]
-    uint64_t* cempty = cfull + 2;  // [2]
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(cempty + 2);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 2);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = (g.M + GBM - 1) / GBM, nt = (g.Nc + GBN - 1) / GBN;
     const int ntiles = mt * nt * g.batch;
@@ -80,10 +79,6 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
         for (int b = 0; b < 2; b++) {
             tc::mbar_init(&tfull[b], 1);
             tc::mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
-        }
-        for (int b = 0; b < 2; b++) {
-            tc::mbar_init(&cfull[b], 1);
-            tc::mbar_init(&cempty[b], 1);
         }
         tc::fence_barrier_init();
         tc::prefetch_tensormap(&mapA);
@@ -103,25 +98,11 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
     };
     if (warp == 0) {
         if (lane == 0) {
-            int kc_global = 0, it = 0;
+            int kc_global = 0;
             bool bad = false;
-            for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x, it++) {
+            for (int t = blockIdx.x; t < ntiles && !bad; t += gridDim.x) {
                 int m0, n0, f;
                 tile_coords(t, m0, n0, f);
-                if (g.mode == 2) {
-                    // the C block of this tile into buffer it % 2, once the store of tile it - 2 has read it
-                    const int cb = it & 1;
-                    if (it >= 2 && !tc::mbar_wait(&cempty[cb], ((it >> 1) - 1) & 1)) {
-                        atomicExch(g.err, 4);
-                        break;
-                    }
-                    const int plane = n0 >= g.o_nc ? 1 : 0, col0 = n0 - plane * g.o_nc;
-                    float* sC = sCb + cb * GBM * GBN;
-                    tc::mbar_arrive_expect_tx(&cfull[cb], (uint32_t)GEMM_C_BYTES);
-                    for (int q = 0; q < GBN / 32; q++)
-                        tc::tma_load_4d(sC + q * GBM * 32, &mapC, &cfull[cb], g.o_col0 + col0 + 32 * q, g.o_row0 + m0,
-                                        plane, f);
-                }
                 for (int kc = 0; kc < nk; kc++, kc_global++) {
                     const int s = kc_global % GSTAGES;
                     if (kc_global >= GSTAGES && !tc::mbar_wait(&empty[s], ((kc_global / GSTAGES) - 1) & 1)) {
@@ -178,53 +159,47 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
             }
         }
     } else {
-        // epilogue warps 2..5: TMEM lane quadrant (warp % 4), rows 32 (warp % 4) .. + 32 of the tile
+        // epilogue warps 2..5: TMEM lane quadrant (warp % 4), rows 32 (warp % 4) .. + 32 of the tile;
+        // thread 64 (warp 2, lane 0) issues the box writes and tracks their bulk groups
         const int quad = warp & 3;
         const int r = quad * 32 + lane;  // row within the tile
-        int it = 0;
+        const bool issuer = threadIdx.x == 64;
+        int it = 0, bx = 0;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
             int m0, n0, f;
             tile_coords(t, m0, n0, f);
             const int b = it & 1;
-            bool ok = tc::mbar_wait(&tfull[b], (it >> 1) & 1);
-            float* sC = sCb + b * GBM * GBN;  // output buffer it % 2
-            if (ok && g.mode == 2) ok = tc::mbar_wait(&cfull[b], (it >> 1) & 1);
-            if (ok && g.mode != 2 && it >= 2) ok = tc::mbar_wait(&cempty[b], ((it >> 1) - 1) & 1);  // buffer free
+            const bool ok = tc::mbar_wait(&tfull[b], (it >> 1) & 1);
             // one decision for the four epilogue warps, so none waits at a barrier the others left
             __syncwarp();
             if (!tc::bar_and(ok, 1, 128)) {
-                if (threadIdx.x == 64) atomicExch(g.err, 3);
+                if (issuer) atomicExch(g.err, 3);
                 break;
             }
             tc::tc_fence_after();
-            const int plane = n0 >= g.o_nc ? 1 : 0, col0 = n0 - plane * g.o_nc;
-            for (int q = 0; q < GBN / 32; q++) {
+            for (int q = 0; q < GBN / 32; q++, bx++) {
                 float v[32];
                 tc::tmem_ld32(tmem + b * GBN + ((uint32_t)(quad * 32) << 16) + q * 32, v);
-                float* row = sC + q * GBM * 32 + r * 32;  // 128 B, 16-byte chunks swizzled by r % 8
+                const int jg = n0 + 32 * q;  // real output column of the chunk
+                const bool live = jg < g.Nc;
+                const int plane = jg >= g.o_nc ? 1 : 0, col = jg - plane * g.o_nc;
+                // the box slot is free once the write issued GNBOX boxes ago has read it
+                if (issuer && bx >= GNBOX) tc::bulk_wait_read_n<GNBOX - 1>();
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+                float* row = sBox + (bx % GNBOX) * GBM * 32 + r * 32;  // 128 B, 16-byte chunks swizzled by r % 8
+                const float sg = g.mode == 2 ? -1.f : 1.f;  // the trailing update adds -acc to C
 #pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    float4* c4 = reinterpret_cast<float4*>(row + 4 * (j ^ (r & 7)));
-                    float4 o;
-                    if (g.mode == 2) {
-                        o = *c4;
-                        o.x -= v[4 * j];
-                        o.y -= v[4 * j + 1];
-                        o.z -= v[4 * j + 2];
-                        o.w -= v[4 * j + 3];
-                    } else {
-                        o = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
-                    }
-                    *c4 = o;
-                }
-                if (g.mode == 1 && m0 + r < g.M) {
+                for (int j = 0; j < 8; j++)
+                    *reinterpret_cast<float4*>(row + 4 * (j ^ (r & 7))) =
+                        make_float4(sg * v[4 * j], sg * v[4 * j + 1], sg * v[4 * j + 2], sg * v[4 * j + 3]);
+                if (g.mode == 1 && live && m0 + r < g.M) {
                     // U(kk = row, j) into the block-real K-major operand of a later update (rows 2n,
                     // p3_ld wide): row j [Ur(:, j) | -Ui(:, j)], row n + j [Ui(:, j) | Ur(:, j)]
                     float* p3f = g.p3 + (size_t)f * g.p3_bstride;
                     const int n = g.p3_n, kk = g.p3_koff + m0 + r, ld = g.p3_ld, kh = g.p3_kh;
 #pragma unroll
                     for (int i = 0; i < 32; i++) {
-                        const int j = col0 + 32 * q + i;
+                        const int j = col + i;
                         if (plane == 0) {
                             p3f[(size_t)j * ld + kk] = v[i];
                             p3f[(size_t)(n + j) * ld + kh + kk] = v[i];
@@ -234,23 +209,25 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
                         }
                     }
                 }
+                tc::fence_proxy_async_smem();
+                asm volatile("bar.sync 1, 128;" ::: "memory");
+                if (issuer) {
+                    const float* box = sBox + (bx % GNBOX) * GBM * 32;
+                    if (live) {
+                        if (g.mode == 2)
+                            tc::tma_reduce_add_4d(&mapC, box, g.o_col0 + col, g.o_row0 + m0, plane, f);
+                        else
+                            tc::tma_store_4d(&mapC, box, g.o_col0 + col, g.o_row0 + m0, plane, f);
+                    }
+                    tc::bulk_commit();  // one group per box (empty for a chunk beyond the output)
+                }
             }
             // the accumulator buffer is free for the MMA of tile it + 2
             tc::tc_fence_before();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(&tempty[b]);
-            // all four epilogue warps have written the tile: one thread stores it
-            tc::fence_proxy_async_smem();
-            asm volatile("bar.sync 1, 128;" ::: "memory");
-            if (warp == 2 && lane == 0) {
-                for (int q = 0; q < GBN / 32; q++)
-                    tc::tma_store_4d(&mapC, sC + q * GBM * 32, g.o_col0 + col0 + 32 * q, g.o_row0 + m0, plane, f);
-                tc::bulk_commit();
-                tc::bulk_wait_read();  // the buffer may be refilled once the store has read it
-                tc::mbar_arrive(&cempty[b]);
-            }
         }
-        if (warp == 2 && lane == 0) tc::bulk_wait_all();
+        if (issuer) tc::bulk_wait_all();
     }
     tc::tc_fence_before();
     __syncthreads();
