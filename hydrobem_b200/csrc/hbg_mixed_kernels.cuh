@@ -19,8 +19,8 @@
 namespace hbg {
 
 constexpr int NBL = 128;  // LU block width (complex columns)
-constexpr int GBM = 128, GBK = 32, GSTAGES = 3, GBN = 256;
-constexpr int GNBOX = 4;  // ring of 32-column output boxes in shared memory
+constexpr int GBM = 128, GBK = 32, GSTAGES = 4, GBN = 256;
+constexpr int GNBOX = 2;  // ring of 32-column output boxes in shared memory
 
 struct GemmArgs {
     int M, Nc, Kp;         // rows, real output columns, real inner dimension
