@@ -260,6 +260,22 @@ __device__ __forceinline__ void cfma_add(float2& x, float2 a, float2 b) {  // x 
     x.y += a.x * b.y + a.y * b.x;
 }
 
+// sum_{kb <= k < ke} a(k) b(k) with four independent partial sums (short dependency chains: these
+// loops read their operands from shared memory and are latency-bound otherwise).
+template <class FA, class FB>
+__device__ __forceinline__ float2 cdot4(int kb, int ke, FA a, FB b) {
+    float2 s0 = make_float2(0.f, 0.f), s1 = s0, s2 = s0, s3 = s0;
+    int k = kb;
+    for (; k + 4 <= ke; k += 4) {
+        cfma_add(s0, a(k), b(k));
+        cfma_add(s1, a(k + 1), b(k + 1));
+        cfma_add(s2, a(k + 2), b(k + 2));
+        cfma_add(s3, a(k + 3), b(k + 3));
+    }
+    for (; k < ke; k++) cfma_add(s0, a(k), b(k));
+    return make_float2((s0.x + s1.x) + (s2.x + s3.x), (s0.y + s1.y) + (s2.y + s3.y));
+}
+
 // Warp-synchronous inverse of the 32 x 32 upper block U (diagonal included) at A (leading
 // dimension DF_LD) into X (leading dimension DF_SLD): X U = I, column by column, lane i owns row i.
 __device__ __forceinline__ void df_inv_upper32(const float2* A, float2* X) {
@@ -270,7 +286,7 @@ __device__ __forceinline__ void df_inv_upper32(const float2* A, float2* X) {
         const float2 inv = make_float2(d.x / dd, -d.y / dd);
         float2 t = make_float2(0.f, 0.f);
         if (i < j)  // X(i, j) = -(sum_{i <= k < j} X(i, k) U(k, j)) / U(j, j)
-            for (int k = i; k < j; k++) cfma_add(t, X[i * DF_SLD + k], A[k * DF_LD + j]);
+            t = cdot4(i, j, [&](int k) { return X[i * DF_SLD + k]; }, [&](int k) { return A[k * DF_LD + j]; });
         __syncwarp();
         if (i < j) X[i * DF_SLD + j] = make_float2(-(t.x * inv.x - t.y * inv.y), -(t.x * inv.y + t.y * inv.x));
         if (i == j) X[j * DF_SLD + j] = inv;
@@ -286,8 +302,10 @@ __device__ __forceinline__ void df_inv_lower32(const float2* A, float2* X) {
     for (int j = DF_BLK - 1; j >= 0; j--) {
         float2 t = make_float2(0.f, 0.f);
         if (i > j) {
-            t = A[i * DF_LD + j];  // k = i: Y(i, i) = 1
-            for (int k = j + 1; k < i; k++) cfma_add(t, X[i * DF_SLD + k], A[k * DF_LD + j]);
+            const float2 a = A[i * DF_LD + j];  // k = i: Y(i, i) = 1
+            t = cdot4(j + 1, i, [&](int k) { return X[i * DF_SLD + k]; }, [&](int k) { return A[k * DF_LD + j]; });
+            t.x += a.x;
+            t.y += a.y;
         }
         __syncwarp();
         if (i > j) X[i * DF_SLD + j] = make_float2(-t.x, -t.y);
@@ -316,23 +334,23 @@ __global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ 
     __syncthreads();
     for (int pb = 0; pb < DF_NB; pb++) {
         const int c0 = pb * DF_BLK;
-        // ---- panel: columns c0 .. c0 + 31, rows c0 .. NBL - 1; warp w < 4 owns rows c0 + w + 4 q
-        if (warp < 4) {
-            for (int j = 0; j < DF_BLK; j++) {
-                const int c = c0 + j;
-                asm volatile("bar.sync 1, 128;" ::: "memory");  // row c is final
-                const float2 d = blk[c * DF_LD + c];
-                const float dd = d.x * d.x + d.y * d.y;
-                if (threadIdx.x == 0 && !(dd > 1e-30f)) atomicExch(err, 10);
-                const float2 inv = make_float2(d.x / dd, -d.y / dd);
-                const float2 u = blk[c * DF_LD + c0 + lane];
-                int r = c + 1 + (((c0 + warp - (c + 1)) % 4) + 4) % 4;
-                for (; r < NBL; r += 4) {
-                    const float2 l = cmulf(blk[r * DF_LD + c], inv);
-                    if (lane > j) cfma_sub(blk[r * DF_LD + c0 + lane], l, u);
-                    __syncwarp();
-                    if (lane == j) blk[r * DF_LD + c] = l;
-                }
+        // ---- panel: columns c0 .. c0 + 31, rows c0 .. NBL - 1; lane = column, warp w owns rows
+        // c0 + w + DF_WARPS q (a few rows a warp, one CTA barrier per pivot)
+        constexpr int DF_WARPS = DF_THREADS / 32;
+        for (int j = 0; j < DF_BLK; j++) {
+            const int c = c0 + j;
+            __syncthreads();  // row c is final
+            const float2 d = blk[c * DF_LD + c];
+            const float dd = d.x * d.x + d.y * d.y;
+            if (threadIdx.x == 0 && !(dd > 1e-30f)) atomicExch(err, 10);
+            const float2 inv = make_float2(d.x / dd, -d.y / dd);
+            const float2 u = blk[c * DF_LD + c0 + lane];
+            int r = c + 1 + (((c0 + warp - (c + 1)) % DF_WARPS) + DF_WARPS) % DF_WARPS;
+            for (; r < NBL; r += DF_WARPS) {
+                const float2 l = cmulf(blk[r * DF_LD + c], inv);
+                if (lane > j) cfma_sub(blk[r * DF_LD + c0 + lane], l, u);
+                __syncwarp();
+                if (lane == j) blk[r * DF_LD + c] = l;
             }
         }
         __syncthreads();
@@ -353,9 +371,8 @@ __global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ 
                 v[e] = make_float2(0.f, 0.f);
                 if (t < DF_BLK * n2) {
                     const int i = t / n2, cc = c0 + DF_BLK + t % n2;
-                    float2 a = make_float2(0.f, 0.f);
-                    for (int k = 0; k <= i; k++) cfma_add(a, Y[i * DF_SLD + k], blk[(c0 + k) * DF_LD + cc]);
-                    v[e] = a;
+                    v[e] = cdot4(0, i + 1, [&](int k) { return Y[i * DF_SLD + k]; },
+                                 [&](int k) { return blk[(c0 + k) * DF_LD + cc]; });
                 }
             }
             __syncthreads();
@@ -370,9 +387,9 @@ __global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ 
         for (int t = threadIdx.x; t < n2 * n2; t += DF_THREADS) {
             const int r = c0 + DF_BLK + t / n2, cc = c0 + DF_BLK + t % n2;
             float2 a = blk[r * DF_LD + cc];
-#pragma unroll 8
-            for (int k = 0; k < DF_BLK; k++) cfma_sub(a, blk[r * DF_LD + c0 + k], blk[(c0 + k) * DF_LD + cc]);
-            blk[r * DF_LD + cc] = a;
+            const float2 p = cdot4(0, DF_BLK, [&](int k) { return blk[r * DF_LD + c0 + k]; },
+                                   [&](int k) { return blk[(c0 + k) * DF_LD + cc]; });
+            blk[r * DF_LD + cc] = make_float2(a.x - p.x, a.y - p.y);
         }
         __syncthreads();
     }
@@ -408,11 +425,12 @@ __global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ 
                 const int Kb = upper ? I : J + 1, Ke = upper ? J - 1 : I;
                 for (int K = Kb; K <= Ke; K++) {
                     const float2* Xd = (upper ? Ui : Li) + K * DF_BLK * DF_SLD;  // X(K, K) when K == I
-                    for (int k = 0; k < DF_BLK; k++) {
-                        const int kk = K * DF_BLK + k;
-                        const float2 x = (K == I) ? Xd[i * DF_SLD + k] : blk[row * DF_LD + kk];
-                        cfma_add(a, x, blk[kk * DF_LD + col]);
-                    }
+                    const float2 p = cdot4(
+                        0, DF_BLK,
+                        [&](int k) { return (K == I) ? Xd[i * DF_SLD + k] : blk[row * DF_LD + K * DF_BLK + k]; },
+                        [&](int k) { return blk[(K * DF_BLK + k) * DF_LD + col]; });
+                    a.x += p.x;
+                    a.y += p.y;
                 }
                 v[e] = a;
             }
@@ -436,9 +454,8 @@ __global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ 
                 const int bi = t / (DF_BLK * DF_BLK), i = (t / DF_BLK) % DF_BLK, j = t % DF_BLK;
                 const int I = upper ? bi : J + 1 + bi;
                 const float2* Xj = (upper ? Ui : Li) + J * DF_BLK * DF_SLD;
-                float2 a = make_float2(0.f, 0.f);
-                for (int k = 0; k < DF_BLK; k++)
-                    cfma_add(a, blk[(I * DF_BLK + i) * DF_LD + J * DF_BLK + k], Xj[k * DF_SLD + j]);
+                const float2 a = cdot4(0, DF_BLK, [&](int k) { return blk[(I * DF_BLK + i) * DF_LD + J * DF_BLK + k]; },
+                                       [&](int k) { return Xj[k * DF_SLD + j]; });
                 v[e] = make_float2(-a.x, -a.y);
             }
         }
