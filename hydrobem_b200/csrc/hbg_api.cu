@@ -161,6 +161,7 @@ struct DeviceCtx {
     bool ready = false;
     double* tables = nullptr;
     float* t2d_f = nullptr;
+    float* t1d_f = nullptr;
     Tables tab{};
 };
 
@@ -191,7 +192,12 @@ static DeviceCtx& device_ctx(int dev) {
     for (size_t i = 0; i < ht.len[1]; i++) t2f[i] = (float)ht.arr[1][i];
     CUDA_OK(cudaMalloc(&d.t2d_f, t2f.size() * sizeof(float)));
     CUDA_OK(cudaMemcpy(d.t2d_f, t2f.data(), t2f.size() * sizeof(float), cudaMemcpyHostToDevice));
-    d.tab = Tables{dp[0], dp[1], dp[2], dp[3], dp[4], dp[5], dp[6], dp[7], d.t2d_f};
+    // TABLE_1D likewise
+    std::vector<float> t1f(ht.len[0]);
+    for (size_t i = 0; i < ht.len[0]; i++) t1f[i] = (float)ht.arr[0][i];
+    CUDA_OK(cudaMalloc(&d.t1d_f, t1f.size() * sizeof(float)));
+    CUDA_OK(cudaMemcpy(d.t1d_f, t1f.data(), t1f.size() * sizeof(float), cudaMemcpyHostToDevice));
+    d.tab = Tables{dp[0], dp[1], dp[2], dp[3], dp[4], dp[5], dp[6], dp[7], d.t2d_f, d.t1d_f};
     static double glx[17][16], glw[17][16];
     memset(glx, 0, sizeof glx);
     memset(glw, 0, sizeof glw);

@@ -35,6 +35,7 @@ struct Tables {
     const double* l0;
     const double* bk;    // scaled K0, K1 tiles
     const float* t2d_f;  // t2d rounded to FP32 (the mixed form's coefficient reads)
+    const float* t1d_f;  // t1d rounded to FP32
 };
 
 // Panels in structure-of-arrays planes (each plane N doubles, plane p at base + p N).
@@ -106,6 +107,32 @@ __device__ __forceinline__ void table1d(double X, double* r) {
         r3 = r3 * t + cb.y;
     }
     r[0] = r0; r[1] = r1; r[2] = r2; r[3] = r3;
+}
+
+// table1d from the FP32 copy (the mixed form): one float4 per Chebyshev term, FP32 Horner chains.
+__device__ __forceinline__ void table1d_f32(double X, double* r) {
+    int i = (int)X;
+    if (i >= XT) i = XT - 1;
+    const float t = (float)(2.0 * (X - i) - 1.0);
+    const float4* c = reinterpret_cast<const float4*>(c_tab.t1d_f + i * (N1 + 1) * 4);
+    float r0 = 0.f, r1 = 0.f, r2 = 0.f, r3 = 0.f;
+#pragma unroll
+    for (int j = N1; j >= 0; j--) {
+        const float4 cc = __ldg(c + j);
+        r0 = r0 * t + cc.x;
+        r1 = r1 * t + cc.y;
+        r2 = r2 * t + cc.z;
+        r3 = r3 * t + cc.w;
+    }
+    r[0] = r0; r[1] = r1; r[2] = r2; r[3] = r3;
+}
+
+template <bool F32>
+__device__ __forceinline__ void table1d_t(double X, double* r) {
+    if constexpr (F32)
+        table1d_f32(X, r);
+    else
+        table1d(X, r);
 }
 
 // 2D tiles of V and V_X (green_inf.rs:78-107): Horner in tx per y power, then in ty
@@ -249,10 +276,11 @@ __device__ inline void far_series(double X, double Y, double w, double& P, doubl
     }
 }
 
+template <bool F32 = false>
 __device__ inline void bessel_j01(double X, double& j0, double& j1) {
     if (X < XT) {
         double f[4];
-        table1d(X, f);
+        table1d_t<F32>(X, f);
         j0 = f[0];
         j1 = f[1];
     } else {
@@ -261,13 +289,14 @@ __device__ inline void bessel_j01(double X, double& j0, double& j1) {
     }
 }
 
+template <bool F32 = false>
 __device__ inline void bessel_jy01(double X, double& j0, double& y0, double& j1, double& y1) {
     if (X >= XT) {
         hankel01(X, j0, y0, j1, y1);
         return;
     }
     double f[4];
-    table1d(X, f);
+    table1d_t<F32>(X, f);
     j0 = f[0];
     j1 = f[1];
     double L = log(0.5 * X) + GAMMA;
@@ -288,7 +317,7 @@ __device__ inline Wave wave_kernel(double X, double Y) {
     double eY = exp(-Y), j0, j1, F, FX;
     if (X < XT && Y < YT) {
         double f[4], v, vx;
-        table1d(X, f);
+        table1d_t<F32>(X, f);
         j0 = f[0];
         j1 = f[1];
         if constexpr (F32)
@@ -300,7 +329,7 @@ __device__ inline Wave wave_kernel(double X, double Y) {
         FX = 2.0 * eY * j1 * lg - 2.0 * eY * j0 * X / (R0 * (Y + R0)) - PI * eY * f[3] - 2.0 * (X / R0) * v -
              2.0 * R0 * vx;
     } else if (Y >= YT) {
-        bessel_j01(X, j0, j1);
+        bessel_j01<F32>(X, j0, j1);
         double P, PX;
         far_series(X, Y, 0.0, P, PX);
         F = -2.0 * P;
@@ -556,7 +585,7 @@ __device__ inline Kern finite_kernel(const FdParams& fd, const TT* T1, const TT*
         }
         if (ordinary) {
             double j0, y0, j1, y1;
-            bessel_jy01(fd.k0 * R, j0, y0, j1, y1);
+            bessel_jy01<F32>(fd.k0 * R, j0, y0, j1, y1);
             re += -fd.A0 * e0 * y0;
             reR += fd.A0 * e0 * fd.k0 * y1;
             reZ += -fd.A0 * e1 * y0;
@@ -620,7 +649,7 @@ __device__ inline Kern finite_kernel(const FdParams& fd, const TT* T1, const TT*
         o.WrR += K * K * F3X;
         Bz -= K * K * F3Y;
         double j0, j1;
-        bessel_j01(fd.k0 * R, j0, j1);
+        bessel_j01<F32>(fd.k0 * R, j0, j1);
         o.Wi = -fd.A0 * e0 * j0;
         o.WiR = fd.A0 * e0 * fd.k0 * j1;
         o.WiZ = -fd.A0 * e1 * j0;
