@@ -234,12 +234,14 @@ def ours(args, world, rank, local, pg):
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    dev_ms = []
+    dev_ms, dev_phases = [], []
     with Clocks(device) as clk:
         e0.record()
         for _ in range(args.steps):
             step()
-            dev_ms.append(nv.last_profile()["total"])
+            ph = nv.last_profile()
+            dev_ms.append(ph["total"])
+            dev_phases.append([round(ph[k], 2) for k in ("statics", "assembly", "lu", "substitution", "forces")])
         e1.record()
         torch.cuda.synchronize()
     barrier()
@@ -290,6 +292,7 @@ def ours(args, world, rank, local, pg):
                          "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
                          "peak_kind": pk, "launches": n, "ms": ms},
             "step_ms": [round(x, 2) for x in dev_ms],
+            "step_phases_ms": {"order": ["statics", "assembly", "lu", "substitution", "forces"], "steps": dev_phases},
             "phases_ms": {k: round(x, 3) for k, x in phases.items()},
             "kernels_ms": {k: round(x[0], 3) for k, x in prof.items() if x[1]},
             "measured_peaks_tflops": {k: round(x, 1) for k, x in pipe_peaks.items()},

@@ -157,6 +157,41 @@ static void gauss_legendre(int n, double* x, double* w) {
     if (n % 2 == 1) x[n / 2] = 0.0;
 }
 
+// Chebyshev truncation of a power-basis block on [-1, 1]^2: p[i * ps + j] (n1 x n2) the coefficient
+// of t1^i t2^j, re-expanded in Chebyshev polynomials T_a(t1) T_b(t2), the series cut to a < m1,
+// b < m2 and returned to the power basis in o[i * m2 + j] (m1 x m2).
+static void cheb_truncate(const double* p, int ps, int n1, int n2, int m1, int m2, double* o) {
+    constexpr int NMAX = 17;
+    double cp[NMAX][NMAX] = {};  // cp[j][k]: coefficient of t^k in T_j
+    cp[0][0] = 1.0;
+    cp[1][1] = 1.0;
+    for (int j = 2; j < NMAX; j++)
+        for (int k = 0; k < NMAX; k++) cp[j][k] = (k > 0 ? 2.0 * cp[j - 1][k - 1] : 0.0) - cp[j - 2][k];
+    std::vector<double> c((size_t)n1 * n2);
+    for (int i = 0; i < n1; i++)
+        for (int j = 0; j < n2; j++) c[(size_t)i * n2 + j] = p[(size_t)i * ps + j];
+    // power -> Chebyshev along t2 (rows), then t1 (columns): p_k = sum_j c_j cp[j][k], top degree first
+    for (int i = 0; i < n1; i++)
+        for (int j = n2 - 1; j >= 0; j--) {
+            double cj = c[(size_t)i * n2 + j] / cp[j][j];
+            for (int k = 0; k < j; k++) c[(size_t)i * n2 + k] -= cj * cp[j][k];
+            c[(size_t)i * n2 + j] = cj;
+        }
+    for (int j = 0; j < n2; j++)
+        for (int i = n1 - 1; i >= 0; i--) {
+            double ci = c[(size_t)i * n2 + j] / cp[i][i];
+            for (int k = 0; k < i; k++) c[(size_t)k * n2 + j] -= ci * cp[i][k];
+            c[(size_t)i * n2 + j] = ci;
+        }
+    for (int ki = 0; ki < m1; ki++)
+        for (int kj = 0; kj < m2; kj++) {
+            double acc = 0.0;
+            for (int a = ki; a < m1; a++)
+                for (int b = kj; b < m2; b++) acc += c[(size_t)a * n2 + b] * cp[a][ki] * cp[b][kj];
+            o[ki * m2 + kj] = acc;
+        }
+}
+
 struct DeviceCtx {
     bool ready = false;
     double* tables = nullptr;
@@ -187,14 +222,26 @@ static DeviceCtx& device_ctx(int dev) {
         dp[i] = d.tables + off;
         off += padded(ht.len[i]);
     }
-    // TABLE_2D rounded to FP32 for the mixed form's coefficient reads
-    std::vector<float> t2f(ht.len[1]);
-    for (size_t i = 0; i < ht.len[1]; i++) t2f[i] = (float)ht.arr[1][i];
+    // The mixed form's FP32 copies of TABLE_2D (cells [YT][XT], per quantity 8 x 8 coefficients, row
+    // j the tx^j terms) and TABLE_1D (cells [XT], N1 + 1 terms of 4 quantities), their Chebyshev
+    // series cut to T2D_FX x T2D_FY and T1D_FN terms
+    constexpr int M2 = N2 + 1;
+    std::vector<float> t2f((size_t)XT * YT * 2 * T2D_FB, 0.f);
+    double blk[M2 * M2];
+    for (int cell = 0; cell < XT * YT; cell++)
+        for (int q = 0; q < 2; q++) {
+            cheb_truncate(ht.arr[1] + ((size_t)cell * 2 + q) * M2 * M2, M2, M2, M2, T2D_FX, T2D_FY, blk);
+            for (int k = 0; k < T2D_FX * T2D_FY; k++) t2f[((size_t)cell * 2 + q) * T2D_FB + k] = (float)blk[k];
+        }
     CUDA_OK(cudaMalloc(&d.t2d_f, t2f.size() * sizeof(float)));
     CUDA_OK(cudaMemcpy(d.t2d_f, t2f.data(), t2f.size() * sizeof(float), cudaMemcpyHostToDevice));
-    // TABLE_1D likewise
-    std::vector<float> t1f(ht.len[0]);
-    for (size_t i = 0; i < ht.len[0]; i++) t1f[i] = (float)ht.arr[0][i];
+    std::vector<float> t1f((size_t)XT * T1D_FN * 4);
+    for (int cell = 0; cell < XT; cell++)
+        for (int q = 0; q < 4; q++) {
+            // the terms of quantity q sit at stride 4: a 17 x 1 block with row stride 4
+            cheb_truncate(ht.arr[0] + (size_t)cell * (N1 + 1) * 4 + q, 4, N1 + 1, 1, T1D_FN, 1, blk);
+            for (int k = 0; k < T1D_FN; k++) t1f[((size_t)cell * T1D_FN + k) * 4 + q] = (float)blk[k];
+        }
     CUDA_OK(cudaMalloc(&d.t1d_f, t1f.size() * sizeof(float)));
     CUDA_OK(cudaMemcpy(d.t1d_f, t1f.data(), t1f.size() * sizeof(float), cudaMemcpyHostToDevice));
     d.tab = Tables{dp[0], dp[1], dp[2], dp[3], dp[4], dp[5], dp[6], dp[7], d.t2d_f, d.t1d_f};
@@ -372,15 +419,12 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
             if (pr.body.vertices[3 * j + 2] < -opt.depth * (1.0 + 1e-12))
                 throw Failure{HB_ERR_VALUE, "a vertex lies below the sea bottom", body_index};
     }
-    // ---- geometry and statics
+    // ---- geometry and statics: buffers here, the device work in run_statics (which the mixed form
+    // calls once its own host-side setup is done, so that no driver call of that setup stands between
+    // the statics and the assembly in the device's queue)
     Workspace& ws = workspace();
     WsBuf dverts(ws, WS_VERTS), dkind(ws, WS_KIND), dplanes(ws, WS_PLANES), dbad(ws, WS_BAD), dst(ws, WS_ST),
         dwork(ws, WS_WORK), dnwork(ws, WS_NWORK);
-    dverts.alloc(sizeof(double) * 12 * N);
-    dkind.alloc(sizeof(int32_t) * N);
-    dplanes.alloc(sizeof(double) * P_PLANES * N);
-    dbad.alloc(sizeof(int32_t));
-    CUDA_OK(cudaMemcpyAsync(dverts.p, pr.body.vertices, sizeof(double) * 12 * N, cudaMemcpyHostToDevice, s));
     std::vector<int32_t> kinds(N, 0);
     if (pr.body.kinds)
         for (int j = 0; j < N; j++) {
@@ -388,11 +432,26 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
             if (k != HBG_WET && k != HBG_INTERIOR) throw Failure{HB_ERR_UNSUPPORTED, "panel kind not on this route", body_index};
             kinds[j] = k;
         }
-    CUDA_OK(cudaMemcpyAsync(dkind.p, kinds.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
-    int32_t big = 0x7fffffff;
-    CUDA_OK(cudaMemcpyAsync(dbad.p, &big, sizeof big, cudaMemcpyHostToDevice, s));
+    const size_t NN = (size_t)N * N;
+    const int work_cap = std::max(1 << 16, 16 * N);
+    dverts.alloc(sizeof(double) * 12 * N);
+    dkind.alloc(sizeof(int32_t) * N);
+    dplanes.alloc(sizeof(double) * P_PLANES * N);
+    dbad.alloc(sizeof(int32_t));
+    dst.alloc(sizeof(double) * 4 * NN);
+    dwork.alloc(sizeof(int32_t) * 2 * work_cap);
+    dnwork.alloc(2 * sizeof(int32_t));  // [adaptive worklist size, queue cursor]
+    const int32_t big = PANELS_VALID;
+    // page-locked: [first invalid panel, adaptive worklist size]
+    int32_t* hflags = static_cast<int32_t*>(ws.host(HS_FLAGS, 2 * sizeof(int32_t)));
+    if (!hflags) throw Failure{HB_ERR_INTERNAL, "page-locked host memory could not be allocated", body_index};
     double* prof = g_profile;
-    {
+    bool statics_ran = false;
+    auto run_statics = [&]() {
+        if (!solve_begin().recorded) solve_begin().record(s);
+        CUDA_OK(cudaMemcpyAsync(dverts.p, pr.body.vertices, sizeof(double) * 12 * N, cudaMemcpyHostToDevice, s));
+        CUDA_OK(cudaMemcpyAsync(dkind.p, kinds.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
+        CUDA_OK(cudaMemcpyAsync(dbad.p, &big, sizeof big, cudaMemcpyHostToDevice, s));
         EventTimer t(s, &prof[0]);
         KernelProfiler& P = profiler();
         P.begin(s);
@@ -400,47 +459,56 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
         P.end(KF_GEOMETRY, 0.0, s);
         g_launches++;
         PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
-        const size_t NN = (size_t)N * N;
-        dst.alloc(sizeof(double) * 4 * NN);
-        const int work_cap = std::max(1 << 16, 16 * N);
-        dwork.alloc(sizeof(int32_t) * 2 * work_cap);
-        dnwork.alloc(sizeof(int32_t));
-        CUDA_OK(cudaMemsetAsync(dnwork.p, 0, sizeof(int32_t), s));
+        CUDA_OK(cudaMemsetAsync(dnwork.p, 0, 2 * sizeof(int32_t), s));
         P.begin(s);
         launch_statics(pv, depth, opt.logarithmic, opt.log_tolerance, dst.as<double>(), dwork.as<int32_t>(),
                        dnwork.as<int32_t>(), work_cap, s);
         // algorithmic bytes: the four FP64 planes written
         P.end(KF_STATICS, 32.0 * (double)NN, s);
-        // one wait for both: the first invalid panel (geometry) and the adaptive worklist size (statics;
-        // on invalid panels the statics are discarded, their kernels only see non-finite values)
-        int32_t bad = 0, nwork = 0;
-        CUDA_OK(cudaMemcpyAsync(&bad, dbad.p, sizeof bad, cudaMemcpyDeviceToHost, s));
-        CUDA_OK(cudaMemcpyAsync(&nwork, dnwork.p, sizeof nwork, cudaMemcpyDeviceToHost, s));
-        CUDA_OK(cudaStreamSynchronize(s));
-        if (bad != big) {
-            Failure f{HB_ERR_VALUE, "invalid panel " + std::to_string(bad + 1) + " (degenerate, non-convex or non-finite)", body_index};
-            throw f;
-        }
-        if (nwork > work_cap) throw Failure{HB_ERR_INTERNAL, "adaptive log-integral worklist overflow", body_index};
+        // the first invalid panel (geometry) and the adaptive worklist size, read at the next wait of the
+        // solve; the adaptive kernel takes the size from device memory and does nothing on invalid panels
+        CUDA_OK(cudaMemcpyAsync(hflags, dbad.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+        CUDA_OK(cudaMemcpyAsync(hflags + 1, dnwork.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
         P.begin(s);
-        launch_statics_adaptive(pv, dwork.as<int32_t>(), nwork, dst.as<double>(), s);
-        P.end(KF_STATICS_ADAPTIVE, 16.0 * nwork, s);
-        g_launches += 1 + (nwork > 0);
+        launch_statics_adaptive_q(pv, dwork.as<int32_t>(), dnwork.as<int32_t>(), work_cap, dbad.as<int32_t>(), big,
+                                  dst.as<double>(), s);
+        P.end(KF_STATICS_ADAPTIVE, 0.0, s);
+        g_launches += 2;
         t.stop();
-        P.flush();
+        statics_ran = true;
+    };
+    // once the stream has passed the statics: invalid panels come first among the failures
+    auto statics_check = [&]() {
+        if (!statics_ran) return;
+        if (hflags[0] != big)
+            throw Failure{HB_ERR_VALUE,
+                          "invalid panel " + std::to_string(hflags[0] + 1) + " (degenerate, non-convex or non-finite)",
+                          body_index};
+        if (hflags[1] > work_cap) throw Failure{HB_ERR_INTERNAL, "adaptive log-integral worklist overflow", body_index};
+    };
+    // the mixed form's assembly kernels skip their work on invalid panels (the flag in device memory),
+    // so that its solve runs without a host wait until the end; the FP64 form waits here
+    PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>(), dbad.as<int32_t>()};
+    if (F == 0 || opt.precision != HBG_MIXED) {
+        run_statics();
+        CUDA_OK(cudaStreamSynchronize(s));
+        profiler().flush();
+        statics_check();
+        if (F == 0) return;
     }
-    PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
-    if (F == 0) return;
     const int nrhs = 6 + H;
     if (opt.precision == HBG_MIXED) {
         const char* msg = "";
         int64_t fq = -1;
-        int rc = mixed_solve_frequencies(pv, dst.as<double>(), pr, opt, fin, depth, s, prof, &g_launches, &msg, &fq);
+        int rc = mixed_solve_frequencies(pv, dst.as<double>(), pr, opt, fin, depth, s, prof, &g_launches, &msg, &fq,
+                                         run_statics);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) statics_check();
         if (rc != 0) throw Failure{rc, msg, body_index, fq};
+        CUDA_OK(e);
         return;
     }
     // ---- frequency batches
-    const size_t NN = (size_t)N * N;
     size_t per_freq = 2 * NN * sizeof(double2) + (size_t)(3 * nrhs + H) * N * sizeof(double2) +
                       (size_t)N * sizeof(int32_t) + (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)FP_PLANES * N * 8 +
                                                               (size_t)6912 * 3 * 8
@@ -476,10 +544,12 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
     // outputs per batch: A, B [6][6], X, FK, SC [H][6]
     const size_t out_per = 72 * sizeof(double) + 3 * (size_t)H * 6 * sizeof(double2);
     dout.alloc(out_per * B);
-    std::vector<unsigned char> hout(out_per * B);
+    // page-locked outputs and pivot flags: their reads queue behind the work
+    unsigned char* hout = static_cast<unsigned char*>(ws.host(HS_OUT, out_per * B + sizeof(int32_t) * B));
+    if (!hout) throw Failure{HB_ERR_INTERNAL, "page-locked host memory could not be allocated", body_index};
+    int32_t* info = reinterpret_cast<int32_t*>(hout + out_per * B);
     std::vector<FreqInfo> fi(B);
     std::vector<FdParams> fdh(B);
-    std::vector<int32_t> info(B);
     for (int f0 = 0; f0 < F; f0 += B) {
         if (opt.cancel && *opt.cancel) throw Failure{HB_ERR_CANCELLED, "the solve was cancelled", body_index, f0};
         const int nb = std::min(B, F - f0);
@@ -552,14 +622,15 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
                           dBo, dXo, dFK, dSC, s);
             P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
             g_launches += 1;
-            CUDA_OK(cudaMemcpyAsync(hout.data(), dout.p, out_per * nb, cudaMemcpyDeviceToHost, s));
-            CUDA_OK(cudaMemcpyAsync(info.data(), dinfo.p, sizeof(int32_t) * nb, cudaMemcpyDeviceToHost, s));
+            CUDA_OK(cudaMemcpyAsync(hout, dout.p, out_per * nb, cudaMemcpyDeviceToHost, s));
+            CUDA_OK(cudaMemcpyAsync(info, dinfo.p, sizeof(int32_t) * nb, cudaMemcpyDeviceToHost, s));
             t.stop();
+            solve_end().record(s);
         }
         CUDA_OK(cudaStreamSynchronize(s));
         CUDA_OK(cudaGetLastError());
         profiler().flush();
-        const double* hb = reinterpret_cast<const double*>(hout.data());
+        const double* hb = reinterpret_cast<const double*>(hout);
         const double* hA = hb;
         const double* hB = hb + 36 * (size_t)nb;
         const double* hX = hb + 72 * (size_t)nb;
@@ -633,6 +704,8 @@ extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_proble
         cudaEventCreate(&e1);
         cudaEventRecord(e0, s);
         phase_timers().flush();
+        solve_begin().recorded = false;
+        solve_end().recorded = false;
         try {
             for (int64_t p = 0; p < n_problems; p++) solve_problem(problems[p], *opt, p, s);
         } catch (...) {
@@ -647,7 +720,8 @@ extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_proble
         cudaEventSynchronize(e1);
         phase_timers().flush();
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventElapsedTime(&ms, solve_begin().recorded ? solve_begin().event() : e0,
+                             solve_end().recorded ? solve_end().event() : e1);
         g_profile[5] = ms;
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);

@@ -24,6 +24,16 @@ constexpr int TS = 8, TW = 8, TV = 16, TD = 5, TN = TD + 1;
 constexpr double XMAX = 0.5;
 constexpr int T1_SIZE = TS * TW * 3 * TN * TN;
 constexpr int T2_SIZE = TS * TV * 3 * TN * TN;
+// The mixed form's FP32 tiles: the same Chebyshev interpolants truncated to degree TFD in each
+// variable, each block of (TFD + 1)^2 power-basis coefficients padded to whole float4 loads.
+constexpr int TFD = 3, TFN = TFD + 1, TFB = (TFN * TFN + 3) / 4 * 4;
+constexpr int T1F_SIZE = TS * TW * 3 * TFB, T2F_SIZE = TS * TV * 3 * TFB;
+// The mixed form's FP32 copies of TABLE_1D and TABLE_2D, their Chebyshev series cut the same way:
+// TABLE_1D to T1D_FN terms per cell (degree 16 stored; the dropped terms sum below 3e-10), TABLE_2D
+// to T2D_FX x T2D_FY terms in (X, Y) per quantity (8 x 8 stored; dropped below 5e-8), each block of
+// T2D_FX T2D_FY coefficients padded to T2D_FB floats (whole float4 loads).
+constexpr int T1D_FN = 8;
+constexpr int T2D_FX = 6, T2D_FY = 7, T2D_FB = (T2D_FX * T2D_FY + 3) / 4 * 4;
 
 struct Tables {
     const double* t1d;   // [30][17][4]     J0, J1, Yt, Yt'
@@ -53,10 +63,16 @@ enum PanelPlane {
     P_PLANES = 73
 };
 
+// The geometry kernel's invalid-panel flag: the lowest invalid panel index, this value when none.
+constexpr int32_t PANELS_VALID = 0x7fffffff;
+
 struct PanelsView {
     int N;
     const double* p;     // P_PLANES planes of N
     const int32_t* kind; // 0 wet, 1 interior
+    // optional: the invalid-panel flag; kernels that see it set (!= PANELS_VALID) skip their work
+    const int32_t* bad = nullptr;
+    __device__ __forceinline__ bool invalid() const { return bad && *(volatile const int32_t*)bad != PANELS_VALID; }
     __device__ __forceinline__ double at(int plane, int j) const { return p[(size_t)plane * N + j]; }
 };
 
@@ -114,10 +130,10 @@ __device__ __forceinline__ void table1d_f32(double X, double* r) {
     int i = (int)X;
     if (i >= XT) i = XT - 1;
     const float t = (float)(2.0 * (X - i) - 1.0);
-    const float4* c = reinterpret_cast<const float4*>(c_tab.t1d_f + i * (N1 + 1) * 4);
+    const float4* c = reinterpret_cast<const float4*>(c_tab.t1d_f + i * T1D_FN * 4);
     float r0 = 0.f, r1 = 0.f, r2 = 0.f, r3 = 0.f;
 #pragma unroll
-    for (int j = N1; j >= 0; j--) {
+    for (int j = T1D_FN - 1; j >= 0; j--) {
         const float4 cc = __ldg(c + j);
         r0 = r0 * t + cc.x;
         r1 = r1 * t + cc.y;
@@ -168,38 +184,37 @@ __device__ __forceinline__ void table2d(double X, double Y, double& v, double& v
     vx = s[1];
 }
 
-// table2d from the FP32 copy of the coefficients, FP32 Horner chains (the mixed form: half the
-// coefficient bytes per evaluation; its matrices are stored in complex64).
+// table2d from the FP32 copy of the coefficients (the mixed form): per cell and quantity a block of
+// T2D_FX x T2D_FY power-basis coefficients (row j: the tx^j terms over the powers of ty), FP32 Horner
+// chains.
 __device__ __forceinline__ void table2d_f32(double X, double Y, double& v, double& vx) {
     int ix = (int)X, iy = (int)Y;
     if (ix >= XT) ix = XT - 1;
     if (iy >= YT) iy = YT - 1;
     const float tx = (float)(2.0 * (X - ix) - 1.0), ty = (float)(2.0 * (Y - iy) - 1.0);
-    constexpr int M = N2 + 1;
-    static_assert(M == 8, "rows of 8 FP32 coefficients: two float4 loads a row");
-    const float* c = c_tab.t2d_f + ((size_t)iy * XT + ix) * 2 * M * M;
+    const float4* c = reinterpret_cast<const float4*>(c_tab.t2d_f + ((size_t)iy * XT + ix) * 2 * T2D_FB);
     float s[2];
 #pragma unroll
     for (int q = 0; q < 2; q++) {
-        const float4* cq = reinterpret_cast<const float4*>(c + q * M * M);
-        float r[M];
+        float cf[T2D_FB];
 #pragma unroll
-        for (int a = 0; a < M; a++) r[a] = 0.f;
-#pragma unroll
-        for (int j = M - 1; j >= 0; j--) {
-            const float4 c0 = __ldg(cq + 2 * j), c1 = __ldg(cq + 2 * j + 1);
-            r[0] = r[0] * tx + c0.x;
-            r[1] = r[1] * tx + c0.y;
-            r[2] = r[2] * tx + c0.z;
-            r[3] = r[3] * tx + c0.w;
-            r[4] = r[4] * tx + c1.x;
-            r[5] = r[5] * tx + c1.y;
-            r[6] = r[6] * tx + c1.z;
-            r[7] = r[7] * tx + c1.w;
+        for (int u = 0; u < T2D_FB / 4; u++) {
+            const float4 a = __ldg(c + q * (T2D_FB / 4) + u);
+            cf[4 * u] = a.x;
+            cf[4 * u + 1] = a.y;
+            cf[4 * u + 2] = a.z;
+            cf[4 * u + 3] = a.w;
         }
-        float acc = 0.f;
+        float r[T2D_FY];
 #pragma unroll
-        for (int a = M - 1; a >= 0; a--) acc = acc * ty + r[a];
+        for (int a = 0; a < T2D_FY; a++) r[a] = cf[(T2D_FX - 1) * T2D_FY + a];
+#pragma unroll
+        for (int j = T2D_FX - 2; j >= 0; j--)
+#pragma unroll
+            for (int a = 0; a < T2D_FY; a++) r[a] = r[a] * tx + cf[j * T2D_FY + a];
+        float acc = r[T2D_FY - 1];
+#pragma unroll
+        for (int a = T2D_FY - 2; a >= 0; a--) acc = acc * ty + r[a];
         s[q] = acc;
     }
     v = s[0];
@@ -475,11 +490,10 @@ __device__ __forceinline__ void phi_tiles(const double* T, int which, double xb,
     v[0] = v0; v[1] = v1; v[2] = v2;
 }
 
-// phi_tiles from FP32 tiles (the mixed form): per tile 3 blocks of 36 coefficients, 432 bytes
-// (27 float4 loads), FP32 Horner chains.
+// phi_tiles from the FP32 tiles of the mixed form: per tile 3 blocks of TFB coefficients of degree
+// TFD in each variable, FP32 Horner chains.
 __device__ __forceinline__ void phi_tiles_f32(const float* T, int which, double xb, double vb, double* v) {
-    constexpr int N = TN;
-    static_assert(TN == 6, "blocks of 36 FP32 coefficients: nine float4 loads a block");
+    constexpr int N = TFN;
     int ny = which == 1 ? TW : TV;
     double ymax = which == 1 ? 1.0 : 2.0;
     double ux = xb * (TS / XMAX), uy = vb * (ny / ymax);
@@ -487,13 +501,13 @@ __device__ __forceinline__ void phi_tiles_f32(const float* T, int which, double 
     if (ix > TS - 1) ix = TS - 1;
     if (iy > ny - 1) iy = ny - 1;
     const float tx = (float)(2.0 * (ux - ix) - 1.0), ty = (float)(2.0 * (uy - iy) - 1.0);
-    const float4* c = reinterpret_cast<const float4*>(T + (size_t)(ix * ny + iy) * 3 * N * N);
+    const float4* c = reinterpret_cast<const float4*>(T + (size_t)(ix * ny + iy) * 3 * TFB);
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-        float cf[N * N];
+        float cf[TFB];
 #pragma unroll
-        for (int u = 0; u < N * N / 4; u++) {
-            const float4 a = __ldg(c + q * (N * N / 4) + u);
+        for (int u = 0; u < TFB / 4; u++) {
+            const float4 a = __ldg(c + q * (TFB / 4) + u);
             cf[4 * u] = a.x;
             cf[4 * u + 1] = a.y;
             cf[4 * u + 2] = a.z;

@@ -145,6 +145,7 @@ __device__ __forceinline__ double free_term(int kind) { return kind == 1 ? -4.0 
 // column-major with leading dimension Np (the mixed form; entry (k, n) at n Np + k).
 struct OutF64 {
     static constexpr bool kF32 = false;  // FP64 coefficient tables
+    static constexpr int kT1 = T1_SIZE, kT2 = T2_SIZE;
     using Tile = double;
     double2* S;
     double2* A;
@@ -159,6 +160,7 @@ struct OutF64 {
 
 struct OutF32 {
     static constexpr bool kF32 = true;  // FP32 coefficient tables and tiles
+    static constexpr int kT1 = T1F_SIZE, kT2 = T2F_SIZE;
     using Tile = float;
     float* S;
     float* A;
@@ -181,6 +183,7 @@ __global__ void __launch_bounds__(256, 2) k_assemble(PanelsView pv, const double
     // statics (n, k) [q][k_local][n_local]; each (k_local, n_local) slot is read and then
     // overwritten with the results (S, A) of entry (n, k) by the one thread that owns it
     __shared__ double sT[4][32][33];
+    if (pv.invalid()) return;  // invalid panels: the solve reports them
     const int N = pv.N;
     const int nt = (N + 31) / 32;
     // tile pair from the linear index: row-block kb <= column-block nb
@@ -217,8 +220,8 @@ __global__ void __launch_bounds__(256, 2) k_assemble(PanelsView pv, const double
         kindk = pv.kind[k];
     }
     const FdParams* fd = FINITE ? fdp + f : nullptr;
-    const typename Out::Tile* T1 = FINITE ? tiles + (size_t)f * (T1_SIZE + T2_SIZE) : nullptr;
-    const typename Out::Tile* T2 = FINITE ? T1 + T1_SIZE : nullptr;
+    const typename Out::Tile* T1 = FINITE ? tiles + (size_t)f * (Out::kT1 + Out::kT2) : nullptr;
+    const typename Out::Tile* T2 = FINITE ? T1 + Out::kT1 : nullptr;
     const double* fp = FINITE ? fpt + (size_t)f * FP_PLANES * N : nullptr;
 #pragma unroll 1
     for (int i = 0; i < 4; i++) {
@@ -279,14 +282,55 @@ void launch_assemble_f64(const PanelsView& pv, const double* st, int F, const Fr
         k_assemble<false, OutF64><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
 }
 
-// The finite-depth tiles of a batch rounded to FP32 (same layout: blocks of 36 coefficients).
-__global__ void k_tiles_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
-    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
-        b[t] = (float)a[t];
+// The finite-depth tiles of a batch for the mixed form: per tile and quantity (one thread each) the
+// power-basis block of degree TN - 1 taken back to Chebyshev coefficients, the series truncated to
+// degree TFD in each variable, returned to the power basis and rounded to FP32.
+__global__ void k_tiles_f32(int F, const double* __restrict__ a, float* __restrict__ b) {
+    constexpr int N = TN, M = TFN, BLOCKS = 3 * (TS * TW + TS * TV);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = t / BLOCKS, blk = t % BLOCKS;
+    if (f >= F) return;
+    // cp[j][k]: coefficient of t^k in the Chebyshev polynomial T_j
+    double cp[N][N];
+    for (int j = 0; j < N; j++)
+        for (int k = 0; k < N; k++) cp[j][k] = 0.0;
+    cp[0][0] = 1.0;
+    cp[1][1] = 1.0;
+    for (int j = 2; j < N; j++)
+        for (int k = 0; k < N; k++) cp[j][k] = (k > 0 ? 2.0 * cp[j - 1][k - 1] : 0.0) - cp[j - 2][k];
+    double c[N][N];
+    const double* p = a + (size_t)f * (T1_SIZE + T2_SIZE) + (size_t)blk * N * N;
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) c[i][j] = p[i * N + j];
+    // power -> Chebyshev along the second variable (rows), then the first (columns): the triangular
+    // system p_k = sum_j c_j cp[j][k], solved from the top degree down
+    for (int i = 0; i < N; i++)
+        for (int j = N - 1; j >= 0; j--) {
+            double cj = c[i][j] / cp[j][j];
+            for (int k = 0; k < j; k++) c[i][k] -= cj * cp[j][k];
+            c[i][j] = cj;
+        }
+    for (int j = 0; j < N; j++)
+        for (int i = N - 1; i >= 0; i--) {
+            double ci = c[i][j] / cp[i][i];
+            for (int k = 0; k < i; k++) c[k][j] -= ci * cp[i][k];
+            c[i][j] = ci;
+        }
+    // the truncated series back in the power basis
+    float* o = b + (size_t)f * (T1F_SIZE + T2F_SIZE) + (size_t)blk * TFB;
+    for (int ki = 0; ki < M; ki++)
+        for (int kj = 0; kj < M; kj++) {
+            double acc = 0.0;
+            for (int ji = ki; ji < M; ji++)
+                for (int jj = kj; jj < M; jj++) acc += c[ji][jj] * cp[ji][ki] * cp[jj][kj];
+            o[ki * M + kj] = (float)acc;
+        }
+    for (int k = M * M; k < TFB; k++) o[k] = 0.f;
 }
 
 void launch_tiles_f32(int F, const double* tiles, float* tiles_f, cudaStream_t s) {
-    k_tiles_f32<<<148, 256, 0, s>>>((size_t)F * (T1_SIZE + T2_SIZE), tiles, tiles_f);
+    int n = F * 3 * (TS * TW + TS * TV);
+    k_tiles_f32<<<(n + 127) / 128, 128, 0, s>>>(F, tiles, tiles_f);
 }
 
 void launch_assemble_f32(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,

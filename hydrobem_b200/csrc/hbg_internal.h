@@ -72,9 +72,26 @@ enum WsSlot {
     WS_SG_IMG, WS_SG_COUNT, WS_COUNT
 };
 
+// Page-locked host buffers of a solve: a device-to-host copy into pageable memory waits for the
+// stream, one into these does not.
+enum HostSlot { HS_FLAGS = 0, HS_NORMS, HS_OUT, HS_COUNT };
+
 struct Workspace {
     void* p[WS_COUNT] = {};
     size_t bytes[WS_COUNT] = {};
+    void* hp[HS_COUNT] = {};
+    size_t hbytes[HS_COUNT] = {};
+    // a page-locked host buffer of at least b bytes for the slot (nullptr when the allocation fails)
+    void* host(int slot, size_t b) {
+        if (b == 0) b = 16;
+        if (hbytes[slot] >= b) return hp[slot];
+        if (hp[slot]) cudaFreeHost(hp[slot]);
+        hp[slot] = nullptr;
+        hbytes[slot] = 0;
+        if (cudaMallocHost(&hp[slot], b) != cudaSuccess) return nullptr;
+        hbytes[slot] = b;
+        return hp[slot];
+    }
     // a buffer of at least b bytes for the slot (nullptr when the allocation fails)
     void* get(int slot, size_t b) {
         if (b == 0) b = 16;
@@ -96,6 +113,11 @@ struct Workspace {
             if (p[i]) cudaFree(p[i]);
             p[i] = nullptr;
             bytes[i] = 0;
+        }
+        for (int i = 0; i < HS_COUNT; i++) {
+            if (hp[i]) cudaFreeHost(hp[i]);
+            hp[i] = nullptr;
+            hbytes[i] = 0;
         }
     }
 };
@@ -120,21 +142,41 @@ inline IrHistory& last_ir_history() {
 }
 
 // Phase timings recorded without waiting: the event pairs are kept until flush(), which the solve
-// calls once its stream has finished, so a phase boundary never stalls the host.
+// calls once its stream has finished, so a phase boundary never stalls the host.  The events come
+// from a per-device pool kept across solves (creating events can take a driver lock, and a host
+// thread held there while the device runs short of queued work would idle the device).
 struct PhaseTimers {
     struct Pending {
         cudaEvent_t a, b;
         double* acc;
+        int dev;
     };
     std::vector<Pending> pend;
+    std::vector<cudaEvent_t> pool[16];
+    static int device() {
+        int d = 0;
+        cudaGetDevice(&d);
+        return d < 0 || d >= 16 ? 0 : d;
+    }
+    cudaEvent_t take(int dev) {
+        if (pool[dev].empty()) {
+            cudaEvent_t e = nullptr;
+            cudaEventCreate(&e);
+            return e;
+        }
+        cudaEvent_t e = pool[dev].back();
+        pool[dev].pop_back();
+        return e;
+    }
+    void give(int dev, cudaEvent_t e) { pool[dev].push_back(e); }
     void flush() {
         for (auto& p : pend) {
             cudaEventSynchronize(p.b);
             float ms = 0.f;
             cudaEventElapsedTime(&ms, p.a, p.b);
             *p.acc += ms;
-            cudaEventDestroy(p.a);
-            cudaEventDestroy(p.b);
+            give(p.dev, p.a);
+            give(p.dev, p.b);
         }
         pend.clear();
     }
@@ -144,31 +186,55 @@ inline PhaseTimers& phase_timers() {
     return t;
 }
 
+// The device span of a solve: `begin` recorded with its first device operation, `end` after the last
+// device operation of each batch is queued (its output readback), before the host waits.  The
+// solve's time runs from one to the other: host work before the first operation (argument checks,
+// sizing, allocation) and the host's wake-up and output handling after the wait are not device time.
+struct SolveMark {
+    cudaEvent_t e[16] = {};
+    int dev = 0;
+    bool recorded = false;
+    void record(cudaStream_t s) {
+        dev = PhaseTimers::device();
+        if (!e[dev]) cudaEventCreate(&e[dev]);
+        cudaEventRecord(e[dev], s);
+        recorded = true;
+    }
+    cudaEvent_t event() const { return e[dev]; }
+};
+inline SolveMark& solve_begin() {
+    static thread_local SolveMark t;
+    return t;
+}
+inline SolveMark& solve_end() {
+    static thread_local SolveMark t;
+    return t;
+}
+
 // Device time of a phase: events on the stream, added to *acc at the next PhaseTimers::flush().
 struct EventTimer {
     cudaEvent_t a{}, b{};
     cudaStream_t s;
     double* acc;
+    int dev;
     bool stopped = false;
-    EventTimer(cudaStream_t st, double* target) : s(st), acc(target) {
-        cudaEventCreate(&a);
-        cudaEventCreate(&b);
+    EventTimer(cudaStream_t st, double* target) : s(st), acc(target), dev(PhaseTimers::device()) {
+        a = phase_timers().take(dev);
+        b = phase_timers().take(dev);
         cudaEventRecord(a, s);
     }
     void stop() {
         cudaEventRecord(b, s);
-        phase_timers().pend.push_back({a, b, acc});
+        phase_timers().pend.push_back({a, b, acc, dev});
         stopped = true;
     }
     ~EventTimer() {
         if (!stopped) {
-            cudaEventDestroy(a);
-            cudaEventDestroy(b);
+            phase_timers().give(dev, a);
+            phase_timers().give(dev, b);
         }
     }
 };
-
-
 
 // Per-frequency data of one batch entry (one body, one omega).
 struct FreqInfo {
@@ -183,6 +249,9 @@ void launch_panel_geometry(int N, const double* verts, const int32_t* kind, doub
 void launch_statics(const PanelsView& pv, double depth, int logint, double tol, double* st, int32_t* work,
                     int32_t* nwork, int work_cap, cudaStream_t s);
 void launch_statics_adaptive(const PanelsView& pv, const int32_t* work, int nwork, double* st, cudaStream_t s);
+// q: [entry count, queue cursor (zero)] in device memory; nothing runs when *bad != clean
+void launch_statics_adaptive_q(const PanelsView& pv, const int32_t* work, int32_t* q, int work_cap,
+                               const int32_t* bad, int32_t clean, double* st, cudaStream_t s);
 
 // finite depth: per-frequency tiles [F][T1 | T2] and fin-point planes [F][FP_PLANES][N]
 void launch_fd_tiles(int F, const FdParams* fd, double* tiles, double* scratch, cudaStream_t s);

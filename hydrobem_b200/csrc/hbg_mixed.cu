@@ -114,7 +114,7 @@ inline int& ir_guess() {
 
 int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgProblem& pr, const HbgOptions& opt,
                             bool fin, double depth, cudaStream_t s, double* prof, int64_t* launches, const char** msg,
-                            int64_t* freq) {
+                            int64_t* freq, const std::function<void()>& start) {
     KernelProfiler& P = profiler();
     const int N = pv.N, F = (int)pr.n_omega, H = (int)pr.n_heading, nrhs = 6 + H;
     const int Np = (N + NBL - 1) / NBL * NBL;
@@ -127,7 +127,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     const size_t prep = prep_rows * 2 * NBL;
     size_t per = 3 * MB * 4 + 3 * prep * 4 + (size_t)(NBL * 2 * NBL + 4 * NBL * NBL) * 4 +
                  (size_t)(nrhs + H) * N * 16 + 4 * (size_t)nrhs * Np * 16 + 64 +
-                 (fin ? (size_t)(T1_SIZE + T2_SIZE) * 12 + (size_t)FP_PLANES * N * 8 + (size_t)6912 * 3 * 8 : 0);
+                 (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)(T1F_SIZE + T2F_SIZE) * 4 + (size_t)FP_PLANES * N * 8 + (size_t)6912 * 3 * 8 : 0);
     per += (size_t)(Np / NBL) * NBL * NBL * 8;  // the diagonal-block inverses
     size_t freeb = 0, totalb = 0;
     if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "cudaMemGetInfo failed", -1);
@@ -167,7 +167,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     FdParams* dfd = (FdParams*)get(WS_FD, sizeof(FdParams) * B);
     double* dheads = (double*)get(WS_HEADS, sizeof(double) * std::max(H, 1));
     double* tiles = fin ? (double*)get(WS_TILES, sizeof(double) * (T1_SIZE + T2_SIZE) * B) : nullptr;
-    float* tiles_f = fin ? (float*)get(WS_TILES_F, sizeof(float) * (T1_SIZE + T2_SIZE) * B) : nullptr;
+    float* tiles_f = fin ? (float*)get(WS_TILES_F, sizeof(float) * (T1F_SIZE + T2F_SIZE) * B) : nullptr;
     // the wave-term network (optional): its parameters, the packed BF16 image the assembly loads, and
     // the count of pairs it served
     const bool sg = opt.surrogate != nullptr;
@@ -179,12 +179,6 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     double* dout = (double*)get(WS_OUT, sizeof(double) * (72 + 3 * (size_t)H * 12) * B);
     if (!okb) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
     last_surrogate_pairs() = 0;
-    if (sg) {
-        cudaMemcpyAsync(sg_params, opt.surrogate, sizeof(float) * SURROGATE_FLOATS, cudaMemcpyHostToDevice, s);
-        launch_sg_pack(sg_params, sg_img, s);
-        cudaMemsetAsync(sg_count, 0, sizeof(unsigned long long), s);
-        (*launches)++;
-    }
     // ---- tensor maps (whole batch; the batch index is the 4th coordinate)
     CUtensorMap mapW, mapPL, mapPU, mapP2, mapP3, mapP3w, mapP3h;
     const uint64_t fb = 4;  // bytes per float
@@ -213,11 +207,14 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     cudaFuncSetAttribute(k_tri_step<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(16));
     std::vector<double> heads(std::max(H, 1));
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
-    cudaMemcpyAsync(dheads, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s);
     std::vector<FreqInfo> fi(B);
     std::vector<FdParams> fdh(B);
     const size_t out_per = 72 + 3 * (size_t)H * 12;
-    std::vector<double> hout(out_per * B), hn(IR_MAX_IT * 2 * (size_t)B);
+    // page-locked: the reads of norms, outputs and the error flag queue behind the work, no host wait
+    double* hout = (double*)ws.host(HS_OUT, sizeof(double) * (out_per * B + 1));
+    double* hn = (double*)ws.host(HS_NORMS, sizeof(double) * IR_MAX_IT * 2 * (size_t)B);
+    if (!hout || !hn) MIXED_FAIL(HB_ERR_INTERNAL, "page-locked host memory could not be allocated", -1);
+    int* herr = reinterpret_cast<int*>(hout + out_per * B);
     // out = bias - M x over the batch (M column-major planar FP32), FP64 accumulation
     const int nz = (N + GEMV_CHUNK - 1) / GEMV_CHUNK;
     double2* part = (double2*)ws.get(WS_PART, (size_t)nz * B * nrhs * N * 16);
@@ -306,6 +303,15 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         P.end(KF_MIXED_GEMM, 2.0 * g.M * (double)g.Nc * g.Kp * nb, s);
         (*launches)++;
     };
+    // ---- the device work: statics, then per batch assembly, LU, refinement, forces
+    start();
+    cudaMemcpyAsync(dheads, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s);
+    if (sg) {
+        cudaMemcpyAsync(sg_params, opt.surrogate, sizeof(float) * SURROGATE_FLOATS, cudaMemcpyHostToDevice, s);
+        launch_sg_pack(sg_params, sg_img, s);
+        cudaMemsetAsync(sg_count, 0, sizeof(unsigned long long), s);
+        (*launches)++;
+    }
     for (int f0 = 0; f0 < F; f0 += B) {
         if (opt.cancel && *opt.cancel) MIXED_FAIL(HB_ERR_CANCELLED, "the solve was cancelled", f0);
         const int nb = std::min(B, F - f0);
@@ -474,13 +480,33 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 k_ir_update<<<nb, 256, 0, s>>>(Np, nrhs, x, r, norms + (size_t)i * 2 * nb);
                 *launches += 1;
             };
-            // the first `guess` corrections without waiting on the host, then one look at all their norms
+            // the forces and the readback of outputs, norms and the error flag (one wait for all)
+            auto forces = [&]() {
+                EventTimer tf(s, &prof[4]);
+                double* dA = dout;
+                double* dB = dout + 36 * (size_t)nb;
+                double2* dX = reinterpret_cast<double2*>(dout + 72 * (size_t)nb);
+                double2* dFK = dX + (size_t)H * 6 * nb;
+                double2* dSC = dFK + (size_t)H * 6 * nb;
+                P.begin(s);
+                launch_forces(pv, nb, dfi, H, x, Np, phiI, opt.density, dA, dB, dX, dFK, dSC, s);
+                P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
+                (*launches)++;
+                cudaMemcpyAsync(hout, dout, sizeof(double) * out_per * nb, cudaMemcpyDeviceToHost, s);
+                cudaMemcpyAsync(herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+                tf.stop();
+                solve_end().record(s);
+            };
+            // the first `guess` corrections and the forces without waiting on the host, then one look
+            // at all the norms; further corrections (and the forces again) only when they fall short
             const int guess = std::min(std::max(ir_guess(), 2), IR_MAX_IT);
             for (int i = 0; i < guess; i++) {
                 correction(i);
                 if (i + 1 < guess) gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL);
             }
-            cudaMemcpyAsync(hn.data(), norms, sizeof(double) * 2 * nb * guess, cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(hn, norms, sizeof(double) * 2 * nb * guess, cudaMemcpyDeviceToHost, s);
+            t.stop();
+            forces();
             cudaStreamSynchronize(s);
             double prev = INFINITY;
             bool stalled = false;
@@ -498,13 +524,14 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             if (converged) {
                 ir_guess() = it + 1;
                 it = guess;  // the corrections that ran (a later one only refines further)
-            } else if (!stalled) {
+            } else if (!stalled && *herr == 0) {
                 // further corrections, one host look each: no residual after the one that meets the test
+                EventTimer t2(s, &prof[3]);
                 for (it = guess; it < IR_MAX_IT; it++) {
                     gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL);
                     correction(it);
-                    cudaMemcpyAsync(hn.data() + (size_t)it * 2 * nb, norms + (size_t)it * 2 * nb,
-                                    sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, s);
+                    cudaMemcpyAsync(hn + (size_t)it * 2 * nb, norms + (size_t)it * 2 * nb, sizeof(double) * 2 * nb,
+                                    cudaMemcpyDeviceToHost, s);
                     cudaStreamSynchronize(s);
                     const double worst = worst_at(it);
                     hist.ratio[hist.n++] = worst;
@@ -518,34 +545,20 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                     if (it >= 3 && !(worst < 0.5 * prev)) break;
                     prev = worst;
                 }
+                t2.stop();
+                if (converged) {
+                    forces();
+                    cudaStreamSynchronize(s);
+                }
             }
-            t.stop();
         }
-        // ---- forces (read back with the error flag: one wait for both)
-        int herr = 0;
-        cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
-        {
-            EventTimer t(s, &prof[4]);
-            double* dA = dout;
-            double* dB = dout + 36 * (size_t)nb;
-            double2* dX = reinterpret_cast<double2*>(dout + 72 * (size_t)nb);
-            double2* dFK = dX + (size_t)H * 6 * nb;
-            double2* dSC = dFK + (size_t)H * 6 * nb;
-            P.begin(s);
-            launch_forces(pv, nb, dfi, H, x, Np, phiI, opt.density, dA, dB, dX, dFK, dSC, s);
-            P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
-            (*launches)++;
-            cudaMemcpyAsync(hout.data(), dout, sizeof(double) * out_per * nb, cudaMemcpyDeviceToHost, s);
-            t.stop();
-        }
-        cudaStreamSynchronize(s);
         P.flush();
         if (cudaGetLastError() != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "CUDA error in the mixed-precision solve", f0);
-        if (herr == 10) MIXED_FAIL(HB_ERR_NUMERICAL, "zero pivot in the unpivoted mixed-precision LU", f0);
-        if (herr != 0) MIXED_FAIL(HB_ERR_INTERNAL, "a tensor-core pipeline wait timed out", f0);
+        if (*herr == 10) MIXED_FAIL(HB_ERR_NUMERICAL, "zero pivot in the unpivoted mixed-precision LU", f0);
+        if (*herr != 0) MIXED_FAIL(HB_ERR_INTERNAL, "a tensor-core pipeline wait timed out", f0);
         if (!converged)
             MIXED_FAIL(HB_ERR_NUMERICAL, "iterative refinement of the mixed-precision solve did not converge", f0);
-        const double* hA = hout.data();
+        const double* hA = hout;
         const double* hB = hA + 36 * (size_t)nb;
         const double* hX = hA + 72 * (size_t)nb;
         const double* hFK = hX + (size_t)H * 12 * nb;

@@ -430,12 +430,9 @@ __device__ __forceinline__ void log_point(const double m[4][3], const double* im
     b = ww * dpsi;
 }
 
-__global__ void __launch_bounds__(AD_WARPS * 32) k_statics_adaptive(PanelsView pv, const int32_t* __restrict__ work,
-                                                                    int nwork, double* __restrict__ st) {
-    __shared__ AdCell stack[AD_WARPS][AD_STACK];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int t = blockIdx.x * AD_WARPS + warp;
-    if (t >= nwork) return;
+// One adaptive pair (worklist entry t) by the calling warp; stk: the warp's stack in shared memory.
+__device__ void adaptive_pair(const PanelsView& pv, const int32_t* __restrict__ work, int t, double* __restrict__ st,
+                              AdCell* stk, int lane) {
     const int N = pv.N;
     const int k = work[2 * t], j = work[2 * t + 1];
     PanelRegs p;
@@ -455,7 +452,6 @@ __global__ void __launch_bounds__(AD_WARPS * 32) k_statics_adaptive(PanelsView p
         wa += __shfl_xor_sync(0xffffffffu, wa, o);
         wb += __shfl_xor_sync(0xffffffffu, wb, o);
     }
-    AdCell* stk = stack[warp];
     int sp = 0;
     if (lane == 0) stk[0] = AdCell{-1.0, 1.0, -1.0, 1.0, wa, wb, 0};
     sp = 1;
@@ -510,6 +506,37 @@ __global__ void __launch_bounds__(AD_WARPS * 32) k_statics_adaptive(PanelsView p
     }
 }
 
+// One warp per worklist entry, the entry count given by the host.
+__global__ void __launch_bounds__(AD_WARPS * 32) k_statics_adaptive(PanelsView pv, const int32_t* __restrict__ work,
+                                                                    int nwork, double* __restrict__ st) {
+    __shared__ AdCell stack[AD_WARPS][AD_STACK];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t = blockIdx.x * AD_WARPS + warp;
+    if (t >= nwork) return;
+    adaptive_pair(pv, work, t, st, stack[warp], lane);
+}
+
+// The same with the entry count in device memory (q[0], capped at work_cap) and the entries taken
+// from a queue (cursor q[1], zero at launch), so that the host need not wait for the count.  No
+// work when the geometry flagged an invalid panel (*bad != clean): the solve reports it.
+__global__ void __launch_bounds__(AD_WARPS * 32) k_statics_adaptive_q(PanelsView pv, const int32_t* __restrict__ work,
+                                                                      int32_t* q, int work_cap,
+                                                                      const int32_t* __restrict__ bad, int32_t clean,
+                                                                      double* __restrict__ st) {
+    __shared__ AdCell stack[AD_WARPS][AD_STACK];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (*bad != clean) return;
+    const int nwork = min(*(volatile int32_t*)q, work_cap);
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(q + 1, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= nwork) return;
+        adaptive_pair(pv, work, t, st, stack[warp], lane);
+        __syncwarp();
+    }
+}
+
 // ------------------------------------------------------------------ host launchers
 void launch_panel_geometry(int N, const double* verts, const int32_t* kind, double* planes, int32_t* bad,
                            cudaStream_t s) {
@@ -524,6 +551,21 @@ void launch_statics(const PanelsView& pv, double depth, int logint, double tol, 
 
 void launch_statics_adaptive(const PanelsView& pv, const int32_t* work, int nwork, double* st, cudaStream_t s) {
     if (nwork > 0) k_statics_adaptive<<<(nwork + AD_WARPS - 1) / AD_WARPS, AD_WARPS * 32, 0, s>>>(pv, work, nwork, st);
+}
+
+void launch_statics_adaptive_q(const PanelsView& pv, const int32_t* work, int32_t* q, int work_cap,
+                               const int32_t* bad, int32_t clean, double* st, cudaStream_t s) {
+    static int grid[16] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 16) dev = 0;
+    if (grid[dev] == 0) {
+        int sms = 0, per = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_statics_adaptive_q, AD_WARPS * 32, 0);
+        grid[dev] = std::max(1, sms * std::max(per, 1));
+    }
+    k_statics_adaptive_q<<<grid[dev], AD_WARPS * 32, 0, s>>>(pv, work, q, work_cap, bad, clean, st);
 }
 
 void set_constants_statics(const double glx[17][16], const double glw[17][16]) {

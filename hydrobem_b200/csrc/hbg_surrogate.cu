@@ -556,6 +556,7 @@ __global__ void __launch_bounds__(256, 1) k_assemble_sg(PanelsView pv, const dou
                                                        unsigned long long* __restrict__ counts) {
     extern __shared__ __align__(16) uint8_t img[];
     __shared__ double sT[4][32][33];
+    if (pv.invalid()) return;  // invalid panels: the solve reports them
     {
         const uint4* src = reinterpret_cast<const uint4*>(img_g);
         uint4* dst = reinterpret_cast<uint4*>(img);
@@ -597,8 +598,8 @@ __global__ void __launch_bounds__(256, 1) k_assemble_sg(PanelsView pv, const dou
         ak = pv.at(P_AREA, kc);
         const int kindk = pv.kind[kc];
         const FdParams* fd = FINITE ? fdp + f : nullptr;
-        const float* T1 = FINITE ? tiles + (size_t)f * (T1_SIZE + T2_SIZE) : nullptr;
-        const float* T2 = FINITE ? T1 + T1_SIZE : nullptr;
+        const float* T1 = FINITE ? tiles + (size_t)f * (T1F_SIZE + T2F_SIZE) : nullptr;
+        const float* T2 = FINITE ? T1 + T1F_SIZE : nullptr;
         const double* fp = FINITE ? fpt + (size_t)f * FP_PLANES * N : nullptr;
 #pragma unroll 1
         for (int i = 0; i < 4; i++) {

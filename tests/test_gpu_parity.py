@@ -189,6 +189,13 @@ def test_error_paths():
     with pytest.raises(nv.HydroBEMError) as e:
         nv.solve(bad, [1.0], [0.0])
     assert e.value.status == 1 and "panel 4" in e.value.message
+    # the mixed form reads the flag only at the end of its solve; its assembly skips the work
+    for depth in (float("inf"), 3.0):
+        with pytest.raises(nv.HydroBEMError) as e:
+            nv.solve(bad, [1.0, 1.5], [0.0], precision=nv.HBG_MIXED, depth=depth)
+        assert e.value.status == 1 and "panel 4" in e.value.message
+    g = nv.solve(v, [1.0], [0.0], precision=nv.HBG_MIXED)  # the context is still usable
+    assert np.isfinite(g["A"]).all()
     import ctypes
 
     flag = (ctypes.c_int32 * 1)(1)
