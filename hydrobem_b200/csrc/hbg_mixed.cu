@@ -163,6 +163,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     float2* r = (float2*)get(WS_R, (size_t)nrhs * Np * B * 8);
     double* norms = (double*)get(WS_NORMS, IR_MAX_IT * 2 * (size_t)B * 8);  // [iteration][batch][2]
     int* err = (int*)get(WS_ERR, sizeof(int));
+    int* tctrl = (int*)get(WS_TRI_CTRL, sizeof(int) * (1 + (size_t)B));  // the triangular sweeps' tickets
     FreqInfo* dfi = (FreqInfo*)get(WS_FI, sizeof(FreqInfo) * B);
     FdParams* dfd = (FdParams*)get(WS_FD, sizeof(FdParams) * B);
     double* dheads = (double*)get(WS_HEADS, sizeof(double) * std::max(H, 1));
@@ -205,6 +206,14 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     cudaFuncSetAttribute(k_tri_step<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(10));
     cudaFuncSetAttribute(k_tri_step<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(12));
     cudaFuncSetAttribute(k_tri_step<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(16));
+    // the persistent sweeps: as many CTAs as fit at once
+    const int nr_sweep = nrhs <= 8 ? 8 : nrhs <= 10 ? 10 : nrhs <= 12 ? 12 : 16;
+    const void* sweep_fn = nr_sweep == 8 ? (const void*)k_tri_sweep<8> : nr_sweep == 10 ? (const void*)k_tri_sweep<10>
+                           : nr_sweep == 12 ? (const void*)k_tri_sweep<12> : (const void*)k_tri_sweep<16>;
+    cudaFuncSetAttribute(sweep_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(nr_sweep));
+    int sweep_per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sweep_per_sm, sweep_fn, TRI_THREADS, tri_smem_bytes(nr_sweep));
+    const int sweep_ctas = n_sm * std::max(sweep_per_sm, 1);
     std::vector<double> heads(std::max(H, 1));
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
     std::vector<FreqInfo> fi(B);
@@ -275,6 +284,24 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     auto trisolve = [&](float2* xv, int nb) {
         const int nblk_i = Np / TB;
         P.begin(s);
+        if (nrhs <= 16) {  // one persistent sweep per direction
+            const int grid = std::min(nblk_i * nb, sweep_ctas);
+            const size_t sm = tri_smem_bytes(nr_sweep);
+            for (int up = 1; up >= 0; up--) {
+                cudaMemsetAsync(tctrl, 0, sizeof(int) * (1 + (size_t)nb), s);
+                if (nr_sweep == 8)
+                    k_tri_sweep<8><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
+                else if (nr_sweep == 10)
+                    k_tri_sweep<10><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
+                else if (nr_sweep == 12)
+                    k_tri_sweep<12><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
+                else
+                    k_tri_sweep<16><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
+                (*launches)++;
+            }
+            P.end(KF_LU_SOLVE, 8.0 * (double)NP2 * nb, s);
+            return;
+        }
         for (int dir = 0; dir < 2; dir++) {
             const int up = dir == 0;
             for (int st = -1; st < nblk_i - 1; st++) {
@@ -555,6 +582,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         P.flush();
         if (cudaGetLastError() != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "CUDA error in the mixed-precision solve", f0);
         if (*herr == 10) MIXED_FAIL(HB_ERR_NUMERICAL, "zero pivot in the unpivoted mixed-precision LU", f0);
+        if (*herr == 8) MIXED_FAIL(HB_ERR_INTERNAL, "a triangular sweep wait timed out", f0);
         if (*herr != 0) MIXED_FAIL(HB_ERR_INTERNAL, "a tensor-core pipeline wait timed out", f0);
         if (!converged)
             MIXED_FAIL(HB_ERR_NUMERICAL, "iterative refinement of the mixed-precision solve did not converge", f0);

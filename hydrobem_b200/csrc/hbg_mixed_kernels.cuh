@@ -921,6 +921,144 @@ __global__ void __launch_bounds__(TRI_THREADS, 2) k_tri_step(int Np, size_t bstr
 
 constexpr size_t tri_smem_bytes(int nr) { return (size_t)TB * nr * (sizeof(float4) + 3 * sizeof(float2)); }
 
+// The same solve as one persistent launch per direction (up to NR right-hand sides): the work items
+// are (k, f), block k in solve order of matrix f, handed out by a ticket counter in the order
+// k nb + f.  An item streams the block row of the factor against the blocks 0 .. k-1 as their
+// solutions are published (ctrl[1 + f] = blocks of matrix f done), subtracts the sum, solves its
+// diagonal block by the stored inverse and publishes it.  An item waits only on items of smaller
+// ticket, which running CTAs hold, so the sweep cannot deadlock; every wait is bounded (error 8).
+// ctrl = [ticket, done[nb]], zero at launch.
+constexpr uint32_t TRI_WAIT_LIMIT = 1u << 20;
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+    asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+template <int NR>
+__global__ void __launch_bounds__(TRI_THREADS, 2) k_tri_sweep(int Np, size_t bstride, const float* __restrict__ W,
+                                                           const float2* __restrict__ DINV, int nrhs,
+                                                           float2* __restrict__ Xall, int nb, int upper_t,
+                                                           int* __restrict__ ctrl, int* __restrict__ err) {
+    extern __shared__ float4 tri_smem4[];  // ys [TB][NR] as {re, im, im, re}, partial sums [3][TB][NR]
+    float4(*ys)[NR] = reinterpret_cast<float4(*)[NR]>(tri_smem4);
+    float2(*pt)[NR] = reinterpret_cast<float2(*)[NR]>(tri_smem4 + TB * NR);
+    __shared__ int s_item, s_stop;
+    const int nblk = Np / TB, items = nblk * nb;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int li = 32 * (warp & 1) + lane;  // local rows li and li + 64
+    const int pq = warp >> 1;               // quarter of each solved block
+    for (;;) {
+        __syncthreads();  // the previous item's shared data consumed
+        if (threadIdx.x == 0) s_item = atomicAdd(ctrl, 1);
+        __syncthreads();
+        const int t = s_item;
+        if (t >= items) return;
+        const int k = t / nb, f = t % nb;
+        const int r0 = (upper_t ? k : nblk - 1 - k) * TB;
+        const float* Mr = W + (size_t)f * bstride;
+        const float* Mi = Mr + (size_t)Np * Np;
+        float2* X = Xall + (size_t)f * nrhs * Np;
+        int* done = ctrl + 1 + f;
+        f32x2 a0[NR], a1[NR];
+#pragma unroll
+        for (int c = 0; c < NR; c++) a0[c] = a1[c] = f2pack(0.f, 0.f);
+#pragma unroll 1
+        for (int kk = 0; kk < k; kk++) {
+            const int s0 = (upper_t ? kk : nblk - 1 - kk) * TB;
+            if (threadIdx.x == 0) {
+                int stop = 0;
+                uint32_t n = 0;
+                while (ld_acquire_gpu(done) <= kk) {
+                    if (*(volatile int*)err != 0) {
+                        stop = 1;
+                        break;
+                    }
+                    if (++n > TRI_WAIT_LIMIT) {
+                        atomicExch(err, 8);
+                        stop = 1;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+                s_stop = stop;
+            }
+            __syncthreads();
+            if (s_stop) return;
+            // the solved block (written by another CTA: read through L2)
+            for (int tt = threadIdx.x; tt < TB * NR; tt += blockDim.x) {
+                const int p = tt % TB, c = tt / TB;
+                ys[p][c] = dup_swap(c < nrhs ? __ldcg(X + (size_t)c * Np + s0 + p) : make_float2(0.f, 0.f));
+            }
+            __syncthreads();
+            const float* pr = Mr + (size_t)(s0 + pq * 32) * Np + r0 + li;
+            const float* pi = Mi + (size_t)(s0 + pq * 32) * Np + r0 + li;
+#pragma unroll 1
+            for (int pc = 0; pc < 32; pc += 16) {
+                float r0v[16], i0v[16], r1v[16], i1v[16];
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    const size_t o = (size_t)(pc + q) * Np;
+                    r0v[q] = __ldg(pr + o);
+                    i0v[q] = __ldg(pi + o);
+                    r1v[q] = __ldg(pr + o + 64);
+                    i1v[q] = __ldg(pi + o + 64);
+                }
+#pragma unroll
+                for (int q = 0; q < 16; q++) {
+                    const f32x2 m0 = f2pack(r0v[q], r0v[q]), n0 = f2pack(-i0v[q], i0v[q]);
+                    const f32x2 m1 = f2pack(r1v[q], r1v[q]), n1 = f2pack(-i1v[q], i1v[q]);
+#pragma unroll
+                    for (int c = 0; c < NR; c++) {
+                        const float4 v4 = ys[pq * 32 + pc + q][c];
+                        const f32x2 v = f2pack(v4.x, v4.y), vs = f2pack(v4.z, v4.w);
+                        a0[c] = ffma2(m0, v, a0[c]);
+                        a0[c] = ffma2(n0, vs, a0[c]);
+                        a1[c] = ffma2(m1, v, a1[c]);
+                        a1[c] = ffma2(n1, vs, a1[c]);
+                    }
+                }
+            }
+            __syncthreads();  // ys read by every warp before the next block overwrites it
+        }
+        if (k > 0) {
+            if (pq > 0)
+#pragma unroll
+                for (int c = 0; c < NR; c++) {
+                    pt[(pq - 1) * TB + li][c] = f2unpack(a0[c]);
+                    pt[(pq - 1) * TB + li + 64][c] = f2unpack(a1[c]);
+                }
+            __syncthreads();
+            if (pq == 0)
+#pragma unroll
+                for (int c = 0; c < NR; c++)
+                    if (c < nrhs) {
+                        float2 s0v = f2unpack(a0[c]), s1v = f2unpack(a1[c]);
+#pragma unroll
+                        for (int h = 0; h < 3; h++) {
+                            const float2 q0 = pt[h * TB + li][c], q1 = pt[h * TB + li + 64][c];
+                            s0v.x += q0.x;
+                            s0v.y += q0.y;
+                            s1v.x += q1.x;
+                            s1v.y += q1.y;
+                        }
+                        float2* x0 = X + (size_t)c * Np + r0 + li;
+                        const float2 v0 = x0[0], v1 = x0[64];
+                        x0[0] = make_float2(v0.x - s0v.x, v0.y - s0v.y);
+                        x0[64] = make_float2(v1.x - s1v.x, v1.y - s1v.y);
+                    }
+        }
+        tri_diag_f32<NR>(DINV + ((size_t)f * nblk + r0 / TB) * TB * TB, X, Np, nrhs, r0, upper_t, ys, pt);
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) st_release_gpu(done, k + 1);
+    }
+}
+
 // FP64 vectors to complex64 (the right-hand sides entering the first correction).
 __global__ void k_to_c64(size_t n, const double2* __restrict__ a, float2* __restrict__ b) {
     for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
