@@ -105,6 +105,31 @@ inline int& ir_guess() {
     return g;
 }
 
+// Side streams for the LU of LU_GROUPS groups of a batch and their fork/join events, per device and
+// host thread (kept across solves).
+constexpr int LU_GROUPS = 3;
+struct SideStreams {
+    cudaStream_t s[LU_GROUPS] = {};
+    cudaEvent_t fork = nullptr, join[LU_GROUPS] = {};
+    bool ok = false;
+};
+static SideStreams& side_streams() {
+    static thread_local SideStreams t[16];
+    int d = 0;
+    cudaGetDevice(&d);
+    if (d < 0 || d >= 16) d = 0;
+    SideStreams& x = t[d];
+    if (!x.ok) {
+        bool ok = true;
+        for (int i = 0; i < LU_GROUPS; i++) {
+            ok = ok && cudaStreamCreateWithFlags(&x.s[i], cudaStreamNonBlocking) == cudaSuccess;
+            ok = ok && cudaEventCreateWithFlags(&x.join[i], cudaEventDisableTiming) == cudaSuccess;
+        }
+        x.ok = ok && cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming) == cudaSuccess;
+    }
+    return x;
+}
+
 #define MIXED_FAIL(code, text, fq) \
     do {                           \
         *msg = text;               \
@@ -322,14 +347,19 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         // the factors read once per direction (8 B per entry)
         P.end(KF_LU_SOLVE, 8.0 * (double)NP2 * nb, s);
     };
-    auto gemm = [&](const CUtensorMap& mA, const CUtensorMap& mB, GemmArgs g, int nb) {
+    // matrices f0 .. f0 + nb of the batch on stream st, at most cap persistent CTAs
+    auto gemm = [&](const CUtensorMap& mA, const CUtensorMap& mB, GemmArgs g, int f0, int nb, cudaStream_t st,
+                    int cap) {
         g.batch = nb;
+        g.b0 = f0;
         const int tiles = ((g.M + GBM - 1) / GBM) * ((g.Nc + GBN - 1) / GBN) * nb;
-        P.begin(s);
-        k_gemm_tf32<<<std::min(tiles, n_sm), GEMM_THREADS, smem, s>>>(mA, mB, mapW, g);
-        P.end(KF_MIXED_GEMM, 2.0 * g.M * (double)g.Nc * g.Kp * nb, s);
+        P.begin(st);
+        k_gemm_tf32<<<std::min(tiles, cap), GEMM_THREADS, smem, st>>>(mA, mB, mapW, g);
+        P.end(KF_MIXED_GEMM, 2.0 * g.M * (double)g.Nc * g.Kp * nb, st);
         (*launches)++;
     };
+    SideStreams& side = side_streams();
+    if (!side.ok) MIXED_FAIL(HB_ERR_INTERNAL, "CUDA streams for the LU could not be created", -1);
     // ---- the device work: statics, then per batch assembly, LU, refinement, forces
     start();
     cudaMemcpyAsync(dheads, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s);
@@ -387,22 +417,32 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             // Two 128-column blocks per outer step: the second block is updated by the first alone, the
             // block row of both is solved, and the trailing matrix is updated once per 256 columns
             // (K' = 512: half the passes over it of a 128-column step).
-            auto diag = [&](int k0) {
-                P.begin(s);
-                k_diag_factor<<<nb, DF_THREADS, dsmem, s>>>(W, Np, MB, k0, PL, PU, DINV, err);
-                P.end(KF_LU_PANEL, 8.0 * NBL * (double)NBL * NBL * nb, s);
+            // The LU of LU_GROUPS groups of the batch on side streams: the diagonal-block factors (one
+            // CTA per matrix, barrier-bound) of one group run beside the tensor-core products of the
+            // others, whose persistent grids leave that many SMs free.
+            struct Half {
+                cudaStream_t st;
+                int f0, nb, cap;
+            };
+            auto diag = [&](const Half& h, int k0) {
+                P.begin(h.st);
+                k_diag_factor<<<h.nb, DF_THREADS, dsmem, h.st>>>(W + (size_t)h.f0 * MB, Np, MB, k0,
+                                                                  PL + (size_t)h.f0 * NBL * 2 * NBL,
+                                                                  PU + (size_t)h.f0 * 4 * NBL * NBL,
+                                                                  DINV + (size_t)h.f0 * nblk * NBL * NBL, err);
+                P.end(KF_LU_PANEL, 8.0 * NBL * (double)NBL * NBL * h.nb, h.st);
                 (*launches)++;
             };
-            auto prep_row = [&](int k0, int c0, int ncols) {  // rows k0..k0+NBL, columns c0..c0+ncols
-                P.begin(s);
-                k_prep_block_row<<<dim3(ncols / 32, NBL / 32, nb), dim3(32, 8), 0, s>>>(W, Np, MB, k0, c0, ncols, P2,
-                                                                                      prep);
-                P.end(KF_MIXED_CONVERT, 2.0 * NBL * (double)ncols * 4 * 3 * nb, s);
+            auto prep_row = [&](const Half& h, int k0, int c0, int ncols) {  // rows k0..k0+NBL, columns c0..c0+ncols
+                P.begin(h.st);
+                k_prep_block_row<<<dim3(ncols / 32, NBL / 32, h.nb), dim3(32, 8), 0, h.st>>>(
+                    W + (size_t)h.f0 * MB, Np, MB, k0, c0, ncols, P2 + (size_t)h.f0 * prep, prep);
+                P.end(KF_MIXED_CONVERT, 2.0 * NBL * (double)ncols * 4 * 3 * h.nb, h.st);
                 (*launches)++;
             };
             GemmArgs g0{};
             g0.err = err;
-            auto gemm_l = [&](int k0, int rows) {  // L(rows below the block) = M(., block k0) U_kk^-1
+            auto gemm_l = [&](const Half& h, int k0, int rows) {  // L(rows below the block) = M(., block k0) U_kk^-1
                 GemmArgs g = g0;
                 g.M = rows;
                 g.Nc = 2 * NBL;
@@ -415,11 +455,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 g.o_row0 = k0 + NBL;
                 g.o_col0 = k0;
                 g.o_nc = NBL;
-                gemm(mapW, mapPU, g, nb);
+                gemm(mapW, mapPU, g, h.f0, h.nb, h.st, h.cap);
             };
             // U(rows k0..k0+NBL, columns c0..c0+ncols) = L_kk^-1 B (prepared in P2), and its block-real
             // copy into P3 (rows of ld floats, this block's rows from koff, second half at kh)
-            auto gemm_u = [&](int k0, int c0, int ncols, int ld, int kh, int koff) {
+            auto gemm_u = [&](const Half& h, int k0, int c0, int ncols, int ld, int kh, int koff) {
                 GemmArgs g = g0;
                 g.M = NBL;
                 g.Nc = 2 * ncols;
@@ -435,11 +475,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 g.p3_ld = ld;
                 g.p3_kh = kh;
                 g.p3_koff = koff;
-                gemm(mapPL, mapP2, g, nb);
+                gemm(mapPL, mapP2, g, h.f0, h.nb, h.st, h.cap);
             };
             // M(rows row0.., columns c0..c0+ncols) -= L(rows, columns a_x0..a_x0+a_kc) U (B operand)
-            auto update = [&](int rows, int row0, int c0, int ncols, int a_x0, int a_kc, const CUtensorMap& mB,
-                              int b_split) {
+            auto update = [&](const Half& h, int rows, int row0, int c0, int ncols, int a_x0, int a_kc,
+                              const CUtensorMap& mB, int b_split) {
                 GemmArgs g = g0;
                 g.M = rows;
                 g.Nc = 2 * ncols;
@@ -453,33 +493,50 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 g.o_col0 = c0;
                 g.o_nc = ncols;
                 g.b_split = b_split;
-                gemm(mapW, mB, g, nb);
+                gemm(mapW, mB, g, h.f0, h.nb, h.st, h.cap);
             };
-            int K0 = 0;
-            for (; K0 + 2 * NBL <= Np; K0 += 2 * NBL) {
+            // one outer step (columns K0 .. K0 + 2 NBL) of one half
+            auto outer_step = [&](const Half& h, int K0) {
                 const int k1 = K0 + NBL, c2 = K0 + 2 * NBL, n = Np - c2;
                 // first block: factor, L below it, U of the second block's columns, update of the second block
-                diag(K0);
-                prep_row(K0, k1, NBL);
-                gemm_l(K0, Np - k1);
-                gemm_u(K0, k1, NBL, 2 * NBL, NBL, 0);
-                update(Np - k1, k1, k1, NBL, K0, NBL, mapP3, 0);
+                diag(h, K0);
+                prep_row(h, K0, k1, NBL);
+                gemm_l(h, K0, Np - k1);
+                gemm_u(h, K0, k1, NBL, 2 * NBL, NBL, 0);
+                update(h, Np - k1, k1, k1, NBL, K0, NBL, mapP3, 0);
                 // U of the first block's rows beyond the panel (while L_KK^-1 is at hand)
                 if (n > 0) {
-                    prep_row(K0, c2, n);
-                    gemm_u(K0, c2, n, 4 * NBL, 2 * NBL, 0);
+                    prep_row(h, K0, c2, n);
+                    gemm_u(h, K0, c2, n, 4 * NBL, 2 * NBL, 0);
                 }
                 // second block
-                diag(k1);
+                diag(h, k1);
                 if (n > 0) {
-                    gemm_l(k1, n);
-                    update(NBL, k1, c2, n, K0, NBL, mapP3h, NBL);  // its rows beyond the panel: -= L21 U13
-                    prep_row(k1, c2, n);
-                    gemm_u(k1, c2, n, 4 * NBL, 2 * NBL, NBL);
-                    update(n, c2, c2, n, K0, 2 * NBL, mapP3w, 0);  // the trailing matrix, K' = 512
+                    gemm_l(h, k1, n);
+                    update(h, NBL, k1, c2, n, K0, NBL, mapP3h, NBL);  // its rows beyond the panel: -= L21 U13
+                    prep_row(h, k1, c2, n);
+                    gemm_u(h, k1, c2, n, 4 * NBL, 2 * NBL, NBL);
+                    update(h, n, c2, c2, n, K0, 2 * NBL, mapP3w, 0);  // the trailing matrix, K' = 512
                 }
+            };
+            const int nh = std::min(LU_GROUPS, nb);
+            Half hs[LU_GROUPS];
+            for (int i = 0, f0 = 0; i < nh; i++) {
+                const int ni = nb / nh + (i < nb % nh ? 1 : 0);
+                hs[i] = Half{side.s[i], f0, ni, std::max(n_sm - (nb - ni), 1)};
+                f0 += ni;
             }
-            if (K0 < Np) diag(K0);  // an odd last block
+            cudaEventRecord(side.fork, s);
+            for (int i = 0; i < nh; i++) cudaStreamWaitEvent(hs[i].st, side.fork, 0);
+            int K0 = 0;
+            for (; K0 + 2 * NBL <= Np; K0 += 2 * NBL)
+                for (int i = 0; i < nh; i++) outer_step(hs[i], K0);
+            if (K0 < Np)  // an odd last block
+                for (int i = 0; i < nh; i++) diag(hs[i], K0);
+            for (int i = 0; i < nh; i++) {
+                cudaEventRecord(side.join[i], hs[i].st);
+                cudaStreamWaitEvent(s, side.join[i], 0);
+            }
             t.stop();
         }
         // ---- refinement: x_{i+1} = x_i + A^-1 (b - A x_i), A^-1 by the TF32 factors, residuals in FP64

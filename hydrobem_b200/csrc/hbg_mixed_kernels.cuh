@@ -29,6 +29,7 @@ struct GemmArgs {
     int mode;              // 0 store, 1 store and scatter into the GEMM3 operand, 2 subtract
     int o_row0, o_col0, o_nc;  // output placement in the planar matrix: column j' -> plane j' / o_nc
     int batch;             // matrices in the launch
+    int b0;                // index of the launch's first matrix in the tensor maps
     int b_split;           // 0: B coordinates (kk, row); > 0: B viewed as [row][2][.]: (kk % b_split, kk / b_split, row)
     float* p3;             // a later update's B operand [F][2 p3_n][p3_ld] (mode 1)
     size_t p3_bstride;
@@ -91,7 +92,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
     tc::tc_fence_after();
     const uint32_t tmem = *tslot;
     auto tile_coords = [&](int t, int& m0, int& n0, int& f) {
-        f = t / (mt * nt);
+        f = g.b0 + t / (mt * nt);
         int r = t % (mt * nt);
         n0 = (r / mt) * GBN;  // row tiles fastest: consecutive CTAs share the B block
         m0 = (r % mt) * GBM;
