@@ -176,7 +176,7 @@ struct OutF32 {
 };
 
 template <bool FINITE, class Out>
-__global__ void __launch_bounds__(256, 2) k_assemble(PanelsView pv, const double* __restrict__ st,
+__global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView pv, const double* __restrict__ st,
                                                   const FreqInfo* __restrict__ fi, const FdParams* __restrict__ fdp,
                                                   const typename Out::Tile* __restrict__ tiles,
                                                   const double* __restrict__ fpt, Out out) {
