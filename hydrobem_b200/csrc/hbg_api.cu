@@ -462,7 +462,7 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
         CUDA_OK(cudaMemsetAsync(dnwork.p, 0, 2 * sizeof(int32_t), s));
         P.begin(s);
         launch_statics(pv, depth, opt.logarithmic, opt.log_tolerance, dst.as<double>(), dwork.as<int32_t>(),
-                       dnwork.as<int32_t>(), work_cap, s);
+                       dnwork.as<int32_t>(), work_cap, s, opt.precision == HBG_MIXED);
         // algorithmic bytes: the four FP64 planes written
         P.end(KF_STATICS, 32.0 * (double)NN, s);
         // the first invalid panel (geometry) and the adaptive worklist size, read at the next wait of the

@@ -246,8 +246,9 @@ void set_constants(const double glx[17][16], const double glw[17][16], const Tab
 void set_constants_statics(const double glx[17][16], const double glw[17][16]);
 void launch_panel_geometry(int N, const double* verts, const int32_t* kind, double* planes, int32_t* bad,
                            cudaStream_t s);
+// mixed: the mixed form's variant (far Rankine points and the order-4 log rule in FP32)
 void launch_statics(const PanelsView& pv, double depth, int logint, double tol, double* st, int32_t* work,
-                    int32_t* nwork, int work_cap, cudaStream_t s);
+                    int32_t* nwork, int work_cap, cudaStream_t s, bool mixed = false);
 void launch_statics_adaptive(const PanelsView& pv, const int32_t* work, int nwork, double* st, cudaStream_t s);
 // q: [entry count, queue cursor (zero)] in device memory; nothing runs when *bad != clean
 void launch_statics_adaptive_q(const PanelsView& pv, const int32_t* work, int32_t* q, int work_cap,

@@ -305,6 +305,70 @@ __device__ inline void log_gauss(const PanelRegs& p, const double* image, int or
     Ld = ld;
 }
 
+// ---- the mixed form's far-field shortcuts (its matrices are rounded to FP32 afterwards)
+// A point farther than MIX_FAR panel radii from the panel: the Rankine integrals by the panel's 3 x 3
+// Gauss rule (the rule the closed forms give way to beyond 1000 radii), in FP32 on FP64 differences.
+// The rule's error falls as (radius / distance)^6, below FP32 rounding at 20 radii.
+constexpr double MIX_FAR = 20.0;
+
+__device__ __forceinline__ void rankine_gauss_f32(const PanelsView& pv, int j, const PanelRegs& p, const double* x,
+                                                  double& S, double& D) {
+    const float n0 = (float)p.n[0], n1 = (float)p.n[1], n2 = (float)p.n[2];
+    float s = 0.f, dd = 0.f;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const float r0 = (float)(x[0] - pv.at(P_GX + 3 * k, j));
+        const float r1 = (float)(x[1] - pv.at(P_GX + 3 * k + 1, j));
+        const float r2 = (float)(x[2] - pv.at(P_GX + 3 * k + 2, j));
+        const float w = (float)pv.at(P_GW + k, j);
+        const float ir = rsqrtf(__fmaf_rn(r0, r0, __fmaf_rn(r1, r1, r2 * r2)));
+        const float wi = w * ir;
+        s += wi;
+        dd = __fmaf_rn(wi * ir * ir, __fmaf_rn(n0, r0, __fmaf_rn(n1, r1, n2 * r2)), dd);
+    }
+    S = s;
+    D = dd;
+}
+
+// Rankine integrals at x: the closed forms, or the FP32 rule for a far point (mixed form only).
+template <bool MIXED>
+__device__ __forceinline__ void rankine_at(const PanelsView& pv, int j, const PanelRegs& p, const double* x, double& S,
+                                           double& D) {
+    if constexpr (MIXED) {
+        const double t0 = x[0] - p.c[0], t1 = x[1] - p.c[1], t2 = x[2] - p.c[2];
+        const double far = MIX_FAR * p.radius;
+        if (t0 * t0 + t1 * t1 + t2 * t2 > far * far) {
+            rankine_gauss_f32(pv, j, p, x, S, D);
+            return;
+        }
+    }
+    rankine(pv, j, p, x, S, D);
+}
+
+// log_gauss with the integrand log(R - dz) and its normal derivative in FP32 (positions, weights and
+// sums in FP64): R - dz = R + |dz| for an image above the panel, so no cancellation.
+__device__ inline void log_gauss_f32(const PanelRegs& p, const double* image, int order, double& L, double& Ld) {
+    double m[4][3];
+    panel_map(p, m);
+    const float n0 = (float)p.n[0], n1 = (float)p.n[1], n2 = (float)p.n[2];
+    double l = 0.0, ld = 0.0;
+    for (int i = 0; i < order; i++)
+        for (int j = 0; j < order; j++) {
+            double xi[3], jac;
+            bilinear(m, c_glx[order][i], c_glx[order][j], xi, jac);
+            const float d0 = (float)(xi[0] - image[0]), d1 = (float)(xi[1] - image[1]), d2 = (float)(xi[2] - image[2]);
+            const float R = sqrtf(__fmaf_rn(d0, d0, __fmaf_rn(d1, d1, d2 * d2)));
+            const float den = R - d2;
+            const float psi = logf(den);
+            const float dpsi = (__fmaf_rn(d0, n0, __fmaf_rn(d1, n1, d2 * n2)) / R - n2) / den;
+            const double ww = c_glw[order][i] * c_glw[order][j] * jac;
+            l += ww * (double)psi;
+            ld += ww * (double)dpsi;
+        }
+    L = l;
+    Ld = ld;
+}
+
 // lo_static.rs:47-55 log_pair
 __device__ __forceinline__ bool log_pair(const PanelRegs& p, const double* x, double tol) {
     double dx = x[0] - p.c[0], dy = x[1] - p.c[1], zz = fabs(x[2] + p.c[2]);
@@ -335,6 +399,9 @@ __device__ inline double log_in_plane(const PanelRegs& p, const double* x) {
 }
 
 // One (row k, panel j) pair: rs, rd and (unless adaptive) dl, dd.  lo_static.rs:59-119
+// MIXED: the mixed form's variant (far Rankine points and the order-4 log rule in FP32, above); the
+// FP64 form runs the reference's arithmetic to the bit.
+template <bool MIXED>
 __global__ void __launch_bounds__(256) k_statics(PanelsView pv, double depth, int logint, double tol,
                                                  double* __restrict__ st, int32_t* __restrict__ work,
                                                  int32_t* __restrict__ nwork, int work_cap) {
@@ -347,18 +414,18 @@ __global__ void __launch_bounds__(256) k_statics(PanelsView pv, double depth, in
     double x[3] = {pv.at(P_C + 0, k), pv.at(P_C + 1, k), pv.at(P_C + 2, k)};
     double xb[3] = {x[0], x[1], -x[2]};
     double s0, d0, sb, db;
-    rankine(pv, j, p, x, s0, d0);
-    rankine(pv, j, p, xb, sb, db);
+    rankine_at<MIXED>(pv, j, p, x, s0, d0);
+    rankine_at<MIXED>(pv, j, p, xb, sb, db);
     double sr = s0 + sb, dr = d0 + db;
     if (depth > 0.0) {
         double h = depth;
         double p1[3] = {x[0], x[1], -x[2] - 2.0 * h}, p3[3] = {x[0], x[1], x[2] + 2.0 * h};
         double p4[3] = {x[0], x[1], x[2] - 2.0 * h}, p5[3] = {x[0], x[1], -x[2] - 4.0 * h};
         double s2, d2, s4, d4, s5, d5, s6, d6;
-        rankine(pv, j, p, p1, s2, d2);
-        rankine(pv, j, p, p3, s4, d4);
-        rankine(pv, j, p, p4, s5, d5);
-        rankine(pv, j, p, p5, s6, d6);
+        rankine_at<MIXED>(pv, j, p, p1, s2, d2);
+        rankine_at<MIXED>(pv, j, p, p3, s4, d4);
+        rankine_at<MIXED>(pv, j, p, p4, s5, d5);
+        rankine_at<MIXED>(pv, j, p, p5, s6, d6);
         sr += (s2 + s4) + s5 + s6;
         dr += (d2 + d4) + d5 + d6;
     }
@@ -376,7 +443,10 @@ __global__ void __launch_bounds__(256) k_statics(PanelsView pv, double depth, in
         int order = log_order(p, xb);
         if (order > 0) {
             double L, Ld, psi, dpsi;
-            log_gauss(p, xb, order, L, Ld);
+            if (MIXED && order == 4)
+                log_gauss_f32(p, xb, order, L, Ld);
+            else
+                log_gauss(p, xb, order, L, Ld);
             psi_terms(p.c, xb, p.n, psi, dpsi);
             dl = L - p.area * psi;
             dd = Ld - p.area * dpsi;
@@ -544,9 +614,12 @@ void launch_panel_geometry(int N, const double* verts, const int32_t* kind, doub
 }
 
 void launch_statics(const PanelsView& pv, double depth, int logint, double tol, double* st, int32_t* work,
-                    int32_t* nwork, int work_cap, cudaStream_t s) {
+                    int32_t* nwork, int work_cap, cudaStream_t s, bool mixed) {
     dim3 grid((pv.N + 31) / 32, (pv.N + 7) / 8);
-    k_statics<<<grid, dim3(32, 8), 0, s>>>(pv, depth, logint, tol, st, work, nwork, work_cap);
+    if (mixed)
+        k_statics<true><<<grid, dim3(32, 8), 0, s>>>(pv, depth, logint, tol, st, work, nwork, work_cap);
+    else
+        k_statics<false><<<grid, dim3(32, 8), 0, s>>>(pv, depth, logint, tol, st, work, nwork, work_cap);
 }
 
 void launch_statics_adaptive(const PanelsView& pv, const int32_t* work, int nwork, double* st, cudaStream_t s) {
