@@ -186,6 +186,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     double2* b = (double2*)get(WS_B, (size_t)nrhs * Np * B * 16);
     double2* x = (double2*)get(WS_XM, (size_t)nrhs * Np * B * 16);
     float2* r = (float2*)get(WS_R, (size_t)nrhs * Np * B * 8);
+    float2* rs = (float2*)get(WS_RS, (size_t)nrhs * Np * B * 8);  // a residual kept for r - A d
     double* norms = (double*)get(WS_NORMS, IR_MAX_IT * 2 * (size_t)B * 8);  // [iteration][batch][2]
     int* err = (int*)get(WS_ERR, sizeof(int));
     int* tctrl = (int*)get(WS_TRI_CTRL, sizeof(int) * (1 + (size_t)B));  // the triangular sweeps' tickets
@@ -283,6 +284,39 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         return true;
     };
     const int nz_tma = (N + GV_CHUNK - 1) / GV_CHUNK;
+    for (auto fn : {(const void*)k_cgemv32_tma<8>, (const void*)k_cgemv32_tma<10>, (const void*)k_cgemv32_tma<12>,
+                    (const void*)k_cgemv32_tma<16>})
+        cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gv32_smem_bytes<16>());
+    // r = rk - M d with the complex64 correction d (FP32 products, FP64 sums; up to 16 columns): the
+    // residual after a correction that is small against the solution
+    auto gemv32 = [&](const float* Mm, const float2* dv, const float2* rk, float2* out, int nb) {
+        CUtensorMap mM, mD;
+        const uint64_t dm[4] = {(uint64_t)Np, (uint64_t)Np, 2, (uint64_t)nb};
+        const uint64_t sm[3] = {(uint64_t)Np * 4, NP2 * 4, MB * 4};
+        const uint32_t bm[4] = {GV_ROWS, GV_COLS, 1, 1};
+        const int nr = nrhs <= 8 ? 8 : nrhs <= 10 ? 10 : nrhs <= 12 ? 12 : 16;
+        const uint64_t dd[4] = {2 * (uint64_t)Np, (uint64_t)nrhs, (uint64_t)nb, 1};
+        const uint64_t sd[3] = {(uint64_t)Np * 8, (uint64_t)nrhs * Np * 8, (uint64_t)nb * nrhs * Np * 8};
+        const uint32_t bd[4] = {2 * GV_COLS, (uint32_t)nr, 1, 1};
+        if (!make_map_box(&mM, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)Mm, dm, sm, bm) ||
+            !make_map_box(&mD, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)dv, dd, sd, bd))
+            return false;
+        P.begin(s);
+        dim3 g((N + GV_ROWS - 1) / GV_ROWS, nb, nz_tma);
+        if (nr == 8)
+            k_cgemv32_tma<8><<<g, GV_THREADS, gv32_smem_bytes<8>(), s>>>(mM, mD, N, nrhs, part, nb, err);
+        else if (nr == 10)
+            k_cgemv32_tma<10><<<g, GV_THREADS, gv32_smem_bytes<10>(), s>>>(mM, mD, N, nrhs, part, nb, err);
+        else if (nr == 12)
+            k_cgemv32_tma<12><<<g, GV_THREADS, gv32_smem_bytes<12>(), s>>>(mM, mD, N, nrhs, part, nb, err);
+        else
+            k_cgemv32_tma<16><<<g, GV_THREADS, gv32_smem_bytes<16>(), s>>>(mM, mD, N, nrhs, part, nb, err);
+        k_gemv_reduce<float2, float2><<<dim3((unsigned)(((size_t)nrhs * N + 255) / 256), nb), 256, 0, s>>>(
+            N, nrhs, nb, nz_tma, part, rk, Np, out, Np);
+        P.end(KF_MIXED_RESIDUAL, 8.0 * (double)N * N * nb, s);
+        *launches += 2;
+        return true;
+    };
     auto gemv = [&](const float* Mm, const double2* xv, int ldx, const double2* bias, auto* out, int nb, int fam) {
         P.begin(s);
         dim3 g((N + 127) / 128, nb, nz);
@@ -582,11 +616,16 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 solve_end().record(s);
             };
             // the first `guess` corrections and the forces without waiting on the host, then one look
-            // at all the norms; further corrections (and the forces again) only when they fall short
+            // at all the norms; further corrections (and the forces again) only when they fall short.
+            // The residual after the first correction is b - A x with FP64 products; after a later one
+            // (|d| ~ 1e-3 |x| and smaller) it is r - A d with FP32 products (the r before the
+            // correction kept in rs); the host-driven corrections beyond `guess` use b - A x again.
             const int guess = std::min(std::max(ir_guess(), 2), IR_MAX_IT);
             for (int i = 0; i < guess; i++) {
+                const bool more = i + 1 < guess, inc = more && i >= 1 && nrhs <= 16 && rs;
+                if (inc) cudaMemcpyAsync(rs, r, sizeof(float2) * nrhs * Np * nb, cudaMemcpyDeviceToDevice, s);
                 correction(i);
-                if (i + 1 < guess) gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL);
+                if (more && !(inc && gemv32(A32, r, rs, r, nb))) gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL);
             }
             cudaMemcpyAsync(hn, norms, sizeof(double) * 2 * nb * guess, cudaMemcpyDeviceToHost, s);
             t.stop();

@@ -609,6 +609,28 @@ __global__ void __launch_bounds__(128) k_cgemv_part(int N, int Np, size_t bstrid
 // chunk of columns n, 16 columns per stage (both FP32 planes, 32 KB, and the 16 complex entries of
 // every right-hand side), GV_STAGES stages in flight from a producer warp, so the bytes in flight do
 // not depend on registers; FP64 accumulation as above.
+// Packed FP32 pairs (fma.rn.f32x2: two FP32 FMAs per instruction).  A complex multiply-add
+// acc += m v is two packed FMAs: acc += (m.re, m.re) (v.re, v.im), then acc += (-m.im, m.im) (v.im, v.re);
+// the right-hand sides are kept in shared memory as {re, im, im, re} so one 16-byte load gives both
+// orders.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2pack(float a, float b) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ float2 f2unpack(f32x2 r) {
+    float2 v;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+    return v;
+}
+__device__ __forceinline__ f32x2 ffma2(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ float4 dup_swap(float2 v) { return make_float4(v.x, v.y, v.y, v.x); }
+
 constexpr int GV_ROWS = 256, GV_COLS = 16, GV_STAGES = 3, GV_CHUNK = 1024;
 constexpr int GV_WORKERS = GV_ROWS / 2;
 constexpr int GV_THREADS = GV_WORKERS + 32;
@@ -708,6 +730,118 @@ __global__ void __launch_bounds__(GV_THREADS) k_cgemv_tma(const __grid_constant_
         }
 }
 
+// The same product with a complex64 vector d (a refinement correction): part = M d over column chunks,
+// each product and each 16-column sum in FP32, the sums added into FP64.  For a correction d that is
+// small against the solution (|d| ~ 1e-3 |x| after the first), FP32 products put errors of ~1e-10 of
+// |A x| into the residual r - M d, far below what the refinement converges to.
+template <int NR>
+__host__ __device__ constexpr size_t gv32_tx_bytes() {
+    return (size_t)2 * GV_COLS * GV_ROWS * 4 + (size_t)NR * GV_COLS * 8;
+}
+template <int NR>
+__host__ __device__ constexpr size_t gv32_stage_bytes() {
+    return (gv32_tx_bytes<NR>() + 1023) / 1024 * 1024;
+}
+template <int NR>
+__host__ __device__ constexpr size_t gv32_smem_bytes() {
+    return 1024 + GV_STAGES * gv32_stage_bytes<NR>() + 128;
+}
+
+template <int NR>
+__global__ void __launch_bounds__(GV_THREADS) k_cgemv32_tma(const __grid_constant__ CUtensorMap mapM,
+                                                               const __grid_constant__ CUtensorMap mapD, int N,
+                                                               int nrhs, double2* __restrict__ part, int F,
+                                                               int* __restrict__ err) {
+    extern __shared__ uint8_t gv_raw[];
+    uint8_t* base = align1024(gv_raw);
+    uint64_t* full = reinterpret_cast<uint64_t*>(base + GV_STAGES * gv32_stage_bytes<NR>());
+    uint64_t* empty = full + GV_STAGES;
+    const int f = blockIdx.y, z = blockIdx.z;
+    const int k0 = blockIdx.x * GV_ROWS;
+    const int nbeg = z * GV_CHUNK, nend = min(N, nbeg + GV_CHUNK);
+    const int nst = (nend - nbeg + GV_COLS - 1) / GV_COLS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < GV_STAGES; s++) {
+            tc::mbar_init(&full[s], 1);
+            tc::mbar_init(&empty[s], GV_WORKERS / 32);
+        }
+        tc::fence_barrier_init();
+    }
+    __syncthreads();
+    if (warp == GV_WORKERS / 32) {
+        if (lane == 0) {
+            tc::prefetch_tensormap(&mapM);
+            tc::prefetch_tensormap(&mapD);
+            for (int si = 0; si < nst; si++) {
+                const int s = si % GV_STAGES;
+                if (si >= GV_STAGES && !tc::mbar_wait(&empty[s], ((si / GV_STAGES) - 1) & 1)) {
+                    atomicExch(err, 6);
+                    break;
+                }
+                uint8_t* st = base + s * gv32_stage_bytes<NR>();
+                const int n0 = nbeg + si * GV_COLS;
+                tc::mbar_arrive_expect_tx(&full[s], (uint32_t)gv32_tx_bytes<NR>());
+                tc::tma_load_4d(st, &mapM, &full[s], k0, n0, 0, f);
+                tc::tma_load_4d(st + GV_COLS * GV_ROWS * 4, &mapM, &full[s], k0, n0, 1, f);
+                tc::tma_load_4d(st + 2 * GV_COLS * GV_ROWS * 4, &mapD, &full[s], 2 * n0, 0, f, 0);
+            }
+        }
+        return;
+    }
+    double2 acc[NR], acd[NR];  // rows k0 + t and k0 + t + GV_WORKERS
+#pragma unroll
+    for (int c = 0; c < NR; c++) acc[c] = acd[c] = make_double2(0.0, 0.0);
+    const int t = threadIdx.x;
+    for (int si = 0; si < nst; si++) {
+        const int s = si % GV_STAGES;
+        if (!tc::mbar_wait(&full[s], (si / GV_STAGES) & 1)) {
+            atomicExch(err, 7);
+            break;
+        }
+        const uint8_t* st = base + s * gv32_stage_bytes<NR>();
+        const float* sMr = reinterpret_cast<const float*>(st);
+        const float* sMi = sMr + GV_COLS * GV_ROWS;
+        const float2* sd = reinterpret_cast<const float2*>(st + 2 * GV_COLS * GV_ROWS * 4);  // [NR][GV_COLS]
+        const int lim = min(GV_COLS, nend - (nbeg + si * GV_COLS));
+        f32x2 a0[NR], a1[NR];
+#pragma unroll
+        for (int c = 0; c < NR; c++) a0[c] = a1[c] = f2pack(0.f, 0.f);
+#pragma unroll 4
+        for (int j = 0; j < lim; j++) {
+            const float mr = sMr[j * GV_ROWS + t], mi = sMi[j * GV_ROWS + t];
+            const float nr = sMr[j * GV_ROWS + t + GV_WORKERS], ni = sMi[j * GV_ROWS + t + GV_WORKERS];
+            const f32x2 m0 = f2pack(mr, mr), q0 = f2pack(-mi, mi), m1 = f2pack(nr, nr), q1 = f2pack(-ni, ni);
+#pragma unroll
+            for (int c = 0; c < NR; c++) {
+                const float2 v = sd[c * GV_COLS + j];
+                const f32x2 vv = f2pack(v.x, v.y), vs = f2pack(v.y, v.x);
+                a0[c] = ffma2(m0, vv, a0[c]);
+                a0[c] = ffma2(q0, vs, a0[c]);
+                a1[c] = ffma2(m1, vv, a1[c]);
+                a1[c] = ffma2(q1, vs, a1[c]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < NR; c++) {
+            const float2 u0 = f2unpack(a0[c]), u1 = f2unpack(a1[c]);
+            acc[c].x += (double)u0.x;
+            acc[c].y += (double)u0.y;
+            acd[c].x += (double)u1.x;
+            acd[c].y += (double)u1.y;
+        }
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[s]);
+    }
+    const int k = k0 + t, kd = k + GV_WORKERS;
+#pragma unroll
+    for (int c = 0; c < NR; c++)
+        if (c < nrhs) {
+            if (k < N) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
+            if (kd < N) part[(((size_t)z * F + f) * nrhs + c) * N + kd] = acd[c];
+        }
+}
+
 template <class T>
 __device__ __forceinline__ T make_out(double x, double y);
 template <>
@@ -719,9 +853,12 @@ __device__ __forceinline__ float2 make_out<float2>(double x, double y) {
     return make_float2((float)x, (float)y);
 }
 
-template <class T>
+__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2((double)v.x, (double)v.y); }
+
+template <class T, class BT = double2>
 __global__ void k_gemv_reduce(int N, int nrhs, int F, int nz, const double2* __restrict__ part,
-                              const double2* __restrict__ bias, int ldb, T* __restrict__ out, int ldo) {
+                              const BT* __restrict__ bias, int ldb, T* __restrict__ out, int ldo) {
     const int f = blockIdx.y;
     const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (size_t)nrhs * N) return;
@@ -732,7 +869,7 @@ __global__ void k_gemv_reduce(int N, int nrhs, int F, int nz, const double2* __r
         sr += v.x;
         si += v.y;
     }
-    double2 b = bias ? bias[((size_t)f * nrhs + c) * ldb + k] : make_double2(0.0, 0.0);
+    double2 b = bias ? to_d2(bias[((size_t)f * nrhs + c) * ldb + k]) : make_double2(0.0, 0.0);
     out[((size_t)f * nrhs + c) * ldo + k] = make_out<T>(b.x - sr, b.y - si);
 }
 
@@ -746,27 +883,6 @@ __global__ void k_gemv_reduce(int N, int nrhs, int F, int nz, const double2* __r
 constexpr int TB = 128;
 constexpr int TRI_THREADS = 256;
 
-// Packed FP32 pairs (fma.rn.f32x2: two FP32 FMAs per instruction).  A complex multiply-add
-// acc += m v is two packed FMAs: acc += (m.re, m.re) (v.re, v.im), then acc += (-m.im, m.im) (v.im, v.re);
-// the right-hand sides are kept in shared memory as {re, im, im, re} so one 16-byte load gives both
-// orders.
-typedef unsigned long long f32x2;
-__device__ __forceinline__ f32x2 f2pack(float a, float b) {
-    f32x2 r;
-    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
-    return r;
-}
-__device__ __forceinline__ float2 f2unpack(f32x2 r) {
-    float2 v;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
-    return v;
-}
-__device__ __forceinline__ f32x2 ffma2(f32x2 a, f32x2 b, f32x2 c) {
-    f32x2 d;
-    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-    return d;
-}
-__device__ __forceinline__ float4 dup_swap(float2 v) { return make_float4(v.x, v.y, v.y, v.x); }
 
 // The diagonal block of U^T (upper_t) or L^T, solved by its stored inverse: y_b = D^T r_b with
 // D = U_bb^-1 (upper part of the stored block, with the diagonal) or L_bb^-1 (lower part, unit
