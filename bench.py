@@ -44,7 +44,7 @@ WORKLOAD = "cylinder r=1 m d=0.5 m, 4096 panels (64x32 side + 64x32 bottom), h=5
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one launch of a kernel family on the
 # benchmark workload, from an ncu capture of the 8-frequency medium case scaled by 5 (every byte of
 # the assembly scales with the frequencies of the launch).
-DRAM_TRAFFIC = {("mixed", "assemble"): 32.1e9}
+DRAM_TRAFFIC = {("mixed", "assemble"): 32.5e9}
 
 CASE_LABELS = {
     "c2": WORKLOAD,
