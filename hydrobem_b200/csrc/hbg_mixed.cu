@@ -109,8 +109,8 @@ inline int& ir_guess() {
 // host thread (kept across solves).
 constexpr int LU_GROUPS = 3;
 struct SideStreams {
-    cudaStream_t s[LU_GROUPS] = {};
-    cudaEvent_t fork = nullptr, join[LU_GROUPS] = {};
+    cudaStream_t s[LU_GROUPS + 1] = {};  // the LU groups, then the right-hand sides
+    cudaEvent_t fork = nullptr, join[LU_GROUPS + 1] = {};
     bool ok = false;
 };
 static SideStreams& side_streams() {
@@ -121,7 +121,7 @@ static SideStreams& side_streams() {
     SideStreams& x = t[d];
     if (!x.ok) {
         bool ok = true;
-        for (int i = 0; i < LU_GROUPS; i++) {
+        for (int i = 0; i <= LU_GROUPS; i++) {
             ok = ok && cudaStreamCreateWithFlags(&x.s[i], cudaStreamNonBlocking) == cudaSuccess;
             ok = ok && cudaEventCreateWithFlags(&x.join[i], cudaEventDisableTiming) == cudaSuccess;
         }
@@ -259,7 +259,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gv_smem_bytes<16>());
     // the TMA form for up to 16 right-hand sides (its maps cover exactly the matrices and vectors
     // of the batch); the register form otherwise
-    auto gemv_tma = [&](const float* Mm, const double2* xv, int ldx, int nb, int nzt) -> bool {
+    auto gemv_tma = [&](const float* Mm, const double2* xv, int ldx, int nb, int nzt, cudaStream_t s) -> bool {
         if (nrhs > 16) return false;
         CUtensorMap mM, mX;
         const uint64_t dm[4] = {(uint64_t)Np, (uint64_t)Np, 2, (uint64_t)nb};
@@ -317,11 +317,12 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         *launches += 2;
         return true;
     };
-    auto gemv = [&](const float* Mm, const double2* xv, int ldx, const double2* bias, auto* out, int nb, int fam) {
+    auto gemv = [&](const float* Mm, const double2* xv, int ldx, const double2* bias, auto* out, int nb, int fam,
+                    cudaStream_t s) {
         P.begin(s);
         dim3 g((N + 127) / 128, nb, nz);
         int nzr = nz;
-        if (gemv_tma(Mm, xv, ldx, nb, nz_tma))
+        if (gemv_tma(Mm, xv, ldx, nb, nz_tma, s))
             nzr = nz_tma;
         else if (nrhs <= 8)
             k_cgemv_part<8><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
@@ -440,8 +441,6 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             P.begin(s);
             launch_boundary(pv, nb, dfi, H, dheads, depth, opt.gravity, u, phiI, s);
             P.end(KF_BOUNDARY, 0.0, s);
-            cudaMemsetAsync(b, 0, sizeof(double2) * nrhs * Np * nb, s);
-            gemv(S32, u, N, nullptr, b, nb, KF_RHS);
             *launches += 1 + (Np > N);
             t.stop();
         }
@@ -562,6 +561,12 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             }
             cudaEventRecord(side.fork, s);
             for (int i = 0; i < nh; i++) cudaStreamWaitEvent(hs[i].st, side.fork, 0);
+            // the right-hand sides b = -S u on their own stream, beside the LU (the refinement needs them)
+            cudaStream_t srhs = side.s[LU_GROUPS];
+            cudaStreamWaitEvent(srhs, side.fork, 0);
+            cudaMemsetAsync(b, 0, sizeof(double2) * nrhs * Np * nb, srhs);
+            gemv(S32, u, N, nullptr, b, nb, KF_RHS, srhs);
+            cudaEventRecord(side.join[LU_GROUPS], srhs);
             int K0 = 0;
             for (; K0 + 2 * NBL <= Np; K0 += 2 * NBL)
                 for (int i = 0; i < nh; i++) outer_step(hs[i], K0);
@@ -571,6 +576,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 cudaEventRecord(side.join[i], hs[i].st);
                 cudaStreamWaitEvent(s, side.join[i], 0);
             }
+            cudaStreamWaitEvent(s, side.join[LU_GROUPS], 0);
             t.stop();
         }
         // ---- refinement: x_{i+1} = x_i + A^-1 (b - A x_i), A^-1 by the TF32 factors, residuals in FP64
@@ -625,7 +631,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 const bool more = i + 1 < guess, inc = more && i >= 1 && nrhs <= 16 && rs;
                 if (inc) cudaMemcpyAsync(rs, r, sizeof(float2) * nrhs * Np * nb, cudaMemcpyDeviceToDevice, s);
                 correction(i);
-                if (more && !(inc && gemv32(A32, r, rs, r, nb))) gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL);
+                if (more && !(inc && gemv32(A32, r, rs, r, nb))) gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL, s);
             }
             cudaMemcpyAsync(hn, norms, sizeof(double) * 2 * nb * guess, cudaMemcpyDeviceToHost, s);
             t.stop();
@@ -651,7 +657,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 // further corrections, one host look each: no residual after the one that meets the test
                 EventTimer t2(s, &prof[3]);
                 for (it = guess; it < IR_MAX_IT; it++) {
-                    gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL);
+                    gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL, s);
                     correction(it);
                     cudaMemcpyAsync(hn + (size_t)it * 2 * nb, norms + (size_t)it * 2 * nb, sizeof(double) * 2 * nb,
                                     cudaMemcpyDeviceToHost, s);
