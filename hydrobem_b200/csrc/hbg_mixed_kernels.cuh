@@ -241,11 +241,11 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
 // [F][2 NBL][2 NBL]) and both inverses per block for the triangular solves.  A pivot of modulus
 // below 1e-30 sets err (the mixed form then reports the frequency; the FP64 form pivots).
 //
-// Blocked by 32 columns: per panel, four warps factor the 32 columns (a lane per column, rows
-// shared round-robin, one named barrier per pivot), one warp each inverts the panel's 32 x 32 unit
-// lower and upper diagonal blocks (warp-synchronous, into a scratch), then all threads form
-// U12 = L_pp^-1 A12 and the trailing update A22 -= L21 U12.  The inverses of the whole 128 x 128
-// factors are then assembled from the diagonal-block inverses in three block-column stages.
+// Blocked by 32 columns: per panel, all sixteen warps factor the 32 columns (a lane per column, rows
+// shared round-robin, one CTA barrier per pivot), then U12 = L_pp^-1 A12 by forward substitution (a
+// warp per column) and the trailing update A22 -= L21 U12.  After the panels, eight warps invert the
+// four 32 x 32 unit lower and four upper diagonal blocks at once (warp-synchronous, into a scratch),
+// and the inverses of the whole 128 x 128 factors are assembled from them in three block-column stages.
 constexpr int DF_THREADS = 512, DF_LD = NBL + 1, DF_BLK = 32, DF_NB = NBL / DF_BLK, DF_SLD = DF_BLK + 1;
 constexpr size_t df_smem_bytes() { return (size_t)(NBL * DF_LD + 2 * DF_NB * DF_BLK * DF_SLD) * sizeof(float2); }
 
@@ -355,32 +355,24 @@ __global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ 
             }
         }
         __syncthreads();
-        // ---- inverses of the panel's diagonal blocks (warps 0 and 1)
-        if (warp == 0) df_inv_lower32(blk + c0 * DF_LD + c0, Li + pb * DF_BLK * DF_SLD);
-        if (warp == 1) df_inv_upper32(blk + c0 * DF_LD + c0, Ui + pb * DF_BLK * DF_SLD);
-        __syncthreads();
         const int n2 = NBL - c0 - DF_BLK;
         if (n2 == 0) break;
-        // ---- U12 = L_pp^-1 A12 (rows c0 .. c0 + 31, columns c0 + 32 ..): into registers, then back
+        // ---- U12 = L_pp^-1 A12 (rows c0 .. c0 + 31, columns c0 + 32 ..) by forward substitution with the
+        // unit lower L_pp: a warp per column, lane = row, the lane's row of L_pp in registers, each solved
+        // entry broadcast by shuffles
         {
-            const float2* Y = Li + pb * DF_BLK * DF_SLD;
-            constexpr int MAXE = (DF_BLK * (NBL - DF_BLK) + DF_THREADS - 1) / DF_THREADS;  // 6
-            float2 v[MAXE];
+            float2 lrow[DF_BLK];
 #pragma unroll
-            for (int e = 0; e < MAXE; e++) {
-                const int t = threadIdx.x + e * DF_THREADS;
-                v[e] = make_float2(0.f, 0.f);
-                if (t < DF_BLK * n2) {
-                    const int i = t / n2, cc = c0 + DF_BLK + t % n2;
-                    v[e] = cdot4(0, i + 1, [&](int k) { return Y[i * DF_SLD + k]; },
-                                 [&](int k) { return blk[(c0 + k) * DF_LD + cc]; });
+            for (int j = 0; j < DF_BLK; j++)
+                lrow[j] = j < lane ? blk[(c0 + lane) * DF_LD + c0 + j] : make_float2(0.f, 0.f);
+            for (int cc = c0 + DF_BLK + warp; cc < NBL; cc += DF_WARPS) {
+                float2 v = blk[(c0 + lane) * DF_LD + cc];
+#pragma unroll
+                for (int j = 0; j < DF_BLK - 1; j++) {
+                    const float2 xj = make_float2(__shfl_sync(0xffffffffu, v.x, j), __shfl_sync(0xffffffffu, v.y, j));
+                    cfma_sub(v, lrow[j], xj);  // lrow[j] = 0 for j >= lane
                 }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int e = 0; e < MAXE; e++) {
-                const int t = threadIdx.x + e * DF_THREADS;
-                if (t < DF_BLK * n2) blk[(c0 + t / n2) * DF_LD + c0 + DF_BLK + t % n2] = v[e];
+                blk[(c0 + lane) * DF_LD + cc] = v;
             }
             __syncthreads();
         }
@@ -394,6 +386,12 @@ __global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ 
         }
         __syncthreads();
     }
+    // ---- inverses of the four 32 x 32 diagonal blocks of L and of U: eight warps, one block each
+    if (warp < DF_NB)
+        df_inv_lower32(blk + warp * DF_BLK * DF_LD + warp * DF_BLK, Li + warp * DF_BLK * DF_SLD);
+    else if (warp < 2 * DF_NB)
+        df_inv_upper32(blk + (warp - DF_NB) * DF_BLK * DF_LD + (warp - DF_NB) * DF_BLK,
+                       Ui + (warp - DF_NB) * DF_BLK * DF_SLD);
     // the factors back to W
     for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) {
         const int r = t / NBL, c = t % NBL;
