@@ -46,6 +46,20 @@ static bool make_map(CUtensorMap* m, void* base, uint64_t d0, uint64_t d1, uint6
            CUDA_SUCCESS;
 }
 
+// The same for FP16 rows: box {64, box_rows} (128 bytes a row, 128-byte swizzle).
+static bool make_map16(CUtensorMap* m, void* base, uint64_t d0, uint64_t d1, uint64_t d2, uint64_t d3, uint64_t s1,
+                       uint64_t s2, uint64_t s3, uint32_t box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[4] = {d0, d1, d2, d3};
+    cuuint64_t strides[3] = {s1, s2, s3};
+    cuuint32_t box[4] = {64, box_rows, 1, 1};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 4, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
 // Rows of 2 w floats viewed as [rows][2][w]: dims {w, 2, rows, d3}, box {32, 1, box_rows, 1}, the
 // 128-byte swizzle (the same shared-memory tile as make_map's).
 static bool make_map_split(CUtensorMap* m, void* base, uint64_t w, uint64_t rows, uint64_t d3, uint64_t row_stride,
@@ -178,6 +192,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     // a later update's B operand: rows of 4 NBL (two 128-row blocks of U) for the 256-deep trailing update
     const size_t p3size = 2 * prep;
     float* P3 = (float*)get(WS_P3, p3size * B * 4);
+    // FP16 operands of the trailing update: P3's 4 NBL-wide layout, and the L rows of the outer step's
+    // two block columns beyond its panel, [rows][Lr (2 NBL) | Li (2 NBL)]
+    __half* P3h = (__half*)get(WS_P3H, p3size * B * 2);
+    const size_t l16_rows = std::max<size_t>(Np > 2 * NBL ? Np - 2 * NBL : 0, GBM);
+    __half* L16 = (__half*)get(WS_L16, l16_rows * 4 * NBL * B * 2);
     float* PL = (float*)get(WS_PL, (size_t)NBL * 2 * NBL * B * 4);
     float* PU = (float*)get(WS_PU, (size_t)4 * NBL * NBL * B * 4);
     float2* DINV = (float2*)get(WS_DINV, nblk * NBL * NBL * B * sizeof(float2));
@@ -207,7 +226,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     if (!okb) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
     last_surrogate_pairs() = 0;
     // ---- tensor maps (whole batch; the batch index is the 4th coordinate)
-    CUtensorMap mapW, mapPL, mapPU, mapP2, mapP3, mapP3w, mapP3h;
+    CUtensorMap mapW, mapPL, mapPU, mapP2, mapP3, mapP3h, mapL16, mapP3w16;
     const uint64_t fb = 4;  // bytes per float
     bool okm = make_map(&mapW, W, Np, Np, 2, B, Np * fb, NP2 * fb, MB * fb, GBM) &&
                make_map(&mapPL, PL, 2 * NBL, NBL, 1, B, 2 * NBL * fb, (uint64_t)NBL * 2 * NBL * fb,
@@ -218,11 +237,14 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                // P3 as rows of 2 NBL (one 128-row block of U), of 4 NBL (two blocks), and the 4 NBL rows
                // viewed as [2][2 NBL] halves (the first block alone: x = kk % NBL, half = kk / NBL)
                make_map(&mapP3, P3, 2 * NBL, prep_rows, 1, B, 2 * NBL * fb, p3size * fb, p3size * fb, GBN) &&
-               make_map(&mapP3w, P3, 4 * NBL, prep_rows, 1, B, 4 * NBL * fb, p3size * fb, p3size * fb, GBN) &&
+               make_map16(&mapP3w16, P3h, 4 * NBL, prep_rows, 1, B, 4 * NBL * 2, p3size * 2, p3size * 2, GBN) &&
+               make_map16(&mapL16, L16, 4 * NBL, l16_rows, 1, B, 4 * NBL * 2, l16_rows * 4 * NBL * 2,
+                          l16_rows * 4 * NBL * 2, GBM) &&
                make_map_split(&mapP3h, P3, 2 * NBL, prep_rows, B, 4 * NBL * fb, p3size * fb, GBN);
     if (!okm) MIXED_FAIL(HB_ERR_INTERNAL, "tensor-map encoding failed", -1);
     const int smem = (int)gemm_smem_bytes();
-    cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_gemm_tf32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_gemm_tf32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     int dev = 0, n_sm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
@@ -384,12 +406,15 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     };
     // matrices f0 .. f0 + nb of the batch on stream st, at most cap persistent CTAs
     auto gemm = [&](const CUtensorMap& mA, const CUtensorMap& mB, GemmArgs g, int f0, int nb, cudaStream_t st,
-                    int cap) {
+                    int cap, bool f16) {
         g.batch = nb;
         g.b0 = f0;
         const int tiles = ((g.M + GBM - 1) / GBM) * ((g.Nc + GBN - 1) / GBN) * nb;
         P.begin(st);
-        k_gemm_tf32<<<std::min(tiles, cap), GEMM_THREADS, smem, st>>>(mA, mB, mapW, g);
+        if (f16)
+            k_gemm_tf32<true><<<std::min(tiles, cap), GEMM_THREADS, smem, st>>>(mA, mB, mapW, g);
+        else
+            k_gemm_tf32<false><<<std::min(tiles, cap), GEMM_THREADS, smem, st>>>(mA, mB, mapW, g);
         P.end(KF_MIXED_GEMM, 2.0 * g.M * (double)g.Nc * g.Kp * nb, st);
         (*launches)++;
     };
@@ -475,8 +500,15 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             };
             GemmArgs g0{};
             g0.err = err;
-            auto gemm_l = [&](const Half& h, int k0, int rows) {  // L(rows below the block) = M(., block k0) U_kk^-1
+            // L(rows below the block) = M(., block k0) U_kk^-1; the rows from h16_row0 on also into L16 at
+            // column offset h16_koff (0: the outer step's first block, NBL: its second)
+            auto gemm_l = [&](const Half& h, int k0, int rows, int h16_row0, int h16_koff) {
                 GemmArgs g = g0;
+                g.h16 = L16;
+                g.h16_bstride = l16_rows * 4 * NBL;
+                g.h16_ld = 4 * NBL;
+                g.h16_row0 = h16_row0;
+                g.h16_koff = h16_koff;
                 g.M = rows;
                 g.Nc = 2 * NBL;
                 g.Kp = 2 * NBL;
@@ -488,7 +520,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 g.o_row0 = k0 + NBL;
                 g.o_col0 = k0;
                 g.o_nc = NBL;
-                gemm(mapW, mapPU, g, h.f0, h.nb, h.st, h.cap);
+                gemm(mapW, mapPU, g, h.f0, h.nb, h.st, h.cap, false);
             };
             // U(rows k0..k0+NBL, columns c0..c0+ncols) = L_kk^-1 B (prepared in P2), and its block-real
             // copy into P3 (rows of ld floats, this block's rows from koff, second half at kh)
@@ -508,7 +540,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 g.p3_ld = ld;
                 g.p3_kh = kh;
                 g.p3_koff = koff;
-                gemm(mapPL, mapP2, g, h.f0, h.nb, h.st, h.cap);
+                g.p3h = ld == 4 * NBL ? P3h : nullptr;  // the trailing update's FP16 copy
+                gemm(mapPL, mapP2, g, h.f0, h.nb, h.st, h.cap, false);
             };
             // M(rows row0.., columns c0..c0+ncols) -= L(rows, columns a_x0..a_x0+a_kc) U (B operand)
             auto update = [&](const Half& h, int rows, int row0, int c0, int ncols, int a_x0, int a_kc,
@@ -526,7 +559,22 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 g.o_col0 = c0;
                 g.o_nc = ncols;
                 g.b_split = b_split;
-                gemm(mapW, mB, g, h.f0, h.nb, h.st, h.cap);
+                gemm(mapW, mB, g, h.f0, h.nb, h.st, h.cap, false);
+            };
+            // the trailing matrix (rows and columns c2.., n of each) -= [L of the step's two blocks] U13,
+            // K' = 512, FP16 operands (L16, P3h), FP32 accumulation and reduction into W
+            auto trailing = [&](const Half& h, int c2, int n) {
+                GemmArgs g = g0;
+                g.M = n;
+                g.Nc = 2 * n;
+                g.Kp = 4 * NBL;
+                g.a_planar = 0;
+                g.a_row0 = 0;
+                g.mode = 2;
+                g.o_row0 = c2;
+                g.o_col0 = c2;
+                g.o_nc = n;
+                gemm(mapL16, mapP3w16, g, h.f0, h.nb, h.st, h.cap, true);
             };
             // one outer step (columns K0 .. K0 + 2 NBL) of one half
             auto outer_step = [&](const Half& h, int K0) {
@@ -534,7 +582,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 // first block: factor, L below it, U of the second block's columns, update of the second block
                 diag(h, K0);
                 prep_row(h, K0, k1, NBL);
-                gemm_l(h, K0, Np - k1);
+                gemm_l(h, K0, Np - k1, c2, 0);
                 gemm_u(h, K0, k1, NBL, 2 * NBL, NBL, 0);
                 update(h, Np - k1, k1, k1, NBL, K0, NBL, mapP3, 0);
                 // U of the first block's rows beyond the panel (while L_KK^-1 is at hand)
@@ -545,11 +593,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 // second block
                 diag(h, k1);
                 if (n > 0) {
-                    gemm_l(h, k1, n);
+                    gemm_l(h, k1, n, c2, NBL);
                     update(h, NBL, k1, c2, n, K0, NBL, mapP3h, NBL);  // its rows beyond the panel: -= L21 U13
                     prep_row(h, k1, c2, n);
                     gemm_u(h, k1, c2, n, 4 * NBL, 2 * NBL, NBL);
-                    update(h, n, c2, c2, n, K0, 2 * NBL, mapP3w, 0);  // the trailing matrix, K' = 512
+                    trailing(h, c2, n);  // the trailing matrix, K' = 512
                 }
             };
             const int nh = std::min(LU_GROUPS, nb);
@@ -757,13 +805,14 @@ int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* 
     g.batch = 1;
     g.err = err;
     const int smem = (int)gemm_smem_bytes();
-    cudaFuncSetAttribute(k_gemm_tf32, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_gemm_tf32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_gemm_tf32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     int dev = 0, n_sm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     // fewer CTAs than tiles, so that the persistent loop and both accumulator buffers are exercised
     const int tiles = (M / GBM) * ((N + GBN - 1) / GBN);
-    k_gemm_tf32<<<std::max(1, std::min(tiles / 3, n_sm)), GEMM_THREADS, smem>>>(mA, mB, mC, g);
+    k_gemm_tf32<false><<<std::max(1, std::min(tiles / 3, n_sm)), GEMM_THREADS, smem>>>(mA, mB, mC, g);
     int herr = 0;
     cudaMemcpy(&herr, err, sizeof(int), cudaMemcpyDeviceToHost);
     cudaMemcpy(C, dC, sizeof(float) * M * N, cudaMemcpyDeviceToHost);

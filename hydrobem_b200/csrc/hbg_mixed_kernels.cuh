@@ -14,6 +14,8 @@
 // on the tensor cores (kind::tf32, FP32 accumulation); the refinement in FP64 restores the
 // accuracy of the solution (iterative refinement against the stored complex64 matrix).
 #pragma once
+#include <cuda_fp16.h>
+
 #include "hbg_tc.cuh"
 
 namespace hbg {
@@ -35,6 +37,12 @@ struct GemmArgs {
     size_t p3_bstride;
     int p3_n;
     int p3_ld, p3_kh, p3_koff;  // row length, offset of the second (imaginary-weight) half, first row of this block
+    __half* p3h;           // mode 1: an FP16 copy of the p3 scatter (same layout), or null
+    // mode 0: an FP16 copy of the output rows from h16_row0 on, [F][rows][h16_ld]: output column j' of
+    // plane p at p * (h16_ld / 2) + h16_koff + j' % o_nc, row o_row0 + i at o_row0 + i - h16_row0
+    __half* h16;
+    size_t h16_bstride;
+    int h16_ld, h16_row0, h16_koff;
     int* err;
 };
 
@@ -54,6 +62,8 @@ constexpr size_t gemm_smem_bytes() { return 1024 + GSTAGES * GEMM_STAGE_BYTES + 
 // a ring of four shared-memory boxes (128-byte swizzle, conflict-free 16-byte accesses) and write it
 // out by TMA: a store, or for the trailing update a TMA reduction that adds -acc to C in L2 (so C
 // never passes through the SM).  The epilogue of one tile overlaps the main loop of the next.
+// F16: the same pipeline on FP16 operands (kind::f16, 64 halves per 128-byte k-chunk row, packed A only).
+template <bool F16 = false>
 __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_constant__ CUtensorMap mapA,
                                                                const __grid_constant__ CUtensorMap mapB,
                                                                const __grid_constant__ CUtensorMap mapC,
@@ -71,7 +81,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = (g.M + GBM - 1) / GBM, nt = (g.Nc + GBN - 1) / GBN;
     const int ntiles = mt * nt * g.batch;
-    const int nk = g.Kp / GBK;
+    constexpr int KE = F16 ? 2 * GBK : GBK;  // operand elements per k-chunk (128 bytes a row either way)
+    const int nk = g.Kp / KE;
     if (threadIdx.x == 0) {
         for (int s = 0; s < GSTAGES; s++) {
             tc::mbar_init(&full[s], 1);
@@ -112,9 +123,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
                         break;
                     }
                     tc::mbar_arrive_expect_tx(&full[s], (uint32_t)GEMM_STAGE_BYTES);
-                    const int kk = kc * GBK;
+                    const int kk = kc * KE;
                     int ax = kk, plane = 0;
-                    if (g.a_planar) {
+                    if (!F16 && g.a_planar) {
                         ax = g.a_x0 + kk % g.a_kc;
                         plane = kk / g.a_kc;
                     }
@@ -128,7 +139,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
         }
     } else if (warp == 1) {
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_tf32(GBM, GBN);
+            const uint32_t idesc = F16 ? tc::idesc_f16(GBM, GBN) : tc::idesc_tf32(GBM, GBN);
             int kc_global = 0, it = 0;
             for (int t = blockIdx.x; t < ntiles; t += gridDim.x, it++) {
                 const int b = it & 1;
@@ -149,10 +160,16 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
                     }
                     tc::tc_fence_after();
                     const uint32_t a0 = tc::smem_u32(sA + s * GBM * GBK), b0 = tc::smem_u32(sB + s * GBN * GBK);
+                    // four MMAs per 128-byte row: K = 8 (tf32) or 16 (f16), 32 bytes apart
 #pragma unroll
-                    for (int k8 = 0; k8 < GBK / 8; k8++)
-                        tc::mma_tf32(d, tc::desc_kmajor_sw128(a0 + 32 * k8), tc::desc_kmajor_sw128(b0 + 32 * k8), idesc,
-                                     (kc | k8) != 0);
+                    for (int k8 = 0; k8 < 4; k8++) {
+                        if constexpr (F16)
+                            tc::mma_f16(d, tc::desc_kmajor_sw128(a0 + 32 * k8), tc::desc_kmajor_sw128(b0 + 32 * k8),
+                                        idesc, (kc | k8) != 0);
+                        else
+                            tc::mma_tf32(d, tc::desc_kmajor_sw128(a0 + 32 * k8), tc::desc_kmajor_sw128(b0 + 32 * k8),
+                                         idesc, (kc | k8) != 0);
+                    }
                     tc::mma_commit(&empty[s]);
                 }
                 tc::mma_commit(&tfull[b]);
@@ -197,17 +214,39 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
                     // U(kk = row, j) into the block-real K-major operand of a later update (rows 2n,
                     // p3_ld wide): row j [Ur(:, j) | -Ui(:, j)], row n + j [Ui(:, j) | Ur(:, j)]
                     float* p3f = g.p3 + (size_t)f * g.p3_bstride;
+                    __half* p3hf = g.p3h ? g.p3h + (size_t)f * g.p3_bstride : nullptr;
                     const int n = g.p3_n, kk = g.p3_koff + m0 + r, ld = g.p3_ld, kh = g.p3_kh;
 #pragma unroll
                     for (int i = 0; i < 32; i++) {
                         const int j = col + i;
+                        size_t o1, o2;
+                        float w1;
                         if (plane == 0) {
-                            p3f[(size_t)j * ld + kk] = v[i];
-                            p3f[(size_t)(n + j) * ld + kh + kk] = v[i];
+                            o1 = (size_t)j * ld + kk;
+                            o2 = (size_t)(n + j) * ld + kh + kk;
+                            w1 = v[i];
                         } else {
-                            p3f[(size_t)j * ld + kh + kk] = -v[i];
-                            p3f[(size_t)(n + j) * ld + kk] = v[i];
+                            o1 = (size_t)j * ld + kh + kk;
+                            o2 = (size_t)(n + j) * ld + kk;
+                            w1 = -v[i];
                         }
+                        p3f[o1] = w1;
+                        p3f[o2] = v[i];
+                        if (p3hf) {
+                            p3hf[o1] = __float2half_rn(w1);
+                            p3hf[o2] = __float2half_rn(v[i]);
+                        }
+                    }
+                }
+                if (g.mode == 0 && g.h16 && live && m0 + r < g.M && g.o_row0 + m0 + r >= g.h16_row0) {
+                    __half* h = g.h16 + (size_t)f * g.h16_bstride + (size_t)(g.o_row0 + m0 + r - g.h16_row0) * g.h16_ld +
+                                plane * (g.h16_ld / 2) + g.h16_koff + col;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        __half2 hv[4];
+#pragma unroll
+                        for (int e = 0; e < 4; e++) hv[e] = __floats2half2_rn(v[8 * j + 2 * e], v[8 * j + 2 * e + 1]);
+                        *reinterpret_cast<uint4*>(h + 8 * j) = *reinterpret_cast<const uint4*>(hv);
                     }
                 }
                 tc::fence_proxy_async_smem();
