@@ -410,6 +410,20 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
         if (!(pr.omegas[i] > 0.0) || !std::isfinite(pr.omegas[i]))
             throw Failure{HB_ERR_VALUE, "an omega is not positive and finite (the limits are not on this route)",
                           body_index, i};
+    // interacting bodies: 6 rigid modes each
+    const int nbod = pr.body.n_bodies > 1 ? (int)pr.body.n_bodies : 1;
+    if (pr.body.n_bodies < 0 || nbod > 64) throw Failure{HB_ERR_VALUE, "n_bodies outside 0..64", body_index};
+    if (nbod > 1 && !pr.body.panel_body) throw Failure{HB_ERR_ARGUMENT, "several bodies without panel_body", body_index};
+    if (pr.body.panel_body)
+        for (int j = 0; j < N; j++)
+            if (pr.body.panel_body[j] < 0 || pr.body.panel_body[j] >= nbod)
+                throw Failure{HB_ERR_VALUE, "a panel_body entry outside 0 .. n_bodies - 1", body_index};
+    if (pr.body.rotation_centers)
+        for (int i = 0; i < 3 * nbod; i++)
+            if (!std::isfinite(pr.body.rotation_centers[i]))
+                throw Failure{HB_ERR_VALUE, "a rotation centre is not finite", body_index};
+    const int D = 6 * nbod;
+    if (D + H > 32) throw Failure{HB_ERR_UNSUPPORTED, "more than 32 right-hand sides (6 per body and one per heading)", body_index};
     if (H > 26) throw Failure{HB_ERR_UNSUPPORTED, "more than 26 headings per solve", body_index};
     const bool fin = finite_depth(opt.depth);
     const double depth = fin ? opt.depth : 0.0;
@@ -424,7 +438,10 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
     // the statics and the assembly in the device's queue)
     Workspace& ws = workspace();
     WsBuf dverts(ws, WS_VERTS), dkind(ws, WS_KIND), dplanes(ws, WS_PLANES), dbad(ws, WS_BAD), dst(ws, WS_ST),
-        dwork(ws, WS_WORK), dnwork(ws, WS_NWORK);
+        dwork(ws, WS_WORK), dnwork(ws, WS_NWORK), dpbody(ws, WS_PBODY), drcen(ws, WS_RCEN);
+    const bool multi = nbod > 1 && pr.body.panel_body;
+    if (multi) dpbody.alloc(sizeof(int32_t) * N);
+    if (pr.body.rotation_centers) drcen.alloc(sizeof(double) * 3 * nbod);
     std::vector<int32_t> kinds(N, 0);
     if (pr.body.kinds)
         for (int j = 0; j < N; j++) {
@@ -452,6 +469,11 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
         CUDA_OK(cudaMemcpyAsync(dverts.p, pr.body.vertices, sizeof(double) * 12 * N, cudaMemcpyHostToDevice, s));
         CUDA_OK(cudaMemcpyAsync(dkind.p, kinds.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
         CUDA_OK(cudaMemcpyAsync(dbad.p, &big, sizeof big, cudaMemcpyHostToDevice, s));
+        if (multi)
+            CUDA_OK(cudaMemcpyAsync(dpbody.p, pr.body.panel_body, sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
+        if (pr.body.rotation_centers)
+            CUDA_OK(cudaMemcpyAsync(drcen.p, pr.body.rotation_centers, sizeof(double) * 3 * nbod,
+                                    cudaMemcpyHostToDevice, s));
         EventTimer t(s, &prof[0]);
         KernelProfiler& P = profiler();
         P.begin(s);
@@ -488,7 +510,8 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
     };
     // the mixed form's assembly kernels skip their work on invalid panels (the flag in device memory),
     // so that its solve runs without a host wait until the end; the FP64 form waits here
-    PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>(), dbad.as<int32_t>()};
+    PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>(), dbad.as<int32_t>(),
+                  multi ? dpbody.as<int32_t>() : nullptr, pr.body.rotation_centers ? drcen.as<double>() : nullptr, nbod};
     if (F == 0 || opt.precision != HBG_MIXED) {
         run_statics();
         CUDA_OK(cudaStreamSynchronize(s));
@@ -496,7 +519,7 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
         statics_check();
         if (F == 0) return;
     }
-    const int nrhs = 6 + H;
+    const int nrhs = D + H;
     if (opt.precision == HBG_MIXED) {
         const char* msg = "";
         int64_t fq = -1;
@@ -542,7 +565,7 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
     dheads.alloc(sizeof(double) * heads.size());
     CUDA_OK(cudaMemcpyAsync(dheads.p, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s));
     // outputs per batch: A, B [6][6], X, FK, SC [H][6]
-    const size_t out_per = 72 * sizeof(double) + 3 * (size_t)H * 6 * sizeof(double2);
+    const size_t out_per = 2 * (size_t)D * D * sizeof(double) + 3 * (size_t)H * D * sizeof(double2);
     dout.alloc(out_per * B);
     // page-locked outputs and pivot flags: their reads queue behind the work
     unsigned char* hout = static_cast<unsigned char*>(ws.host(HS_OUT, out_per * B + sizeof(int32_t) * B));
@@ -612,10 +635,10 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
             EventTimer t(s, &prof[4]);
             double* base = dout.as<double>();
             double* dAo = base;
-            double* dBo = base + 36 * (size_t)nb;
-            double2* dXo = reinterpret_cast<double2*>(base + 72 * (size_t)nb);
-            double2* dFK = dXo + (size_t)H * 6 * nb;
-            double2* dSC = dFK + (size_t)H * 6 * nb;
+            double* dBo = base + (size_t)D * D * nb;
+            double2* dXo = reinterpret_cast<double2*>(base + 2 * (size_t)D * D * nb);
+            double2* dFK = dXo + (size_t)H * D * nb;
+            double2* dSC = dFK + (size_t)H * D * nb;
             KernelProfiler& P = profiler();
             P.begin(s);
             launch_forces(pv, nb, dfi.as<FreqInfo>(), H, dX.as<double2>(), N, dphiI.as<double2>(), opt.density, dAo,
@@ -632,21 +655,22 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
         profiler().flush();
         const double* hb = reinterpret_cast<const double*>(hout);
         const double* hA = hb;
-        const double* hB = hb + 36 * (size_t)nb;
-        const double* hX = hb + 72 * (size_t)nb;
-        const double* hFK = hX + (size_t)H * 12 * nb;
-        const double* hSC = hFK + (size_t)H * 12 * nb;
+        const size_t DD = (size_t)D * D;
+        const double* hB = hb + DD * nb;
+        const double* hX = hb + 2 * DD * nb;
+        const double* hFK = hX + (size_t)H * 2 * D * nb;
+        const double* hSC = hFK + (size_t)H * 2 * D * nb;
         for (int i = 0; i < nb; i++) {
             if (info[i] != 0)
                 throw Failure{HB_ERR_NUMERICAL, "singular system matrix (zero pivot " + std::to_string(info[i]) + ")",
                               body_index, f0 + i};
-            for (int q = 0; q < 36; q++)
-                if (!std::isfinite(hA[36 * i + q]) || !std::isfinite(hB[36 * i + q]))
+            for (size_t q = 0; q < DD; q++)
+                if (!std::isfinite(hA[DD * i + q]) || !std::isfinite(hB[DD * i + q]))
                     throw Failure{HB_ERR_NUMERICAL, "non-finite solution", body_index, f0 + i};
             const size_t fo = (size_t)(f0 + i);
-            if (pr.out.added_mass) memcpy(pr.out.added_mass + fo * 36, hA + 36 * i, 36 * sizeof(double));
-            if (pr.out.radiation_damping) memcpy(pr.out.radiation_damping + fo * 36, hB + 36 * i, 36 * sizeof(double));
-            const size_t hx = (size_t)H * 12;
+            if (pr.out.added_mass) memcpy(pr.out.added_mass + fo * DD, hA + DD * i, DD * sizeof(double));
+            if (pr.out.radiation_damping) memcpy(pr.out.radiation_damping + fo * DD, hB + DD * i, DD * sizeof(double));
+            const size_t hx = (size_t)H * 2 * D;
             if (pr.out.excitation) memcpy(pr.out.excitation + fo * hx, hX + hx * i, hx * sizeof(double));
             if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));

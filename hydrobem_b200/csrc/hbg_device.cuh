@@ -72,7 +72,23 @@ struct PanelsView {
     const int32_t* kind; // 0 wet, 1 interior
     // optional: the invalid-panel flag; kernels that see it set (!= PANELS_VALID) skip their work
     const int32_t* bad = nullptr;
+    // the bodies of a multi-body problem: body index of each panel (null: all body 0), the rotation
+    // centre of each body (3 per body; null: the origin), the body count
+    const int32_t* body = nullptr;
+    const double* rcen = nullptr;
+    int nbod = 1;
     __device__ __forceinline__ bool invalid() const { return bad && *(volatile const int32_t*)bad != PANELS_VALID; }
+    // generalized normal of rigid mode `mode` (body mode / 6: surge, sway, heave, roll, pitch, yaw about
+    // its rotation centre) on panel j: zero on the panels of the other bodies
+    __device__ __forceinline__ double gen_normal(int j, int mode) const {
+        const int b = mode / 6, m = mode - 6 * (mode / 6);
+        if ((body ? body[j] : 0) != b) return 0.0;
+        const double nx = at(P_N, j), ny = at(P_N + 1, j), nz = at(P_N + 2, j);
+        if (m < 3) return m == 0 ? nx : m == 1 ? ny : nz;
+        const double cx = at(P_C, j) - (rcen ? rcen[3 * b] : 0.0), cy = at(P_C + 1, j) - (rcen ? rcen[3 * b + 1] : 0.0),
+                     cz = at(P_C + 2, j) - (rcen ? rcen[3 * b + 2] : 0.0);
+        return m == 3 ? cy * nz - cz * ny : m == 4 ? cz * nx - cx * nz : cx * ny - cy * nx;
+    }
     __device__ __forceinline__ double at(int plane, int j) const { return p[(size_t)plane * N + j]; }
 };
 

@@ -355,7 +355,7 @@ __global__ void k_boundary(PanelsView pv, int F, const FreqInfo* __restrict__ fi
     int f = blockIdx.y;
     int N = pv.N;
     if (j >= N) return;
-    const int nrhs = 6 + H;
+    const int nrad = 6 * pv.nbod, nrhs = nrad + H;
     double c[3], n[3];
     for (int d = 0; d < 3; d++) {
         c[d] = pv.at(P_C + d, j);
@@ -363,8 +363,8 @@ __global__ void k_boundary(PanelsView pv, int F, const FreqInfo* __restrict__ fi
     }
     bool wet = pv.kind[j] == 0;
     double2* uf = u + (size_t)f * nrhs * N;
-    double nj[6] = {n[0], n[1], n[2], c[1] * n[2] - c[2] * n[1], c[2] * n[0] - c[0] * n[2], c[0] * n[1] - c[1] * n[0]};
-    for (int m = 0; m < 6; m++) uf[(size_t)m * N + j] = make_double2(wet ? nj[m] : 0.0, 0.0);
+    // radiation columns: the generalized normal of each rigid mode of each body (lo_frequency.rs:236-251)
+    for (int m = 0; m < nrad; m++) uf[(size_t)m * N + j] = make_double2(wet ? pv.gen_normal(j, m) : 0.0, 0.0);
     double k = fi[f].k, w = fi[f].omega;
     double Z = exp(k * c[2]), Zz = k * Z;
     if (depth > 0.0) {
@@ -389,7 +389,7 @@ __global__ void k_boundary(PanelsView pv, int F, const FreqInfo* __restrict__ fi
         double dr = gxr * n[0] + gyr * n[1] + gzr * n[2];
         double di = gxi * n[0] + gyi * n[1] + gzi * n[2];
         phiI[((size_t)f * H + h) * N + j] = make_double2(pr, pi);
-        uf[(size_t)(6 + h) * N + j] = make_double2(wet ? -dr : 0.0, wet ? -di : 0.0);
+        uf[(size_t)(nrad + h) * N + j] = make_double2(wet ? -dr : 0.0, wet ? -di : 0.0);
     }
 }
 
@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(256) k_forces(PanelsView pv, const FreqInfo* _
                                                 double2* __restrict__ SC) {
     __shared__ double red[256];
     int f = blockIdx.x, N = pv.N;
-    int nrhs = 6 + H;
+    const int D = 6 * pv.nbod, nrhs = D + H;
     const double2* pf = phi + (size_t)f * nrhs * ldphi;
     const double2* pif = phiI + (size_t)f * H * N;
     double w = fi[f].omega;
@@ -475,29 +475,24 @@ __global__ void __launch_bounds__(256) k_forces(PanelsView pv, const FreqInfo* _
         __syncthreads();
         return r;
     };
-    // columns: c < 6 radiation (phi_c), 6 <= c < 6 + H diffraction (phi_S + phi_I), then H of phi_I
-    for (int col = 0; col < 6 + 2 * H; col++) {
-        for (int i = 0; i < 6; i++) {
+    // columns: c < D radiation (phi_c), D <= c < D + H diffraction (phi_S + phi_I), then H of phi_I;
+    // coordinates i < D: the rigid modes of every body (D = 6 per body)
+    for (int col = 0; col < D + 2 * H; col++) {
+        for (int i = 0; i < D; i++) {
             double sr = 0.0, si = 0.0;
             for (int j = threadIdx.x; j < N; j += blockDim.x) {
                 if (pv.kind[j] != 0) continue;
-                double c[3] = {pv.at(P_C, j), pv.at(P_C + 1, j), pv.at(P_C + 2, j)};
-                double n[3] = {pv.at(P_N, j), pv.at(P_N + 1, j), pv.at(P_N + 2, j)};
-                double nj = i == 0 ? n[0] : i == 1 ? n[1] : i == 2 ? n[2]
-                          : i == 3 ? c[1] * n[2] - c[2] * n[1]
-                          : i == 4 ? c[2] * n[0] - c[0] * n[2]
-                                   : c[0] * n[1] - c[1] * n[0];
-                double wgt = nj * pv.at(P_AREA, j);
+                double wgt = pv.gen_normal(j, i) * pv.at(P_AREA, j);
                 double2 v;
-                if (col < 6 + H) {
+                if (col < D + H) {
                     v = pf[(size_t)col * ldphi + j];
-                    if (col >= 6) {
-                        double2 pI = pif[(size_t)(col - 6) * N + j];
+                    if (col >= D) {
+                        double2 pI = pif[(size_t)(col - D) * N + j];
                         v.x += pI.x;
                         v.y += pI.y;
                     }
                 } else {
-                    v = pif[(size_t)(col - 6 - H) * N + j];
+                    v = pif[(size_t)(col - D - H) * N + j];
                 }
                 sr += wgt * v.x;
                 si += wgt * v.y;
@@ -505,24 +500,24 @@ __global__ void __launch_bounds__(256) k_forces(PanelsView pv, const FreqInfo* _
             sr = block_sum(sr);
             si = block_sum(si);
             if (threadIdx.x == 0) {
-                if (col < 6) {
+                if (col < D) {
                     double zr = -rho * sr, zi = -rho * si;
-                    Aout[((size_t)f * 6 + i) * 6 + col] = zr;
-                    Bout[((size_t)f * 6 + i) * 6 + col] = -w * zi;
+                    Aout[((size_t)f * D + i) * D + col] = zr;
+                    Bout[((size_t)f * D + i) * D + col] = -w * zi;
                 } else {
                     // i w rho (sr + i si) = (-w rho si, w rho sr)
                     double2 val = make_double2(-w * rho * si, w * rho * sr);
-                    if (col < 6 + H)
-                        X[((size_t)f * H + (col - 6)) * 6 + i] = val;
+                    if (col < D + H)
+                        X[((size_t)f * H + (col - D)) * D + i] = val;
                     else
-                        FK[((size_t)f * H + (col - 6 - H)) * 6 + i] = val;
+                        FK[((size_t)f * H + (col - D - H)) * D + i] = val;
                 }
             }
         }
     }
     __syncthreads();
-    if (threadIdx.x < 6 * H) {
-        size_t o = (size_t)f * H * 6 + threadIdx.x;
+    for (int t = threadIdx.x; t < D * H; t += blockDim.x) {
+        size_t o = (size_t)f * H * D + t;
         SC[o] = make_double2(X[o].x - FK[o].x, X[o].y - FK[o].y);
     }
 }

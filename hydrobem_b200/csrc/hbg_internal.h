@@ -69,7 +69,7 @@ enum WsSlot {
     WS_VERTS = 0, WS_KIND, WS_PLANES, WS_BAD, WS_ST, WS_WORK, WS_NWORK, WS_S, WS_A, WS_U, WS_RHS, WS_X, WS_PHII,
     WS_IPIV, WS_INFO, WS_FI, WS_FD, WS_TILES, WS_SCR, WS_FPT, WS_HEADS, WS_OUT, WS_S32, WS_A32, WS_W, WS_P2,
     WS_P3, WS_PL, WS_PU, WS_B, WS_XM, WS_R, WS_NORMS, WS_ERR, WS_PART, WS_DINV, WS_TILES_F, WS_SG_PARAMS,
-    WS_SG_IMG, WS_SG_COUNT, WS_TRI_CTRL, WS_RS, WS_L16, WS_P3H, WS_COUNT
+    WS_SG_IMG, WS_SG_COUNT, WS_TRI_CTRL, WS_RS, WS_L16, WS_P3H, WS_PBODY, WS_RCEN, WS_COUNT
 };
 
 // Page-locked host buffers of a solve: a device-to-host copy into pageable memory waits for the

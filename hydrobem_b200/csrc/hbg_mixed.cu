@@ -155,10 +155,10 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                             bool fin, double depth, cudaStream_t s, double* prof, int64_t* launches, const char** msg,
                             int64_t* freq, const std::function<void()>& start) {
     KernelProfiler& P = profiler();
-    const int N = pv.N, F = (int)pr.n_omega, H = (int)pr.n_heading, nrhs = 6 + H;
+    const int N = pv.N, F = (int)pr.n_omega, H = (int)pr.n_heading, D = 6 * pv.nbod, nrhs = D + H;
     const int Np = (N + NBL - 1) / NBL * NBL;
     const size_t NP2 = (size_t)Np * Np, MB = 2 * NP2;  // floats per matrix (two planes)
-    if (nrhs > 32) MIXED_FAIL(HB_ERR_UNSUPPORTED, "more than 26 headings per solve", -1);
+    if (nrhs > 32) MIXED_FAIL(HB_ERR_UNSUPPORTED, "more than 32 right-hand sides (6 per body and one per heading)", -1);
     if (!encode_fn()) MIXED_FAIL(HB_ERR_UNSUPPORTED, "the driver offers no tensor-map encoder (TMA)", -1);
     // ---- batch size from free memory
     // GEMM operand buffers of the block row (rows 2n <= 2 (Np - NBL), 2 NBL wide), per frequency
@@ -222,7 +222,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     unsigned long long* sg_count = sg ? (unsigned long long*)get(WS_SG_COUNT, sizeof(unsigned long long)) : nullptr;
     double* scr = fin ? (double*)get(WS_SCR, sizeof(double) * 6912 * 3 * B) : nullptr;
     double* fpt = fin ? (double*)get(WS_FPT, sizeof(double) * FP_PLANES * N * B) : nullptr;
-    double* dout = (double*)get(WS_OUT, sizeof(double) * (72 + 3 * (size_t)H * 12) * B);
+    double* dout = (double*)get(WS_OUT, sizeof(double) * (2 * (size_t)D * D + 3 * (size_t)H * 2 * D) * B);
     if (!okb) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
     last_surrogate_pairs() = 0;
     // ---- tensor maps (whole batch; the batch index is the 4th coordinate)
@@ -266,7 +266,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
     std::vector<FreqInfo> fi(B);
     std::vector<FdParams> fdh(B);
-    const size_t out_per = 72 + 3 * (size_t)H * 12;
+    const size_t out_per = 2 * (size_t)D * D + 3 * (size_t)H * 2 * D, DD = (size_t)D * D;
     // page-locked: the reads of norms, outputs and the error flag queue behind the work, no host wait
     double* hout = (double*)ws.host(HS_OUT, sizeof(double) * (out_per * B + 1));
     double* hn = (double*)ws.host(HS_NORMS, sizeof(double) * IR_MAX_IT * 2 * (size_t)B);
@@ -656,10 +656,10 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             auto forces = [&]() {
                 EventTimer tf(s, &prof[4]);
                 double* dA = dout;
-                double* dB = dout + 36 * (size_t)nb;
-                double2* dX = reinterpret_cast<double2*>(dout + 72 * (size_t)nb);
-                double2* dFK = dX + (size_t)H * 6 * nb;
-                double2* dSC = dFK + (size_t)H * 6 * nb;
+                double* dB = dout + DD * nb;
+                double2* dX = reinterpret_cast<double2*>(dout + 2 * DD * nb);
+                double2* dFK = dX + (size_t)H * D * nb;
+                double2* dSC = dFK + (size_t)H * D * nb;
                 P.begin(s);
                 launch_forces(pv, nb, dfi, H, x, Np, phiI, opt.density, dA, dB, dX, dFK, dSC, s);
                 P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
@@ -737,17 +737,17 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         if (!converged)
             MIXED_FAIL(HB_ERR_NUMERICAL, "iterative refinement of the mixed-precision solve did not converge", f0);
         const double* hA = hout;
-        const double* hB = hA + 36 * (size_t)nb;
-        const double* hX = hA + 72 * (size_t)nb;
-        const double* hFK = hX + (size_t)H * 12 * nb;
-        const double* hSC = hFK + (size_t)H * 12 * nb;
+        const double* hB = hA + DD * nb;
+        const double* hX = hA + 2 * DD * nb;
+        const double* hFK = hX + (size_t)H * 2 * D * nb;
+        const double* hSC = hFK + (size_t)H * 2 * D * nb;
         for (int i = 0; i < nb; i++) {
-            const size_t fo = (size_t)(f0 + i), hx = (size_t)H * 12;
-            for (int q = 0; q < 36; q++)
-                if (!std::isfinite(hA[36 * i + q]) || !std::isfinite(hB[36 * i + q]))
+            const size_t fo = (size_t)(f0 + i), hx = (size_t)H * 2 * D;
+            for (size_t q = 0; q < DD; q++)
+                if (!std::isfinite(hA[DD * i + q]) || !std::isfinite(hB[DD * i + q]))
                     MIXED_FAIL(HB_ERR_NUMERICAL, "non-finite solution", f0 + i);
-            if (pr.out.added_mass) memcpy(pr.out.added_mass + fo * 36, hA + 36 * i, 36 * sizeof(double));
-            if (pr.out.radiation_damping) memcpy(pr.out.radiation_damping + fo * 36, hB + 36 * i, 36 * sizeof(double));
+            if (pr.out.added_mass) memcpy(pr.out.added_mass + fo * DD, hA + DD * i, DD * sizeof(double));
+            if (pr.out.radiation_damping) memcpy(pr.out.radiation_damping + fo * DD, hB + DD * i, DD * sizeof(double));
             if (pr.out.excitation) memcpy(pr.out.excitation + fo * hx, hX + hx * i, hx * sizeof(double));
             if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));

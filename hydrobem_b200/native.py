@@ -28,7 +28,8 @@ ip = ctypes.POINTER(ctypes.c_int32)
 
 
 class HbgBody(ctypes.Structure):
-    _fields_ = [("n_panels", ctypes.c_int64), ("vertices", dp), ("kinds", ip)]
+    _fields_ = [("n_panels", ctypes.c_int64), ("vertices", dp), ("kinds", ip), ("panel_body", ip),
+                ("n_bodies", ctypes.c_int32), ("rotation_centers", dp)]
 
 
 class HbgOutputs(ctypes.Structure):
@@ -143,25 +144,36 @@ def default_options(**kw) -> HbgOptions:
 
 
 class Body:
-    """The inputs and output arrays of one body of a batch (kept alive across the call)."""
+    """The inputs and output arrays of one problem of a batch (kept alive across the call): the panels of
+    one rigid body, or of interacting bodies with panel_body (the body of each panel) and
+    rotation_centers [n_bodies][3] (None: the origin); 6 rigid modes per body, D = 6 n_bodies."""
 
-    def __init__(self, vertices, omegas, headings_deg=(), kinds=None):
+    def __init__(self, vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None):
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 4, 3)
         self.kinds = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
+        self.panel_body = None if panel_body is None else np.ascontiguousarray(panel_body, dtype=np.int32)
+        self.n_bodies = 1 if self.panel_body is None else int(self.panel_body.max()) + 1
+        self.centers = None if rotation_centers is None else \
+            np.ascontiguousarray(rotation_centers, dtype=np.float64).reshape(-1, 3)
+        if self.centers is not None:
+            self.n_bodies = max(self.n_bodies, self.centers.shape[0])
         self.omegas = np.ascontiguousarray(omegas, dtype=np.float64).reshape(-1)
         self.headings = np.ascontiguousarray(headings_deg, dtype=np.float64).reshape(-1)
-        F, H = self.omegas.size, self.headings.size
-        self.A = np.zeros((F, 6, 6))
-        self.B = np.zeros((F, 6, 6))
-        self.X = np.zeros((F, H, 6), dtype=np.complex128)
-        self.FK = np.zeros((F, H, 6), dtype=np.complex128)
-        self.SC = np.zeros((F, H, 6), dtype=np.complex128)
+        F, H, D = self.omegas.size, self.headings.size, 6 * self.n_bodies
+        self.A = np.zeros((F, D, D))
+        self.B = np.zeros((F, D, D))
+        self.X = np.zeros((F, H, D), dtype=np.complex128)
+        self.FK = np.zeros((F, H, D), dtype=np.complex128)
+        self.SC = np.zeros((F, H, D), dtype=np.complex128)
 
     def problem(self) -> HbgProblem:
         p = HbgProblem()
         p.body.n_panels = self.vertices.shape[0]
         p.body.vertices = self.vertices.ctypes.data_as(dp)
         p.body.kinds = None if self.kinds is None else self.kinds.ctypes.data_as(ip)
+        p.body.panel_body = None if self.panel_body is None else self.panel_body.ctypes.data_as(ip)
+        p.body.n_bodies = self.n_bodies
+        p.body.rotation_centers = None if self.centers is None else self.centers.ctypes.data_as(dp)
         p.omegas = self.omegas.ctypes.data_as(dp)
         p.n_omega = self.omegas.size
         p.headings_deg = self.headings.ctypes.data_as(dp)
@@ -185,9 +197,9 @@ def solve_batch(bodies, **options):
     return [b.results() for b in bodies]
 
 
-def solve(vertices, omegas, headings_deg=(), kinds=None, **options):
-    """One body through the GPU path: dict of A, B [F][6][6], X, FK, SC [F][H][6]."""
-    return solve_batch([Body(vertices, omegas, headings_deg, kinds)], **options)[0]
+def solve(vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None, **options):
+    """One problem through the GPU path: dict of A, B [F][D][D], X, FK, SC [F][H][D], D = 6 per body."""
+    return solve_batch([Body(vertices, omegas, headings_deg, kinds, panel_body, rotation_centers)], **options)[0]
 
 
 def last_profile():

@@ -50,7 +50,7 @@ typedef int32_t HbStatus;
 #define HB_C128 7
 
 /* The version of this library's ABI (its own numbering; the reference's hb_abi_version is 8). */
-#define HBG_ABI_VERSION 2
+#define HBG_ABI_VERSION 3
 
 /* ==================================================================== batched entry */
 
@@ -62,18 +62,26 @@ typedef int32_t HbStatus;
 #define HBG_WET 0      /* wetted body surface */
 #define HBG_INTERIOR 1 /* interior free surface z = 0 (irregular-frequency removal) */
 
-/* One body: n_panels quadrilaterals, vertices [n_panels][4][3] (a triangle repeats its last
- * vertex, the right-hand-rule normal into the fluid: docs/reference/inputs-meshes.md §1);
- * kinds [n_panels] or NULL (all wet).  Rigid modes about the origin, body frame = global frame. */
+/* One problem's panels: n_panels quadrilaterals, vertices [n_panels][4][3] (a triangle repeats its
+ * last vertex, the right-hand-rule normal into the fluid: docs/reference/inputs-meshes.md §1);
+ * kinds [n_panels] or NULL (all wet).  Global frame.  Interacting bodies (the reference's several
+ * bodies of one model, crates/hydrobem/src/lo_frequency.rs:236-251, low_order.rs:313): n_bodies > 1
+ * with panel_body [n_panels] the body of each panel (0 .. n_bodies - 1) and rotation_centers
+ * [n_bodies][3] the point each body's rotations are about (NULL: the origin); n_bodies 0 or 1 and
+ * panel_body NULL: one rigid body.  The rigid modes are 6 per body (surge, sway, heave, roll, pitch,
+ * yaw), D = 6 n_bodies in all. */
 typedef struct HbgBody {
     int64_t n_panels;
     const double *vertices;
     const int32_t *kinds;
+    const int32_t *panel_body;
+    int32_t n_bodies;
+    const double *rotation_centers;
 } HbgBody;
 
-/* Outputs of one body, caller-allocated host arrays (NULL: not wanted), float64:
- *   added_mass, radiation_damping  [n_omega][6][6]   (coordinate i, radiation mode j)
- *   excitation, froude_krylov, scattering  [n_omega][n_heading][6][2]  (re, im)          */
+/* Outputs of one problem, caller-allocated host arrays (NULL: not wanted), float64, D = 6 n_bodies:
+ *   added_mass, radiation_damping  [n_omega][D][D]   (coordinate i, radiation mode j)
+ *   excitation, froude_krylov, scattering  [n_omega][n_heading][D][2]  (re, im)          */
 typedef struct HbgOutputs {
     double *added_mass;
     double *radiation_damping;

@@ -194,39 +194,51 @@ def incident(c, depth, k, omega, beta, grav=GRAVITY):
     return phi, grad
 
 
-def rigid_normals(c, n, kinds):
-    """n_j = (n, c x n) about the origin; 0 off the wetted surface (lo_geometry.rs:805-811)."""
-    nj = np.concatenate([n, np.cross(c, n)], axis=1)
+def rigid_normals(c, n, kinds, panel_body=None, centers=None):
+    """Generalized normals [N][6 n_bodies]: for body b's modes, (n, (c - R_b) x n) on its panels and 0
+    elsewhere; 0 off the wetted surface (lo_geometry.rs:805-811, lo_frequency.rs:236-251). One body
+    about the origin when panel_body and centers are None."""
+    nb = 1 if panel_body is None else int(np.max(panel_body)) + 1
+    if centers is not None:
+        nb = max(nb, len(centers))
+    body = np.zeros(len(c), int) if panel_body is None else np.asarray(panel_body)
+    R = np.zeros((nb, 3)) if centers is None else np.asarray(centers, dtype=float).reshape(-1, 3)
+    nj = np.zeros((len(c), 6 * nb))
+    for b in range(nb):
+        on = body == b
+        nj[on, 6 * b:6 * b + 3] = n[on]
+        nj[on, 6 * b + 3:6 * b + 6] = np.cross(c[on] - R[b], n[on])
     if kinds is not None:
         nj[np.asarray(kinds) != WET] = 0.0
     return nj
 
 
 def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY, rho=DENSITY, logint=True,
-                    want_matrices=False):
-    """A, B [6][6], X, FK, SC [H][6] of one frequency, all in float64 (complex128)."""
+                    want_matrices=False, panel_body=None, centers=None):
+    """A, B [D][D], X, FK, SC [H][D] of one frequency (D = 6 per body), all in float64 (complex128)."""
     c, n, area = panel_arrays(panels)
     N = len(panels)
     S, A = assemble(panels, kinds, st, depth, omega, grav, logint)
     k = lib().hbo_wavenumber(omega, depth if depth else np.inf, grav)
     wet = np.ones(N, bool) if kinds is None else (np.asarray(kinds) == WET)
-    nj = rigid_normals(c, n, kinds)
+    nj = rigid_normals(c, n, kinds, panel_body, centers)
+    D = nj.shape[1]
     H = len(headings_rad)
-    u = np.zeros((N, 6 + H), dtype=np.complex128)
-    u[:, :6] = nj
+    u = np.zeros((N, D + H), dtype=np.complex128)
+    u[:, :D] = nj
     phiI = np.zeros((H, N), dtype=np.complex128)
     for h, beta in enumerate(headings_rad):
         pI, gr = incident(c, depth, k, omega, beta, grav)
         phiI[h] = pI
         d = (gr * n).sum(axis=1)
-        u[:, 6 + h] = np.where(wet, -d, 0.0)
+        u[:, D + h] = np.where(wet, -d, 0.0)
     rhs = S @ (-u)
     phi = np.linalg.solve(A, rhs)
     w = (nj * area[:, None]) * wet[:, None]          # n_i A_j on the body panels
-    z = -rho * (w.T @ phi[:, :6])                    # [i][c]
+    z = -rho * (w.T @ phi[:, :D])                    # [i][c]
     out = {"A": z.real, "B": -omega * z.imag}
     if H:
-        x = w.T @ (phi[:, 6:] + phiI.T)              # [i][h]
+        x = w.T @ (phi[:, D:] + phiI.T)              # [i][h]
         fk = w.T @ phiI.T
         iwr = 1j * omega * rho
         out["X"] = (iwr * x).T
@@ -238,11 +250,13 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
 
 
 def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GRAVITY, rho=DENSITY, logint=True,
-               tol=1e-4):
-    """The whole path for one body: statics once, then every frequency. Arrays [F][6][6], [F][H][6]."""
+               tol=1e-4, panel_body=None, centers=None):
+    """The whole path for one problem: statics once, then every frequency. Arrays [F][D][D], [F][H][D]
+    (D = 6 per body; interacting bodies by panel_body and their rotation centers)."""
     panels = make_panels(verts, kinds)
     st = statics(panels, kinds, depth, logint, tol)
     heads = np.radians(np.asarray(headings_deg, dtype=float))
-    res = [solve_frequency(panels, kinds, st, depth, w, heads, grav, rho, logint) for w in omegas]
+    res = [solve_frequency(panels, kinds, st, depth, w, heads, grav, rho, logint, panel_body=panel_body,
+                           centers=centers) for w in omegas]
     out = {k: np.array([r[k] for r in res]) for k in res[0]}
     return out

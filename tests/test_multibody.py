@@ -1,0 +1,137 @@
+"""Interacting bodies: several rigid bodies in one problem, 6 modes each (the reference's several bodies
+of one model: crates/hydrobem/src/lo_frequency.rs:236-251 radiation columns per body, 1039-1115 forces
+per coordinate, low_order.rs:313 generalized normals about each body's rotation centre).
+
+The oracle is checked on CPU by linearity (a rigid body split into two bodies that rotate about the same
+point: the single body's matrices are the sums of the two-body blocks); the GPU forms against the oracle
+on two cylinders that interact.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from hydrobem_b200 import meshes
+from oracle import oracle as O
+
+OMEGAS = 2.0 * math.pi / np.array([2.0, 4.0, 7.0])
+HEADS = [0.0, 45.0]
+
+
+def scaled_error(got, ref, floor=1e-3):
+    ref = np.asarray(ref)
+    got = np.asarray(got)
+    peak = np.abs(ref).max()
+    scale = np.maximum(np.abs(ref).max(axis=0, keepdims=True), floor * peak)
+    return float((np.abs(got - ref) / scale).max())
+
+
+def two_cylinders(gap=3.0):
+    """Two cylinders (r 1 m, draft 0.5 m, 128 panels each) at x = -gap and x = +gap."""
+    a = meshes.cylinder(1.0, 0.5, 16, 4, 4).copy()
+    b = a.copy()
+    a[..., 0] -= gap
+    b[..., 0] += gap
+    v = np.concatenate([a, b])
+    body = np.r_[np.zeros(len(a), np.int32), np.ones(len(b), np.int32)]
+    return v, body, [[-gap, 0.0, 0.0], [gap, 0.0, 0.0]]
+
+
+def split_cylinder():
+    """One cylinder whose panels are assigned to two bodies by the sign of the centroid's x."""
+    v = meshes.cylinder(1.0, 0.5, 16, 4, 4)
+    body = (v.mean(axis=1)[:, 0] > 0.0).astype(np.int32)
+    return v, body
+
+
+def block_sums(r, F, H):
+    """The 12-mode results of a split body summed over the body blocks (6 modes)."""
+    out = {"A": r["A"].reshape(F, 2, 6, 2, 6).sum(axis=(1, 3)), "B": r["B"].reshape(F, 2, 6, 2, 6).sum(axis=(1, 3))}
+    for k in ("X", "FK", "SC"):
+        out[k] = r[k].reshape(F, H, 2, 6).sum(axis=2)
+    return out
+
+
+def test_oracle_split_body_is_linear():
+    v, body = split_cylinder()
+    one = O.solve_body(v, OMEGAS[:2], HEADS, depth=math.inf)
+    two = O.solve_body(v, OMEGAS[:2], HEADS, depth=math.inf, panel_body=body, centers=[[0, 0, 0], [0, 0, 0]])
+    assert two["A"].shape == (2, 12, 12) and two["X"].shape == (2, 2, 12)
+    summed = block_sums(two, 2, len(HEADS))
+    for k in ("A", "B", "X", "FK", "SC"):
+        assert scaled_error(summed[k], one[k]) <= 1e-10, k
+
+
+def test_oracle_rotation_centre_shifts_moments():
+    """Moving the rotation centre by r changes the roll/pitch/yaw normals by -(r x n): the translation
+    columns of A are unchanged and the moment rows pick up -(r x F)."""
+    v = meshes.cylinder(1.0, 0.5, 16, 4, 4)
+    r = np.array([0.3, -0.2, 0.1])
+    base = O.solve_body(v, OMEGAS[:1], [], depth=math.inf)
+    moved = O.solve_body(v, OMEGAS[:1], [], depth=math.inf, panel_body=np.zeros(len(v), np.int32), centers=[r])
+    assert np.allclose(moved["A"][:, :3, :3], base["A"][:, :3, :3], rtol=1e-12, atol=0.0)
+    # row i >= 3 (moment about R): M_R = M_0 - r x F for the translation columns
+    F0 = base["A"][0, :3, :3]
+    expect = base["A"][0, 3:, :3] - np.cross(r, F0.T).T
+    assert np.allclose(moved["A"][0, 3:, :3], expect, rtol=1e-10, atol=1e-12 * np.abs(F0).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("depth", [math.inf, 3.0])
+def test_gpu_two_interacting_bodies(depth):
+    from hydrobem_b200 import native as nv
+
+    v, body, centers = two_cylinders()
+    gpu = nv.solve(v, OMEGAS, HEADS, depth=depth, panel_body=body, rotation_centers=centers)
+    ref = O.solve_body(v, OMEGAS, HEADS, depth=depth, panel_body=body, centers=centers)
+    assert gpu["A"].shape == (3, 12, 12) and gpu["X"].shape == (3, 2, 12)
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "FK", "SC")}
+    assert max(errs.values()) <= 1e-9, errs
+    # the two bodies are mirror images about x = 0 and the heading-0 wave comes along x: their heave
+    # added masses agree
+    assert abs(gpu["A"][0, 2, 2] - gpu["A"][0, 8, 8]) <= 1e-9 * abs(gpu["A"][0, 2, 2])
+
+
+@pytest.mark.gpu
+def test_gpu_mixed_two_interacting_bodies():
+    from hydrobem_b200 import native as nv
+
+    v, body, centers = two_cylinders()
+    gpu = nv.solve(v, OMEGAS, HEADS, depth=3.0, panel_body=body, rotation_centers=centers, precision=nv.HBG_MIXED)
+    ref = O.solve_body(v, OMEGAS, HEADS, depth=3.0, panel_body=body, centers=centers)
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    assert max(errs.values()) <= 1e-5, errs
+
+
+@pytest.mark.gpu
+def test_gpu_split_body_is_linear():
+    from hydrobem_b200 import native as nv
+
+    v, body = split_cylinder()
+    one = nv.solve(v, OMEGAS, HEADS)
+    two = nv.solve(v, OMEGAS, HEADS, panel_body=body, rotation_centers=[[0, 0, 0], [0, 0, 0]])
+    summed = block_sums(two, len(OMEGAS), len(HEADS))
+    for k in ("A", "B", "X", "FK", "SC"):
+        assert scaled_error(summed[k], one[k]) <= 1e-10, k
+
+
+@pytest.mark.gpu
+def test_gpu_body_arguments_checked():
+    import ctypes
+
+    from hydrobem_b200 import native as nv
+
+    v, body, centers = two_cylinders()
+    bad = body.copy()
+    bad[5] = 7
+    b = nv.Body(v, OMEGAS[:1], [], panel_body=bad, rotation_centers=centers)
+    b.n_bodies = 2
+    arr = (nv.HbgProblem * 1)(b.problem())
+    opt = nv.default_options()
+    assert nv.lib().hbg_solve_batch(arr, 1, ctypes.byref(opt)) == 1  # HB_ERR_VALUE
+    # more right-hand sides than the solve takes: 6 bodies (36 modes)
+    many = nv.Body(np.concatenate([v, v, v]), OMEGAS[:1], [], panel_body=np.r_[body, body + 2, body + 4])
+    arr = (nv.HbgProblem * 1)(many.problem())
+    assert nv.lib().hbg_solve_batch(arr, 1, ctypes.byref(opt)) == 3  # HB_ERR_UNSUPPORTED
