@@ -1,7 +1,10 @@
 // hbg_model.cu -- the model/solve/results subset of the reference's C ABI (hydrobem.h), for the
-// items of the low-order open-sea route of one rigid body.  Objects: the model (""),
+// items of the low-order open-sea route of rigid bodies.  Objects: the model (""),
 // "environment", "options", "meshes/<name>" (kind panels: vertices [P,4,3], symmetry) and
-// "bodies/<name>" (mesh, interior_surface, interior_surface_mesh).  A mesh with symmetry planes
+// "bodies/<name>" (mesh, interior_surface, interior_surface_mesh, position, rotation_center; yaw 0).
+// Several bodies interact in one solve, 6 rigid modes each in the order the bodies were added, each
+// mesh moved to the body's position and the modes about its rotation centre (body-local, as the
+// reference's document_schema.rs:281-285 items).  A mesh with symmetry planes
 // is expanded to the full mesh (the stored elements, then their x, y and xy reflections,
 // geometry.rs:208-235), which solves the same discrete equations as the reference's character
 // decomposition.  Items and routes outside this subset are refused with HB_ERR_UNSUPPORTED, as the
@@ -27,6 +30,8 @@ struct BodyObj {
     std::string mesh;
     std::string interior = "detect";
     std::string interior_mesh;
+    double position[3] = {0.0, 0.0, 0.0};         // the global position of the body origin
+    double rotation_center[3] = {0.0, 0.0, 0.0};  // body-local
 };
 
 struct Quantity {
@@ -215,6 +220,15 @@ extern "C" HbStatus hb_set_reals(HbModel* model, uint64_t object, const char* it
                 return HB_OK;
             }
         }
+        if (is_body(model, object) && (it == "position" || it == "rotation_center")) {
+            if (ndim != 1 || shape[0] != 3) return refuse(HB_ERR_VALUE, it + " has 3 values");
+            for (double x : v)
+                if (!std::isfinite(x)) return refuse(HB_ERR_VALUE, it + " must be finite");
+            BodyObj& b = model->bodies[object - OBJ_BODY0];
+            double* dst = it == "position" ? b.position : b.rotation_center;
+            for (int d = 0; d < 3; d++) dst[d] = v[d];
+            return HB_OK;
+        }
         if (is_mesh(model, object) && it == "vertices") {
             if (ndim != 3 || shape[1] != 4 || shape[2] != 3) return refuse(HB_ERR_VALUE, "vertices have the shape (P, 4, 3)");
             for (double x : v)
@@ -232,6 +246,8 @@ extern "C" HbStatus hb_set_real(HbModel* model, uint64_t object, const char* ite
         std::lock_guard<std::mutex> g(model->lock);
         std::string it(item);
         if (std::isnan(value)) return refuse(HB_ERR_VALUE, "NaN");
+        if (is_body(model, object) && it == "yaw")
+            return value == 0.0 ? HB_OK : refuse(HB_ERR_UNSUPPORTED, "a body rotated about z (yaw != 0) is not on this route");
         if (object == OBJ_ENV) {
             if (it == "depth") {
                 if (!(value > 0.0)) return refuse(HB_ERR_VALUE, "depth > 0 (inf for infinite depth)");
@@ -333,36 +349,42 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
             HbModel* m;
             ~Done() { m->solving = false; }
         } done{model};
-        std::vector<double> verts, omegas, heads;
-        std::vector<int32_t> kinds;
+        std::vector<double> verts, omegas, heads, centers;
+        std::vector<int32_t> kinds, panel_body;
         HbgOptions opt;
         hbg_default_options(&opt);
         {
             std::lock_guard<std::mutex> g(model->lock);
-            if (model->bodies.size() != 1)
-                return refuse(HB_ERR_UNSUPPORTED, "this route solves one rigid body per model (hbg_solve_batch takes many)");
-            const BodyObj& b = model->bodies[0];
-            const MeshObj* mesh = nullptr;
-            const MeshObj* lid = nullptr;
-            for (auto& m : model->meshes) {
-                if (m.name == b.mesh) mesh = &m;
-                if (m.name == b.interior_mesh) lid = &m;
-            }
-            if (!mesh || mesh->vertices.empty()) return refuse(HB_ERR_VALUE, "the body has no panels mesh");
-            verts = expand(*mesh);
-            size_t P = verts.size() / 12;
-            kinds.assign(P, HBG_WET);
-            if (b.interior == "detect")
-                for (size_t p = 0; p < P; p++) {
-                    bool z0 = true;
-                    for (int i = 0; i < 4; i++) z0 = z0 && verts[12 * p + 3 * i + 2] == 0.0;
-                    if (z0) kinds[p] = HBG_INTERIOR;
+            if (model->bodies.empty()) return refuse(HB_ERR_VALUE, "the model has no body");
+            for (size_t bi = 0; bi < model->bodies.size(); bi++) {
+                const BodyObj& b = model->bodies[bi];
+                const MeshObj* mesh = nullptr;
+                const MeshObj* lid = nullptr;
+                for (auto& m : model->meshes) {
+                    if (m.name == b.mesh) mesh = &m;
+                    if (m.name == b.interior_mesh) lid = &m;
                 }
-            if (b.interior == "mesh") {
-                if (!lid) return refuse(HB_ERR_VALUE, "interior_surface_mesh names no mesh");
-                std::vector<double> lv = expand(*lid);
-                verts.insert(verts.end(), lv.begin(), lv.end());
-                kinds.resize(verts.size() / 12, HBG_INTERIOR);
+                if (!mesh || mesh->vertices.empty()) return refuse(HB_ERR_VALUE, "the body has no panels mesh");
+                std::vector<double> bv = expand(*mesh);
+                size_t P = bv.size() / 12;
+                std::vector<int32_t> bk(P, HBG_WET);
+                if (b.interior == "detect")
+                    for (size_t p = 0; p < P; p++) {
+                        bool z0 = true;
+                        for (int i = 0; i < 4; i++) z0 = z0 && bv[12 * p + 3 * i + 2] == 0.0;
+                        if (z0) bk[p] = HBG_INTERIOR;
+                    }
+                if (b.interior == "mesh") {
+                    if (!lid) return refuse(HB_ERR_VALUE, "interior_surface_mesh names no mesh");
+                    std::vector<double> lv = expand(*lid);
+                    bv.insert(bv.end(), lv.begin(), lv.end());
+                    bk.resize(bv.size() / 12, HBG_INTERIOR);
+                }
+                for (size_t q = 0; q < bv.size(); q++) bv[q] += b.position[q % 3];  // body to global
+                verts.insert(verts.end(), bv.begin(), bv.end());
+                kinds.insert(kinds.end(), bk.begin(), bk.end());
+                panel_body.insert(panel_body.end(), bk.size(), (int32_t)bi);
+                for (int d = 0; d < 3; d++) centers.push_back(b.position[d] + b.rotation_center[d]);
             }
             const std::vector<double>& f = model->frequency_input == "omegas" ? model->omegas : model->periods;
             for (double x : f) {
@@ -382,12 +404,15 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         }
         opt.cancel = reinterpret_cast<const volatile int32_t*>(&model->cancel);
         if (model->cancel.exchange(0) != 0) return refuse(HB_ERR_CANCELLED, "the solve was cancelled");
-        const size_t F = omegas.size(), H = heads.size();
-        std::vector<double> A(F * 36), B(F * 36), X(F * H * 12), FK(F * H * 12), SC(F * H * 12);
+        const size_t F = omegas.size(), H = heads.size(), NB = centers.size() / 3, D = 6 * NB;
+        std::vector<double> A(F * D * D), B(F * D * D), X(F * H * D * 2), FK(F * H * D * 2), SC(F * H * D * 2);
         HbgProblem pr{};
         pr.body.n_panels = (int64_t)(verts.size() / 12);
         pr.body.vertices = verts.data();
         pr.body.kinds = kinds.data();
+        pr.body.panel_body = panel_body.data();
+        pr.body.n_bodies = (int32_t)NB;
+        pr.body.rotation_centers = centers.data();
         pr.omegas = omegas.data();
         pr.n_omega = (int64_t)F;
         pr.headings_deg = heads.data();
@@ -414,26 +439,27 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         auto r = std::make_unique<HbResults>();
         add_quantity(r.get(), "omegas", HB_F64, {F}, omegas.data(), F * 8);
         add_quantity(r.get(), "headings", HB_F64, {H}, heads.data(), H * 8);
-        std::vector<float> a32(F * 36), b32(F * 36), x32(F * H * 12), fk32(F * H * 12), sc32(F * H * 12);
-        for (size_t i = 0; i < F * 36; i++) {
+        std::vector<float> a32(F * D * D), b32(F * D * D), x32(F * H * D * 2), fk32(F * H * D * 2), sc32(F * H * D * 2);
+        for (size_t i = 0; i < F * D * D; i++) {
             a32[i] = (float)A[i];
             b32[i] = (float)B[i];
         }
-        for (size_t i = 0; i < F * H * 12; i++) {
+        for (size_t i = 0; i < F * H * D * 2; i++) {
             x32[i] = (float)X[i];
             fk32[i] = (float)FK[i];
             sc32[i] = (float)SC[i];
         }
-        add_quantity(r.get(), "added_mass", HB_F32, {F, 6, 6}, a32.data(), a32.size() * 4);
-        add_quantity(r.get(), "radiation_damping", HB_F32, {F, 6, 6}, b32.data(), b32.size() * 4);
-        add_quantity(r.get(), "excitation_diffraction", HB_C64, {F, H, 6}, x32.data(), x32.size() * 4);
-        add_quantity(r.get(), "excitation_froude_krylov", HB_C64, {F, H, 6}, fk32.data(), fk32.size() * 4);
-        add_quantity(r.get(), "excitation_scattering", HB_C64, {F, H, 6}, sc32.data(), sc32.size() * 4);
-        add_quantity(r.get(), "added_mass_f64", HB_F64, {F, 6, 6}, A.data(), A.size() * 8);
-        add_quantity(r.get(), "radiation_damping_f64", HB_F64, {F, 6, 6}, B.data(), B.size() * 8);
-        add_quantity(r.get(), "excitation_diffraction_f64", HB_C128, {F, H, 6}, X.data(), X.size() * 8);
-        add_quantity(r.get(), "excitation_froude_krylov_f64", HB_C128, {F, H, 6}, FK.data(), FK.size() * 8);
-        add_quantity(r.get(), "excitation_scattering_f64", HB_C128, {F, H, 6}, SC.data(), SC.size() * 8);
+        // [F][D][D] and [F][H][D]: coordinate i and mode j of every body, bodies in the order added
+        add_quantity(r.get(), "added_mass", HB_F32, {F, D, D}, a32.data(), a32.size() * 4);
+        add_quantity(r.get(), "radiation_damping", HB_F32, {F, D, D}, b32.data(), b32.size() * 4);
+        add_quantity(r.get(), "excitation_diffraction", HB_C64, {F, H, D}, x32.data(), x32.size() * 4);
+        add_quantity(r.get(), "excitation_froude_krylov", HB_C64, {F, H, D}, fk32.data(), fk32.size() * 4);
+        add_quantity(r.get(), "excitation_scattering", HB_C64, {F, H, D}, sc32.data(), sc32.size() * 4);
+        add_quantity(r.get(), "added_mass_f64", HB_F64, {F, D, D}, A.data(), A.size() * 8);
+        add_quantity(r.get(), "radiation_damping_f64", HB_F64, {F, D, D}, B.data(), B.size() * 8);
+        add_quantity(r.get(), "excitation_diffraction_f64", HB_C128, {F, H, D}, X.data(), X.size() * 8);
+        add_quantity(r.get(), "excitation_froude_krylov_f64", HB_C128, {F, H, D}, FK.data(), FK.size() * 8);
+        add_quantity(r.get(), "excitation_scattering_f64", HB_C128, {F, H, D}, SC.data(), SC.size() * 8);
         {
             std::lock_guard<std::mutex> g(model->lock);
             model->results = std::make_unique<HbResults>(*r);

@@ -91,9 +91,12 @@ def test_model_layer_items_and_refusals():
         # null out-pointers are refused and change nothing
         assert L.hb_object(m, b"environment", None) == 7
         assert L.hb_model_new(None) == 7
-        # no body: this route solves exactly one
+        # a body item outside the route, and a model without a body
+        rc, _ = _obj(L, m, "bodies/nothing")
+        assert rc == 1
         L.hb_model_solve.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
-        assert L.hb_model_solve(m, None, None, None) == 3
+        assert L.hb_model_solve(m, None, None, None) == 1
+        assert b"no body" in L.hb_last_error_message()
     finally:
         assert L.hb_model_free(m) == 0
 

@@ -135,3 +135,65 @@ def test_gpu_body_arguments_checked():
     many = nv.Body(np.concatenate([v, v, v]), OMEGAS[:1], [], panel_body=np.r_[body, body + 2, body + 4])
     arr = (nv.HbgProblem * 1)(many.problem())
     assert nv.lib().hbg_solve_batch(arr, 1, ctypes.byref(opt)) == 3  # HB_ERR_UNSUPPORTED
+
+
+@pytest.mark.gpu
+def test_gpu_two_bodies_through_the_model_abi():
+    """Two bodies of one mesh placed by position, rotation centres body-local: the model layer's solve
+    equals the batched entry's with the panels moved and labelled by hand."""
+    import ctypes
+
+    from hydrobem_b200 import native as nv
+
+    cyl = np.ascontiguousarray(meshes.cylinder(1.0, 0.5, 16, 4, 4))
+    L = nv.lib()
+    m = ctypes.c_void_p()
+    assert L.hb_model_new(ctypes.byref(m)) == 0
+    try:
+        def obj(path):
+            o = ctypes.c_uint64()
+            assert L.hb_object(m, path.encode(), ctypes.byref(o)) == 0, L.hb_last_error_message()
+            return o.value
+
+        L.hb_add.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                             ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64)]
+        L.hb_set_reals.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, nv.dp,
+                                   ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t]
+        L.hb_set_text.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_char_p]
+        L.hb_set_real.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_double]
+        out = ctypes.c_uint64()
+        assert L.hb_add(m, 0, b"meshes", None, b"cyl", -1, ctypes.byref(out)) == 0
+        assert L.hb_set_reals(m, obj("meshes/cyl"), b"vertices", cyl.ctypes.data_as(nv.dp),
+                              (ctypes.c_size_t * 3)(*cyl.shape), 3) == 0
+        rc_local = np.array([0.1, 0.0, -0.2])
+        for name, x in ((b"west", -3.0), (b"east", 3.0)):
+            assert L.hb_add(m, 0, b"bodies", None, name, -1, ctypes.byref(out)) == 0
+            b = obj("bodies/" + name.decode())
+            assert L.hb_set_text(m, b, b"mesh", b"cyl") == 0
+            pos = np.array([x, 0.0, 0.0])
+            assert L.hb_set_reals(m, b, b"position", pos.ctypes.data_as(nv.dp), (ctypes.c_size_t * 1)(3), 1) == 0
+            assert L.hb_set_reals(m, b, b"rotation_center", rc_local.ctypes.data_as(nv.dp),
+                                  (ctypes.c_size_t * 1)(3), 1) == 0
+            assert L.hb_set_real(m, b, b"yaw", 0.0) == 0
+            assert L.hb_set_real(m, b, b"yaw", 10.0) == 3  # a rotated body is not on this route
+        env = obj("environment")
+        w = np.ascontiguousarray(OMEGAS)
+        h = np.ascontiguousarray(HEADS, dtype=np.float64)
+        assert L.hb_set_reals(m, env, b"omegas", w.ctypes.data_as(nv.dp), (ctypes.c_size_t * 1)(w.size), 1) == 0
+        assert L.hb_set_reals(m, env, b"headings", h.ctypes.data_as(nv.dp), (ctypes.c_size_t * 1)(h.size), 1) == 0
+        res = ctypes.c_void_p()
+        L.hb_model_solve.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        assert L.hb_model_solve(m, None, None, ctypes.byref(res)) == 0, L.hb_last_error_message()
+        L.hb_results_quantity.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(nv.HbColumn)]
+        c = nv.HbColumn()
+        assert L.hb_results_quantity(res, b"added_mass_f64", ctypes.byref(c)) == 0
+        shape = tuple(c.shape[i] for i in range(c.ndim))
+        A = np.ctypeslib.as_array(ctypes.cast(c.data, ctypes.POINTER(ctypes.c_double)), shape=shape).copy()
+        L.hb_results_free(res)
+    finally:
+        L.hb_model_free(m)
+    assert A.shape == (len(OMEGAS), 12, 12)
+    v, body, _ = two_cylinders()
+    direct = nv.solve(v, OMEGAS, HEADS, panel_body=body,
+                      rotation_centers=[[-3.0 + rc_local[0], 0.0, rc_local[2]], [3.0 + rc_local[0], 0.0, rc_local[2]]])
+    assert np.abs(A - direct["A"]).max() <= 1e-12 * np.abs(direct["A"]).max()
