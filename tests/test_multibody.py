@@ -197,3 +197,35 @@ def test_gpu_two_bodies_through_the_model_abi():
     direct = nv.solve(v, OMEGAS, HEADS, panel_body=body,
                       rotation_centers=[[-3.0 + rc_local[0], 0.0, rc_local[2]], [3.0 + rc_local[0], 0.0, rc_local[2]]])
     assert np.abs(A - direct["A"]).max() <= 1e-12 * np.abs(direct["A"]).max()
+
+
+def three_cylinder_array(n_phi=16, n_z=4, n_r=4):
+    """The array of the surrogate configuration at a reduced panel count: three cylinders of radius 1 m
+    and draft 1 m, 4 m apart along x, each rotating about its own axis at the waterline."""
+    one = meshes.cylinder(1.0, 1.0, n_phi, n_z, n_r)
+    parts, body, centers = [], [], []
+    for b, x in enumerate((-4.0, 0.0, 4.0)):
+        c = one.copy()
+        c[..., 0] += x
+        parts.append(c)
+        body.append(np.full(len(c), b, np.int32))
+        centers.append([x, 0.0, 0.0])
+    return np.concatenate(parts), np.concatenate(body), centers
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gpu_three_cylinder_array(precision):
+    """18 modes and one heading: 19 right-hand sides, beyond the 16 of the persistent sweeps and the TMA
+    residual, so the stepwise solves and the register-form products run."""
+    from hydrobem_b200 import native as nv
+
+    v, body, centers = three_cylinder_array()
+    omegas = OMEGAS[:2]
+    prec = nv.HBG_MIXED if precision == "mixed" else nv.HBG_FP64
+    gpu = nv.solve(v, omegas, [0.0], panel_body=body, rotation_centers=centers, precision=prec)
+    ref = O.solve_body(v, omegas, [0.0], depth=math.inf, panel_body=body, centers=centers)
+    assert gpu["A"].shape == (2, 18, 18)
+    keys = ("A", "B", "X", "FK", "SC") if precision == "fp64" else ("A", "B", "X")
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in keys}
+    assert max(errs.values()) <= (1e-9 if precision == "fp64" else 1e-5), errs
