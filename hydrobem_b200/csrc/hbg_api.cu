@@ -536,12 +536,31 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
                       (size_t)N * sizeof(int32_t) + (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)FP_PLANES * N * 8 +
                                                               (size_t)6912 * 3 * 8
                                                         : 0);
-    size_t freeb = 0, totalb = 0;
-    CUDA_OK(cudaMemGetInfo(&freeb, &totalb));
-    const size_t reusable = ws.bytes[WS_S] + ws.bytes[WS_A];
-    int B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)(freeb + reusable)) / per_freq);
-    if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
-    B = std::min(B, F);
+    // the batch size from free memory, kept per thread and device for the same problem shape while the
+    // workspace holds its buffers (cudaMemGetInfo can take milliseconds)
+    int B = 0;
+    {
+        struct BatchChoice {
+            int N = -1, nrhs = -1, fin = -1, F = -1, B = 0;
+            int64_t max_batch = -2;
+        };
+        static thread_local BatchChoice last[16];
+        int dev_b = 0;
+        cudaGetDevice(&dev_b);
+        BatchChoice& c = last[dev_b < 0 || dev_b >= 16 ? 0 : dev_b];
+        const bool same = c.N == N && c.nrhs == nrhs && c.fin == (int)fin && c.F == F && c.max_batch == opt.max_batch;
+        if (same && c.B > 0 && ws.bytes[WS_S] >= sizeof(double2) * NN * c.B && ws.bytes[WS_A] >= sizeof(double2) * NN * c.B) {
+            B = c.B;
+        } else {
+            size_t freeb = 0, totalb = 0;
+            CUDA_OK(cudaMemGetInfo(&freeb, &totalb));
+            const size_t reusable = ws.bytes[WS_S] + ws.bytes[WS_A];
+            B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)(freeb + reusable)) / per_freq);
+            if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
+            B = std::min(B, F);
+            c = BatchChoice{N, nrhs, (int)fin, F, B, opt.max_batch};
+        }
+    }
     WsBuf dS(ws, WS_S), dA(ws, WS_A), du(ws, WS_U), drhs(ws, WS_RHS), dX(ws, WS_X), dphiI(ws, WS_PHII),
         dipiv(ws, WS_IPIV), dinfo(ws, WS_INFO), dfi(ws, WS_FI), dfd(ws, WS_FD), dtiles(ws, WS_TILES),
         dscr(ws, WS_SCR), dfpt(ws, WS_FPT), dheads(ws, WS_HEADS), dout(ws, WS_OUT);

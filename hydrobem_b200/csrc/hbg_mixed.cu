@@ -168,16 +168,33 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                  (size_t)(nrhs + H) * N * 16 + 4 * (size_t)nrhs * Np * 16 + 64 +
                  (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)(T1F_SIZE + T2F_SIZE) * 4 + (size_t)FP_PLANES * N * 8 + (size_t)6912 * 3 * 8 : 0);
     per += (size_t)(Np / NBL) * NBL * NBL * 8;  // the diagonal-block inverses
-    size_t freeb = 0, totalb = 0;
-    if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "cudaMemGetInfo failed", -1);
-    {
-        Workspace& w0 = workspace();
-        freeb += w0.bytes[WS_S32] + w0.bytes[WS_A32] + w0.bytes[WS_W] + w0.bytes[WS_DINV];
-    }
-    int B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)freeb) / per);
-    if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
-    B = std::min(B, F);
+    // The batch size from free memory; cudaMemGetInfo can take milliseconds, so the decision is kept per
+    // thread and device for the same problem shape while the workspace still holds its buffers.
     Workspace& ws = workspace();
+    int B = 0;
+    {
+        struct BatchChoice {
+            int N = -1, nrhs = -1, fin = -1, F = -1, B = 0;
+            int64_t max_batch = -2;
+        };
+        static thread_local BatchChoice last[16];
+        int dev_b = 0;
+        cudaGetDevice(&dev_b);
+        BatchChoice& c = last[dev_b < 0 || dev_b >= 16 ? 0 : dev_b];
+        const bool same = c.N == N && c.nrhs == nrhs && c.fin == (int)fin && c.F == F && c.max_batch == opt.max_batch;
+        if (same && c.B > 0 && ws.bytes[WS_S32] >= MB * (size_t)c.B * 4 && ws.bytes[WS_W] >= MB * (size_t)c.B * 4) {
+            B = c.B;
+        } else {
+            size_t freeb = 0, totalb = 0;
+            if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess)
+                MIXED_FAIL(HB_ERR_INTERNAL, "cudaMemGetInfo failed", -1);
+            freeb += ws.bytes[WS_S32] + ws.bytes[WS_A32] + ws.bytes[WS_W] + ws.bytes[WS_DINV];
+            B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)freeb) / per);
+            if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
+            B = std::min(B, F);
+            c = BatchChoice{N, nrhs, (int)fin, F, B, opt.max_batch};
+        }
+    }
     const size_t nblk = (size_t)Np / NBL;
     bool okb = true;
     auto get = [&](int slot, size_t bytes) -> void* {
