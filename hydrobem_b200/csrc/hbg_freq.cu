@@ -451,81 +451,85 @@ void launch_rhs_f64(int N, int F, int nrhs, const double2* S, size_t mat_stride,
 // ------------------------------------------------------------------ forces
 // lo_frequency.rs:1039-1115: z = sum_j n_i phi_c A_j over the wetted panels; A = Re(-rho z),
 // B = -w Im(-rho z); X = i w rho sum n_i (phi_S + phi_I) A_j, FK the phi_I part, SC = X - FK.
-// One block per frequency; fixed-order block reductions (deterministic).
+// One block per (column, body, frequency): each thread accumulates the body's six coordinates (and for a
+// diffraction column the incident part beside the total) over its panels in one pass, then warp
+// shuffles and a fixed-order sum over the warps (deterministic).
 __global__ void __launch_bounds__(256) k_forces(PanelsView pv, const FreqInfo* __restrict__ fi, int H,
                                                 const double2* __restrict__ phi, int ldphi,
                                                 const double2* __restrict__ phiI,
                                                 double rho, double* __restrict__ Aout, double* __restrict__ Bout,
                                                 double2* __restrict__ X, double2* __restrict__ FK,
                                                 double2* __restrict__ SC) {
-    __shared__ double red[256];
-    int f = blockIdx.x, N = pv.N;
+    __shared__ double red[8][24];
+    const int col = blockIdx.x, b = blockIdx.y, f = blockIdx.z, N = pv.N;
     const int D = 6 * pv.nbod, nrhs = D + H;
-    const double2* pf = phi + (size_t)f * nrhs * ldphi;
-    const double2* pif = phiI + (size_t)f * H * N;
-    double w = fi[f].omega;
-    auto block_sum = [&](double v) -> double {
-        red[threadIdx.x] = v;
-        __syncthreads();
-        for (int s = 128; s > 0; s >>= 1) {
-            if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
-            __syncthreads();
+    const bool diff = col >= D;
+    const double2* pc = phi + ((size_t)f * nrhs + col) * ldphi;
+    const double2* pI = diff ? phiI + ((size_t)f * H + (col - D)) * N : nullptr;
+    const double r0 = pv.rcen ? pv.rcen[3 * b] : 0.0, r1 = pv.rcen ? pv.rcen[3 * b + 1] : 0.0,
+                 r2 = pv.rcen ? pv.rcen[3 * b + 2] : 0.0;
+    double acc[24];
+#pragma unroll
+    for (int k = 0; k < 24; k++) acc[k] = 0.0;
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        if (pv.kind[j] != 0 || (pv.body ? pv.body[j] : 0) != b) continue;
+        const double nx = pv.at(P_N, j), ny = pv.at(P_N + 1, j), nz = pv.at(P_N + 2, j);
+        const double cx = pv.at(P_C, j) - r0, cy = pv.at(P_C + 1, j) - r1, cz = pv.at(P_C + 2, j) - r2;
+        const double ar = pv.at(P_AREA, j);
+        const double nj[6] = {nx, ny, nz, cy * nz - cz * ny, cz * nx - cx * nz, cx * ny - cy * nx};
+        double2 v = pc[j], vi = make_double2(0.0, 0.0);
+        if (diff) {
+            vi = pI[j];
+            v.x += vi.x;
+            v.y += vi.y;
         }
-        double r = red[0];
-        __syncthreads();
-        return r;
-    };
-    // columns: c < D radiation (phi_c), D <= c < D + H diffraction (phi_S + phi_I), then H of phi_I;
-    // coordinates i < D: the rigid modes of every body (D = 6 per body)
-    for (int col = 0; col < D + 2 * H; col++) {
-        for (int i = 0; i < D; i++) {
-            double sr = 0.0, si = 0.0;
-            for (int j = threadIdx.x; j < N; j += blockDim.x) {
-                if (pv.kind[j] != 0) continue;
-                double wgt = pv.gen_normal(j, i) * pv.at(P_AREA, j);
-                double2 v;
-                if (col < D + H) {
-                    v = pf[(size_t)col * ldphi + j];
-                    if (col >= D) {
-                        double2 pI = pif[(size_t)(col - D) * N + j];
-                        v.x += pI.x;
-                        v.y += pI.y;
-                    }
-                } else {
-                    v = pif[(size_t)(col - D - H) * N + j];
-                }
-                sr += wgt * v.x;
-                si += wgt * v.y;
-            }
-            sr = block_sum(sr);
-            si = block_sum(si);
-            if (threadIdx.x == 0) {
-                if (col < D) {
-                    double zr = -rho * sr, zi = -rho * si;
-                    Aout[((size_t)f * D + i) * D + col] = zr;
-                    Bout[((size_t)f * D + i) * D + col] = -w * zi;
-                } else {
-                    // i w rho (sr + i si) = (-w rho si, w rho sr)
-                    double2 val = make_double2(-w * rho * si, w * rho * sr);
-                    if (col < D + H)
-                        X[((size_t)f * H + (col - D)) * D + i] = val;
-                    else
-                        FK[((size_t)f * H + (col - D - H)) * D + i] = val;
-                }
-            }
+#pragma unroll
+        for (int m = 0; m < 6; m++) {
+            const double wgt = nj[m] * ar;
+            acc[2 * m] += wgt * v.x;
+            acc[2 * m + 1] += wgt * v.y;
+            acc[12 + 2 * m] += wgt * vi.x;
+            acc[12 + 2 * m + 1] += wgt * vi.y;
         }
     }
+    const int nv = diff ? 24 : 12, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < 24; k++) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[warp][k] = v;
+    }
     __syncthreads();
-    for (int t = threadIdx.x; t < D * H; t += blockDim.x) {
-        size_t o = (size_t)f * H * D + t;
-        SC[o] = make_double2(X[o].x - FK[o].x, X[o].y - FK[o].y);
+    __shared__ double tot[24];
+    if (threadIdx.x < nv) {
+        double t = 0.0;
+        for (int w8 = 0; w8 < (int)(blockDim.x >> 5); w8++) t += red[w8][threadIdx.x];
+        tot[threadIdx.x] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int m = threadIdx.x, i = 6 * b + m;
+        const double w = fi[f].omega;
+        const double sr = tot[2 * m], si = tot[2 * m + 1];
+        if (!diff) {
+            Aout[((size_t)f * D + i) * D + col] = -rho * sr;
+            Bout[((size_t)f * D + i) * D + col] = -w * (-rho * si);
+        } else {
+            // i w rho (sr + i si) = (-w rho si, w rho sr)
+            const size_t o = ((size_t)f * H + (col - D)) * D + i;
+            const double fr = tot[12 + 2 * m], fim = tot[12 + 2 * m + 1];
+            const double2 x = make_double2(-w * rho * si, w * rho * sr), fk = make_double2(-w * rho * fim, w * rho * fr);
+            X[o] = x;
+            FK[o] = fk;
+            SC[o] = make_double2(x.x - fk.x, x.y - fk.y);
+        }
     }
 }
 
 void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, int ldphi,
                    const double2* phiI, double rho, double* A, double* B, double2* X, double2* FK, double2* SC,
                    cudaStream_t s) {
-    k_forces<<<F, 256, 0, s>>>(pv, fi, H, phi, ldphi, phiI, rho, A, B, X, FK, SC);
+    k_forces<<<dim3(6 * pv.nbod + H, pv.nbod, F), 256, 0, s>>>(pv, fi, H, phi, ldphi, phiI, rho, A, B, X, FK, SC);
 }
 
 }  // namespace hbg
