@@ -401,10 +401,57 @@ struct DevBuf {
 static bool finite_depth(double d) { return std::isfinite(d) && d > 0.0; }
 
 // One body through the whole path; outputs to the caller's host arrays.
-static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t body_index, cudaStream_t s) {
-    const int64_t N64 = pr.body.n_panels;
+// The panels of a body given as one symmetry sector followed by their mirror images (image g of panel n
+// at g Ns + n; reflections in the order e, x, y, xy of the character table; a mirrored quadrilateral
+// has its vertex order reversed so that its normal still points into the fluid), with the kinds and
+// the bodies of the images those of their sector panels.
+static void mirror_sector(const HbgBody& b, int G, std::vector<double>& v, std::vector<int32_t>& kind,
+                          std::vector<int32_t>& body) {
+    const size_t Ns = (size_t)b.n_panels;
+    std::vector<std::pair<double, double>> refl = {{1.0, 1.0}};
+    if (b.symmetry == HBG_SYM_YZ || b.symmetry == HBG_SYM_BOTH) refl.push_back({-1.0, 1.0});
+    if (b.symmetry == HBG_SYM_XZ || b.symmetry == HBG_SYM_BOTH) refl.push_back({1.0, -1.0});
+    if (b.symmetry == HBG_SYM_BOTH) refl.push_back({-1.0, -1.0});
+    v.resize(12 * Ns * G);
+    kind.resize(Ns * G);
+    body.resize(b.panel_body ? Ns * G : 0);
+    for (int g = 0; g < G; g++) {
+        const double sx = refl[g].first, sy = refl[g].second;
+        const bool flip = sx * sy < 0.0;
+        for (size_t p = 0; p < Ns; p++) {
+            double* o = &v[12 * (g * Ns + p)];
+            for (int i = 0; i < 4; i++) {
+                const double* q = b.vertices + 12 * p + 3 * (flip && (i & 1) ? 4 - i : i);
+                o[3 * i] = sx * q[0];
+                o[3 * i + 1] = sy * q[1];
+                o[3 * i + 2] = q[2];
+            }
+            kind[g * Ns + p] = b.kinds ? b.kinds[p] : HBG_WET;
+            if (b.panel_body) body[g * Ns + p] = b.panel_body[p];
+        }
+    }
+}
+
+static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_t body_index, cudaStream_t s) {
+    const int64_t N64 = pr_in.body.n_panels;
     if (N64 < 1 || N64 > 60000) throw Failure{HB_ERR_VALUE, "panel count outside 1..60000", body_index};
-    const int N = (int)N64;
+    // symmetry sectors: G systems of Nm = n_panels unknowns per frequency over the N = G Nm panels
+    const int sym = pr_in.body.symmetry;
+    if (sym < HBG_SYM_NONE || sym > HBG_SYM_BOTH) throw Failure{HB_ERR_VALUE, "symmetry outside 0..3", body_index};
+    const int G = sym == HBG_SYM_BOTH ? 4 : sym != HBG_SYM_NONE ? 2 : 1;
+    if (G > 1 && opt.precision == HBG_MIXED && opt.surrogate)
+        throw Failure{HB_ERR_UNSUPPORTED, "symmetry sectors with the wave-term network are not on this route", body_index};
+    HbgProblem pr = pr_in;
+    std::vector<double> mverts;
+    std::vector<int32_t> mkinds, mbody;
+    if (G > 1) {
+        mirror_sector(pr_in.body, G, mverts, mkinds, mbody);
+        pr.body.n_panels = N64 * G;
+        pr.body.vertices = mverts.data();
+        pr.body.kinds = mkinds.data();
+        pr.body.panel_body = pr_in.body.panel_body ? mbody.data() : nullptr;
+    }
+    const int N = (int)(N64 * G), Nm = (int)N64;
     const int F = (int)pr.n_omega, H = (int)pr.n_heading;
     for (int i = 0; i < F; i++)
         if (!(pr.omegas[i] > 0.0) || !std::isfinite(pr.omegas[i]))
@@ -449,13 +496,13 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
             if (k != HBG_WET && k != HBG_INTERIOR) throw Failure{HB_ERR_UNSUPPORTED, "panel kind not on this route", body_index};
             kinds[j] = k;
         }
-    const size_t NN = (size_t)N * N;
+    const size_t NS = (size_t)Nm * N, NN = (size_t)Nm * Nm;  // a statics plane (sector rows), a system matrix
     const int work_cap = std::max(1 << 16, 16 * N);
     dverts.alloc(sizeof(double) * 12 * N);
     dkind.alloc(sizeof(int32_t) * N);
     dplanes.alloc(sizeof(double) * P_PLANES * N);
     dbad.alloc(sizeof(int32_t));
-    dst.alloc(sizeof(double) * 4 * NN);
+    dst.alloc(sizeof(double) * 4 * NS);
     dwork.alloc(sizeof(int32_t) * 2 * work_cap);
     dnwork.alloc(2 * sizeof(int32_t));  // [adaptive worklist size, queue cursor]
     const int32_t big = PANELS_VALID;
@@ -481,12 +528,13 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
         P.end(KF_GEOMETRY, 0.0, s);
         g_launches++;
         PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
+        pv.G = G;
         CUDA_OK(cudaMemsetAsync(dnwork.p, 0, 2 * sizeof(int32_t), s));
         P.begin(s);
         launch_statics(pv, depth, opt.logarithmic, opt.log_tolerance, dst.as<double>(), dwork.as<int32_t>(),
                        dnwork.as<int32_t>(), work_cap, s, opt.precision == HBG_MIXED);
         // algorithmic bytes: the four FP64 planes written
-        P.end(KF_STATICS, 32.0 * (double)NN, s);
+        P.end(KF_STATICS, 32.0 * (double)NS, s);
         // the first invalid panel (geometry) and the adaptive worklist size, read at the next wait of the
         // solve; the adaptive kernel takes the size from device memory and does nothing on invalid panels
         CUDA_OK(cudaMemcpyAsync(hflags, dbad.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -511,7 +559,7 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
     // the mixed form's assembly kernels skip their work on invalid panels (the flag in device memory),
     // so that its solve runs without a host wait until the end; the FP64 form waits here
     PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>(), dbad.as<int32_t>(),
-                  multi ? dpbody.as<int32_t>() : nullptr, pr.body.rotation_centers ? drcen.as<double>() : nullptr, nbod};
+                  multi ? dpbody.as<int32_t>() : nullptr, pr.body.rotation_centers ? drcen.as<double>() : nullptr, nbod, G};
     if (F == 0 || opt.precision != HBG_MIXED) {
         run_statics();
         CUDA_OK(cudaStreamSynchronize(s));
@@ -532,8 +580,11 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
         return;
     }
     // ---- frequency batches
-    size_t per_freq = 2 * NN * sizeof(double2) + (size_t)(3 * nrhs + H) * N * sizeof(double2) +
-                      (size_t)N * sizeof(int32_t) + (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)FP_PLANES * N * 8 +
+    // per frequency: G systems (S, A, right-hand sides, solutions, pivots), the boundary values and incident
+    // wave of every panel, with sectors the projected right-hand sides and the recombined potentials
+    size_t per_freq = G * (2 * NN * sizeof(double2) + (size_t)2 * nrhs * Nm * sizeof(double2) + (size_t)Nm * 4 + 4) +
+                      (size_t)(nrhs + H) * N * sizeof(double2) + (G > 1 ? (size_t)2 * nrhs * N * sizeof(double2) : 0) +
+                      (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)FP_PLANES * N * 8 +
                                                               (size_t)6912 * 3 * 8
                                                         : 0);
     // the batch size from free memory, kept per thread and device for the same problem shape while the
@@ -541,15 +592,17 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
     int B = 0;
     {
         struct BatchChoice {
-            int N = -1, nrhs = -1, fin = -1, F = -1, B = 0;
+            int N = -1, G = -1, nrhs = -1, fin = -1, F = -1, B = 0;
             int64_t max_batch = -2;
         };
         static thread_local BatchChoice last[16];
         int dev_b = 0;
         cudaGetDevice(&dev_b);
         BatchChoice& c = last[dev_b < 0 || dev_b >= 16 ? 0 : dev_b];
-        const bool same = c.N == N && c.nrhs == nrhs && c.fin == (int)fin && c.F == F && c.max_batch == opt.max_batch;
-        if (same && c.B > 0 && ws.bytes[WS_S] >= sizeof(double2) * NN * c.B && ws.bytes[WS_A] >= sizeof(double2) * NN * c.B) {
+        const bool same = c.N == N && c.G == G && c.nrhs == nrhs && c.fin == (int)fin && c.F == F &&
+                          c.max_batch == opt.max_batch;
+        const size_t mats = NN * G * (size_t)std::max(c.B, 0);
+        if (same && c.B > 0 && ws.bytes[WS_S] >= sizeof(double2) * mats && ws.bytes[WS_A] >= sizeof(double2) * mats) {
             B = c.B;
         } else {
             size_t freeb = 0, totalb = 0;
@@ -558,20 +611,25 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
             B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)(freeb + reusable)) / per_freq);
             if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
             B = std::min(B, F);
-            c = BatchChoice{N, nrhs, (int)fin, F, B, opt.max_batch};
+            c = BatchChoice{N, G, nrhs, (int)fin, F, B, opt.max_batch};
         }
     }
+    const size_t BS = (size_t)B * G;  // systems per batch
     WsBuf dS(ws, WS_S), dA(ws, WS_A), du(ws, WS_U), drhs(ws, WS_RHS), dX(ws, WS_X), dphiI(ws, WS_PHII),
         dipiv(ws, WS_IPIV), dinfo(ws, WS_INFO), dfi(ws, WS_FI), dfd(ws, WS_FD), dtiles(ws, WS_TILES),
-        dscr(ws, WS_SCR), dfpt(ws, WS_FPT), dheads(ws, WS_HEADS), dout(ws, WS_OUT);
-    dS.alloc(sizeof(double2) * NN * B);
-    dA.alloc(sizeof(double2) * NN * B);
+        dscr(ws, WS_SCR), dfpt(ws, WS_FPT), dheads(ws, WS_HEADS), dout(ws, WS_OUT), dup(ws, WS_UP), dphi(ws, WS_PHI);
+    dS.alloc(sizeof(double2) * NN * BS);
+    dA.alloc(sizeof(double2) * NN * BS);
     du.alloc(sizeof(double2) * (size_t)nrhs * N * B);
-    drhs.alloc(sizeof(double2) * (size_t)nrhs * N * B);
-    dX.alloc(sizeof(double2) * (size_t)nrhs * N * B);
+    drhs.alloc(sizeof(double2) * (size_t)nrhs * Nm * BS);
+    dX.alloc(sizeof(double2) * (size_t)nrhs * Nm * BS);
+    if (G > 1) {
+        dup.alloc(sizeof(double2) * (size_t)nrhs * Nm * BS);
+        dphi.alloc(sizeof(double2) * (size_t)nrhs * N * B);
+    }
     dphiI.alloc(sizeof(double2) * (size_t)std::max(H, 1) * N * B);
-    dipiv.alloc(sizeof(int32_t) * (size_t)N * B);
-    dinfo.alloc(sizeof(int32_t) * B);
+    dipiv.alloc(sizeof(int32_t) * (size_t)Nm * BS);
+    dinfo.alloc(sizeof(int32_t) * BS);
     dfi.alloc(sizeof(FreqInfo) * B);
     dfd.alloc(sizeof(FdParams) * B);
     if (fin) {
@@ -587,14 +645,14 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
     const size_t out_per = 2 * (size_t)D * D * sizeof(double) + 3 * (size_t)H * D * sizeof(double2);
     dout.alloc(out_per * B);
     // page-locked outputs and pivot flags: their reads queue behind the work
-    unsigned char* hout = static_cast<unsigned char*>(ws.host(HS_OUT, out_per * B + sizeof(int32_t) * B));
+    unsigned char* hout = static_cast<unsigned char*>(ws.host(HS_OUT, out_per * B + sizeof(int32_t) * BS));
     if (!hout) throw Failure{HB_ERR_INTERNAL, "page-locked host memory could not be allocated", body_index};
     int32_t* info = reinterpret_cast<int32_t*>(hout + out_per * B);
     std::vector<FreqInfo> fi(B);
     std::vector<FdParams> fdh(B);
     for (int f0 = 0; f0 < F; f0 += B) {
         if (opt.cancel && *opt.cancel) throw Failure{HB_ERR_CANCELLED, "the solve was cancelled", body_index, f0};
-        const int nb = std::min(B, F - f0);
+        const int nb = std::min(B, F - f0), ns = nb * G;
         for (int i = 0; i < nb; i++) {
             double w = pr.omegas[f0 + i], K = w * w / opt.gravity;
             fi[i].omega = w;
@@ -620,33 +678,39 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
             P.begin(s);
             launch_assemble_f64(pv, dst.as<double>(), nb, dfi.as<FreqInfo>(), dfd.as<FdParams>(), dtiles.as<double>(),
                                 dfpt.as<double>(), fin, dS.as<double2>(), dA.as<double2>(), NN, s);
+            if (G > 1) launch_sectors_f64(dS.as<double2>(), dA.as<double2>(), nb, G, Nm, NN, s);
             // algorithmic bytes per pair: 4 statics read (32 B), S and A written (32 B)
-            P.end(KF_ASSEMBLE, 64.0 * (double)NN * nb, s);
+            P.end(KF_ASSEMBLE, 64.0 * (double)NN * ns, s);
             P.begin(s);
             launch_boundary(pv, nb, dfi.as<FreqInfo>(), H, dheads.as<double>(), depth, opt.gravity, du.as<double2>(),
                             dphiI.as<double2>(), s);
             P.end(KF_BOUNDARY, 0.0, s);
+            const double2* urhs = du.as<double2>();
+            if (G > 1) {
+                launch_project(du.as<double2>(), dup.as<double2>(), nb, G, Nm, nrhs, Nm, s);
+                urhs = dup.as<double2>();
+            }
             P.begin(s);
-            launch_rhs_f64(N, nb, nrhs, dS.as<double2>(), NN, du.as<double2>(), drhs.as<double2>(), s);
+            launch_rhs_f64(Nm, ns, nrhs, dS.as<double2>(), NN, urhs, drhs.as<double2>(), s);
             // S read once (16 B per entry)
-            P.end(KF_RHS, 16.0 * (double)NN * nb, s);
-            g_launches += 3;
+            P.end(KF_RHS, 16.0 * (double)NN * ns, s);
+            g_launches += 3 + 2 * (G > 1);
             t.stop();
         }
         {
             EventTimer t(s, &prof[2]);
-            lu_factor_f64(N, nb, dA.as<double2>(), NN, dipiv.as<int32_t>(), dinfo.as<int32_t>(), s, &g_launches);
+            lu_factor_f64(Nm, ns, dA.as<double2>(), NN, dipiv.as<int32_t>(), dinfo.as<int32_t>(), s, &g_launches);
             t.stop();
         }
         {
             EventTimer t(s, &prof[3]);
             KernelProfiler& P = profiler();
             P.begin(s);
-            if (lu_solve_f64(N, nb, dA.as<double2>(), NN, dipiv.as<int32_t>(), nrhs, drhs.as<double2>(),
+            if (lu_solve_f64(Nm, ns, dA.as<double2>(), NN, dipiv.as<int32_t>(), nrhs, drhs.as<double2>(),
                              dX.as<double2>(), s))
                 throw Failure{HB_ERR_UNSUPPORTED, "too many right-hand sides or panels for the substitution kernel", body_index};
             // the factors read once (16 B per entry)
-            P.end(KF_LU_SOLVE, 16.0 * (double)NN * nb, s);
+            P.end(KF_LU_SOLVE, 16.0 * (double)NN * ns, s);
             g_launches += 1;
             t.stop();
         }
@@ -659,13 +723,20 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
             double2* dFK = dXo + (size_t)H * D * nb;
             double2* dSC = dFK + (size_t)H * D * nb;
             KernelProfiler& P = profiler();
+            // the potentials of every panel: the sector solutions recombined (one system: as solved)
+            const double2* phi = dX.as<double2>();
+            if (G > 1) {
+                launch_recombine(dX.as<double2>(), dphi.as<double2>(), nb, G, Nm, nrhs, Nm, s);
+                phi = dphi.as<double2>();
+                g_launches++;
+            }
             P.begin(s);
-            launch_forces(pv, nb, dfi.as<FreqInfo>(), H, dX.as<double2>(), N, dphiI.as<double2>(), opt.density, dAo,
-                          dBo, dXo, dFK, dSC, s);
+            launch_forces(pv, nb, dfi.as<FreqInfo>(), H, phi, N, dphiI.as<double2>(), opt.density, dAo, dBo, dXo, dFK,
+                          dSC, s);
             P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
             g_launches += 1;
             CUDA_OK(cudaMemcpyAsync(hout, dout.p, out_per * nb, cudaMemcpyDeviceToHost, s));
-            CUDA_OK(cudaMemcpyAsync(info, dinfo.p, sizeof(int32_t) * nb, cudaMemcpyDeviceToHost, s));
+            CUDA_OK(cudaMemcpyAsync(info, dinfo.p, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, s));
             t.stop();
             solve_end().record(s);
         }
@@ -680,9 +751,11 @@ static void solve_problem(const HbgProblem& pr, const HbgOptions& opt, int64_t b
         const double* hFK = hX + (size_t)H * 2 * D * nb;
         const double* hSC = hFK + (size_t)H * 2 * D * nb;
         for (int i = 0; i < nb; i++) {
-            if (info[i] != 0)
-                throw Failure{HB_ERR_NUMERICAL, "singular system matrix (zero pivot " + std::to_string(info[i]) + ")",
-                              body_index, f0 + i};
+            for (int c = 0; c < G; c++)
+                if (info[i * G + c] != 0)
+                    throw Failure{HB_ERR_NUMERICAL,
+                                  "singular system matrix (zero pivot " + std::to_string(info[i * G + c]) + ")",
+                                  body_index, f0 + i};
             for (size_t q = 0; q < DD; q++)
                 if (!std::isfinite(hA[DD * i + q]) || !std::isfinite(hB[DD * i + q]))
                     throw Failure{HB_ERR_NUMERICAL, "non-finite solution", body_index, f0 + i};
@@ -828,7 +901,21 @@ extern "C" HbStatus hbg_debug_matrices(const HbgBody* body, double omega, const 
             return fail({HB_ERR_UNSUPPORTED, "no CUDA device: this library runs the path on the GPU only"});
         CUDA_OK(cudaSetDevice(opt->device));
         device_ctx(opt->device);
-        const int N = (int)body->n_panels;
+        // with symmetry planes: the sector's panels mirrored, statics of the sector rows, G sector matrices
+        const int sym = body->symmetry;
+        if (sym < HBG_SYM_NONE || sym > HBG_SYM_BOTH) return fail({HB_ERR_VALUE, "symmetry outside 0..3"});
+        const int G = sym == HBG_SYM_BOTH ? 4 : sym != HBG_SYM_NONE ? 2 : 1;
+        const int Nm = (int)body->n_panels, N = Nm * G;
+        std::vector<double> mverts;
+        std::vector<int32_t> kinds, mbody;
+        if (G > 1) {
+            mirror_sector(*body, G, mverts, kinds, mbody);
+        } else {
+            kinds.assign(N, 0);
+            if (body->kinds)
+                for (int j = 0; j < N; j++) kinds[j] = body->kinds[j];
+        }
+        const double* verts = G > 1 ? mverts.data() : body->vertices;
         const bool fin = finite_depth(opt->depth);
         const double depth = fin ? opt->depth : 0.0;
         cudaStream_t s = 0;
@@ -837,17 +924,15 @@ extern "C" HbStatus hbg_debug_matrices(const HbgBody* body, double omega, const 
         dkind.alloc(sizeof(int32_t) * N);
         dplanes.alloc(sizeof(double) * P_PLANES * N);
         dbad.alloc(sizeof(int32_t));
-        CUDA_OK(cudaMemcpy(dverts.p, body->vertices, sizeof(double) * 12 * N, cudaMemcpyHostToDevice));
-        std::vector<int32_t> kinds(N, 0);
-        if (body->kinds)
-            for (int j = 0; j < N; j++) kinds[j] = body->kinds[j];
+        CUDA_OK(cudaMemcpy(dverts.p, verts, sizeof(double) * 12 * N, cudaMemcpyHostToDevice));
         CUDA_OK(cudaMemcpy(dkind.p, kinds.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
         int32_t big = 0x7fffffff;
         CUDA_OK(cudaMemcpy(dbad.p, &big, sizeof big, cudaMemcpyHostToDevice));
         launch_panel_geometry(N, dverts.as<double>(), dkind.as<int32_t>(), dplanes.as<double>(), dbad.as<int32_t>(), s);
         PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
-        const size_t NN = (size_t)N * N;
-        dst.alloc(sizeof(double) * 4 * NN);
+        pv.G = G;
+        const size_t NS = (size_t)Nm * N, NN = (size_t)Nm * Nm;
+        dst.alloc(sizeof(double) * 4 * NS);
         const int cap = std::max(1 << 16, 16 * N);
         dwork.alloc(sizeof(int32_t) * 2 * cap);
         dnwork.alloc(sizeof(int32_t));
@@ -872,15 +957,16 @@ extern "C" HbStatus hbg_debug_matrices(const HbgBody* body, double omega, const 
             launch_fd_tiles(1, dfd.as<FdParams>(), dtiles.as<double>(), dscr.as<double>(), s);
             launch_fin_points(pv, 1, dfd.as<FdParams>(), dfpt.as<double>(), s);
         }
-        dS.alloc(sizeof(double2) * NN);
-        dA.alloc(sizeof(double2) * NN);
+        dS.alloc(sizeof(double2) * NN * G);
+        dA.alloc(sizeof(double2) * NN * G);
         launch_assemble_f64(pv, dst.as<double>(), 1, dfi.as<FreqInfo>(), dfd.as<FdParams>(), dtiles.as<double>(),
                             dfpt.as<double>(), fin, dS.as<double2>(), dA.as<double2>(), NN, s);
+        if (G > 1) launch_sectors_f64(dS.as<double2>(), dA.as<double2>(), 1, G, Nm, NN, s);
         CUDA_OK(cudaDeviceSynchronize());
         CUDA_OK(cudaGetLastError());
-        if (statics) CUDA_OK(cudaMemcpy(statics, dst.p, sizeof(double) * 4 * NN, cudaMemcpyDeviceToHost));
-        if (S) CUDA_OK(cudaMemcpy(S, dS.p, sizeof(double2) * NN, cudaMemcpyDeviceToHost));
-        if (A) CUDA_OK(cudaMemcpy(A, dA.p, sizeof(double2) * NN, cudaMemcpyDeviceToHost));
+        if (statics) CUDA_OK(cudaMemcpy(statics, dst.p, sizeof(double) * 4 * NS, cudaMemcpyDeviceToHost));
+        if (S) CUDA_OK(cudaMemcpy(S, dS.p, sizeof(double2) * NN * G, cudaMemcpyDeviceToHost));
+        if (A) CUDA_OK(cudaMemcpy(A, dA.p, sizeof(double2) * NN * G, cudaMemcpyDeviceToHost));
         return HB_OK;
     } catch (const Failure& f) {
         return fail(f);

@@ -77,6 +77,10 @@ struct PanelsView {
     const int32_t* body = nullptr;
     const double* rcen = nullptr;
     int nbod = 1;
+    // symmetry sectors (lo_geometry.rs:25-36): the N panels are the Ns = N / G panels of one sector
+    // followed by their images under each reflection of the group (image g of panel n at g Ns + n,
+    // order e, then x, y, xy reflections); the statics and the system matrices have the Ns sector rows
+    int G = 1;
     __device__ __forceinline__ bool invalid() const { return bad && *(volatile const int32_t*)bad != PANELS_VALID; }
     // generalized normal of rigid mode `mode` (body mode / 6: surge, sway, heave, roll, pitch, yaw about
     // its rotation centre) on panel j: zero on the panels of the other bodies

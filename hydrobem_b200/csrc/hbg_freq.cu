@@ -175,7 +175,12 @@ struct OutF32 {
     }
 };
 
-template <bool FINITE, class Out>
+// Symmetry sectors (SECT, G = pv.G > 1): block y = f G + g assembles the image block g of frequency f,
+// M_g(k, n) = S(x_k, panel g n), over the Ns = N / G sector panels; a reflection keeps depths and
+// horizontal distances, so (k, g n) and (n, g k) still share one pair kernel.  The statics of the image
+// block are the Ns x Ns block g of the Ns x N statics; the free term sits on the diagonal of block 0.
+// k_sectors then combines the G blocks of a frequency into its G sector matrices.
+template <bool FINITE, class Out, bool SECT>
 __global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView pv, const double* __restrict__ st,
                                                   const FreqInfo* __restrict__ fi, const FdParams* __restrict__ fdp,
                                                   const typename Out::Tile* __restrict__ tiles,
@@ -184,7 +189,7 @@ __global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView 
     // overwritten with the results (S, A) of entry (n, k) by the one thread that owns it
     __shared__ double sT[4][32][33];
     if (pv.invalid()) return;  // invalid panels: the solve reports them
-    const int N = pv.N;
+    const int G = SECT ? pv.G : 1, Nf = pv.N, N = SECT ? Nf / G : Nf;
     const int nt = (N + 31) / 32;
     // tile pair from the linear index: row-block kb <= column-block nb
     int idx = blockIdx.x, kb = 0;
@@ -193,67 +198,74 @@ __global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView 
         kb++;
     }
     const int nb = kb + idx;
-    const int f = blockIdx.y;
+    const int y = blockIdx.y, f = SECT ? y / G : y, g = SECT ? y - f * G : 0;
     const int K0 = kb * 32, N0 = nb * 32;
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const size_t NN = (size_t)N * N;
+    const size_t NN = (size_t)N * Nf;  // one statics plane
+    const double* stg = st + (size_t)g * N * N;
     const FreqInfo info = fi[f];
     const double K = info.K, logc = info.logc;
-    // statics of (n, k): rows n in N0, panels k in K0
+    // statics of (n, g k): rows n in N0, panels k in K0
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         int n = N0 + tx, k = K0 + ty + 8 * i;
         if (n < N && k < N)
 #pragma unroll
-            for (int q = 0; q < 4; q++) sT[q][ty + 8 * i][tx] = __ldg(st + q * NN + (size_t)n + (size_t)k * N);
+            for (int q = 0; q < 4; q++) sT[q][ty + 8 * i][tx] = __ldg(stg + q * NN + (size_t)n + (size_t)k * N);
     }
     __syncthreads();
     const int k = K0 + tx;
-    double xk[3] = {0, 0, 0}, nk[3] = {0, 0, 0}, ak = 0;
+    // xk: the field point of row k; ck, nk, ak: panel g k (the source of entry (n, g k))
+    double xk[3] = {0, 0, 0}, ck[3] = {0, 0, 0}, nk[3] = {0, 0, 0}, ak = 0;
     int kindk = 0;
     if (k < N) {
+        const int gk = g * N + k;
         for (int d = 0; d < 3; d++) {
-            xk[d] = pv.at(P_C + d, k);
-            nk[d] = pv.at(P_N + d, k);
+            ck[d] = pv.at(P_C + d, gk);
+            nk[d] = pv.at(P_N + d, gk);
+            xk[d] = SECT ? pv.at(P_C + d, k) : ck[d];
         }
-        ak = pv.at(P_AREA, k);
+        ak = pv.at(P_AREA, gk);
         kindk = pv.kind[k];
     }
     const FdParams* fd = FINITE ? fdp + f : nullptr;
     const typename Out::Tile* T1 = FINITE ? tiles + (size_t)f * (Out::kT1 + Out::kT2) : nullptr;
     const typename Out::Tile* T2 = FINITE ? T1 + Out::kT1 : nullptr;
-    const double* fp = FINITE ? fpt + (size_t)f * FP_PLANES * N : nullptr;
+    const double* fp = FINITE ? fpt + (size_t)f * FP_PLANES * Nf : nullptr;
 #pragma unroll 1
     for (int i = 0; i < 4; i++) {
         const int nl = ty + 8 * i, n = N0 + nl;
         bool live = k < N && n < N && (kb != nb || k <= n);
         if (!live) continue;
-        double xn[3], nn3[3];
+        // cn, nn3, an: panel g n (the source of entry (k, g n)); xn: the field point of row n
+        double xn[3], cn[3], nn3[3];
+        const int gn = g * N + n;
         for (int d = 0; d < 3; d++) {
-            xn[d] = pv.at(P_C + d, n);
-            nn3[d] = pv.at(P_N + d, n);
+            cn[d] = pv.at(P_C + d, gn);
+            nn3[d] = pv.at(P_N + d, gn);
+            xn[d] = SECT ? pv.at(P_C + d, n) : cn[d];
         }
-        double an = pv.at(P_AREA, n);
+        double an = pv.at(P_AREA, gn);
         int kindn = pv.kind[n];
         // R without contraction: the finite-depth kernel switches form at R = h/2 exactly
-        double dx = xk[0] - xn[0], dy = xk[1] - xn[1];
+        double dx = xk[0] - cn[0], dy = xk[1] - cn[1];
         double R = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
         Kern w;
         if (FINITE) {
-            w = finite_kernel<Out::kF32>(*fd, T1, T2, R, xk[2], xn[2], fp + k, fp + n, N);
+            w = finite_kernel<Out::kF32>(*fd, T1, T2, R, xk[2], cn[2], fp + k, fp + n, Nf);
         } else {
-            w = pair_kernel_inf<Out::kF32>(K, R, xk[2], xn[2]);
+            w = pair_kernel_inf<Out::kF32>(K, R, xk[2], cn[2]);
         }
-        // entry (k, n): the field point x_k against panel n
+        // entry (k, n): the field point x_k against panel g n
         size_t o1 = (size_t)k + (size_t)n * N;
         double2 s1, d1;
-        apply_kernel(__ldg(st + o1), __ldg(st + NN + o1), __ldg(st + 2 * NN + o1), __ldg(st + 3 * NN + o1), an,
-                     nn3[0], nn3[1], nn3[2], kindn, xk, xn, K, logc, w, R, false, s1, d1);
-        out.put(f, k, n, s1, make_double2((k == n ? free_term(kindk) : 0.0) - d1.x, -d1.y));
+        apply_kernel(__ldg(stg + o1), __ldg(stg + NN + o1), __ldg(stg + 2 * NN + o1), __ldg(stg + 3 * NN + o1), an,
+                     nn3[0], nn3[1], nn3[2], kindn, xk, cn, K, logc, w, R, false, s1, d1);
+        out.put(y, k, n, s1, make_double2((g == 0 && k == n ? free_term(kindk) : 0.0) - d1.x, -d1.y));
         if (n != k) {
             double2 s2, d2;
             apply_kernel(sT[0][tx][nl], sT[1][tx][nl], sT[2][tx][nl], sT[3][tx][nl], ak, nk[0], nk[1], nk[2], kindk,
-                         xn, xk, K, logc, w, R, true, s2, d2);
+                         xn, ck, K, logc, w, R, true, s2, d2);
             sT[0][tx][nl] = s2.x;
             sT[1][tx][nl] = s2.y;
             sT[2][tx][nl] = -d2.x;
@@ -266,20 +278,112 @@ __global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView 
     for (int i = 0; i < 4; i++) {
         int n = N0 + tx, kl = ty + 8 * i, kk = K0 + kl;
         if (n < N && kk < N && (kb != nb || n > kk))
-            out.put(f, n, kk, make_double2(sT[0][kl][tx], sT[1][kl][tx]), make_double2(sT[2][kl][tx], sT[3][kl][tx]));
+            out.put(y, n, kk, make_double2(sT[0][kl][tx], sT[1][kl][tx]), make_double2(sT[2][kl][tx], sT[3][kl][tx]));
+    }
+}
+
+template <class Out>
+static void assemble(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
+                     const typename Out::Tile* tiles, const double* fpt, bool finite, Out o, cudaStream_t s) {
+    const int nt = (pv.N / pv.G + 31) / 32;
+    dim3 grid(nt * (nt + 1) / 2, F * pv.G), blk(32, 8);
+    if (pv.G > 1) {
+        if (finite)
+            k_assemble<true, Out, true><<<grid, blk, 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
+        else
+            k_assemble<false, Out, true><<<grid, blk, 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
+    } else if (finite) {
+        k_assemble<true, Out, false><<<grid, blk, 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
+    } else {
+        k_assemble<false, Out, false><<<grid, blk, 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
     }
 }
 
 void launch_assemble_f64(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
                          const double* tiles, const double* fpt, bool finite, double2* S, double2* A,
                          size_t mat_stride, cudaStream_t s) {
-    int nt = (pv.N + 31) / 32;
-    dim3 grid(nt * (nt + 1) / 2, F);
-    OutF64 o{S, A, mat_stride, pv.N};
-    if (finite)
-        k_assemble<true, OutF64><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
-    else
-        k_assemble<false, OutF64><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
+    assemble(pv, st, F, fi, fd, tiles, fpt, finite, OutF64{S, A, mat_stride, pv.N / pv.G}, s);
+}
+
+// ------------------------------------------------------------------ symmetry sectors
+// Characters of the reflection group, elements e, x, y, xy reflections (lo_geometry.rs:25-36):
+// chi_c(g) = (-1)^popc(c & g) for G = 2 and 4.
+__device__ __forceinline__ bool chi_neg(int c, int g) { return __popc(c & g) & 1; }
+
+// The G image blocks M_g of each frequency (matrices f G .. f G + G - 1 of S and of A) replaced in
+// place by the sector matrices sum_g chi_c(g) M_g (lo_frequency.rs:276-346: S_c(k, n) =
+// sum_g chi_c(g) S(k, g n), A_c likewise; the free term of block 0 enters every sector).  Entries
+// (k, n) < Nm of `nplanes` planes, each entry `comps` consecutive T at (n ld + k) comps; sums in FP64.
+template <typename T>
+__global__ void k_sectors(T* __restrict__ S, T* __restrict__ A, int G, int Nm, int ld, int comps, size_t plane,
+                          int nplanes, size_t mstride) {
+    const int f = blockIdx.y;
+    const size_t per = (size_t)Nm * Nm * comps * nplanes;
+    for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * per; t += (size_t)gridDim.x * blockDim.x) {
+        const size_t e = t < per ? t : t - per;
+        T* M = t < per ? S : A;
+        const int c = (int)(e % comps);
+        const size_t r = e / comps;
+        const int k = (int)(r % Nm), n = (int)((r / Nm) % Nm), p = (int)(r / ((size_t)Nm * Nm));
+        T* b = M + (size_t)f * G * mstride + (size_t)p * plane + ((size_t)n * ld + k) * comps + c;
+        double v[4];
+        for (int g = 0; g < G; g++) v[g] = (double)b[(size_t)g * mstride];
+        for (int cc = 0; cc < G; cc++) {
+            double w = 0.0;
+            for (int g = 0; g < G; g++) w += chi_neg(cc, g) ? -v[g] : v[g];
+            b[(size_t)cc * mstride] = (T)w;
+        }
+    }
+}
+
+void launch_sectors_f64(double2* S, double2* A, int F, int G, int Nm, size_t mat_stride, cudaStream_t s) {
+    k_sectors<double><<<dim3(296, F), 256, 0, s>>>(reinterpret_cast<double*>(S), reinterpret_cast<double*>(A), G, Nm,
+                                                    Nm, 2, 0, 1, 2 * mat_stride);
+}
+
+void launch_sectors_f32(float* S, float* A, int F, int G, int Nm, int Np, cudaStream_t s) {
+    const size_t plane = (size_t)Np * Np;
+    k_sectors<float><<<dim3(296, F), 256, 0, s>>>(S, A, G, Nm, Np, 1, plane, 2, 2 * plane);
+}
+
+// Right-hand-side vectors projected on the sectors (lo_frequency.rs:875-884): up[f G + c][col][n] =
+// (1/G) sum_g chi_c(g) u[f][col][g Nm + n]; u holds every panel (Nf = G Nm), up has leading dimension ldp.
+__global__ void k_project(const double2* __restrict__ u, double2* __restrict__ up, int G, int Nm, int nrhs, int ldp) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x, col = blockIdx.y, sys = blockIdx.z;
+    if (n >= Nm) return;
+    const int f = sys / G, c = sys - f * G, Nf = G * Nm;
+    const double2* uf = u + ((size_t)f * nrhs + col) * Nf + n;
+    double re = 0.0, im = 0.0;
+    for (int g = 0; g < G; g++) {
+        const double2 v = uf[(size_t)g * Nm];
+        re += chi_neg(c, g) ? -v.x : v.x;
+        im += chi_neg(c, g) ? -v.y : v.y;
+    }
+    up[((size_t)sys * nrhs + col) * ldp + n] = make_double2(re / G, im / G);
+}
+
+void launch_project(const double2* u, double2* up, int F, int G, int Nm, int nrhs, int ldp, cudaStream_t s) {
+    k_project<<<dim3((Nm + 127) / 128, nrhs, F * G), 128, 0, s>>>(u, up, G, Nm, nrhs, ldp);
+}
+
+// The potentials on every panel from the sector solutions (lo_frequency.rs:931-943):
+// phi[f][col][g Nm + n] = sum_c chi_c(g) x[f G + c][col][n] (x with leading dimension ldx).
+__global__ void k_recombine(const double2* __restrict__ x, double2* __restrict__ phi, int G, int Nm, int nrhs,
+                            int ldx) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x, col = blockIdx.y, f = blockIdx.z / G,
+              g = blockIdx.z - f * G;
+    if (n >= Nm) return;
+    double re = 0.0, im = 0.0;
+    for (int c = 0; c < G; c++) {
+        const double2 v = x[((size_t)(f * G + c) * nrhs + col) * ldx + n];
+        re += chi_neg(c, g) ? -v.x : v.x;
+        im += chi_neg(c, g) ? -v.y : v.y;
+    }
+    phi[((size_t)f * nrhs + col) * G * Nm + (size_t)g * Nm + n] = make_double2(re, im);
+}
+
+void launch_recombine(const double2* x, double2* phi, int F, int G, int Nm, int nrhs, int ldx, cudaStream_t s) {
+    k_recombine<<<dim3((Nm + 127) / 128, nrhs, F * G), 128, 0, s>>>(x, phi, G, Nm, nrhs, ldx);
 }
 
 // The finite-depth tiles of a batch for the mixed form: per tile and quantity (one thread each) the
@@ -336,13 +440,7 @@ void launch_tiles_f32(int F, const double* tiles, float* tiles_f, cudaStream_t s
 void launch_assemble_f32(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
                          const float* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
                          cudaStream_t s) {
-    int nt = (pv.N + 31) / 32;
-    dim3 grid(nt * (nt + 1) / 2, F);
-    OutF32 o{S, A, 2 * (size_t)Np * Np, Np};
-    if (finite)
-        k_assemble<true, OutF32><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
-    else
-        k_assemble<false, OutF32><<<grid, dim3(32, 8), 0, s>>>(pv, st, fi, fd, tiles, fpt, o);
+    assemble(pv, st, F, fi, fd, tiles, fpt, finite, OutF32{S, A, 2 * (size_t)Np * Np, Np}, s);
 }
 
 // ------------------------------------------------------------------ boundary values

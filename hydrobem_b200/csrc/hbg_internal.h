@@ -69,7 +69,7 @@ enum WsSlot {
     WS_VERTS = 0, WS_KIND, WS_PLANES, WS_BAD, WS_ST, WS_WORK, WS_NWORK, WS_S, WS_A, WS_U, WS_RHS, WS_X, WS_PHII,
     WS_IPIV, WS_INFO, WS_FI, WS_FD, WS_TILES, WS_SCR, WS_FPT, WS_HEADS, WS_OUT, WS_S32, WS_A32, WS_W, WS_P2,
     WS_P3, WS_PL, WS_PU, WS_B, WS_XM, WS_R, WS_NORMS, WS_ERR, WS_PART, WS_DINV, WS_TILES_F, WS_SG_PARAMS,
-    WS_SG_IMG, WS_SG_COUNT, WS_TRI_CTRL, WS_RS, WS_L16, WS_P3H, WS_PBODY, WS_RCEN, WS_COUNT
+    WS_SG_IMG, WS_SG_COUNT, WS_TRI_CTRL, WS_RS, WS_L16, WS_P3H, WS_PBODY, WS_RCEN, WS_UP, WS_PHI, WS_COUNT
 };
 
 // Page-locked host buffers of a solve: a device-to-host copy into pageable memory waits for the
@@ -258,7 +258,8 @@ void launch_statics_adaptive_q(const PanelsView& pv, const int32_t* work, int32_
 void launch_fd_tiles(int F, const FdParams* fd, double* tiles, double* scratch, cudaStream_t s);
 void launch_fin_points(const PanelsView& pv, int F, const FdParams* fd, double* fpt, cudaStream_t s);
 
-// assembly of S and A (complex128, column-major N x N per frequency, stride mat_stride elements)
+// assembly of S and A (complex128, column-major Nm x Nm per matrix, stride mat_stride elements; Nm =
+// pv.N / pv.G, and with symmetry sectors the G image blocks of each frequency, matrices f G + g)
 void launch_assemble_f64(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
                          const double* tiles, const double* fpt, bool finite, double2* S, double2* A,
                          size_t mat_stride, cudaStream_t s);
@@ -266,6 +267,13 @@ void launch_assemble_f32(const PanelsView& pv, const double* st, int F, const Fr
                          const float* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
                          cudaStream_t s);
 void launch_tiles_f32(int F, const double* tiles, float* tiles_f, cudaStream_t s);
+// symmetry sectors: the image blocks of F frequencies into their sector matrices (in place), the
+// right-hand sides projected on the sectors up[F G][nrhs][ldp], the potentials of every panel
+// phi[F][nrhs][G Nm] from the sector solutions x[F G][nrhs][ldx]
+void launch_sectors_f64(double2* S, double2* A, int F, int G, int Nm, size_t mat_stride, cudaStream_t s);
+void launch_sectors_f32(float* S, float* A, int F, int G, int Nm, int Np, cudaStream_t s);
+void launch_project(const double2* u, double2* up, int F, int G, int Nm, int nrhs, int ldp, cudaStream_t s);
+void launch_recombine(const double2* x, double2* phi, int F, int G, int Nm, int nrhs, int ldx, cudaStream_t s);
 // the wave-term network inside the mixed assembly: its parameters followed by the outputs' means and
 // spreads
 constexpr int SURROGATE_FLOATS = 50822 + 12;

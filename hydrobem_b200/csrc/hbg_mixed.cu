@@ -155,8 +155,10 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                             bool fin, double depth, cudaStream_t s, double* prof, int64_t* launches, const char** msg,
                             int64_t* freq, const std::function<void()>& start) {
     KernelProfiler& P = profiler();
-    const int N = pv.N, F = (int)pr.n_omega, H = (int)pr.n_heading, D = 6 * pv.nbod, nrhs = D + H;
-    const int Np = (N + NBL - 1) / NBL * NBL;
+    // N panels; with symmetry sectors G systems of Nm = N / G unknowns per frequency (one of N otherwise)
+    const int N = pv.N, G = pv.G, Nm = N / G, F = (int)pr.n_omega, H = (int)pr.n_heading, D = 6 * pv.nbod,
+              nrhs = D + H;
+    const int Np = (Nm + NBL - 1) / NBL * NBL;
     const size_t NP2 = (size_t)Np * Np, MB = 2 * NP2;  // floats per matrix (two planes)
     if (nrhs > 32) MIXED_FAIL(HB_ERR_UNSUPPORTED, "more than 32 right-hand sides (6 per body and one per heading)", -1);
     if (!encode_fn()) MIXED_FAIL(HB_ERR_UNSUPPORTED, "the driver offers no tensor-map encoder (TMA)", -1);
@@ -164,25 +166,30 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     // GEMM operand buffers of the block row (rows 2n <= 2 (Np - NBL), 2 NBL wide), per frequency
     const size_t prep_rows = std::max<size_t>(2 * (size_t)(Np - NBL), GBN);
     const size_t prep = prep_rows * 2 * NBL;
-    size_t per = 3 * MB * 4 + 3 * prep * 4 + (size_t)(NBL * 2 * NBL + 4 * NBL * NBL) * 4 +
-                 (size_t)(nrhs + H) * N * 16 + 4 * (size_t)nrhs * Np * 16 + 64 +
+    // per system: the matrices, the LU operands, the diagonal-block inverses, the refinement vectors
+    size_t per_sys = 3 * MB * 4 + 3 * prep * 4 + (size_t)(NBL * 2 * NBL + 4 * NBL * NBL) * 4 +
+                     4 * (size_t)nrhs * Np * 16 + 64 + (size_t)(Np / NBL) * NBL * NBL * 8;
+    // per frequency: G systems, the boundary values and incident wave of every panel (with sectors also
+    // the projected right-hand sides and the recombined potentials), the finite-depth tiles
+    size_t per = G * per_sys + (size_t)(nrhs + H) * N * 16 + (G > 1 ? (size_t)2 * nrhs * N * 16 : 0) +
                  (fin ? (size_t)(T1_SIZE + T2_SIZE) * 8 + (size_t)(T1F_SIZE + T2F_SIZE) * 4 + (size_t)FP_PLANES * N * 8 + (size_t)6912 * 3 * 8 : 0);
-    per += (size_t)(Np / NBL) * NBL * NBL * 8;  // the diagonal-block inverses
     // The batch size from free memory; cudaMemGetInfo can take milliseconds, so the decision is kept per
     // thread and device for the same problem shape while the workspace still holds its buffers.
     Workspace& ws = workspace();
     int B = 0;
     {
         struct BatchChoice {
-            int N = -1, nrhs = -1, fin = -1, F = -1, B = 0;
+            int N = -1, G = -1, nrhs = -1, fin = -1, F = -1, B = 0;
             int64_t max_batch = -2;
         };
         static thread_local BatchChoice last[16];
         int dev_b = 0;
         cudaGetDevice(&dev_b);
         BatchChoice& c = last[dev_b < 0 || dev_b >= 16 ? 0 : dev_b];
-        const bool same = c.N == N && c.nrhs == nrhs && c.fin == (int)fin && c.F == F && c.max_batch == opt.max_batch;
-        if (same && c.B > 0 && ws.bytes[WS_S32] >= MB * (size_t)c.B * 4 && ws.bytes[WS_W] >= MB * (size_t)c.B * 4) {
+        const bool same = c.N == N && c.G == G && c.nrhs == nrhs && c.fin == (int)fin && c.F == F &&
+                          c.max_batch == opt.max_batch;
+        const size_t mats = MB * (size_t)std::max(c.B, 0) * G * 4;
+        if (same && c.B > 0 && ws.bytes[WS_S32] >= mats && ws.bytes[WS_W] >= mats) {
             B = c.B;
         } else {
             size_t freeb = 0, totalb = 0;
@@ -192,40 +199,44 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)freeb) / per);
             if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
             B = std::min(B, F);
-            c = BatchChoice{N, nrhs, (int)fin, F, B, opt.max_batch};
+            c = BatchChoice{N, G, nrhs, (int)fin, F, B, opt.max_batch};
         }
     }
     const size_t nblk = (size_t)Np / NBL;
+    const int BS = B * G;  // systems per batch
     bool okb = true;
     auto get = [&](int slot, size_t bytes) -> void* {
         void* q = ws.get(slot, bytes);
         okb = okb && q != nullptr;
         return q;
     };
-    float* S32 = (float*)get(WS_S32, MB * B * 4);
-    float* A32 = (float*)get(WS_A32, MB * B * 4);
-    float* W = (float*)get(WS_W, MB * B * 4);
-    float* P2 = (float*)get(WS_P2, prep * B * 4);
+    float* S32 = (float*)get(WS_S32, MB * BS * 4);
+    float* A32 = (float*)get(WS_A32, MB * BS * 4);
+    float* W = (float*)get(WS_W, MB * BS * 4);
+    float* P2 = (float*)get(WS_P2, prep * BS * 4);
     // a later update's B operand: rows of 4 NBL (two 128-row blocks of U) for the 256-deep trailing update
     const size_t p3size = 2 * prep;
-    float* P3 = (float*)get(WS_P3, p3size * B * 4);
+    float* P3 = (float*)get(WS_P3, p3size * BS * 4);
     // FP16 operands of the trailing update: P3's 4 NBL-wide layout, and the L rows of the outer step's
     // two block columns beyond its panel, [rows][Lr (2 NBL) | Li (2 NBL)]
-    __half* P3h = (__half*)get(WS_P3H, p3size * B * 2);
+    __half* P3h = (__half*)get(WS_P3H, p3size * BS * 2);
     const size_t l16_rows = std::max<size_t>(Np > 2 * NBL ? Np - 2 * NBL : 0, GBM);
-    __half* L16 = (__half*)get(WS_L16, l16_rows * 4 * NBL * B * 2);
-    float* PL = (float*)get(WS_PL, (size_t)NBL * 2 * NBL * B * 4);
-    float* PU = (float*)get(WS_PU, (size_t)4 * NBL * NBL * B * 4);
-    float2* DINV = (float2*)get(WS_DINV, nblk * NBL * NBL * B * sizeof(float2));
+    __half* L16 = (__half*)get(WS_L16, l16_rows * 4 * NBL * BS * 2);
+    float* PL = (float*)get(WS_PL, (size_t)NBL * 2 * NBL * BS * 4);
+    float* PU = (float*)get(WS_PU, (size_t)4 * NBL * NBL * BS * 4);
+    float2* DINV = (float2*)get(WS_DINV, nblk * NBL * NBL * BS * sizeof(float2));
     double2* u = (double2*)get(WS_U, (size_t)nrhs * N * B * 16);
     double2* phiI = (double2*)get(WS_PHII, (size_t)std::max(H, 1) * N * B * 16);
-    double2* b = (double2*)get(WS_B, (size_t)nrhs * Np * B * 16);
-    double2* x = (double2*)get(WS_XM, (size_t)nrhs * Np * B * 16);
-    float2* r = (float2*)get(WS_R, (size_t)nrhs * Np * B * 8);
-    float2* rs = (float2*)get(WS_RS, (size_t)nrhs * Np * B * 8);  // a residual kept for r - A d
-    double* norms = (double*)get(WS_NORMS, IR_MAX_IT * 2 * (size_t)B * 8);  // [iteration][batch][2]
+    // symmetry sectors: the right-hand sides projected on the sectors, the potentials of every panel
+    double2* up = G > 1 ? (double2*)get(WS_UP, (size_t)nrhs * Nm * BS * 16) : nullptr;
+    double2* phi = G > 1 ? (double2*)get(WS_PHI, (size_t)nrhs * N * B * 16) : nullptr;
+    double2* b = (double2*)get(WS_B, (size_t)nrhs * Np * BS * 16);
+    double2* x = (double2*)get(WS_XM, (size_t)nrhs * Np * BS * 16);
+    float2* r = (float2*)get(WS_R, (size_t)nrhs * Np * BS * 8);
+    float2* rs = (float2*)get(WS_RS, (size_t)nrhs * Np * BS * 8);  // a residual kept for r - A d
+    double* norms = (double*)get(WS_NORMS, IR_MAX_IT * 2 * (size_t)BS * 8);  // [iteration][batch][2]
     int* err = (int*)get(WS_ERR, sizeof(int));
-    int* tctrl = (int*)get(WS_TRI_CTRL, sizeof(int) * (1 + (size_t)B));  // the triangular sweeps' tickets
+    int* tctrl = (int*)get(WS_TRI_CTRL, sizeof(int) * (1 + (size_t)BS));  // the triangular sweeps' tickets
     FreqInfo* dfi = (FreqInfo*)get(WS_FI, sizeof(FreqInfo) * B);
     FdParams* dfd = (FdParams*)get(WS_FD, sizeof(FdParams) * B);
     double* dheads = (double*)get(WS_HEADS, sizeof(double) * std::max(H, 1));
@@ -245,19 +256,19 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     // ---- tensor maps (whole batch; the batch index is the 4th coordinate)
     CUtensorMap mapW, mapPL, mapPU, mapP2, mapP3, mapP3h, mapL16, mapP3w16;
     const uint64_t fb = 4;  // bytes per float
-    bool okm = make_map(&mapW, W, Np, Np, 2, B, Np * fb, NP2 * fb, MB * fb, GBM) &&
-               make_map(&mapPL, PL, 2 * NBL, NBL, 1, B, 2 * NBL * fb, (uint64_t)NBL * 2 * NBL * fb,
+    bool okm = make_map(&mapW, W, Np, Np, 2, BS, Np * fb, NP2 * fb, MB * fb, GBM) &&
+               make_map(&mapPL, PL, 2 * NBL, NBL, 1, BS, 2 * NBL * fb, (uint64_t)NBL * 2 * NBL * fb,
                         (uint64_t)NBL * 2 * NBL * fb, GBM) &&
-               make_map(&mapPU, PU, 2 * NBL, 2 * NBL, 1, B, 2 * NBL * fb, (uint64_t)4 * NBL * NBL * fb,
+               make_map(&mapPU, PU, 2 * NBL, 2 * NBL, 1, BS, 2 * NBL * fb, (uint64_t)4 * NBL * NBL * fb,
                         (uint64_t)4 * NBL * NBL * fb, GBN) &&
-               make_map(&mapP2, P2, 2 * NBL, prep_rows, 1, B, 2 * NBL * fb, prep * fb, prep * fb, GBN) &&
+               make_map(&mapP2, P2, 2 * NBL, prep_rows, 1, BS, 2 * NBL * fb, prep * fb, prep * fb, GBN) &&
                // P3 as rows of 2 NBL (one 128-row block of U), of 4 NBL (two blocks), and the 4 NBL rows
                // viewed as [2][2 NBL] halves (the first block alone: x = kk % NBL, half = kk / NBL)
-               make_map(&mapP3, P3, 2 * NBL, prep_rows, 1, B, 2 * NBL * fb, p3size * fb, p3size * fb, GBN) &&
-               make_map16(&mapP3w16, P3h, 4 * NBL, prep_rows, 1, B, 4 * NBL * 2, p3size * 2, p3size * 2, GBN) &&
-               make_map16(&mapL16, L16, 4 * NBL, l16_rows, 1, B, 4 * NBL * 2, l16_rows * 4 * NBL * 2,
+               make_map(&mapP3, P3, 2 * NBL, prep_rows, 1, BS, 2 * NBL * fb, p3size * fb, p3size * fb, GBN) &&
+               make_map16(&mapP3w16, P3h, 4 * NBL, prep_rows, 1, BS, 4 * NBL * 2, p3size * 2, p3size * 2, GBN) &&
+               make_map16(&mapL16, L16, 4 * NBL, l16_rows, 1, BS, 4 * NBL * 2, l16_rows * 4 * NBL * 2,
                           l16_rows * 4 * NBL * 2, GBM) &&
-               make_map_split(&mapP3h, P3, 2 * NBL, prep_rows, B, 4 * NBL * fb, p3size * fb, GBN);
+               make_map_split(&mapP3h, P3, 2 * NBL, prep_rows, BS, 4 * NBL * fb, p3size * fb, GBN);
     if (!okm) MIXED_FAIL(HB_ERR_INTERNAL, "tensor-map encoding failed", -1);
     const int smem = (int)gemm_smem_bytes();
     cudaFuncSetAttribute(k_gemm_tf32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -286,12 +297,12 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     const size_t out_per = 2 * (size_t)D * D + 3 * (size_t)H * 2 * D, DD = (size_t)D * D;
     // page-locked: the reads of norms, outputs and the error flag queue behind the work, no host wait
     double* hout = (double*)ws.host(HS_OUT, sizeof(double) * (out_per * B + 1));
-    double* hn = (double*)ws.host(HS_NORMS, sizeof(double) * IR_MAX_IT * 2 * (size_t)B);
+    double* hn = (double*)ws.host(HS_NORMS, sizeof(double) * IR_MAX_IT * 2 * (size_t)BS);
     if (!hout || !hn) MIXED_FAIL(HB_ERR_INTERNAL, "page-locked host memory could not be allocated", -1);
     int* herr = reinterpret_cast<int*>(hout + out_per * B);
     // out = bias - M x over the batch (M column-major planar FP32), FP64 accumulation
-    const int nz = (N + GEMV_CHUNK - 1) / GEMV_CHUNK;
-    double2* part = (double2*)ws.get(WS_PART, (size_t)nz * B * nrhs * N * 16);
+    const int nz = (Nm + GEMV_CHUNK - 1) / GEMV_CHUNK;
+    double2* part = (double2*)ws.get(WS_PART, (size_t)nz * BS * nrhs * Nm * 16);
     if (!part) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
     for (auto fn : {(const void*)k_cgemv_tma<8>, (const void*)k_cgemv_tma<10>, (const void*)k_cgemv_tma<12>,
                     (const void*)k_cgemv_tma<16>})
@@ -311,18 +322,18 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         if (!make_map_box(&mM, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)Mm, dm, sm, bm) ||
             !make_map_box(&mX, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void*)xv, dx, sx, bx))
             return false;
-        dim3 g((N + GV_ROWS - 1) / GV_ROWS, nb, nzt);
+        dim3 g((Nm + GV_ROWS - 1) / GV_ROWS, nb, nzt);
         if (nr == 8)
-            k_cgemv_tma<8><<<g, GV_THREADS, gv_smem_bytes<8>(), s>>>(mM, mX, N, nrhs, part, nb, err);
+            k_cgemv_tma<8><<<g, GV_THREADS, gv_smem_bytes<8>(), s>>>(mM, mX, Nm, nrhs, part, nb, err);
         else if (nr == 10)
-            k_cgemv_tma<10><<<g, GV_THREADS, gv_smem_bytes<10>(), s>>>(mM, mX, N, nrhs, part, nb, err);
+            k_cgemv_tma<10><<<g, GV_THREADS, gv_smem_bytes<10>(), s>>>(mM, mX, Nm, nrhs, part, nb, err);
         else if (nr == 12)
-            k_cgemv_tma<12><<<g, GV_THREADS, gv_smem_bytes<12>(), s>>>(mM, mX, N, nrhs, part, nb, err);
+            k_cgemv_tma<12><<<g, GV_THREADS, gv_smem_bytes<12>(), s>>>(mM, mX, Nm, nrhs, part, nb, err);
         else
-            k_cgemv_tma<16><<<g, GV_THREADS, gv_smem_bytes<16>(), s>>>(mM, mX, N, nrhs, part, nb, err);
+            k_cgemv_tma<16><<<g, GV_THREADS, gv_smem_bytes<16>(), s>>>(mM, mX, Nm, nrhs, part, nb, err);
         return true;
     };
-    const int nz_tma = (N + GV_CHUNK - 1) / GV_CHUNK;
+    const int nz_tma = (Nm + GV_CHUNK - 1) / GV_CHUNK;
     for (auto fn : {(const void*)k_cgemv32_tma<8>, (const void*)k_cgemv32_tma<10>, (const void*)k_cgemv32_tma<12>,
                     (const void*)k_cgemv32_tma<16>})
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gv32_smem_bytes<16>());
@@ -341,41 +352,41 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             !make_map_box(&mD, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)dv, dd, sd, bd))
             return false;
         P.begin(s);
-        dim3 g((N + GV_ROWS - 1) / GV_ROWS, nb, nz_tma);
+        dim3 g((Nm + GV_ROWS - 1) / GV_ROWS, nb, nz_tma);
         if (nr == 8)
-            k_cgemv32_tma<8><<<g, GV_THREADS, gv32_smem_bytes<8>(), s>>>(mM, mD, N, nrhs, part, nb, err);
+            k_cgemv32_tma<8><<<g, GV_THREADS, gv32_smem_bytes<8>(), s>>>(mM, mD, Nm, nrhs, part, nb, err);
         else if (nr == 10)
-            k_cgemv32_tma<10><<<g, GV_THREADS, gv32_smem_bytes<10>(), s>>>(mM, mD, N, nrhs, part, nb, err);
+            k_cgemv32_tma<10><<<g, GV_THREADS, gv32_smem_bytes<10>(), s>>>(mM, mD, Nm, nrhs, part, nb, err);
         else if (nr == 12)
-            k_cgemv32_tma<12><<<g, GV_THREADS, gv32_smem_bytes<12>(), s>>>(mM, mD, N, nrhs, part, nb, err);
+            k_cgemv32_tma<12><<<g, GV_THREADS, gv32_smem_bytes<12>(), s>>>(mM, mD, Nm, nrhs, part, nb, err);
         else
-            k_cgemv32_tma<16><<<g, GV_THREADS, gv32_smem_bytes<16>(), s>>>(mM, mD, N, nrhs, part, nb, err);
-        k_gemv_reduce<float2, float2><<<dim3((unsigned)(((size_t)nrhs * N + 255) / 256), nb), 256, 0, s>>>(
-            N, nrhs, nb, nz_tma, part, rk, Np, out, Np);
-        P.end(KF_MIXED_RESIDUAL, 8.0 * (double)N * N * nb, s);
+            k_cgemv32_tma<16><<<g, GV_THREADS, gv32_smem_bytes<16>(), s>>>(mM, mD, Nm, nrhs, part, nb, err);
+        k_gemv_reduce<float2, float2><<<dim3((unsigned)(((size_t)nrhs * Nm + 255) / 256), nb), 256, 0, s>>>(
+            Nm, nrhs, nb, nz_tma, part, rk, Np, out, Np);
+        P.end(KF_MIXED_RESIDUAL, 8.0 * (double)Nm * Nm * nb, s);
         *launches += 2;
         return true;
     };
     auto gemv = [&](const float* Mm, const double2* xv, int ldx, const double2* bias, auto* out, int nb, int fam,
                     cudaStream_t s) {
         P.begin(s);
-        dim3 g((N + 127) / 128, nb, nz);
+        dim3 g((Nm + 127) / 128, nb, nz);
         int nzr = nz;
         if (gemv_tma(Mm, xv, ldx, nb, nz_tma, s))
             nzr = nz_tma;
         else if (nrhs <= 8)
-            k_cgemv_part<8><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
+            k_cgemv_part<8><<<g, 128, 0, s>>>(Nm, Np, MB, nrhs, Mm, xv, ldx, part, nb);
         else if (nrhs <= 10)
-            k_cgemv_part<10><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
+            k_cgemv_part<10><<<g, 128, 0, s>>>(Nm, Np, MB, nrhs, Mm, xv, ldx, part, nb);
         else if (nrhs <= 12)
-            k_cgemv_part<12><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
+            k_cgemv_part<12><<<g, 128, 0, s>>>(Nm, Np, MB, nrhs, Mm, xv, ldx, part, nb);
         else if (nrhs <= 16)
-            k_cgemv_part<16><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
+            k_cgemv_part<16><<<g, 128, 0, s>>>(Nm, Np, MB, nrhs, Mm, xv, ldx, part, nb);
         else
-            k_cgemv_part<32><<<g, 128, 0, s>>>(N, Np, MB, nrhs, Mm, xv, ldx, part, nb);
-        k_gemv_reduce<<<dim3((unsigned)(((size_t)nrhs * N + 255) / 256), nb), 256, 0, s>>>(N, nrhs, nb, nzr, part,
-                                                                                          bias, Np, out, Np);
-        P.end(fam, 8.0 * (double)N * N * nb, s);
+            k_cgemv_part<32><<<g, 128, 0, s>>>(Nm, Np, MB, nrhs, Mm, xv, ldx, part, nb);
+        k_gemv_reduce<<<dim3((unsigned)(((size_t)nrhs * Nm + 255) / 256), nb), 256, 0, s>>>(Nm, nrhs, nb, nzr, part,
+                                                                                           bias, Np, out, Np);
+        P.end(fam, 8.0 * (double)Nm * Nm * nb, s);
         *launches += 2;
     };
     // d = A^-1 d in place (complex64) with the FP32 factors in W: U^T y = d, then L^T d = y, the
@@ -448,7 +459,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     }
     for (int f0 = 0; f0 < F; f0 += B) {
         if (opt.cancel && *opt.cancel) MIXED_FAIL(HB_ERR_CANCELLED, "the solve was cancelled", f0);
-        const int nb = std::min(B, F - f0);
+        const int nb = std::min(B, F - f0), ns = nb * G;  // frequencies, systems
         for (int i = 0; i < nb; i++) {
             double w = pr.omegas[f0 + i], K = w * w / opt.gravity;
             fi[i].omega = w;
@@ -476,14 +487,18 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 launch_assemble_f32_sg(pv, st, nb, dfi, dfd, tiles_f, fpt, fin, S32, A32, Np, sg_img, sg_count, s);
             else
                 launch_assemble_f32(pv, st, nb, dfi, dfd, tiles_f, fpt, fin, S32, A32, Np, s);
+            if (G > 1) {
+                launch_sectors_f32(S32, A32, nb, G, Nm, Np, s);
+                (*launches)++;
+            }
             // algorithmic bytes per pair: 4 FP64 statics read (32 B), S and A written as complex64 (16 B)
-            P.end(KF_ASSEMBLE, 48.0 * (double)N * N * nb, s);
-            if (Np > N) k_pad_identity<<<dim3(64, nb), 256, 0, s>>>(A32, N, Np, MB);
-            cudaMemcpyAsync(W, A32, MB * nb * 4, cudaMemcpyDeviceToDevice, s);
+            P.end(KF_ASSEMBLE, 48.0 * (double)Nm * N * nb, s);
+            if (Np > Nm) k_pad_identity<<<dim3(64, ns), 256, 0, s>>>(A32, Nm, Np, MB);
+            cudaMemcpyAsync(W, A32, MB * ns * 4, cudaMemcpyDeviceToDevice, s);
             P.begin(s);
             launch_boundary(pv, nb, dfi, H, dheads, depth, opt.gravity, u, phiI, s);
             P.end(KF_BOUNDARY, 0.0, s);
-            *launches += 1 + (Np > N);
+            *launches += 1 + (Np > Nm);
             t.stop();
         }
         // ---- LU of M = A^T without pivoting, blocked by NBL, the products on the tensor cores
@@ -617,11 +632,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                     trailing(h, c2, n);  // the trailing matrix, K' = 512
                 }
             };
-            const int nh = std::min(LU_GROUPS, nb);
+            const int nh = std::min(LU_GROUPS, ns);
             Half hs[LU_GROUPS];
             for (int i = 0, f0 = 0; i < nh; i++) {
-                const int ni = nb / nh + (i < nb % nh ? 1 : 0);
-                hs[i] = Half{side.s[i], f0, ni, std::max(n_sm - (nb - ni), 1)};
+                const int ni = ns / nh + (i < ns % nh ? 1 : 0);
+                hs[i] = Half{side.s[i], f0, ni, std::max(n_sm - (ns - ni), 1)};
                 f0 += ni;
             }
             cudaEventRecord(side.fork, s);
@@ -629,8 +644,12 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             // the right-hand sides b = -S u on their own stream, beside the LU (the refinement needs them)
             cudaStream_t srhs = side.s[LU_GROUPS];
             cudaStreamWaitEvent(srhs, side.fork, 0);
-            cudaMemsetAsync(b, 0, sizeof(double2) * nrhs * Np * nb, srhs);
-            gemv(S32, u, N, nullptr, b, nb, KF_RHS, srhs);
+            cudaMemsetAsync(b, 0, sizeof(double2) * nrhs * Np * ns, srhs);
+            if (G > 1) {  // projected on the sectors first
+                launch_project(u, up, nb, G, Nm, nrhs, Nm, srhs);
+                (*launches)++;
+            }
+            gemv(S32, G > 1 ? up : u, Nm, nullptr, b, ns, KF_RHS, srhs);
             cudaEventRecord(side.join[LU_GROUPS], srhs);
             int K0 = 0;
             for (; K0 + 2 * NBL <= Np; K0 += 2 * NBL)
@@ -649,24 +668,24 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         bool converged = false;
         {
             EventTimer t(s, &prof[3]);
-            cudaMemsetAsync(x, 0, sizeof(double2) * nrhs * Np * nb, s);
-            k_to_c64<<<592, 256, 0, s>>>((size_t)nrhs * Np * nb, b, r);
+            cudaMemsetAsync(x, 0, sizeof(double2) * nrhs * Np * ns, s);
+            k_to_c64<<<592, 256, 0, s>>>((size_t)nrhs * Np * ns, b, r);
             (*launches)++;
             IrHistory& hist = last_ir_history();
             hist.n = 0;
             // the largest relative correction over the batch at iteration i (norms of slot i)
             auto worst_at = [&](int i) {
                 double worst = 0.0;
-                for (int f = 0; f < nb; f++) {
-                    double ratio = hn[(size_t)i * 2 * nb + 2 * f] / std::max(hn[(size_t)i * 2 * nb + 2 * f + 1], 1e-300);
+                for (int f = 0; f < ns; f++) {
+                    double ratio = hn[(size_t)i * 2 * ns + 2 * f] / std::max(hn[(size_t)i * 2 * ns + 2 * f + 1], 1e-300);
                     if (!std::isfinite(ratio)) ratio = INFINITY;
                     worst = std::max(worst, ratio);
                 }
                 return worst;
             };
             auto correction = [&](int i) {  // d = A^-1 r (FP32), x += d, norms into slot i
-                trisolve(r, nb);
-                k_ir_update<<<nb, 256, 0, s>>>(Np, nrhs, x, r, norms + (size_t)i * 2 * nb);
+                trisolve(r, ns);
+                k_ir_update<<<ns, 256, 0, s>>>(Np, nrhs, x, r, norms + (size_t)i * 2 * ns);
                 *launches += 1;
             };
             // the forces and the readback of outputs, norms and the error flag (one wait for all)
@@ -677,8 +696,12 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 double2* dX = reinterpret_cast<double2*>(dout + 2 * DD * nb);
                 double2* dFK = dX + (size_t)H * D * nb;
                 double2* dSC = dFK + (size_t)H * D * nb;
+                if (G > 1) {  // the potentials of every panel from the sector solutions
+                    launch_recombine(x, phi, nb, G, Nm, nrhs, Np, s);
+                    (*launches)++;
+                }
                 P.begin(s);
-                launch_forces(pv, nb, dfi, H, x, Np, phiI, opt.density, dA, dB, dX, dFK, dSC, s);
+                launch_forces(pv, nb, dfi, H, G > 1 ? phi : x, G > 1 ? N : Np, phiI, opt.density, dA, dB, dX, dFK, dSC, s);
                 P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
                 (*launches)++;
                 cudaMemcpyAsync(hout, dout, sizeof(double) * out_per * nb, cudaMemcpyDeviceToHost, s);
@@ -694,11 +717,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             const int guess = std::min(std::max(ir_guess(), 2), IR_MAX_IT);
             for (int i = 0; i < guess; i++) {
                 const bool more = i + 1 < guess, inc = more && i >= 1 && nrhs <= 16 && rs;
-                if (inc) cudaMemcpyAsync(rs, r, sizeof(float2) * nrhs * Np * nb, cudaMemcpyDeviceToDevice, s);
+                if (inc) cudaMemcpyAsync(rs, r, sizeof(float2) * nrhs * Np * ns, cudaMemcpyDeviceToDevice, s);
                 correction(i);
-                if (more && !(inc && gemv32(A32, r, rs, r, nb))) gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL, s);
+                if (more && !(inc && gemv32(A32, r, rs, r, ns))) gemv(A32, x, Np, b, r, ns, KF_MIXED_RESIDUAL, s);
             }
-            cudaMemcpyAsync(hn, norms, sizeof(double) * 2 * nb * guess, cudaMemcpyDeviceToHost, s);
+            cudaMemcpyAsync(hn, norms, sizeof(double) * 2 * ns * guess, cudaMemcpyDeviceToHost, s);
             t.stop();
             forces();
             cudaStreamSynchronize(s);
@@ -722,9 +745,9 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 // further corrections, one host look each: no residual after the one that meets the test
                 EventTimer t2(s, &prof[3]);
                 for (it = guess; it < IR_MAX_IT; it++) {
-                    gemv(A32, x, Np, b, r, nb, KF_MIXED_RESIDUAL, s);
+                    gemv(A32, x, Np, b, r, ns, KF_MIXED_RESIDUAL, s);
                     correction(it);
-                    cudaMemcpyAsync(hn + (size_t)it * 2 * nb, norms + (size_t)it * 2 * nb, sizeof(double) * 2 * nb,
+                    cudaMemcpyAsync(hn + (size_t)it * 2 * ns, norms + (size_t)it * 2 * ns, sizeof(double) * 2 * ns,
                                     cudaMemcpyDeviceToHost, s);
                     cudaStreamSynchronize(s);
                     const double worst = worst_at(it);

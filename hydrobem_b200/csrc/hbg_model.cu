@@ -351,6 +351,7 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         } done{model};
         std::vector<double> verts, omegas, heads, centers;
         std::vector<int32_t> kinds, panel_body;
+        int32_t symmetry = HBG_SYM_NONE;
         HbgOptions opt;
         hbg_default_options(&opt);
         {
@@ -365,7 +366,18 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
                     if (m.name == b.interior_mesh) lid = &m;
                 }
                 if (!mesh || mesh->vertices.empty()) return refuse(HB_ERR_VALUE, "the body has no panels mesh");
-                std::vector<double> bv = expand(*mesh);
+                // A lone body whose mesh (and interior mesh) declare the same symmetry planes, placed on
+                // them, is solved by symmetry sectors (the stored panels, one system per sector); any
+                // other arrangement by its whole mirrored mesh.
+                const int msym = mesh->symmetry == "yz" ? HBG_SYM_YZ : mesh->symmetry == "xz" ? HBG_SYM_XZ
+                                 : mesh->symmetry == "xz_and_yz"                         ? HBG_SYM_BOTH
+                                                                                         : HBG_SYM_NONE;
+                const bool on_planes = (!(msym & HBG_SYM_YZ) || b.position[0] == 0.0) &&
+                                       (!(msym & HBG_SYM_XZ) || b.position[1] == 0.0);
+                const bool sectors = model->bodies.size() == 1 && msym != HBG_SYM_NONE && on_planes &&
+                                     (b.interior != "mesh" || (lid && lid->symmetry == mesh->symmetry));
+                std::vector<double> bv = sectors ? mesh->vertices : expand(*mesh);
+                if (sectors) symmetry = msym;
                 size_t P = bv.size() / 12;
                 std::vector<int32_t> bk(P, HBG_WET);
                 if (b.interior == "detect")
@@ -376,7 +388,7 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
                     }
                 if (b.interior == "mesh") {
                     if (!lid) return refuse(HB_ERR_VALUE, "interior_surface_mesh names no mesh");
-                    std::vector<double> lv = expand(*lid);
+                    std::vector<double> lv = sectors ? lid->vertices : expand(*lid);
                     bv.insert(bv.end(), lv.begin(), lv.end());
                     bk.resize(bv.size() / 12, HBG_INTERIOR);
                 }
@@ -413,6 +425,7 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         pr.body.panel_body = panel_body.data();
         pr.body.n_bodies = (int32_t)NB;
         pr.body.rotation_centers = centers.data();
+        pr.body.symmetry = symmetry;
         pr.omegas = omegas.data();
         pr.n_omega = (int64_t)F;
         pr.headings_deg = heads.data();

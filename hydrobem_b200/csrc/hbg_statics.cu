@@ -399,16 +399,17 @@ __device__ inline double log_in_plane(const PanelRegs& p, const double* x) {
 }
 
 // One (row k, panel j) pair: rs, rd and (unless adaptive) dl, dd.  lo_static.rs:59-119
+// Four planes of Nr x N (rows k < Nr = N / G, the sector's points; every panel j), entry at k + j Nr.
 // MIXED: the mixed form's variant (far Rankine points and the order-4 log rule in FP32, above); the
 // FP64 form runs the reference's arithmetic to the bit.
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_statics(PanelsView pv, double depth, int logint, double tol,
                                                  double* __restrict__ st, int32_t* __restrict__ work,
                                                  int32_t* __restrict__ nwork, int work_cap) {
-    int N = pv.N;
+    const int N = pv.N, Nr = N / pv.G;  // rows: the sector's panels; columns: all panels
     int k = blockIdx.x * 32 + threadIdx.x;
     int j = blockIdx.y * 8 + threadIdx.y;
-    if (k >= N || j >= N) return;
+    if (k >= Nr || j >= N) return;
     PanelRegs p;
     load_panel(pv, j, p);
     double x[3] = {pv.at(P_C + 0, k), pv.at(P_C + 1, k), pv.at(P_C + 2, k)};
@@ -429,7 +430,7 @@ __global__ void __launch_bounds__(256) k_statics(PanelsView pv, double depth, in
         sr += (s2 + s4) + s5 + s6;
         dr += (d2 + d4) + d5 + d6;
     }
-    size_t NN = (size_t)N * N, o = (size_t)k + (size_t)j * N;
+    size_t NN = (size_t)Nr * N, o = (size_t)k + (size_t)j * Nr;
     st[o] = sr;
     st[NN + o] = dr;
     double dl = 0.0, dd = 0.0;
@@ -570,7 +571,8 @@ __device__ void adaptive_pair(const PanelsView& pv, const int32_t* __restrict__ 
     if (lane == 0) {
         double psi, dpsi;
         psi_terms(p.c, xb, p.n, psi, dpsi);
-        size_t NN = (size_t)N * N, o = (size_t)k + (size_t)j * N;
+        const int Nr = N / pv.G;
+        size_t NN = (size_t)Nr * N, o = (size_t)k + (size_t)j * Nr;
         st[2 * NN + o] = acc0 - p.area * psi;
         st[3 * NN + o] = acc1 - p.area * dpsi;
     }
@@ -615,7 +617,7 @@ void launch_panel_geometry(int N, const double* verts, const int32_t* kind, doub
 
 void launch_statics(const PanelsView& pv, double depth, int logint, double tol, double* st, int32_t* work,
                     int32_t* nwork, int work_cap, cudaStream_t s, bool mixed) {
-    dim3 grid((pv.N + 31) / 32, (pv.N + 7) / 8);
+    dim3 grid((pv.N / pv.G + 31) / 32, (pv.N + 7) / 8);
     if (mixed)
         k_statics<true><<<grid, dim3(32, 8), 0, s>>>(pv, depth, logint, tol, st, work, nwork, work_cap);
     else

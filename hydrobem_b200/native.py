@@ -29,7 +29,11 @@ ip = ctypes.POINTER(ctypes.c_int32)
 
 class HbgBody(ctypes.Structure):
     _fields_ = [("n_panels", ctypes.c_int64), ("vertices", dp), ("kinds", ip), ("panel_body", ip),
-                ("n_bodies", ctypes.c_int32), ("rotation_centers", dp)]
+                ("n_bodies", ctypes.c_int32), ("rotation_centers", dp), ("symmetry", ctypes.c_int32)]
+
+
+# HbgBody.symmetry: one sector's panels given, their mirror images added by the library
+SYM_NONE, SYM_YZ, SYM_XZ, SYM_BOTH = 0, 1, 2, 3
 
 
 class HbgOutputs(ctypes.Structure):
@@ -146,9 +150,12 @@ def default_options(**kw) -> HbgOptions:
 class Body:
     """The inputs and output arrays of one problem of a batch (kept alive across the call): the panels of
     one rigid body, or of interacting bodies with panel_body (the body of each panel) and
-    rotation_centers [n_bodies][3] (None: the origin); 6 rigid modes per body, D = 6 n_bodies."""
+    rotation_centers [n_bodies][3] (None: the origin); 6 rigid modes per body, D = 6 n_bodies.  With
+    symmetry (SYM_YZ, SYM_XZ, SYM_BOTH) the panels are one sector of a body mirrored in those planes."""
 
-    def __init__(self, vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None):
+    def __init__(self, vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None,
+                 symmetry=SYM_NONE):
+        self.symmetry = int(symmetry)
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 4, 3)
         self.kinds = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
         self.panel_body = None if panel_body is None else np.ascontiguousarray(panel_body, dtype=np.int32)
@@ -174,6 +181,7 @@ class Body:
         p.body.panel_body = None if self.panel_body is None else self.panel_body.ctypes.data_as(ip)
         p.body.n_bodies = self.n_bodies
         p.body.rotation_centers = None if self.centers is None else self.centers.ctypes.data_as(dp)
+        p.body.symmetry = self.symmetry
         p.omegas = self.omegas.ctypes.data_as(dp)
         p.n_omega = self.omegas.size
         p.headings_deg = self.headings.ctypes.data_as(dp)
@@ -197,9 +205,11 @@ def solve_batch(bodies, **options):
     return [b.results() for b in bodies]
 
 
-def solve(vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None, **options):
+def solve(vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None,
+          symmetry=SYM_NONE, **options):
     """One problem through the GPU path: dict of A, B [F][D][D], X, FK, SC [F][H][D], D = 6 per body."""
-    return solve_batch([Body(vertices, omegas, headings_deg, kinds, panel_body, rotation_centers)], **options)[0]
+    return solve_batch([Body(vertices, omegas, headings_deg, kinds, panel_body, rotation_centers, symmetry)],
+                       **options)[0]
 
 
 def last_profile():
@@ -214,20 +224,25 @@ def last_launch_count() -> int:
     return c.value
 
 
-def debug_matrices(vertices, omega, kinds=None, **options):
+def debug_matrices(vertices, omega, kinds=None, symmetry=SYM_NONE, **options):
     """(statics [N][N][4] with entry [k][j], S, A complex128 [N][N] with entry [k][n]) of one
-    body at one frequency, FP64 form (test support)."""
+    body at one frequency, FP64 form (test support).  With symmetry (G sectors of the n given panels):
+    statics [n][G n][4] (the sector rows against every panel) and S, A [G][n][n] (the sector matrices)."""
     v = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 4, 3)
     k = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
-    N = v.shape[0]
-    body = HbgBody(N, v.ctypes.data_as(dp), None if k is None else k.ctypes.data_as(ip))
-    st = np.zeros((4, N, N))       # plane, j, k  (entry (k, j) at k + j N)
-    S = np.zeros((N, N), dtype=np.complex128)   # [n][k] (column-major)
-    A = np.zeros((N, N), dtype=np.complex128)
+    n = v.shape[0]
+    G = {SYM_NONE: 1, SYM_YZ: 2, SYM_XZ: 2, SYM_BOTH: 4}.get(int(symmetry), 1)
+    body = HbgBody(n, v.ctypes.data_as(dp), None if k is None else k.ctypes.data_as(ip))
+    body.symmetry = int(symmetry)
+    st = np.zeros((4, G * n, n))   # plane, j, k  (entry (k, j) at k + j n)
+    S = np.zeros((G, n, n), dtype=np.complex128)   # [c][n][k] (column-major)
+    A = np.zeros((G, n, n), dtype=np.complex128)
     opt = default_options(**options)
     check(lib().hbg_debug_matrices(ctypes.byref(body), omega, ctypes.byref(opt), st.ctypes.data_as(dp),
                                    S.ctypes.data_as(dp), A.ctypes.data_as(dp)))
-    return st.transpose(2, 1, 0), S.T, A.T
+    if G == 1:
+        return st.transpose(2, 1, 0), S[0].T, A[0].T
+    return st.transpose(2, 1, 0), S.transpose(0, 2, 1), A.transpose(0, 2, 1)
 
 
 KERNEL_FAMILIES = ["geometry", "statics", "statics_adaptive", "fd_tiles", "assemble", "boundary", "rhs", "lu_panel",

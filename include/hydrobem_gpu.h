@@ -50,7 +50,7 @@ typedef int32_t HbStatus;
 #define HB_C128 7
 
 /* The version of this library's ABI (its own numbering; the reference's hb_abi_version is 8). */
-#define HBG_ABI_VERSION 3
+#define HBG_ABI_VERSION 4
 
 /* ==================================================================== batched entry */
 
@@ -69,7 +69,17 @@ typedef int32_t HbStatus;
  * with panel_body [n_panels] the body of each panel (0 .. n_bodies - 1) and rotation_centers
  * [n_bodies][3] the point each body's rotations are about (NULL: the origin); n_bodies 0 or 1 and
  * panel_body NULL: one rigid body.  The rigid modes are 6 per body (surge, sway, heave, roll, pitch,
- * yaw), D = 6 n_bodies in all. */
+ * yaw), D = 6 n_bodies in all.
+ * Symmetry planes (the reference's mesh symmetry, crates/hydrobem/src/lo_geometry.rs:25-36): with
+ * symmetry != HBG_SYM_NONE the n_panels panels are one sector of the body (x >= 0 for the yz plane,
+ * y >= 0 for the xz plane), kinds and panel_body are given for them, and the library adds their mirror
+ * images (orientation restored); the solve then runs one system of n_panels unknowns per sector (2 or
+ * 4 per frequency) instead of one of 2 or 4 n_panels: 4 or 16 times less LU work.  Each body keeps
+ * its rotation centre; the results are those of the whole mirrored body. */
+#define HBG_SYM_NONE 0
+#define HBG_SYM_YZ 1   /* mirror x -> -x */
+#define HBG_SYM_XZ 2   /* mirror y -> -y */
+#define HBG_SYM_BOTH 3 /* both planes: 4 sectors */
 typedef struct HbgBody {
     int64_t n_panels;
     const double *vertices;
@@ -77,6 +87,7 @@ typedef struct HbgBody {
     const int32_t *panel_body;
     int32_t n_bodies;
     const double *rotation_centers;
+    int32_t symmetry;
 } HbgBody;
 
 /* Outputs of one problem, caller-allocated host arrays (NULL: not wanted), float64, D = 6 n_bodies:
@@ -147,6 +158,9 @@ HbStatus hbg_last_launch_count(int64_t *count);
 /* Test support: the static influence data (planes rs, rd, dl, dd; entry (k, j) at k + j N of each
  * plane, N*N doubles per plane) and the matrices S and A = 2 pi I - D (column-major complex128,
  * N*N (re, im) pairs) of one body at one frequency, FP64 form.  Any output pointer may be NULL.
+ * With body->symmetry (G = 2 or 4 sectors of n = n_panels): the statics of the sector rows against
+ * all G n panels (entry (k, j) at k + j n, n G n doubles per plane), and the G sector matrices S_c,
+ * A_c one after the other (n*n pairs each).
  * Replaces no reference interface (it exposes compute_static, lo_static.rs:254-308, and
  * Frequency::matrices, lo_frequency.rs:276-312, for the parity tests). */
 HbStatus hbg_debug_matrices(const HbgBody *body, double omega, const HbgOptions *opt, double *statics, double *S,

@@ -9,6 +9,9 @@ and adds, in numpy, the steps that are short formulas of ``crates/hydrobem/src/`
 - right-hand sides -S u and the dense solve  ``lo_frequency.rs:823-955`` (LU with partial pivoting:
   LAPACK ``zgesv`` through numpy, standing in for faer's blocked LU, ``linalg.rs:134-252``)
 - pressure integration A, B, X, FK, SC  ``lo_frequency.rs:1039-1115``
+- symmetry sectors (a body given as one sector of its mirror-symmetric mesh): the matrices of the
+  mirrored mesh's sector rows summed over the reflections with the group's characters, one system
+  per sector, the potentials recombined  ``lo_geometry.rs:25-36``, ``lo_frequency.rs:276-346,823-943``
 
 Parity: pinned against the reference's golden kernel files (``tests/data/green_inf_reference.txt``,
 ``green_fin_reference.txt``, ``panel_reference.txt``, ``dispersion_reference.txt``) and against the
@@ -213,9 +216,53 @@ def rigid_normals(c, n, kinds, panel_body=None, centers=None):
     return nj
 
 
+# ------------------------------------------------------------------ symmetry sectors
+SYM_NONE, SYM_YZ, SYM_XZ, SYM_BOTH = 0, 1, 2, 3
+
+
+def sector_count(symmetry: int) -> int:
+    return {SYM_NONE: 1, SYM_YZ: 2, SYM_XZ: 2, SYM_BOTH: 4}[int(symmetry)]
+
+
+def character(c: int, g: int) -> float:
+    """chi_c(g) of the reflection group, elements e, x, y, xy reflections (lo_geometry.rs:25-36)."""
+    return -1.0 if bin(c & g).count("1") % 2 else 1.0
+
+
+def mirror_sector(verts, symmetry):
+    """The panels of a sector followed by their images in the group's element order (image g of panel n
+    at g Ns + n); a reflection that reverses orientation takes the vertices as v0 v3 v2 v1."""
+    v = np.asarray(verts, dtype=np.float64).reshape(-1, 4, 3)
+    refl = {SYM_NONE: [], SYM_YZ: [(-1.0, 1.0)], SYM_XZ: [(1.0, -1.0)],
+            SYM_BOTH: [(-1.0, 1.0), (1.0, -1.0), (-1.0, -1.0)]}[int(symmetry)]
+    out = [v]
+    for sx, sy in refl:
+        w = v * np.array([sx, sy, 1.0])
+        out.append(w[:, [0, 3, 2, 1]] if sx * sy < 0 else w)
+    return np.concatenate(out)
+
+
+def sector_solve(S, A, u, G):
+    """phi on every panel of the mirrored mesh from the G sector systems (lo_frequency.rs:823-943): for
+    character c, S_c and A_c the sums over g of chi_c(g) times the column block g of the sector rows,
+    right-hand sides -S_c U_c with U_c = (1/G) sum_g chi_c(g) u(g n), and phi(g n) = sum_c chi_c(g) x_c(n)."""
+    Ns = S.shape[0] // G
+    blk = lambda M, g: M[:Ns, g * Ns:(g + 1) * Ns]
+    phi = np.zeros((S.shape[0], u.shape[1]), dtype=np.complex128)
+    for c in range(G):
+        Sc = sum(character(c, g) * blk(S, g) for g in range(G))
+        Ac = sum(character(c, g) * blk(A, g) for g in range(G))
+        Uc = sum(character(c, g) * u[g * Ns:(g + 1) * Ns] for g in range(G)) / G
+        xc = np.linalg.solve(Ac, Sc @ (-Uc))
+        for g in range(G):
+            phi[g * Ns:(g + 1) * Ns] += character(c, g) * xc
+    return phi
+
+
 def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY, rho=DENSITY, logint=True,
-                    want_matrices=False, panel_body=None, centers=None):
-    """A, B [D][D], X, FK, SC [H][D] of one frequency (D = 6 per body), all in float64 (complex128)."""
+                    want_matrices=False, panel_body=None, centers=None, sectors=1):
+    """A, B [D][D], X, FK, SC [H][D] of one frequency (D = 6 per body), all in float64 (complex128).
+    sectors > 1: the panels are a mirrored mesh (mirror_sector) solved by its symmetry sectors."""
     c, n, area = panel_arrays(panels)
     N = len(panels)
     S, A = assemble(panels, kinds, st, depth, omega, grav, logint)
@@ -233,7 +280,7 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
         d = (gr * n).sum(axis=1)
         u[:, D + h] = np.where(wet, -d, 0.0)
     rhs = S @ (-u)
-    phi = np.linalg.solve(A, rhs)
+    phi = np.linalg.solve(A, rhs) if sectors == 1 else sector_solve(S, A, u, sectors)
     w = (nj * area[:, None]) * wet[:, None]          # n_i A_j on the body panels
     z = -rho * (w.T @ phi[:, :D])                    # [i][c]
     out = {"A": z.real, "B": -omega * z.imag}
@@ -250,13 +297,19 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
 
 
 def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GRAVITY, rho=DENSITY, logint=True,
-               tol=1e-4, panel_body=None, centers=None):
+               tol=1e-4, panel_body=None, centers=None, symmetry=SYM_NONE):
     """The whole path for one problem: statics once, then every frequency. Arrays [F][D][D], [F][H][D]
-    (D = 6 per body; interacting bodies by panel_body and their rotation centers)."""
+    (D = 6 per body; interacting bodies by panel_body and their rotation centers).  With symmetry the
+    panels (and kinds, panel_body) are one sector: mirrored, then solved by sectors."""
+    G = sector_count(symmetry)
+    if G > 1:
+        verts = mirror_sector(verts, symmetry)
+        kinds = None if kinds is None else np.tile(np.asarray(kinds), G)
+        panel_body = None if panel_body is None else np.tile(np.asarray(panel_body), G)
     panels = make_panels(verts, kinds)
     st = statics(panels, kinds, depth, logint, tol)
     heads = np.radians(np.asarray(headings_deg, dtype=float))
     res = [solve_frequency(panels, kinds, st, depth, w, heads, grav, rho, logint, panel_body=panel_body,
-                           centers=centers) for w in omegas]
+                           centers=centers, sectors=G) for w in omegas]
     out = {k: np.array([r[k] for r in res]) for k in res[0]}
     return out

@@ -111,3 +111,20 @@ def test_mixed_many_headings():
     ref = O.solve_body(v, omegas, heads, depth=3.0)
     errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
     assert max(errs.values()) <= MIXED_TOL, errs
+
+
+def test_mixed_large_barge_with_lid():
+    """An 80 m x 20 m barge of 10 m draught: 16448 wetted panels and a 2048-panel interior lid (18496
+    unknowns), 8 headings.  Too large for the oracle; the FP64 form, pinned on the oracle at smaller
+    sizes, is the reference here, and the refinement must still converge in a few corrections."""
+    v = meshes.box(40.0, 10.0, 10.0, n=(64, 32, 75), lid=True)
+    kinds = np.zeros(len(v), np.int32)
+    kinds[-64 * 32:] = 1
+    omegas = np.array([0.3, 0.8])
+    heads = list(np.arange(8) * 22.5)
+    mixed = nv.solve(v, omegas, heads, kinds=kinds, precision=nv.HBG_MIXED)
+    hist = nv.last_ir_history()
+    fp64 = nv.solve(v, omegas, heads, kinds=kinds)
+    errs = {k: scaled_error(mixed[k], fp64[k]) for k in ("A", "B", "X")}
+    assert max(errs.values()) <= MIXED_TOL, (errs, hist)
+    assert hist[-1] <= 1e-7 and len(hist) <= 12, hist
