@@ -1,6 +1,7 @@
 // hbg_all.cu -- the main translation unit of libhydrobem_gpu.so (hbg_statics.cu is the other one,
 // compiled without floating-point contraction).
 #include "hbg_freq.cu"
+#include "hbg_motion.cu"
 #include "hbg_lu.cu"
 #include "hbg_mixed.cu"
 #include "hbg_peaks.cu"

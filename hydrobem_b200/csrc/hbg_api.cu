@@ -471,6 +471,34 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
                 throw Failure{HB_ERR_VALUE, "a rotation centre is not finite", body_index};
     const int D = 6 * nbod;
     if (D + H > 32) throw Failure{HB_ERR_UNSUPPORTED, "more than 32 right-hand sides (6 per body and one per heading)", body_index};
+    // motions (motion.rs) need the rigid-body data; the hydrostatics records need only the panels
+    const HbgRigid* rigid = pr.rigid;
+    const bool motions = pr.out.motions != nullptr && H > 0;
+    if (pr.out.motions && !rigid)
+        throw Failure{HB_ERR_VALUE, "motions need the rigid-body data (mass, centre of gravity, inertia)", body_index};
+    if (rigid) {
+        if (!rigid->mass || !rigid->center_of_gravity || !rigid->inertia || !rigid->inertia_origin)
+            throw Failure{HB_ERR_ARGUMENT, "rigid data without mass, centre of gravity, inertia or its origin", body_index};
+        for (int b = 0; b < nbod; b++) {
+            const double m = rigid->mass[b];
+            if (!(std::isnan(m) || (m >= 0.0 && std::isfinite(m))))
+                throw Failure{HB_ERR_VALUE, "a mass is negative or infinite", body_index};
+            const int k = rigid->inertia_kind ? rigid->inertia_kind[b] : HBG_INERTIA_COMPONENTS;
+            if (k != HBG_INERTIA_COMPONENTS && k != HBG_INERTIA_GYRATION)
+                throw Failure{HB_ERR_VALUE, "inertia_kind is neither components nor radii of gyration", body_index};
+            for (int i = 0; i < 3; i++)
+                if (!std::isfinite(rigid->center_of_gravity[3 * b + i]) || !std::isfinite(rigid->inertia_origin[3 * b + i]))
+                    throw Failure{HB_ERR_VALUE, "a centre of gravity or inertia origin is not finite", body_index};
+            for (int i = 0; i < 9; i++)
+                if (!std::isfinite(rigid->inertia[9 * b + i]))
+                    throw Failure{HB_ERR_VALUE, "an inertia entry is not finite", body_index};
+        }
+        for (int i = 0; i < D * D; i++)
+            if ((rigid->stiffness && !std::isfinite(rigid->stiffness[i])) ||
+                (rigid->damping && !std::isfinite(rigid->damping[i])))
+                throw Failure{HB_ERR_VALUE, "an additional stiffness or damping entry is not finite", body_index};
+    }
+    const bool hydro = rigid || pr.out.hydrostatics;
     if (H > 26) throw Failure{HB_ERR_UNSUPPORTED, "more than 26 headings per solve", body_index};
     const bool fin = finite_depth(opt.depth);
     const double depth = fin ? opt.depth : 0.0;
@@ -485,10 +513,32 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     // the statics and the assembly in the device's queue)
     Workspace& ws = workspace();
     WsBuf dverts(ws, WS_VERTS), dkind(ws, WS_KIND), dplanes(ws, WS_PLANES), dbad(ws, WS_BAD), dst(ws, WS_ST),
-        dwork(ws, WS_WORK), dnwork(ws, WS_NWORK), dpbody(ws, WS_PBODY), drcen(ws, WS_RCEN);
+        dwork(ws, WS_WORK), dnwork(ws, WS_NWORK), dpbody(ws, WS_PBODY), drcen(ws, WS_RCEN), drig(ws, WS_RIGID),
+        dhyd(ws, WS_HYD);
     const bool multi = nbod > 1 && pr.body.panel_body;
     if (multi) dpbody.alloc(sizeof(int32_t) * N);
     if (pr.body.rotation_centers) drcen.alloc(sizeof(double) * 3 * nbod);
+    // the rigid data [n_bodies][RIGID_PER_BODY] then the additional stiffness and damping (D x D each); the
+    // hydrostatics records [n_bodies][HBG_HS] then the motion matrices M, C, B_ext (D x D each)
+    const size_t DD2 = (size_t)D * D;
+    std::vector<double> rigid_host;
+    if (rigid) {
+        rigid_host.assign((size_t)nbod * RIGID_PER_BODY + 2 * DD2, 0.0);
+        for (int b = 0; b < nbod; b++) {
+            double* r = &rigid_host[(size_t)b * RIGID_PER_BODY];
+            r[0] = rigid->mass[b];
+            for (int i = 0; i < 3; i++) r[1 + i] = rigid->center_of_gravity[3 * b + i];
+            r[4] = rigid->inertia_kind ? rigid->inertia_kind[b] : HBG_INERTIA_COMPONENTS;
+            for (int i = 0; i < 9; i++) r[5 + i] = rigid->inertia[9 * b + i];
+            for (int i = 0; i < 3; i++) r[14 + i] = rigid->inertia_origin[3 * b + i];
+        }
+        double* ext = &rigid_host[(size_t)nbod * RIGID_PER_BODY];
+        if (rigid->stiffness) memcpy(ext, rigid->stiffness, sizeof(double) * DD2);
+        if (rigid->damping) memcpy(ext + DD2, rigid->damping, sizeof(double) * DD2);
+        drig.alloc(sizeof(double) * rigid_host.size());
+    }
+    if (hydro) dhyd.alloc(sizeof(double) * ((size_t)nbod * HBG_HS + 3 * DD2));
+    const double* mot_mats = hydro ? dhyd.as<double>() + (size_t)nbod * HBG_HS : nullptr;
     std::vector<int32_t> kinds(N, 0);
     if (pr.body.kinds)
         for (int j = 0; j < N; j++) {
@@ -529,6 +579,21 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         g_launches++;
         PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
         pv.G = G;
+        if (hydro) {  // the hydrostatics and motion matrices of every body, once per problem
+            if (rigid)
+                CUDA_OK(cudaMemcpyAsync(drig.p, rigid_host.data(), sizeof(double) * rigid_host.size(),
+                                        cudaMemcpyHostToDevice, s));
+            PanelsView pb{N, dplanes.as<double>(), dkind.as<int32_t>(), nullptr, multi ? dpbody.as<int32_t>() : nullptr,
+                          pr.body.rotation_centers ? drcen.as<double>() : nullptr, nbod, G};
+            const double* rg = rigid ? drig.as<double>() : nullptr;
+            const double* ext = rigid ? rg + (size_t)nbod * RIGID_PER_BODY : nullptr;
+            double* hs = dhyd.as<double>();
+            double* mm = hs + (size_t)nbod * HBG_HS;
+            launch_hydrostatics(pb, rg, rigid && rigid->stiffness ? ext : nullptr,
+                                rigid && rigid->damping ? ext + DD2 : nullptr, opt.density, opt.gravity, hs, mm,
+                                mm + DD2, mm + 2 * DD2, s);
+            g_launches++;
+        }
         CUDA_OK(cudaMemsetAsync(dnwork.p, 0, 2 * sizeof(int32_t), s));
         P.begin(s);
         launch_statics(pv, depth, opt.logarithmic, opt.log_tolerance, dst.as<double>(), dwork.as<int32_t>(),
@@ -565,6 +630,8 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         CUDA_OK(cudaStreamSynchronize(s));
         profiler().flush();
         statics_check();
+        if (pr.out.hydrostatics)
+            CUDA_OK(cudaMemcpy(pr.out.hydrostatics, dhyd.p, sizeof(double) * nbod * HBG_HS, cudaMemcpyDeviceToHost));
         if (F == 0) return;
     }
     const int nrhs = D + H;
@@ -572,11 +639,13 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         const char* msg = "";
         int64_t fq = -1;
         int rc = mixed_solve_frequencies(pv, dst.as<double>(), pr, opt, fin, depth, s, prof, &g_launches, &msg, &fq,
-                                         run_statics);
+                                         run_statics, motions ? mot_mats : nullptr);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e == cudaSuccess) statics_check();
         if (rc != 0) throw Failure{rc, msg, body_index, fq};
         CUDA_OK(e);
+        if (pr.out.hydrostatics)
+            CUDA_OK(cudaMemcpy(pr.out.hydrostatics, dhyd.p, sizeof(double) * nbod * HBG_HS, cudaMemcpyDeviceToHost));
         return;
     }
     // ---- frequency batches
@@ -641,13 +710,16 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
     dheads.alloc(sizeof(double) * heads.size());
     CUDA_OK(cudaMemcpyAsync(dheads.p, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s));
-    // outputs per batch: A, B [6][6], X, FK, SC [H][6]
-    const size_t out_per = 2 * (size_t)D * D * sizeof(double) + 3 * (size_t)H * D * sizeof(double2);
+    // outputs per batch: A, B [D][D], X, FK, SC, motions [H][D]
+    const size_t out_per = 2 * (size_t)D * D * sizeof(double) + 4 * (size_t)H * D * sizeof(double2);
+    WsBuf derr(ws, WS_ERR);
+    derr.alloc(sizeof(int32_t));
     dout.alloc(out_per * B);
     // page-locked outputs and pivot flags: their reads queue behind the work
-    unsigned char* hout = static_cast<unsigned char*>(ws.host(HS_OUT, out_per * B + sizeof(int32_t) * BS));
+    unsigned char* hout = static_cast<unsigned char*>(ws.host(HS_OUT, out_per * B + sizeof(int32_t) * (BS + 1)));
     if (!hout) throw Failure{HB_ERR_INTERNAL, "page-locked host memory could not be allocated", body_index};
     int32_t* info = reinterpret_cast<int32_t*>(hout + out_per * B);
+    int32_t* herr = info + BS;
     std::vector<FreqInfo> fi(B);
     std::vector<FdParams> fdh(B);
     for (int f0 = 0; f0 < F; f0 += B) {
@@ -735,8 +807,15 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
                           dSC, s);
             P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
             g_launches += 1;
+            CUDA_OK(cudaMemsetAsync(derr.p, 0, sizeof(int32_t), s));
+            if (motions) {
+                launch_motions(nb, D, H, dfi.as<FreqInfo>(), dAo, dBo, dXo, mot_mats, mot_mats + DD2, mot_mats + 2 * DD2,
+                               dSC + (size_t)H * D * nb, derr.as<int32_t>(), s);
+                g_launches++;
+            }
             CUDA_OK(cudaMemcpyAsync(hout, dout.p, out_per * nb, cudaMemcpyDeviceToHost, s));
             CUDA_OK(cudaMemcpyAsync(info, dinfo.p, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, s));
+            CUDA_OK(cudaMemcpyAsync(herr, derr.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
             t.stop();
             solve_end().record(s);
         }
@@ -750,6 +829,8 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         const double* hX = hb + 2 * DD * nb;
         const double* hFK = hX + (size_t)H * 2 * D * nb;
         const double* hSC = hFK + (size_t)H * 2 * D * nb;
+        const double* hMo = hSC + (size_t)H * 2 * D * nb;
+        if (*herr != 0) throw Failure{HB_ERR_NUMERICAL, "singular motion equation", body_index, f0};
         for (int i = 0; i < nb; i++) {
             for (int c = 0; c < G; c++)
                 if (info[i * G + c] != 0)
@@ -766,6 +847,7 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
             if (pr.out.excitation) memcpy(pr.out.excitation + fo * hx, hX + hx * i, hx * sizeof(double));
             if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
+            if (motions) memcpy(pr.out.motions + fo * hx, hMo + hx * i, hx * sizeof(double));
         }
     }
 }

@@ -69,7 +69,7 @@ enum WsSlot {
     WS_VERTS = 0, WS_KIND, WS_PLANES, WS_BAD, WS_ST, WS_WORK, WS_NWORK, WS_S, WS_A, WS_U, WS_RHS, WS_X, WS_PHII,
     WS_IPIV, WS_INFO, WS_FI, WS_FD, WS_TILES, WS_SCR, WS_FPT, WS_HEADS, WS_OUT, WS_S32, WS_A32, WS_W, WS_P2,
     WS_P3, WS_PL, WS_PU, WS_B, WS_XM, WS_R, WS_NORMS, WS_ERR, WS_PART, WS_DINV, WS_TILES_F, WS_SG_PARAMS,
-    WS_SG_IMG, WS_SG_COUNT, WS_TRI_CTRL, WS_RS, WS_L16, WS_P3H, WS_PBODY, WS_RCEN, WS_UP, WS_PHI, WS_COUNT
+    WS_SG_IMG, WS_SG_COUNT, WS_TRI_CTRL, WS_RS, WS_L16, WS_P3H, WS_PBODY, WS_RCEN, WS_UP, WS_PHI, WS_RIGID, WS_HYD, WS_COUNT
 };
 
 // Page-locked host buffers of a solve: a device-to-host copy into pageable memory waits for the
@@ -293,6 +293,15 @@ void launch_boundary(const PanelsView& pv, int F, const FreqInfo* fi, int H, con
 // rhs[F][nrhs][N] = -S u
 void launch_rhs_f64(int N, int F, int nrhs, const double2* S, size_t mat_stride, const double2* u, double2* rhs,
                     cudaStream_t s);
+// the rigid data of the motions as uploaded, per body: mass (NaN: displaced), centre of gravity (3),
+// inertia kind, inertia (9), inertia origin (3)
+constexpr int RIGID_PER_BODY = 17;
+// hydrostatics of each body (records of HBG_HS doubles) and the block-diagonal motion matrices M, C and
+// the additional damping B_ext (D x D row-major); the motions xi[F][H][D] of F frequencies
+void launch_hydrostatics(const PanelsView& pv, const double* rig, const double* cext, const double* bext, double rho,
+                         double grav, double* hs, double* MM, double* CC, double* BB, cudaStream_t s);
+void launch_motions(int F, int D, int H, const FreqInfo* fi, const double* A, const double* B, const double2* X,
+                    const double* MM, const double* CC, const double* BB, double2* xi, int* err, cudaStream_t s);
 // forces: out[F][...] A, B [6][6], X, FK, SC [H][6] complex, all f64
 void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, int ldphi,
                    const double2* phiI, double rho, double* A, double* B, double2* X, double2* FK, double2* SC,

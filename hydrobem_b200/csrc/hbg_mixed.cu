@@ -153,7 +153,7 @@ static SideStreams& side_streams() {
 
 int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgProblem& pr, const HbgOptions& opt,
                             bool fin, double depth, cudaStream_t s, double* prof, int64_t* launches, const char** msg,
-                            int64_t* freq, const std::function<void()>& start) {
+                            int64_t* freq, const std::function<void()>& start, const double* motion) {
     KernelProfiler& P = profiler();
     // N panels; with symmetry sectors G systems of Nm = N / G unknowns per frequency (one of N otherwise)
     const int N = pv.N, G = pv.G, Nm = N / G, F = (int)pr.n_omega, H = (int)pr.n_heading, D = 6 * pv.nbod,
@@ -250,7 +250,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     unsigned long long* sg_count = sg ? (unsigned long long*)get(WS_SG_COUNT, sizeof(unsigned long long)) : nullptr;
     double* scr = fin ? (double*)get(WS_SCR, sizeof(double) * 6912 * 3 * B) : nullptr;
     double* fpt = fin ? (double*)get(WS_FPT, sizeof(double) * FP_PLANES * N * B) : nullptr;
-    double* dout = (double*)get(WS_OUT, sizeof(double) * (2 * (size_t)D * D + 3 * (size_t)H * 2 * D) * B);
+    double* dout = (double*)get(WS_OUT, sizeof(double) * (2 * (size_t)D * D + 4 * (size_t)H * 2 * D) * B);
     if (!okb) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
     last_surrogate_pairs() = 0;
     // ---- tensor maps (whole batch; the batch index is the 4th coordinate)
@@ -294,7 +294,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
     std::vector<FreqInfo> fi(B);
     std::vector<FdParams> fdh(B);
-    const size_t out_per = 2 * (size_t)D * D + 3 * (size_t)H * 2 * D, DD = (size_t)D * D;
+    // per frequency: A, B [D][D], X, FK, SC, motions [H][D] complex
+    const size_t out_per = 2 * (size_t)D * D + 4 * (size_t)H * 2 * D, DD = (size_t)D * D;
     // page-locked: the reads of norms, outputs and the error flag queue behind the work, no host wait
     double* hout = (double*)ws.host(HS_OUT, sizeof(double) * (out_per * B + 1));
     double* hn = (double*)ws.host(HS_NORMS, sizeof(double) * IR_MAX_IT * 2 * (size_t)BS);
@@ -704,6 +705,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 launch_forces(pv, nb, dfi, H, G > 1 ? phi : x, G > 1 ? N : Np, phiI, opt.density, dA, dB, dX, dFK, dSC, s);
                 P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
                 (*launches)++;
+                if (motion && H > 0) {  // the motion equation of every frequency (motion.rs:121-158)
+                    launch_motions(nb, D, H, dfi, dA, dB, dX, motion, motion + DD, motion + 2 * DD,
+                                   dSC + (size_t)H * D * nb, err, s);
+                    (*launches)++;
+                }
                 cudaMemcpyAsync(hout, dout, sizeof(double) * out_per * nb, cudaMemcpyDeviceToHost, s);
                 cudaMemcpyAsync(herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
                 tf.stop();
@@ -773,6 +779,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         if (cudaGetLastError() != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "CUDA error in the mixed-precision solve", f0);
         if (*herr == 10) MIXED_FAIL(HB_ERR_NUMERICAL, "zero pivot in the unpivoted mixed-precision LU", f0);
         if (*herr == 8) MIXED_FAIL(HB_ERR_INTERNAL, "a triangular sweep wait timed out", f0);
+        if (*herr == 11) MIXED_FAIL(HB_ERR_NUMERICAL, "singular motion equation", f0);
         if (*herr != 0) MIXED_FAIL(HB_ERR_INTERNAL, "a tensor-core pipeline wait timed out", f0);
         if (!converged)
             MIXED_FAIL(HB_ERR_NUMERICAL, "iterative refinement of the mixed-precision solve did not converge", f0);
@@ -781,6 +788,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         const double* hX = hA + 2 * DD * nb;
         const double* hFK = hX + (size_t)H * 2 * D * nb;
         const double* hSC = hFK + (size_t)H * 2 * D * nb;
+        const double* hMo = hSC + (size_t)H * 2 * D * nb;
         for (int i = 0; i < nb; i++) {
             const size_t fo = (size_t)(f0 + i), hx = (size_t)H * 2 * D;
             for (size_t q = 0; q < DD; q++)
@@ -791,6 +799,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             if (pr.out.excitation) memcpy(pr.out.excitation + fo * hx, hX + hx * i, hx * sizeof(double));
             if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
+            if (motion && pr.out.motions) memcpy(pr.out.motions + fo * hx, hMo + hx * i, hx * sizeof(double));
         }
         last_ir_iterations() = it;
     }

@@ -32,6 +32,17 @@ struct BodyObj {
     std::string interior_mesh;
     double position[3] = {0.0, 0.0, 0.0};         // the global position of the body origin
     double rotation_center[3] = {0.0, 0.0, 0.0};  // body-local
+    // mass properties (document_schema.rs:287-297): centre of gravity (body-local), mass given or
+    // "displaced", inertia as components or radii of gyration about inertia_origin
+    bool has_cg = false;
+    double cg[3] = {0.0, 0.0, 0.0};
+    int mass_kind = 0;  // 0 none, 1 given, 2 displaced
+    double mass = 0.0;
+    std::string inertia_input = "radii_of_gyration";
+    double I[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // Ixx, Ixy, Ixz, Iyy, Iyz, Izz
+    double gyration[9] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    std::string inertia_origin = "center_of_gravity";  // or rotation_center, or point
+    double inertia_point[3] = {0.0, 0.0, 0.0};          // body-local
 };
 
 struct Quantity {
@@ -60,6 +71,7 @@ struct HbModel {
     double log_tolerance = 1e-4;
     std::string precision = "fp64";
     int64_t device = 0;
+    bool motion = false;
     std::vector<hbg::MeshObj> meshes;
     std::vector<hbg::BodyObj> bodies;
     std::unique_ptr<HbResults> results;
@@ -220,13 +232,31 @@ extern "C" HbStatus hb_set_reals(HbModel* model, uint64_t object, const char* it
                 return HB_OK;
             }
         }
-        if (is_body(model, object) && (it == "position" || it == "rotation_center")) {
+        if (is_body(model, object) && (it == "position" || it == "rotation_center" || it == "center_of_gravity" ||
+                                       it == "inertia_origin")) {
             if (ndim != 1 || shape[0] != 3) return refuse(HB_ERR_VALUE, it + " has 3 values");
             for (double x : v)
                 if (!std::isfinite(x)) return refuse(HB_ERR_VALUE, it + " must be finite");
             BodyObj& b = model->bodies[object - OBJ_BODY0];
-            double* dst = it == "position" ? b.position : b.rotation_center;
+            double* dst = it == "position" ? b.position : it == "rotation_center" ? b.rotation_center
+                          : it == "center_of_gravity"                          ? b.cg
+                                                                               : b.inertia_point;
             for (int d = 0; d < 3; d++) dst[d] = v[d];
+            if (it == "center_of_gravity") b.has_cg = true;
+            if (it == "inertia_origin") b.inertia_origin = "point";
+            return HB_OK;
+        }
+        if (is_body(model, object) && it == "radii_of_gyration") {
+            const bool diag = ndim == 1 && shape[0] == 3, full = ndim == 2 && shape[0] == 3 && shape[1] == 3;
+            if (!diag && !full) return refuse(HB_ERR_VALUE, "radii_of_gyration has 3 values or 3 x 3");
+            for (double x : v)
+                if (!std::isfinite(x)) return refuse(HB_ERR_VALUE, "radii_of_gyration must be finite");
+            if (full)
+                for (int i = 0; i < 3; i++)
+                    for (int j = 0; j < i; j++)
+                        if (v[3 * i + j] != v[3 * j + i]) return refuse(HB_ERR_VALUE, "radii_of_gyration is symmetric");
+            BodyObj& b = model->bodies[object - OBJ_BODY0];
+            for (int k = 0; k < 9; k++) b.gyration[k] = full ? v[k] : (k % 4 == 0 ? v[k / 4] : 0.0);
             return HB_OK;
         }
         if (is_mesh(model, object) && it == "vertices") {
@@ -248,6 +278,22 @@ extern "C" HbStatus hb_set_real(HbModel* model, uint64_t object, const char* ite
         if (std::isnan(value)) return refuse(HB_ERR_VALUE, "NaN");
         if (is_body(model, object) && it == "yaw")
             return value == 0.0 ? HB_OK : refuse(HB_ERR_UNSUPPORTED, "a body rotated about z (yaw != 0) is not on this route");
+        if (is_body(model, object)) {
+            BodyObj& b = model->bodies[object - OBJ_BODY0];
+            if (it == "mass") {
+                if (!(value >= 0.0) || !std::isfinite(value)) return refuse(HB_ERR_VALUE, "mass >= 0 and finite");
+                b.mass = value;
+                b.mass_kind = 1;
+                return HB_OK;
+            }
+            static const char* comp[6] = {"Ixx", "Ixy", "Ixz", "Iyy", "Iyz", "Izz"};
+            for (int k = 0; k < 6; k++)
+                if (it == comp[k]) {
+                    if (!std::isfinite(value)) return refuse(HB_ERR_VALUE, it + " must be finite");
+                    b.I[k] = value;
+                    return HB_OK;
+                }
+        }
         if (object == OBJ_ENV) {
             if (it == "depth") {
                 if (!(value > 0.0)) return refuse(HB_ERR_VALUE, "depth > 0 (inf for infinite depth)");
@@ -276,6 +322,10 @@ extern "C" HbStatus hb_set_bool(HbModel* model, uint64_t object, const char* ite
         std::string it(item);
         if (object == OBJ_OPTIONS && it == "logarithmic_integration") {
             model->logarithmic = value != 0;
+            return HB_OK;
+        }
+        if (object == OBJ_OPTIONS && it == "motion") {
+            model->motion = value != 0;
             return HB_OK;
         }
         return refuse(HB_ERR_UNSUPPORTED, "the item \"" + it + "\" of this object is not on this route");
@@ -336,6 +386,21 @@ extern "C" HbStatus hb_set_text(HbModel* model, uint64_t object, const char* ite
                 return b.interior = v, HB_OK;
             }
             if (it == "interior_surface_mesh") return b.interior_mesh = v, HB_OK;
+            if (it == "mass") {
+                if (v != "displaced") return refuse(HB_ERR_VALUE, "mass is a number or \"displaced\"");
+                b.mass_kind = 2;
+                return HB_OK;
+            }
+            if (it == "inertia_input") {
+                if (v != "components" && v != "radii_of_gyration")
+                    return refuse(HB_ERR_VALUE, "inertia_input is components or radii_of_gyration");
+                return b.inertia_input = v, HB_OK;
+            }
+            if (it == "inertia_origin") {
+                if (v != "center_of_gravity" && v != "rotation_center")
+                    return refuse(HB_ERR_VALUE, "inertia_origin is center_of_gravity, rotation_center or a point");
+                return b.inertia_origin = v, HB_OK;
+            }
         }
         return refuse(HB_ERR_UNSUPPORTED, "the item \"" + it + "\" of this object is not on this route");
     });
@@ -352,6 +417,10 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         std::vector<double> verts, omegas, heads, centers;
         std::vector<int32_t> kinds, panel_body;
         int32_t symmetry = HBG_SYM_NONE;
+        // mass properties in the global frame (all bodies or none: the weight terms and the motions)
+        std::vector<double> rmass, rcg, rinertia, rorigin;
+        std::vector<int32_t> rkind;
+        bool all_rigid = true;
         HbgOptions opt;
         hbg_default_options(&opt);
         {
@@ -397,7 +466,20 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
                 kinds.insert(kinds.end(), bk.begin(), bk.end());
                 panel_body.insert(panel_body.end(), bk.size(), (int32_t)bi);
                 for (int d = 0; d < 3; d++) centers.push_back(b.position[d] + b.rotation_center[d]);
+                all_rigid = all_rigid && b.has_cg && b.mass_kind != 0;
+                rmass.push_back(b.mass_kind == 2 ? NAN : b.mass);
+                for (int d = 0; d < 3; d++) rcg.push_back(b.position[d] + b.cg[d]);
+                const bool comps = b.inertia_input == "components";
+                rkind.push_back(comps ? HBG_INERTIA_COMPONENTS : HBG_INERTIA_GYRATION);
+                const double J[9] = {b.I[0], b.I[1], b.I[2], b.I[1], b.I[3], b.I[4], b.I[2], b.I[4], b.I[5]};
+                for (int k = 0; k < 9; k++) rinertia.push_back(comps ? J[k] : b.gyration[k]);
+                const double* o = b.inertia_origin == "center_of_gravity" ? b.cg
+                                  : b.inertia_origin == "rotation_center" ? b.rotation_center
+                                                                          : b.inertia_point;
+                for (int d = 0; d < 3; d++) rorigin.push_back(b.position[d] + o[d]);
             }
+            if (model->motion && !all_rigid)
+                return refuse(HB_ERR_VALUE, "the motions need the mass and center_of_gravity of every body");
             const std::vector<double>& f = model->frequency_input == "omegas" ? model->omegas : model->periods;
             for (double x : f) {
                 double w = model->frequency_input == "omegas" ? x : (x > 0.0 ? 2.0 * PI / x : INFINITY);
@@ -417,8 +499,12 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         opt.cancel = reinterpret_cast<const volatile int32_t*>(&model->cancel);
         if (model->cancel.exchange(0) != 0) return refuse(HB_ERR_CANCELLED, "the solve was cancelled");
         const size_t F = omegas.size(), H = heads.size(), NB = centers.size() / 3, D = 6 * NB;
-        std::vector<double> A(F * D * D), B(F * D * D), X(F * H * D * 2), FK(F * H * D * 2), SC(F * H * D * 2);
+        std::vector<double> A(F * D * D), B(F * D * D), X(F * H * D * 2), FK(F * H * D * 2), SC(F * H * D * 2),
+            MO(F * H * D * 2), HS(NB * HBG_HS);
+        const bool want_motion = model->motion && H > 0;
+        HbgRigid rig{rmass.data(), rcg.data(), rkind.data(), rinertia.data(), rorigin.data(), nullptr, nullptr};
         HbgProblem pr{};
+        pr.rigid = all_rigid ? &rig : nullptr;
         pr.body.n_panels = (int64_t)(verts.size() / 12);
         pr.body.vertices = verts.data();
         pr.body.kinds = kinds.data();
@@ -430,7 +516,8 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         pr.n_omega = (int64_t)F;
         pr.headings_deg = heads.data();
         pr.n_heading = (int64_t)H;
-        pr.out = HbgOutputs{A.data(), B.data(), X.data(), FK.data(), SC.data()};
+        pr.out = HbgOutputs{A.data(), B.data(), X.data(), FK.data(), SC.data(), want_motion ? MO.data() : nullptr,
+                            HS.data()};
         if (progress) {
             HbProgress pg{};
             pg.stage = 0;
@@ -473,6 +560,48 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         add_quantity(r.get(), "excitation_diffraction_f64", HB_C128, {F, H, D}, X.data(), X.size() * 8);
         add_quantity(r.get(), "excitation_froude_krylov_f64", HB_C128, {F, H, D}, FK.data(), FK.size() * 8);
         add_quantity(r.get(), "excitation_scattering_f64", HB_C128, {F, H, D}, SC.data(), SC.size() * 8);
+        if (want_motion) {
+            std::vector<float> m32(F * H * D * 2);
+            for (size_t i = 0; i < m32.size(); i++) m32[i] = (float)MO[i];
+            add_quantity(r.get(), "motion", HB_C64, {F, H, D}, m32.data(), m32.size() * 4);
+            add_quantity(r.get(), "motion_f64", HB_C128, {F, H, D}, MO.data(), MO.size() * 8);
+        }
+        {
+            // the hydrostatics of every body (quantities.rs:102-112), body coordinates as the reference's
+            std::vector<double> vols(NB * 3), vol(NB), disp(NB), cb(NB * 3), aw(NB), wc(NB * 2), crg(NB * 36), cw(NB * 36),
+                mass(NB), cgo(NB * 3), gm(NB * 2);
+            const double rg = model->density * model->gravity;
+            for (size_t b = 0; b < NB; b++) {
+                const double* h = &HS[b * HBG_HS];
+                const BodyObj& bo = model->bodies[b];
+                for (int k = 0; k < 3; k++) vols[3 * b + k] = h[k];
+                vol[b] = (h[0] + h[1] + h[2]) / 3.0;
+                disp[b] = h[82];
+                for (int k = 0; k < 3; k++) cb[3 * b + k] = h[3 + k] - bo.position[k];
+                aw[b] = h[6];
+                for (int k = 0; k < 2; k++) wc[2 * b + k] = h[7 + k] - bo.position[k];
+                for (int k = 0; k < 36; k++) {
+                    crg[36 * b + k] = h[9 + k];
+                    cw[36 * b + k] = h[45 + k];
+                }
+                mass[b] = h[81];
+                for (int k = 0; k < 3; k++) cgo[3 * b + k] = bo.has_cg ? bo.cg[k] : NAN;
+                const bool weight = all_rigid && h[0] != 0.0;
+                gm[2 * b] = weight ? h[45 + 3 * 6 + 3] / (rg * h[0]) : NAN;
+                gm[2 * b + 1] = weight ? h[45 + 4 * 6 + 4] / (rg * h[0]) : NAN;
+            }
+            add_quantity(r.get(), "hydrostatics_volumes", HB_F64, {NB, 3}, vols.data(), vols.size() * 8);
+            add_quantity(r.get(), "hydrostatics_volume", HB_F64, {NB}, vol.data(), vol.size() * 8);
+            add_quantity(r.get(), "hydrostatics_displaced_mass", HB_F64, {NB}, disp.data(), disp.size() * 8);
+            add_quantity(r.get(), "hydrostatics_center_of_buoyancy", HB_F64, {NB, 3}, cb.data(), cb.size() * 8);
+            add_quantity(r.get(), "hydrostatics_waterplane_area", HB_F64, {NB}, aw.data(), aw.size() * 8);
+            add_quantity(r.get(), "hydrostatics_waterplane_centroid", HB_F64, {NB, 2}, wc.data(), wc.size() * 8);
+            add_quantity(r.get(), "hydrostatics_stiffness_rho_g", HB_F64, {NB, 6, 6}, crg.data(), crg.size() * 8);
+            add_quantity(r.get(), "hydrostatics_stiffness", HB_F64, {NB, 6, 6}, cw.data(), cw.size() * 8);
+            add_quantity(r.get(), "hydrostatics_mass", HB_F64, {NB}, mass.data(), mass.size() * 8);
+            add_quantity(r.get(), "hydrostatics_center_of_gravity", HB_F64, {NB, 3}, cgo.data(), cgo.size() * 8);
+            add_quantity(r.get(), "hydrostatics_metacentric_height", HB_F64, {NB, 2}, gm.data(), gm.size() * 8);
+        }
         {
             std::lock_guard<std::mutex> g(model->lock);
             model->results = std::make_unique<HbResults>(*r);

@@ -38,12 +38,30 @@ SYM_NONE, SYM_YZ, SYM_XZ, SYM_BOTH = 0, 1, 2, 3
 
 class HbgOutputs(ctypes.Structure):
     _fields_ = [("added_mass", dp), ("radiation_damping", dp), ("excitation", dp), ("froude_krylov", dp),
-                ("scattering", dp)]
+                ("scattering", dp), ("motions", dp), ("hydrostatics", dp)]
+
+
+class HbgRigid(ctypes.Structure):
+    _fields_ = [("mass", dp), ("center_of_gravity", dp), ("inertia_kind", ip), ("inertia", dp),
+                ("inertia_origin", dp), ("stiffness", dp), ("damping", dp)]
 
 
 class HbgProblem(ctypes.Structure):
     _fields_ = [("body", HbgBody), ("omegas", dp), ("n_omega", ctypes.c_int64), ("headings_deg", dp),
-                ("n_heading", ctypes.c_int64), ("out", HbgOutputs)]
+                ("n_heading", ctypes.c_int64), ("out", HbgOutputs), ("rigid", ctypes.POINTER(HbgRigid))]
+
+
+# HbgRigid.inertia_kind, and the record of HbgOutputs.hydrostatics (HBG_HS doubles per body)
+INERTIA_COMPONENTS, INERTIA_GYRATION = 0, 1
+HBG_HS = 83
+
+
+def hydrostatics_record(h):
+    """The fields of one body's hydrostatics record (global frame)."""
+    h = np.asarray(h, dtype=np.float64)
+    return {"volumes": h[0:3], "center_of_buoyancy": h[3:6], "waterplane_area": h[6],
+            "waterplane_centroid": h[7:9], "stiffness_rho_g": h[9:45].reshape(6, 6),
+            "stiffness": h[45:81].reshape(6, 6), "mass": h[81], "displaced_mass": h[82]}
 
 
 class HbgOptions(ctypes.Structure):
@@ -151,10 +169,13 @@ class Body:
     """The inputs and output arrays of one problem of a batch (kept alive across the call): the panels of
     one rigid body, or of interacting bodies with panel_body (the body of each panel) and
     rotation_centers [n_bodies][3] (None: the origin); 6 rigid modes per body, D = 6 n_bodies.  With
-    symmetry (SYM_YZ, SYM_XZ, SYM_BOTH) the panels are one sector of a body mirrored in those planes."""
+    symmetry (SYM_YZ, SYM_XZ, SYM_BOTH) the panels are one sector of a body mirrored in those planes.
+    rigid: the mass properties for the motions, a dict of mass [n_bodies] (NaN: displaced),
+    center_of_gravity [n_bodies][3], inertia [n_bodies][3][3] about inertia_origin [n_bodies][3],
+    inertia_kind [n_bodies] (INERTIA_COMPONENTS / INERTIA_GYRATION), optional stiffness, damping [D][D]."""
 
     def __init__(self, vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None,
-                 symmetry=SYM_NONE):
+                 symmetry=SYM_NONE, rigid=None):
         self.symmetry = int(symmetry)
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 4, 3)
         self.kinds = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
@@ -172,6 +193,23 @@ class Body:
         self.X = np.zeros((F, H, D), dtype=np.complex128)
         self.FK = np.zeros((F, H, D), dtype=np.complex128)
         self.SC = np.zeros((F, H, D), dtype=np.complex128)
+        self.HS = np.zeros((self.n_bodies, HBG_HS))
+        self.MO = np.zeros((F, H, D), dtype=np.complex128) if rigid is not None else None
+        self._rigid = None
+        if rigid is not None:
+            nb = self.n_bodies
+            arr = lambda k, shape: np.ascontiguousarray(np.broadcast_to(np.asarray(rigid[k], dtype=np.float64), shape))
+            self._rig_keep = {
+                "mass": arr("mass", (nb,)), "cg": arr("center_of_gravity", (nb, 3)),
+                "kind": np.ascontiguousarray(np.broadcast_to(np.asarray(rigid.get("inertia_kind", 0), np.int32), (nb,))),
+                "inertia": arr("inertia", (nb, 3, 3)), "origin": arr("inertia_origin", (nb, 3)),
+                "stiffness": None if rigid.get("stiffness") is None else arr("stiffness", (D, D)),
+                "damping": None if rigid.get("damping") is None else arr("damping", (D, D))}
+            k = self._rig_keep
+            self._rigid = HbgRigid(k["mass"].ctypes.data_as(dp), k["cg"].ctypes.data_as(dp), k["kind"].ctypes.data_as(ip),
+                                   k["inertia"].ctypes.data_as(dp), k["origin"].ctypes.data_as(dp),
+                                   None if k["stiffness"] is None else k["stiffness"].ctypes.data_as(dp),
+                                   None if k["damping"] is None else k["damping"].ctypes.data_as(dp))
 
     def problem(self) -> HbgProblem:
         p = HbgProblem()
@@ -191,10 +229,17 @@ class Body:
         p.out.excitation = self.X.ctypes.data_as(dp)
         p.out.froude_krylov = self.FK.ctypes.data_as(dp)
         p.out.scattering = self.SC.ctypes.data_as(dp)
+        p.out.motions = None if self.MO is None else self.MO.ctypes.data_as(dp)
+        p.out.hydrostatics = self.HS.ctypes.data_as(dp)
+        p.rigid = None if self._rigid is None else ctypes.pointer(self._rigid)
         return p
 
     def results(self):
-        return {"A": self.A, "B": self.B, "X": self.X, "FK": self.FK, "SC": self.SC}
+        out = {"A": self.A, "B": self.B, "X": self.X, "FK": self.FK, "SC": self.SC,
+               "hydrostatics": [hydrostatics_record(h) for h in self.HS]}
+        if self.MO is not None:
+            out["motions"] = self.MO
+        return out
 
 
 def solve_batch(bodies, **options):
@@ -206,9 +251,10 @@ def solve_batch(bodies, **options):
 
 
 def solve(vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None,
-          symmetry=SYM_NONE, **options):
-    """One problem through the GPU path: dict of A, B [F][D][D], X, FK, SC [F][H][D], D = 6 per body."""
-    return solve_batch([Body(vertices, omegas, headings_deg, kinds, panel_body, rotation_centers, symmetry)],
+          symmetry=SYM_NONE, rigid=None, **options):
+    """One problem through the GPU path: dict of A, B [F][D][D], X, FK, SC [F][H][D], D = 6 per body, the
+    hydrostatics records of the bodies, and with rigid the motions [F][H][D]."""
+    return solve_batch([Body(vertices, omegas, headings_deg, kinds, panel_body, rotation_centers, symmetry, rigid)],
                        **options)[0]
 
 

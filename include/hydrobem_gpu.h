@@ -50,7 +50,7 @@ typedef int32_t HbStatus;
 #define HB_C128 7
 
 /* The version of this library's ABI (its own numbering; the reference's hb_abi_version is 8). */
-#define HBG_ABI_VERSION 4
+#define HBG_ABI_VERSION 5
 
 /* ==================================================================== batched entry */
 
@@ -90,15 +90,50 @@ typedef struct HbgBody {
     int32_t symmetry;
 } HbgBody;
 
+/* The rigid-body data of the motions (crates/hydrobem/src/motion.rs, hydrostatics.rs:315-356), per body
+ * in the global frame of the panels:
+ *   mass [n_bodies]             kg; NaN: the displaced mass rho V (V the x estimate of the volume)
+ *   center_of_gravity [n_bodies][3]
+ *   inertia_kind [n_bodies]     HBG_INERTIA_COMPONENTS: inertia [3][3] in kg m^2; HBG_INERTIA_GYRATION:
+ *                               radii of gyration r [3][3] in m, I_ij = m r_ij |r_ij| with the mass in use
+ *   inertia [n_bodies][3][3]    about inertia_origin, body axes
+ *   inertia_origin [n_bodies][3]  the point the inertia is about
+ *   stiffness, damping [D][D]   additional matrices about the rotation centres, or NULL
+ * The motion equation of each frequency: (C - w^2 (M + A) + i w (B + B_ext)) xi = X (motion.rs:121-158),
+ * C the hydrostatic stiffness with the weight terms plus the additional stiffness, M the rigid inertia
+ * about the rotation centres. */
+#define HBG_INERTIA_COMPONENTS 0
+#define HBG_INERTIA_GYRATION 1
+typedef struct HbgRigid {
+    const double *mass;
+    const double *center_of_gravity;
+    const int32_t *inertia_kind;
+    const double *inertia;
+    const double *inertia_origin;
+    const double *stiffness;
+    const double *damping;
+} HbgRigid;
+
+/* The hydrostatics record of one body (hydrostatics.rs:143-313), HBG_HS doubles, global frame:
+ *   [0..3) the three volume estimates (x n_x, y n_y, z n_z), [3..6) the centre of buoyancy,
+ *   [6] the waterplane area, [7..9) its centroid (x, y), [9..45) the stiffness of the rho g terms,
+ *   [45..81) the stiffness with the weight terms, [81] the mass in use (NaN without one), [82] the
+ *   displaced mass rho V_x; stiffness matrices 6 x 6 row-major about the rotation centre. */
+#define HBG_HS 83
+
 /* Outputs of one problem, caller-allocated host arrays (NULL: not wanted), float64, D = 6 n_bodies:
  *   added_mass, radiation_damping  [n_omega][D][D]   (coordinate i, radiation mode j)
- *   excitation, froude_krylov, scattering  [n_omega][n_heading][D][2]  (re, im)          */
+ *   excitation, froude_krylov, scattering, motions  [n_omega][n_heading][D][2]  (re, im)
+ *   hydrostatics  [n_bodies][HBG_HS]
+ * motions needs the problem's rigid data. */
 typedef struct HbgOutputs {
     double *added_mass;
     double *radiation_damping;
     double *excitation;
     double *froude_krylov;
     double *scattering;
+    double *motions;
+    double *hydrostatics;
 } HbgOutputs;
 
 typedef struct HbgProblem {
@@ -108,6 +143,7 @@ typedef struct HbgProblem {
     const double *headings_deg;
     int64_t n_heading;
     HbgOutputs out;
+    const HbgRigid *rigid; /* NULL: no motions */
 } HbgProblem;
 
 typedef struct HbgOptions {

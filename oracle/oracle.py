@@ -9,6 +9,8 @@ and adds, in numpy, the steps that are short formulas of ``crates/hydrobem/src/`
 - right-hand sides -S u and the dense solve  ``lo_frequency.rs:823-955`` (LU with partial pivoting:
   LAPACK ``zgesv`` through numpy, standing in for faer's blocked LU, ``linalg.rs:134-252``)
 - pressure integration A, B, X, FK, SC  ``lo_frequency.rs:1039-1115``
+- hydrostatics, rigid inertia and the motion equation of each frequency  ``hydrostatics.rs:116-356``,
+  ``motion.rs:121-158``
 - symmetry sectors (a body given as one sector of its mirror-symmetric mesh): the matrices of the
   mirrored mesh's sector rows summed over the reflections with the group's characters, one system
   per sector, the potentials recombined  ``lo_geometry.rs:25-36``, ``lo_frequency.rs:276-346,823-943``
@@ -296,8 +298,83 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
     return out
 
 
+# ------------------------------------------------------------------ hydrostatics and motions
+def hydrostatics(c, n, area, kinds=None, panel_body=None, centers=None, rho=DENSITY, grav=GRAVITY, rigid=None):
+    """The hydrostatics of every body (hydrostatics.rs:116-313; one quadrature point per panel, its centroid
+    with n dS = area n, quadrature.rs:152-159) and, with rigid (the dict of native.Body), the motion matrices:
+    (records, M, C, B_ext) with M the rigid inertia about the rotation centres (hydrostatics.rs:315-356), C
+    the restoring matrix with the weight terms plus the additional stiffness, all D x D."""
+    nb = 1 if panel_body is None else int(np.max(panel_body)) + 1
+    if centers is not None:
+        nb = max(nb, len(centers))
+    body = np.zeros(len(c), int) if panel_body is None else np.asarray(panel_body)
+    R = np.zeros((nb, 3)) if centers is None else np.asarray(centers, dtype=float).reshape(-1, 3)
+    wet = np.ones(len(c), bool) if kinds is None else np.asarray(kinds) == WET
+    D = 6 * nb
+    M, C, Bx = np.zeros((D, D)), np.zeros((D, D)), np.zeros((D, D))
+    recs = []
+    for b in range(nb):
+        on = wet & (body == b)
+        x, y, z = c[on, 0] - R[b, 0], c[on, 1] - R[b, 1], c[on, 2]
+        nds = area[on, None] * n[on]
+        vx, vy, V = (x * nds[:, 0]).sum(), (y * nds[:, 1]).sum(), (z * nds[:, 2]).sum()
+        mx, my, mz = (0.5 * x * x * nds[:, 0]).sum(), (0.5 * y * y * nds[:, 1]).sum(), (0.5 * z * z * nds[:, 2]).sum()
+        aw, ax, ay = -nds[:, 2].sum(), -(x * nds[:, 2]).sum(), -(y * nds[:, 2]).sum()
+        axx, ayy, axy = -(x * x * nds[:, 2]).sum(), -(y * y * nds[:, 2]).sum(), -(x * y * nds[:, 2]).sum()
+        rg, Vzb = rho * grav, mz - R[b, 2] * V
+        crg = np.zeros((6, 6))
+        crg[2, 2] = rg * aw
+        crg[2, 3] = crg[3, 2] = rg * ay
+        crg[2, 4] = crg[4, 2] = -rg * ax
+        crg[3, 3] = rg * (ayy + Vzb)
+        crg[3, 4] = crg[4, 3] = -rg * axy
+        crg[3, 5] = -rg * mx
+        crg[4, 4] = rg * (axx + Vzb)
+        crg[4, 5] = -rg * my
+        cw = crg.copy()
+        mass = np.nan
+        Mb = np.zeros((6, 6))
+        if rigid is not None:
+            m0 = np.asarray(rigid["mass"], float).reshape(-1)[b]
+            mass = rho * vx if np.isnan(m0) else m0
+            cg = np.asarray(rigid["center_of_gravity"], float).reshape(-1, 3)[b]
+            g = cg - R[b]
+            mg = mass * grav
+            cw[3, 3] -= mg * g[2]
+            cw[3, 5] += mg * g[0]
+            cw[4, 4] -= mg * g[2]
+            cw[4, 5] += mg * g[1]
+            J = np.asarray(rigid["inertia"], float).reshape(-1, 3, 3)[b].copy()
+            if int(np.broadcast_to(np.asarray(rigid.get("inertia_kind", 0)), (nb,))[b]) == 1:  # radii of gyration
+                J = mass * J * np.abs(J)
+            a = cg - np.asarray(rigid["inertia_origin"], float).reshape(-1, 3)[b]
+            J += -mass * (np.dot(a, a) * np.eye(3) - np.outer(a, a)) + mass * (np.dot(g, g) * np.eye(3) - np.outer(g, g))
+            S = np.array([[0.0, -g[2], g[1]], [g[2], 0.0, -g[0]], [-g[1], g[0], 0.0]])
+            Mb[:3, :3] = mass * np.eye(3)
+            Mb[:3, 3:] = -mass * S
+            Mb[3:, :3] = mass * S
+            Mb[3:, 3:] = J
+        M[6 * b:6 * b + 6, 6 * b:6 * b + 6] = Mb
+        C[6 * b:6 * b + 6, 6 * b:6 * b + 6] = cw
+        recs.append({"volumes": np.array([vx, vy, V]), "center_of_buoyancy": np.array([mx / V + R[b, 0], my / V + R[b, 1], mz / V]),
+                     "waterplane_area": aw, "waterplane_centroid": np.array([ax / aw + R[b, 0], ay / aw + R[b, 1]]),
+                     "stiffness_rho_g": crg, "stiffness": cw, "mass": mass, "displaced_mass": rho * vx})
+    if rigid is not None:
+        if rigid.get("stiffness") is not None:
+            C += np.asarray(rigid["stiffness"], float)
+        if rigid.get("damping") is not None:
+            Bx += np.asarray(rigid["damping"], float)
+    return recs, M, C, Bx
+
+
+def motions(A, B, X, omega, M, C, Bx):
+    """xi [H][D] of one frequency: (C - w^2 (M + A) + i w (B + B_ext)) xi = X (motion.rs:121-158)."""
+    Z = C - omega * omega * (M + A) + 1j * omega * (B + Bx)
+    return np.linalg.solve(Z, np.asarray(X).T).T
+
+
 def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GRAVITY, rho=DENSITY, logint=True,
-               tol=1e-4, panel_body=None, centers=None, symmetry=SYM_NONE):
+               tol=1e-4, panel_body=None, centers=None, symmetry=SYM_NONE, rigid=None):
     """The whole path for one problem: statics once, then every frequency. Arrays [F][D][D], [F][H][D]
     (D = 6 per body; interacting bodies by panel_body and their rotation centers).  With symmetry the
     panels (and kinds, panel_body) are one sector: mirrored, then solved by sectors."""
@@ -312,4 +389,10 @@ def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GR
     res = [solve_frequency(panels, kinds, st, depth, w, heads, grav, rho, logint, panel_body=panel_body,
                            centers=centers, sectors=G) for w in omegas]
     out = {k: np.array([r[k] for r in res]) for k in res[0]}
+    c, n, area = panel_arrays(panels)
+    recs, M, C, Bx = hydrostatics(c, n, area, kinds, panel_body, centers, rho, grav, rigid)
+    out["hydrostatics"] = recs
+    if rigid is not None and len(heads):
+        out["motions"] = np.array([motions(out["A"][i], out["B"][i], out["X"][i], w, M, C, Bx)
+                                   for i, w in enumerate(omegas)])
     return out

@@ -10,7 +10,8 @@ Every fixture is a compressed .npz of numbers the reference's test suite holds o
 - cylinder_fd.npz    tests/data/cylinder_finite_depth.txt (eigenfunction-matching A, B)
 - hulme.npz          tests/data/hulme1982_full.txt (hemisphere A, B, Hulme 1982)
 - lo_cylinder_drift.npz  the reference solver's own outputs of that regression problem
-  (tests/data/regression/lo_cylinder_drift.npz: A, B, X, FK, SC of a floating cylinder, f32)
+  (tests/data/regression/lo_cylinder_drift.npz: A, B, X, FK, SC, the motions (RAO) and the
+  hydrostatics of a floating cylinder with its mass and inertia, f32 / f64 as the reference stores them)
 - meshes.npz         SHA-256 digests and small copies of the reference's procedural meshes
   (tests/python/meshes.py imported from the reference) for the configs' bodies
 """
@@ -56,7 +57,11 @@ def main(argv):
     np.savez_compressed(HERE / "hulme.npz", vals=np.array([[float(t) for t in x] for x in r]))
     d = np.load(data / "regression" / "lo_cylinder_drift.npz")
     keep = ["omegas", "headings", "added_mass", "radiation_damping", "excitation_diffraction",
-            "excitation_froude_krylov", "excitation_scattering"]
+            "excitation_froude_krylov", "excitation_scattering", "motion", "hydrostatics_volumes",
+            "hydrostatics_volume", "hydrostatics_displaced_mass", "hydrostatics_center_of_buoyancy",
+            "hydrostatics_waterplane_area", "hydrostatics_waterplane_centroid", "hydrostatics_stiffness_rho_g",
+            "hydrostatics_stiffness", "hydrostatics_mass", "hydrostatics_center_of_gravity",
+            "hydrostatics_metacentric_height"]
     np.savez_compressed(HERE / "lo_cylinder_drift.npz", **{k: d[k] for k in keep})
     sys.path.insert(0, str(root / "tests" / "python"))
     import meshes  # the reference's procedural meshes (numpy only)
