@@ -499,6 +499,19 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
                 throw Failure{HB_ERR_VALUE, "an additional stiffness or damping entry is not finite", body_index};
     }
     const bool hydro = rigid || pr.out.hydrostatics;
+    // field points (lo_frequency.rs:1392-1470): in the fluid at z <= 0, above the sea bed
+    const int nfp = pr.field_points && pr.n_field_points > 0 ? (int)pr.n_field_points : 0;
+    if (pr.n_field_points < 0 || pr.n_field_points > 100000)
+        throw Failure{HB_ERR_VALUE, "n_field_points outside 0..100000", body_index};
+    for (int p = 0; p < nfp; p++) {
+        const double* q = pr.field_points + 3 * p;
+        if (!std::isfinite(q[0]) || !std::isfinite(q[1]) || !std::isfinite(q[2]) || q[2] > 0.0)
+            throw Failure{HB_ERR_VALUE, "a field point is not finite or lies above the free surface", body_index};
+        if (finite_depth(opt.depth) && q[2] < -opt.depth)
+            throw Failure{HB_ERR_VALUE, "a field point lies below the sea bed", body_index};
+    }
+    const bool field = nfp > 0 && (pr.out.field_radiation || pr.out.field_incident || pr.out.field_scattering ||
+                                 pr.out.field_diffraction);
     if (H > 26) throw Failure{HB_ERR_UNSUPPORTED, "more than 26 headings per solve", body_index};
     const bool fin = finite_depth(opt.depth);
     const double depth = fin ? opt.depth : 0.0;
@@ -538,6 +551,12 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         drig.alloc(sizeof(double) * rigid_host.size());
     }
     if (hydro) dhyd.alloc(sizeof(double) * ((size_t)nbod * HBG_HS + 3 * DD2));
+    // the field points and their statics rows [4][P][N] (entry (p, j) at p + j P)
+    WsBuf dpts(ws, WS_FPTS), dfst(ws, WS_FST);
+    if (field) {
+        dpts.alloc(sizeof(double) * 3 * nfp);
+        dfst.alloc(sizeof(double) * 4 * (size_t)nfp * N);
+    }
     const double* mot_mats = hydro ? dhyd.as<double>() + (size_t)nbod * HBG_HS : nullptr;
     std::vector<int32_t> kinds(N, 0);
     if (pr.body.kinds)
@@ -557,7 +576,8 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     dnwork.alloc(2 * sizeof(int32_t));  // [adaptive worklist size, queue cursor]
     const int32_t big = PANELS_VALID;
     // page-locked: [first invalid panel, adaptive worklist size]
-    int32_t* hflags = static_cast<int32_t*>(ws.host(HS_FLAGS, 2 * sizeof(int32_t)));
+    // [first invalid panel, adaptive worklist size, that of the field points]
+    int32_t* hflags = static_cast<int32_t*>(ws.host(HS_FLAGS, 3 * sizeof(int32_t)));
     if (!hflags) throw Failure{HB_ERR_INTERNAL, "page-locked host memory could not be allocated", body_index};
     double* prof = g_profile;
     bool statics_ran = false;
@@ -609,6 +629,20 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
                                   dst.as<double>(), s);
         P.end(KF_STATICS_ADAPTIVE, 0.0, s);
         g_launches += 2;
+        hflags[2] = 0;
+        if (field) {  // the statics rows of the field points (FP64 rules), the worklist reused after the above
+            CUDA_OK(cudaMemcpyAsync(dpts.p, pr.field_points, sizeof(double) * 3 * nfp, cudaMemcpyHostToDevice, s));
+            PanelsView pq{N, dplanes.as<double>(), dkind.as<int32_t>()};
+            pq.rows = dpts.as<double>();
+            pq.nrows = nfp;
+            CUDA_OK(cudaMemsetAsync(dnwork.p, 0, 2 * sizeof(int32_t), s));
+            launch_statics(pq, depth, opt.logarithmic, opt.log_tolerance, dfst.as<double>(), dwork.as<int32_t>(),
+                           dnwork.as<int32_t>(), work_cap, s, false);
+            CUDA_OK(cudaMemcpyAsync(hflags + 2, dnwork.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+            launch_statics_adaptive_q(pq, dwork.as<int32_t>(), dnwork.as<int32_t>(), work_cap, dbad.as<int32_t>(), big,
+                                      dfst.as<double>(), s);
+            g_launches += 2;
+        }
         t.stop();
         statics_ran = true;
     };
@@ -619,7 +653,8 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
             throw Failure{HB_ERR_VALUE,
                           "invalid panel " + std::to_string(hflags[0] + 1) + " (degenerate, non-convex or non-finite)",
                           body_index};
-        if (hflags[1] > work_cap) throw Failure{HB_ERR_INTERNAL, "adaptive log-integral worklist overflow", body_index};
+        if (hflags[1] > work_cap || hflags[2] > work_cap)
+            throw Failure{HB_ERR_INTERNAL, "adaptive log-integral worklist overflow", body_index};
     };
     // the mixed form's assembly kernels skip their work on invalid panels (the flag in device memory),
     // so that its solve runs without a host wait until the end; the FP64 form waits here
@@ -639,7 +674,8 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         const char* msg = "";
         int64_t fq = -1;
         int rc = mixed_solve_frequencies(pv, dst.as<double>(), pr, opt, fin, depth, s, prof, &g_launches, &msg, &fq,
-                                         run_statics, motions ? mot_mats : nullptr);
+                                         run_statics, motions ? mot_mats : nullptr,
+                                         FieldArgs{field ? dpts.as<double>() : nullptr, field ? nfp : 0, dfst.as<double>()});
         cudaError_t e = cudaStreamSynchronize(s);
         if (e == cudaSuccess) statics_check();
         if (rc != 0) throw Failure{rc, msg, body_index, fq};
@@ -710,8 +746,12 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
     dheads.alloc(sizeof(double) * heads.size());
     CUDA_OK(cudaMemcpyAsync(dheads.p, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s));
-    // outputs per batch: A, B [D][D], X, FK, SC, motions [H][D]
-    const size_t out_per = 2 * (size_t)D * D * sizeof(double) + 4 * (size_t)H * D * sizeof(double2);
+    // outputs per batch: A, B [D][D], X, FK, SC, motions [H][D], field values [P][D] and 3 x [P][H]
+    const int Pf = field ? nfp : 0;
+    const size_t out_per = 2 * (size_t)D * D * sizeof(double) + 4 * (size_t)H * D * sizeof(double2) +
+                           (size_t)Pf * (D + 3 * H) * sizeof(double2);
+    WsBuf dfq(ws, WS_FQ);
+    if (field && fin) dfq.alloc(sizeof(double) * FP_PLANES * (size_t)(N + nfp) * B);
     WsBuf derr(ws, WS_ERR);
     derr.alloc(sizeof(int32_t));
     dout.alloc(out_per * B);
@@ -744,8 +784,9 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
                 P.begin(s);
                 launch_fd_tiles(nb, dfd.as<FdParams>(), dtiles.as<double>(), dscr.as<double>(), s);
                 launch_fin_points(pv, nb, dfd.as<FdParams>(), dfpt.as<double>(), s);
+                if (field) launch_field_fin(pv, dpts.as<double>(), nfp, nb, dfd.as<FdParams>(), dfq.as<double>(), s);
                 P.end(KF_FD_TILES, 0.0, s);
-                g_launches += 3;
+                g_launches += 3 + field;
             }
             P.begin(s);
             launch_assemble_f64(pv, dst.as<double>(), nb, dfi.as<FreqInfo>(), dfd.as<FdParams>(), dtiles.as<double>(),
@@ -813,6 +854,15 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
                                dSC + (size_t)H * D * nb, derr.as<int32_t>(), s);
                 g_launches++;
             }
+            if (field) {  // the field points from the potentials of every panel
+                double2* fr = dSC + 2 * (size_t)H * D * nb;
+                double2* fi_ = fr + (size_t)nfp * D * nb;
+                launch_field(pv, dpts.as<double>(), nfp, dfst.as<double>(), nb, dfi.as<FreqInfo>(), dfd.as<FdParams>(),
+                             dtiles.as<double>(), dfq.as<double>(), fin, H, dheads.as<double>(), depth, opt.gravity,
+                             phi, N, du.as<double2>(), dphiI.as<double2>(), fr, fi_, fi_ + (size_t)nfp * H * nb,
+                             fi_ + 2 * (size_t)nfp * H * nb, s);
+                g_launches++;
+            }
             CUDA_OK(cudaMemcpyAsync(hout, dout.p, out_per * nb, cudaMemcpyDeviceToHost, s));
             CUDA_OK(cudaMemcpyAsync(info, dinfo.p, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, s));
             CUDA_OK(cudaMemcpyAsync(herr, derr.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -830,6 +880,8 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         const double* hFK = hX + (size_t)H * 2 * D * nb;
         const double* hSC = hFK + (size_t)H * 2 * D * nb;
         const double* hMo = hSC + (size_t)H * 2 * D * nb;
+        const double* hFr = hMo + (size_t)H * 2 * D * nb;
+        const double* hFi = hFr + (size_t)Pf * 2 * D * nb;
         if (*herr != 0) throw Failure{HB_ERR_NUMERICAL, "singular motion equation", body_index, f0};
         for (int i = 0; i < nb; i++) {
             for (int c = 0; c < G; c++)
@@ -848,6 +900,13 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
             if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
             if (motions) memcpy(pr.out.motions + fo * hx, hMo + hx * i, hx * sizeof(double));
+            if (field) {
+                const size_t pd = (size_t)nfp * 2 * D, ph = (size_t)nfp * 2 * H;
+                if (pr.out.field_radiation) memcpy(pr.out.field_radiation + fo * pd, hFr + pd * i, pd * sizeof(double));
+                double* dst3[3] = {pr.out.field_incident, pr.out.field_scattering, pr.out.field_diffraction};
+                for (int q = 0; q < 3; q++)
+                    if (dst3[q]) memcpy(dst3[q] + fo * ph, hFi + ph * ((size_t)q * nb + i), ph * sizeof(double));
+            }
         }
     }
 }

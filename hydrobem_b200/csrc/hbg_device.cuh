@@ -81,6 +81,9 @@ struct PanelsView {
     // followed by their images under each reflection of the group (image g of panel n at g Ns + n,
     // order e, then x, y, xy reflections); the statics and the system matrices have the Ns sector rows
     int G = 1;
+    // field points as the statics' rows instead of the sector's centroids: nrows points (x, y, z)
+    const double* rows = nullptr;
+    int nrows = 0;
     __device__ __forceinline__ bool invalid() const { return bad && *(volatile const int32_t*)bad != PANELS_VALID; }
     // generalized normal of rigid mode `mode` (body mode / 6: surge, sway, heave, roll, pitch, yaw about
     // its rotation centre) on panel j: zero on the panels of the other bodies

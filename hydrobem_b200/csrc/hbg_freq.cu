@@ -305,6 +305,154 @@ void launch_assemble_f64(const PanelsView& pv, const double* st, int F, const Fr
     assemble(pv, st, F, fi, fd, tiles, fpt, finite, OutF64{S, A, mat_stride, pv.N / pv.G}, s);
 }
 
+// ------------------------------------------------------------------ field points
+// The fin_point data of the panels' depths followed by those of the field points, planes of N + P per
+// frequency (green_fin.rs:937-952), so that the finite-depth pair kernel reads both with one stride.
+__global__ void k_field_fin(PanelsView pv, const double* __restrict__ pts, int P, int F,
+                            const FdParams* __restrict__ fdp, double* __restrict__ fq) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, f = blockIdx.y, N = pv.N, L = N + P;
+    if (t >= L || f >= F) return;
+    const FdParams& fd = fdp[f];
+    const double z = t < N ? pv.at(P_C + 2, t) : pts[3 * (t - N) + 2], h = fd.h, k0 = fd.k0;
+    double* o = fq + (size_t)f * FP_PLANES * L + t;
+    double d = 0, a = 0, b = 0, c = 0;
+    if (fd.mode == 0) {
+        d = exp(k0 * z);
+        a = exp(-k0 * (z + h));
+        b = exp(-k0 * (h - z));
+        c = exp(-k0 * (z + 2.0 * h));
+    }
+    o[0] = d;
+    o[(size_t)L] = a;
+    o[2 * (size_t)L] = b;
+    o[3 * (size_t)L] = c;
+    for (int n = 0; n < FIN_ROOTS; n++) {
+        double sn, cn;
+        sincos(fd.kn[n] * (z + h), &sn, &cn);
+        o[(size_t)(4 + 2 * n) * L] = cn;
+        o[(size_t)(5 + 2 * n) * L] = sn;
+    }
+}
+
+void launch_field_fin(const PanelsView& pv, const double* pts, int P, int F, const FdParams* fd, double* fq,
+                      cudaStream_t s) {
+    k_field_fin<<<dim3((pv.N + P + 127) / 128, F), 128, 0, s>>>(pv, pts, P, F, fd, fq);
+}
+
+// lo_frequency.rs:1392-1470 field_values at one point (block) of one frequency: over the panels (the
+// interior ones take no part) the influence (S, D) of panel j at the point, from the point's statics row
+// and the FP64 pair kernel; per radiation column c the sum of phi_c D - S u_c, per heading the sum of
+// (phi_S + phi_I) D; then the elevation (z = 0) or p / (rho g): radiation w^2/g (1/4 pi) sum, incident
+// (-i w / g) phi_I(x), scattered (-i w / g) (1/4 pi) sum, and their total.  The sums: per thread over
+// its panels, then warp shuffles and the warps in a fixed order (deterministic).
+constexpr int FIELD_COLS = 32;
+
+template <bool FINITE>
+__global__ void __launch_bounds__(256) k_field(PanelsView pv, const double* __restrict__ pts, int P,
+                                               const double* __restrict__ stp, const FreqInfo* __restrict__ fi,
+                                               const FdParams* __restrict__ fdp, const double* __restrict__ tiles,
+                                               const double* __restrict__ fq, int H, const double* __restrict__ heads,
+                                               double depth, double grav, const double2* __restrict__ phi, int ldphi,
+                                               const double2* __restrict__ u, const double2* __restrict__ phiI,
+                                               double2* __restrict__ frad, double2* __restrict__ finc,
+                                               double2* __restrict__ fsca, double2* __restrict__ fdif) {
+    __shared__ double2 red[8][FIELD_COLS];
+    const int p = blockIdx.x, f = blockIdx.y, N = pv.N, nrad = 6 * pv.nbod, nrhs = nrad + H;
+    const double x[3] = {pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]};
+    const FreqInfo info = fi[f];
+    const double K = info.K, logc = info.logc;
+    const size_t NP = (size_t)P * N;
+    const double2* ph = phi + (size_t)f * nrhs * ldphi;
+    const double2* uf = u + (size_t)f * nrhs * N;
+    const double2* pI = phiI + (size_t)f * H * N;
+    const double* T1 = FINITE ? tiles + (size_t)f * (T1_SIZE + T2_SIZE) : nullptr;
+    const double* fqf = FINITE ? fq + (size_t)f * FP_PLANES * (N + P) : nullptr;
+    double2 acc[FIELD_COLS];
+#pragma unroll
+    for (int c = 0; c < FIELD_COLS; c++) acc[c] = make_double2(0.0, 0.0);
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        if (pv.kind[j] != 0) continue;
+        const double cj[3] = {pv.at(P_C, j), pv.at(P_C + 1, j), pv.at(P_C + 2, j)};
+        const double dx = x[0] - cj[0], dy = x[1] - cj[1];
+        const double R = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+        const Kern w = FINITE ? finite_kernel<false>(fdp[f], T1, T1 + T1_SIZE, R, x[2], cj[2], fqf + N + p, fqf + j, N + P)
+                              : pair_kernel_inf<false>(K, R, x[2], cj[2]);
+        const size_t o = (size_t)p + (size_t)j * P;
+        double2 S, D;
+        apply_kernel(stp[o], stp[NP + o], stp[2 * NP + o], stp[3 * NP + o], pv.at(P_AREA, j), pv.at(P_N, j),
+                     pv.at(P_N + 1, j), pv.at(P_N + 2, j), 0, x, cj, K, logc, w, R, false, S, D);
+#pragma unroll
+        for (int c = 0; c < FIELD_COLS; c++) {
+            if (c >= nrhs) break;
+            double2 v = ph[(size_t)c * ldphi + j];
+            if (c < nrad) {  // phi_c D - S u_c
+                const double2 uc = uf[(size_t)c * N + j];
+                acc[c].x += v.x * D.x - v.y * D.y - (S.x * uc.x - S.y * uc.y);
+                acc[c].y += v.x * D.y + v.y * D.x - (S.x * uc.y + S.y * uc.x);
+            } else {  // (phi_S + phi_I) D on the wetted panels
+                const double2 vi = pI[(size_t)(c - nrad) * N + j];
+                v.x += vi.x;
+                v.y += vi.y;
+                acc[c].x += v.x * D.x - v.y * D.y;
+                acc[c].y += v.x * D.y + v.y * D.x;
+            }
+        }
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+    for (int c = 0; c < FIELD_COLS; c++) {
+        double a = acc[c].x, b = acc[c].y;
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if (lane == 0) red[warp][c] = make_double2(a, b);
+    }
+    __syncthreads();
+    const int c = threadIdx.x;
+    if (c >= nrhs) return;
+    double2 v = make_double2(0.0, 0.0);
+    for (int w8 = 0; w8 < (int)(blockDim.x >> 5); w8++) {
+        v.x += red[w8][c].x;
+        v.y += red[w8][c].y;
+    }
+    const double wv = info.omega, q = 1.0 / (4.0 * PI);
+    if (c < nrad) {
+        const double s = wv * wv / grav * q;
+        frad[((size_t)f * P + p) * nrad + c] = make_double2(s * v.x, s * v.y);
+        return;
+    }
+    // the incident wave at the point (low_order.rs:1441-1459), as the boundary values
+    const int h = c - nrad;
+    const double k = info.k;
+    double Z = exp(k * x[2]);
+    if (depth > 0.0) Z = (Z + exp(-k * (x[2] + 2.0 * depth))) / (1.0 + exp(-2.0 * k * depth));
+    double sb, cb;
+    sincos(heads[h], &sb, &cb);
+    double sp, cp;
+    sincos(-k * (x[0] * cb + x[1] * sb), &sp, &cp);
+    const double pir = -(grav / wv) * sp * Z, pii = (grav / wv) * cp * Z;
+    // (-i w / g) times phi_I and times phi_S = v / 4 pi
+    const double2 ei = make_double2(wv / grav * pii, -wv / grav * pir);
+    const double2 es = make_double2(wv / grav * q * v.y, -wv / grav * q * v.x);
+    const size_t oh = ((size_t)f * P + p) * H + h;
+    finc[oh] = ei;
+    fsca[oh] = es;
+    fdif[oh] = make_double2(ei.x + es.x, ei.y + es.y);
+}
+
+void launch_field(const PanelsView& pv, const double* pts, int P, const double* stp, int F, const FreqInfo* fi,
+                  const FdParams* fd, const double* tiles, const double* fq, bool finite, int H, const double* heads,
+                  double depth, double grav, const double2* phi, int ldphi, const double2* u, const double2* phiI,
+                  double2* frad, double2* finc, double2* fsca, double2* fdif, cudaStream_t s) {
+    if (finite)
+        k_field<true><<<dim3(P, F), 256, 0, s>>>(pv, pts, P, stp, fi, fd, tiles, fq, H, heads, depth, grav, phi, ldphi,
+                                                 u, phiI, frad, finc, fsca, fdif);
+    else
+        k_field<false><<<dim3(P, F), 256, 0, s>>>(pv, pts, P, stp, fi, fd, tiles, fq, H, heads, depth, grav, phi,
+                                                  ldphi, u, phiI, frad, finc, fsca, fdif);
+}
+
 // ------------------------------------------------------------------ symmetry sectors
 // Characters of the reflection group, elements e, x, y, xy reflections (lo_geometry.rs:25-36):
 // chi_c(g) = (-1)^popc(c & g) for G = 2 and 4.

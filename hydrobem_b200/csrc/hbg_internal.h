@@ -69,7 +69,7 @@ enum WsSlot {
     WS_VERTS = 0, WS_KIND, WS_PLANES, WS_BAD, WS_ST, WS_WORK, WS_NWORK, WS_S, WS_A, WS_U, WS_RHS, WS_X, WS_PHII,
     WS_IPIV, WS_INFO, WS_FI, WS_FD, WS_TILES, WS_SCR, WS_FPT, WS_HEADS, WS_OUT, WS_S32, WS_A32, WS_W, WS_P2,
     WS_P3, WS_PL, WS_PU, WS_B, WS_XM, WS_R, WS_NORMS, WS_ERR, WS_PART, WS_DINV, WS_TILES_F, WS_SG_PARAMS,
-    WS_SG_IMG, WS_SG_COUNT, WS_TRI_CTRL, WS_RS, WS_L16, WS_P3H, WS_PBODY, WS_RCEN, WS_UP, WS_PHI, WS_RIGID, WS_HYD, WS_COUNT
+    WS_SG_IMG, WS_SG_COUNT, WS_TRI_CTRL, WS_RS, WS_L16, WS_P3H, WS_PBODY, WS_RCEN, WS_UP, WS_PHI, WS_RIGID, WS_HYD, WS_FPTS, WS_FST, WS_FQ, WS_COUNT
 };
 
 // Page-locked host buffers of a solve: a device-to-host copy into pageable memory waits for the
@@ -293,6 +293,14 @@ void launch_boundary(const PanelsView& pv, int F, const FreqInfo* fi, int H, con
 // rhs[F][nrhs][N] = -S u
 void launch_rhs_f64(int N, int F, int nrhs, const double2* S, size_t mat_stride, const double2* u, double2* rhs,
                     cudaStream_t s);
+// field points: the fin-point planes of the panels then the P points ([F][FP_PLANES][N + P]); the elevation
+// or p / (rho g) at each point, radiation [F][P][D], incident, scattered and total [F][P][H]
+void launch_field_fin(const PanelsView& pv, const double* pts, int P, int F, const FdParams* fd, double* fq,
+                      cudaStream_t s);
+void launch_field(const PanelsView& pv, const double* pts, int P, const double* stp, int F, const FreqInfo* fi,
+                  const FdParams* fd, const double* tiles, const double* fq, bool finite, int H, const double* heads,
+                  double depth, double grav, const double2* phi, int ldphi, const double2* u, const double2* phiI,
+                  double2* frad, double2* finc, double2* fsca, double2* fdif, cudaStream_t s);
 // the rigid data of the motions as uploaded, per body: mass (NaN: displaced), centre of gravity (3),
 // inertia kind, inertia (9), inertia origin (3)
 constexpr int RIGID_PER_BODY = 17;

@@ -153,7 +153,8 @@ static SideStreams& side_streams() {
 
 int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgProblem& pr, const HbgOptions& opt,
                             bool fin, double depth, cudaStream_t s, double* prof, int64_t* launches, const char** msg,
-                            int64_t* freq, const std::function<void()>& start, const double* motion) {
+                            int64_t* freq, const std::function<void()>& start, const double* motion,
+                            const FieldArgs& field) {
     KernelProfiler& P = profiler();
     // N panels; with symmetry sectors G systems of Nm = N / G unknowns per frequency (one of N otherwise)
     const int N = pv.N, G = pv.G, Nm = N / G, F = (int)pr.n_omega, H = (int)pr.n_heading, D = 6 * pv.nbod,
@@ -250,7 +251,10 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     unsigned long long* sg_count = sg ? (unsigned long long*)get(WS_SG_COUNT, sizeof(unsigned long long)) : nullptr;
     double* scr = fin ? (double*)get(WS_SCR, sizeof(double) * 6912 * 3 * B) : nullptr;
     double* fpt = fin ? (double*)get(WS_FPT, sizeof(double) * FP_PLANES * N * B) : nullptr;
-    double* dout = (double*)get(WS_OUT, sizeof(double) * (2 * (size_t)D * D + 4 * (size_t)H * 2 * D) * B);
+    const int nfp = field.P;
+    double* dout = (double*)get(WS_OUT, sizeof(double) *
+                                            (2 * (size_t)D * D + 4 * (size_t)H * 2 * D + (size_t)nfp * 2 * (D + 3 * H)) * B);
+    double* fq = nfp && fin ? (double*)get(WS_FQ, sizeof(double) * FP_PLANES * (size_t)(N + nfp) * B) : nullptr;
     if (!okb) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
     last_surrogate_pairs() = 0;
     // ---- tensor maps (whole batch; the batch index is the 4th coordinate)
@@ -294,8 +298,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
     std::vector<FreqInfo> fi(B);
     std::vector<FdParams> fdh(B);
-    // per frequency: A, B [D][D], X, FK, SC, motions [H][D] complex
-    const size_t out_per = 2 * (size_t)D * D + 4 * (size_t)H * 2 * D, DD = (size_t)D * D;
+    // per frequency: A, B [D][D], X, FK, SC, motions [H][D] complex, field values [P][D] and 3 x [P][H]
+    const size_t out_per = 2 * (size_t)D * D + 4 * (size_t)H * 2 * D + (size_t)nfp * 2 * (D + 3 * H), DD = (size_t)D * D;
     // page-locked: the reads of norms, outputs and the error flag queue behind the work, no host wait
     double* hout = (double*)ws.host(HS_OUT, sizeof(double) * (out_per * B + 1));
     double* hn = (double*)ws.host(HS_NORMS, sizeof(double) * IR_MAX_IT * 2 * (size_t)BS);
@@ -480,8 +484,9 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 launch_fd_tiles(nb, dfd, tiles, scr, s);
                 launch_tiles_f32(nb, tiles, tiles_f, s);
                 launch_fin_points(pv, nb, dfd, fpt, s);
+                if (nfp) launch_field_fin(pv, field.pts, nfp, nb, dfd, fq, s);
                 P.end(KF_FD_TILES, 0.0, s);
-                *launches += 4;
+                *launches += 4 + (nfp > 0);
             }
             P.begin(s);
             if (sg)
@@ -710,6 +715,14 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                                    dSC + (size_t)H * D * nb, err, s);
                     (*launches)++;
                 }
+                if (nfp) {  // the field points from the potentials of every panel
+                    double2* fr = dSC + 2 * (size_t)H * D * nb;
+                    double2* fi_ = fr + (size_t)nfp * D * nb;
+                    launch_field(pv, field.pts, nfp, field.stp, nb, dfi, dfd, tiles, fq, fin, H, dheads, depth,
+                                 opt.gravity, G > 1 ? phi : x, G > 1 ? N : Np, u, phiI, fr, fi_, fi_ + (size_t)nfp * H * nb,
+                                 fi_ + 2 * (size_t)nfp * H * nb, s);
+                    (*launches)++;
+                }
                 cudaMemcpyAsync(hout, dout, sizeof(double) * out_per * nb, cudaMemcpyDeviceToHost, s);
                 cudaMemcpyAsync(herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
                 tf.stop();
@@ -789,6 +802,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         const double* hFK = hX + (size_t)H * 2 * D * nb;
         const double* hSC = hFK + (size_t)H * 2 * D * nb;
         const double* hMo = hSC + (size_t)H * 2 * D * nb;
+        const double* hFr = hMo + (size_t)H * 2 * D * nb;
+        const double* hFi = hFr + (size_t)nfp * 2 * D * nb;
         for (int i = 0; i < nb; i++) {
             const size_t fo = (size_t)(f0 + i), hx = (size_t)H * 2 * D;
             for (size_t q = 0; q < DD; q++)
@@ -800,6 +815,13 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
             if (motion && pr.out.motions) memcpy(pr.out.motions + fo * hx, hMo + hx * i, hx * sizeof(double));
+            if (nfp) {
+                const size_t pd = (size_t)nfp * 2 * D, ph = (size_t)nfp * 2 * H;
+                if (pr.out.field_radiation) memcpy(pr.out.field_radiation + fo * pd, hFr + pd * i, pd * sizeof(double));
+                double* dst3[3] = {pr.out.field_incident, pr.out.field_scattering, pr.out.field_diffraction};
+                for (int q = 0; q < 3; q++)
+                    if (dst3[q]) memcpy(dst3[q] + fo * ph, hFi + ph * ((size_t)q * nb + i), ph * sizeof(double));
+            }
         }
         last_ir_iterations() = it;
     }

@@ -8,15 +8,22 @@
 
 namespace hbg {
 
+// The field points of a problem on the device: P points [P][3] and their statics rows [4][P][N].
+struct FieldArgs {
+    const double* pts;
+    int P;
+    const double* stp;
+};
+
 // Solve every frequency of one body in the mixed form.  start() queues the statics st (FP64,
 // [4][N*N]) on stream s; it is called once the host-side setup (batch sizing, buffers, kernel
 // attributes) is done, before the first assembly.  motion: the motion matrices M, C, B_ext (D x D each,
-// one after the other, written by the statics stage) when the problem wants motions, else null.
-// Returns 0, or an HbStatus with the message in *msg and the frequency in *freq.
+// one after the other, written by the statics stage) when the problem wants motions, else null; field:
+// the field points (P = 0: none).  Returns 0, or an HbStatus with the message in *msg and the frequency in *freq.
 int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgProblem& pr, const HbgOptions& opt,
                             bool finite, double depth, cudaStream_t s, double* prof, int64_t* launches,
                             const char** msg, int64_t* freq, const std::function<void()>& start,
-                            const double* motion);
+                            const double* motion, const FieldArgs& field);
 
 int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* C, bool subtract, const char** msg);
 int measure_peaks(double* out, const char** msg);

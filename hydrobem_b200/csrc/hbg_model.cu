@@ -72,6 +72,8 @@ struct HbModel {
     std::string precision = "fp64";
     int64_t device = 0;
     bool motion = false;
+    bool field_pressure = false;
+    std::vector<double> field_points;  // [P][3] global
     std::vector<hbg::MeshObj> meshes;
     std::vector<hbg::BodyObj> bodies;
     std::unique_ptr<HbResults> results;
@@ -171,7 +173,7 @@ extern "C" HbStatus hb_object(HbModel* model, const char* path, uint64_t* object
         std::string p(path);
         if (p.empty()) return *object = OBJ_MODEL, HB_OK;
         if (p == "environment") return *object = OBJ_ENV, HB_OK;
-        if (p == "options") return *object = OBJ_OPTIONS, HB_OK;
+        if (p == "options" || p == "first_order") return *object = OBJ_OPTIONS, HB_OK;
         for (size_t i = 0; i < model->meshes.size(); i++)
             if (p == "meshes/" + model->meshes[i].name) return *object = OBJ_MESH0 + i, HB_OK;
         for (size_t i = 0; i < model->bodies.size(); i++)
@@ -244,6 +246,14 @@ extern "C" HbStatus hb_set_reals(HbModel* model, uint64_t object, const char* it
             for (int d = 0; d < 3; d++) dst[d] = v[d];
             if (it == "center_of_gravity") b.has_cg = true;
             if (it == "inertia_origin") b.inertia_origin = "point";
+            return HB_OK;
+        }
+        if (object == OBJ_OPTIONS && it == "field_points") {
+            if (ndim != 2 || shape[1] != 3) return refuse(HB_ERR_VALUE, "field_points have the shape (N, 3)");
+            for (size_t i = 0; i < v.size(); i++)
+                if (!std::isfinite(v[i]) || (i % 3 == 2 && v[i] > 0.0))
+                    return refuse(HB_ERR_VALUE, "field_points are finite, at z <= 0");
+            model->field_points = v;
             return HB_OK;
         }
         if (is_body(model, object) && it == "radii_of_gyration") {
@@ -326,6 +336,10 @@ extern "C" HbStatus hb_set_bool(HbModel* model, uint64_t object, const char* ite
         }
         if (object == OBJ_OPTIONS && it == "motion") {
             model->motion = value != 0;
+            return HB_OK;
+        }
+        if (object == OBJ_OPTIONS && it == "field_pressure") {
+            model->field_pressure = value != 0;
             return HB_OK;
         }
         return refuse(HB_ERR_UNSUPPORTED, "the item \"" + it + "\" of this object is not on this route");
@@ -501,6 +515,13 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         const size_t F = omegas.size(), H = heads.size(), NB = centers.size() / 3, D = 6 * NB;
         std::vector<double> A(F * D * D), B(F * D * D), X(F * H * D * 2), FK(F * H * D * 2), SC(F * H * D * 2),
             MO(F * H * D * 2), HS(NB * HBG_HS);
+        std::vector<double> fpts;
+        {
+            std::lock_guard<std::mutex> g(model->lock);
+            if (model->field_pressure) fpts = model->field_points;
+        }
+        const size_t NP = fpts.size() / 3;
+        std::vector<double> FR(F * NP * D * 2), FI(F * NP * H * 2), FS(F * NP * H * 2), FDF(F * NP * H * 2);
         const bool want_motion = model->motion && H > 0;
         HbgRigid rig{rmass.data(), rcg.data(), rkind.data(), rinertia.data(), rorigin.data(), nullptr, nullptr};
         HbgProblem pr{};
@@ -517,7 +538,10 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         pr.headings_deg = heads.data();
         pr.n_heading = (int64_t)H;
         pr.out = HbgOutputs{A.data(), B.data(), X.data(), FK.data(), SC.data(), want_motion ? MO.data() : nullptr,
-                            HS.data()};
+                            HS.data(), NP ? FR.data() : nullptr, NP ? FI.data() : nullptr, NP ? FS.data() : nullptr,
+                            NP ? FDF.data() : nullptr};
+        pr.field_points = NP ? fpts.data() : nullptr;
+        pr.n_field_points = (int64_t)NP;
         if (progress) {
             HbProgress pg{};
             pg.stage = 0;
@@ -560,6 +584,21 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         add_quantity(r.get(), "excitation_diffraction_f64", HB_C128, {F, H, D}, X.data(), X.size() * 8);
         add_quantity(r.get(), "excitation_froude_krylov_f64", HB_C128, {F, H, D}, FK.data(), FK.size() * 8);
         add_quantity(r.get(), "excitation_scattering_f64", HB_C128, {F, H, D}, SC.data(), SC.size() * 8);
+        if (NP) {  // quantities.rs:58-62: the points, then the elevation or p / (rho g) per column and heading
+            add_quantity(r.get(), "field_points", HB_F64, {NP, 3}, fpts.data(), fpts.size() * 8);
+            const std::pair<const char*, std::vector<double>*> fq[4] = {{"field_points_pressure_radiation", &FR},
+                                                                        {"field_points_pressure_incident", &FI},
+                                                                        {"field_points_pressure_scattering", &FS},
+                                                                        {"field_points_pressure_diffraction", &FDF}};
+            for (int q = 0; q < 4; q++) {
+                std::vector<double>& v = *fq[q].second;
+                std::vector<float> v32(v.size());
+                for (size_t i = 0; i < v.size(); i++) v32[i] = (float)v[i];
+                const size_t cols = q == 0 ? D : H;
+                add_quantity(r.get(), fq[q].first, HB_C64, {F, NP, cols}, v32.data(), v32.size() * 4);
+                add_quantity(r.get(), std::string(fq[q].first) + "_f64", HB_C128, {F, NP, cols}, v.data(), v.size() * 8);
+            }
+        }
         if (want_motion) {
             std::vector<float> m32(F * H * D * 2);
             for (size_t i = 0; i < m32.size(); i++) m32[i] = (float)MO[i];

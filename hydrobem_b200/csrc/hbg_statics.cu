@@ -399,20 +399,23 @@ __device__ inline double log_in_plane(const PanelRegs& p, const double* x) {
 }
 
 // One (row k, panel j) pair: rs, rd and (unless adaptive) dl, dd.  lo_static.rs:59-119
-// Four planes of Nr x N (rows k < Nr = N / G, the sector's points; every panel j), entry at k + j Nr.
+// Four planes of Nr x N (rows k < Nr = N / G, the sector's points, or the Nr field points; every panel
+// j), entry at k + j Nr.
 // MIXED: the mixed form's variant (far Rankine points and the order-4 log rule in FP32, above); the
 // FP64 form runs the reference's arithmetic to the bit.
 template <bool MIXED>
 __global__ void __launch_bounds__(256) k_statics(PanelsView pv, double depth, int logint, double tol,
                                                  double* __restrict__ st, int32_t* __restrict__ work,
                                                  int32_t* __restrict__ nwork, int work_cap) {
-    const int N = pv.N, Nr = N / pv.G;  // rows: the sector's panels; columns: all panels
+    // rows: the sector's panels (or the field points); columns: all panels
+    const int N = pv.N, Nr = pv.rows ? pv.nrows : N / pv.G;
     int k = blockIdx.x * 32 + threadIdx.x;
     int j = blockIdx.y * 8 + threadIdx.y;
     if (k >= Nr || j >= N) return;
     PanelRegs p;
     load_panel(pv, j, p);
-    double x[3] = {pv.at(P_C + 0, k), pv.at(P_C + 1, k), pv.at(P_C + 2, k)};
+    double x[3];
+    for (int d = 0; d < 3; d++) x[d] = pv.rows ? pv.rows[3 * k + d] : pv.at(P_C + d, k);
     double xb[3] = {x[0], x[1], -x[2]};
     double s0, d0, sb, db;
     rankine_at<MIXED>(pv, j, p, x, s0, d0);
@@ -508,7 +511,9 @@ __device__ void adaptive_pair(const PanelsView& pv, const int32_t* __restrict__ 
     const int k = work[2 * t], j = work[2 * t + 1];
     PanelRegs p;
     load_panel(pv, j, p);
-    double xb[3] = {pv.at(P_C + 0, k), pv.at(P_C + 1, k), -pv.at(P_C + 2, k)};
+    double xb[3];
+    for (int d = 0; d < 3; d++) xb[d] = pv.rows ? pv.rows[3 * k + d] : pv.at(P_C + d, k);
+    xb[2] = -xb[2];
     double m[4][3];
     panel_map(p, m);
     double tt[3] = {xb[0] - p.c[0], xb[1] - p.c[1], xb[2] - p.c[2]};
@@ -571,7 +576,7 @@ __device__ void adaptive_pair(const PanelsView& pv, const int32_t* __restrict__ 
     if (lane == 0) {
         double psi, dpsi;
         psi_terms(p.c, xb, p.n, psi, dpsi);
-        const int Nr = N / pv.G;
+        const int Nr = pv.rows ? pv.nrows : N / pv.G;
         size_t NN = (size_t)Nr * N, o = (size_t)k + (size_t)j * Nr;
         st[2 * NN + o] = acc0 - p.area * psi;
         st[3 * NN + o] = acc1 - p.area * dpsi;
@@ -617,7 +622,7 @@ void launch_panel_geometry(int N, const double* verts, const int32_t* kind, doub
 
 void launch_statics(const PanelsView& pv, double depth, int logint, double tol, double* st, int32_t* work,
                     int32_t* nwork, int work_cap, cudaStream_t s, bool mixed) {
-    dim3 grid((pv.N / pv.G + 31) / 32, (pv.N + 7) / 8);
+    dim3 grid(((pv.rows ? pv.nrows : pv.N / pv.G) + 31) / 32, (pv.N + 7) / 8);
     if (mixed)
         k_statics<true><<<grid, dim3(32, 8), 0, s>>>(pv, depth, logint, tol, st, work, nwork, work_cap);
     else

@@ -38,7 +38,8 @@ SYM_NONE, SYM_YZ, SYM_XZ, SYM_BOTH = 0, 1, 2, 3
 
 class HbgOutputs(ctypes.Structure):
     _fields_ = [("added_mass", dp), ("radiation_damping", dp), ("excitation", dp), ("froude_krylov", dp),
-                ("scattering", dp), ("motions", dp), ("hydrostatics", dp)]
+                ("scattering", dp), ("motions", dp), ("hydrostatics", dp), ("field_radiation", dp),
+                ("field_incident", dp), ("field_scattering", dp), ("field_diffraction", dp)]
 
 
 class HbgRigid(ctypes.Structure):
@@ -48,7 +49,8 @@ class HbgRigid(ctypes.Structure):
 
 class HbgProblem(ctypes.Structure):
     _fields_ = [("body", HbgBody), ("omegas", dp), ("n_omega", ctypes.c_int64), ("headings_deg", dp),
-                ("n_heading", ctypes.c_int64), ("out", HbgOutputs), ("rigid", ctypes.POINTER(HbgRigid))]
+                ("n_heading", ctypes.c_int64), ("out", HbgOutputs), ("rigid", ctypes.POINTER(HbgRigid)),
+                ("field_points", dp), ("n_field_points", ctypes.c_int64)]
 
 
 # HbgRigid.inertia_kind, and the record of HbgOutputs.hydrostatics (HBG_HS doubles per body)
@@ -172,10 +174,11 @@ class Body:
     symmetry (SYM_YZ, SYM_XZ, SYM_BOTH) the panels are one sector of a body mirrored in those planes.
     rigid: the mass properties for the motions, a dict of mass [n_bodies] (NaN: displaced),
     center_of_gravity [n_bodies][3], inertia [n_bodies][3][3] about inertia_origin [n_bodies][3],
-    inertia_kind [n_bodies] (INERTIA_COMPONENTS / INERTIA_GYRATION), optional stiffness, damping [D][D]."""
+    inertia_kind [n_bodies] (INERTIA_COMPONENTS / INERTIA_GYRATION), optional stiffness, damping [D][D].
+    points: field points [P][3] (global, z <= 0) for the elevation or p / (rho g) there."""
 
     def __init__(self, vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None,
-                 symmetry=SYM_NONE, rigid=None):
+                 symmetry=SYM_NONE, rigid=None, points=None):
         self.symmetry = int(symmetry)
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 4, 3)
         self.kinds = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
@@ -194,6 +197,12 @@ class Body:
         self.FK = np.zeros((F, H, D), dtype=np.complex128)
         self.SC = np.zeros((F, H, D), dtype=np.complex128)
         self.HS = np.zeros((self.n_bodies, HBG_HS))
+        self.points = None if points is None else np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
+        P = 0 if self.points is None else self.points.shape[0]
+        self.FR = np.zeros((F, P, D), dtype=np.complex128)
+        self.FI = np.zeros((F, P, H), dtype=np.complex128)
+        self.FS = np.zeros((F, P, H), dtype=np.complex128)
+        self.FD = np.zeros((F, P, H), dtype=np.complex128)
         self.MO = np.zeros((F, H, D), dtype=np.complex128) if rigid is not None else None
         self._rigid = None
         if rigid is not None:
@@ -232,6 +241,13 @@ class Body:
         p.out.motions = None if self.MO is None else self.MO.ctypes.data_as(dp)
         p.out.hydrostatics = self.HS.ctypes.data_as(dp)
         p.rigid = None if self._rigid is None else ctypes.pointer(self._rigid)
+        if self.points is not None and self.points.shape[0]:
+            p.field_points = self.points.ctypes.data_as(dp)
+            p.n_field_points = self.points.shape[0]
+            p.out.field_radiation = self.FR.ctypes.data_as(dp)
+            p.out.field_incident = self.FI.ctypes.data_as(dp)
+            p.out.field_scattering = self.FS.ctypes.data_as(dp)
+            p.out.field_diffraction = self.FD.ctypes.data_as(dp)
         return p
 
     def results(self):
@@ -239,6 +255,9 @@ class Body:
                "hydrostatics": [hydrostatics_record(h) for h in self.HS]}
         if self.MO is not None:
             out["motions"] = self.MO
+        if self.points is not None:
+            out.update({"field_radiation": self.FR, "field_incident": self.FI, "field_scattering": self.FS,
+                        "field_diffraction": self.FD})
         return out
 
 
@@ -251,11 +270,12 @@ def solve_batch(bodies, **options):
 
 
 def solve(vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None,
-          symmetry=SYM_NONE, rigid=None, **options):
+          symmetry=SYM_NONE, rigid=None, points=None, **options):
     """One problem through the GPU path: dict of A, B [F][D][D], X, FK, SC [F][H][D], D = 6 per body, the
-    hydrostatics records of the bodies, and with rigid the motions [F][H][D]."""
-    return solve_batch([Body(vertices, omegas, headings_deg, kinds, panel_body, rotation_centers, symmetry, rigid)],
-                       **options)[0]
+    hydrostatics records of the bodies, with rigid the motions [F][H][D], with points the field values
+    field_radiation [F][P][D] and field_incident, field_scattering, field_diffraction [F][P][H]."""
+    return solve_batch([Body(vertices, omegas, headings_deg, kinds, panel_body, rotation_centers, symmetry, rigid,
+                             points)], **options)[0]
 
 
 def last_profile():

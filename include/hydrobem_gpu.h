@@ -50,7 +50,7 @@ typedef int32_t HbStatus;
 #define HB_C128 7
 
 /* The version of this library's ABI (its own numbering; the reference's hb_abi_version is 8). */
-#define HBG_ABI_VERSION 5
+#define HBG_ABI_VERSION 6
 
 /* ==================================================================== batched entry */
 
@@ -125,7 +125,12 @@ typedef struct HbgRigid {
  *   added_mass, radiation_damping  [n_omega][D][D]   (coordinate i, radiation mode j)
  *   excitation, froude_krylov, scattering, motions  [n_omega][n_heading][D][2]  (re, im)
  *   hydrostatics  [n_bodies][HBG_HS]
- * motions needs the problem's rigid data. */
+ *   field_radiation  [n_omega][n_field_points][D][2]: the elevation (z = 0) or p / (rho g) per unit
+ *                    displacement of each radiation mode
+ *   field_incident, field_scattering, field_diffraction  [n_omega][n_field_points][n_heading][2]: the
+ *                    incident, scattered and total waves there, per unit wave amplitude
+ *                    (lo_frequency.rs:1392-1470)
+ * motions needs the problem's rigid data, the field outputs its field points. */
 typedef struct HbgOutputs {
     double *added_mass;
     double *radiation_damping;
@@ -134,6 +139,10 @@ typedef struct HbgOutputs {
     double *scattering;
     double *motions;
     double *hydrostatics;
+    double *field_radiation;
+    double *field_incident;
+    double *field_scattering;
+    double *field_diffraction;
 } HbgOutputs;
 
 typedef struct HbgProblem {
@@ -143,7 +152,9 @@ typedef struct HbgProblem {
     const double *headings_deg;
     int64_t n_heading;
     HbgOutputs out;
-    const HbgRigid *rigid; /* NULL: no motions */
+    const HbgRigid *rigid;       /* NULL: no motions */
+    const double *field_points;  /* [n_field_points][3], global, in the fluid at z <= 0; NULL: none */
+    int64_t n_field_points;
 } HbgProblem;
 
 typedef struct HbgOptions {

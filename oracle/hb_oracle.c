@@ -1273,3 +1273,51 @@ int hbo_assemble(int N, const hbo_panel *pg, const int32_t *kind, const double *
     free(fpt);
     return 0;
 }
+
+/* lo_frequency.rs:1392-1470 field_values, the influence rows of the field points: (S, D column) of every
+ * panel j at every point x_p (the static row of the point, lo_static.rs:59-119, then the pair kernel and
+ * apply_kernel as for a collocation point); S, D [P][N] complex as (re, im) pairs. */
+int hbo_field_influence(int N, const hbo_panel *pg, const int32_t *kind, int P, const double *pts, double depth,
+                        double omega, double grav, int logint, double tol, double *S, double *D) {
+    gl_init();
+    double K = omega * omega / grav;
+    double logc = logint ? 1.0 : 0.0;
+    int finite = isfinite(depth) && depth > 0.0;
+    fdepth *fd = NULL;
+    finpoint *fpt = NULL;
+    if (finite) {
+        fd = (fdepth *)malloc(sizeof(fdepth));
+        make_finite_depth(fd, depth, K, 0);
+        fpt = (finpoint *)malloc(sizeof(finpoint) * N);
+        for (int j = 0; j < N; j++) fin_point(fd, pg[j].c[2], fpt + j);
+    }
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int p = 0; p < P; p++) {
+        const double *x = pts + 3 * p;
+        double *row = (double *)malloc(sizeof(double) * 4 * N);
+        static_row(N, pg, kind, x, logint, tol, depth, row);
+        finpoint fx;
+        if (finite) fin_point(fd, x[2], &fx);
+        for (int j = 0; j < N; j++) {
+            double w[8], R;
+            if (finite) {
+                double dx = x[0] - pg[j].c[0], dy = x[1] - pg[j].c[1];
+                R = sqrt(dx * dx + dy * dy);
+                finite_kernel(fd, R, x[2], pg[j].c[2], &fx, fpt + j, w);
+            } else {
+                pair_kernel_inf(K, x, pg[j].c, w, &R);
+            }
+            double s[2], d[2];
+            apply_kernel(pg + j, kind ? kind[j] : HBO_WET, row + 4 * (size_t)j, x, K, logc, w, R, 0, s, d);
+            size_t o = (size_t)p * N + j;
+            S[2 * o] = s[0];
+            S[2 * o + 1] = s[1];
+            D[2 * o] = d[0];
+            D[2 * o + 1] = d[1];
+        }
+        free(row);
+    }
+    free(fd);
+    free(fpt);
+    return 0;
+}

@@ -61,6 +61,10 @@ int hbo_statics(int N, const hbo_panel *pg, const int32_t *kind, double depth, i
 int hbo_assemble(int N, const hbo_panel *pg, const int32_t *kind, const double *statics, double depth,
                  double omega, double grav, int logint, double *S, double *A);
 
+/* the influence rows of P field points: (S, D column) of every panel at every point, [P][N] complex */
+int hbo_field_influence(int N, const hbo_panel *pg, const int32_t *kind, int P, const double *pts, double depth,
+                        double omega, double grav, int logint, double tol, double *S, double *D);
+
 /* wave number of the incident wave: K for infinite depth, dispersion_x0(K h)/h otherwise */
 double hbo_wavenumber(double omega, double depth, double grav);
 

@@ -9,6 +9,8 @@ and adds, in numpy, the steps that are short formulas of ``crates/hydrobem/src/`
 - right-hand sides -S u and the dense solve  ``lo_frequency.rs:823-955`` (LU with partial pivoting:
   LAPACK ``zgesv`` through numpy, standing in for faer's blocked LU, ``linalg.rs:134-252``)
 - pressure integration A, B, X, FK, SC  ``lo_frequency.rs:1039-1115``
+- field points: the elevation or p / (rho g) of the radiation, incident, scattered and total waves at
+  points in the fluid by Green's identity over the panels  ``lo_frequency.rs:1392-1470``
 - hydrostatics, rigid inertia and the motion equation of each frequency  ``hydrostatics.rs:116-356``,
   ``motion.rs:121-158``
 - symmetry sectors (a body given as one sector of its mirror-symmetric mesh): the matrices of the
@@ -89,6 +91,8 @@ def lib():
                                ctypes.c_int, dp, dp]
     L.hbo_wavenumber.argtypes = [ctypes.c_double] * 3
     L.hbo_wavenumber.restype = ctypes.c_double
+    L.hbo_field_influence.argtypes = [ctypes.c_int, pp, ip, ctypes.c_int, dp, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, dp]
     rc = L.hbo_load_tables(str(TABLES).encode())
     if rc != 0:
         raise RuntimeError(f"oracle: cannot load the Green-function tables {TABLES} (code {rc})")
@@ -262,7 +266,7 @@ def sector_solve(S, A, u, G):
 
 
 def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY, rho=DENSITY, logint=True,
-                    want_matrices=False, panel_body=None, centers=None, sectors=1):
+                    want_matrices=False, panel_body=None, centers=None, sectors=1, points=None, tol=1e-4):
     """A, B [D][D], X, FK, SC [H][D] of one frequency (D = 6 per body), all in float64 (complex128).
     sectors > 1: the panels are a mirrored mesh (mirror_sector) solved by its symmetry sectors."""
     c, n, area = panel_arrays(panels)
@@ -293,9 +297,50 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
         out["X"] = (iwr * x).T
         out["FK"] = (iwr * fk).T
         out["SC"] = (iwr * (x - fk)).T
+    if points is not None and len(points):
+        out.update(field_values(panels, kinds, points, depth, omega, headings_rad, phi, u, phiI, D, grav, logint, tol))
     if want_matrices:
         out["S"], out["Amat"], out["rhs"], out["phi"] = S, A, rhs, phi
     return out
+
+
+# ------------------------------------------------------------------ field points
+def field_influence(panels, kinds, pts, depth, omega, grav=GRAVITY, logint=True, tol=1e-4):
+    """(S, D) [P][N] complex128: the influence of every panel at every field point."""
+    n = len(panels)
+    p = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 3)
+    S = np.zeros((len(p), n), dtype=np.complex128)
+    D = np.zeros((len(p), n), dtype=np.complex128)
+    k = np.zeros(n, np.int32) if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
+    d = depth if (depth is not None and np.isfinite(depth) and depth > 0) else np.inf
+    lib().hbo_field_influence(n, panels, _ip(k), len(p), _dp(p), d, omega, grav, int(logint), tol,
+                              S.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                              D.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return S, D
+
+
+def field_values(panels, kinds, pts, depth, omega, heads_rad, phi, u, phiI, nrad, grav=GRAVITY, logint=True,
+                 tol=1e-4):
+    """lo_frequency.rs:1392-1470: at each point the elevation (z = 0) or p / (rho g): radiation
+    w^2/g (1/4 pi) sum_j (phi_c D - S u_c) [P][nrad]; per heading the incident wave (-i w / g) phi_I, the
+    scattered (-i w / g) (1/4 pi) sum_j (phi_S + phi_I) D (phi_I on the wetted panels) and their sum
+    [P][H]; the interior panels take no part.  phi, u [N][nrhs], phiI [H][N]."""
+    S, D = field_influence(panels, kinds, pts, depth, omega, grav, logint, tol)
+    interior = np.zeros(len(panels), bool) if kinds is None else np.asarray(kinds) != WET
+    S[:, interior] = 0.0
+    D[:, interior] = 0.0
+    frad = (omega * omega / grav) * (D @ phi[:, :nrad] - S @ u[:, :nrad]) / (4.0 * np.pi)
+    H = len(heads_rad)
+    p = np.asarray(pts, dtype=np.float64).reshape(-1, 3)
+    k = lib().hbo_wavenumber(omega, depth if depth else np.inf, grav)
+    finc = np.zeros((len(p), H), dtype=np.complex128)
+    fsca = np.zeros_like(finc)
+    for h, beta in enumerate(heads_rad):
+        pI, _ = incident(p, depth, k, omega, beta, grav)
+        v = D @ (phi[:, nrad + h] + np.where(interior, 0.0, phiI[h]))
+        finc[:, h] = pI * (-1j * omega / grav)
+        fsca[:, h] = v / (4.0 * np.pi) * (-1j * omega / grav)
+    return {"field_radiation": frad, "field_incident": finc, "field_scattering": fsca, "field_diffraction": finc + fsca}
 
 
 # ------------------------------------------------------------------ hydrostatics and motions
@@ -374,7 +419,7 @@ def motions(A, B, X, omega, M, C, Bx):
 
 
 def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GRAVITY, rho=DENSITY, logint=True,
-               tol=1e-4, panel_body=None, centers=None, symmetry=SYM_NONE, rigid=None):
+               tol=1e-4, panel_body=None, centers=None, symmetry=SYM_NONE, rigid=None, points=None):
     """The whole path for one problem: statics once, then every frequency. Arrays [F][D][D], [F][H][D]
     (D = 6 per body; interacting bodies by panel_body and their rotation centers).  With symmetry the
     panels (and kinds, panel_body) are one sector: mirrored, then solved by sectors."""
@@ -387,7 +432,7 @@ def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GR
     st = statics(panels, kinds, depth, logint, tol)
     heads = np.radians(np.asarray(headings_deg, dtype=float))
     res = [solve_frequency(panels, kinds, st, depth, w, heads, grav, rho, logint, panel_body=panel_body,
-                           centers=centers, sectors=G) for w in omegas]
+                           centers=centers, sectors=G, points=points, tol=tol) for w in omegas]
     out = {k: np.array([r[k] for r in res]) for k in res[0]}
     c, n, area = panel_arrays(panels)
     recs, M, C, Bx = hydrostatics(c, n, area, kinds, panel_body, centers, rho, grav, rigid)

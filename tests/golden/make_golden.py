@@ -12,6 +12,9 @@ Every fixture is a compressed .npz of numbers the reference's test suite holds o
 - lo_cylinder_drift.npz  the reference solver's own outputs of that regression problem
   (tests/data/regression/lo_cylinder_drift.npz: A, B, X, FK, SC, the motions (RAO) and the
   hydrostatics of a floating cylinder with its mass and inertia, f32 / f64 as the reference stores them)
+- lo_cylinder_field.npz  the reference solver's own field-point outputs of its regression problem
+  lo_cylinder_field_body_points (the same cylinder held fixed, three points: the elevation at z = 0
+  and p / (rho g) below, per radiation column and heading, complex64)
 - meshes.npz         SHA-256 digests and small copies of the reference's procedural meshes
   (tests/python/meshes.py imported from the reference) for the configs' bodies
 """
@@ -63,6 +66,10 @@ def main(argv):
             "hydrostatics_stiffness", "hydrostatics_mass", "hydrostatics_center_of_gravity",
             "hydrostatics_metacentric_height"]
     np.savez_compressed(HERE / "lo_cylinder_drift.npz", **{k: d[k] for k in keep})
+    d = np.load(data / "regression" / "lo_cylinder_field_body_points.npz")
+    keep = ["omegas", "headings", "field_points", "field_points_pressure_radiation", "field_points_pressure_incident",
+            "field_points_pressure_scattering", "field_points_pressure_diffraction"]
+    np.savez_compressed(HERE / "lo_cylinder_field.npz", **{k: d[k] for k in keep})
     sys.path.insert(0, str(root / "tests" / "python"))
     import meshes  # the reference's procedural meshes (numpy only)
 
