@@ -7,5 +7,6 @@
 #include "hbg_peaks.cu"
 #include "hbg_surrogate.cu"
 #include "hbg_api.cu"
+#include "hbg_gdf.cu"
 #include "hbg_model.cu"
 #include "hbg_noalloc.cu"

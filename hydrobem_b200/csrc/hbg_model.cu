@@ -209,6 +209,38 @@ extern "C" HbStatus hb_add(HbModel* model, uint64_t parent, const char* list, co
     });
 }
 
+// hydrobem.h:879-886 hb_model_load_mesh for a low-order GDF file: a new mesh of the model with its panels
+// and the symmetry planes of its ISX / ISY flags (x = 0: yz, y = 0: xz); ULEN and GRAV stay in the file
+// (the environment keeps its own gravity).  Higher-order files and the SPL / discretization options of the
+// reference are not on this route.
+extern "C" HbStatus hb_model_load_mesh(HbModel* model, const char* name, const char* path, const HbMeshOptions* options,
+                                       uint64_t* out) {
+    return guard([&]() -> HbStatus {
+        if (!model || !name || !path || !out) return refuse(HB_ERR_ARGUMENT, "null argument");
+        if (options && (options->higher_order || options->spl_path || options->discretization ||
+                        options->panel_size > 0.0))
+            return refuse(HB_ERR_UNSUPPORTED, "higher-order meshes are not on this route");
+        std::string label;
+        double ulen = 0.0, grav = 0.0;
+        int isx = 0, isy = 0;
+        std::vector<double> v;
+        read_gdf(path, options && options->zero_trailer, label, ulen, grav, isx, isy, v);
+        for (double x : v)
+            if (!std::isfinite(x)) return refuse(HB_ERR_VALUE, std::string(path) + ": non-finite vertex coordinate");
+        std::lock_guard<std::mutex> g(model->lock);
+        const std::string n(name);
+        if (n.empty()) return refuse(HB_ERR_VALUE, "a mesh needs a name");
+        for (auto& m : model->meshes)
+            if (m.name == n) return refuse(HB_ERR_VALUE, "a mesh of that name exists");
+        MeshObj m{n};
+        m.vertices.swap(v);
+        m.symmetry = isx && isy ? "xz_and_yz" : isx ? "yz" : isy ? "xz" : "none";
+        model->meshes.push_back(std::move(m));
+        *out = OBJ_MESH0 + model->meshes.size() - 1;
+        return HB_OK;
+    });
+}
+
 extern "C" HbStatus hb_set_reals(HbModel* model, uint64_t object, const char* item, const double* data,
                                  const size_t* shape, size_t ndim) {
     return guard([&]() -> HbStatus {

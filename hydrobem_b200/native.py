@@ -261,6 +261,23 @@ class Body:
         return out
 
 
+class HbgGdf(ctypes.Structure):
+    _fields_ = [("label", ctypes.c_char * 256), ("ulen", ctypes.c_double), ("gravity", ctypes.c_double),
+                ("isx", ctypes.c_int32), ("isy", ctypes.c_int32), ("n_panels", ctypes.c_int64), ("vertices", dp)]
+
+
+def read_gdf(path, zero_trailer=False):
+    """A low-order GDF file through hbg_read_gdf: dict of label, ulen, gravity, isx, isy and vertices [P][4][3]."""
+    g = HbgGdf()
+    L = lib()
+    check(L.hbg_read_gdf(str(path).encode(), int(bool(zero_trailer)), ctypes.byref(g)))
+    try:
+        v = np.ctypeslib.as_array(g.vertices, shape=(g.n_panels * 12,)).copy().reshape(-1, 4, 3)
+    finally:
+        L.hbg_gdf_free(ctypes.byref(g))
+    return {"label": g.label.decode(), "ulen": g.ulen, "gravity": g.gravity, "isx": g.isx, "isy": g.isy, "vertices": v}
+
+
 def solve_batch(bodies, **options):
     """Solve a list of Body on the GPU through hbg_solve_batch; returns the list of result dicts."""
     arr = (HbgProblem * len(bodies))(*[b.problem() for b in bodies])

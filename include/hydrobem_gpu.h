@@ -202,6 +202,41 @@ HbStatus hbg_release_workspace(void);
 /* The kernels launched by the last hbg_solve_batch of this thread. */
 HbStatus hbg_last_launch_count(int64_t *count);
 
+/* ---- mesh files */
+
+/* A low-order GDF file as read (crates/hydrobem/src/gdf.rs:511-535): the label line, ULEN, GRAV, the symmetry
+ * flags ISX (x = 0 a plane of symmetry) and ISY (y = 0), and n_panels panels of 4 vertices, vertices
+ * [n_panels][4][3] owned by the library until hbg_gdf_free. */
+typedef struct HbgGdf {
+    char label[256];
+    double ulen;
+    double gravity;
+    int32_t isx;
+    int32_t isy;
+    int64_t n_panels;
+    double *vertices;
+} HbgGdf;
+
+/* Reads a low-order GDF file: Fortran list-directed records (free format, commas as spaces, D exponents,
+ * text after a line's numbers a comment); a trailing record of zeros only with zero_trailer.  HB_ERR_IO
+ * when the file cannot be read, HB_ERR_VALUE with the reason for a malformed one. */
+HbStatus hbg_read_gdf(const char *path, int32_t zero_trailer, HbgGdf *out);
+HbStatus hbg_gdf_free(HbgGdf *gdf);
+
+/* The reference's options of hb_model_load_mesh (hydrobem.h:835-852); on this route only zero_trailer is
+ * read, a higher-order file is HB_ERR_UNSUPPORTED. */
+typedef struct HbMeshOptions {
+    int32_t higher_order;
+    int32_t zero_trailer;
+    const char *spl_path;
+    const int32_t *discretization;
+    size_t discretization_rows;
+    double panel_size;
+    int32_t spline_order;
+    int32_t outer_quadrature;
+    int32_t inner_quadrature;
+} HbMeshOptions;
+
 /* Test support: the static influence data (planes rs, rd, dl, dd; entry (k, j) at k + j N of each
  * plane, N*N doubles per plane) and the matrices S and A = 2 pi I - D (column-major complex128,
  * N*N (re, im) pairs) of one body at one frequency, FP64 form.  Any output pointer may be NULL.
@@ -288,6 +323,11 @@ HbStatus hbg_statics_noalloc(const double *d_vertices, const int32_t *d_kinds, i
 /* ==================================================================== reference ABI subset */
 
 typedef struct HbModel HbModel;
+
+/* A mesh of the model read from a low-order GDF file (hydrobem.h:879-886): its panels and the symmetry
+ * planes of ISX / ISY; `out` the new mesh object. */
+HbStatus hb_model_load_mesh(HbModel *model, const char *name, const char *path, const HbMeshOptions *options,
+                            uint64_t *out);
 typedef struct HbResults HbResults;
 
 typedef struct HbLocation {
