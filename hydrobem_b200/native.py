@@ -90,7 +90,8 @@ EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_
            "hb_object", "hb_add", "hb_set_bool", "hb_set_int", "hb_set_real", "hb_set_text", "hb_set_reals",
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
            "hbg_statics_noalloc", "hbg_measure_peaks", "hbg_last_ir_history", "hbg_surrogate_train",
-           "hbg_surrogate_grad", "hbg_surrogate_eval", "hbg_last_surrogate_pairs"]
+           "hbg_surrogate_grad", "hbg_surrogate_eval", "hbg_last_surrogate_pairs", "hbg_read_gdf", "hbg_gdf_free",
+           "hb_model_load_mesh"]
 
 _lib = None
 
