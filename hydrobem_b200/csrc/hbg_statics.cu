@@ -404,7 +404,7 @@ __device__ inline double log_in_plane(const PanelRegs& p, const double* x) {
 // MIXED: the mixed form's variant (far Rankine points and the order-4 log rule in FP32, above); the
 // FP64 form runs the reference's arithmetic to the bit.
 template <bool MIXED>
-__global__ void __launch_bounds__(256) k_statics(PanelsView pv, double depth, int logint, double tol,
+__global__ void __launch_bounds__(256, 2) k_statics(PanelsView pv, double depth, int logint, double tol,
                                                  double* __restrict__ st, int32_t* __restrict__ work,
                                                  int32_t* __restrict__ nwork, int work_cap) {
     // rows: the sector's panels (or the field points); columns: all panels
