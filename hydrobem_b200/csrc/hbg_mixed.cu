@@ -504,7 +504,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             P.begin(s);
             launch_boundary(pv, nb, dfi, H, dheads, depth, opt.gravity, u, phiI, s);
             P.end(KF_BOUNDARY, 0.0, s);
-            *launches += 1 + (Np > Nm);
+            *launches += 2 + (Np > Nm);  // the assembly, the boundary values, the identity padding
             t.stop();
         }
         // ---- LU of M = A^T without pivoting, blocked by NBL, the products on the tensor cores
