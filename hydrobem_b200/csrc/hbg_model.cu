@@ -141,6 +141,43 @@ static std::vector<double> expand(const MeshObj& m) {
     return out;
 }
 
+// interior.rs:79-138 projected: the interior free surface as the vertical projection onto z = z0 (the free
+// surface in body coordinates) of the downward-facing wetted panels, vertex order reversed so that the
+// projected panels face up; panels lying in z0 (a zero-draft part) and vertical ones (|n_z| <= 1e-6) are
+// skipped; an upward-facing panel makes the projection multi-valued.  The normal is the panel's: the unit
+// cross product of its diagonals (geometry.rs:160-165).  why: the reason when the surface cannot be made.
+static std::vector<double> projected_lid(const std::vector<double>& v, double z0, std::string& why) {
+    constexpr double SLOPE = 1e-6, PLANE_TOL = 1e-6;
+    const size_t P = v.size() / 12;
+    double ext = 1.0;
+    for (double x : v) ext = std::max(ext, std::fabs(x));
+    const double tol = PLANE_TOL * ext;
+    std::vector<double> out;
+    for (size_t p = 0; p < P; p++) {
+        const double* q = &v[12 * p];
+        bool flat = true;
+        for (int i = 0; i < 4; i++) flat = flat && std::fabs(q[3 * i + 2] - z0) <= tol;
+        if (flat) continue;
+        const double d1[3] = {q[6] - q[0], q[7] - q[1], q[8] - q[2]}, d2[3] = {q[9] - q[3], q[10] - q[4], q[11] - q[5]};
+        const double n[3] = {d1[1] * d2[2] - d1[2] * d2[1], d1[2] * d2[0] - d1[0] * d2[2], d1[0] * d2[1] - d1[1] * d2[0]};
+        const double nn = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        const double nz = nn > 0.0 ? n[2] / nn : 0.0;
+        if (nz > SLOPE) {
+            why = "wetted element " + std::to_string(p + 1) +
+                  " faces upward, so the vertical projection of the wetted surface is multi-valued";
+            return {};
+        }
+        if (nz >= -SLOPE) continue;  // vertical
+        for (int i = 0; i < 4; i++) {
+            out.push_back(q[3 * (3 - i)]);
+            out.push_back(q[3 * (3 - i) + 1]);
+            out.push_back(z0);
+        }
+    }
+    if (out.empty()) why = "no wetted element faces downward";
+    return out;
+}
+
 }  // namespace hbg
 
 using namespace hbg;
@@ -427,8 +464,8 @@ extern "C" HbStatus hb_set_text(HbModel* model, uint64_t object, const char* ite
             BodyObj& b = model->bodies[object - OBJ_BODY0];
             if (it == "mesh") return b.mesh = v, HB_OK;
             if (it == "interior_surface") {
-                if (v != "none" && v != "detect" && v != "mesh")
-                    return refuse(HB_ERR_UNSUPPORTED, "interior_surface none, detect or mesh on this route");
+                if (v != "none" && v != "detect" && v != "mesh" && v != "projected")
+                    return refuse(HB_ERR_UNSUPPORTED, "interior_surface none, detect, projected or mesh on this route");
                 return b.interior = v, HB_OK;
             }
             if (it == "interior_surface_mesh") return b.interior_mesh = v, HB_OK;
@@ -501,6 +538,13 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
                         for (int i = 0; i < 4; i++) z0 = z0 && bv[12 * p + 3 * i + 2] == 0.0;
                         if (z0) bk[p] = HBG_INTERIOR;
                     }
+                if (b.interior == "projected") {
+                    std::string why;
+                    std::vector<double> lv = projected_lid(bv, -b.position[2], why);
+                    if (!why.empty()) return refuse(HB_ERR_VALUE, "body '" + b.name + "': interior surface 'projected': " + why);
+                    bv.insert(bv.end(), lv.begin(), lv.end());
+                    bk.resize(bv.size() / 12, HBG_INTERIOR);
+                }
                 if (b.interior == "mesh") {
                     if (!lid) return refuse(HB_ERR_VALUE, "interior_surface_mesh names no mesh");
                     std::vector<double> lv = sectors ? lid->vertices : expand(*lid);

@@ -304,6 +304,31 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
     return out
 
 
+# ------------------------------------------------------------------ generated interior surface
+def projected_lid(verts, z0=0.0):
+    """interior.rs:79-138 projected: the downward-facing panels (unit normal of the diagonals' cross product
+    with n_z < -1e-6) projected onto z = z0 with their vertex order reversed (facing up); panels in z0 and
+    vertical ones skipped; an upward-facing panel (n_z > 1e-6) raises ValueError."""
+    v = np.asarray(verts, dtype=np.float64).reshape(-1, 4, 3)
+    tol = 1e-6 * max(1.0, np.abs(v).max())
+    out = []
+    for k, q in enumerate(v):
+        if np.all(np.abs(q[:, 2] - z0) <= tol):
+            continue
+        n = np.cross(q[2] - q[0], q[3] - q[1])
+        nz = n[2] / np.linalg.norm(n)
+        if nz > 1e-6:
+            raise ValueError(f"wetted element {k + 1} faces upward")
+        if nz >= -1e-6:
+            continue
+        w = q[::-1].copy()
+        w[:, 2] = z0
+        out.append(w)
+    if not out:
+        raise ValueError("no wetted element faces downward")
+    return np.array(out)
+
+
 # ------------------------------------------------------------------ field points
 def field_influence(panels, kinds, pts, depth, omega, grav=GRAVITY, logint=True, tol=1e-4):
     """(S, D) [P][N] complex128: the influence of every panel at every field point."""
