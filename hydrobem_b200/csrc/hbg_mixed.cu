@@ -121,7 +121,7 @@ inline int& ir_guess() {
 
 // Side streams for the LU of LU_GROUPS groups of a batch and their fork/join events, per device and
 // host thread (kept across solves).
-constexpr int LU_GROUPS = 3;
+constexpr int LU_GROUPS = 4;
 struct SideStreams {
     cudaStream_t s[LU_GROUPS + 1] = {};  // the LU groups, then the right-hand sides
     cudaEvent_t fork = nullptr, join[LU_GROUPS + 1] = {};
