@@ -673,15 +673,54 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     if (opt.precision == HBG_MIXED) {
         const char* msg = "";
         int64_t fq = -1;
+        std::vector<int64_t> fallback;  // frequencies the mixed form hands to the FP64 form
         int rc = mixed_solve_frequencies(pv, dst.as<double>(), pr, opt, fin, depth, s, prof, &g_launches, &msg, &fq,
                                          run_statics, motions ? mot_mats : nullptr,
-                                         FieldArgs{field ? dpts.as<double>() : nullptr, field ? nfp : 0, dfst.as<double>()});
+                                         FieldArgs{field ? dpts.as<double>() : nullptr, field ? nfp : 0, dfst.as<double>()},
+                                         &fallback);
         cudaError_t e = cudaStreamSynchronize(s);
         if (e == cudaSuccess) statics_check();
         if (rc != 0) throw Failure{rc, msg, body_index, fq};
         CUDA_OK(e);
         if (pr.out.hydrostatics)
             CUDA_OK(cudaMemcpy(pr.out.hydrostatics, dhyd.p, sizeof(double) * nbod * HBG_HS, cudaMemcpyDeviceToHost));
+        if (!fallback.empty()) {
+            // the frequencies whose refinement did not converge, solved again by the FP64 form (pivoted LU)
+            const size_t nf = fallback.size(), DDo = (size_t)D * D, HD = (size_t)H * 2 * D;
+            const size_t PD = (size_t)(field ? nfp : 0) * 2 * D, PH = (size_t)(field ? nfp : 0) * 2 * H;
+            std::vector<double> om(nf), a(nf * DDo), b(nf * DDo), x(nf * HD), fk(nf * HD), sc(nf * HD), mo(nf * HD),
+                fr(nf * PD), fi(nf * PH), fs(nf * PH), fdf(nf * PH);
+            for (size_t i = 0; i < nf; i++) om[i] = pr.omegas[fallback[i]];
+            HbgProblem sub = pr_in;
+            sub.omegas = om.data();
+            sub.n_omega = (int64_t)nf;
+            sub.out = HbgOutputs{a.data(), b.data(), x.data(), fk.data(), sc.data(), motions ? mo.data() : nullptr,
+                                 nullptr, PD ? fr.data() : nullptr, PH ? fi.data() : nullptr, PH ? fs.data() : nullptr,
+                                 PH ? fdf.data() : nullptr};
+            HbgOptions o64 = opt;
+            o64.precision = HBG_FP64;
+            o64.surrogate = nullptr;
+            solve_problem(sub, o64, body_index, s);
+            for (size_t i = 0; i < nf; i++) {
+                const size_t fo = (size_t)fallback[i];
+                auto put = [&](double* dst, const std::vector<double>& src, size_t per) {
+                    if (dst && per) memcpy(dst + fo * per, src.data() + i * per, per * sizeof(double));
+                };
+                put(pr.out.added_mass, a, DDo);
+                put(pr.out.radiation_damping, b, DDo);
+                put(pr.out.excitation, x, HD);
+                put(pr.out.froude_krylov, fk, HD);
+                put(pr.out.scattering, sc, HD);
+                if (motions) put(pr.out.motions, mo, HD);
+                if (field) {
+                    put(pr.out.field_radiation, fr, PD);
+                    put(pr.out.field_incident, fi, PH);
+                    put(pr.out.field_scattering, fs, PH);
+                    put(pr.out.field_diffraction, fdf, PH);
+                }
+            }
+            last_fallback_count() += (int64_t)nf;
+        }
         return;
     }
     // ---- frequency batches
@@ -935,6 +974,7 @@ extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_proble
         if (!problems || !opt || n_problems < 0) return fail({HB_ERR_ARGUMENT, "null argument"});
         for (int i = 0; i < 6; i++) g_profile[i] = 0.0;
         g_launches = 0;
+        last_fallback_count() = 0;
         profiler().reset();
         for (int64_t p = 0; p < n_problems; p++) {
             const HbgProblem& pr = problems[p];
@@ -1023,6 +1063,12 @@ extern "C" HbStatus hbg_release_workspace(void) {
             g_ws[d]->release();
             cudaSetDevice(cur);
         }
+    return HB_OK;
+}
+
+extern "C" HbStatus hbg_last_fallback_count(int64_t* count) {
+    if (!count) return fail({HB_ERR_ARGUMENT, "null argument"});
+    *count = last_fallback_count();
     return HB_OK;
 }
 

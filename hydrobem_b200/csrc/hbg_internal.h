@@ -301,6 +301,11 @@ void launch_field(const PanelsView& pv, const double* pts, int P, const double* 
                   const FdParams* fd, const double* tiles, const double* fq, bool finite, int H, const double* heads,
                   double depth, double grav, const double2* phi, int ldphi, const double2* u, const double2* phiI,
                   double2* frad, double2* finc, double2* fsca, double2* fdif, cudaStream_t s);
+// frequencies of the last hbg_solve_batch of this thread that the mixed form handed to the FP64 form
+inline int64_t& last_fallback_count() {
+    static thread_local int64_t n = 0;
+    return n;
+}
 // the rigid data of the motions as uploaded, per body: mass (NaN: displaced), centre of gravity (3),
 // inertia kind, inertia (9), inertia origin (3)
 constexpr int RIGID_PER_BODY = 17;

@@ -154,7 +154,7 @@ static SideStreams& side_streams() {
 int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgProblem& pr, const HbgOptions& opt,
                             bool fin, double depth, cudaStream_t s, double* prof, int64_t* launches, const char** msg,
                             int64_t* freq, const std::function<void()>& start, const double* motion,
-                            const FieldArgs& field) {
+                            const FieldArgs& field, std::vector<int64_t>* fallback) {
     KernelProfiler& P = profiler();
     // N panels; with symmetry sectors G systems of Nm = N / G unknowns per frequency (one of N otherwise)
     const int N = pv.N, G = pv.G, Nm = N / G, F = (int)pr.n_omega, H = (int)pr.n_heading, D = 6 * pv.nbod,
@@ -790,12 +790,32 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         }
         P.flush();
         if (cudaGetLastError() != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "CUDA error in the mixed-precision solve", f0);
-        if (*herr == 10) MIXED_FAIL(HB_ERR_NUMERICAL, "zero pivot in the unpivoted mixed-precision LU", f0);
         if (*herr == 8) MIXED_FAIL(HB_ERR_INTERNAL, "a triangular sweep wait timed out", f0);
         if (*herr == 11) MIXED_FAIL(HB_ERR_NUMERICAL, "singular motion equation", f0);
-        if (*herr != 0) MIXED_FAIL(HB_ERR_INTERNAL, "a tensor-core pipeline wait timed out", f0);
-        if (!converged)
-            MIXED_FAIL(HB_ERR_NUMERICAL, "iterative refinement of the mixed-precision solve did not converge", f0);
+        if (*herr != 0 && *herr != 10) MIXED_FAIL(HB_ERR_INTERNAL, "a tensor-core pipeline wait timed out", f0);
+        // Frequencies the reduced-precision factors cannot solve (a zero pivot of the unpivoted LU: the whole
+        // batch; a system whose corrections do not contract, as near an irregular frequency) go to the FP64
+        // form; a system counts as solved when its own predicted error, as the batch test, is below IR_TOL.
+        std::vector<char> redo(nb, 0);
+        if (*herr == 10) {
+            std::fill(redo.begin(), redo.end(), 1);
+        } else if (!converged) {
+            const int last = last_ir_history().n - 1;
+            for (int q = 0; q < ns; q++) {
+                auto ratio = [&](int i) {
+                    const double r = hn[(size_t)i * 2 * ns + 2 * q] / std::max(hn[(size_t)i * 2 * ns + 2 * q + 1], 1e-300);
+                    return std::isfinite(r) ? r : INFINITY;
+                };
+                const double rl = last >= 0 ? ratio(last) : INFINITY;
+                const double rho = last >= 1 ? std::min(1.0, rl / std::max(ratio(last - 1), 1e-300)) : 1.0;
+                if (!(rl * rho <= IR_TOL)) redo[q / G] = 1;
+            }
+        }
+        if (!fallback) {
+            for (int i = 0; i < nb; i++)
+                if (redo[i])
+                    MIXED_FAIL(HB_ERR_NUMERICAL, "iterative refinement of the mixed-precision solve did not converge", f0 + i);
+        }
         const double* hA = hout;
         const double* hB = hA + DD * nb;
         const double* hX = hA + 2 * DD * nb;
@@ -806,6 +826,10 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         const double* hFi = hFr + (size_t)nfp * 2 * D * nb;
         for (int i = 0; i < nb; i++) {
             const size_t fo = (size_t)(f0 + i), hx = (size_t)H * 2 * D;
+            if (redo[i]) {
+                fallback->push_back((int64_t)fo);
+                continue;
+            }
             for (size_t q = 0; q < DD; q++)
                 if (!std::isfinite(hA[DD * i + q]) || !std::isfinite(hB[DD * i + q]))
                     MIXED_FAIL(HB_ERR_NUMERICAL, "non-finite solution", f0 + i);

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstdint>
 #include <functional>
+#include <vector>
 
 #include "../../include/hydrobem_gpu.h"
 #include "hbg_internal.h"
@@ -19,11 +20,12 @@ struct FieldArgs {
 // [4][N*N]) on stream s; it is called once the host-side setup (batch sizing, buffers, kernel
 // attributes) is done, before the first assembly.  motion: the motion matrices M, C, B_ext (D x D each,
 // one after the other, written by the statics stage) when the problem wants motions, else null; field:
-// the field points (P = 0: none).  Returns 0, or an HbStatus with the message in *msg and the frequency in *freq.
+// the field points (P = 0: none); fallback: receives the frequencies whose refinement did not converge (or
+// whose unpivoted LU met a zero pivot), their outputs left unwritten for the FP64 form.  Returns 0, or an HbStatus with the message in *msg and the frequency in *freq.
 int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgProblem& pr, const HbgOptions& opt,
                             bool finite, double depth, cudaStream_t s, double* prof, int64_t* launches,
                             const char** msg, int64_t* freq, const std::function<void()>& start,
-                            const double* motion, const FieldArgs& field);
+                            const double* motion, const FieldArgs& field, std::vector<int64_t>* fallback);
 
 int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* C, bool subtract, const char** msg);
 int measure_peaks(double* out, const char** msg);

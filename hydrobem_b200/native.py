@@ -91,7 +91,7 @@ EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
            "hbg_statics_noalloc", "hbg_measure_peaks", "hbg_last_ir_history", "hbg_surrogate_train",
            "hbg_surrogate_grad", "hbg_surrogate_eval", "hbg_last_surrogate_pairs", "hbg_read_gdf", "hbg_gdf_free",
-           "hb_model_load_mesh"]
+           "hb_model_load_mesh", "hbg_last_fallback_count"]
 
 _lib = None
 
@@ -300,6 +300,13 @@ def last_profile():
     v = (ctypes.c_double * 6)()
     lib().hbg_last_profile(v)
     return dict(zip(("statics", "assembly", "lu", "substitution", "forces", "total"), list(v)))
+
+
+def last_fallback_count() -> int:
+    """Frequencies of the last solve that the mixed form handed to the FP64 form."""
+    c = ctypes.c_int64()
+    lib().hbg_last_fallback_count(ctypes.byref(c))
+    return c.value
 
 
 def last_launch_count() -> int:

@@ -199,6 +199,12 @@ HbStatus hbg_kernel_profile(int32_t family, double *ms, int64_t *launches, doubl
  * nothing); this frees them.  No counterpart in the reference (its buffers are per solve). */
 HbStatus hbg_release_workspace(void);
 
+/* The frequencies of the last hbg_solve_batch of this thread that the mixed form solved with the FP64 form
+ * instead: those whose iterative refinement did not converge (its reduced-precision factors do not
+ * contract the error, as next to an irregular frequency of a body without an interior lid) or whose
+ * unpivoted LU met a zero pivot. */
+HbStatus hbg_last_fallback_count(int64_t *count);
+
 /* The kernels launched by the last hbg_solve_batch of this thread. */
 HbStatus hbg_last_launch_count(int64_t *count);
 

@@ -128,3 +128,34 @@ def test_mixed_large_barge_with_lid():
     errs = {k: scaled_error(mixed[k], fp64[k]) for k in ("A", "B", "X")}
     assert max(errs.values()) <= MIXED_TOL, (errs, hist)
     assert hist[-1] <= 1e-7 and len(hist) <= 12, hist
+
+
+def _c3_body(index):
+    """Body `index` of the 64-body configuration (seed 20261203: cylinders or hemispheres of radius
+    U[0.5, 3], draught U[0.3, 2], N ~ U[800, 6000] rounded to the generators' grids, 16 frequencies with
+    K r ~ U[0.1, 10], headings 0 and 45 degrees)."""
+    rng = np.random.default_rng(20261203)
+    for b in range(index + 1):
+        r, d, n = rng.uniform(0.5, 3.0), rng.uniform(0.3, 2.0), int(rng.uniform(800, 6000))
+        if rng.uniform() < 0.5:
+            nphi = max(8, int(round(np.sqrt(n) / 4)) * 4)
+            nz = max(2, int(round(n / (2 * nphi))))
+            v = meshes.cylinder(r, d, nphi, nz, nz)
+        else:
+            nphi = max(8, int(round(np.sqrt(2 * n) / 4)) * 4)
+            v = meshes.hemisphere(r, max(2, int(round(n / nphi))), nphi)
+        omegas = np.sqrt(rng.uniform(0.1, 10.0, 16) / r * 9.80665)
+    return v, omegas
+
+
+def test_mixed_falls_back_to_fp64_where_refinement_cannot_converge():
+    """A shallow cylinder without an interior lid (r = 2.7 m, draught 0.31 m, 2912 panels) over K r up to
+    10: next to its irregular frequencies the reduced-precision factors no longer contract the error, and
+    those frequencies are solved by the FP64 form; the whole answer stays within the bar."""
+    v, omegas = _c3_body(30)
+    assert len(v) == 2912
+    gpu = nv.solve(v, omegas, [0.0, 45.0], precision=nv.HBG_MIXED)
+    assert 1 <= nv.last_fallback_count() < len(omegas)
+    ref = nv.solve(v, omegas, [0.0, 45.0])
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    assert max(errs.values()) <= MIXED_TOL, errs
