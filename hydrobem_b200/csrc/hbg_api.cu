@@ -689,14 +689,14 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
             const size_t nf = fallback.size(), DDo = (size_t)D * D, HD = (size_t)H * 2 * D;
             const size_t PD = (size_t)(field ? nfp : 0) * 2 * D, PH = (size_t)(field ? nfp : 0) * 2 * H;
             std::vector<double> om(nf), a(nf * DDo), b(nf * DDo), x(nf * HD), fk(nf * HD), sc(nf * HD), mo(nf * HD),
-                fr(nf * PD), fi(nf * PH), fs(nf * PH), fdf(nf * PH);
+                hk(nf * HD), fr(nf * PD), fi(nf * PH), fs(nf * PH), fdf(nf * PH);
             for (size_t i = 0; i < nf; i++) om[i] = pr.omegas[fallback[i]];
             HbgProblem sub = pr_in;
             sub.omegas = om.data();
             sub.n_omega = (int64_t)nf;
             sub.out = HbgOutputs{a.data(), b.data(), x.data(), fk.data(), sc.data(), motions ? mo.data() : nullptr,
                                  nullptr, PD ? fr.data() : nullptr, PH ? fi.data() : nullptr, PH ? fs.data() : nullptr,
-                                 PH ? fdf.data() : nullptr};
+                                 PH ? fdf.data() : nullptr, hk.data()};
             HbgOptions o64 = opt;
             o64.precision = HBG_FP64;
             o64.surrogate = nullptr;
@@ -712,6 +712,7 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
                 put(pr.out.froude_krylov, fk, HD);
                 put(pr.out.scattering, sc, HD);
                 if (motions) put(pr.out.motions, mo, HD);
+                put(pr.out.haskind, hk, HD);
                 if (field) {
                     put(pr.out.field_radiation, fr, PD);
                     put(pr.out.field_incident, fi, PH);
@@ -787,7 +788,8 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     CUDA_OK(cudaMemcpyAsync(dheads.p, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s));
     // outputs per batch: A, B [D][D], X, FK, SC, motions [H][D], field values [P][D] and 3 x [P][H]
     const int Pf = field ? nfp : 0;
-    const size_t out_per = 2 * (size_t)D * D * sizeof(double) + 4 * (size_t)H * D * sizeof(double2) +
+    // outputs per batch: ..., then the Haskind exciting force [H][D]
+    const size_t out_per = 2 * (size_t)D * D * sizeof(double) + 5 * (size_t)H * D * sizeof(double2) +
                            (size_t)Pf * (D + 3 * H) * sizeof(double2);
     WsBuf dfq(ws, WS_FQ);
     if (field && fin) dfq.alloc(sizeof(double) * FP_PLANES * (size_t)(N + nfp) * B);
@@ -886,7 +888,9 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
             launch_forces(pv, nb, dfi.as<FreqInfo>(), H, phi, N, dphiI.as<double2>(), opt.density, dAo, dBo, dXo, dFK,
                           dSC, s);
             P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
-            g_launches += 1;
+            launch_haskind(pv, nb, dfi.as<FreqInfo>(), H, phi, N, du.as<double2>(), dphiI.as<double2>(), opt.density,
+                           dSC + 2 * (size_t)H * D * nb + (size_t)Pf * (D + 3 * H) * nb, s);
+            g_launches += 1 + (H > 0);
             CUDA_OK(cudaMemsetAsync(derr.p, 0, sizeof(int32_t), s));
             if (motions) {
                 launch_motions(nb, D, H, dfi.as<FreqInfo>(), dAo, dBo, dXo, mot_mats, mot_mats + DD2, mot_mats + 2 * DD2,
@@ -921,6 +925,7 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         const double* hMo = hSC + (size_t)H * 2 * D * nb;
         const double* hFr = hMo + (size_t)H * 2 * D * nb;
         const double* hFi = hFr + (size_t)Pf * 2 * D * nb;
+        const double* hHK = hFi + (size_t)Pf * 2 * 3 * H * nb;
         if (*herr != 0) throw Failure{HB_ERR_NUMERICAL, "singular motion equation", body_index, f0};
         for (int i = 0; i < nb; i++) {
             for (int c = 0; c < G; c++)
@@ -939,6 +944,7 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
             if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
             if (motions) memcpy(pr.out.motions + fo * hx, hMo + hx * i, hx * sizeof(double));
+            if (pr.out.haskind) memcpy(pr.out.haskind + fo * hx, hHK + hx * i, hx * sizeof(double));
             if (field) {
                 const size_t pd = (size_t)nfp * 2 * D, ph = (size_t)nfp * 2 * H;
                 if (pr.out.field_radiation) memcpy(pr.out.field_radiation + fo * pd, hFr + pd * i, pd * sizeof(double));
@@ -1277,4 +1283,5 @@ extern "C" HbStatus hb_last_error_location(HbLocation* location) {
     return HB_OK;
 }
 
-extern "C" uint32_t hb_abi_version(void) { return HBG_ABI_VERSION; }
+extern "C" uint32_t hb_abi_version(void) { return HB_ABI_VERSION; }
+extern "C" uint32_t hbg_library_version(void) { return HBG_ABI_VERSION; }

@@ -778,4 +778,72 @@ void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const
     k_forces<<<dim3(6 * pv.nbod + H, pv.nbod, F), 256, 0, s>>>(pv, fi, H, phi, ldphi, phiI, rho, A, B, X, FK, SC);
 }
 
+// ------------------------------------------------------------------ Haskind excitation
+// lo_frequency.rs:1118-1171 on this route's panels (wetted and interior; interior panels take no part):
+// HK(h, c) = i w rho sum over wetted j of (n_c(j) phi_I(h, j) - phi_c(j) dphi_I/dn(h, j)) A_j, with n_c the
+// generalized normal of radiation column c (zero off its body) and dphi_I/dn = -u(D + h, j), the boundary
+// value of diffraction column h on a wetted panel.  One block per (radiation column, frequency); the
+// headings in chunks of eight, each chunk one pass over the panels, warp shuffles and a fixed-order sum
+// over the warps.  Output [F][H][D] as the other exciting forces (solve_driver.rs:376-383).
+__global__ void __launch_bounds__(256) k_haskind(PanelsView pv, const FreqInfo* __restrict__ fi, int H,
+                                                 const double2* __restrict__ phi, int ldphi,
+                                                 const double2* __restrict__ u, const double2* __restrict__ phiI,
+                                                 double rho, double2* __restrict__ HK) {
+    __shared__ double red[8][16];
+    __shared__ double tot[16];
+    const int c = blockIdx.x, f = blockIdx.y, N = pv.N;
+    const int D = 6 * pv.nbod, nrhs = D + H;
+    const double2* pc = phi + ((size_t)f * nrhs + c) * ldphi;
+    const double2* ud = u + ((size_t)f * nrhs + D) * N;
+    const double2* pI = phiI + (size_t)f * H * N;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int h0 = 0; h0 < H; h0 += 8) {
+        const int nh = min(8, H - h0);
+        double acc[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) acc[k] = 0.0;
+        for (int j = threadIdx.x; j < N; j += blockDim.x) {
+            if (pv.kind[j] != 0) continue;
+            const double ar = pv.at(P_AREA, j);
+            const double nc = pv.gen_normal(j, c) * ar;
+            const double2 p = pc[j];
+            const double px = p.x * ar, py = p.y * ar;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (q < nh) {
+                    const double2 I = pI[(size_t)(h0 + q) * N + j];
+                    const double2 un = ud[(size_t)(h0 + q) * N + j];  // -dphi_I/dn
+                    acc[2 * q] += nc * I.x + (px * un.x - py * un.y);
+                    acc[2 * q + 1] += nc * I.y + (px * un.y + py * un.x);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            double v = acc[k];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp][k] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < 2 * nh) {
+            double t = 0.0;
+            for (int w8 = 0; w8 < (int)(blockDim.x >> 5); w8++) t += red[w8][threadIdx.x];
+            tot[threadIdx.x] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x < nh) {
+            const double w = fi[f].omega, vr = tot[2 * threadIdx.x], vi = tot[2 * threadIdx.x + 1];
+            // i w rho (vr + i vi)
+            HK[((size_t)f * H + h0 + threadIdx.x) * D + c] = make_double2(-w * rho * vi, w * rho * vr);
+        }
+        __syncthreads();
+    }
+}
+
+void launch_haskind(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, int ldphi,
+                    const double2* u, const double2* phiI, double rho, double2* HK, cudaStream_t s) {
+    if (H <= 0) return;
+    k_haskind<<<dim3(6 * pv.nbod, F), 256, 0, s>>>(pv, fi, H, phi, ldphi, u, phiI, rho, HK);
+}
+
 }  // namespace hbg

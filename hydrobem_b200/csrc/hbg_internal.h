@@ -319,6 +319,10 @@ void launch_motions(int F, int D, int H, const FreqInfo* fi, const double* A, co
 void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, int ldphi,
                    const double2* phiI, double rho, double* A, double* B, double2* X, double2* FK, double2* SC,
                    cudaStream_t s);
+// Haskind exciting force HK [F][H][D] from the radiation potentials, the incident wave and the diffraction
+// columns' boundary values u (lo_frequency.rs:1118-1171)
+void launch_haskind(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, int ldphi,
+                    const double2* u, const double2* phiI, double rho, double2* HK, cudaStream_t s);
 // host-side finite-depth scalars of one ordinary frequency (green_fin.rs:874-934)
 void make_fd_params(double h, double K, FdParams& fd);
 double dispersion_x0(double H);

@@ -299,7 +299,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     std::vector<FreqInfo> fi(B);
     std::vector<FdParams> fdh(B);
     // per frequency: A, B [D][D], X, FK, SC, motions [H][D] complex, field values [P][D] and 3 x [P][H]
-    const size_t out_per = 2 * (size_t)D * D + 4 * (size_t)H * 2 * D + (size_t)nfp * 2 * (D + 3 * H), DD = (size_t)D * D;
+    // A, B [D][D], X, FK, SC, motions [H][D], field values [P][D] and 3 x [P][H], Haskind [H][D]
+    const size_t out_per = 2 * (size_t)D * D + 5 * (size_t)H * 2 * D + (size_t)nfp * 2 * (D + 3 * H), DD = (size_t)D * D;
     // page-locked: the reads of norms, outputs and the error flag queue behind the work, no host wait
     double* hout = (double*)ws.host(HS_OUT, sizeof(double) * (out_per * B + 1));
     double* hn = (double*)ws.host(HS_NORMS, sizeof(double) * IR_MAX_IT * 2 * (size_t)BS);
@@ -709,7 +710,9 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                 P.begin(s);
                 launch_forces(pv, nb, dfi, H, G > 1 ? phi : x, G > 1 ? N : Np, phiI, opt.density, dA, dB, dX, dFK, dSC, s);
                 P.end(KF_FORCES, 16.0 * (double)N * (nrhs + H) * nb, s);
-                (*launches)++;
+                launch_haskind(pv, nb, dfi, H, G > 1 ? phi : x, G > 1 ? N : Np, u, phiI, opt.density,
+                               dSC + 2 * (size_t)H * D * nb + (size_t)nfp * (D + 3 * H) * nb, s);
+                *launches += 1 + (H > 0);
                 if (motion && H > 0) {  // the motion equation of every frequency (motion.rs:121-158)
                     launch_motions(nb, D, H, dfi, dA, dB, dX, motion, motion + DD, motion + 2 * DD,
                                    dSC + (size_t)H * D * nb, err, s);
@@ -782,7 +785,10 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                     prev = worst;
                 }
                 t2.stop();
-                if (converged) {
+                // the outputs read back so far are those of the iterate after `guess` corrections; the
+                // keep-or-redo test below looks at the last correction, so the outputs must be its
+                // iterate's, converged or not
+                if (hist.n > guess) {
                     forces();
                     cudaStreamSynchronize(s);
                 }
@@ -824,6 +830,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         const double* hMo = hSC + (size_t)H * 2 * D * nb;
         const double* hFr = hMo + (size_t)H * 2 * D * nb;
         const double* hFi = hFr + (size_t)nfp * 2 * D * nb;
+        const double* hHK = hFi + (size_t)nfp * 2 * 3 * H * nb;
         for (int i = 0; i < nb; i++) {
             const size_t fo = (size_t)(f0 + i), hx = (size_t)H * 2 * D;
             if (redo[i]) {
@@ -839,6 +846,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
             if (motion && pr.out.motions) memcpy(pr.out.motions + fo * hx, hMo + hx * i, hx * sizeof(double));
+            if (pr.out.haskind) memcpy(pr.out.haskind + fo * hx, hHK + hx * i, hx * sizeof(double));
             if (nfp) {
                 const size_t pd = (size_t)nfp * 2 * D, ph = (size_t)nfp * 2 * H;
                 if (pr.out.field_radiation) memcpy(pr.out.field_radiation + fo * pd, hFr + pd * i, pd * sizeof(double));

@@ -590,7 +590,7 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         if (model->cancel.exchange(0) != 0) return refuse(HB_ERR_CANCELLED, "the solve was cancelled");
         const size_t F = omegas.size(), H = heads.size(), NB = centers.size() / 3, D = 6 * NB;
         std::vector<double> A(F * D * D), B(F * D * D), X(F * H * D * 2), FK(F * H * D * 2), SC(F * H * D * 2),
-            MO(F * H * D * 2), HS(NB * HBG_HS);
+            MO(F * H * D * 2), HK(F * H * D * 2), HS(NB * HBG_HS);
         std::vector<double> fpts;
         {
             std::lock_guard<std::mutex> g(model->lock);
@@ -615,7 +615,7 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         pr.n_heading = (int64_t)H;
         pr.out = HbgOutputs{A.data(), B.data(), X.data(), FK.data(), SC.data(), want_motion ? MO.data() : nullptr,
                             HS.data(), NP ? FR.data() : nullptr, NP ? FI.data() : nullptr, NP ? FS.data() : nullptr,
-                            NP ? FDF.data() : nullptr};
+                            NP ? FDF.data() : nullptr, HK.data()};
         pr.field_points = NP ? fpts.data() : nullptr;
         pr.n_field_points = (int64_t)NP;
         if (progress) {
@@ -660,6 +660,12 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         add_quantity(r.get(), "excitation_diffraction_f64", HB_C128, {F, H, D}, X.data(), X.size() * 8);
         add_quantity(r.get(), "excitation_froude_krylov_f64", HB_C128, {F, H, D}, FK.data(), FK.size() * 8);
         add_quantity(r.get(), "excitation_scattering_f64", HB_C128, {F, H, D}, SC.data(), SC.size() * 8);
+        if (H) {  // solve_driver.rs:370-384: [F][H][K], K = D radiation columns (rigid modes) on this route
+            std::vector<float> hk32(HK.size());
+            for (size_t i = 0; i < HK.size(); i++) hk32[i] = (float)HK[i];
+            add_quantity(r.get(), "excitation_haskind", HB_C64, {F, H, D}, hk32.data(), hk32.size() * 4);
+            add_quantity(r.get(), "excitation_haskind_f64", HB_C128, {F, H, D}, HK.data(), HK.size() * 8);
+        }
         if (NP) {  // quantities.rs:58-62: the points, then the elevation or p / (rho g) per column and heading
             add_quantity(r.get(), "field_points", HB_F64, {NP, 3}, fpts.data(), fpts.size() * 8);
             const std::pair<const char*, std::vector<double>*> fq[4] = {{"field_points_pressure_radiation", &FR},

@@ -39,7 +39,7 @@ SYM_NONE, SYM_YZ, SYM_XZ, SYM_BOTH = 0, 1, 2, 3
 class HbgOutputs(ctypes.Structure):
     _fields_ = [("added_mass", dp), ("radiation_damping", dp), ("excitation", dp), ("froude_krylov", dp),
                 ("scattering", dp), ("motions", dp), ("hydrostatics", dp), ("field_radiation", dp),
-                ("field_incident", dp), ("field_scattering", dp), ("field_diffraction", dp)]
+                ("field_incident", dp), ("field_scattering", dp), ("field_diffraction", dp), ("haskind", dp)]
 
 
 class HbgRigid(ctypes.Structure):
@@ -86,6 +86,7 @@ class HbColumn(ctypes.Structure):
 EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_debug_gemm_tf32",
            "hbg_last_ir_iterations", "hbg_last_profile", "hbg_last_launch_count",
            "hbg_profile_kernels", "hbg_kernel_profile", "hbg_release_workspace", "hb_abi_version",
+           "hbg_library_version",
            "hb_last_error_message", "hb_last_error_location", "hb_model_new", "hb_model_free", "hb_model_cancel",
            "hb_object", "hb_add", "hb_set_bool", "hb_set_int", "hb_set_real", "hb_set_text", "hb_set_reals",
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
@@ -140,6 +141,7 @@ def lib():
     L.hb_last_error_message.restype = ctypes.c_char_p
     L.hb_last_error_location.argtypes = [ctypes.POINTER(HbLocation)]
     L.hb_abi_version.restype = ctypes.c_uint32
+    L.hbg_library_version.restype = ctypes.c_uint32
     _lib = L
     return L
 
@@ -197,6 +199,7 @@ class Body:
         self.X = np.zeros((F, H, D), dtype=np.complex128)
         self.FK = np.zeros((F, H, D), dtype=np.complex128)
         self.SC = np.zeros((F, H, D), dtype=np.complex128)
+        self.HK = np.zeros((F, H, D), dtype=np.complex128)
         self.HS = np.zeros((self.n_bodies, HBG_HS))
         self.points = None if points is None else np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
         P = 0 if self.points is None else self.points.shape[0]
@@ -239,6 +242,7 @@ class Body:
         p.out.excitation = self.X.ctypes.data_as(dp)
         p.out.froude_krylov = self.FK.ctypes.data_as(dp)
         p.out.scattering = self.SC.ctypes.data_as(dp)
+        p.out.haskind = self.HK.ctypes.data_as(dp)
         p.out.motions = None if self.MO is None else self.MO.ctypes.data_as(dp)
         p.out.hydrostatics = self.HS.ctypes.data_as(dp)
         p.rigid = None if self._rigid is None else ctypes.pointer(self._rigid)
@@ -252,7 +256,7 @@ class Body:
         return p
 
     def results(self):
-        out = {"A": self.A, "B": self.B, "X": self.X, "FK": self.FK, "SC": self.SC,
+        out = {"A": self.A, "B": self.B, "X": self.X, "FK": self.FK, "SC": self.SC, "HK": self.HK,
                "hydrostatics": [hydrostatics_record(h) for h in self.HS]}
         if self.MO is not None:
             out["motions"] = self.MO
@@ -458,3 +462,93 @@ def last_ir_iterations() -> int:
     n = ctypes.c_int32()
     lib().hbg_last_ir_iterations(ctypes.byref(n))
     return n.value
+
+
+_HB_DTYPES = {1: np.float64, 2: np.float32, 3: np.int32, 4: np.int64, 5: np.uint64, 6: np.complex64, 7: np.complex128}
+
+
+class Model:
+    """The reference's object model through the C ABI: hb_model_new, hb_object, hb_add, hb_set_*,
+    hb_model_solve (crates/hydrobem-c/include/hydrobem.h:507-814).  Items are set by object path
+    ("" the model, "environment", "options", "meshes/<name>", "bodies/<name>"); every call checks its
+    status and raises HydroBEMError with the library's message."""
+
+    def __init__(self):
+        self.L = L = lib()
+        L.hb_add.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                             ctypes.c_int64, ctypes.POINTER(ctypes.c_uint64)]
+        L.hb_object.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_uint64)]
+        L.hb_set_reals.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, dp,
+                                   ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t]
+        L.hb_set_ints.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64),
+                                  ctypes.POINTER(ctypes.c_size_t), ctypes.c_size_t]
+        L.hb_set_text.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_char_p]
+        L.hb_set_real.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_double]
+        L.hb_set_int.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_int64]
+        L.hb_set_bool.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_char_p, ctypes.c_int32]
+        L.hb_model_solve.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        L.hb_model_free.argtypes = [ctypes.c_void_p]
+        L.hb_results_quantity.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(HbColumn)]
+        L.hb_results_free.argtypes = [ctypes.c_void_p]
+        self.m = ctypes.c_void_p()
+        check(L.hb_model_new(ctypes.byref(self.m)))
+
+    def close(self):
+        if self.m:
+            self.L.hb_model_free(self.m)
+            self.m = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def obj(self, path: str) -> int:
+        o = ctypes.c_uint64()
+        check(self.L.hb_object(self.m, path.encode(), ctypes.byref(o)))
+        return o.value
+
+    def add(self, lst: str, name: str, parent: str = "") -> int:
+        o = ctypes.c_uint64()
+        check(self.L.hb_add(self.m, self.obj(parent), lst.encode(), None, name.encode(), -1, ctypes.byref(o)))
+        return o.value
+
+    def reals(self, path: str, item: str, values):
+        a = np.ascontiguousarray(values, dtype=np.float64)
+        shape = (ctypes.c_size_t * max(a.ndim, 1))(*(a.shape or (1,)))
+        check(self.L.hb_set_reals(self.m, self.obj(path), item.encode(), a.ctypes.data_as(dp), shape, a.ndim))
+
+    def real(self, path: str, item: str, value: float):
+        check(self.L.hb_set_real(self.m, self.obj(path), item.encode(), float(value)))
+
+    def text(self, path: str, item: str, value: str):
+        check(self.L.hb_set_text(self.m, self.obj(path), item.encode(), value.encode()))
+
+    def boolean(self, path: str, item: str, value: bool):
+        check(self.L.hb_set_bool(self.m, self.obj(path), item.encode(), int(bool(value))))
+
+    def solve(self) -> "Results":
+        r = ctypes.c_void_p()
+        check(self.L.hb_model_solve(self.m, None, None, ctypes.byref(r)))
+        return Results(self.L, r)
+
+
+class Results:
+    """hb_results_quantity views copied into numpy arrays of the column's element type."""
+
+    def __init__(self, L, handle):
+        self.L, self.r = L, handle
+
+    def quantity(self, name: str) -> np.ndarray:
+        col = HbColumn()
+        check(self.L.hb_results_quantity(self.r, name.encode(), ctypes.byref(col)))
+        dt = np.dtype(_HB_DTYPES[col.dtype])
+        shape = tuple(col.shape[i] for i in range(col.ndim))
+        buf = (ctypes.c_char * (col.count * dt.itemsize)).from_address(col.data)
+        return np.frombuffer(buf, dtype=dt).copy().reshape(shape)
+
+    def free(self):
+        if self.r:
+            self.L.hb_results_free(self.r)
+            self.r = ctypes.c_void_p()

@@ -49,8 +49,12 @@ typedef int32_t HbStatus;
 #define HB_C64 6
 #define HB_C128 7
 
-/* The version of this library's ABI (its own numbering; the reference's hb_abi_version is 8). */
-#define HBG_ABI_VERSION 6
+/* The version of the reference's ABI that the hb_* subset of this header mirrors
+ * (crates/hydrobem-c/src/info.rs:15, capi/include/hydrobem.h:208): hb_abi_version() returns it, so a
+ * caller built against hydrobem.h and comparing with its HB_ABI_VERSION accepts this library. */
+#define HB_ABI_VERSION 8
+/* The revision of this library's own hbg_* entry points and structs (hbg_library_version()). */
+#define HBG_ABI_VERSION 7
 
 /* ==================================================================== batched entry */
 
@@ -123,7 +127,7 @@ typedef struct HbgRigid {
 
 /* Outputs of one problem, caller-allocated host arrays (NULL: not wanted), float64, D = 6 n_bodies:
  *   added_mass, radiation_damping  [n_omega][D][D]   (coordinate i, radiation mode j)
- *   excitation, froude_krylov, scattering, motions  [n_omega][n_heading][D][2]  (re, im)
+ *   excitation, froude_krylov, scattering, motions, haskind  [n_omega][n_heading][D][2]  (re, im)
  *   hydrostatics  [n_bodies][HBG_HS]
  *   field_radiation  [n_omega][n_field_points][D][2]: the elevation (z = 0) or p / (rho g) per unit
  *                    displacement of each radiation mode
@@ -143,6 +147,8 @@ typedef struct HbgOutputs {
     double *field_incident;
     double *field_scattering;
     double *field_diffraction;
+    double *haskind; /* [F][H][D] complex: the exciting force by the Haskind relation from the radiation
+                      * potentials (lo_frequency.rs:1118-1171; the reference's excitation_haskind) */
 } HbgOutputs;
 
 typedef struct HbgProblem {
@@ -372,8 +378,10 @@ typedef int32_t (*HbProgressFn)(const HbProgress *progress, void *user);
 
 #define HB_NO_OBJECT UINT64_MAX
 
-/* hydrobem.h:233 */
+/* hydrobem.h:233: returns HB_ABI_VERSION (8), the ABI of the reference header this subset mirrors */
 uint32_t hb_abi_version(void);
+/* No counterpart in the reference: the revision of the hbg_* entry points (HBG_ABI_VERSION). */
+uint32_t hbg_library_version(void);
 /* hydrobem.h:247, 256 */
 const char *hb_last_error_message(void);
 HbStatus hb_last_error_location(HbLocation *location);
@@ -402,7 +410,8 @@ HbStatus hb_set_ints(HbModel *model, uint64_t object, const char *item, const in
 HbStatus hb_model_solve(HbModel *model, HbProgressFn progress, void *user, HbResults **out);
 /* hydrobem.h:1146, 1154, 1164: quantities omegas, headings, added_mass and radiation_damping
  * (HB_F32 [F][D][K]), excitation_diffraction, excitation_froude_krylov, excitation_scattering
- * (HB_C64 [F][H][D]); the extension quantities <name>_f64 (HB_F64 / HB_C128) keep double precision. */
+ * (HB_C64 [F][H][D]), excitation_haskind (HB_C64 [F][H][K], K = D radiation columns); the extension
+ * quantities <name>_f64 (HB_F64 / HB_C128) keep double precision. */
 void hb_results_free(HbResults *results);
 HbStatus hb_results_has(HbResults *results, const char *name, int32_t *has);
 HbStatus hb_results_quantity(HbResults *results, const char *name, HbColumn *column);

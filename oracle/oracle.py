@@ -9,6 +9,7 @@ and adds, in numpy, the steps that are short formulas of ``crates/hydrobem/src/`
 - right-hand sides -S u and the dense solve  ``lo_frequency.rs:823-955`` (LU with partial pivoting:
   LAPACK ``zgesv`` through numpy, standing in for faer's blocked LU, ``linalg.rs:134-252``)
 - pressure integration A, B, X, FK, SC  ``lo_frequency.rs:1039-1115``
+- the Haskind exciting force HK from the radiation potentials  ``lo_frequency.rs:1118-1171``
 - field points: the elevation or p / (rho g) of the radiation, incident, scattered and total waves at
   points in the fluid by Green's identity over the panels  ``lo_frequency.rs:1392-1470``
 - hydrostatics, rigid inertia and the motion equation of each frequency  ``hydrostatics.rs:116-356``,
@@ -267,7 +268,7 @@ def sector_solve(S, A, u, G):
 
 def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY, rho=DENSITY, logint=True,
                     want_matrices=False, panel_body=None, centers=None, sectors=1, points=None, tol=1e-4):
-    """A, B [D][D], X, FK, SC [H][D] of one frequency (D = 6 per body), all in float64 (complex128).
+    """A, B [D][D], X, FK, SC, HK [H][D] of one frequency (D = 6 per body), all in float64 (complex128).
     sectors > 1: the panels are a mirrored mesh (mirror_sector) solved by its symmetry sectors."""
     c, n, area = panel_arrays(panels)
     N = len(panels)
@@ -280,10 +281,12 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
     u = np.zeros((N, D + H), dtype=np.complex128)
     u[:, :D] = nj
     phiI = np.zeros((H, N), dtype=np.complex128)
+    dphiI = np.zeros((H, N), dtype=np.complex128)
     for h, beta in enumerate(headings_rad):
         pI, gr = incident(c, depth, k, omega, beta, grav)
         phiI[h] = pI
         d = (gr * n).sum(axis=1)
+        dphiI[h] = d
         u[:, D + h] = np.where(wet, -d, 0.0)
     rhs = S @ (-u)
     phi = np.linalg.solve(A, rhs) if sectors == 1 else sector_solve(S, A, u, sectors)
@@ -297,6 +300,10 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
         out["X"] = (iwr * x).T
         out["FK"] = (iwr * fk).T
         out["SC"] = (iwr * (x - fk)).T
+        # Haskind relation (lo_frequency.rs:1118-1171): i w rho sum over wetted panels of
+        # (n_c phi_I - phi_c dphi_I/dn) A_j, per radiation column c; given [h][c] as the other forces
+        hk = w.T @ phiI.T - ((phi[:, :D] * (area * wet)[:, None]).T @ dphiI.T)
+        out["HK"] = (iwr * hk).T
     if points is not None and len(points):
         out.update(field_values(panels, kinds, points, depth, omega, headings_rad, phi, u, phiI, D, grav, logint, tol))
     if want_matrices:

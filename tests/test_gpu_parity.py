@@ -32,7 +32,7 @@ def scaled_error(got, ref, floor=1e-3):
     return float((np.abs(got - ref) / scale).max())
 
 
-def compare(gpu, ref, keys=("A", "B", "X", "FK", "SC")):
+def compare(gpu, ref, keys=("A", "B", "X", "FK", "SC", "HK")):
     errs = {k: scaled_error(gpu[k], ref[k]) for k in keys if k in ref and np.asarray(ref[k]).size}
     assert max(errs.values()) <= TOL, errs
     return errs

@@ -65,7 +65,7 @@ def test_mixed_config1_cylinder():
     gpu = nv.solve(v, omegas, [0.0], precision=nv.HBG_MIXED)
     its = nv.last_ir_iterations()
     ref = O.solve_body(v, omegas, [0.0], depth=math.inf)
-    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= MIXED_TOL, (errs, its)
     assert 1 <= its <= 12
 
@@ -76,7 +76,7 @@ def test_mixed_finite_depth_four_headings():
     heads = [0.0, 30.0, 60.0, 90.0]
     gpu = nv.solve(v, omegas, heads, depth=5.0, precision=nv.HBG_MIXED)
     ref = O.solve_body(v, omegas, heads, depth=5.0)
-    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= MIXED_TOL, errs
 
 
@@ -87,7 +87,7 @@ def test_mixed_padding_and_uneven_bodies():
     out = nv.solve_batch(bodies, precision=nv.HBG_MIXED)
     for b, g in zip(bodies, out):
         ref = O.solve_body(b.vertices, b.omegas, b.headings, depth=math.inf)
-        errs = {k: scaled_error(g[k], ref[k]) for k in ("A", "B", "X")}
+        errs = {k: scaled_error(g[k], ref[k]) for k in ("A", "B", "X", "HK")}
         assert max(errs.values()) <= MIXED_TOL, errs
 
 
@@ -98,7 +98,7 @@ def test_mixed_interior_lid():
     omegas = np.array([1.0, 2.0, 3.5])
     gpu = nv.solve(v, omegas, [0.0, 45.0], kinds=kinds, precision=nv.HBG_MIXED)
     ref = O.solve_body(v, omegas, [0.0, 45.0], depth=math.inf, kinds=kinds)
-    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= MIXED_TOL, errs
 
 
@@ -109,7 +109,7 @@ def test_mixed_many_headings():
     omegas = np.array([0.9, 2.2])
     gpu = nv.solve(v, omegas, heads, depth=3.0, precision=nv.HBG_MIXED)
     ref = O.solve_body(v, omegas, heads, depth=3.0)
-    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= MIXED_TOL, errs
 
 
@@ -125,7 +125,7 @@ def test_mixed_large_barge_with_lid():
     mixed = nv.solve(v, omegas, heads, kinds=kinds, precision=nv.HBG_MIXED)
     hist = nv.last_ir_history()
     fp64 = nv.solve(v, omegas, heads, kinds=kinds)
-    errs = {k: scaled_error(mixed[k], fp64[k]) for k in ("A", "B", "X")}
+    errs = {k: scaled_error(mixed[k], fp64[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= MIXED_TOL, (errs, hist)
     assert hist[-1] <= 1e-7 and len(hist) <= 12, hist
 
@@ -157,5 +157,23 @@ def test_mixed_falls_back_to_fp64_where_refinement_cannot_converge():
     gpu = nv.solve(v, omegas, [0.0, 45.0], precision=nv.HBG_MIXED)
     assert 1 <= nv.last_fallback_count() < len(omegas)
     ref = nv.solve(v, omegas, [0.0, 45.0])
-    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "HK")}
+    assert max(errs.values()) <= MIXED_TOL, errs
+
+
+def test_mixed_fallback_after_corrections_beyond_the_first_look():
+    """The refinement queues as many corrections as the previous batch needed before the host looks at
+    the norms.  After a 128-panel body (one diagonal block: two corrections suffice) the shallow
+    cylinder's batch needs more than those; its systems that converge only in the corrections the host
+    adds one by one must report the outputs of their last iterate, not those read back at the first
+    look, while the ones that cannot converge go to the FP64 form."""
+    small = meshes.cylinder(1.0, 0.5, 16, 4, 4)
+    assert len(small) == 128
+    nv.solve(small, np.array([1.0, 2.0]), [0.0], precision=nv.HBG_MIXED)
+    assert len(nv.last_ir_history()) == 2, nv.last_ir_history()
+    v, omegas = _c3_body(30)
+    gpu = nv.solve(v, omegas, [0.0, 45.0], precision=nv.HBG_MIXED)
+    assert 1 <= nv.last_fallback_count() < len(omegas)
+    ref = nv.solve(v, omegas, [0.0, 45.0])
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= MIXED_TOL, errs

@@ -49,7 +49,7 @@ def split_cylinder():
 def block_sums(r, F, H):
     """The 12-mode results of a split body summed over the body blocks (6 modes)."""
     out = {"A": r["A"].reshape(F, 2, 6, 2, 6).sum(axis=(1, 3)), "B": r["B"].reshape(F, 2, 6, 2, 6).sum(axis=(1, 3))}
-    for k in ("X", "FK", "SC"):
+    for k in ("X", "FK", "SC", "HK"):
         out[k] = r[k].reshape(F, H, 2, 6).sum(axis=2)
     return out
 
@@ -60,7 +60,7 @@ def test_oracle_split_body_is_linear():
     two = O.solve_body(v, OMEGAS[:2], HEADS, depth=math.inf, panel_body=body, centers=[[0, 0, 0], [0, 0, 0]])
     assert two["A"].shape == (2, 12, 12) and two["X"].shape == (2, 2, 12)
     summed = block_sums(two, 2, len(HEADS))
-    for k in ("A", "B", "X", "FK", "SC"):
+    for k in ("A", "B", "X", "FK", "SC", "HK"):
         assert scaled_error(summed[k], one[k]) <= 1e-10, k
 
 
@@ -87,7 +87,7 @@ def test_gpu_two_interacting_bodies(depth):
     gpu = nv.solve(v, OMEGAS, HEADS, depth=depth, panel_body=body, rotation_centers=centers)
     ref = O.solve_body(v, OMEGAS, HEADS, depth=depth, panel_body=body, centers=centers)
     assert gpu["A"].shape == (3, 12, 12) and gpu["X"].shape == (3, 2, 12)
-    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "FK", "SC")}
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "FK", "SC", "HK")}
     assert max(errs.values()) <= 1e-9, errs
     # the two bodies are mirror images about x = 0 and the heading-0 wave comes along x: their heave
     # added masses agree
@@ -113,7 +113,7 @@ def test_gpu_split_body_is_linear():
     one = nv.solve(v, OMEGAS, HEADS)
     two = nv.solve(v, OMEGAS, HEADS, panel_body=body, rotation_centers=[[0, 0, 0], [0, 0, 0]])
     summed = block_sums(two, len(OMEGAS), len(HEADS))
-    for k in ("A", "B", "X", "FK", "SC"):
+    for k in ("A", "B", "X", "FK", "SC", "HK"):
         assert scaled_error(summed[k], one[k]) <= 1e-10, k
 
 
@@ -226,6 +226,6 @@ def test_gpu_three_cylinder_array(precision):
     gpu = nv.solve(v, omegas, [0.0], panel_body=body, rotation_centers=centers, precision=prec)
     ref = O.solve_body(v, omegas, [0.0], depth=math.inf, panel_body=body, centers=centers)
     assert gpu["A"].shape == (2, 18, 18)
-    keys = ("A", "B", "X", "FK", "SC") if precision == "fp64" else ("A", "B", "X")
+    keys = ("A", "B", "X", "FK", "SC", "HK") if precision == "fp64" else ("A", "B", "X", "HK")
     errs = {k: scaled_error(gpu[k], ref[k]) for k in keys}
     assert max(errs.values()) <= (1e-9 if precision == "fp64" else 1e-5), errs

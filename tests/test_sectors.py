@@ -82,7 +82,7 @@ def test_gpu_sectors_against_the_oracle(precision, sym, depth):
     prec = nv.HBG_MIXED if precision == "mixed" else nv.HBG_FP64
     gpu = nv.solve(sector, omegas, heads, symmetry=sym, depth=depth, precision=prec)
     ref = O.solve_body(sector, omegas, heads, depth=depth, symmetry=sym)
-    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "FK", "SC")}
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "FK", "SC", "HK")}
     assert max(errs.values()) <= (MIXED_TOL if precision == "mixed" else FP64_TOL), errs
 
 
@@ -98,7 +98,7 @@ def test_gpu_sectors_with_an_interior_lid(precision):
     prec = nv.HBG_MIXED if precision == "mixed" else nv.HBG_FP64
     gpu = nv.solve(q, omegas, [20.0], kinds=kinds, symmetry=nv.SYM_BOTH, precision=prec)
     ref = O.solve_body(q, omegas, [20.0], kinds=kinds, symmetry=O.SYM_BOTH)
-    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= (MIXED_TOL if precision == "mixed" else FP64_TOL), errs
 
 
@@ -115,7 +115,7 @@ def test_gpu_sectors_two_bodies():
     gpu = nv.solve(sector, omegas, [0.0, 60.0], panel_body=body, rotation_centers=centers, symmetry=nv.SYM_YZ)
     ref = O.solve_body(sector, omegas, [0.0, 60.0], panel_body=body, centers=centers, symmetry=O.SYM_YZ)
     assert gpu["A"].shape == (2, 12, 12)
-    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X")}
+    errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= FP64_TOL, errs
 
 
@@ -158,7 +158,7 @@ def test_gpu_sectors_equal_the_whole_mesh_at_size():
     whole = nv.solve(O.mirror_sector(q, O.SYM_BOTH), omegas, heads, depth=5.0)
     for prec, tol in ((nv.HBG_FP64, 1e-9), (nv.HBG_MIXED, MIXED_TOL)):
         sec = nv.solve(q, omegas, heads, symmetry=nv.SYM_BOTH, depth=5.0, precision=prec)
-        errs = {k: scaled_error(sec[k], whole[k]) for k in ("A", "B", "X")}
+        errs = {k: scaled_error(sec[k], whole[k]) for k in ("A", "B", "X", "HK")}
         assert max(errs.values()) <= tol, (prec, errs)
 
 
