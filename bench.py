@@ -10,9 +10,8 @@ frequency) is larger than the 126 MB L2, so no L2 flush is needed between steps.
 
 Arms:
   (default)         this library, through its C ABI (hbg_solve_batch), precision --precision
-  --impl reference  the CPU restatement of the reference's path (oracle/, C + LAPACK) on the host
-                    cores, timed on a bounded sample of the same workload (statics + a few
-                    frequencies), scaled to the whole job.
+  --impl reference  the CPU restatement of the reference's path (oracle/, C + LAPACK) in its default
+                    (production) arithmetic on all the host cores, every step one whole job.
 
 Multi-GPU (torchrun): every rank solves its own copy of the job on its own GPU (independent
 (body, frequency) units, no collective on the data path: weak scaling); the step time is the max
@@ -160,45 +159,69 @@ def reduce_max(pg, values, device="cpu"):
     return [float(x) for x in t.cpu()]
 
 
-def cpu_reference(args, world, rank, pg):
-    """The reference's CPU path (the oracle restatement: C + LAPACK) on the host cores."""
-    if rank != 0:
-        return None
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count()
+
+
+def cpu_job(production=True):
+    """One whole job of the benchmark workload on the host cores by the CPU restatement of the reference
+    (oracle/: C with OpenMP over rows, LAPACK ?gesv through scipy's threaded OpenBLAS): statics once, then
+    every frequency -- no sampling.  production: the reference's default arithmetic (float32 Gauss tiers,
+    direct wave-kernel tables, float32 static rows, complex64 matrices and LU); otherwise its diagnostic
+    double path.  Returns (job seconds, statics seconds, mean seconds per frequency)."""
     from oracle import oracle as O
 
     v, omegas = workload()
     heads = np.radians(HEADINGS)
-    cores = os.cpu_count()
     O.lib()
-    sample_f = 2
-
-    def one_step():
-        t0 = time.perf_counter()
-        pan = O.make_panels(v)
+    t0 = time.perf_counter()
+    pan = O.make_panels(v)
+    with O.ProductionMode(production):
         st = O.statics(pan, None, DEPTH)
-        t1 = time.perf_counter()
-        for w in omegas[:: max(1, len(omegas) // sample_f)][:sample_f]:
-            O.solve_frequency(pan, None, st, DEPTH, w, heads)
-        t2 = time.perf_counter()
-        per_freq = (t2 - t1) / sample_f
-        return (t1 - t0) + len(omegas) * per_freq, t1 - t0, per_freq
+    t1 = time.perf_counter()
+    for w in omegas:
+        O.solve_frequency(pan, None, st, DEPTH, w, heads, production=production)
+    t2 = time.perf_counter()
+    return t2 - t0, t1 - t0, (t2 - t1) / len(omegas)
 
+
+def cpu_reference(args, world, rank, pg):
+    """The reference's CPU path in its default (production) arithmetic, restated in oracle/, on all the
+    host's cores: every step one whole job (statics + every frequency)."""
+    if rank != 0:
+        return None
+    cores = host_cores()
     for _ in range(min(args.warmup, 1)):
-        one_step()
-    times = [one_step() for _ in range(args.steps)]
+        cpu_job(True)
+    times = [cpu_job(True) for _ in range(args.steps)]
     job = float(np.mean([t[0] for t in times]))
-    value = len(omegas) / job
-    sample = (f"statics + {sample_f} of the {len(omegas)} frequencies per step, job time = statics + 40 x the "
-              f"mean per-frequency time (statics {np.mean([t[1] for t in times]):.2f} s, "
-              f"{np.mean([t[2] for t in times]):.2f} s per frequency)")
+    F = len(workload()[1])
+    value = F / job
+    sample = (f"the whole job every step: statics ({np.mean([t[1] for t in times]):.2f} s) + all {F} frequencies "
+              f"({np.mean([t[2] for t in times]):.3f} s each); {cores} threads on {cpu_model()}")
     line = {"metric": "freq solves/s at N=4096", "value": value, "unit": "freq solves/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": job * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": CASE_LABELS[CASE], "form": "FP64 (the reference's diagnostic double path)",
+            "steps": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": job * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c64+f32", "data": "synthetic",
+            "config": {"workload": CASE_LABELS[CASE],
+                       "form": "production (the reference's default path: float32 Gauss tiers, direct tables, "
+                               "complex64 LU)",
                        "l2": "inputs larger than L2"},
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "freq solves/s", "cores": cores, "kind": "port",
-                             "sample": sample},
+                             "mode": "production", "cpu": cpu_model(), "sample": sample},
             "e2e": {"value": value, "unit": "freq solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     return line
 
@@ -376,22 +399,17 @@ def surrogate_comparison(nv, v, omegas, device, plain, train_steps):
 
 
 def cpu_baseline_quick():
-    """The oracle on a bounded sample of the same workload (statics + 2 frequencies), scaled."""
-    from oracle import oracle as O
-
-    v, omegas = workload()
-    heads = np.radians(HEADINGS)
-    t0 = time.perf_counter()
-    pan = O.make_panels(v)
-    st = O.statics(pan, None, DEPTH)
-    t1 = time.perf_counter()
-    for w in (omegas[0], omegas[len(omegas) // 2]):
-        O.solve_frequency(pan, None, st, DEPTH, w, heads)
-    t2 = time.perf_counter()
-    per = (t2 - t1) / 2
-    job = (t1 - t0) + len(omegas) * per
-    return {"value": len(omegas) / job, "unit": "freq solves/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"statics ({t1 - t0:.2f} s) + 2 of 40 frequencies ({per:.2f} s each), scaled to the job"}
+    """The CPU restatement of the reference on one whole job (no sampling) in its default production
+    arithmetic, and beside it one whole job of its diagnostic double path (the FP64 form's semantics)."""
+    cores = host_cores()
+    job, st, per = cpu_job(True)
+    djob, dst, dper = cpu_job(False)
+    F = len(workload()[1])
+    return {"value": F / job, "unit": "freq solves/s", "cores": cores, "kind": "port", "mode": "production",
+            "cpu": cpu_model(),
+            "sample": f"one whole job: statics ({st:.2f} s) + all {F} frequencies ({per:.3f} s each)",
+            "diag_fp64": {"value": F / djob, "unit": "freq solves/s",
+                          "sample": f"one whole job: statics ({dst:.2f} s) + all {F} frequencies ({dper:.3f} s each)"}}
 
 
 def main():

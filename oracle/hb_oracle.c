@@ -35,6 +35,9 @@
 
 static double *T1D, *T2D, *T2DD, *TASY, *TMETA, *TQ, *TL0, *TBK;
 static double *tables_blob;
+static int g_prod; /* the reference's production arithmetic (hbo_set_production) */
+
+void hbo_set_production(int on) { g_prod = on != 0; }
 
 int hbo_load_tables(const char *path) {
     if (tables_blob) return 0;
@@ -275,6 +278,7 @@ static int make_one(const double *v12, int kind, hbo_panel *g) {
             sum += g->gw[3 * i + j];
         }
     for (int k = 0; k < 9; k++) g->gw[k] *= area / sum;
+    memcpy(g->q, q, sizeof q);
     return 0;
 }
 
@@ -289,12 +293,15 @@ int hbo_make_panels(int np, const double *verts, hbo_panel *out) {
 }
 
 /* ------------------------------------------------------------------ Rankine integrals */
-/* panel_integrals.rs:226-275 rankine(), diagnostic mode: closed forms within 1000 radii */
+/* panel_integrals.rs:226-275 rankine(): closed forms within 1000 radii (diagnostic mode) or FAR_RATIO =
+ * 12 radii (production), the 3 x 3 FP64 rule beyond */
+#define FAR_RATIO 12.0
+#define EXACT_RATIO 2.0
 static void rankine(const hbo_panel *p, const double *x, double *S, double *D) {
     double rc[3];
     sub3(x, p->c, rc);
     double dist = norm3(rc);
-    if (dist > 1000.0 * p->radius) {
+    if (dist > (g_prod ? FAR_RATIO : 1000.0) * p->radius) {
         double s = 0.0, dd = 0.0;
         for (int k = 0; k < 9; k++) {
             double r[3];
@@ -340,6 +347,85 @@ static void rankine(const hbo_panel *p, const double *x, double *S, double *D) {
 }
 
 void hbo_rankine(const hbo_panel *p, const double x[3], double out[2]) { rankine(p, x, &out[0], &out[1]); }
+
+/* The float32 Gauss tiers of the production path (panel_integrals.rs:190-216): for orders 3, 4, 5, 6 the
+ * n x n points of the bilinear map relative to the centroid and the weights scaled to the exact area,
+ * each block padded with zero weights to a multiple of 8 (lengths 16, 16, 32, 40). */
+#define TIER_FLOATS 416
+static const int TIER_OFF[4] = {0, 64, 128, 256}, TIER_LEN[4] = {16, 16, 32, 40};
+static void panel_tiers(const hbo_panel *p, float *tq) {
+    memset(tq, 0, sizeof(float) * TIER_FLOATS);
+    for (int t = 0; t < 4; t++) {
+        const int n = 3 + t, cnt = n * n, len = TIER_LEN[t];
+        float *b = tq + TIER_OFF[t];
+        double pts[36][3], ww[36], wsum = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) {
+                double jac;
+                bilinear((const double(*)[3])p->q, GL_X[n][i], GL_X[n][j], pts[i * n + j], &jac);
+                ww[i * n + j] = GL_W[n][i] * GL_W[n][j] * jac;
+                wsum += ww[i * n + j];
+            }
+        for (int k = 0; k < cnt; k++) {
+            b[k] = (float)(pts[k][0] - p->c[0]);
+            b[len + k] = (float)(pts[k][1] - p->c[1]);
+            b[2 * len + k] = (float)(pts[k][2] - p->c[2]);
+            b[3 * len + k] = (float)(ww[k] * p->area / wsum);
+        }
+    }
+}
+
+/* panel_integrals.rs:288-300 rankine_tier: 0 (order 3) beyond 8 radii, 1 (4) from 4, 2 (5) from 3,
+ * 3 (6) from 2, -1 (closed forms) within 2 */
+static inline int rankine_tier(double r) {
+    return r >= 8.0 ? 0 : r >= 4.0 ? 1 : r >= 3.0 ? 2 : r >= EXACT_RATIO ? 3 : -1;
+}
+
+/* panel_integrals.rs:305-357 rankine_gauss: the tier's rule in float32 on the point taken relative to the
+ * centroid in double, eight accumulator lanes summed in double */
+static void rankine_gauss(const hbo_panel *p, const float *tq, const double *x, int t, double *S, double *D) {
+    const int len = TIER_LEN[t];
+    const float *b = tq + TIER_OFF[t];
+    const float px = (float)(x[0] - p->c[0]), py = (float)(x[1] - p->c[1]), pz = (float)(x[2] - p->c[2]);
+    const float nx = (float)p->n[0], ny = (float)p->n[1], nz = (float)p->n[2];
+    float sacc[8] = {0}, dacc[8] = {0};
+    for (int k = 0; k < len; k += 8)
+        for (int l = 0; l < 8; l++) {
+            const float rx = px - b[k + l], ry = py - b[len + k + l], rz = pz - b[2 * len + k + l];
+            const float w = b[3 * len + k + l];
+            const float r2 = fmaf(rz, rz, fmaf(rx, rx, ry * ry));
+            const float ir = 1.0f / sqrtf(r2);
+            const float nr = fmaf(nz, rz, fmaf(nx, rx, ny * ry));
+            sacc[l] = fmaf(w, ir, sacc[l]);
+            dacc[l] = fmaf(w * nr, ir * (ir * ir), dacc[l]);
+        }
+    double s = 0.0, d = 0.0;
+    for (int l = 0; l < 8; l++) {
+        s += (double)sacc[l];
+        d += (double)dacc[l];
+    }
+    *S = s;
+    *D = d;
+}
+
+/* panel_integrals.rs:359-363 rankine_any: the tier rule, or the closed forms within 2 radii (the
+ * diagnostic mode: always the closed forms) */
+static void rankine_any(const hbo_panel *p, const float *tq, const double *x, double *S, double *D) {
+    double rc[3];
+    sub3(x, p->c, rc);
+    const int t = (g_prod && tq) ? rankine_tier(norm3(rc) / p->radius) : -1;
+    if (t < 0)
+        rankine(p, x, S, D);
+    else
+        rankine_gauss(p, tq, x, t, S, D);
+}
+
+void hbo_rankine_any(const hbo_panel *p, const double x[3], double out[2]) {
+    gl_init();
+    float tq[TIER_FLOATS];
+    panel_tiers(p, tq);
+    rankine_any(p, tq, x, &out[0], &out[1]);
+}
 
 /* panel_integrals.rs:281-286 psi_terms */
 static inline void psi_terms(const double *xi, const double *pp, const double *n, double *psi, double *dpsi) {
@@ -408,6 +494,18 @@ static void log_singularity(const hbo_panel *p, const double *image, double *L, 
     double t[3];
     sub3(image, p->c, t);
     double dist = norm3(t);
+    if (g_prod && dist > FAR_RATIO * p->radius) {  /* production: the 3 x 3 rule far away (380-392) */
+        double l = 0.0, ld = 0.0;
+        for (int k = 0; k < 9; k++) {
+            double psi, dpsi;
+            psi_terms(p->gx[k], image, p->n, &psi, &dpsi);
+            l += p->gw[k] * psi;
+            ld += p->gw[k] * dpsi;
+        }
+        *L = l;
+        *Ld = ld;
+        return;
+    }
     log_ctx c;
     panel_map(p, c.map);
     c.p = p;
@@ -481,9 +579,11 @@ static inline int log_pair(const hbo_panel *p, const double *x, double tol) {
     return d * d * tol < 0.6 * p->radius * p->radius;
 }
 
-/* lo_static.rs:59-119 static_row (field point x against every panel) */
+/* lo_static.rs:59-119 static_row (field point x against every panel); tiers: the panels' float32 Gauss
+ * tiers in the production mode (rankine_pair = rankine_any at the point and its free-surface image),
+ * NULL in the diagnostic mode */
 static void static_row(int N, const hbo_panel *pg, const int32_t *kind, const double *x, int logint, double tol,
-                       double depth, double *row) {
+                       double depth, const float *tiers, double *row) {
     int finite = isfinite(depth) && depth > 0.0;
     double xb[3] = {x[0], x[1], -x[2]};
     double xp[6][3];
@@ -495,14 +595,15 @@ static void static_row(int N, const hbo_panel *pg, const int32_t *kind, const do
     }
     for (int j = 0; j < N; j++) {
         const hbo_panel *p = pg + j;
+        const float *tq = tiers ? tiers + (size_t)j * TIER_FLOATS : NULL;
         double s0, d0, sb, db;
-        rankine(p, x, &s0, &d0);
-        rankine(p, xb, &sb, &db);
+        rankine_any(p, tq, x, &s0, &d0);
+        rankine_any(p, tq, xb, &sb, &db);
         double sr = s0 + sb, dr = d0 + db;
         if (finite) {
             double s2, d2, s4, d4, s5, d5, s6, d6;
-            rankine(p, xp[1], &s2, &d2);
-            rankine(p, xp[3], &s4, &d4);
+            rankine_any(p, tq, xp[1], &s2, &d2);
+            rankine_any(p, tq, xp[3], &s4, &d4);
             rankine(p, xp[4], &s5, &d5);
             rankine(p, xp[5], &s6, &d6);
             sr += (s2 + s4) + s5 + s6;
@@ -529,13 +630,23 @@ static void static_row(int N, const hbo_panel *pg, const int32_t *kind, const do
             e[2] = 0.0;
             e[3] = 0.0;
         }
+        if (tiers)  /* production: the static rows are stored in float32 */
+            for (int q = 0; q < 4; q++) e[q] = (double)(float)e[q];
     }
 }
 
 int hbo_statics(int N, const hbo_panel *pg, const int32_t *kind, double depth, int logint, double tol, double *out) {
     gl_init();
+    float *tiers = NULL;
+    if (g_prod) {
+        tiers = (float *)malloc(sizeof(float) * TIER_FLOATS * (size_t)(N > 0 ? N : 1));
+        if (!tiers) return 1;
+#pragma omp parallel for schedule(static)
+        for (int j = 0; j < N; j++) panel_tiers(pg + j, tiers + (size_t)j * TIER_FLOATS);
+    }
 #pragma omp parallel for schedule(dynamic, 4)
-    for (int k = 0; k < N; k++) static_row(N, pg, kind, pg[k].c, logint, tol, depth, out + (size_t)k * N * 4);
+    for (int k = 0; k < N; k++) static_row(N, pg, kind, pg[k].c, logint, tol, depth, tiers, out + (size_t)k * N * 4);
+    free(tiers);
     return 0;
 }
 
@@ -570,6 +681,25 @@ static void table2d(double X, double Y, double *v, double *vx) {
     }
     *v = s[0];
     *vx = s[1];
+}
+
+/* green_inf.rs:114-139 table2d_direct: the first nq of (F, F_X, c, c_X) (c = e^-Y J0) from the direct
+ * tables of the production path, X < XT, Y < YT */
+static void table2d_direct(double X, double Y, int nq, double *f) {
+    int ix = (int)X, iy = (int)Y;
+    double tx = 2.0 * (X - ix) - 1.0, ty = 2.0 * (Y - iy) - 1.0;
+    enum { M = N3 + 1 };
+    const double *c = T2DD + ((size_t)iy * XT + ix) * 4 * M * M;
+    for (int q = 0; q < nq; q++) {
+        const double *cq = c + q * M * M;
+        double r[M];
+        for (int a = 0; a < M; a++) r[a] = 0.0;
+        for (int j = M - 1; j >= 0; j--)
+            for (int a = 0; a < M; a++) r[a] = r[a] * tx + cq[j * M + a];
+        double sq = 0.0;
+        for (int a = M - 1; a >= 0; a--) sq = sq * ty + r[a];
+        f[q] = sq;
+    }
 }
 
 /* green_inf.rs:145-172 hankel01: (J0, Y0, J1, Y1) for x >= XT */
@@ -673,6 +803,18 @@ static void bessel_jy01(double X, double *j0, double *y0, double *j1, double *y1
  * out = F, FX, FY, I, IX, IY, c */
 void hbo_wave_kernel(double X, double Y, double *out) {
     double R0 = sqrt(X * X + Y * Y);
+    if (g_prod && X < XT && Y < YT && (X >= 2.0 || Y >= 2.0)) {  /* green_inf.rs:319-330 */
+        double f[4];
+        table2d_direct(X, Y, 4, f);
+        out[0] = f[0];
+        out[1] = f[1];
+        out[2] = -f[0] - 2.0 / R0;
+        out[6] = f[2];
+        out[3] = -2.0 * PI * f[2];
+        out[4] = 2.0 * PI * f[3];
+        out[5] = -out[3];
+        return;
+    }
     double eY = exp(-Y), j0, j1, F, FX;
     if (X < XT && Y < YT) {
         double f[4], v, vx;
@@ -709,10 +851,15 @@ void hbo_wave_kernel(double X, double Y, double *out) {
     out[5] = -out[3];
 }
 
-/* green_inf.rs:647-675 wave_real, diagnostic mode */
+/* green_inf.rs:657-675 wave_real (the direct tables first in the production mode) */
 static void wave_real(double X, double Y, double *F, double *FX, double *FY) {
     double R0 = sqrt(X * X + Y * Y);
-    if (Y >= YT) {
+    if (g_prod && X < XT && Y < YT && (X >= 2.0 || Y >= 2.0)) {
+        double f[2];
+        table2d_direct(X, Y, 2, f);
+        *F = f[0];
+        *FX = f[1];
+    } else if (Y >= YT) {
         double P, PX;
         far_series(X, Y, 0.0, &P, &PX);
         *F = -2.0 * P;
@@ -1221,8 +1368,31 @@ static void apply_kernel(const hbo_panel *p, int kindj, const double *st, const 
 /* lo_frequency.rs:74-84 free_term */
 static double free_term(int kind) { return kind == HBO_INTERIOR ? -4.0 * PI : 2.0 * PI; }
 
+static void put_entry(double *M, float *M32, size_t o, double re, double im) {
+    if (M32) {
+        M32[2 * o] = (float)re;
+        M32[2 * o + 1] = (float)im;
+    } else {
+        M[2 * o] = re;
+        M[2 * o + 1] = im;
+    }
+}
+
+static int assemble_into(int N, const hbo_panel *pg, const int32_t *kind, const double *statics, double depth,
+                         double omega, double grav, int logint, double *S, double *A, float *S32, float *A32);
+
 int hbo_assemble(int N, const hbo_panel *pg, const int32_t *kind, const double *statics, double depth, double omega,
                  double grav, int logint, double *S, double *A) {
+    return assemble_into(N, pg, kind, statics, depth, omega, grav, logint, S, A, NULL, NULL);
+}
+
+int hbo_assemble_c64(int N, const hbo_panel *pg, const int32_t *kind, const double *statics, double depth,
+                     double omega, double grav, int logint, float *S, float *A) {
+    return assemble_into(N, pg, kind, statics, depth, omega, grav, logint, NULL, NULL, S, A);
+}
+
+static int assemble_into(int N, const hbo_panel *pg, const int32_t *kind, const double *statics, double depth,
+                         double omega, double grav, int logint, double *S, double *A, float *S32, float *A32) {
     double K = omega * omega / grav;
     double logc = logint ? 1.0 : 0.0;
     int finite = isfinite(depth) && depth > 0.0;
@@ -1254,18 +1424,14 @@ int hbo_assemble(int N, const hbo_panel *pg, const int32_t *kind, const double *
             double s1[2], d1[2];
             apply_kernel(pg + n, kn, statics + ((size_t)k * N + n) * 4, xk, K, logc, w, R, 0, s1, d1);
             size_t o = (size_t)k + (size_t)n * N;
-            S[2 * o] = s1[0];
-            S[2 * o + 1] = s1[1];
-            A[2 * o] = (k == n ? free_term(kk) : 0.0) - d1[0];
-            A[2 * o + 1] = -d1[1];
+            put_entry(S, S32, o, s1[0], s1[1]);
+            put_entry(A, A32, o, (k == n ? free_term(kk) : 0.0) - d1[0], -d1[1]);
             if (n != k) {
                 double s2[2], d2[2];
                 apply_kernel(pg + k, kk, statics + ((size_t)n * N + k) * 4, xn, K, logc, w, R, 1, s2, d2);
                 size_t o2 = (size_t)n + (size_t)k * N;
-                S[2 * o2] = s2[0];
-                S[2 * o2 + 1] = s2[1];
-                A[2 * o2] = -d2[0];
-                A[2 * o2 + 1] = -d2[1];
+                put_entry(S, S32, o2, s2[0], s2[1]);
+                put_entry(A, A32, o2, -d2[0], -d2[1]);
             }
         }
     }
@@ -1295,7 +1461,7 @@ int hbo_field_influence(int N, const hbo_panel *pg, const int32_t *kind, int P, 
     for (int p = 0; p < P; p++) {
         const double *x = pts + 3 * p;
         double *row = (double *)malloc(sizeof(double) * 4 * N);
-        static_row(N, pg, kind, x, logint, tol, depth, row);
+        static_row(N, pg, kind, x, logint, tol, depth, NULL, row);
         finpoint fx;
         if (finite) fin_point(fd, x[2], &fx);
         for (int j = 0; j < N; j++) {

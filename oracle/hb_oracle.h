@@ -29,12 +29,22 @@ typedef struct hbo_panel {
     double em[4][3];     /* outward in-plane unit normals of the edges */
     double gx[9][3];     /* 3 x 3 Gauss points of the bilinear map of the projected vertices */
     double gw[9];
+    double q[4][3];      /* the projected vertices as given (a repeated vertex kept): the bilinear map */
 } hbo_panel;
 
 /* surface kinds (low_order.rs:224-238): only these two reach the configs' route */
 enum { HBO_WET = 0, HBO_INTERIOR = 1 };
 
 int hbo_load_tables(const char *path);                      /* 0 ok, else error */
+
+/* Arithmetic of the reference's default (production) path instead of its diagnostic double path
+ * (HB_DIAG_DOUBLE off, crates/hydrobem/src/env_hooks.rs:51-56), process-wide until switched back:
+ * Rankine integrals by float32 Gauss tiers of orders 6, 5, 4, 3 from 2 to 3, 4, 8 and beyond 8 panel
+ * radii (panel_integrals.rs:288-363) and by the 3 x 3 FP64 rule beyond 12 radii where the closed forms
+ * are called directly (229-240); the log-singularity integral by the 3 x 3 rule beyond 12 radii
+ * (380-392); the wave kernel from the direct 2-D tables outside [0, 2)^2 (green_inf.rs:316-330,
+ * 661-667); static rows rounded to float32 (lo_static.rs:59-119 with R = f32).  0: diagnostic. */
+void hbo_set_production(int on);
 
 /* geometry.rs:120-199 make_panel + panel_integrals.rs:145-217 make_panel_geom.
  * Returns 0, or 1 + index of the first invalid panel. */
@@ -49,6 +59,9 @@ double hbo_dispersion_xn(double H, int n);
 /* mode: 0 ordinary, 1 omega = 0, 2 omega = inf.  out: Wr WrR WrZ Wrz Wi WiR WiZ Wiz */
 void hbo_finite_kernel(double h, double K, int mode, double R, double z, double zeta, double out[8]);
 void hbo_rankine(const hbo_panel *p, const double x[3], double out[2]);
+/* the rule the static rows use at x: the float32 Gauss tier by distance in the production mode
+ * (panel_integrals.rs:359-363 rankine_any), the closed forms otherwise */
+void hbo_rankine_any(const hbo_panel *p, const double x[3], double out[2]);
 void hbo_log_singularity(const hbo_panel *p, const double image[3], double out[2]);
 double hbo_log_in_plane(const hbo_panel *p, const double x[3]);
 
@@ -60,6 +73,11 @@ int hbo_statics(int N, const hbo_panel *pg, const int32_t *kind, double depth, i
  * (lo_frequency.rs:276-537 with G = 1). depth <= 0 or inf: infinite depth. */
 int hbo_assemble(int N, const hbo_panel *pg, const int32_t *kind, const double *statics, double depth,
                  double omega, double grav, int logint, double *S, double *A);
+
+/* the same with S and A stored as complex64 (the production path's matrices, lo_frequency.rs:1-6: f64
+ * kernels, f32 storage) */
+int hbo_assemble_c64(int N, const hbo_panel *pg, const int32_t *kind, const double *statics, double depth,
+                     double omega, double grav, int logint, float *S, float *A);
 
 /* the influence rows of P field points: (S, D column) of every panel at every point, [P][N] complex */
 int hbo_field_influence(int N, const hbo_panel *pg, const int32_t *kind, int P, const double *pts, double depth,

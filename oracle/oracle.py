@@ -54,6 +54,7 @@ class Panel(ctypes.Structure):
         ("em", ctypes.c_double * 12),
         ("gx", ctypes.c_double * 27),
         ("gw", ctypes.c_double * 9),
+        ("q", ctypes.c_double * 12),
     ]
 
 
@@ -76,6 +77,7 @@ def lib():
     ip = ctypes.POINTER(ctypes.c_int32)
     pp = ctypes.POINTER(Panel)
     L.hbo_load_tables.argtypes = [ctypes.c_char_p]
+    L.hbo_set_production.argtypes = [ctypes.c_int]
     L.hbo_make_panels_kinds.argtypes = [ctypes.c_int, dp, ip, pp]
     L.hbo_wave_kernel.argtypes = [ctypes.c_double, ctypes.c_double, dp]
     L.hbo_dispersion_x0.argtypes = [ctypes.c_double]
@@ -84,12 +86,16 @@ def lib():
     L.hbo_dispersion_xn.restype = ctypes.c_double
     L.hbo_finite_kernel.argtypes = [ctypes.c_double] * 2 + [ctypes.c_int] + [ctypes.c_double] * 3 + [dp]
     L.hbo_rankine.argtypes = [pp, dp, dp]
+    L.hbo_rankine_any.argtypes = [pp, dp, dp]
     L.hbo_log_singularity.argtypes = [pp, dp, dp]
     L.hbo_log_in_plane.argtypes = [pp, dp]
     L.hbo_log_in_plane.restype = ctypes.c_double
     L.hbo_statics.argtypes = [ctypes.c_int, pp, ip, ctypes.c_double, ctypes.c_int, ctypes.c_double, dp]
     L.hbo_assemble.argtypes = [ctypes.c_int, pp, ip, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                ctypes.c_int, dp, dp]
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.hbo_assemble_c64.argtypes = [ctypes.c_int, pp, ip, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_int, fp, fp]
     L.hbo_wavenumber.argtypes = [ctypes.c_double] * 3
     L.hbo_wavenumber.restype = ctypes.c_double
     L.hbo_field_influence.argtypes = [ctypes.c_int, pp, ip, ctypes.c_int, dp, ctypes.c_double, ctypes.c_double,
@@ -157,6 +163,13 @@ def rankine(panel, x):
     return out
 
 
+def rankine_any(panel, x):
+    out = np.zeros(2)
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    lib().hbo_rankine_any(ctypes.byref(panel), _dp(xx), _dp(out))
+    return out
+
+
 def log_singularity(panel, image):
     out = np.zeros(2)
     xx = np.ascontiguousarray(image, dtype=np.float64)
@@ -173,17 +186,36 @@ def statics(panels, kinds, depth, logint=True, tol=1e-4) -> np.ndarray:
     return out
 
 
-def assemble(panels, kinds, st, depth, omega, grav=GRAVITY, logint=True):
-    """(S, A) complex128 N x N (entry [k, n]) of one ordinary frequency."""
+def assemble(panels, kinds, st, depth, omega, grav=GRAVITY, logint=True, dtype=np.complex128):
+    """(S, A) N x N (entry [k, n], Fortran order) of one ordinary frequency, complex128 or (the production
+    path's storage) complex64."""
     n = len(panels)
-    S = np.zeros((n, n), dtype=np.complex128, order="F")
-    A = np.zeros((n, n), dtype=np.complex128, order="F")
+    S = np.empty((n, n), dtype=dtype, order="F")
+    A = np.empty((n, n), dtype=dtype, order="F")
     k = np.zeros(n, np.int32) if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
     d = depth if (depth is not None and np.isfinite(depth) and depth > 0) else np.inf
-    lib().hbo_assemble(n, panels, _ip(k), _dp(st), d, omega, grav, int(logint),
-                       S.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                       A.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    if np.dtype(dtype) == np.complex64:
+        fp = ctypes.POINTER(ctypes.c_float)
+        lib().hbo_assemble_c64(n, panels, _ip(k), _dp(st), d, omega, grav, int(logint),
+                               S.ctypes.data_as(fp), A.ctypes.data_as(fp))
+    else:
+        lib().hbo_assemble(n, panels, _ip(k), _dp(st), d, omega, grav, int(logint),
+                           S.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                           A.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
     return S, A
+
+
+def lu_solve(A, B):
+    """A X = B by LAPACK ?gesv (LU with partial pivoting; scipy's threaded OpenBLAS: cgesv for complex64,
+    zgesv for complex128), standing in for faer's blocked LU (linalg.rs:134-252, 321-354).  A is
+    overwritten when it is a Fortran-ordered array of the solve's type."""
+    from scipy.linalg import lapack
+
+    gesv = lapack.cgesv if A.dtype == np.complex64 else lapack.zgesv
+    lu, piv, x, info = gesv(A, np.asarray(B, dtype=A.dtype), overwrite_a=True, overwrite_b=False)
+    if info != 0:
+        raise np.linalg.LinAlgError(f"singular matrix (?gesv info {info})")
+    return x
 
 
 # ------------------------------------------------------------------ one frequency
@@ -249,6 +281,23 @@ def mirror_sector(verts, symmetry):
     return np.concatenate(out)
 
 
+class ProductionMode:
+    """Context in which the oracle computes the reference's default (production) arithmetic instead of
+    its diagnostic double path: float32 Gauss tiers for the Rankine integrals, the direct 2-D tables of
+    the wave kernel, float32 static rows (hbo_set_production), and -- in solve_frequency -- complex64
+    matrices, right-hand sides and LU (LAPACK cgesv through numpy; linalg.rs:321-354 with R = f32)."""
+
+    def __init__(self, on=True):
+        self.on = bool(on)
+
+    def __enter__(self):
+        lib().hbo_set_production(int(self.on))
+        return self
+
+    def __exit__(self, *a):
+        lib().hbo_set_production(0)
+
+
 def sector_solve(S, A, u, G):
     """phi on every panel of the mirrored mesh from the G sector systems (lo_frequency.rs:823-943): for
     character c, S_c and A_c the sums over g of chi_c(g) times the column block g of the sector rows,
@@ -260,19 +309,26 @@ def sector_solve(S, A, u, G):
         Sc = sum(character(c, g) * blk(S, g) for g in range(G))
         Ac = sum(character(c, g) * blk(A, g) for g in range(G))
         Uc = sum(character(c, g) * u[g * Ns:(g + 1) * Ns] for g in range(G)) / G
-        xc = np.linalg.solve(Ac, Sc @ (-Uc))
+        xc = lu_solve(np.asfortranarray(Ac), Sc @ (-Uc))
         for g in range(G):
             phi[g * Ns:(g + 1) * Ns] += character(c, g) * xc
     return phi
 
 
 def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY, rho=DENSITY, logint=True,
-                    want_matrices=False, panel_body=None, centers=None, sectors=1, points=None, tol=1e-4):
+                    want_matrices=False, panel_body=None, centers=None, sectors=1, points=None, tol=1e-4,
+                    production=False):
     """A, B [D][D], X, FK, SC, HK [H][D] of one frequency (D = 6 per body), all in float64 (complex128).
-    sectors > 1: the panels are a mirrored mesh (mirror_sector) solved by its symmetry sectors."""
+    sectors > 1: the panels are a mirrored mesh (mirror_sector) solved by its symmetry sectors.
+    production: the reference's default path (class production) -- statics computed in that mode are
+    expected; the matrices, right-hand sides and LU in complex64, the forces summed in float64."""
     c, n, area = panel_arrays(panels)
     N = len(panels)
-    S, A = assemble(panels, kinds, st, depth, omega, grav, logint)
+    with ProductionMode(production):
+        S, A = assemble(panels, kinds, st, depth, omega, grav, logint,
+                        dtype=np.complex64 if production else np.complex128)
+    if want_matrices:
+        A0 = A.copy()
     k = lib().hbo_wavenumber(omega, depth if depth else np.inf, grav)
     wet = np.ones(N, bool) if kinds is None else (np.asarray(kinds) == WET)
     nj = rigid_normals(c, n, kinds, panel_body, centers)
@@ -288,8 +344,9 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
         d = (gr * n).sum(axis=1)
         dphiI[h] = d
         u[:, D + h] = np.where(wet, -d, 0.0)
-    rhs = S @ (-u)
-    phi = np.linalg.solve(A, rhs) if sectors == 1 else sector_solve(S, A, u, sectors)
+    uu = u.astype(S.dtype)
+    rhs = S @ (-uu)
+    phi = (lu_solve(A, rhs) if sectors == 1 else sector_solve(S, A, uu, sectors)).astype(np.complex128)
     w = (nj * area[:, None]) * wet[:, None]          # n_i A_j on the body panels
     z = -rho * (w.T @ phi[:, :D])                    # [i][c]
     out = {"A": z.real, "B": -omega * z.imag}
@@ -307,7 +364,7 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
     if points is not None and len(points):
         out.update(field_values(panels, kinds, points, depth, omega, headings_rad, phi, u, phiI, D, grav, logint, tol))
     if want_matrices:
-        out["S"], out["Amat"], out["rhs"], out["phi"] = S, A, rhs, phi
+        out["S"], out["Amat"], out["rhs"], out["phi"] = S, A0, rhs, phi
     return out
 
 
@@ -451,7 +508,8 @@ def motions(A, B, X, omega, M, C, Bx):
 
 
 def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GRAVITY, rho=DENSITY, logint=True,
-               tol=1e-4, panel_body=None, centers=None, symmetry=SYM_NONE, rigid=None, points=None):
+               tol=1e-4, panel_body=None, centers=None, symmetry=SYM_NONE, rigid=None, points=None,
+               production=False):
     """The whole path for one problem: statics once, then every frequency. Arrays [F][D][D], [F][H][D]
     (D = 6 per body; interacting bodies by panel_body and their rotation centers).  With symmetry the
     panels (and kinds, panel_body) are one sector: mirrored, then solved by sectors."""
@@ -461,10 +519,12 @@ def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GR
         kinds = None if kinds is None else np.tile(np.asarray(kinds), G)
         panel_body = None if panel_body is None else np.tile(np.asarray(panel_body), G)
     panels = make_panels(verts, kinds)
-    st = statics(panels, kinds, depth, logint, tol)
+    with ProductionMode(production):
+        st = statics(panels, kinds, depth, logint, tol)
     heads = np.radians(np.asarray(headings_deg, dtype=float))
     res = [solve_frequency(panels, kinds, st, depth, w, heads, grav, rho, logint, panel_body=panel_body,
-                           centers=centers, sectors=G, points=points, tol=tol) for w in omegas]
+                           centers=centers, sectors=G, points=points, tol=tol, production=production)
+           for w in omegas]
     out = {k: np.array([r[k] for r in res]) for k in res[0]}
     c, n, area = panel_arrays(panels)
     recs, M, C, Bx = hydrostatics(c, n, area, kinds, panel_body, centers, rho, grav, rigid)
