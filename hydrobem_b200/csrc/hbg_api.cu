@@ -1185,6 +1185,53 @@ extern "C" HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const f
     }
 }
 
+extern "C" HbStatus hbg_debug_lu_f64(int32_t n, int32_t batch, const double* A, int32_t nrhs, const double* B,
+                                     double* X) {
+    try {
+        if (!A || !B || !X) return fail({HB_ERR_ARGUMENT, "null argument"});
+        if (n <= 0 || batch <= 0 || nrhs <= 0 || nrhs > 32) return fail({HB_ERR_VALUE, "debug LU: n, batch > 0, 0 < nrhs <= 32"});
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            return fail({HB_ERR_UNSUPPORTED, "no CUDA device: this library runs the path on the GPU only"});
+        device_ctx(0);
+        const size_t NN = (size_t)n * n, nb = (size_t)nrhs * n;
+        double2 *dA = nullptr, *dB = nullptr, *dX = nullptr;
+        int32_t *dp = nullptr, *di = nullptr;
+        auto release = [&]() {
+            cudaFree(dA);
+            cudaFree(dB);
+            cudaFree(dX);
+            cudaFree(dp);
+            cudaFree(di);
+        };
+        if (cudaMalloc(&dA, sizeof(double2) * NN * batch) != cudaSuccess ||
+            cudaMalloc(&dB, sizeof(double2) * nb * batch) != cudaSuccess ||
+            cudaMalloc(&dX, sizeof(double2) * nb * batch) != cudaSuccess ||
+            cudaMalloc(&dp, sizeof(int32_t) * (size_t)n * batch) != cudaSuccess ||
+            cudaMalloc(&di, sizeof(int32_t) * batch) != cudaSuccess) {
+            release();
+            return fail({HB_ERR_INTERNAL, "device memory allocation failed"});
+        }
+        cudaStream_t s = nullptr;
+        cudaMemcpy(dA, A, sizeof(double2) * NN * batch, cudaMemcpyHostToDevice);
+        cudaMemcpy(dB, B, sizeof(double2) * nb * batch, cudaMemcpyHostToDevice);
+        int64_t launches = 0;
+        lu_factor_f64(n, batch, dA, NN, dp, di, s, &launches);
+        lu_solve_f64(n, batch, dA, NN, dp, nrhs, dB, dX, s);
+        std::vector<int32_t> info(batch);
+        cudaMemcpy(info.data(), di, sizeof(int32_t) * batch, cudaMemcpyDeviceToHost);
+        cudaMemcpy(X, dX, sizeof(double2) * nb * batch, cudaMemcpyDeviceToHost);
+        const cudaError_t e = cudaGetLastError();
+        release();
+        if (e != cudaSuccess) return fail({HB_ERR_INTERNAL, std::string("CUDA: ") + cudaGetErrorString(e)});
+        for (int f = 0; f < batch; f++)
+            if (info[f]) return fail({HB_ERR_NUMERICAL, "singular matrix (zero pivot " + std::to_string(info[f]) + ")"});
+        return HB_OK;
+    } catch (const Failure& f) {
+        return fail(f);
+    }
+}
+
 static int current_device_ready() {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)

@@ -10,220 +10,395 @@
 
 namespace hbg {
 
-constexpr int NB = 32;  // panel width
-
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
 
-// Panel k0..k0+nb-1, rows k0..N-1, one block per matrix: for each column the pivot (largest
-// modulus, first index on a tie), the row swap inside the panel, the scaled column and the
-// rank-1 update of the panel's remaining columns.
-__global__ void __launch_bounds__(1024) k_panel_f64(int N, int k0, int nb, double2* __restrict__ Aall, size_t stride,
-                                                    int32_t* __restrict__ ipiv, int32_t* __restrict__ info) {
+// Blocking of the factorization: panels of LU_NB columns, each factored recursively (halves) down to
+// strips of at most LU_BASE columns; the matrices of a batch in LU_F64_GROUPS groups on side streams,
+// so that one group's strips (one CTA per matrix) run beside the other groups' trailing updates.
+constexpr int LU_NB = 128;
+constexpr int LU_BASE = 8;
+constexpr int LU_F64_GROUPS = 4;
+
+// ------------------------------------------------------------------ base strip
+// Columns c0 .. c0 + w - 1 (w <= LU_BASE), rows c0 .. N - 1, one CTA per matrix: for each column the
+// pivot (largest modulus, first index on a tie: LAPACK's izamax), the swap of the two rows inside the
+// strip, the column scaled by the pivot and the rank-1 update of the strip's remaining columns.  The
+// candidates of the next column's pivot are taken while its entries are updated (one pass a column).
+__global__ void __launch_bounds__(512) k_lu_base(int N, int c0, int w, double2* __restrict__ Aall, size_t stride,
+                                                 int32_t* __restrict__ ipiv, int32_t* __restrict__ info) {
     __shared__ double sval[32];
     __shared__ int sidx[32];
-    __shared__ double2 prow[NB];
+    __shared__ double2 prow[LU_BASE];
     __shared__ int spiv;
     const int f = blockIdx.x;
     double2* A = Aall + (size_t)f * stride;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int j = 0; j < nb; j++) {
-        const int col = k0 + j;
-        double best = -1.0;
-        int bi = col;
-        for (int i = col + threadIdx.x; i < N; i += blockDim.x) {
-            double v = cabs2(A[(size_t)i + (size_t)col * N]);
-            if (v > best) {
-                best = v;
-                bi = i;
-            }
-        }
+    double best = -1.0;
+    int bi = N;
+    for (int i = c0 + threadIdx.x; i < N; i += blockDim.x) {
+        const double v = cabs2(A[(size_t)i + (size_t)c0 * N]);
+        if (v > best) best = v, bi = i;
+    }
+    for (int j = 0; j < w; j++) {
+        const int col = c0 + j;
         for (int o = 16; o > 0; o >>= 1) {
-            double ov = __shfl_down_sync(0xffffffffu, best, o);
-            int oi = __shfl_down_sync(0xffffffffu, bi, o);
-            if (ov > best || (ov == best && oi < bi)) {
-                best = ov;
-                bi = oi;
-            }
+            const double ov = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) best = ov, bi = oi;
         }
-        if (lane == 0) {
-            sval[warp] = best;
-            sidx[warp] = bi;
-        }
+        if (lane == 0) sval[warp] = best, sidx[warp] = bi;
         __syncthreads();
         if (warp == 0) {
             best = lane < nw ? sval[lane] : -1.0;
             bi = lane < nw ? sidx[lane] : N;
             for (int o = 16; o > 0; o >>= 1) {
-                double ov = __shfl_down_sync(0xffffffffu, best, o);
-                int oi = __shfl_down_sync(0xffffffffu, bi, o);
-                if (ov > best || (ov == best && oi < bi)) {
-                    best = ov;
-                    bi = oi;
-                }
+                const double ov = __shfl_down_sync(0xffffffffu, best, o);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi)) best = ov, bi = oi;
             }
             if (lane == 0) {
-                spiv = bi;
-                ipiv[(size_t)f * N + col] = bi;
+                const int p = bi < N ? bi : col;
+                spiv = p;
+                ipiv[(size_t)f * N + col] = p;
                 if (!(best > 0.0) && info[f] == 0) info[f] = col + 1;
             }
         }
         __syncthreads();
         const int p = spiv;
-        // swap rows col and p in the panel's columns; keep the pivot row in shared memory
-        for (int c = threadIdx.x; c < nb; c += blockDim.x) {
-            size_t a = (size_t)col + (size_t)(k0 + c) * N, b = (size_t)p + (size_t)(k0 + c) * N;
-            double2 va = A[a], vb = A[b];
+        if (threadIdx.x < w) {  // swap rows col and p inside the strip; the pivot row to shared memory
+            const size_t a = (size_t)col + (size_t)(c0 + threadIdx.x) * N, b = (size_t)p + (size_t)(c0 + threadIdx.x) * N;
+            const double2 va = A[a], vb = A[b];
             if (p != col) {
                 A[a] = vb;
                 A[b] = va;
             }
-            prow[c] = vb;
+            prow[threadIdx.x] = vb;
         }
         __syncthreads();
-        double2 piv = prow[j];
-        double d = cabs2(piv);
-        double2 inv = d > 0.0 ? make_double2(piv.x / d, -piv.y / d) : make_double2(0.0, 0.0);
+        const double2 piv = prow[j];
+        const double d = cabs2(piv);
+        const double2 inv = d > 0.0 ? make_double2(piv.x / d, -piv.y / d) : make_double2(0.0, 0.0);
+        best = -1.0;
+        bi = N;
         for (int i = col + 1 + threadIdx.x; i < N; i += blockDim.x) {
-            double2 l = cmul(A[(size_t)i + (size_t)col * N], inv);
+            // the row's entries loaded together (independent reads in flight), then updated and stored
+            double2 v[LU_BASE];
+            const double2 a = A[(size_t)i + (size_t)col * N];
+#pragma unroll
+            for (int c = 0; c < LU_BASE; c++)
+                if (c > j && c < w) v[c] = A[(size_t)i + (size_t)(c0 + c) * N];
+            const double2 l = cmul(a, inv);
             A[(size_t)i + (size_t)col * N] = l;
-            for (int c = j + 1; c < nb; c++) {
-                size_t o = (size_t)i + (size_t)(k0 + c) * N;
-                A[o] = csub(A[o], cmul(l, prow[c]));
-            }
-        }
-        __syncthreads();
-    }
-}
-
-// The panel's row swaps on every column outside it (one thread per column).
-__global__ void k_laswp_f64(int N, int k0, int nb, double2* __restrict__ Aall, size_t stride,
-                            const int32_t* __restrict__ ipiv) {
-    const int f = blockIdx.y;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= N - nb) return;
-    if (c >= k0) c += nb;
-    double2* A = Aall + (size_t)f * stride + (size_t)c * N;
-    const int32_t* pv = ipiv + (size_t)f * N;
-    for (int j = 0; j < nb; j++) {
-        int r = k0 + j, p = pv[r];
-        if (p != r) {
-            double2 t = A[r];
-            A[r] = A[p];
-            A[p] = t;
-        }
-    }
-}
-
-// U12 = L11^-1 A12: one warp per column right of the panel, lane i holding row k0 + i.
-__global__ void k_trsm_f64(int N, int k0, int nb, double2* __restrict__ Aall, size_t stride) {
-    __shared__ double2 L[NB][NB + 1];
-    const int f = blockIdx.y;
-    double2* A = Aall + (size_t)f * stride;
-    for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) {
-        int r = t % nb, c = t / nb;
-        L[r][c] = A[(size_t)(k0 + r) + (size_t)(k0 + c) * N];
-    }
-    __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const int col = k0 + nb + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (col >= N) return;
-    double2 x = lane < nb ? A[(size_t)(k0 + lane) + (size_t)col * N] : make_double2(0.0, 0.0);
-    for (int p = 0; p < nb; p++) {
-        double2 xp = make_double2(__shfl_sync(0xffffffffu, x.x, p), __shfl_sync(0xffffffffu, x.y, p));
-        if (lane > p && lane < nb) x = csub(x, cmul(L[lane][p], xp));
-    }
-    if (lane < nb) A[(size_t)(k0 + lane) + (size_t)col * N] = x;
-}
-
-// Trailing update C -= L21 U12 (K = nb), 64 x 64 tiles, 256 threads of 4 x 4 complex each, the
-// K dimension staged through shared memory in chunks of 16.
-__global__ void __launch_bounds__(256) k_gemm_update_f64(int N, int k0, int nb, double2* __restrict__ Aall,
-                                                        size_t stride) {
-    constexpr int KC = 16;
-    __shared__ double2 As[KC][64];
-    __shared__ double2 Bs[KC][64 + 1];
-    const int f = blockIdx.z;
-    double2* A = Aall + (size_t)f * stride;
-    const int r0 = k0 + nb + blockIdx.x * 64, c0 = k0 + nb + blockIdx.y * 64;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    double2 acc[4][4];
 #pragma unroll
-    for (int a = 0; a < 4; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = make_double2(0.0, 0.0);
-    for (int kc = 0; kc < nb; kc += KC) {
-        const int kn = min(KC, nb - kc);
-        __syncthreads();
-        for (int t = threadIdx.x; t < 64 * KC; t += 256) {
-            int r = t & 63, kk = t >> 6;
-            As[kk][r] = (kk < kn && r0 + r < N) ? A[(size_t)(r0 + r) + (size_t)(k0 + kc + kk) * N] : make_double2(0.0, 0.0);
-            int kb = t % KC, cc = t / KC;
-            Bs[kb][cc] = (kb < kn && c0 + cc < N) ? A[(size_t)(k0 + kc + kb) + (size_t)(c0 + cc) * N] : make_double2(0.0, 0.0);
-        }
-        __syncthreads();
-#pragma unroll 4
-        for (int kk = 0; kk < KC; kk++) {
-            double2 av[4], bv[4];
-#pragma unroll
-            for (int a = 0; a < 4; a++) av[a] = As[kk][tx + 16 * a];
-#pragma unroll
-            for (int b = 0; b < 4; b++) bv[b] = Bs[kk][ty + 16 * b];
-#pragma unroll
-            for (int a = 0; a < 4; a++)
-#pragma unroll
-                for (int b = 0; b < 4; b++) {
-                    acc[a][b].x += av[a].x * bv[b].x - av[a].y * bv[b].y;
-                    acc[a][b].y += av[a].x * bv[b].y + av[a].y * bv[b].x;
+            for (int c = 0; c < LU_BASE; c++)
+                if (c > j && c < w) {
+                    v[c] = csub(v[c], cmul(l, prow[c]));
+                    A[(size_t)i + (size_t)(c0 + c) * N] = v[c];
+                    if (c == j + 1) {
+                        const double m = cabs2(v[c]);
+                        if (m > best) best = m, bi = i;
+                    }
                 }
         }
     }
-#pragma unroll
-    for (int b = 0; b < 4; b++) {
-        int c = c0 + ty + 16 * b;
-        if (c >= N) continue;
-#pragma unroll
-        for (int a = 0; a < 4; a++) {
-            int r = r0 + tx + 16 * a;
-            if (r < N) {
-                size_t o = (size_t)r + (size_t)c * N;
-                A[o] = csub(A[o], acc[a][b]);
-            }
+}
+
+// ------------------------------------------------------------------ row interchanges
+// The swaps of rows r0 .. r1 - 1 (in order, LAPACK's zlaswp) on the columns [ca, cb) and [cc, cd), one
+// thread per column.
+__global__ void k_lu_laswp(int N, int r0, int r1, int ca, int cb, int cc, int cd, double2* __restrict__ Aall,
+                           size_t stride, const int32_t* __restrict__ ipiv) {
+    const int f = blockIdx.y;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, n1 = cb - ca;
+    if (t >= n1 + (cd - cc)) return;
+    const int col = t < n1 ? ca + t : cc + (t - n1);
+    double2* A = Aall + (size_t)f * stride + (size_t)col * N;
+    const int32_t* pv = ipiv + (size_t)f * N;
+    for (int r = r0; r < r1; r++) {
+        const int p = pv[r];
+        if (p != r) {
+            const double2 x = A[r];
+            A[r] = A[p];
+            A[p] = x;
         }
     }
 }
 
+// ------------------------------------------------------------------ triangular solve of a block row
+// B := L^-1 B for the unit lower n1 x n1 block L at (c0, c0) and B the rows c0 .. c0 + n1 - 1, columns
+// [cb, ce): L's strictly lower part packed by columns in shared memory (column p: rows p + 1 .. n1 - 1),
+// a warp per column of B, lane l holding rows l, l + 32, ... (NQ of them), each solved entry broadcast
+// by shuffles.
+template <int NQ>
+__global__ void __launch_bounds__(1024) k_lu_trsm(int N, int c0, int n1, int cb, int ce, double2* __restrict__ Aall,
+                                                  size_t stride) {
+    extern __shared__ double2 Lc[];
+    const int f = blockIdx.y;
+    double2* A = Aall + (size_t)f * stride;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    auto off = [n1](int p) { return p * (2 * n1 - p - 1) / 2; };
+    for (int p = warp; p < n1 - 1; p += nw)
+        for (int r = p + 1 + lane; r < n1; r += 32) Lc[off(p) + r - p - 1] = A[(size_t)(c0 + r) + (size_t)(c0 + p) * N];
+    __syncthreads();
+    for (int col = cb + blockIdx.x * nw + warp; col < ce; col += gridDim.x * nw) {
+        double2 x[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            const int r = lane + 32 * q;
+            x[q] = r < n1 ? A[(size_t)(c0 + r) + (size_t)col * N] : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int sblk = 0; sblk < NQ; sblk++) {
+            for (int pp = 0; pp < 32; pp++) {
+                const int p = 32 * sblk + pp;
+                if (p >= n1 - 1) break;
+                const double2 xp = make_double2(__shfl_sync(0xffffffffu, x[sblk].x, pp),
+                                                __shfl_sync(0xffffffffu, x[sblk].y, pp));
+                const int base = off(p) - p - 1;  // L(r, p) at base + r
+#pragma unroll
+                for (int q = sblk; q < NQ; q++) {
+                    const int r = lane + 32 * q;
+                    if (r > p && r < n1) x[q] = csub(x[q], cmul(Lc[base + r], xp));
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+            const int r = lane + 32 * q;
+            if (r < n1) A[(size_t)(c0 + r) + (size_t)col * N] = x[q];
+        }
+    }
+}
+
+// ------------------------------------------------------------------ trailing update on FP64 warp MMA
+// C -= A B inside one matrix of the batch (C rows r0 .., columns c0 ..; A rows r0 .., columns k0 ..
+// k0 + K; B rows k0 .. k0 + K, columns c0 ..), complex128 column-major.  The complex product as a real
+// one on the interleaved (re, im) layout: C_r (2M x n) -= Ahat (2M x 2K) B_r (2K x n), where B_r and C_r
+// are the matrices' own memory read as doubles and Ahat(2r + c, 2k + c') is a_r, -a_i, a_i, a_r for
+// (c, c') = (0, 0), (0, 1), (1, 0), (1, 1), read on the fly from A's interleaved tile.  Tiles of 64 x 64
+// complex per CTA, eight warps of 32 real rows x 32 columns (4 x 4 m8n8k4 f64 tiles each), K staged by
+// cp.async in chunks of 16 complex (double-buffered, zero-filled beyond the edges), the sum subtracted
+// from C in place.
+constexpr int ZG_M = 64, ZG_N = 64, ZG_K = 16;
+constexpr int ZG_AP = 2 * ZG_M + 8;  // doubles per k-column of the A tile (padded: conflict-free fragments)
+constexpr int ZG_BP = 2 * ZG_K + 4;  // doubles per column of the B tile
+constexpr int ZG_SMEM = (2 * ZG_K * ZG_AP + 2 * ZG_N * ZG_BP) * 8;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool ok) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(ok ? 16 : 0) : "memory");
+}
+
+__global__ void __launch_bounds__(256, 2) k_lu_zgemm(int N, size_t stride, int r0, int c0, int k0, int M, int n, int K,
+                                                     double2* __restrict__ Aall) {
+    extern __shared__ double zg_smem[];
+    double* As = zg_smem;                      // [2][ZG_K][ZG_AP]
+    double* Bs = zg_smem + 2 * ZG_K * ZG_AP;   // [2][ZG_N][ZG_BP]
+    const int f = blockIdx.z;
+    double2* A = Aall + (size_t)f * stride;
+    const int tm = blockIdx.x * ZG_M, tn = blockIdx.y * ZG_N;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp & 3, wn = warp >> 2;
+    const int nchunk = (K + ZG_K - 1) / ZG_K;
+    auto load = [&](int buf, int kc) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int idx = tid + 256 * q;
+            {  // A: k-column kk, complex row rr
+                const int kk = idx >> 6, rr = idx & 63, kg = kc * ZG_K + kk;
+                const bool ok = tm + rr < M && kg < K;
+                const double2* src = ok ? A + (size_t)(r0 + tm + rr) + (size_t)(k0 + kg) * N : A;
+                cp_async16(As + (size_t)(buf * ZG_K + kk) * ZG_AP + 2 * rr, src, ok);
+            }
+            {  // B: column cc, complex row kk
+                const int cc = idx >> 4, kk = idx & 15, kg = kc * ZG_K + kk;
+                const bool ok = tn + cc < n && kg < K;
+                const double2* src = ok ? A + (size_t)(k0 + kg) + (size_t)(c0 + tn + cc) * N : A;
+                cp_async16(Bs + (size_t)(buf * ZG_N + cc) * ZG_BP + 2 * kk, src, ok);
+            }
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+    load(0, 0);
+    for (int kc = 0; kc < nchunk; kc++) {
+        if (kc + 1 < nchunk) {
+            load((kc + 1) & 1, kc + 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const double* Ab = As + (size_t)(kc & 1) * ZG_K * ZG_AP;
+        const double* Bb = Bs + (size_t)(kc & 1) * ZG_N * ZG_BP;
+#pragma unroll
+        for (int ks = 0; ks < 2 * ZG_K / 4; ks++) {
+            const int kq = 4 * ks + (lane & 3), k = kq >> 1, cpart = kq & 1;
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int R = wm * 32 + 8 * i + (lane >> 2);
+                const double v = Ab[k * ZG_AP + (R ^ cpart)];
+                a[i] = ((R & 1) == 0 && cpart) ? -v : v;
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) b[j] = Bb[(wn * 32 + 8 * j + (lane >> 2)) * ZG_BP + kq];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                                 : "+d"(acc[i][j][0]), "+d"(acc[i][j][1])
+                                 : "d"(a[i]), "d"(b[j]));
+        }
+        __syncthreads();  // the buffer is refilled by the next iteration's load
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int R = wm * 32 + 8 * i + (lane >> 2), crow = tm + (R >> 1);
+        if (crow >= M) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const int ccol = tn + wn * 32 + 8 * j + 2 * (lane & 3) + e;
+                if (ccol < n) {
+                    double* c = reinterpret_cast<double*>(A + (size_t)(r0 + crow) + (size_t)(c0 + ccol) * N) + (R & 1);
+                    *c -= acc[i][j][e];
+                }
+            }
+    }
+}
+
+// ------------------------------------------------------------------ the factorization
+namespace {
+struct LuF64Streams {
+    cudaStream_t s[LU_F64_GROUPS] = {};
+    cudaEvent_t fork = nullptr, join[LU_F64_GROUPS] = {};
+    bool ok = false;
+};
+LuF64Streams& lu_f64_streams() {
+    static thread_local LuF64Streams t[16];
+    int d = 0;
+    cudaGetDevice(&d);
+    if (d < 0 || d >= 16) d = 0;
+    LuF64Streams& x = t[d];
+    if (!x.ok) {
+        bool ok = true;
+        for (int i = 0; i < LU_F64_GROUPS; i++) {
+            ok = ok && cudaStreamCreateWithFlags(&x.s[i], cudaStreamNonBlocking) == cudaSuccess;
+            ok = ok && cudaEventCreateWithFlags(&x.join[i], cudaEventDisableTiming) == cudaSuccess;
+        }
+        x.ok = ok && cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming) == cudaSuccess;
+    }
+    return x;
+}
+
+struct LuF64 {
+    int N, F;  // matrix order, matrices of this group
+    double2* A;
+    size_t stride;
+    int32_t* ipiv;
+    int32_t* info;
+    cudaStream_t s;
+    int64_t* launches;
+
+    void laswp(int r0, int r1, int ca, int cb, int cc, int cd) {
+        const int cols = (cb - ca) + (cd - cc);
+        if (cols <= 0 || r1 <= r0) return;
+        KernelProfiler& P = profiler();
+        P.begin(s);
+        k_lu_laswp<<<dim3((cols + 127) / 128, F), 128, 0, s>>>(N, r0, r1, ca, cb, cc, cd, A, stride, ipiv);
+        P.end(KF_LU_LASWP, (double)F * cols * (r1 - r0) * 64.0, s);
+        (*launches)++;
+    }
+    void trsm(int c0, int n1, int cb, int ce) {
+        if (ce <= cb || n1 <= 1) return;
+        KernelProfiler& P = profiler();
+        const int cols = ce - cb;
+        const size_t sm = sizeof(double2) * (size_t)n1 * (n1 - 1) / 2;
+        // each CTA loads the triangle once and walks many columns: a few CTAs per matrix
+        const int threads = 1024, nw = threads / 32;
+        const int gx = std::max(1, std::min((cols + nw - 1) / nw, 16));
+        P.begin(s);
+        if (n1 <= 32)
+            k_lu_trsm<1><<<dim3(gx, F), threads, sm, s>>>(N, c0, n1, cb, ce, A, stride);
+        else if (n1 <= 64)
+            k_lu_trsm<2><<<dim3(gx, F), threads, sm, s>>>(N, c0, n1, cb, ce, A, stride);
+        else
+            k_lu_trsm<4><<<dim3(gx, F), threads, sm, s>>>(N, c0, n1, cb, ce, A, stride);
+        // complex TRSM: 4 n1^2 cols real flops
+        P.end(KF_LU_TRSM, (double)F * 4.0 * n1 * (double)n1 * cols, s);
+        (*launches)++;
+    }
+    void gemm(int r0, int c0, int k0, int M, int n, int K) {
+        if (M <= 0 || n <= 0 || K <= 0) return;
+        KernelProfiler& P = profiler();
+        P.begin(s);
+        k_lu_zgemm<<<dim3((M + ZG_M - 1) / ZG_M, (n + ZG_N - 1) / ZG_N, F), 256, ZG_SMEM, s>>>(N, stride, r0, c0, k0, M, n,
+                                                                                              K, A);
+        // complex C -= A B: 8 M n K real flops
+        P.end(KF_LU_GEMM, (double)F * 8.0 * M * (double)n * K, s);
+        (*launches)++;
+    }
+    // columns c0 .. c0 + w - 1, rows c0 .. N - 1 (dgetrf2's recursion: the left half, its interchanges and
+    // triangular solve on the right half, the update of the right half, the right half, its
+    // interchanges on the left half)
+    void panel(int c0, int w) {
+        if (w <= LU_BASE) {
+            KernelProfiler& P = profiler();
+            const double m = N - c0;
+            P.begin(s);
+            k_lu_base<<<F, 512, 0, s>>>(N, c0, w, A, stride, ipiv, info);
+            P.end(KF_LU_PANEL, (double)F * 8.0 * (m * w * w - (double)w * w * w / 3.0), s);
+            (*launches)++;
+            return;
+        }
+        const int n1 = w / 2 / LU_BASE * LU_BASE > 0 ? w / 2 / LU_BASE * LU_BASE : w / 2, n2 = w - n1;
+        panel(c0, n1);
+        laswp(c0, c0 + n1, c0 + n1, c0 + w, 0, 0);
+        trsm(c0, n1, c0 + n1, c0 + w);
+        gemm(c0 + n1, c0 + n1, c0, N - c0 - n1, n2, n1);
+        panel(c0 + n1, n2);
+        laswp(c0 + n1, c0 + w, c0, c0 + n1, 0, 0);
+    }
+    void factor() {
+        for (int k0 = 0; k0 < N; k0 += LU_NB) {
+            const int nb = std::min(LU_NB, N - k0);
+            panel(k0, nb);
+            laswp(k0, k0 + nb, 0, k0, k0 + nb, N);
+            trsm(k0, nb, k0 + nb, N);
+            gemm(k0 + nb, k0 + nb, k0, N - k0 - nb, N - k0 - nb, nb);
+        }
+    }
+};
+}  // namespace
+
 int lu_factor_f64(int N, int F, double2* A, size_t stride, int32_t* ipiv, int32_t* info, cudaStream_t s,
                   int64_t* launches) {
-    KernelProfiler& P = profiler();
+    cudaFuncSetAttribute(k_lu_zgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, ZG_SMEM);
+    cudaFuncSetAttribute(k_lu_trsm<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(double2) * LU_NB * (LU_NB - 1) / 2));
     cudaMemsetAsync(info, 0, sizeof(int32_t) * F, s);
-    for (int k0 = 0; k0 < N; k0 += NB) {
-        int nb = N - k0 < NB ? N - k0 : NB;
-        const double m = N - k0;
-        P.begin(s);
-        k_panel_f64<<<F, 1024, 0, s>>>(N, k0, nb, A, stride, ipiv, info);
-        // complex LU of an m x nb panel: 8 (m nb^2 - nb^3 / 3) real flops
-        P.end(KF_LU_PANEL, F * 8.0 * (m * nb * nb - nb * (double)nb * nb / 3.0), s);
-        (*launches)++;
-        if (N - nb > 0) {
-            P.begin(s);
-            k_laswp_f64<<<dim3((N - nb + 127) / 128, F), 128, 0, s>>>(N, k0, nb, A, stride, ipiv);
-            P.end(KF_LU_LASWP, F * 2.0 * nb * (N - nb) * 16.0 * 2.0, s);
-            (*launches)++;
-        }
-        int right = N - k0 - nb;
-        if (right > 0) {
-            P.begin(s);
-            k_trsm_f64<<<dim3((right + 7) / 8, F), 256, 0, s>>>(N, k0, nb, A, stride);
-            P.end(KF_LU_TRSM, F * 4.0 * nb * (double)nb * right, s);
-            dim3 g((right + 63) / 64, (right + 63) / 64, F);
-            P.begin(s);
-            k_gemm_update_f64<<<g, 256, 0, s>>>(N, k0, nb, A, stride);
-            // complex C -= L U: 8 m n k real flops
-            P.end(KF_LU_GEMM, F * 8.0 * (double)right * right * nb, s);
-            (*launches) += 2;
-        }
+    LuF64Streams& side = lu_f64_streams();
+    const int ng = side.ok ? std::min(LU_F64_GROUPS, F) : 1;
+    if (ng <= 1) {
+        LuF64{N, F, A, stride, ipiv, info, s, launches}.factor();
+        return 0;
+    }
+    cudaEventRecord(side.fork, s);
+    for (int g = 0, f0 = 0; g < ng; g++) {
+        const int fg = F / ng + (g < F % ng ? 1 : 0);
+        cudaStreamWaitEvent(side.s[g], side.fork, 0);
+        LuF64{N, fg, A + (size_t)f0 * stride, stride, ipiv + (size_t)f0 * N, info + f0, side.s[g], launches}.factor();
+        cudaEventRecord(side.join[g], side.s[g]);
+        cudaStreamWaitEvent(s, side.join[g], 0);
+        f0 += fg;
     }
     return 0;
 }

@@ -280,8 +280,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     int dev = 0, n_sm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    const int dsmem = (int)df_smem_bytes();
-    cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, dsmem);
+    const int dsmem = (int)df2_smem_bytes();
+    cudaFuncSetAttribute(k_diag_factor2, cudaFuncAttributeMaxDynamicSharedMemorySize, dsmem);
     cudaFuncSetAttribute(k_tri_step<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(8));
     cudaFuncSetAttribute(k_tri_step<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(10));
     cudaFuncSetAttribute(k_tri_step<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(12));
@@ -523,7 +523,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             };
             auto diag = [&](const Half& h, int k0) {
                 P.begin(h.st);
-                k_diag_factor<<<h.nb, DF_THREADS, dsmem, h.st>>>(W + (size_t)h.f0 * MB, Np, MB, k0,
+                k_diag_factor2<<<2 * h.nb, DF2_THREADS, dsmem, h.st>>>(W + (size_t)h.f0 * MB, Np, MB, k0,
                                                                   PL + (size_t)h.f0 * NBL * 2 * NBL,
                                                                   PU + (size_t)h.f0 * 4 * NBL * NBL,
                                                                   DINV + (size_t)h.f0 * nblk * NBL * NBL, err);
@@ -643,7 +643,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             Half hs[LU_GROUPS];
             for (int i = 0, f0 = 0; i < nh; i++) {
                 const int ni = ns / nh + (i < ns % nh ? 1 : 0);
-                hs[i] = Half{side.s[i], f0, ni, std::max(n_sm - (ns - ni), 1)};
+                hs[i] = Half{side.s[i], f0, ni, std::max(n_sm - 2 * (ns - ni), 1)};  // diagonal factors: two CTAs a matrix
                 f0 += ni;
             }
             cudaEventRecord(side.fork, s);

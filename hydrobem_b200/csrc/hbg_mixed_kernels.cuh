@@ -542,6 +542,305 @@ __global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ 
     }
 }
 
+// Two CTAs per matrix (blockIdx.x = 2 f + side), each factoring the same 128 x 128 diagonal block of
+// M = A^T in its own shared memory (M = L U, no pivoting), then side 0 forms L^-1 (and writes the
+// factors back to W) and side 1 forms U^-1: the inverses, as much work as the factorization, run on two
+// SMs at once.  Outputs as k_diag_factor's: PL ([Lr | Li] rows of L^-1), PU (U^-1 block-real K-major),
+// DINV (U^-1 on and above the diagonal, L^-1 below it).
+//
+// The factorization, blocked by 32 columns: the panel's rows are held in registers (warp w the rows
+// c0 + w + 16 q, lane the column), each pivot row published through shared memory with one CTA barrier
+// a column; U12 = L_pp^-1 A12 by forward substitution (a warp per column); the trailing update A22 -=
+// L21 U12 in 4 x 4 register tiles.  The inverses: the four 32 x 32 diagonal blocks by one warp each
+// (a lane per row, the row in registers), then the off-diagonal blocks block column by block column
+// (U^-1(I, J) = -(sum_{I <= K < J} X(I, K) U(K, J)) X(J, J); L^-1(I, J) = -(sum_{J < K <= I} Y(I, K)
+// L(K, J)) Y(J, J)) in 2 x 2 register tiles.
+constexpr int DF2_THREADS = 512;
+constexpr size_t df2_smem_bytes() {
+    return (size_t)(NBL * DF_LD + DF_NB * DF_BLK * DF_SLD + 2 * DF_BLK) * sizeof(float2);
+}
+
+// Y = L^-1 of the unit lower 32 x 32 block at A (leading dimension DF_LD) into X (DF_SLD): lane i holds
+// row i of Y, the columns from the last: Y(i, j) = -sum_{j < k <= i} Y(i, k) L(k, j).
+__device__ __forceinline__ void df2_inv_lower32(const float2* A, float2* X) {
+    const int i = threadIdx.x & 31;
+    float2 y[DF_BLK];
+#pragma unroll
+    for (int k = 0; k < DF_BLK; k++) y[k] = make_float2(k == i ? 1.f : 0.f, 0.f);
+#pragma unroll
+    for (int j = DF_BLK - 2; j >= 0; j--) {
+        float2 t = make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = j + 1; k < DF_BLK; k++) cfma_add(t, y[k], A[k * DF_LD + j]);  // y[k] = 0 for k > i
+        if (i > j) y[j] = make_float2(-t.x, -t.y);
+    }
+#pragma unroll
+    for (int k = 0; k < DF_BLK; k++) X[i * DF_SLD + k] = y[k];
+}
+
+// X = U^-1 of the upper 32 x 32 block at A into X: lane i holds row i of X, the columns from the
+// first: X(i, j) = (delta_ij - sum_{i <= k < j} X(i, k) U(k, j)) / U(j, j).
+__device__ __forceinline__ void df2_inv_upper32(const float2* A, float2* X) {
+    const int i = threadIdx.x & 31;
+    float2 x[DF_BLK];
+#pragma unroll
+    for (int j = 0; j < DF_BLK; j++) {
+        float2 t = make_float2(j == i ? 1.f : 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < j; k++) cfma_sub(t, x[k], A[k * DF_LD + j]);  // x[k] = 0 for k < i
+        const float2 d = A[j * DF_LD + j];
+        const float dd = d.x * d.x + d.y * d.y;
+        const float2 inv = make_float2(d.x / dd, -d.y / dd);
+        x[j] = j < i ? make_float2(0.f, 0.f) : cmulf(t, inv);
+    }
+#pragma unroll
+    for (int k = 0; k < DF_BLK; k++) X[i * DF_SLD + k] = x[k];
+}
+
+__global__ void __launch_bounds__(DF2_THREADS) k_diag_factor2(float* __restrict__ W, int Np, size_t bstride, int k0,
+                                                              float* __restrict__ PL, float* __restrict__ PU,
+                                                              float2* __restrict__ DINV, int* __restrict__ err) {
+    extern __shared__ float2 df_smem[];
+    float2* blk = df_smem;                        // [NBL][DF_LD]
+    float2* Xd = blk + NBL * DF_LD;               // [DF_NB][DF_BLK][DF_SLD]: this side's diagonal-block inverses
+    float2* prow = Xd + DF_NB * DF_BLK * DF_SLD;  // [2][DF_BLK]: the published pivot rows
+    const int f = blockIdx.x >> 1, side = blockIdx.x & 1;
+    float* Wr = W + (size_t)f * bstride;
+    float* Wi = Wr + (size_t)Np * Np;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int NWARP = DF2_THREADS / 32;  // 16
+    for (int t = threadIdx.x; t < NBL * NBL; t += DF2_THREADS) {
+        const int r = t / NBL, c = t % NBL;
+        const size_t o = (size_t)(k0 + r) * Np + k0 + c;
+        blk[r * DF_LD + c] = make_float2(Wr[o], Wi[o]);
+    }
+    __syncthreads();
+    for (int pb = 0; pb < DF_NB; pb++) {
+        const int c0 = pb * DF_BLK;
+        // ---- panel: rows c0 .. NBL - 1 of columns c0 .. c0 + 31 in registers
+        float2 v[NBL / NWARP];
+#pragma unroll
+        for (int q = 0; q < NBL / NWARP; q++) {
+            const int r = c0 + warp + NWARP * q;
+            v[q] = r < NBL ? blk[r * DF_LD + c0 + lane] : make_float2(0.f, 0.f);
+        }
+        if (warp == 0) prow[lane] = v[0];
+        for (int j = 0; j < DF_BLK; j++) {
+            const int c = c0 + j;
+            __syncthreads();  // pivot row c published in prow[j & 1]
+            const float2 u = prow[(j & 1) * DF_BLK + lane];
+            const float2 d = prow[(j & 1) * DF_BLK + j];
+            const float dd = d.x * d.x + d.y * d.y;
+            if (threadIdx.x == 0 && !(dd > 1e-30f)) atomicExch(err, 10);
+            const float2 inv = make_float2(d.x / dd, -d.y / dd);
+#pragma unroll
+            for (int q = 0; q < NBL / NWARP; q++) {
+                const int r = c0 + warp + NWARP * q;
+                if (r > c && r < NBL) {  // warp-uniform
+                    const float2 a = make_float2(__shfl_sync(0xffffffffu, v[q].x, j), __shfl_sync(0xffffffffu, v[q].y, j));
+                    const float2 l = cmulf(a, inv);
+                    if (lane == j) v[q] = l;
+                    if (lane > j) cfma_sub(v[q], l, u);
+                }
+            }
+            if (j + 1 < DF_BLK && warp == (j + 1) % NWARP)  // row c + 1 is final: publish it
+                prow[((j + 1) & 1) * DF_BLK + lane] = ((j + 1) / NWARP) ? v[1] : v[0];
+        }
+#pragma unroll
+        for (int q = 0; q < NBL / NWARP; q++) {
+            const int r = c0 + warp + NWARP * q;
+            if (r < NBL) blk[r * DF_LD + c0 + lane] = v[q];
+        }
+        __syncthreads();
+        const int n2 = NBL - c0 - DF_BLK;
+        if (n2 == 0) break;
+        // ---- U12 = L_pp^-1 A12: a warp per column, lane = row, the lane's row of L_pp in registers
+        {
+            float2 lrow[DF_BLK];
+#pragma unroll
+            for (int j = 0; j < DF_BLK; j++)
+                lrow[j] = j < lane ? blk[(c0 + lane) * DF_LD + c0 + j] : make_float2(0.f, 0.f);
+            for (int cc = c0 + DF_BLK + warp; cc < NBL; cc += NWARP) {
+                float2 x = blk[(c0 + lane) * DF_LD + cc];
+#pragma unroll
+                for (int j = 0; j < DF_BLK - 1; j++) {
+                    const float2 xj = make_float2(__shfl_sync(0xffffffffu, x.x, j), __shfl_sync(0xffffffffu, x.y, j));
+                    cfma_sub(x, lrow[j], xj);  // lrow[j] = 0 for j >= lane
+                }
+                blk[(c0 + lane) * DF_LD + cc] = x;
+            }
+        }
+        __syncthreads();
+        // ---- A22 -= L21 U12 in 4 x 4 tiles
+        {
+            const int tc = n2 / 4, ntile = tc * tc, b0 = c0 + DF_BLK;
+            for (int t = threadIdx.x; t < ntile; t += DF2_THREADS) {
+                const int rb = b0 + 4 * (t / tc), cb = b0 + 4 * (t % tc);
+                float2 acc[4][4];
+#pragma unroll
+                for (int a = 0; a < 4; a++)
+#pragma unroll
+                    for (int b = 0; b < 4; b++) acc[a][b] = make_float2(0.f, 0.f);
+#pragma unroll 4
+                for (int k = 0; k < DF_BLK; k++) {
+                    float2 av[4], bv[4];
+#pragma unroll
+                    for (int a = 0; a < 4; a++) av[a] = blk[(rb + a) * DF_LD + c0 + k];
+#pragma unroll
+                    for (int b = 0; b < 4; b++) bv[b] = blk[(c0 + k) * DF_LD + cb + b];
+#pragma unroll
+                    for (int a = 0; a < 4; a++)
+#pragma unroll
+                        for (int b = 0; b < 4; b++) cfma_add(acc[a][b], av[a], bv[b]);
+                }
+#pragma unroll
+                for (int a = 0; a < 4; a++)
+#pragma unroll
+                    for (int b = 0; b < 4; b++) {
+                        float2& x = blk[(rb + a) * DF_LD + cb + b];
+                        x = make_float2(x.x - acc[a][b].x, x.y - acc[a][b].y);
+                    }
+            }
+        }
+        __syncthreads();
+    }
+    // ---- the factors back to W (side 0), the diagonal-block inverses of this side's triangle
+    if (side == 0)
+        for (int t = threadIdx.x; t < NBL * NBL; t += DF2_THREADS) {
+            const int r = t / NBL, c = t % NBL;
+            const size_t o = (size_t)(k0 + r) * Np + k0 + c;
+            Wr[o] = blk[r * DF_LD + c].x;
+            Wi[o] = blk[r * DF_LD + c].y;
+        }
+    if (warp < DF_NB) {
+        const float2* Ab = blk + warp * DF_BLK * DF_LD + warp * DF_BLK;
+        if (side == 0)
+            df2_inv_lower32(Ab, Xd + warp * DF_BLK * DF_SLD);
+        else
+            df2_inv_upper32(Ab, Xd + warp * DF_BLK * DF_SLD);
+    }
+    __syncthreads();
+    // ---- the off-diagonal blocks of the inverse, in place in blk, one block column per stage; 2 x 2
+    // tiles, at most DF_NB - 1 blocks a stage (768 tiles): two per thread
+    const bool upper = side == 1;
+    for (int st = 1; st < DF_NB; st++) {
+        const int J = upper ? st : DF_NB - 1 - st;
+        const int nI = st, ntile = nI * (DF_BLK / 2) * (DF_BLK / 2);
+        float2 tv[2][2][2];
+        // T(I, J) = sum_K X(I, K) U(K, J)  (upper: I <= K < J)  or  sum_K Y(I, K) L(K, J)  (lower: J < K <= I)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int t = threadIdx.x + e * DF2_THREADS;
+#pragma unroll
+            for (int a = 0; a < 2; a++) tv[e][a][0] = tv[e][a][1] = make_float2(0.f, 0.f);
+            if (t < ntile) {
+                const int bi = t / 256, i0 = 2 * ((t / 16) % 16), j0 = 2 * (t % 16);
+                const int I = upper ? bi : J + 1 + bi;
+                const int Kb = upper ? I : J + 1, Ke = upper ? J - 1 : I;
+                for (int K = Kb; K <= Ke; K++) {
+                    const bool diag = K == I;  // X(I, I) from the scratch, else the block stored in blk
+                    const float2* Xs = diag ? Xd + I * DF_BLK * DF_SLD + i0 * DF_SLD
+                                            : blk + (I * DF_BLK + i0) * DF_LD + K * DF_BLK;
+                    const int xld = diag ? DF_SLD : DF_LD;
+                    const float2* Bs = blk + (K * DF_BLK) * DF_LD + J * DF_BLK + j0;
+#pragma unroll 4
+                    for (int k = 0; k < DF_BLK; k++) {
+                        const float2 x0 = Xs[k], x1 = Xs[xld + k];
+                        const float2 b0 = Bs[k * DF_LD], b1 = Bs[k * DF_LD + 1];
+                        cfma_add(tv[e][0][0], x0, b0);
+                        cfma_add(tv[e][0][1], x0, b1);
+                        cfma_add(tv[e][1][0], x1, b0);
+                        cfma_add(tv[e][1][1], x1, b1);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int t = threadIdx.x + e * DF2_THREADS;
+            if (t < ntile) {
+                const int bi = t / 256, i0 = 2 * ((t / 16) % 16), j0 = 2 * (t % 16);
+                const int I = upper ? bi : J + 1 + bi;
+#pragma unroll
+                for (int a = 0; a < 2; a++)
+#pragma unroll
+                    for (int b = 0; b < 2; b++) blk[(I * DF_BLK + i0 + a) * DF_LD + J * DF_BLK + j0 + b] = tv[e][a][b];
+            }
+        }
+        __syncthreads();
+        // X(I, J) = -T(I, J) X(J, J)
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int t = threadIdx.x + e * DF2_THREADS;
+#pragma unroll
+            for (int a = 0; a < 2; a++) tv[e][a][0] = tv[e][a][1] = make_float2(0.f, 0.f);
+            if (t < ntile) {
+                const int bi = t / 256, i0 = 2 * ((t / 16) % 16), j0 = 2 * (t % 16);
+                const int I = upper ? bi : J + 1 + bi;
+                const float2* Ts = blk + (I * DF_BLK + i0) * DF_LD + J * DF_BLK;
+                const float2* Xj = Xd + J * DF_BLK * DF_SLD + j0;
+#pragma unroll 4
+                for (int k = 0; k < DF_BLK; k++) {
+                    const float2 x0 = Ts[k], x1 = Ts[DF_LD + k];
+                    const float2 b0 = Xj[k * DF_SLD], b1 = Xj[k * DF_SLD + 1];
+                    cfma_sub(tv[e][0][0], x0, b0);
+                    cfma_sub(tv[e][0][1], x0, b1);
+                    cfma_sub(tv[e][1][0], x1, b0);
+                    cfma_sub(tv[e][1][1], x1, b1);
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int t = threadIdx.x + e * DF2_THREADS;
+            if (t < ntile) {
+                const int bi = t / 256, i0 = 2 * ((t / 16) % 16), j0 = 2 * (t % 16);
+                const int I = upper ? bi : J + 1 + bi;
+#pragma unroll
+                for (int a = 0; a < 2; a++)
+#pragma unroll
+                    for (int b = 0; b < 2; b++) blk[(I * DF_BLK + i0 + a) * DF_LD + J * DF_BLK + j0 + b] = tv[e][a][b];
+            }
+        }
+        __syncthreads();
+    }
+    // ---- outputs: this side's triangle of the inverse
+    auto inv_at = [&](int i, int c) -> float2 {  // U^-1 (i <= c, side 1) or L^-1 (i > c, side 0)
+        const int bi = i / DF_BLK, bc = c / DF_BLK;
+        if (bi == bc) return Xd[bi * DF_BLK * DF_SLD + (i % DF_BLK) * DF_SLD + c % DF_BLK];
+        return blk[i * DF_LD + c];
+    };
+    {
+        float2* D = DINV + ((size_t)f * (Np / NBL) + k0 / NBL) * NBL * NBL;
+        for (int t = threadIdx.x; t < NBL * NBL; t += DF2_THREADS) {
+            const int i = t / NBL, c = t % NBL;
+            if ((i > c) == !upper) D[t] = inv_at(i, c);
+        }
+    }
+    if (!upper) {
+        float* PLf = PL + (size_t)f * NBL * 2 * NBL;
+        for (int t = threadIdx.x; t < NBL * NBL; t += DF2_THREADS) {  // [Lr | Li] rows of L^-1 (c fastest)
+            const int i = t / NBL, c = t % NBL;
+            const float2 l = i > c ? inv_at(i, c) : make_float2(i == c ? 1.f : 0.f, 0.f);
+            PLf[(size_t)i * 2 * NBL + c] = l.x;
+            PLf[(size_t)i * 2 * NBL + NBL + c] = l.y;
+        }
+    } else {
+        float* PUf = PU + (size_t)f * 2 * NBL * 2 * NBL;
+        for (int t = threadIdx.x; t < NBL * NBL; t += DF2_THREADS) {
+            // U^-1 block-real K-major (i fastest): row c: [Ur(:, c); -Ui(:, c)], row NBL + c: [Ui(:, c); Ur(:, c)]
+            const int c = t / NBL, i = t % NBL;
+            const float2 u = i <= c ? inv_at(i, c) : make_float2(0.f, 0.f);
+            PUf[(size_t)c * 2 * NBL + i] = u.x;
+            PUf[(size_t)c * 2 * NBL + NBL + i] = -u.y;
+            PUf[(size_t)(NBL + c) * 2 * NBL + i] = u.y;
+            PUf[(size_t)(NBL + c) * 2 * NBL + NBL + i] = u.x;
+        }
+    }
+}
+
 // The block row B = rows k0..k0+NBL, columns c0..c0+n in the block-real K-major form
 // [F][2n][2 NBL]: row j: [Br(:, j); -Bi(:, j)], row n + j: [Bi(:, j); Br(:, j)] (32 x 32 tiles
 // transposed through shared memory).

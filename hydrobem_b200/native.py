@@ -92,7 +92,7 @@ EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
            "hbg_statics_noalloc", "hbg_measure_peaks", "hbg_last_ir_history", "hbg_surrogate_train",
            "hbg_surrogate_grad", "hbg_surrogate_eval", "hbg_last_surrogate_pairs", "hbg_read_gdf", "hbg_gdf_free",
-           "hb_model_load_mesh", "hbg_last_fallback_count"]
+           "hb_model_load_mesh", "hbg_last_fallback_count", "hbg_debug_lu_f64"]
 
 _lib = None
 
@@ -124,6 +124,8 @@ def lib():
     fp = ctypes.POINTER(ctypes.c_float)
     L.hbg_debug_gemm_tf32.argtypes = [ctypes.c_int32] * 3 + [fp, fp, fp, ctypes.c_int32]
     L.hbg_last_ir_iterations.argtypes = [ctypes.POINTER(ctypes.c_int32)]
+    L.hbg_debug_lu_f64.argtypes = [ctypes.c_int32, ctypes.c_int32, dp, ctypes.c_int32, dp, dp]
+    L.hbg_debug_lu_f64.restype = ctypes.c_int32
     L.hbg_measure_peaks.argtypes = [dp]
     L.hbg_last_ir_history.argtypes = [dp, ctypes.POINTER(ctypes.c_int32)]
     L.hbg_surrogate_train.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
@@ -358,6 +360,19 @@ def kernel_profile():
         lib().hbg_kernel_profile(i, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(w))
         out[name] = (ms.value, n.value, w.value)
     return out
+
+
+def debug_lu_f64(A, B):
+    """X = A^-1 B by the FP64 form's LU on the GPU: A [batch][n][n], B [batch][n][nrhs] complex."""
+    A = np.asarray(A, dtype=np.complex128)
+    B = np.asarray(B, dtype=np.complex128)
+    batch, n, _ = A.shape
+    nrhs = B.shape[2]
+    Ac = np.ascontiguousarray(A.transpose(0, 2, 1))  # column-major per matrix
+    Bc = np.ascontiguousarray(B.transpose(0, 2, 1))  # [batch][nrhs][n]
+    X = np.zeros_like(Bc)
+    check(lib().hbg_debug_lu_f64(n, batch, Ac.ctypes.data_as(dp), nrhs, Bc.ctypes.data_as(dp), X.ctypes.data_as(dp)))
+    return X.transpose(0, 2, 1)
 
 
 def debug_gemm_tf32(A, B, C=None):

@@ -268,6 +268,13 @@ HbStatus hbg_debug_matrices(const HbgBody *body, double omega, const HbgOptions 
 HbStatus hbg_debug_gemm_tf32(int32_t M, int32_t N, int32_t K, const float *A, const float *B, float *C,
                              int32_t subtract);
 
+/* Test support: X = A^-1 B for `batch` complex128 systems of order n by the FP64 form's LU (partial
+ * pivoting, the FP64 warp-MMA trailing update) and substitution: A [batch][n][n] column-major (entry
+ * (i, j) at 2 (i + j n)), B and X [batch][nrhs][n], interleaved (re, im) host arrays; nrhs <= 32.
+ * HB_ERR_NUMERICAL on an exactly singular matrix.  Replaces no reference interface (the dense solve
+ * of Real::lu_solve, linalg.rs:100-201 and 321-354, exposed for its numerics test). */
+HbStatus hbg_debug_lu_f64(int32_t n, int32_t batch, const double *A, int32_t nrhs, const double *B, double *X);
+
 /* Measured compute peaks of the current device, for the benchmark's rooflines: out3[0] FP64 FMA,
  * out3[1] FP64 warp MMA (mma.sync m8n8k4), out3[2] TF32 tcgen05 MMA, all dense TFLOP/s, each from
  * a kernel that keeps its pipe busy from registers or shared memory.  Replaces no reference
