@@ -51,7 +51,16 @@ CASE_LABELS = {
     "small": "cylinder r=1 m d=0.5 m, 2048 panels (32x16 side + 32x16 bottom), h=5 m, 4 periods 1.5-20 s, "
              "4 headings (profiling cut)",
     "tiny": "cylinder r=1 m d=0.5 m, 32 panels, h=5 m, 3 periods 1.5-20 s, 4 headings (host-logic tests)",
+    "c3": "64 uneven bodies (seed 20261203: truncated cylinders or hemispheres, 840-5928 panels, 223044 in all), "
+          "16 frequencies each (K r ~ U[0.1, 10]), headings 0 and 45 deg, infinite depth",
+    "c4": "three cylinders r=1 m d=1 m 4 m apart (3 x 4096 panels, 18 interacting modes), 32 frequencies "
+          "K a = 0.1-2, heading 0 deg, infinite depth",
+    "c5": "barge 80 x 20 x 10 m: 16448 wetted + 2048 interior-lid panels, 100 frequencies K L ~ U[0.05, 8] "
+          "(L = 80 m, seed 5), 8 headings, infinite depth",
 }
+# one-body cases: with N GPUs every rank solves its own copy of the job (weak scaling); the others are
+# fixed workloads whose (body, frequency) units are split over the ranks (strong scaling)
+SINGLE_BODY = ("c2", "medium", "small", "tiny")
 
 
 CASE = "c2"
@@ -72,6 +81,26 @@ def workload():
     v = meshes.cylinder(1.0, 0.5, 64, 32, 32)
     periods = np.linspace(1.5, 20.0, N_PERIODS)
     return v, 2.0 * math.pi / periods
+
+
+def case_problems():
+    """The problems of the case as keyword dicts of native.Body, and the depth."""
+    from hydrobem_b200 import meshes
+
+    if CASE in SINGLE_BODY:
+        v, omegas = workload()
+        return [dict(vertices=v, omegas=omegas, headings_deg=HEADINGS)], DEPTH
+    if CASE == "c3":
+        return [dict(vertices=v, omegas=om, headings_deg=[0.0, 45.0]) for v, om in meshes.uneven_bodies(64)], math.inf
+    if CASE == "c4":
+        v, pb, centers = meshes.cylinder_array()
+        omegas = np.sqrt(np.linspace(0.1, 2.0, 32) * meshes.GRAVITY)
+        return [dict(vertices=v, omegas=omegas, headings_deg=[0.0], panel_body=pb, rotation_centers=centers)], math.inf
+    if CASE == "c5":
+        v, kinds = meshes.barge()
+        omegas = np.sqrt(np.random.default_rng(5).uniform(0.05, 8.0, 100) / 80.0 * meshes.GRAVITY)
+        return [dict(vertices=v, omegas=omegas, headings_deg=list(np.arange(8) * 22.5), kinds=kinds)], math.inf
+    raise ValueError(CASE)
 
 
 def measured_peaks():
@@ -203,6 +232,9 @@ def cpu_reference(args, world, rank, pg):
     host's cores: every step one whole job (statics + every frequency)."""
     if rank != 0:
         return None
+    if CASE not in SINGLE_BODY:
+        return {"impl": "reference", "unavailable": "the CPU reference arm times the one-body cases (c2, medium, "
+                                                    "small, tiny)"}
     cores = host_cores()
     for _ in range(min(args.warmup, 1)):
         cpu_job(True)
@@ -231,19 +263,27 @@ def ours(args, world, rank, local, pg):
 
     from hydrobem_b200 import native as nv
 
+    from hydrobem_b200 import partition
+
     device = local if torch.cuda.is_available() else 0
     torch.cuda.set_device(device)
-    v, omegas = workload()
+    probs, depth = case_problems()
+    weak = CASE in SINGLE_BODY
+    jobs = probs * world if weak else probs  # weak: one copy of the job per rank
+    # this rank's (body, frequency) runs: the planner splits the units by their modelled cost
+    runs = partition.plan([(len(p["vertices"]), len(p["omegas"])) for p in jobs], world)[rank]
+    mine = [dict(jobs[r.body], omegas=np.asarray(jobs[r.body]["omegas"])[r.f0:r.f1]) for r in runs]
     precision = nv.HBG_MIXED if args.precision == "mixed" else nv.HBG_FP64
-    body = nv.Body(v, omegas, HEADINGS)
-    arr = (nv.HbgProblem * 1)(body.problem())
-    opt = nv.default_options(precision=precision, depth=DEPTH, device=device)
+    bodies = [nv.Body(**m) for m in mine]
+    arr = (nv.HbgProblem * max(len(bodies), 1))(*[b.problem() for b in bodies])
+    opt = nv.default_options(precision=precision, depth=depth, device=device)
     import ctypes
 
     L = nv.lib()
 
     def step():
-        nv.check(L.hbg_solve_batch(arr, 1, ctypes.byref(opt)))
+        if bodies:
+            nv.check(L.hbg_solve_batch(arr, len(bodies), ctypes.byref(opt)))
 
     def barrier():
         if pg is not None:
@@ -280,12 +320,16 @@ def ours(args, world, rank, local, pg):
     phases = nv.last_profile()
     ir = {"iterations": nv.last_ir_iterations(), "history": [float(f"{x:.3g}") for x in nv.last_ir_history()]} \
         if precision == nv.HBG_MIXED else None
+    fallbacks = nv.last_fallback_count() if precision == nv.HBG_MIXED else None
     pipe_peaks = nv.measure_peaks()  # FP64 FMA / FP64 MMA / TF32 tcgen05 of this device, measured here
     if rank != 0:
         return None
-    F = len(omegas)
-    value = world * F / (step_ms * 1e-3)
-    e2e = world * F / (e2e_ms * 1e-3)
+    F = sum(len(p["omegas"]) for p in jobs)  # frequency solves of the whole job over all ranks
+    value = F / (step_ms * 1e-3)
+    e2e = F / (e2e_ms * 1e-3)
+    h2d = sum(b.vertices.nbytes + b.omegas.nbytes + b.headings.nbytes + (0 if b.kinds is None else b.kinds.nbytes)
+              for b in bodies)
+    d2h = sum(b.A.nbytes + b.B.nbytes + b.X.nbytes + b.FK.nbytes + b.SC.nbytes + b.HK.nbytes for b in bodies)
     peaks, peak_kind = measured_peaks()
     # the dominant kernel family by device time; in the mixed form the LU families run on concurrent
     # streams (their per-launch event times overlap one another), so the choice is among the others
@@ -305,14 +349,15 @@ def ours(args, world, rank, local, pg):
         peak, bound, unit, pk = peaks["hbm_gbs"], "hbm", "GB/s", f"hbm copy ({peak_kind})"
     traffic = DRAM_TRAFFIC.get((args.precision, fam)) if CASE == "c2" else None
     clocks = clk.summary()
-    line = {"metric": "freq solves/s at N=4096", "value": value, "unit": "freq solves/s", "n_gpus": world,
+    line = {"metric": "freq solves/s at N=4096" if CASE == "c2" else "freq solves/s", "value": value,
+            "unit": "freq solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == nv.HBG_FP64 else "c64+tf32",
-            "data": "synthetic",
+            "scaling": "weak" if weak else "strong", "vs_baseline": None,
+            "dtype": "f64" if precision == nv.HBG_FP64 else "c64+tf32", "data": "synthetic",
             "config": {"workload": CASE_LABELS[CASE], "form": args.precision, "l2": "inputs larger than L2 (no flush)",
-                       "parallelism": f"replicas x{world}"},
-            "e2e": {"value": e2e, "unit": "freq solves/s", "h2d_bytes_per_step": int(v.nbytes + omegas.nbytes + 32),
-                    "d2h_bytes_per_step": int(F * (72 + 3 * len(HEADINGS) * 12) * 8)},
+                       "parallelism": (f"one copy of the job per rank x{world}" if weak else
+                                       f"(body, frequency) units split over {world} ranks by modelled cost")},
+            "e2e": {"value": e2e, "unit": "freq solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches) * args.steps,
             "roofline": {"bound": bound, "kernel": fam, "achieved": achieved, "peak": peak, "unit": unit,
                          "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
@@ -325,36 +370,49 @@ def ours(args, world, rank, local, pg):
             "clocks": clocks}
     if ir is not None:
         line["refinement"] = ir
-    if precision == nv.HBG_MIXED and not args.no_plain:
-        line["plain_fp64"], plain = plain_comparison(nv, v, omegas, device, body)
-        if args.surrogate_steps > 0:
-            line["surrogate"] = surrogate_comparison(nv, v, omegas, device, plain, args.surrogate_steps)
-    if world == 1 and not args.no_cpu_baseline:
+    if fallbacks is not None:
+        line["fp64_fallback_frequencies"] = fallbacks
+    if precision == nv.HBG_MIXED and not args.no_plain and bodies:
+        line["plain_fp64"], plain = plain_comparison(nv, mine, bodies, depth, device)
+        if args.surrogate_steps > 0 and CASE in SINGLE_BODY:
+            v, omegas = workload()
+            line["surrogate"] = surrogate_comparison(nv, v, omegas, device, plain[0], args.surrogate_steps)
+    if world == 1 and not args.no_cpu_baseline and CASE in SINGLE_BODY:
         line["cpu_baseline"] = cpu_baseline_quick()
     return line
 
 
-def plain_comparison(nv, v, omegas, device, mixed_body):
-    """The plain FP64 form of the same job (the correctness oracle of the mixed form): its throughput,
-    the speed-up of the mixed form, and the error of the mixed A, B, X against it (per entry, over the
-    entry's largest modulus across frequencies, floor 1e-3 of the quantity's peak)."""
+def plain_comparison(nv, mine, mixed_bodies, depth, device, max_solves=400):
+    """The plain FP64 form of the same problems (the correctness oracle of the mixed form): its
+    throughput, the speed-up of the mixed form, and the error of the mixed A, B, X against it (per entry,
+    over the entry's largest modulus across frequencies, floor 1e-3 of the quantity's peak).  When the job
+    has more than max_solves frequency solves the FP64 form runs on the first frequencies of each problem
+    (the same count for each), and the comparison covers those."""
     import ctypes
 
-    body = nv.Body(v, omegas, HEADINGS)
-    arr = (nv.HbgProblem * 1)(body.problem())
-    opt = nv.default_options(precision=nv.HBG_FP64, depth=DEPTH, device=device)
+    total = sum(len(m["omegas"]) for m in mine)
+    keep = None if total <= max_solves else max(1, max_solves // len(mine))
+    sub = [dict(m, omegas=np.asarray(m["omegas"])[:keep]) for m in mine]
+    bodies = [nv.Body(**m) for m in sub]
+    arr = (nv.HbgProblem * len(bodies))(*[b.problem() for b in bodies])
+    opt = nv.default_options(precision=nv.HBG_FP64, depth=depth, device=device)
     L = nv.lib()
-    nv.check(L.hbg_solve_batch(arr, 1, ctypes.byref(opt)))  # warm-up
+    nv.check(L.hbg_solve_batch(arr, len(bodies), ctypes.byref(opt)))  # warm-up
     ms = []
     for _ in range(2):
-        nv.check(L.hbg_solve_batch(arr, 1, ctypes.byref(opt)))
+        nv.check(L.hbg_solve_batch(arr, len(bodies), ctypes.byref(opt)))
         ms.append(nv.last_profile()["total"])
     step = float(np.mean(ms))
-
-    mixed = mixed_body.results()
-    plain = body.results()
-    return {"value": len(omegas) / (step * 1e-3), "ms_per_step": step,
-            "err_vs_fp64": {k: scaled_error(mixed[k], plain[k]) for k in ("A", "B", "X")}}, plain
+    plain = [b.results() for b in bodies]
+    mixed = [b.results() for b in mixed_bodies]
+    nf = sum(len(m["omegas"]) for m in sub)
+    err = {k: max(scaled_error(np.asarray(mx[k])[:len(pl[k])], pl[k]) for mx, pl in zip(mixed, plain))
+           for k in ("A", "B", "X", "HK")}
+    out = {"value": nf / (step * 1e-3), "ms_per_step": step, "err_vs_fp64": err,
+           "phases_ms": {k: round(x, 2) for k, x in nv.last_profile().items()}}
+    if keep is not None:
+        out["frequencies"] = f"the first {keep} of each problem ({nf} solves)"
+    return out, plain
 
 
 def scaled_error(got, ref):
@@ -423,7 +481,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--surrogate-steps", type=int, default=4000,
                     help="training steps of the wave-term network measured beside the mixed form (0: skip)")
-    ap.add_argument("--case", default="c2", choices=["c2", "medium", "small", "tiny"])
+    ap.add_argument("--case", default="c2", choices=list(CASE_LABELS))
     args = ap.parse_args()
     global CASE
     CASE = args.case

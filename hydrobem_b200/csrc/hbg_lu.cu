@@ -23,11 +23,31 @@ constexpr int LU_F64_GROUPS = 4;
 
 // ------------------------------------------------------------------ base strip
 // Columns c0 .. c0 + w - 1 (w <= LU_BASE), rows c0 .. N - 1, one CTA per matrix: for each column the
-// pivot (largest modulus, first index on a tie: LAPACK's izamax), the swap of the two rows inside the
-// strip, the column scaled by the pivot and the rank-1 update of the strip's remaining columns.  The
-// candidates of the next column's pivot are taken while its entries are updated (one pass a column).
-__global__ void __launch_bounds__(512) k_lu_base(int N, int c0, int w, double2* __restrict__ Aall, size_t stride,
-                                                 int32_t* __restrict__ ipiv, int32_t* __restrict__ info) {
+// pivot (largest modulus, first index on a tie: LAPACK's izamax), the swap of the two rows across the
+// whole panel (columns pk0 .. pk0 + pnb - 1: the recursion then needs no interchanges of its own), the
+// column scaled by the pivot and the rank-1 update of the strip's remaining columns.  The candidates of
+// the next column's pivot are taken while its entries are updated (one pass a column); each thread
+// updates two rows at a time, their loads in flight together.
+__device__ __forceinline__ void lu_base_row(double2* A, int N, int i, int c0, int col, int j, int w, double2 inv,
+                                            const double2* prow, double2 a, double2* v, double& best, int& bi,
+                                            bool store) {
+    if (!store) return;
+    const double2 l = cmul(a, inv);
+    A[(size_t)i + (size_t)col * N] = l;
+#pragma unroll
+    for (int c = 0; c < LU_BASE; c++)
+        if (c > j && c < w) {
+            v[c] = csub(v[c], cmul(l, prow[c]));
+            A[(size_t)i + (size_t)(c0 + c) * N] = v[c];
+            if (c == j + 1) {
+                const double m = cabs2(v[c]);
+                if (m > best) best = m, bi = i;
+            }
+        }
+}
+
+__global__ void __launch_bounds__(512) k_lu_base(int N, int c0, int w, int pk0, int pnb, double2* __restrict__ Aall,
+                                                 size_t stride, int32_t* __restrict__ ipiv, int32_t* __restrict__ info) {
     __shared__ double sval[32];
     __shared__ int sidx[32];
     __shared__ double2 prow[LU_BASE];
@@ -67,40 +87,35 @@ __global__ void __launch_bounds__(512) k_lu_base(int N, int c0, int w, double2* 
         }
         __syncthreads();
         const int p = spiv;
-        if (threadIdx.x < w) {  // swap rows col and p inside the strip; the pivot row to shared memory
-            const size_t a = (size_t)col + (size_t)(c0 + threadIdx.x) * N, b = (size_t)p + (size_t)(c0 + threadIdx.x) * N;
-            const double2 va = A[a], vb = A[b];
-            if (p != col) {
-                A[a] = vb;
+        if (p != col)  // swap rows col and p across the panel
+            for (int t = threadIdx.x; t < pnb; t += blockDim.x) {
+                const size_t a = (size_t)col + (size_t)(pk0 + t) * N, b = (size_t)p + (size_t)(pk0 + t) * N;
+                const double2 va = A[a];
+                A[a] = A[b];
                 A[b] = va;
             }
-            prow[threadIdx.x] = vb;
-        }
+        __syncthreads();
+        if (threadIdx.x < w) prow[threadIdx.x] = A[(size_t)col + (size_t)(c0 + threadIdx.x) * N];
         __syncthreads();
         const double2 piv = prow[j];
         const double d = cabs2(piv);
         const double2 inv = d > 0.0 ? make_double2(piv.x / d, -piv.y / d) : make_double2(0.0, 0.0);
         best = -1.0;
         bi = N;
-        for (int i = col + 1 + threadIdx.x; i < N; i += blockDim.x) {
-            // the row's entries loaded together (independent reads in flight), then updated and stored
-            double2 v[LU_BASE];
-            const double2 a = A[(size_t)i + (size_t)col * N];
+        const int step = blockDim.x;
+        for (int i = col + 1 + threadIdx.x; i < N; i += 2 * step) {
+            const int i2 = i + step;
+            const bool two = i2 < N;
+            double2 v0[LU_BASE], v1[LU_BASE];
+            const double2 a0 = A[(size_t)i + (size_t)col * N];
+            const double2 a1 = two ? A[(size_t)i2 + (size_t)col * N] : make_double2(0.0, 0.0);
 #pragma unroll
-            for (int c = 0; c < LU_BASE; c++)
-                if (c > j && c < w) v[c] = A[(size_t)i + (size_t)(c0 + c) * N];
-            const double2 l = cmul(a, inv);
-            A[(size_t)i + (size_t)col * N] = l;
-#pragma unroll
-            for (int c = 0; c < LU_BASE; c++)
-                if (c > j && c < w) {
-                    v[c] = csub(v[c], cmul(l, prow[c]));
-                    A[(size_t)i + (size_t)(c0 + c) * N] = v[c];
-                    if (c == j + 1) {
-                        const double m = cabs2(v[c]);
-                        if (m > best) best = m, bi = i;
-                    }
-                }
+            for (int c = 0; c < LU_BASE; c++) {
+                if (c > j && c < w) v0[c] = A[(size_t)i + (size_t)(c0 + c) * N];
+                if (two && c > j && c < w) v1[c] = A[(size_t)i2 + (size_t)(c0 + c) * N];
+            }
+            lu_base_row(A, N, i, c0, col, j, w, inv, prow, a0, v0, best, bi, true);
+            lu_base_row(A, N, i2, c0, col, j, w, inv, prow, a1, v1, best, bi, two);
         }
     }
 }
@@ -126,55 +141,121 @@ __global__ void k_lu_laswp(int N, int r0, int r1, int ca, int cb, int cc, int cd
     }
 }
 
-// ------------------------------------------------------------------ triangular solve of a block row
-// B := L^-1 B for the unit lower n1 x n1 block L at (c0, c0) and B the rows c0 .. c0 + n1 - 1, columns
-// [cb, ce): L's strictly lower part packed by columns in shared memory (column p: rows p + 1 .. n1 - 1),
-// a warp per column of B, lane l holding rows l, l + 32, ... (NQ of them), each solved entry broadcast
-// by shuffles.
-template <int NQ>
-__global__ void __launch_bounds__(1024) k_lu_trsm(int N, int c0, int n1, int cb, int ce, double2* __restrict__ Aall,
-                                                  size_t stride) {
+// ------------------------------------------------------------------ triangular solves of a block row
+// B := L^-1 B (lower: L the unit lower n1 x n1 block of the factor at (c0, c0)) or B := U^-1 B (upper: U
+// the upper block, diagonal included), B the rows c0 .. c0 + n1 - 1, columns [cb, ce) of the matrix X
+// (the factor matrix itself inside the LU, the right-hand sides in the substitution).  The triangle is
+// packed by columns in shared memory; a warp takes CPW columns of B at once (independent chains), lane
+// l holding rows l, l + 32, ... (NQ of them), each solved entry broadcast by shuffles.
+template <int NQ, int CPW, bool UPPER>
+__global__ void __launch_bounds__(512) k_lu_trsm(int N, int c0, int n1, int cb, int ce, const double2* __restrict__ Lall,
+                                                 size_t lstride, double2* __restrict__ Xall, size_t xstride) {
     extern __shared__ double2 Lc[];
     const int f = blockIdx.y;
-    double2* A = Aall + (size_t)f * stride;
+    const double2* L = Lall + (size_t)f * lstride;
+    double2* X = Xall + (size_t)f * xstride;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    auto off = [n1](int p) { return p * (2 * n1 - p - 1) / 2; };
-    for (int p = warp; p < n1 - 1; p += nw)
-        for (int r = p + 1 + lane; r < n1; r += 32) Lc[off(p) + r - p - 1] = A[(size_t)(c0 + r) + (size_t)(c0 + p) * N];
+    // lower: column p holds rows p + 1 .. n1 - 1 at loff(p) + r - p - 1;
+    // upper: column p holds rows 0 .. p at uoff(p) + r
+    auto loff = [n1](int p) { return p * (2 * n1 - p - 1) / 2; };
+    auto uoff = [](int p) { return p * (p + 1) / 2; };
+    if (UPPER) {
+        for (int p = warp; p < n1; p += nw)
+            for (int r = lane; r <= p; r += 32) Lc[uoff(p) + r] = L[(size_t)(c0 + r) + (size_t)(c0 + p) * N];
+    } else {
+        for (int p = warp; p < n1 - 1; p += nw)
+            for (int r = p + 1 + lane; r < n1; r += 32) Lc[loff(p) + r - p - 1] = L[(size_t)(c0 + r) + (size_t)(c0 + p) * N];
+    }
     __syncthreads();
-    for (int col = cb + blockIdx.x * nw + warp; col < ce; col += gridDim.x * nw) {
-        double2 x[NQ];
+    for (int col0 = cb + (blockIdx.x * nw + warp) * CPW; col0 < ce; col0 += gridDim.x * nw * CPW) {
+        double2 x[CPW][NQ];
 #pragma unroll
-        for (int q = 0; q < NQ; q++) {
-            const int r = lane + 32 * q;
-            x[q] = r < n1 ? A[(size_t)(c0 + r) + (size_t)col * N] : make_double2(0.0, 0.0);
-        }
+        for (int c = 0; c < CPW; c++)
 #pragma unroll
-        for (int sblk = 0; sblk < NQ; sblk++) {
-            for (int pp = 0; pp < 32; pp++) {
-                const int p = 32 * sblk + pp;
-                if (p >= n1 - 1) break;
-                const double2 xp = make_double2(__shfl_sync(0xffffffffu, x[sblk].x, pp),
-                                                __shfl_sync(0xffffffffu, x[sblk].y, pp));
-                const int base = off(p) - p - 1;  // L(r, p) at base + r
+            for (int q = 0; q < NQ; q++) {
+                const int r = lane + 32 * q;
+                x[c][q] = (r < n1 && col0 + c < ce) ? X[(size_t)(c0 + r) + (size_t)(col0 + c) * N] : make_double2(0.0, 0.0);
+            }
+        if (!UPPER) {
 #pragma unroll
-                for (int q = sblk; q < NQ; q++) {
-                    const int r = lane + 32 * q;
-                    if (r > p && r < n1) x[q] = csub(x[q], cmul(Lc[base + r], xp));
+            for (int sblk = 0; sblk < NQ; sblk++) {
+                for (int pp = 0; pp < 32; pp++) {
+                    const int p = 32 * sblk + pp;
+                    if (p >= n1 - 1) break;
+                    double2 xp[CPW];
+#pragma unroll
+                    for (int c = 0; c < CPW; c++)
+                        xp[c] = make_double2(__shfl_sync(0xffffffffu, x[c][sblk].x, pp), __shfl_sync(0xffffffffu, x[c][sblk].y, pp));
+                    const int base = loff(p) - p - 1;  // L(r, p) at base + r
+#pragma unroll
+                    for (int q = sblk; q < NQ; q++) {
+                        const int r = lane + 32 * q;
+                        if (r > p && r < n1) {
+                            const double2 l = Lc[base + r];
+#pragma unroll
+                            for (int c = 0; c < CPW; c++) x[c][q] = csub(x[c][q], cmul(l, xp[c]));
+                        }
+                    }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int sblk = NQ - 1; sblk >= 0; sblk--) {
+                for (int pp = 31; pp >= 0; pp--) {
+                    const int p = 32 * sblk + pp;
+                    if (p >= n1) continue;
+                    const double2 d = Lc[uoff(p) + p];
+                    const double dd = cabs2(d);
+                    const double2 dinv = dd > 0.0 ? make_double2(d.x / dd, -d.y / dd) : make_double2(0.0, 0.0);
+                    double2 xp[CPW];
+#pragma unroll
+                    for (int c = 0; c < CPW; c++) {
+                        if (lane == pp) x[c][sblk] = cmul(x[c][sblk], dinv);
+                        xp[c] = make_double2(__shfl_sync(0xffffffffu, x[c][sblk].x, pp), __shfl_sync(0xffffffffu, x[c][sblk].y, pp));
+                    }
+#pragma unroll
+                    for (int q = 0; q <= sblk; q++) {
+                        const int r = lane + 32 * q;
+                        if (r < p) {
+                            const double2 u = Lc[uoff(p) + r];
+#pragma unroll
+                            for (int c = 0; c < CPW; c++) x[c][q] = csub(x[c][q], cmul(u, xp[c]));
+                        }
+                    }
                 }
             }
         }
 #pragma unroll
-        for (int q = 0; q < NQ; q++) {
-            const int r = lane + 32 * q;
-            if (r < n1) A[(size_t)(c0 + r) + (size_t)col * N] = x[q];
-        }
+        for (int c = 0; c < CPW; c++)
+#pragma unroll
+            for (int q = 0; q < NQ; q++) {
+                const int r = lane + 32 * q;
+                if (r < n1 && col0 + c < ce) X[(size_t)(c0 + r) + (size_t)(col0 + c) * N] = x[c][q];
+            }
     }
 }
 
+template <bool UPPER>
+static void launch_lu_trsm(int N, int F, int c0, int n1, int cb, int ce, const double2* L, size_t lstride, double2* X,
+                           size_t xstride, cudaStream_t s) {
+    constexpr int CPW = 4, threads = 512, nw = threads / 32;
+    const int cols = ce - cb;
+    const size_t sm = sizeof(double2) * (size_t)n1 * (UPPER ? n1 + 1 : n1 - 1) / 2;
+    // each CTA loads the triangle once and walks many columns: a few CTAs per matrix
+    const int gx = std::max(1, std::min((cols + nw * CPW - 1) / (nw * CPW), 16));
+    const dim3 g(gx, F);
+    if (n1 <= 32)
+        k_lu_trsm<1, CPW, UPPER><<<g, threads, sm, s>>>(N, c0, n1, cb, ce, L, lstride, X, xstride);
+    else if (n1 <= 64)
+        k_lu_trsm<2, CPW, UPPER><<<g, threads, sm, s>>>(N, c0, n1, cb, ce, L, lstride, X, xstride);
+    else
+        k_lu_trsm<4, CPW, UPPER><<<g, threads, sm, s>>>(N, c0, n1, cb, ce, L, lstride, X, xstride);
+}
+
 // ------------------------------------------------------------------ trailing update on FP64 warp MMA
-// C -= A B inside one matrix of the batch (C rows r0 .., columns c0 ..; A rows r0 .., columns k0 ..
-// k0 + K; B rows k0 .. k0 + K, columns c0 ..), complex128 column-major.  The complex product as a real
+// C -= A B for each matrix of the batch (A rows r0 .., columns k0 .. k0 + K of one matrix; B rows k0 ..
+// k0 + K, columns c0 .. and C rows r0 .., columns c0 .. of another -- the same one inside the LU, the
+// right-hand sides in the substitution), complex128 column-major, leading dimension N.  The complex product as a real
 // one on the interleaved (re, im) layout: C_r (2M x n) -= Ahat (2M x 2K) B_r (2K x n), where B_r and C_r
 // are the matrices' own memory read as doubles and Ahat(2r + c, 2k + c') is a_r, -a_i, a_i, a_r for
 // (c, c') = (0, 0), (0, 1), (1, 0), (1, 1), read on the fly from A's interleaved tile.  Tiles of 64 x 64
@@ -191,13 +272,14 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool ok
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(ok ? 16 : 0) : "memory");
 }
 
-__global__ void __launch_bounds__(256, 2) k_lu_zgemm(int N, size_t stride, int r0, int c0, int k0, int M, int n, int K,
-                                                     double2* __restrict__ Aall) {
+__global__ void __launch_bounds__(256, 2) k_lu_zgemm(int N, const double2* Aall, size_t astride, double2* Call,
+                                                     size_t cstride, int r0, int c0, int k0, int M, int n, int K) {
     extern __shared__ double zg_smem[];
     double* As = zg_smem;                      // [2][ZG_K][ZG_AP]
     double* Bs = zg_smem + 2 * ZG_K * ZG_AP;   // [2][ZG_N][ZG_BP]
     const int f = blockIdx.z;
-    double2* A = Aall + (size_t)f * stride;
+    const double2* A = Aall + (size_t)f * astride;  // the A operand (rows r0 .., columns k0 ..)
+    double2* C = Call + (size_t)f * cstride;        // the B operand (rows k0 .., columns c0 ..) and C
     const int tm = blockIdx.x * ZG_M, tn = blockIdx.y * ZG_N;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp & 3, wn = warp >> 2;
     const int nchunk = (K + ZG_K - 1) / ZG_K;
@@ -214,7 +296,7 @@ __global__ void __launch_bounds__(256, 2) k_lu_zgemm(int N, size_t stride, int r
             {  // B: column cc, complex row kk
                 const int cc = idx >> 4, kk = idx & 15, kg = kc * ZG_K + kk;
                 const bool ok = tn + cc < n && kg < K;
-                const double2* src = ok ? A + (size_t)(k0 + kg) + (size_t)(c0 + tn + cc) * N : A;
+                const double2* src = ok ? C + (size_t)(k0 + kg) + (size_t)(c0 + tn + cc) * N : C;
                 cp_async16(Bs + (size_t)(buf * ZG_N + cc) * ZG_BP + 2 * kk, src, ok);
             }
         }
@@ -268,7 +350,7 @@ __global__ void __launch_bounds__(256, 2) k_lu_zgemm(int N, size_t stride, int r
             for (int e = 0; e < 2; e++) {
                 const int ccol = tn + wn * 32 + 8 * j + 2 * (lane & 3) + e;
                 if (ccol < n) {
-                    double* c = reinterpret_cast<double*>(A + (size_t)(r0 + crow) + (size_t)(c0 + ccol) * N) + (R & 1);
+                    double* c = reinterpret_cast<double*>(C + (size_t)(r0 + crow) + (size_t)(c0 + ccol) * N) + (R & 1);
                     *c -= acc[i][j][e];
                 }
             }
@@ -320,56 +402,47 @@ struct LuF64 {
     void trsm(int c0, int n1, int cb, int ce) {
         if (ce <= cb || n1 <= 1) return;
         KernelProfiler& P = profiler();
-        const int cols = ce - cb;
-        const size_t sm = sizeof(double2) * (size_t)n1 * (n1 - 1) / 2;
-        // each CTA loads the triangle once and walks many columns: a few CTAs per matrix
-        const int threads = 1024, nw = threads / 32;
-        const int gx = std::max(1, std::min((cols + nw - 1) / nw, 16));
         P.begin(s);
-        if (n1 <= 32)
-            k_lu_trsm<1><<<dim3(gx, F), threads, sm, s>>>(N, c0, n1, cb, ce, A, stride);
-        else if (n1 <= 64)
-            k_lu_trsm<2><<<dim3(gx, F), threads, sm, s>>>(N, c0, n1, cb, ce, A, stride);
-        else
-            k_lu_trsm<4><<<dim3(gx, F), threads, sm, s>>>(N, c0, n1, cb, ce, A, stride);
+        launch_lu_trsm<false>(N, F, c0, n1, cb, ce, A, stride, A, stride, s);
         // complex TRSM: 4 n1^2 cols real flops
-        P.end(KF_LU_TRSM, (double)F * 4.0 * n1 * (double)n1 * cols, s);
+        P.end(KF_LU_TRSM, (double)F * 4.0 * n1 * (double)n1 * (ce - cb), s);
         (*launches)++;
     }
     void gemm(int r0, int c0, int k0, int M, int n, int K) {
         if (M <= 0 || n <= 0 || K <= 0) return;
         KernelProfiler& P = profiler();
         P.begin(s);
-        k_lu_zgemm<<<dim3((M + ZG_M - 1) / ZG_M, (n + ZG_N - 1) / ZG_N, F), 256, ZG_SMEM, s>>>(N, stride, r0, c0, k0, M, n,
-                                                                                              K, A);
+        k_lu_zgemm<<<dim3((M + ZG_M - 1) / ZG_M, (n + ZG_N - 1) / ZG_N, F), 256, ZG_SMEM, s>>>(N, A, stride, A, stride, r0,
+                                                                                              c0, k0, M, n, K);
         // complex C -= A B: 8 M n K real flops
         P.end(KF_LU_GEMM, (double)F * 8.0 * M * (double)n * K, s);
         (*launches)++;
     }
-    // columns c0 .. c0 + w - 1, rows c0 .. N - 1 (dgetrf2's recursion: the left half, its interchanges and
-    // triangular solve on the right half, the update of the right half, the right half, its
-    // interchanges on the left half)
+    // columns c0 .. c0 + w - 1, rows c0 .. N - 1 of the panel pk0 .. pk0 + pnb - 1 (dgetrf2's recursion:
+    // the left half, the triangular solve of the right half's block row, the update of the right half,
+    // the right half; the strips swap their rows across the whole panel, so no interchanges between)
+    int pk0 = 0, pnb = 0;
     void panel(int c0, int w) {
         if (w <= LU_BASE) {
             KernelProfiler& P = profiler();
             const double m = N - c0;
             P.begin(s);
-            k_lu_base<<<F, 512, 0, s>>>(N, c0, w, A, stride, ipiv, info);
+            k_lu_base<<<F, 512, 0, s>>>(N, c0, w, pk0, pnb, A, stride, ipiv, info);
             P.end(KF_LU_PANEL, (double)F * 8.0 * (m * w * w - (double)w * w * w / 3.0), s);
             (*launches)++;
             return;
         }
         const int n1 = w / 2 / LU_BASE * LU_BASE > 0 ? w / 2 / LU_BASE * LU_BASE : w / 2, n2 = w - n1;
         panel(c0, n1);
-        laswp(c0, c0 + n1, c0 + n1, c0 + w, 0, 0);
         trsm(c0, n1, c0 + n1, c0 + w);
         gemm(c0 + n1, c0 + n1, c0, N - c0 - n1, n2, n1);
         panel(c0 + n1, n2);
-        laswp(c0 + n1, c0 + w, c0, c0 + n1, 0, 0);
     }
     void factor() {
         for (int k0 = 0; k0 < N; k0 += LU_NB) {
             const int nb = std::min(LU_NB, N - k0);
+            pk0 = k0;
+            pnb = nb;
             panel(k0, nb);
             laswp(k0, k0 + nb, 0, k0, k0 + nb, N);
             trsm(k0, nb, k0 + nb, N);
@@ -379,11 +452,17 @@ struct LuF64 {
 };
 }  // namespace
 
+static void lu_f64_attributes() {
+    cudaFuncSetAttribute(k_lu_zgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, ZG_SMEM);
+    cudaFuncSetAttribute(k_lu_trsm<4, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(double2) * LU_NB * (LU_NB - 1) / 2));
+    cudaFuncSetAttribute(k_lu_trsm<4, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(double2) * LU_NB * (LU_NB + 1) / 2));
+}
+
 int lu_factor_f64(int N, int F, double2* A, size_t stride, int32_t* ipiv, int32_t* info, cudaStream_t s,
                   int64_t* launches) {
-    cudaFuncSetAttribute(k_lu_zgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, ZG_SMEM);
-    cudaFuncSetAttribute(k_lu_trsm<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(sizeof(double2) * LU_NB * (LU_NB - 1) / 2));
+    lu_f64_attributes();
     cudaMemsetAsync(info, 0, sizeof(int32_t) * F, s);
     LuF64Streams& side = lu_f64_streams();
     const int ng = side.ok ? std::min(LU_F64_GROUPS, F) : 1;
@@ -404,29 +483,25 @@ int lu_factor_f64(int N, int F, double2* A, size_t stride, int32_t* ipiv, int32_
 }
 
 // ------------------------------------------------------------------ substitution
-// One block per matrix: the row permutation from the swaps (in shared memory), the gather of P B
-// into X, then forward substitution with the unit lower factor and back substitution with the
-// upper factor, in blocks of 32 rows: a warp per right-hand side solves the 32 x 32 triangle,
-// then every thread updates its rows of the rest with the block's solution.
-// Bin and X are [F][nrhs][N] (one column per right-hand side).
-template <int NR>
-__global__ void __launch_bounds__(1024) k_lu_solve_f64(int N, const double2* __restrict__ LUall, size_t stride,
-                                                       const int32_t* __restrict__ ipiv, int nrhs,
-                                                       const double2* __restrict__ Ball, double2* __restrict__ Xall) {
+// X = A^-1 B with the factors: the row interchanges gathered into a permutation (one CTA per matrix),
+// P B gathered into X, then blocked forward and back substitution over the LU_NB-row blocks: each block
+// solved by the triangular kernel (unit lower, then upper with its diagonal), the rest of the right-hand
+// sides updated by the warp-MMA product with the block's factor columns -- every factor entry read once
+// per direction, all the batch's matrices in each launch.  B and X are [F][nrhs][N].
+__global__ void k_lu_permute(int N, const int32_t* __restrict__ ipiv, int nrhs, const double2* __restrict__ Ball,
+                             double2* __restrict__ Xall) {
     extern __shared__ int32_t perm[];
-    __shared__ double2 xs[32][NR];
     const int f = blockIdx.x;
-    const double2* LU = LUall + (size_t)f * stride;
+    const int32_t* pv = ipiv + (size_t)f * N;
     const double2* B = Ball + (size_t)f * nrhs * N;
     double2* X = Xall + (size_t)f * nrhs * N;
-    const int32_t* pv = ipiv + (size_t)f * N;
     for (int i = threadIdx.x; i < N; i += blockDim.x) perm[i] = i;
     __syncthreads();
     if (threadIdx.x == 0)
         for (int i = 0; i < N; i++) {
-            int p = pv[i];
+            const int p = pv[i];
             if (p != i) {
-                int t = perm[i];
+                const int t = perm[i];
                 perm[i] = perm[p];
                 perm[p] = t;
             }
@@ -434,91 +509,30 @@ __global__ void __launch_bounds__(1024) k_lu_solve_f64(int N, const double2* __r
     __syncthreads();
     for (int c = 0; c < nrhs; c++)
         for (int i = threadIdx.x; i < N; i += blockDim.x) X[(size_t)c * N + i] = B[(size_t)c * N + perm[i]];
-    __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // forward: L y = P b
-    for (int b0 = 0; b0 < N; b0 += 32) {
-        int bn = min(32, N - b0);
-        if (warp < nrhs) {
-            double2 x = lane < bn ? X[(size_t)warp * N + b0 + lane] : make_double2(0.0, 0.0);
-            for (int p = 0; p < bn; p++) {
-                double2 xp = make_double2(__shfl_sync(0xffffffffu, x.x, p), __shfl_sync(0xffffffffu, x.y, p));
-                if (lane > p && lane < bn) x = csub(x, cmul(LU[(size_t)(b0 + lane) + (size_t)(b0 + p) * N], xp));
-            }
-            if (lane < bn) {
-                X[(size_t)warp * N + b0 + lane] = x;
-                xs[lane][warp] = x;
-            }
-        }
-        __syncthreads();
-        for (int i = b0 + bn + threadIdx.x; i < N; i += blockDim.x) {
-            double2 acc[NR];
-#pragma unroll
-            for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
-            for (int p = 0; p < bn; p++) {
-                double2 l = LU[(size_t)i + (size_t)(b0 + p) * N];
-#pragma unroll
-                for (int c = 0; c < NR; c++) {
-                    acc[c].x += l.x * xs[p][c].x - l.y * xs[p][c].y;
-                    acc[c].y += l.x * xs[p][c].y + l.y * xs[p][c].x;
-                }
-            }
-            for (int c = 0; c < nrhs; c++) X[(size_t)c * N + i] = csub(X[(size_t)c * N + i], acc[c]);
-        }
-        __syncthreads();
-    }
-    // backward: U x = y, blocks from the bottom
-    const int nblk = (N + 31) / 32;
-    for (int bb = nblk - 1; bb >= 0; bb--) {
-        int b0 = bb * 32, bn = min(32, N - b0);
-        if (warp < nrhs) {
-            double2 x = lane < bn ? X[(size_t)warp * N + b0 + lane] : make_double2(0.0, 0.0);
-            for (int p = bn - 1; p >= 0; p--) {
-                if (lane == p) {
-                    double2 up = LU[(size_t)(b0 + p) + (size_t)(b0 + p) * N];
-                    double d = cabs2(up);
-                    x = make_double2((x.x * up.x + x.y * up.y) / d, (x.y * up.x - x.x * up.y) / d);
-                }
-                double2 xp = make_double2(__shfl_sync(0xffffffffu, x.x, p), __shfl_sync(0xffffffffu, x.y, p));
-                if (lane < p) x = csub(x, cmul(LU[(size_t)(b0 + lane) + (size_t)(b0 + p) * N], xp));
-            }
-            if (lane < bn) {
-                X[(size_t)warp * N + b0 + lane] = x;
-                xs[lane][warp] = x;
-            }
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < b0; i += blockDim.x) {
-            double2 acc[NR];
-#pragma unroll
-            for (int c = 0; c < NR; c++) acc[c] = make_double2(0.0, 0.0);
-            for (int p = 0; p < bn; p++) {
-                double2 u = LU[(size_t)i + (size_t)(b0 + p) * N];
-#pragma unroll
-                for (int c = 0; c < NR; c++) {
-                    acc[c].x += u.x * xs[p][c].x - u.y * xs[p][c].y;
-                    acc[c].y += u.x * xs[p][c].y + u.y * xs[p][c].x;
-                }
-            }
-            for (int c = 0; c < nrhs; c++) X[(size_t)c * N + i] = csub(X[(size_t)c * N + i], acc[c]);
-        }
-        __syncthreads();
-    }
 }
 
 int lu_solve_f64(int N, int F, const double2* LU, size_t stride, const int32_t* ipiv, int nrhs, const double2* B,
                  double2* X, cudaStream_t s) {
-    size_t smem = sizeof(int32_t) * (size_t)N;
+    const size_t smem = sizeof(int32_t) * (size_t)N;
     if (nrhs > 32 || smem > 200 * 1024) return 1;
-    if (nrhs <= 8) {
-        cudaFuncSetAttribute(k_lu_solve_f64<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_lu_solve_f64<8><<<F, 1024, smem, s>>>(N, LU, stride, ipiv, nrhs, B, X);
-    } else if (nrhs <= 16) {
-        cudaFuncSetAttribute(k_lu_solve_f64<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_lu_solve_f64<16><<<F, 1024, smem, s>>>(N, LU, stride, ipiv, nrhs, B, X);
-    } else {
-        cudaFuncSetAttribute(k_lu_solve_f64<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_lu_solve_f64<32><<<F, 1024, smem, s>>>(N, LU, stride, ipiv, nrhs, B, X);
+    lu_f64_attributes();
+    cudaFuncSetAttribute(k_lu_permute, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_lu_permute<<<F, 512, smem, s>>>(N, ipiv, nrhs, B, X);
+    const size_t xs = (size_t)nrhs * N;
+    auto update = [&](int r0, int k0, int M, int K) {
+        if (M > 0)
+            k_lu_zgemm<<<dim3((M + ZG_M - 1) / ZG_M, 1, F), 256, ZG_SMEM, s>>>(N, LU, stride, X, xs, r0, 0, k0, M, nrhs,
+                                                                                K);
+    };
+    for (int b0 = 0; b0 < N; b0 += LU_NB) {  // L y = P b
+        const int nb = std::min(LU_NB, N - b0);
+        if (nb > 1) launch_lu_trsm<false>(N, F, b0, nb, 0, nrhs, LU, stride, X, xs, s);
+        update(b0 + nb, b0, N - b0 - nb, nb);
+    }
+    for (int b0 = (N - 1) / LU_NB * LU_NB; b0 >= 0; b0 -= LU_NB) {  // U x = y, the last block first
+        const int nb = std::min(LU_NB, N - b0);
+        launch_lu_trsm<true>(N, F, b0, nb, 0, nrhs, LU, stride, X, xs, s);
+        update(0, b0, b0, nb);
     }
     return 0;
 }

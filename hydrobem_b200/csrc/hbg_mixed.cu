@@ -9,6 +9,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "hbg_mixed.h"
@@ -252,8 +253,9 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     double* scr = fin ? (double*)get(WS_SCR, sizeof(double) * 6912 * 3 * B) : nullptr;
     double* fpt = fin ? (double*)get(WS_FPT, sizeof(double) * FP_PLANES * N * B) : nullptr;
     const int nfp = field.P;
-    double* dout = (double*)get(WS_OUT, sizeof(double) *
-                                            (2 * (size_t)D * D + 4 * (size_t)H * 2 * D + (size_t)nfp * 2 * (D + 3 * H)) * B);
+    // A, B [D][D], X, FK, SC, motions, Haskind [H][D], field values [P][D] and 3 x [P][H] per frequency
+    const size_t out_per = 2 * (size_t)D * D + 5 * (size_t)H * 2 * D + (size_t)nfp * 2 * (D + 3 * H), DD = (size_t)D * D;
+    double* dout = (double*)get(WS_OUT, sizeof(double) * out_per * B);
     double* fq = nfp && fin ? (double*)get(WS_FQ, sizeof(double) * FP_PLANES * (size_t)(N + nfp) * B) : nullptr;
     if (!okb) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
     last_surrogate_pairs() = 0;
@@ -287,9 +289,12 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     cudaFuncSetAttribute(k_tri_step<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(12));
     cudaFuncSetAttribute(k_tri_step<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(16));
     // the persistent sweeps: as many CTAs as fit at once
-    const int nr_sweep = nrhs <= 8 ? 8 : nrhs <= 10 ? 10 : nrhs <= 12 ? 12 : 16;
-    const void* sweep_fn = nr_sweep == 8 ? (const void*)k_tri_sweep<8> : nr_sweep == 10 ? (const void*)k_tri_sweep<10>
-                           : nr_sweep == 12 ? (const void*)k_tri_sweep<12> : (const void*)k_tri_sweep<16>;
+    const int nr_sweep = nrhs <= 8 ? 8 : nrhs <= 10 ? 10 : nrhs <= 12 ? 12 : nrhs <= 16 ? 16 : 32;
+    const void* sweep_fn = nr_sweep == 8    ? (const void*)k_tri_sweep<8>
+                           : nr_sweep == 10 ? (const void*)k_tri_sweep<10>
+                           : nr_sweep == 12 ? (const void*)k_tri_sweep<12>
+                           : nr_sweep == 16 ? (const void*)k_tri_sweep<16>
+                                            : (const void*)k_tri_sweep<32>;
     cudaFuncSetAttribute(sweep_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(nr_sweep));
     int sweep_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&sweep_per_sm, sweep_fn, TRI_THREADS, tri_smem_bytes(nr_sweep));
@@ -298,9 +303,6 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     for (int h = 0; h < H; h++) heads[h] = pr.headings_deg[h] * PI / 180.0;
     std::vector<FreqInfo> fi(B);
     std::vector<FdParams> fdh(B);
-    // per frequency: A, B [D][D], X, FK, SC, motions [H][D] complex, field values [P][D] and 3 x [P][H]
-    // A, B [D][D], X, FK, SC, motions [H][D], field values [P][D] and 3 x [P][H], Haskind [H][D]
-    const size_t out_per = 2 * (size_t)D * D + 5 * (size_t)H * 2 * D + (size_t)nfp * 2 * (D + 3 * H), DD = (size_t)D * D;
     // page-locked: the reads of norms, outputs and the error flag queue behind the work, no host wait
     double* hout = (double*)ws.host(HS_OUT, sizeof(double) * (out_per * B + 1));
     double* hn = (double*)ws.host(HS_NORMS, sizeof(double) * IR_MAX_IT * 2 * (size_t)BS);
@@ -400,7 +402,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     auto trisolve = [&](float2* xv, int nb) {
         const int nblk_i = Np / TB;
         P.begin(s);
-        if (nrhs <= 16) {  // one persistent sweep per direction
+        if (nrhs <= 32) {  // one persistent sweep per direction
             const int grid = std::min(nblk_i * nb, sweep_ctas);
             const size_t sm = tri_smem_bytes(nr_sweep);
             for (int up = 1; up >= 0; up--) {
@@ -411,8 +413,10 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                     k_tri_sweep<10><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
                 else if (nr_sweep == 12)
                     k_tri_sweep<12><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
-                else
+                else if (nr_sweep == 16)
                     k_tri_sweep<16><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
+                else
+                    k_tri_sweep<32><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
                 (*launches)++;
             }
             P.end(KF_LU_SOLVE, 8.0 * (double)NP2 * nb, s);
@@ -795,7 +799,14 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             }
         }
         P.flush();
-        if (cudaGetLastError() != cudaSuccess) MIXED_FAIL(HB_ERR_INTERNAL, "CUDA error in the mixed-precision solve", f0);
+        {
+            const cudaError_t ce = cudaGetLastError();
+            if (ce != cudaSuccess) {
+                static thread_local std::string why;
+                why = std::string("CUDA error in the mixed-precision solve: ") + cudaGetErrorString(ce);
+                MIXED_FAIL(HB_ERR_INTERNAL, why.c_str(), f0);
+            }
+        }
         if (*herr == 8) MIXED_FAIL(HB_ERR_INTERNAL, "a triangular sweep wait timed out", f0);
         if (*herr == 11) MIXED_FAIL(HB_ERR_NUMERICAL, "singular motion equation", f0);
         if (*herr != 0 && *herr != 10) MIXED_FAIL(HB_ERR_INTERNAL, "a tensor-core pipeline wait timed out", f0);

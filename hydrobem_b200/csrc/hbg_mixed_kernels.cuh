@@ -1393,7 +1393,7 @@ __device__ __forceinline__ void st_release_gpu(int* p, int v) {
 }
 
 template <int NR>
-__global__ void __launch_bounds__(TRI_THREADS, 2) k_tri_sweep(int Np, size_t bstride, const float* __restrict__ W,
+__global__ void __launch_bounds__(TRI_THREADS, NR > 16 ? 1 : 2) k_tri_sweep(int Np, size_t bstride, const float* __restrict__ W,
                                                            const float2* __restrict__ DINV, int nrhs,
                                                            float2* __restrict__ Xall, int nb, int upper_t,
                                                            int* __restrict__ ctrl, int* __restrict__ err) {

@@ -128,3 +128,51 @@ def reflect_full(quarter_panels: np.ndarray) -> np.ndarray:
 
 def config_cylinder(n_phi, n_z, n_r, radius=1.0, draft=0.5) -> np.ndarray:
     return cylinder(radius, draft, n_phi=n_phi, n_z=n_z, n_r=n_r, quarter=False)
+
+
+GRAVITY = 9.80665
+
+
+def uneven_bodies(count=64, seed=20261203):
+    """The batched uneven workload: ``count`` bodies drawn from ``seed`` -- truncated cylinders (radius
+    U[0.5, 3] m, draught U[0.3, 2] m) or hemispheres (radius U[0.5, 3] m) with panel counts N ~ U[800,
+    6000] rounded to the generators' grids -- each with 16 frequencies of wavenumber K r ~ U[0.1, 10].
+    Returns [(vertices, omegas)]; the grids are drawn first and a mesh is built only for the bodies
+    asked for, so ``uneven_bodies(count)[i]`` is the same body for every count > i."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        r, d, n = rng.uniform(0.5, 3.0), rng.uniform(0.3, 2.0), int(rng.uniform(800, 6000))
+        if rng.uniform() < 0.5:
+            nphi = max(8, int(round(np.sqrt(n) / 4)) * 4)
+            nz = max(2, int(round(n / (2 * nphi))))
+            v = cylinder(r, d, nphi, nz, nz)
+        else:
+            nphi = max(8, int(round(np.sqrt(2 * n) / 4)) * 4)
+            v = hemisphere(r, max(2, int(round(n / nphi))), nphi)
+        omegas = np.sqrt(rng.uniform(0.1, 10.0, 16) / r * GRAVITY)
+        out.append((v, omegas))
+    return out
+
+
+def cylinder_array(n_phi=64, n_z=32, n_r=32, spacing=4.0):
+    """Three cylinders of radius 1 m and draught 1 m, ``spacing`` apart along x, each rotating about its own
+    axis at the waterline: (vertices, panel body, rotation centres)."""
+    one = cylinder(1.0, 1.0, n_phi, n_z, n_r)
+    parts, body, centers = [], [], []
+    for b, x in enumerate((-spacing, 0.0, spacing)):
+        c = one.copy()
+        c[..., 0] += x
+        parts.append(c)
+        body.append(np.full(len(c), b, np.int32))
+        centers.append([x, 0.0, 0.0])
+    return np.concatenate(parts), np.concatenate(body), centers
+
+
+def barge(n=(64, 32, 75)):
+    """The 80 m x 20 m barge of 10 m draught with its interior waterplane lid: (vertices, kinds) with the
+    lid's nx ny panels last and of kind 1 (interior surface)."""
+    v = box(40.0, 10.0, 10.0, n=n, lid=True)
+    kinds = np.zeros(len(v), np.int32)
+    kinds[-n[0] * n[1]:] = 1
+    return v, kinds

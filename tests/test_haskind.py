@@ -82,7 +82,7 @@ def test_gpu_haskind_identity_hemisphere(precision, hemi_oracle):
 
     quarter = meshes.hemisphere(1.0, 24, 24, quarter=True)
     prec = nv.HBG_MIXED if precision == "mixed" else nv.HBG_FP64
-    gpu = nv.solve(quarter, OMEGAS, HEADS, symmetry=nv.HBG_SYM_BOTH, precision=prec)
+    gpu = nv.solve(quarter, OMEGAS, HEADS, symmetry=nv.SYM_BOTH, precision=prec)
     ref = hemi_oracle
     scale = np.maximum(np.abs(ref["HK"]).max(axis=0, keepdims=True), 1e-3 * peak(ref["HK"]))
     err = float((np.abs(gpu["HK"] - ref["HK"]) / scale).max())

@@ -131,21 +131,10 @@ def test_mixed_large_barge_with_lid():
 
 
 def _c3_body(index):
-    """Body `index` of the 64-body configuration (seed 20261203: cylinders or hemispheres of radius
-    U[0.5, 3], draught U[0.3, 2], N ~ U[800, 6000] rounded to the generators' grids, 16 frequencies with
-    K r ~ U[0.1, 10], headings 0 and 45 degrees)."""
-    rng = np.random.default_rng(20261203)
-    for b in range(index + 1):
-        r, d, n = rng.uniform(0.5, 3.0), rng.uniform(0.3, 2.0), int(rng.uniform(800, 6000))
-        if rng.uniform() < 0.5:
-            nphi = max(8, int(round(np.sqrt(n) / 4)) * 4)
-            nz = max(2, int(round(n / (2 * nphi))))
-            v = meshes.cylinder(r, d, nphi, nz, nz)
-        else:
-            nphi = max(8, int(round(np.sqrt(2 * n) / 4)) * 4)
-            v = meshes.hemisphere(r, max(2, int(round(n / nphi))), nphi)
-        omegas = np.sqrt(rng.uniform(0.1, 10.0, 16) / r * 9.80665)
-    return v, omegas
+    """Body `index` of the 64-body configuration (meshes.uneven_bodies: seed 20261203, cylinders or
+    hemispheres of radius U[0.5, 3], draught U[0.3, 2], N ~ U[800, 6000] rounded to the generators'
+    grids, 16 frequencies with K r ~ U[0.1, 10])."""
+    return meshes.uneven_bodies(index + 1)[index]
 
 
 def test_mixed_falls_back_to_fp64_where_refinement_cannot_converge():

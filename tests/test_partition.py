@@ -20,9 +20,9 @@ ROOT = Path(__file__).resolve().parents[1]
 
 
 def c3_sizes():
-    """Panel and frequency counts of the 64-body configuration, drawn as tests/test_mixed.py's _c3_body
-    draws its bodies (seed 20261203: cylinders with n_phi (n_z + n_r) panels, n_r = n_z, or hemispheres
-    with n_theta n_phi panels; N ~ U[800, 6000] rounded to those grids; 16 frequencies each)."""
+    """Panel and frequency counts of the 64-body configuration, drawn as meshes.uneven_bodies draws its
+    bodies (seed 20261203: cylinders with n_phi (n_z + n_r) panels, n_r = n_z, or hemispheres with
+    n_theta n_phi panels; N ~ U[800, 6000] rounded to those grids; 16 frequencies each)."""
     rng = np.random.default_rng(20261203)
     out = []
     for _ in range(64):
@@ -42,12 +42,11 @@ def c3_sizes():
 
 def test_c3_sizes_follow_the_generators():
     """The counts above are those of the meshes the GPU tests build (a few bodies checked)."""
-    from test_mixed import _c3_body
+    from hydrobem_b200 import meshes
 
     sizes = c3_sizes()
-    for b in (0, 1, 30):
-        v, om = _c3_body(b)
-        assert (len(v), len(om)) == sizes[b]
+    bodies = meshes.uneven_bodies(64)
+    assert [(len(v), len(om)) for v, om in bodies] == sizes
 
 
 def test_plan_covers_every_unit_once():

@@ -87,7 +87,7 @@ def _gpu_solver(precision):
     prec = nv.HBG_MIXED if precision == "mixed" else nv.HBG_FP64
 
     def solve(v, w, depth):
-        return nv.solve(v, w, [], symmetry=nv.HBG_SYM_BOTH, depth=depth, precision=prec)
+        return nv.solve(v, w, [], symmetry=nv.SYM_BOTH, depth=depth, precision=prec)
 
     return solve
 
