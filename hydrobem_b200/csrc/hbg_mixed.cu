@@ -315,10 +315,9 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     for (auto fn : {(const void*)k_cgemv_tma<8>, (const void*)k_cgemv_tma<10>, (const void*)k_cgemv_tma<12>,
                     (const void*)k_cgemv_tma<16>})
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gv_smem_bytes<16>());
-    // the TMA form for up to 16 right-hand sides (its maps cover exactly the matrices and vectors
-    // of the batch); the register form otherwise
+    // the TMA form (its maps cover exactly the matrices and vectors of the batch), beyond 16 right-hand
+    // sides in column chunks of 16 (the matrix streamed once a chunk); the register form if a map fails
     auto gemv_tma = [&](const float* Mm, const double2* xv, int ldx, int nb, int nzt, cudaStream_t s) -> bool {
-        if (nrhs > 16) return false;
         CUtensorMap mM, mX;
         const uint64_t dm[4] = {(uint64_t)Np, (uint64_t)Np, 2, (uint64_t)nb};
         const uint64_t sm[3] = {(uint64_t)Np * 4, NP2 * 4, MB * 4};
@@ -331,22 +330,24 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             !make_map_box(&mX, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void*)xv, dx, sx, bx))
             return false;
         dim3 g((Nm + GV_ROWS - 1) / GV_ROWS, nb, nzt);
-        if (nr == 8)
-            k_cgemv_tma<8><<<g, GV_THREADS, gv_smem_bytes<8>(), s>>>(mM, mX, Nm, nrhs, part, nb, err);
-        else if (nr == 10)
-            k_cgemv_tma<10><<<g, GV_THREADS, gv_smem_bytes<10>(), s>>>(mM, mX, Nm, nrhs, part, nb, err);
-        else if (nr == 12)
-            k_cgemv_tma<12><<<g, GV_THREADS, gv_smem_bytes<12>(), s>>>(mM, mX, Nm, nrhs, part, nb, err);
-        else
-            k_cgemv_tma<16><<<g, GV_THREADS, gv_smem_bytes<16>(), s>>>(mM, mX, Nm, nrhs, part, nb, err);
+        for (int c0 = 0; c0 < nrhs; c0 += 16) {
+            if (nr == 8)
+                k_cgemv_tma<8><<<g, GV_THREADS, gv_smem_bytes<8>(), s>>>(mM, mX, Nm, nrhs, c0, part, nb, err);
+            else if (nr == 10)
+                k_cgemv_tma<10><<<g, GV_THREADS, gv_smem_bytes<10>(), s>>>(mM, mX, Nm, nrhs, c0, part, nb, err);
+            else if (nr == 12)
+                k_cgemv_tma<12><<<g, GV_THREADS, gv_smem_bytes<12>(), s>>>(mM, mX, Nm, nrhs, c0, part, nb, err);
+            else
+                k_cgemv_tma<16><<<g, GV_THREADS, gv_smem_bytes<16>(), s>>>(mM, mX, Nm, nrhs, c0, part, nb, err);
+        }
         return true;
     };
     const int nz_tma = (Nm + GV_CHUNK - 1) / GV_CHUNK;
     for (auto fn : {(const void*)k_cgemv32_tma<8>, (const void*)k_cgemv32_tma<10>, (const void*)k_cgemv32_tma<12>,
                     (const void*)k_cgemv32_tma<16>})
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gv32_smem_bytes<16>());
-    // r = rk - M d with the complex64 correction d (FP32 products, FP64 sums; up to 16 columns): the
-    // residual after a correction that is small against the solution
+    // r = rk - M d with the complex64 correction d (FP32 products, FP64 sums; beyond 16 columns in chunks):
+    // the residual after a correction that is small against the solution
     auto gemv32 = [&](const float* Mm, const float2* dv, const float2* rk, float2* out, int nb) {
         CUtensorMap mM, mD;
         const uint64_t dm[4] = {(uint64_t)Np, (uint64_t)Np, 2, (uint64_t)nb};
@@ -361,14 +362,16 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             return false;
         P.begin(s);
         dim3 g((Nm + GV_ROWS - 1) / GV_ROWS, nb, nz_tma);
-        if (nr == 8)
-            k_cgemv32_tma<8><<<g, GV_THREADS, gv32_smem_bytes<8>(), s>>>(mM, mD, Nm, nrhs, part, nb, err);
-        else if (nr == 10)
-            k_cgemv32_tma<10><<<g, GV_THREADS, gv32_smem_bytes<10>(), s>>>(mM, mD, Nm, nrhs, part, nb, err);
-        else if (nr == 12)
-            k_cgemv32_tma<12><<<g, GV_THREADS, gv32_smem_bytes<12>(), s>>>(mM, mD, Nm, nrhs, part, nb, err);
-        else
-            k_cgemv32_tma<16><<<g, GV_THREADS, gv32_smem_bytes<16>(), s>>>(mM, mD, Nm, nrhs, part, nb, err);
+        for (int c0 = 0; c0 < nrhs; c0 += 16) {
+            if (nr == 8)
+                k_cgemv32_tma<8><<<g, GV_THREADS, gv32_smem_bytes<8>(), s>>>(mM, mD, Nm, nrhs, c0, part, nb, err);
+            else if (nr == 10)
+                k_cgemv32_tma<10><<<g, GV_THREADS, gv32_smem_bytes<10>(), s>>>(mM, mD, Nm, nrhs, c0, part, nb, err);
+            else if (nr == 12)
+                k_cgemv32_tma<12><<<g, GV_THREADS, gv32_smem_bytes<12>(), s>>>(mM, mD, Nm, nrhs, c0, part, nb, err);
+            else
+                k_cgemv32_tma<16><<<g, GV_THREADS, gv32_smem_bytes<16>(), s>>>(mM, mD, Nm, nrhs, c0, part, nb, err);
+        }
         k_gemv_reduce<float2, float2><<<dim3((unsigned)(((size_t)nrhs * Nm + 255) / 256), nb), 256, 0, s>>>(
             Nm, nrhs, nb, nz_tma, part, rk, Np, out, Np);
         P.end(KF_MIXED_RESIDUAL, 8.0 * (double)Nm * Nm * nb, s);
@@ -742,7 +745,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             // correction kept in rs); the host-driven corrections beyond `guess` use b - A x again.
             const int guess = std::min(std::max(ir_guess(), 2), IR_MAX_IT);
             for (int i = 0; i < guess; i++) {
-                const bool more = i + 1 < guess, inc = more && i >= 1 && nrhs <= 16 && rs;
+                const bool more = i + 1 < guess, inc = more && i >= 1 && rs;
                 if (inc) cudaMemcpyAsync(rs, r, sizeof(float2) * nrhs * Np * ns, cudaMemcpyDeviceToDevice, s);
                 correction(i);
                 if (more && !(inc && gemv32(A32, r, rs, r, ns))) gemv(A32, x, Np, b, r, ns, KF_MIXED_RESIDUAL, s);

@@ -986,7 +986,7 @@ __host__ __device__ constexpr size_t gv_smem_bytes() {
 template <int NR>
 __global__ void __launch_bounds__(GV_THREADS) k_cgemv_tma(const __grid_constant__ CUtensorMap mapM,
                                                              const __grid_constant__ CUtensorMap mapX, int N,
-                                                             int nrhs, double2* __restrict__ part, int F,
+                                                             int nrhs, int c0, double2* __restrict__ part, int F,
                                                              int* __restrict__ err) {
     extern __shared__ uint8_t gv_raw[];
     uint8_t* base = align1024(gv_raw);
@@ -1020,7 +1020,7 @@ __global__ void __launch_bounds__(GV_THREADS) k_cgemv_tma(const __grid_constant_
                 tc::mbar_arrive_expect_tx(&full[s], (uint32_t)gv_tx_bytes<NR>());
                 tc::tma_load_4d(st, &mapM, &full[s], k0, n0, 0, f);
                 tc::tma_load_4d(st + GV_COLS * GV_ROWS * 4, &mapM, &full[s], k0, n0, 1, f);
-                tc::tma_load_4d(st + 2 * GV_COLS * GV_ROWS * 4, &mapX, &full[s], 2 * n0, 0, f, 0);
+                tc::tma_load_4d(st + 2 * GV_COLS * GV_ROWS * 4, &mapX, &full[s], 2 * n0, c0, f, 0);
             }
         }
         return;
@@ -1060,9 +1060,9 @@ __global__ void __launch_bounds__(GV_THREADS) k_cgemv_tma(const __grid_constant_
     const int k = k0 + t, kd = k + GV_WORKERS;
 #pragma unroll
     for (int c = 0; c < NR; c++)
-        if (c < nrhs) {
-            if (k < N) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
-            if (kd < N) part[(((size_t)z * F + f) * nrhs + c) * N + kd] = acd[c];
+        if (c0 + c < nrhs) {
+            if (k < N) part[(((size_t)z * F + f) * nrhs + c0 + c) * N + k] = acc[c];
+            if (kd < N) part[(((size_t)z * F + f) * nrhs + c0 + c) * N + kd] = acd[c];
         }
 }
 
@@ -1086,7 +1086,7 @@ __host__ __device__ constexpr size_t gv32_smem_bytes() {
 template <int NR>
 __global__ void __launch_bounds__(GV_THREADS) k_cgemv32_tma(const __grid_constant__ CUtensorMap mapM,
                                                                const __grid_constant__ CUtensorMap mapD, int N,
-                                                               int nrhs, double2* __restrict__ part, int F,
+                                                               int nrhs, int c0, double2* __restrict__ part, int F,
                                                                int* __restrict__ err) {
     extern __shared__ uint8_t gv_raw[];
     uint8_t* base = align1024(gv_raw);
@@ -1120,7 +1120,7 @@ __global__ void __launch_bounds__(GV_THREADS) k_cgemv32_tma(const __grid_constan
                 tc::mbar_arrive_expect_tx(&full[s], (uint32_t)gv32_tx_bytes<NR>());
                 tc::tma_load_4d(st, &mapM, &full[s], k0, n0, 0, f);
                 tc::tma_load_4d(st + GV_COLS * GV_ROWS * 4, &mapM, &full[s], k0, n0, 1, f);
-                tc::tma_load_4d(st + 2 * GV_COLS * GV_ROWS * 4, &mapD, &full[s], 2 * n0, 0, f, 0);
+                tc::tma_load_4d(st + 2 * GV_COLS * GV_ROWS * 4, &mapD, &full[s], 2 * n0, c0, f, 0);
             }
         }
         return;
@@ -1172,9 +1172,9 @@ __global__ void __launch_bounds__(GV_THREADS) k_cgemv32_tma(const __grid_constan
     const int k = k0 + t, kd = k + GV_WORKERS;
 #pragma unroll
     for (int c = 0; c < NR; c++)
-        if (c < nrhs) {
-            if (k < N) part[(((size_t)z * F + f) * nrhs + c) * N + k] = acc[c];
-            if (kd < N) part[(((size_t)z * F + f) * nrhs + c) * N + kd] = acd[c];
+        if (c0 + c < nrhs) {
+            if (k < N) part[(((size_t)z * F + f) * nrhs + c0 + c) * N + k] = acc[c];
+            if (kd < N) part[(((size_t)z * F + f) * nrhs + c0 + c) * N + kd] = acd[c];
         }
 }
 

@@ -10,8 +10,10 @@ Every fixture is a compressed .npz of numbers the reference's test suite holds o
 - cylinder_fd.npz    tests/data/cylinder_finite_depth.txt (eigenfunction-matching A, B)
 - hulme.npz          tests/data/hulme1982_full.txt (hemisphere A, B, Hulme 1982)
 - lo_cylinder_drift.npz  the reference solver's own outputs of that regression problem
-  (tests/data/regression/lo_cylinder_drift.npz: A, B, X, FK, SC, the motions (RAO) and the
-  hydrostatics of a floating cylinder with its mass and inertia, f32 / f64 as the reference stores them)
+  (tests/data/regression/lo_cylinder_drift.npz: A, B, X, FK, SC, the Haskind exciting force, the
+  motions (RAO), the Kochin functions with their angular derivatives, the mean drift by momentum
+  conservation and the hydrostatics of a floating cylinder with its mass and inertia, f32 / f64 as the
+  reference stores them)
 - lo_cylinder_field.npz  the reference solver's own field-point outputs of its regression problem
   lo_cylinder_field_body_points (the same cylinder held fixed, three points: the elevation at z = 0
   and p / (rho g) below, per radiation column and heading, complex64)
@@ -60,7 +62,10 @@ def main(argv):
     np.savez_compressed(HERE / "hulme.npz", vals=np.array([[float(t) for t in x] for x in r]))
     d = np.load(data / "regression" / "lo_cylinder_drift.npz")
     keep = ["omegas", "headings", "added_mass", "radiation_damping", "excitation_diffraction",
-            "excitation_froude_krylov", "excitation_scattering", "motion", "hydrostatics_volumes",
+            "excitation_froude_krylov", "excitation_scattering", "excitation_haskind", "motion",
+            "radiation_mode_ids", "kochin_angles", "kochin_radiation", "kochin_radiation_derivative",
+            "kochin_diffraction", "kochin_diffraction_derivative", "drift_momentum_conservation",
+            "drift_heading_pairs", "hydrostatics_volumes",
             "hydrostatics_volume", "hydrostatics_displaced_mass", "hydrostatics_center_of_buoyancy",
             "hydrostatics_waterplane_area", "hydrostatics_waterplane_centroid", "hydrostatics_stiffness_rho_g",
             "hydrostatics_stiffness", "hydrostatics_mass", "hydrostatics_center_of_gravity",

@@ -116,3 +116,43 @@ def test_gpu_haskind_through_the_model_abi():
     scale = np.maximum(np.abs(ref["HK"]).max(axis=0, keepdims=True), 1e-3 * peak(ref["HK"]))
     assert float((np.abs(hk - ref["HK"]) / scale).max()) <= 1e-9
     assert float((np.abs(hk32 - ref["HK"]) / scale).max()) <= 1e-6
+
+
+GOLDEN = __import__("pathlib").Path(__file__).resolve().parent / "golden" / "lo_cylinder_drift.npz"
+
+
+def _scaled(got, ref, floor=1e-3):
+    ref = np.asarray(ref)
+    scale = np.maximum(np.abs(ref).max(axis=0, keepdims=True), floor * np.abs(ref).max())
+    return float((np.abs(np.asarray(got) - ref) / scale).max())
+
+
+def test_oracle_haskind_against_the_reference_solve():
+    """The reference's stored Haskind force of its regression problem lo_cylinder_drift (a quarter
+    cylinder with two symmetry planes; float32 outputs of its production path): the oracle's to 2e-5."""
+    g = np.load(GOLDEN)
+    quarter = meshes.cylinder(1.0, 0.5, 8, 4, 4, quarter=True)
+    ref = O.solve_body(quarter, g["omegas"], g["headings"], symmetry=O.SYM_BOTH)
+    assert ref["HK"].shape == g["excitation_haskind"].shape
+    assert _scaled(ref["HK"], g["excitation_haskind"]) <= 2e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_gpu_haskind_against_the_reference_solve(precision):
+    from hydrobem_b200 import native as nv
+
+    g = np.load(GOLDEN)
+    with nv.Model() as m:
+        m.add("meshes", "cyl")
+        m.reals("meshes/cyl", "vertices", meshes.cylinder(1.0, 0.5, 8, 4, 4, quarter=True))
+        m.text("meshes/cyl", "symmetry", "xz_and_yz")
+        m.add("bodies", "body")
+        m.text("bodies/body", "mesh", "cyl")
+        m.reals("environment", "omegas", g["omegas"])
+        m.reals("environment", "headings", g["headings"])
+        m.text("options", "gpu_precision", precision)
+        res = m.solve()
+        hk = res.quantity("excitation_haskind_f64")
+        res.free()
+    assert _scaled(hk, g["excitation_haskind"]) <= 2e-5
