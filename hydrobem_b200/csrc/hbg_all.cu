@@ -2,6 +2,7 @@
 // compiled without floating-point contraction).
 #include "hbg_freq.cu"
 #include "hbg_motion.cu"
+#include "hbg_kochin.cu"
 #include "hbg_lu.cu"
 #include "hbg_mixed.cu"
 #include "hbg_peaks.cu"

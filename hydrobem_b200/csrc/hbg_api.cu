@@ -473,6 +473,11 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     if (D + H > 32) throw Failure{HB_ERR_UNSUPPORTED, "more than 32 right-hand sides (6 per body and one per heading)", body_index};
     // motions (motion.rs) need the rigid-body data; the hydrostatics records need only the panels
     const HbgRigid* rigid = pr.rigid;
+    // the Kochin functions and the momentum drift (the motions enter when the rigid data are given)
+    const int TK = pr.kochin_angles > 0 && H > 0 ? pr.kochin_angles : 0;
+    if (pr.kochin_angles < 0) throw Failure{HB_ERR_VALUE, "negative Kochin angle count", body_index};
+    if ((size_t)TK * H > (size_t)KOCHIN_MAX_HT)
+        throw Failure{HB_ERR_UNSUPPORTED, "Kochin angles x headings above 4096", body_index};
     const bool motions = pr.out.motions != nullptr && H > 0;
     if (pr.out.motions && !rigid)
         throw Failure{HB_ERR_VALUE, "motions need the rigid-body data (mass, centre of gravity, inertia)", body_index};
@@ -688,15 +693,19 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
             // the frequencies whose refinement did not converge, solved again by the FP64 form (pivoted LU)
             const size_t nf = fallback.size(), DDo = (size_t)D * D, HD = (size_t)H * 2 * D;
             const size_t PD = (size_t)(field ? nfp : 0) * 2 * D, PH = (size_t)(field ? nfp : 0) * 2 * H;
+            const size_t RD = (size_t)TK * 2 * D, RH = (size_t)TK * 2 * H, RR = TK ? (size_t)H * H * 6 : 0;
             std::vector<double> om(nf), a(nf * DDo), b(nf * DDo), x(nf * HD), fk(nf * HD), sc(nf * HD), mo(nf * HD),
-                hk(nf * HD), fr(nf * PD), fi(nf * PH), fs(nf * PH), fdf(nf * PH);
+                hk(nf * HD), fr(nf * PD), fi(nf * PH), fs(nf * PH), fdf(nf * PH), kr(nf * RD), krt(nf * RD),
+                kd(nf * RH), kdt(nf * RH), dr(nf * RR);
             for (size_t i = 0; i < nf; i++) om[i] = pr.omegas[fallback[i]];
             HbgProblem sub = pr_in;
             sub.omegas = om.data();
             sub.n_omega = (int64_t)nf;
             sub.out = HbgOutputs{a.data(), b.data(), x.data(), fk.data(), sc.data(), motions ? mo.data() : nullptr,
                                  nullptr, PD ? fr.data() : nullptr, PH ? fi.data() : nullptr, PH ? fs.data() : nullptr,
-                                 PH ? fdf.data() : nullptr, hk.data()};
+                                 PH ? fdf.data() : nullptr, hk.data(), RD ? kr.data() : nullptr,
+                                 RD ? krt.data() : nullptr, RH ? kd.data() : nullptr, RH ? kdt.data() : nullptr,
+                                 RR ? dr.data() : nullptr};
             HbgOptions o64 = opt;
             o64.precision = HBG_FP64;
             o64.surrogate = nullptr;
@@ -713,6 +722,11 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
                 put(pr.out.scattering, sc, HD);
                 if (motions) put(pr.out.motions, mo, HD);
                 put(pr.out.haskind, hk, HD);
+                put(pr.out.kochin_radiation, kr, RD);
+                put(pr.out.kochin_radiation_derivative, krt, RD);
+                put(pr.out.kochin_diffraction, kd, RH);
+                put(pr.out.kochin_diffraction_derivative, kdt, RH);
+                put(pr.out.drift, dr, RR);
                 if (field) {
                     put(pr.out.field_radiation, fr, PD);
                     put(pr.out.field_incident, fi, PH);
@@ -788,9 +802,11 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     CUDA_OK(cudaMemcpyAsync(dheads.p, heads.data(), sizeof(double) * heads.size(), cudaMemcpyHostToDevice, s));
     // outputs per batch: A, B [D][D], X, FK, SC, motions [H][D], field values [P][D] and 3 x [P][H]
     const int Pf = field ? nfp : 0;
-    // outputs per batch: ..., then the Haskind exciting force [H][D]
+    // outputs per batch: ..., then the Haskind exciting force [H][D], then (TK > 0) the Kochin functions
+    // kr, krt [TK][D], kd, kdt [TK][H] and the drift [H][H][3]
+    const size_t kochin_per = (size_t)TK * 2 * (D + H) + (TK ? (size_t)3 * H * H : 0);
     const size_t out_per = 2 * (size_t)D * D * sizeof(double) + 5 * (size_t)H * D * sizeof(double2) +
-                           (size_t)Pf * (D + 3 * H) * sizeof(double2);
+                           (size_t)Pf * (D + 3 * H) * sizeof(double2) + kochin_per * sizeof(double2);
     WsBuf dfq(ws, WS_FQ);
     if (field && fin) dfq.alloc(sizeof(double) * FP_PLANES * (size_t)(N + nfp) * B);
     WsBuf derr(ws, WS_ERR);
@@ -906,6 +922,18 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
                              fi_ + 2 * (size_t)nfp * H * nb, s);
                 g_launches++;
             }
+            if (TK) {  // the Kochin functions, then the momentum drift (with the motions when computed)
+                double2* kr = dSC + 3 * (size_t)H * D * nb + (size_t)Pf * (D + 3 * H) * nb;
+                double2* krt = kr + (size_t)TK * D * nb;
+                double2* kd = krt + (size_t)TK * D * nb;
+                double2* kdt = kd + (size_t)TK * H * nb;
+                double2* dr = kdt + (size_t)TK * H * nb;
+                launch_kochin(pv, nb, dfi.as<FreqInfo>(), TK, H, depth, phi, N, du.as<double2>(), dphiI.as<double2>(),
+                              kr, krt, kd, kdt, s);
+                launch_drift(nb, D, H, TK, dfi.as<FreqInfo>(), depth, opt.gravity, opt.density, dheads.as<double>(), kr,
+                             krt, kd, kdt, motions ? dSC + (size_t)H * D * nb : nullptr, dr, s);
+                g_launches += 2;
+            }
             CUDA_OK(cudaMemcpyAsync(hout, dout.p, out_per * nb, cudaMemcpyDeviceToHost, s));
             CUDA_OK(cudaMemcpyAsync(info, dinfo.p, sizeof(int32_t) * ns, cudaMemcpyDeviceToHost, s));
             CUDA_OK(cudaMemcpyAsync(herr, derr.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
@@ -926,6 +954,7 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         const double* hFr = hMo + (size_t)H * 2 * D * nb;
         const double* hFi = hFr + (size_t)Pf * 2 * D * nb;
         const double* hHK = hFi + (size_t)Pf * 2 * 3 * H * nb;
+        const double* hKr = hHK + (size_t)H * 2 * D * nb;
         if (*herr != 0) throw Failure{HB_ERR_NUMERICAL, "singular motion equation", body_index, f0};
         for (int i = 0; i < nb; i++) {
             for (int c = 0; c < G; c++)
@@ -943,7 +972,7 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
             if (pr.out.excitation) memcpy(pr.out.excitation + fo * hx, hX + hx * i, hx * sizeof(double));
             if (pr.out.froude_krylov) memcpy(pr.out.froude_krylov + fo * hx, hFK + hx * i, hx * sizeof(double));
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
-            if (motions) memcpy(pr.out.motions + fo * hx, hMo + hx * i, hx * sizeof(double));
+            if (motions && pr.out.motions) memcpy(pr.out.motions + fo * hx, hMo + hx * i, hx * sizeof(double));
             if (pr.out.haskind) memcpy(pr.out.haskind + fo * hx, hHK + hx * i, hx * sizeof(double));
             if (field) {
                 const size_t pd = (size_t)nfp * 2 * D, ph = (size_t)nfp * 2 * H;
@@ -952,6 +981,7 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
                 for (int q = 0; q < 3; q++)
                     if (dst3[q]) memcpy(dst3[q] + fo * ph, hFi + ph * ((size_t)q * nb + i), ph * sizeof(double));
             }
+            if (TK) copy_kochin(pr.out, hKr, TK, D, H, nb, i, fo);
         }
     }
 }

@@ -323,6 +323,16 @@ void launch_forces(const PanelsView& pv, int F, const FreqInfo* fi, int H, const
 // columns' boundary values u (lo_frequency.rs:1118-1171)
 void launch_haskind(const PanelsView& pv, int F, const FreqInfo* fi, int H, const double2* phi, int ldphi,
                     const double2* u, const double2* phiI, double rho, double2* HK, cudaStream_t s);
+// Kochin functions kr, krt [F][T][D], kd, kdt [F][T][H] of the solved potentials on T global angles, and the
+// momentum drift [F][H][H][3] from them and the motions xi [F][H][D] (null: a fixed body)
+void launch_kochin(const PanelsView& pv, int F, const FreqInfo* fi, int T, int H, double depth, const double2* phi,
+                   int ldphi, const double2* u, const double2* phiI, double2* kr, double2* krt, double2* kd,
+                   double2* kdt, cudaStream_t s);
+void launch_drift(int F, int D, int H, int T, const FreqInfo* fi, double depth, double grav, double rho,
+                  const double* heads, const double2* kr, const double2* krt, const double2* kd, const double2* kdt,
+                  const double2* xi, double2* drift, cudaStream_t s);
+constexpr int KOCHIN_MAX_HT = 4096;  // headings x Kochin angles of one problem (the drift's shared memory)
+
 // host-side finite-depth scalars of one ordinary frequency (green_fin.rs:874-934)
 void make_fd_params(double h, double K, FdParams& fd);
 double dispersion_x0(double H);

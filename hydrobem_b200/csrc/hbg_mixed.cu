@@ -254,7 +254,11 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     double* fpt = fin ? (double*)get(WS_FPT, sizeof(double) * FP_PLANES * N * B) : nullptr;
     const int nfp = field.P;
     // A, B [D][D], X, FK, SC, motions, Haskind [H][D], field values [P][D] and 3 x [P][H] per frequency
-    const size_t out_per = 2 * (size_t)D * D + 5 * (size_t)H * 2 * D + (size_t)nfp * 2 * (D + 3 * H), DD = (size_t)D * D;
+    // the Kochin functions kr, krt [TK][D], kd, kdt [TK][H] and the drift [H][H][3] after them
+    const int TK = pr.kochin_angles > 0 && H > 0 ? pr.kochin_angles : 0;
+    const size_t kochin_per = ((size_t)TK * 2 * (D + H) + (TK ? (size_t)3 * H * H : 0)) * 2;
+    const size_t out_per = 2 * (size_t)D * D + 5 * (size_t)H * 2 * D + (size_t)nfp * 2 * (D + 3 * H) + kochin_per,
+                 DD = (size_t)D * D;
     double* dout = (double*)get(WS_OUT, sizeof(double) * out_per * B);
     double* fq = nfp && fin ? (double*)get(WS_FQ, sizeof(double) * FP_PLANES * (size_t)(N + nfp) * B) : nullptr;
     if (!okb) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
@@ -733,6 +737,16 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                                  fi_ + 2 * (size_t)nfp * H * nb, s);
                     (*launches)++;
                 }
+                if (TK) {  // the Kochin functions, then the momentum drift (with the motions when computed)
+                    double2* kr = dSC + 3 * (size_t)H * D * nb + (size_t)nfp * (D + 3 * H) * nb;
+                    double2* krt = kr + (size_t)TK * D * nb;
+                    double2* kd = krt + (size_t)TK * D * nb;
+                    double2* kdt = kd + (size_t)TK * H * nb;
+                    launch_kochin(pv, nb, dfi, TK, H, depth, G > 1 ? phi : x, G > 1 ? N : Np, u, phiI, kr, krt, kd, kdt, s);
+                    launch_drift(nb, D, H, TK, dfi, depth, opt.gravity, opt.density, dheads, kr, krt, kd, kdt,
+                                 motion ? dSC + (size_t)H * D * nb : nullptr, kdt + (size_t)TK * H * nb, s);
+                    *launches += 2;
+                }
                 cudaMemcpyAsync(hout, dout, sizeof(double) * out_per * nb, cudaMemcpyDeviceToHost, s);
                 cudaMemcpyAsync(herr, err, sizeof(int), cudaMemcpyDeviceToHost, s);
                 tf.stop();
@@ -845,6 +859,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         const double* hFr = hMo + (size_t)H * 2 * D * nb;
         const double* hFi = hFr + (size_t)nfp * 2 * D * nb;
         const double* hHK = hFi + (size_t)nfp * 2 * 3 * H * nb;
+        const double* hKr = hHK + (size_t)H * 2 * D * nb;
         for (int i = 0; i < nb; i++) {
             const size_t fo = (size_t)(f0 + i), hx = (size_t)H * 2 * D;
             if (redo[i]) {
@@ -861,6 +876,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             if (pr.out.scattering) memcpy(pr.out.scattering + fo * hx, hSC + hx * i, hx * sizeof(double));
             if (motion && pr.out.motions) memcpy(pr.out.motions + fo * hx, hMo + hx * i, hx * sizeof(double));
             if (pr.out.haskind) memcpy(pr.out.haskind + fo * hx, hHK + hx * i, hx * sizeof(double));
+            if (TK) copy_kochin(pr.out, hKr, TK, D, H, nb, i, fo);
             if (nfp) {
                 const size_t pd = (size_t)nfp * 2 * D, ph = (size_t)nfp * 2 * H;
                 if (pr.out.field_radiation) memcpy(pr.out.field_radiation + fo * pd, hFr + pd * i, pd * sizeof(double));

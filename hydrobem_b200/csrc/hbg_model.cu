@@ -73,6 +73,9 @@ struct HbModel {
     int64_t device = 0;
     bool motion = false;
     bool field_pressure = false;
+    // the mean drift by momentum conservation (Kochin functions on kochin_angles angles, 0: automatic)
+    bool drift_momentum = false, drift_bidirectional = false;
+    int64_t kochin_angles = 0;
     std::vector<double> field_points;  // [P][3] global
     std::vector<hbg::MeshObj> meshes;
     std::vector<hbg::BodyObj> bodies;
@@ -411,6 +414,14 @@ extern "C" HbStatus hb_set_bool(HbModel* model, uint64_t object, const char* ite
             model->field_pressure = value != 0;
             return HB_OK;
         }
+        if (object == OBJ_OPTIONS && it == "drift_momentum_conservation") {
+            model->drift_momentum = value != 0;
+            return HB_OK;
+        }
+        if (object == OBJ_OPTIONS && it == "drift_bidirectional") {
+            model->drift_bidirectional = value != 0;
+            return HB_OK;
+        }
         return refuse(HB_ERR_UNSUPPORTED, "the item \"" + it + "\" of this object is not on this route");
     });
 }
@@ -423,6 +434,11 @@ extern "C" HbStatus hb_set_int(HbModel* model, uint64_t object, const char* item
         if (object == OBJ_OPTIONS && it == "gpu_device") {
             if (value < 0) return refuse(HB_ERR_VALUE, "gpu_device >= 0");
             model->device = value;
+            return HB_OK;
+        }
+        if (object == OBJ_OPTIONS && it == "drift_momentum_conservation_angles") {  // document_schema.rs:249
+            if (value < 1 || value > 65536) return refuse(HB_ERR_VALUE, "drift_momentum_conservation_angles 1..65536 or auto");
+            model->kochin_angles = value;
             return HB_OK;
         }
         return refuse(HB_ERR_UNSUPPORTED, "the item \"" + it + "\" of this object is not on this route");
@@ -448,6 +464,11 @@ extern "C" HbStatus hb_set_text(HbModel* model, uint64_t object, const char* ite
         if (object == OBJ_OPTIONS && it == "gpu_precision") {
             if (v != "fp64" && v != "mixed") return refuse(HB_ERR_VALUE, "gpu_precision is fp64 or mixed");
             model->precision = v;
+            return HB_OK;
+        }
+        if (object == OBJ_OPTIONS && it == "drift_momentum_conservation_angles") {
+            if (v != "auto") return refuse(HB_ERR_VALUE, "drift_momentum_conservation_angles 1..65536 or auto");
+            model->kochin_angles = 0;
             return HB_OK;
         }
         if (is_mesh(model, object)) {
@@ -599,6 +620,27 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         const size_t NP = fpts.size() / 3;
         std::vector<double> FR(F * NP * D * 2), FI(F * NP * H * 2), FS(F * NP * H * 2), FDF(F * NP * H * 2);
         const bool want_motion = model->motion && H > 0;
+        // the Kochin angles of the momentum drift: given, or the reference's automatic count
+        // (response.rs:109-176): 8 ceil((2 ceil(k R) + 96) / 8), k the largest wave number, R the largest
+        // horizontal distance of a vertex from the origin
+        size_t T = 0;
+        if (model->drift_momentum && H > 0) {
+            if (model->kochin_angles > 0) {
+                T = (size_t)model->kochin_angles;
+            } else {
+                double kmax = 0.0, R = 0.0;
+                const bool fin = std::isfinite(opt.depth) && opt.depth > 0.0;
+                for (double w : omegas) {
+                    const double K = w * w / opt.gravity;
+                    kmax = std::max(kmax, fin ? dispersion_x0(K * opt.depth) / opt.depth : K);
+                }
+                for (size_t q = 0; q + 2 < verts.size(); q += 3) R = std::max(R, std::hypot(verts[q], verts[q + 1]));
+                const size_t n = 2 * (size_t)std::ceil(kmax * R) + 96;
+                T = 8 * ((n + 7) / 8);
+            }
+        }
+        std::vector<double> KR(F * T * D * 2), KRT(F * T * D * 2), KD(F * T * H * 2), KDT(F * T * H * 2),
+            DR(T ? F * H * H * 3 * 2 : 0);
         HbgRigid rig{rmass.data(), rcg.data(), rkind.data(), rinertia.data(), rorigin.data(), nullptr, nullptr};
         HbgProblem pr{};
         pr.rigid = all_rigid ? &rig : nullptr;
@@ -615,7 +657,9 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
         pr.n_heading = (int64_t)H;
         pr.out = HbgOutputs{A.data(), B.data(), X.data(), FK.data(), SC.data(), want_motion ? MO.data() : nullptr,
                             HS.data(), NP ? FR.data() : nullptr, NP ? FI.data() : nullptr, NP ? FS.data() : nullptr,
-                            NP ? FDF.data() : nullptr, HK.data()};
+                            NP ? FDF.data() : nullptr, HK.data(), T ? KR.data() : nullptr, T ? KRT.data() : nullptr,
+                            T ? KD.data() : nullptr, T ? KDT.data() : nullptr, T ? DR.data() : nullptr};
+        pr.kochin_angles = (int32_t)T;
         pr.field_points = NP ? fpts.data() : nullptr;
         pr.n_field_points = (int64_t)NP;
         if (progress) {
@@ -680,6 +724,41 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
                 add_quantity(r.get(), fq[q].first, HB_C64, {F, NP, cols}, v32.data(), v32.size() * 4);
                 add_quantity(r.get(), std::string(fq[q].first) + "_f64", HB_C128, {F, NP, cols}, v.data(), v.size() * 8);
             }
+        }
+        if (T) {  // quantities.rs:79-88: the Kochin functions, the drift of the heading pairs
+            std::vector<double> ang(T);
+            for (size_t t = 0; t < T; t++) ang[t] = 2.0 * PI * (double)t / (double)T;
+            add_quantity(r.get(), "kochin_angles", HB_F64, {T}, ang.data(), T * 8);
+            const std::pair<const char*, std::vector<double>*> kq[4] = {{"kochin_radiation", &KR},
+                                                                        {"kochin_radiation_derivative", &KRT},
+                                                                        {"kochin_diffraction", &KD},
+                                                                        {"kochin_diffraction_derivative", &KDT}};
+            for (int q = 0; q < 4; q++) {
+                std::vector<double>& v = *kq[q].second;
+                std::vector<float> v32(v.size());
+                for (size_t i = 0; i < v.size(); i++) v32[i] = (float)v[i];
+                const size_t cols = q < 2 ? D : H;
+                add_quantity(r.get(), kq[q].first, HB_C64, {F, T, cols}, v32.data(), v32.size() * 4);
+                add_quantity(r.get(), std::string(kq[q].first) + "_f64", HB_C128, {F, T, cols}, v.data(), v.size() * 8);
+            }
+            // heading_pairs.rs:12-25: (h, h) unidirectional, every h_a <= h_b bidirectional
+            std::vector<std::pair<size_t, size_t>> hp;
+            for (size_t a = 0; a < H; a++)
+                for (size_t b = a; b < (model->drift_bidirectional ? H : a + 1); b++) hp.emplace_back(a, b);
+            std::vector<double> dv, pairs;
+            for (size_t fq = 0; fq < F; fq++)
+                for (auto& p : hp)
+                    for (int c = 0; c < 3; c++) {
+                        const double* z = &DR[((((fq * H + p.first) * H + p.second) * 3) + c) * 2];
+                        dv.push_back(z[0]);
+                        dv.push_back(z[1]);
+                    }
+            for (auto& p : hp) {
+                pairs.push_back(heads[p.first]);
+                pairs.push_back(heads[p.second]);
+            }
+            add_quantity(r.get(), "drift_momentum_conservation", HB_C128, {F, hp.size(), 3}, dv.data(), dv.size() * 8);
+            add_quantity(r.get(), "drift_heading_pairs", HB_F64, {hp.size(), 2}, pairs.data(), pairs.size() * 8);
         }
         if (want_motion) {
             std::vector<float> m32(F * H * D * 2);

@@ -39,7 +39,9 @@ SYM_NONE, SYM_YZ, SYM_XZ, SYM_BOTH = 0, 1, 2, 3
 class HbgOutputs(ctypes.Structure):
     _fields_ = [("added_mass", dp), ("radiation_damping", dp), ("excitation", dp), ("froude_krylov", dp),
                 ("scattering", dp), ("motions", dp), ("hydrostatics", dp), ("field_radiation", dp),
-                ("field_incident", dp), ("field_scattering", dp), ("field_diffraction", dp), ("haskind", dp)]
+                ("field_incident", dp), ("field_scattering", dp), ("field_diffraction", dp), ("haskind", dp),
+                ("kochin_radiation", dp), ("kochin_radiation_derivative", dp), ("kochin_diffraction", dp),
+                ("kochin_diffraction_derivative", dp), ("drift", dp)]
 
 
 class HbgRigid(ctypes.Structure):
@@ -50,7 +52,7 @@ class HbgRigid(ctypes.Structure):
 class HbgProblem(ctypes.Structure):
     _fields_ = [("body", HbgBody), ("omegas", dp), ("n_omega", ctypes.c_int64), ("headings_deg", dp),
                 ("n_heading", ctypes.c_int64), ("out", HbgOutputs), ("rigid", ctypes.POINTER(HbgRigid)),
-                ("field_points", dp), ("n_field_points", ctypes.c_int64)]
+                ("field_points", dp), ("n_field_points", ctypes.c_int64), ("kochin_angles", ctypes.c_int32)]
 
 
 # HbgRigid.inertia_kind, and the record of HbgOutputs.hydrostatics (HBG_HS doubles per body)
@@ -183,7 +185,7 @@ class Body:
     points: field points [P][3] (global, z <= 0) for the elevation or p / (rho g) there."""
 
     def __init__(self, vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None,
-                 symmetry=SYM_NONE, rigid=None, points=None):
+                 symmetry=SYM_NONE, rigid=None, points=None, kochin_angles=0, motions=None):
         self.symmetry = int(symmetry)
         self.vertices = np.ascontiguousarray(vertices, dtype=np.float64).reshape(-1, 4, 3)
         self.kinds = None if kinds is None else np.ascontiguousarray(kinds, dtype=np.int32)
@@ -202,6 +204,13 @@ class Body:
         self.FK = np.zeros((F, H, D), dtype=np.complex128)
         self.SC = np.zeros((F, H, D), dtype=np.complex128)
         self.HK = np.zeros((F, H, D), dtype=np.complex128)
+        T = int(kochin_angles) if H else 0
+        self.kochin_angles = T
+        self.KR = np.zeros((F, T, D), dtype=np.complex128)
+        self.KRT = np.zeros((F, T, D), dtype=np.complex128)
+        self.KD = np.zeros((F, T, H), dtype=np.complex128)
+        self.KDT = np.zeros((F, T, H), dtype=np.complex128)
+        self.DRIFT = np.zeros((F, H, H, 3), dtype=np.complex128)
         self.HS = np.zeros((self.n_bodies, HBG_HS))
         self.points = None if points is None else np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3)
         P = 0 if self.points is None else self.points.shape[0]
@@ -209,7 +218,10 @@ class Body:
         self.FI = np.zeros((F, P, H), dtype=np.complex128)
         self.FS = np.zeros((F, P, H), dtype=np.complex128)
         self.FD = np.zeros((F, P, H), dtype=np.complex128)
-        self.MO = np.zeros((F, H, D), dtype=np.complex128) if rigid is not None else None
+        # the motions when rigid data are given (motions=False leaves them out: then a drift is that of the
+        # fixed body)
+        want_mo = rigid is not None if motions is None else bool(motions)
+        self.MO = np.zeros((F, H, D), dtype=np.complex128) if want_mo else None
         self._rigid = None
         if rigid is not None:
             nb = self.n_bodies
@@ -245,6 +257,13 @@ class Body:
         p.out.froude_krylov = self.FK.ctypes.data_as(dp)
         p.out.scattering = self.SC.ctypes.data_as(dp)
         p.out.haskind = self.HK.ctypes.data_as(dp)
+        if self.kochin_angles:
+            p.kochin_angles = self.kochin_angles
+            p.out.kochin_radiation = self.KR.ctypes.data_as(dp)
+            p.out.kochin_radiation_derivative = self.KRT.ctypes.data_as(dp)
+            p.out.kochin_diffraction = self.KD.ctypes.data_as(dp)
+            p.out.kochin_diffraction_derivative = self.KDT.ctypes.data_as(dp)
+            p.out.drift = self.DRIFT.ctypes.data_as(dp)
         p.out.motions = None if self.MO is None else self.MO.ctypes.data_as(dp)
         p.out.hydrostatics = self.HS.ctypes.data_as(dp)
         p.rigid = None if self._rigid is None else ctypes.pointer(self._rigid)
@@ -262,6 +281,9 @@ class Body:
                "hydrostatics": [hydrostatics_record(h) for h in self.HS]}
         if self.MO is not None:
             out["motions"] = self.MO
+        if self.kochin_angles:
+            out.update({"kr": self.KR, "krt": self.KRT, "kd": self.KD, "kdt": self.KDT, "drift": self.DRIFT,
+                        "kochin_angles": 2.0 * np.pi * np.arange(self.kochin_angles) / self.kochin_angles})
         if self.points is not None:
             out.update({"field_radiation": self.FR, "field_incident": self.FI, "field_scattering": self.FS,
                         "field_diffraction": self.FD})
@@ -294,12 +316,14 @@ def solve_batch(bodies, **options):
 
 
 def solve(vertices, omegas, headings_deg=(), kinds=None, panel_body=None, rotation_centers=None,
-          symmetry=SYM_NONE, rigid=None, points=None, **options):
+          symmetry=SYM_NONE, rigid=None, points=None, kochin_angles=0, **options):
     """One problem through the GPU path: dict of A, B [F][D][D], X, FK, SC [F][H][D], D = 6 per body, the
     hydrostatics records of the bodies, with rigid the motions [F][H][D], with points the field values
-    field_radiation [F][P][D] and field_incident, field_scattering, field_diffraction [F][P][H]."""
+    field_radiation [F][P][D] and field_incident, field_scattering, field_diffraction [F][P][H]; with
+    kochin_angles = T > 0 the Kochin functions kr, krt [F][T][D], kd, kdt [F][T][H] and the momentum drift
+    [F][H][H][3] (the motions included with rigid)."""
     return solve_batch([Body(vertices, omegas, headings_deg, kinds, panel_body, rotation_centers, symmetry, rigid,
-                             points)], **options)[0]
+                             points, kochin_angles)], **options)[0]
 
 
 def last_profile():

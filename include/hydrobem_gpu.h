@@ -149,6 +149,18 @@ typedef struct HbgOutputs {
     double *field_diffraction;
     double *haskind; /* [F][H][D] complex: the exciting force by the Haskind relation from the radiation
                       * potentials (lo_frequency.rs:1118-1171; the reference's excitation_haskind) */
+    /* with HbgProblem.kochin_angles = T > 0 (lo_frequency.rs:1277-1374, response.rs:183-300):
+     *   kochin_radiation, kochin_radiation_derivative  [F][T][D][2]: the Kochin functions of the radiation
+     *       potentials on the angles 2 pi t / T and their angular derivatives, per unit velocity
+     *   kochin_diffraction, kochin_diffraction_derivative  [F][T][H][2]: those of the scattered wave
+     *   drift  [F][H][H][3][2]: the mean drift by momentum conservation (surge, sway force, yaw moment
+     *       about the global z axis) of every heading pair, the motions included when they are asked for
+     *       (`motions` not NULL; a fixed body otherwise); the equal pairs are real */
+    double *kochin_radiation;
+    double *kochin_radiation_derivative;
+    double *kochin_diffraction;
+    double *kochin_diffraction_derivative;
+    double *drift;
 } HbgOutputs;
 
 typedef struct HbgProblem {
@@ -161,6 +173,8 @@ typedef struct HbgProblem {
     const HbgRigid *rigid;       /* NULL: no motions */
     const double *field_points;  /* [n_field_points][3], global, in the fluid at z <= 0; NULL: none */
     int64_t n_field_points;
+    int32_t kochin_angles;       /* T > 0: the Kochin functions on T angles and the momentum drift (needs
+                                  * headings; T * n_heading <= 4096); 0: none */
 } HbgProblem;
 
 typedef struct HbgOptions {

@@ -10,6 +10,8 @@ and adds, in numpy, the steps that are short formulas of ``crates/hydrobem/src/`
   LAPACK ``zgesv`` through numpy, standing in for faer's blocked LU, ``linalg.rs:134-252``)
 - pressure integration A, B, X, FK, SC  ``lo_frequency.rs:1039-1115``
 - the Haskind exciting force HK from the radiation potentials  ``lo_frequency.rs:1118-1171``
+- Kochin functions of the radiation and scattered waves  ``lo_frequency.rs:1277-1374``,
+  ``low_order.rs:1417-1452``, and the mean drift by momentum conservation  ``response.rs:51-300``
 - field points: the elevation or p / (rho g) of the radiation, incident, scattered and total waves at
   points in the fluid by Green's identity over the panels  ``lo_frequency.rs:1392-1470``
 - hydrostatics, rigid inertia and the motion equation of each frequency  ``hydrostatics.rs:116-356``,
@@ -315,9 +317,122 @@ def sector_solve(S, A, u, G):
     return phi
 
 
+def depth_factor(z, depth, k):
+    """(Z, dZ/dz) of the wave's vertical profile at depths z (low_order.rs:1401-1412): e^{kz} in infinite
+    depth, cosh k(z + h) / cosh kh in depth h."""
+    Z = np.exp(k * z)
+    Zz = k * Z
+    if depth is not None and np.isfinite(depth) and depth > 0:
+        b = np.exp(-k * (z + 2.0 * depth))
+        dd = 1.0 + np.exp(-2.0 * k * depth)
+        Zz = k * (Z - b) / dd
+        Z = (Z + b) / dd
+    return Z, Zz
+
+
+def kochin(c, n, area, wet, depth, k, phi, u, phiI, D, n_angles):
+    """Kochin functions of one frequency on n_angles global angles theta_t = 2 pi t / n_angles
+    (lo_frequency.rs:1277-1374 on this route's panels, the frame at the origin with no yaw): Green's
+    identity with the far-field kernel (low_order.rs:1417-1431: g = Z e^{i k (x cos + y sin)}, its normal
+    derivative gn and the theta-derivatives gt, gnt) over the wetted panels, the interior panels taking no
+    part.  Radiation column c: H = sum_j phi_c Dx - Sx u_c; heading h (scattered formulation): H = sum_j
+    (phi_S + phi_I) Dx.  Returns (kr, krt) [T][D] and (kd, kdt) [T][H], H_t the theta-derivative."""
+    th = 2.0 * np.pi * np.arange(n_angles) / n_angles
+    cs, sn = np.cos(th)[:, None], np.sin(th)[:, None]
+    x, y = c[None, :, 0], c[None, :, 1]
+    Z, Zz = depth_factor(c[:, 2], depth, k)
+    e = np.exp(1j * k * (x * cs + y * sn))
+    ik = 1j * k
+    dt = -x * sn + y * cs
+    dnt = -n[None, :, 0] * sn + n[None, :, 1] * cs
+    g = Z[None] * e
+    gn = e * (Z[None] * ik * (n[None, :, 0] * cs + n[None, :, 1] * sn) + Zz[None] * n[None, :, 2])
+    gt = g * ik * dt
+    gnt = gn * ik * dt + e * Z[None] * ik * dnt
+    w = (area * wet)[None]
+    Sx, Dx, St, Dt = w * g, w * gn, w * gt, w * gnt
+    kr = Dx @ phi[:, :D] - Sx @ u[:, :D]
+    krt = Dt @ phi[:, :D] - St @ u[:, :D]
+    tot = phi[:, D:] + np.where(wet[:, None], phiI.T, 0.0)
+    return kr, krt, Dx @ tot, Dt @ tot
+
+
+def kochin_angle_count(verts, omegas, depth, grav=GRAVITY):
+    """The reference's automatic count (response.rs:109-176): 8 ceil((2 ceil(k R) + 96) / 8) for the
+    largest wave number k and the largest horizontal distance R of a vertex from the origin."""
+    k = max(lib().hbo_wavenumber(w, depth if depth else np.inf, grav) for w in omegas)
+    R = float(np.hypot(np.asarray(verts)[..., 0], np.asarray(verts)[..., 1]).max())
+    n = 2 * int(np.ceil(k * R)) + 96
+    return 8 * ((n + 7) // 8)
+
+
+def momentum_drift(omegas, headings_deg, kd, kdt, kr, krt, xi, depth=np.inf, grav=GRAVITY, rho=DENSITY):
+    """Mean drift forces by momentum conservation from the Kochin functions (response.rs:183-300):
+    surge, sway force and yaw moment of every heading pair [F][H][H][3] (complex; the equal pairs are the
+    real unidirectional coefficients).  kd, kdt [F][T][H]; kr, krt [F][T][K] and xi [F][H][K] the motions
+    of the radiation columns (None: a fixed body)."""
+    F, T, H = kd.shape
+    th = 2.0 * np.pi * np.arange(T) / T
+    dth = 2.0 * np.pi / T
+    beta = np.radians(np.asarray(headings_deg, dtype=float))
+    lo = -(T - 1) // 2 if T % 2 else -(T - 1) // 2
+    modes = np.arange(lo, -lo + 1)
+
+    def coefficients(v):  # the trigonometric interpolant's coefficients (and the Nyquist one for even T)
+        c = np.array([(v * np.exp(-2j * np.pi * m * np.arange(T) / T)).sum() / T for m in modes])
+        if T % 2 == 0:
+            c = np.append(c, (v * (-1.0) ** np.arange(T)).sum() / T)
+        return c
+
+    def value(c, b):  # the interpolant at angle b
+        e = np.exp(1j * modes * b)
+        if T % 2 == 0:
+            e = np.append(e, np.cos(T / 2 * b))
+        return (c * e).sum()
+
+    out = np.zeros((F, H, H, 3), dtype=np.complex128)
+    for f, w in enumerate(omegas):
+        K0 = w * w / grav
+        k = lib().hbo_wavenumber(w, depth if depth else np.inf, grav)
+        C, Ke = 2.0 * np.pi * K0, K0
+        if depth is not None and np.isfinite(depth) and depth > 0:
+            x = k * depth
+            A0 = 2.0 * np.pi * k / (-np.expm1(-4.0 * x) + 4.0 * x * np.exp(-2.0 * x))
+            C = A0 * (1.0 + np.exp(-2.0 * x)) ** 2
+            Ke = K0 + k * k * depth / np.cosh(x) ** 2
+        fac = -(1j * C / (4.0 * np.pi)) * np.sqrt(2.0 / (np.pi * k)) * np.exp(1j * np.pi / 4.0)
+        a, e, q = 1j * grav / w, np.exp(-1j * np.pi / 4.0), np.sqrt(2.0 * np.pi / k)
+        b = kd[f].T.astype(np.complex128)   # [H][T]
+        bt = kdt[f].T.astype(np.complex128)
+        if xi is not None and kr is not None:
+            b = b + 1j * w * (xi[f] @ kr[f].T)
+            bt = bt + 1j * w * (xi[f] @ krt[f].T)
+        b, bt = fac * b, fac * bt
+        cf = [coefficients(b[i]) for i in range(H)]
+        cft = [coefficients(bt[i]) for i in range(H)]
+        bb = np.array([[value(cf[i], beta[j]) for j in range(H)] for i in range(H)])
+        bbt = np.array([[value(cft[i], beta[j]) for j in range(H)] for i in range(H)])
+        s = rho * Ke / 4.0
+        for i in range(H):
+            for j in range(H):
+                pij = b[i] * np.conj(b[j])
+                sx, sy = (pij * np.cos(th)).sum(), (pij * np.sin(th)).sum()
+                dd = (bt[i] * np.conj(b[j]) - b[i] * np.conj(bt[j])).sum() * (-0.5j)
+                cx = -s * q * np.conj(a) * e * bb[i, j]
+                cy = -s * q * a * np.conj(e) * np.conj(bb[j, i])
+                o = out[f, i, j]
+                o[0] = -s * sx * dth + cx * np.cos(beta[j]) + cy * np.cos(beta[i])
+                o[1] = -s * sy * dth + cx * np.sin(beta[j]) + cy * np.sin(beta[i])
+                o[2] = (s / k) * dd * dth - (s / k) * q * (1j * np.conj(a) * e * bbt[i, j]
+                                                            - 1j * a * np.conj(e) * np.conj(bbt[j, i]))
+                if i == j:
+                    out[f, i, j] = o.real
+    return out
+
+
 def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY, rho=DENSITY, logint=True,
                     want_matrices=False, panel_body=None, centers=None, sectors=1, points=None, tol=1e-4,
-                    production=False):
+                    production=False, kochin_angles=0):
     """A, B [D][D], X, FK, SC, HK [H][D] of one frequency (D = 6 per body), all in float64 (complex128).
     sectors > 1: the panels are a mirrored mesh (mirror_sector) solved by its symmetry sectors.
     production: the reference's default path (class production) -- statics computed in that mode are
@@ -363,6 +478,9 @@ def solve_frequency(panels, kinds, st, depth, omega, headings_rad, grav=GRAVITY,
         out["HK"] = (iwr * hk).T
     if points is not None and len(points):
         out.update(field_values(panels, kinds, points, depth, omega, headings_rad, phi, u, phiI, D, grav, logint, tol))
+    if kochin_angles and H:
+        out["kr"], out["krt"], out["kd"], out["kdt"] = kochin(c, n, area, wet, depth, k, phi, u, phiI, D,
+                                                               kochin_angles)
     if want_matrices:
         out["S"], out["Amat"], out["rhs"], out["phi"] = S, A0, rhs, phi
     return out
@@ -509,7 +627,7 @@ def motions(A, B, X, omega, M, C, Bx):
 
 def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GRAVITY, rho=DENSITY, logint=True,
                tol=1e-4, panel_body=None, centers=None, symmetry=SYM_NONE, rigid=None, points=None,
-               production=False):
+               production=False, kochin_angles=0):
     """The whole path for one problem: statics once, then every frequency. Arrays [F][D][D], [F][H][D]
     (D = 6 per body; interacting bodies by panel_body and their rotation centers).  With symmetry the
     panels (and kinds, panel_body) are one sector: mirrored, then solved by sectors."""
@@ -522,8 +640,11 @@ def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GR
     with ProductionMode(production):
         st = statics(panels, kinds, depth, logint, tol)
     heads = np.radians(np.asarray(headings_deg, dtype=float))
+    if kochin_angles == "auto":
+        kochin_angles = kochin_angle_count(verts, omegas, depth, grav)
     res = [solve_frequency(panels, kinds, st, depth, w, heads, grav, rho, logint, panel_body=panel_body,
-                           centers=centers, sectors=G, points=points, tol=tol, production=production)
+                           centers=centers, sectors=G, points=points, tol=tol, production=production,
+                           kochin_angles=kochin_angles)
            for w in omegas]
     out = {k: np.array([r[k] for r in res]) for k in res[0]}
     c, n, area = panel_arrays(panels)
@@ -532,4 +653,8 @@ def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GR
     if rigid is not None and len(heads):
         out["motions"] = np.array([motions(out["A"][i], out["B"][i], out["X"][i], w, M, C, Bx)
                                    for i, w in enumerate(omegas)])
+    if kochin_angles and len(heads):
+        out["kochin_angles"] = 2.0 * np.pi * np.arange(kochin_angles) / kochin_angles
+        out["drift"] = momentum_drift(omegas, headings_deg, out["kd"], out["kdt"], out["kr"], out["krt"],
+                                      out.get("motions"), depth, grav, rho)
     return out
