@@ -9,6 +9,7 @@
 // geometry.rs:208-235), which solves the same discrete equations as the reference's character
 // decomposition.  Items and routes outside this subset are refused with HB_ERR_UNSUPPORTED, as the
 // reference refuses routes it lacks.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <map>
@@ -117,18 +118,18 @@ static void add_quantity(HbResults* r, const std::string& name, int32_t dtype, s
     r->q.push_back(std::move(q));
 }
 
-// The full panels of a mesh with its symmetry planes (the reflected copies, orientation restored).
-static std::vector<double> expand(const MeshObj& m) {
+// The full panels of stored panels with symmetry planes (the reflected copies, orientation restored).
+static std::vector<double> reflect(const std::vector<double>& vertices, const std::string& symmetry) {
     std::vector<std::pair<double, double>> refl = {{1.0, 1.0}};
-    if (m.symmetry == "yz" || m.symmetry == "xz_and_yz") refl.push_back({-1.0, 1.0});
-    if (m.symmetry == "xz" || m.symmetry == "xz_and_yz") refl.push_back({1.0, -1.0});
-    if (m.symmetry == "xz_and_yz") refl.push_back({-1.0, -1.0});
-    size_t P = m.vertices.size() / 12;
+    if (symmetry == "yz" || symmetry == "xz_and_yz") refl.push_back({-1.0, 1.0});
+    if (symmetry == "xz" || symmetry == "xz_and_yz") refl.push_back({1.0, -1.0});
+    if (symmetry == "xz_and_yz") refl.push_back({-1.0, -1.0});
+    size_t P = vertices.size() / 12;
     std::vector<double> out;
-    out.reserve(refl.size() * m.vertices.size());
+    out.reserve(refl.size() * vertices.size());
     for (auto [sx, sy] : refl)
         for (size_t p = 0; p < P; p++) {
-            const double* v = &m.vertices[12 * p];
+            const double* v = &vertices[12 * p];
             int order[4] = {0, 1, 2, 3};
             if (sx * sy < 0) {
                 order[1] = 3;
@@ -143,6 +144,8 @@ static std::vector<double> expand(const MeshObj& m) {
         }
     return out;
 }
+
+static std::vector<double> expand(const MeshObj& m) { return reflect(m.vertices, m.symmetry); }
 
 // interior.rs:79-138 projected: the interior free surface as the vertical projection onto z = z0 (the free
 // surface in body coordinates) of the downward-facing wetted panels, vertex order reversed so that the
@@ -179,6 +182,321 @@ static std::vector<double> projected_lid(const std::vector<double>& v, double z0
     }
     if (out.empty()) why = "no wetted element faces downward";
     return out;
+}
+
+// ------------------------------------------------------------------ graded interior surface
+// interior.rs:139-515 graded, on the stored panels of a mesh whose symmetry flags isx / isy declare the
+// planes x = 0 / y = 0.  The waterline is rebuilt as closed contours in the quadrant x, y >= 0, each
+// region fanned from its area centroid to every waterline segment, the rays cut at
+// t_k = sin(pi k / (2N)), N = ceil(mean ray / mean segment); the innermost cell a triangle, the others
+// quadrilaterals.  The output is stored-form panels (reflected like the mesh), facing up.
+namespace graded {
+
+struct P2 {
+    double x, y;
+};
+using Loop = std::vector<P2>;
+
+static double dist(P2 a, P2 b) { return std::hypot(a.x - b.x, a.y - b.y); }
+static double orient(P2 o, P2 a, P2 b) { return (a.x - o.x) * (b.y - o.y) - (a.y - o.y) * (b.x - o.x); }
+
+// polygon.rs:94-99
+static double seg_dist(P2 x, P2 a, P2 b) {
+    const double ex = b.x - a.x, ey = b.y - a.y, ee = ex * ex + ey * ey;
+    const double t = ee > 0.0 ? std::min(1.0, std::max(0.0, ((x.x - a.x) * ex + (x.y - a.y) * ey) / ee)) : 0.0;
+    return dist(x, P2{a.x + t * ex, a.y + t * ey});
+}
+
+// polygon.rs:81-90: the segments pq and ab cross, or an end lies exactly on the other
+static bool meet(P2 p, P2 q, P2 a, P2 b) {
+    const double d1 = orient(a, b, p), d2 = orient(a, b, q), d3 = orient(p, q, a), d4 = orient(p, q, b);
+    if (((d1 > 0 && d2 < 0) || (d1 < 0 && d2 > 0)) && ((d3 > 0 && d4 < 0) || (d3 < 0 && d4 > 0))) return true;
+    auto on = [](P2 o, P2 e, P2 x, double d) {
+        return d == 0.0 && x.x >= std::min(o.x, e.x) && x.x <= std::max(o.x, e.x) && x.y >= std::min(o.y, e.y) &&
+               x.y <= std::max(o.y, e.y);
+    };
+    return on(a, b, p, d1) || on(a, b, q, d2) || on(p, q, a, d3) || on(p, q, b, d4);
+}
+
+// polygon.rs:111-149: two loops, or two edges of one loop that do not follow each other, cross or
+// come within tol
+static bool loops_meet(const std::vector<Loop>& loops, double tol) {
+    struct E {
+        size_t l, k;
+        P2 a, b;
+    };
+    std::vector<E> e;
+    for (size_t l = 0; l < loops.size(); l++)
+        for (size_t k = 0; k < loops[l].size(); k++) e.push_back({l, k, loops[l][k], loops[l][(k + 1) % loops[l].size()]});
+    auto lo = [&](const E& s, int c) { return (c ? std::min(s.a.y, s.b.y) : std::min(s.a.x, s.b.x)) - tol; };
+    auto hi = [&](const E& s, int c) { return (c ? std::max(s.a.y, s.b.y) : std::max(s.a.x, s.b.x)) + tol; };
+    for (size_t i = 0; i < e.size(); i++)
+        for (size_t j = i + 1; j < e.size(); j++) {
+            const E &f = e[i], &g = e[j];
+            if (lo(f, 0) > hi(g, 0) || lo(g, 0) > hi(f, 0) || lo(f, 1) > hi(g, 1) || lo(g, 1) > hi(f, 1)) continue;
+            if (f.l == g.l) {
+                const size_t n = loops[f.l].size();
+                if (n <= 3 || (f.k + 1) % n == g.k || (g.k + 1) % n == f.k) continue;
+            }
+            if (meet(f.a, f.b, g.a, g.b) || seg_dist(f.a, g.a, g.b) <= tol || seg_dist(f.b, g.a, g.b) <= tol ||
+                seg_dist(g.a, f.a, f.b) <= tol || seg_dist(g.b, f.a, f.b) <= tol)
+                return true;
+        }
+    return false;
+}
+
+static double signed_area(const Loop& l) {
+    double a = 0.0;
+    for (size_t k = 0; k < l.size(); k++) a += l[k].x * l[(k + 1) % l.size()].y - l[(k + 1) % l.size()].x * l[k].y;
+    return 0.5 * a;
+}
+
+static bool inside(const Loop& l, P2 x) {
+    bool c = false;
+    for (size_t k = 0; k < l.size(); k++) {
+        const P2 p = l[k], q = l[(k + 1) % l.size()];
+        if ((p.y > x.y) != (q.y > x.y) && x.x < p.x + (x.y - p.y) / (q.y - p.y) * (q.x - p.x)) c = !c;
+    }
+    return c;
+}
+
+static std::vector<double> lid(const std::vector<double>& v, bool isx, bool isy, double z0, std::string& why) {
+    constexpr double SLOPE = 1e-6, PLANE_TOL = 1e-6;
+    const size_t P = v.size() / 12;
+    double ext = 1.0;  // the mesh reference length
+    for (double x : v) ext = std::max(ext, std::fabs(x));
+    const double tol = PLANE_TOL * ext;
+    // interior.rs:158-214 waterline segments, the body section on their left
+    std::vector<std::pair<P2, P2>> segs;
+    for (size_t p = 0; p < P; p++) {
+        const double* q = &v[12 * p];
+        const double d1[3] = {q[6] - q[0], q[7] - q[1], q[8] - q[2]}, d2[3] = {q[9] - q[3], q[10] - q[4], q[11] - q[5]};
+        double n[3] = {d1[1] * d2[2] - d1[2] * d2[1], d1[2] * d2[0] - d1[0] * d2[2], d1[0] * d2[1] - d1[1] * d2[0]};
+        const double nn = std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+        if (nn > 0.0)
+            for (double& c : n) c /= nn;
+        if (std::hypot(n[0], n[1]) < SLOPE) continue;
+        for (int i = 0; i < 4; i++) {
+            const double *u = q + 3 * i, *w = q + 3 * ((i + 1) % 4);
+            if (std::fabs(u[2] - z0) > tol || std::fabs(w[2] - z0) > tol) continue;
+            P2 a{u[0], u[1]}, b{w[0], w[1]};
+            if (dist(a, b) <= tol) continue;
+            if ((b.x - a.x) * -n[1] + (b.y - a.y) * n[0] < 0.0) std::swap(a, b);
+            segs.push_back({a, b});
+        }
+    }
+    if (segs.empty()) return why = "the wetted surface has no waterline", std::vector<double>{};
+    double mx = 0.0, my = 0.0;
+    for (auto& s : segs) mx += s.first.x + s.second.x, my += s.first.y + s.second.y;
+    const double sx = isx && mx < 0.0 ? -1.0 : 1.0, sy = isy && my < 0.0 ? -1.0 : 1.0;
+    for (auto& s : segs) {
+        s.first = {sx * s.first.x, sy * s.first.y};
+        s.second = {sx * s.second.x, sy * s.second.y};
+        if (sx * sy < 0.0) std::swap(s.first, s.second);
+    }
+    // interior.rs:217-272 open chains and closed loops
+    const size_t n = segs.size();
+    std::vector<long> nxt(n, -1), prv(n, -1);
+    for (size_t i = 0; i < n; i++)
+        for (size_t j = 0; j < n; j++) {
+            if (i == j || dist(segs[i].second, segs[j].first) > tol) continue;
+            if (nxt[i] >= 0 || prv[j] >= 0) return why = "waterline contours touch or cross", std::vector<double>{};
+            nxt[i] = (long)j;
+            prv[j] = (long)i;
+        }
+    std::vector<bool> used(n, false);
+    std::vector<Loop> chains, loops;
+    for (size_t s = 0; s < n; s++) {
+        if (prv[s] >= 0) continue;
+        Loop c{segs[s].first};
+        for (long k = (long)s; k >= 0; k = nxt[k]) {
+            used[k] = true;
+            c.push_back(segs[k].second);
+        }
+        chains.push_back(c);
+    }
+    for (size_t s = 0; s < n; s++) {
+        if (used[s]) continue;
+        Loop c;
+        for (long k = (long)s; !used[k];) {
+            used[k] = true;
+            c.push_back(segs[k].first);
+            k = nxt[k];
+            if (k < 0) return why = "broken waterline loop", std::vector<double>{};
+        }
+        loops.push_back(c);
+    }
+    // interior.rs:274-340 the open chains closed along the symmetry axes: the quadrant boundary
+    // traversed +x along y = 0, then -y along x = 0, wrapping through the corner
+    const bool ax_x = isy, ax_y = isx;
+    auto on_x = [&](P2 p) { return ax_x && std::fabs(p.y) <= tol && (p.x >= -tol || !ax_y); };
+    auto on_y = [&](P2 p) { return ax_y && std::fabs(p.x) <= tol && (p.y >= -tol || !ax_x); };
+    auto key_start = [&](P2 p) { return on_x(p) ? std::make_pair(0, p.x) : std::make_pair(1, -p.y); };
+    auto key_end = [&](P2 p) { return on_y(p) ? std::make_pair(1, -p.y) : std::make_pair(0, p.x); };
+    const std::string open = "the waterline does not close";
+    for (auto& c : chains)
+        if (!(on_x(c.front()) || on_y(c.front())) || !(on_x(c.back()) || on_y(c.back()))) return why = open, std::vector<double>{};
+    std::vector<bool> cused(chains.size(), false);
+    for (size_t c0 = 0; c0 < chains.size(); c0++) {
+        if (cused[c0]) continue;
+        Loop l;
+        for (size_t c = c0;;) {
+            cused[c] = true;
+            l.insert(l.end(), chains[c].begin(), chains[c].end());
+            const auto ke = key_end(chains[c].back());
+            long best = -1;
+            bool wrap = false;
+            for (int pass = 0; pass < 2 && best < 0; pass++) {
+                for (size_t d = 0; d < chains.size(); d++) {
+                    if (cused[d] && d != c0) continue;
+                    const auto ks = key_start(chains[d].front());
+                    if (pass == 0 && ks < ke) continue;
+                    if (best < 0 || ks < key_start(chains[best].front())) best = (long)d;
+                }
+                wrap = pass == 1;
+            }
+            if (best < 0) return why = open, std::vector<double>{};
+            if (ke.first == 0 && key_start(chains[best].front()).first == 1 && !wrap) return why = open, std::vector<double>{};
+            if (wrap) {
+                if (!(ax_x && ax_y)) return why = open, std::vector<double>{};
+                l.push_back(P2{0.0, 0.0});
+            }
+            if ((size_t)best == c0) break;
+            c = (size_t)best;
+        }
+        loops.push_back(l);
+    }
+    // interior.rs:343-357 repeated points (and the closing repetition) dropped
+    for (auto& l : loops) {
+        Loop c;
+        for (P2 p : l)
+            if (c.empty() || dist(c.back(), p) > tol) c.push_back(p);
+        while (c.size() > 1 && dist(c.front(), c.back()) <= tol) c.pop_back();
+        l = c;
+    }
+    if (loops_meet(loops, tol)) return why = "waterline contours cross or touch", std::vector<double>{};
+    // interior.rs:360-391 outer loops (counter-clockwise); an opening refuses the fan
+    std::vector<Loop> outers, holes;
+    for (auto& l : loops)
+        if (l.size() >= 3) (signed_area(l) > 0.0 ? outers : holes).push_back(l);
+    if (outers.empty()) return why = "no enclosed region", std::vector<double>{};
+    for (auto& h : holes) {
+        bool owned = false;
+        for (auto& o : outers) owned = owned || inside(o, h[0]);
+        if (!owned) return why = "a waterline contour lies outside the body", std::vector<double>{};
+        return why = "a waterplane region has an opening (a moonpool); use 'waterline'", std::vector<double>{};
+    }
+    std::vector<double> out;
+    // interior.rs:394-409 a polygon of the quadrant as a stored panel
+    auto emit = [&](std::initializer_list<P2> cs) {
+        double w[4][3];
+        int k = 0;
+        for (P2 p : cs) w[k][0] = sx * p.x, w[k][1] = sy * p.y, w[k][2] = z0, k++;
+        if (sx * sy < 0.0) std::reverse(&w[0], &w[k]);
+        if (k == 3)
+            for (int d = 0; d < 3; d++) w[3][d] = w[2][d];
+        for (int i = 0; i < 4; i++)
+            for (int d = 0; d < 3; d++) out.push_back(w[i][d]);
+    };
+    // interior.rs:447-517 the fan of each region
+    for (const Loop& l : outers) {
+        double a = 0.0, cx = 0.0, cy = 0.0;
+        bool on_y0 = false, on_x0 = false;
+        for (size_t i = 0; i < l.size(); i++) {
+            const P2 p = l[i], q = l[(i + 1) % l.size()];
+            const double c = p.x * q.y - p.y * q.x;
+            a += 0.5 * c;
+            cx += (p.x + q.x) * c / 6.0;
+            cy += (p.y + q.y) * c / 6.0;
+            on_y0 = on_y0 || (ax_x && std::fabs(p.y) <= tol && std::fabs(q.y) <= tol);
+            on_x0 = on_x0 || (ax_y && std::fabs(p.x) <= tol && std::fabs(q.x) <= tol);
+        }
+        P2 c{cx / a, cy / a};
+        if (on_x0) c.x = 0.0;
+        if (on_y0) c.y = 0.0;
+        std::vector<std::pair<P2, P2>> fan;
+        double ray = 0.0, seg = 0.0;
+        for (size_t i = 0; i < l.size(); i++) {
+            const P2 p = l[i], q = l[(i + 1) % l.size()];
+            const double s = orient(c, p, q);
+            if (std::fabs(s) <= tol * dist(p, q)) continue;  // an edge through the centroid bounds no area
+            if (s < 0.0)
+                return why = "a ray from the centroid of a waterplane region meets its waterline more than once; use 'waterline'",
+                       std::vector<double>{};
+            fan.push_back({p, q});
+            ray += 0.5 * (dist(c, p) + dist(c, q));
+            seg += dist(p, q);
+        }
+        if (fan.empty()) return why = "no enclosed region", std::vector<double>{};
+        const int N = std::max(1, (int)std::ceil(ray / seg - 1e-9));
+        std::vector<double> t(N + 1);
+        for (int k = 0; k <= N; k++) t[k] = k == N ? 1.0 : std::sin(0.5 * PI * k / N);
+        auto at = [&](P2 p, double s) { return P2{c.x + s * (p.x - c.x), c.y + s * (p.y - c.y)}; };
+        for (auto& [p, q] : fan) {
+            emit({c, at(p, t[1]), at(q, t[1])});
+            for (int k = 1; k < N; k++) emit({at(p, t[k]), at(p, t[k + 1]), at(q, t[k + 1]), at(q, t[k])});
+        }
+    }
+    return out;
+}
+
+}  // namespace graded
+
+// The panels of body b in body coordinates (bv [P][4][3]) with their kinds (bk), the interior surface
+// appended.  form -1: a lone body whose mesh (and interior mesh) declare the same symmetry planes,
+// placed on them, keeps the stored panels (solved by symmetry sectors, one system per sector; sym set
+// to its planes), any other arrangement takes its whole mirrored mesh; 0: always the mirrored mesh;
+// 1: always the stored panels (sym the mesh's planes).
+static HbStatus body_panels(const HbModel* model, const BodyObj& b, int form, std::vector<double>& bv,
+                            std::vector<int32_t>& bk, int32_t& sym) {
+    const MeshObj* mesh = nullptr;
+    const MeshObj* lid = nullptr;
+    for (auto& m : model->meshes) {
+        if (m.name == b.mesh) mesh = &m;
+        if (m.name == b.interior_mesh) lid = &m;
+    }
+    if (!mesh || mesh->vertices.empty()) return refuse(HB_ERR_VALUE, "the body has no panels mesh");
+    const int msym = mesh->symmetry == "yz" ? HBG_SYM_YZ : mesh->symmetry == "xz" ? HBG_SYM_XZ
+                     : mesh->symmetry == "xz_and_yz"                         ? HBG_SYM_BOTH
+                                                                             : HBG_SYM_NONE;
+    const bool on_planes = (!(msym & HBG_SYM_YZ) || b.position[0] == 0.0) &&
+                           (!(msym & HBG_SYM_XZ) || b.position[1] == 0.0);
+    const bool sectors = form == 1 || (form == -1 && msym != HBG_SYM_NONE && on_planes &&
+                                       (b.interior != "mesh" || (lid && lid->symmetry == mesh->symmetry)));
+    bv = sectors ? mesh->vertices : expand(*mesh);
+    sym = sectors ? msym : HBG_SYM_NONE;
+    size_t P = bv.size() / 12;
+    bk.assign(P, HBG_WET);
+    if (b.interior == "detect")
+        for (size_t p = 0; p < P; p++) {
+            bool z0 = true;
+            for (int i = 0; i < 4; i++) z0 = z0 && bv[12 * p + 3 * i + 2] == 0.0;
+            if (z0) bk[p] = HBG_INTERIOR;
+        }
+    if (b.interior == "projected") {
+        std::string why;
+        std::vector<double> lv = projected_lid(bv, -b.position[2], why);
+        if (!why.empty()) return refuse(HB_ERR_VALUE, "body '" + b.name + "': interior surface 'projected': " + why);
+        bv.insert(bv.end(), lv.begin(), lv.end());
+        bk.resize(bv.size() / 12, HBG_INTERIOR);
+    }
+    if (b.interior == "graded") {
+        // generated on the stored panels and reflected like them (interior.rs:521-575)
+        std::string why;
+        std::vector<double> lv = graded::lid(mesh->vertices, (msym & HBG_SYM_YZ) != 0, (msym & HBG_SYM_XZ) != 0,
+                                             -b.position[2], why);
+        if (!why.empty()) return refuse(HB_ERR_VALUE, "body '" + b.name + "': interior surface 'graded': " + why);
+        if (!sectors) lv = reflect(lv, mesh->symmetry);
+        bv.insert(bv.end(), lv.begin(), lv.end());
+        bk.resize(bv.size() / 12, HBG_INTERIOR);
+    }
+    if (b.interior == "mesh") {
+        if (!lid) return refuse(HB_ERR_VALUE, "interior_surface_mesh names no mesh");
+        std::vector<double> lv = sectors ? lid->vertices : expand(*lid);
+        bv.insert(bv.end(), lv.begin(), lv.end());
+        bk.resize(bv.size() / 12, HBG_INTERIOR);
+    }
+    return HB_OK;
 }
 
 }  // namespace hbg
@@ -485,8 +803,9 @@ extern "C" HbStatus hb_set_text(HbModel* model, uint64_t object, const char* ite
             BodyObj& b = model->bodies[object - OBJ_BODY0];
             if (it == "mesh") return b.mesh = v, HB_OK;
             if (it == "interior_surface") {
-                if (v != "none" && v != "detect" && v != "mesh" && v != "projected")
-                    return refuse(HB_ERR_UNSUPPORTED, "interior_surface none, detect, projected or mesh on this route");
+                if (v != "none" && v != "detect" && v != "mesh" && v != "projected" && v != "graded")
+                    return refuse(HB_ERR_UNSUPPORTED,
+                                  "interior_surface none, detect, projected, graded or mesh on this route");
                 return b.interior = v, HB_OK;
             }
             if (it == "interior_surface_mesh") return b.interior_mesh = v, HB_OK;
@@ -532,46 +851,11 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
             if (model->bodies.empty()) return refuse(HB_ERR_VALUE, "the model has no body");
             for (size_t bi = 0; bi < model->bodies.size(); bi++) {
                 const BodyObj& b = model->bodies[bi];
-                const MeshObj* mesh = nullptr;
-                const MeshObj* lid = nullptr;
-                for (auto& m : model->meshes) {
-                    if (m.name == b.mesh) mesh = &m;
-                    if (m.name == b.interior_mesh) lid = &m;
-                }
-                if (!mesh || mesh->vertices.empty()) return refuse(HB_ERR_VALUE, "the body has no panels mesh");
-                // A lone body whose mesh (and interior mesh) declare the same symmetry planes, placed on
-                // them, is solved by symmetry sectors (the stored panels, one system per sector); any
-                // other arrangement by its whole mirrored mesh.
-                const int msym = mesh->symmetry == "yz" ? HBG_SYM_YZ : mesh->symmetry == "xz" ? HBG_SYM_XZ
-                                 : mesh->symmetry == "xz_and_yz"                         ? HBG_SYM_BOTH
-                                                                                         : HBG_SYM_NONE;
-                const bool on_planes = (!(msym & HBG_SYM_YZ) || b.position[0] == 0.0) &&
-                                       (!(msym & HBG_SYM_XZ) || b.position[1] == 0.0);
-                const bool sectors = model->bodies.size() == 1 && msym != HBG_SYM_NONE && on_planes &&
-                                     (b.interior != "mesh" || (lid && lid->symmetry == mesh->symmetry));
-                std::vector<double> bv = sectors ? mesh->vertices : expand(*mesh);
-                if (sectors) symmetry = msym;
-                size_t P = bv.size() / 12;
-                std::vector<int32_t> bk(P, HBG_WET);
-                if (b.interior == "detect")
-                    for (size_t p = 0; p < P; p++) {
-                        bool z0 = true;
-                        for (int i = 0; i < 4; i++) z0 = z0 && bv[12 * p + 3 * i + 2] == 0.0;
-                        if (z0) bk[p] = HBG_INTERIOR;
-                    }
-                if (b.interior == "projected") {
-                    std::string why;
-                    std::vector<double> lv = projected_lid(bv, -b.position[2], why);
-                    if (!why.empty()) return refuse(HB_ERR_VALUE, "body '" + b.name + "': interior surface 'projected': " + why);
-                    bv.insert(bv.end(), lv.begin(), lv.end());
-                    bk.resize(bv.size() / 12, HBG_INTERIOR);
-                }
-                if (b.interior == "mesh") {
-                    if (!lid) return refuse(HB_ERR_VALUE, "interior_surface_mesh names no mesh");
-                    std::vector<double> lv = sectors ? lid->vertices : expand(*lid);
-                    bv.insert(bv.end(), lv.begin(), lv.end());
-                    bk.resize(bv.size() / 12, HBG_INTERIOR);
-                }
+                std::vector<double> bv;
+                std::vector<int32_t> bk;
+                int32_t bsym = HBG_SYM_NONE;
+                if (HbStatus st = body_panels(model, b, model->bodies.size() == 1 ? -1 : 0, bv, bk, bsym)) return st;
+                if (bsym != HBG_SYM_NONE) symmetry = bsym;
                 for (size_t q = 0; q < bv.size(); q++) bv[q] += b.position[q % 3];  // body to global
                 verts.insert(verts.end(), bv.begin(), bv.end());
                 kinds.insert(kinds.end(), bk.begin(), bk.end());
@@ -807,6 +1091,57 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
             model->results = std::make_unique<HbResults>(*r);
         }
         if (out) *out = r.release();
+        return HB_OK;
+    });
+}
+
+// hydrobem.h:975-987 hb_model_panels: the panels as the solve uses them, host work only (a results
+// object in place of the reference's table).  Roles
+// "wetted" and "lid" (the interior free surface), comma separated, null for both; the stored form of
+// each body's symmetric mesh unless include_reflections.  Quantities: vertices (HB_F64 [P][4][3],
+// global), body (HB_I32 [P], zero-based in the order added), kind (HB_I32 [P], HBG_WET / HBG_INTERIOR).
+extern "C" HbStatus hb_model_panels(HbModel* model, const char* role, int32_t include_reflections, HbResults** out) {
+    return guard([&]() -> HbStatus {
+        if (!model || !out) return refuse(HB_ERR_ARGUMENT, "null model or out-pointer");
+        *out = nullptr;
+        bool want[2] = {role == nullptr, role == nullptr};
+        if (role) {
+            std::string r(role);
+            size_t a = 0;
+            while (a <= r.size()) {
+                size_t e = r.find(',', a);
+                if (e == std::string::npos) e = r.size();
+                const std::string w = r.substr(a, e - a);
+                if (w == "wetted") want[HBG_WET] = true;
+                else if (w == "lid") want[HBG_INTERIOR] = true;
+                else return refuse(HB_ERR_UNSUPPORTED, "panel role '" + w + "' is not on this route (wetted, lid)");
+                a = e + 1;
+            }
+        }
+        std::vector<double> verts;
+        std::vector<int32_t> body, kind;
+        {
+            std::lock_guard<std::mutex> g(model->lock);
+            for (size_t bi = 0; bi < model->bodies.size(); bi++) {
+                const BodyObj& b = model->bodies[bi];
+                std::vector<double> bv;
+                std::vector<int32_t> bk;
+                int32_t sym = HBG_SYM_NONE;
+                if (HbStatus st = body_panels(model, b, include_reflections ? 0 : 1, bv, bk, sym)) return st;
+                for (size_t p = 0; p < bk.size(); p++) {
+                    if (!want[bk[p]]) continue;
+                    for (int q = 0; q < 12; q++) verts.push_back(bv[12 * p + q] + b.position[q % 3]);
+                    body.push_back((int32_t)bi);
+                    kind.push_back(bk[p]);
+                }
+            }
+        }
+        auto r = std::make_unique<HbResults>();
+        const size_t P = kind.size();
+        add_quantity(r.get(), "vertices", HB_F64, {P, 4, 3}, verts.data(), verts.size() * sizeof(double));
+        add_quantity(r.get(), "body", HB_I32, {P}, body.data(), P * sizeof(int32_t));
+        add_quantity(r.get(), "kind", HB_I32, {P}, kind.data(), P * sizeof(int32_t));
+        *out = r.release();
         return HB_OK;
     });
 }

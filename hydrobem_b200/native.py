@@ -94,7 +94,7 @@ EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
            "hbg_statics_noalloc", "hbg_measure_peaks", "hbg_last_ir_history", "hbg_surrogate_train",
            "hbg_surrogate_grad", "hbg_surrogate_eval", "hbg_last_surrogate_pairs", "hbg_read_gdf", "hbg_gdf_free",
-           "hb_model_load_mesh", "hbg_last_fallback_count", "hbg_debug_lu_f64"]
+           "hb_model_load_mesh", "hbg_last_fallback_count", "hbg_debug_lu_f64", "hb_model_panels"]
 
 _lib = None
 
@@ -529,6 +529,7 @@ class Model:
         L.hb_model_free.argtypes = [ctypes.c_void_p]
         L.hb_results_quantity.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(HbColumn)]
         L.hb_results_free.argtypes = [ctypes.c_void_p]
+        L.hb_model_panels.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
         self.m = ctypes.c_void_p()
         check(L.hb_model_new(ctypes.byref(self.m)))
 
@@ -566,6 +567,18 @@ class Model:
 
     def boolean(self, path: str, item: str, value: bool):
         check(self.L.hb_set_bool(self.m, self.obj(path), item.encode(), int(bool(value))))
+
+    def panels(self, role: str | None = None, include_reflections: bool = False) -> dict:
+        """hb_model_panels (host work, no device): vertices [P][4][3], body [P], kind [P] of the roles
+        ("wetted", "lid", comma separated; None both), stored symmetric form unless include_reflections."""
+        r = ctypes.c_void_p()
+        check(self.L.hb_model_panels(self.m, None if role is None else role.encode(), int(bool(include_reflections)),
+                                     ctypes.byref(r)))
+        res = Results(self.L, r)
+        try:
+            return {k: res.quantity(k) for k in ("vertices", "body", "kind")}
+        finally:
+            res.free()
 
     def solve(self) -> "Results":
         r = ctypes.c_void_p()

@@ -433,6 +433,11 @@ HbStatus hb_model_solve(HbModel *model, HbProgressFn progress, void *user, HbRes
  * (HB_F32 [F][D][K]), excitation_diffraction, excitation_froude_krylov, excitation_scattering
  * (HB_C64 [F][H][D]), excitation_haskind (HB_C64 [F][H][K], K = D radiation columns); the extension
  * quantities <name>_f64 (HB_F64 / HB_C128) keep double precision. */
+/* hydrobem.h:975-987 (a results object in place of the reference's HbTable): the panels as the solve uses
+ * them, host work only; role "wetted", "lid" or both comma separated (null: both); the stored form of a
+ * symmetric mesh unless include_reflections.  Quantities vertices (HB_F64 [P][4][3], global), body
+ * (HB_I32 [P]) and kind (HB_I32 [P], HBG_WET / HBG_INTERIOR). */
+HbStatus hb_model_panels(HbModel *model, const char *role, int32_t include_reflections, HbResults **out);
 void hb_results_free(HbResults *results);
 HbStatus hb_results_has(HbResults *results, const char *name, int32_t *has);
 HbStatus hb_results_quantity(HbResults *results, const char *name, HbColumn *column);

@@ -511,6 +511,277 @@ def projected_lid(verts, z0=0.0):
     return np.array(out)
 
 
+def _dist(a, b):
+    return float(np.hypot(a[0] - b[0], a[1] - b[1]))
+
+
+def _orient(o, a, b):
+    return (a[0] - o[0]) * (b[1] - o[1]) - (a[1] - o[1]) * (b[0] - o[0])
+
+
+def _seg_dist(x, a, b):
+    """polygon.rs:94-99 the distance from x to the segment ab."""
+    e = (b[0] - a[0], b[1] - a[1])
+    w = (x[0] - a[0], x[1] - a[1])
+    ee = e[0] * e[0] + e[1] * e[1]
+    t = min(1.0, max(0.0, (w[0] * e[0] + w[1] * e[1]) / ee)) if ee > 0.0 else 0.0
+    return _dist(x, (a[0] + t * e[0], a[1] + t * e[1]))
+
+
+def _meet(p, q, a, b):
+    """polygon.rs:81-90 whether the segments pq and ab cross or touch."""
+    d1, d2, d3, d4 = _orient(a, b, p), _orient(a, b, q), _orient(p, q, a), _orient(p, q, b)
+    if ((d1 > 0 and d2 < 0) or (d1 < 0 and d2 > 0)) and ((d3 > 0 and d4 < 0) or (d3 < 0 and d4 > 0)):
+        return True
+
+    def on(o, e, x, d):
+        return d == 0.0 and min(o[0], e[0]) <= x[0] <= max(o[0], e[0]) and min(o[1], e[1]) <= x[1] <= max(o[1], e[1])
+
+    return on(a, b, p, d1) or on(a, b, q, d2) or on(p, q, a, d3) or on(p, q, b, d4)
+
+
+def _loops_meet(loops, tol):
+    """polygon.rs:111-149 whether two loops, or two non-adjacent edges of one loop, cross or come within tol."""
+    edges = [(li, k, lp[k], lp[(k + 1) % len(lp)]) for li, lp in enumerate(loops) for k in range(len(lp))]
+    for i in range(len(edges)):
+        for j in range(i + 1, len(edges)):
+            e, f = edges[i], edges[j]
+            if (min(e[2][0], e[3][0]) - tol > max(f[2][0], f[3][0]) + tol
+                    or min(f[2][0], f[3][0]) - tol > max(e[2][0], e[3][0]) + tol
+                    or min(e[2][1], e[3][1]) - tol > max(f[2][1], f[3][1]) + tol
+                    or min(f[2][1], f[3][1]) - tol > max(e[2][1], e[3][1]) + tol):
+                continue
+            if e[0] == f[0]:
+                n = len(loops[e[0]])
+                if n <= 3 or (e[1] + 1) % n == f[1] or (f[1] + 1) % n == e[1]:
+                    continue
+            if (_meet(e[2], e[3], f[2], f[3]) or _seg_dist(e[2], f[2], f[3]) <= tol or _seg_dist(e[3], f[2], f[3]) <= tol
+                    or _seg_dist(f[2], e[2], e[3]) <= tol or _seg_dist(f[3], e[2], e[3]) <= tol):
+                return True
+    return False
+
+
+def _inside(loop, x):
+    """polygon.rs:29-39 crossing-number test."""
+    c = False
+    n = len(loop)
+    for k in range(n):
+        p, q = loop[k], loop[(k + 1) % n]
+        if (p[1] > x[1]) != (q[1] > x[1]) and x[0] < p[0] + (x[1] - p[1]) / (q[1] - p[1]) * (q[0] - p[0]):
+            c = not c
+    return c
+
+
+def _signed_area(loop):
+    n = len(loop)
+    return 0.5 * sum(loop[k][0] * loop[(k + 1) % n][1] - loop[(k + 1) % n][0] * loop[k][1] for k in range(n))
+
+
+def graded_lid(verts, isx=0, isy=0, z0=0.0, reference_length=1.0):
+    """interior.rs:139-515 graded: the interior free surface fanned from the area centroid of each
+    waterplane region to its waterline segments, the rays divided at t_k = sin(pi k / (2N)).
+
+    ``verts`` [P][4][3] the stored panels of the mesh (one sector when isx / isy declare the planes
+    x = 0 / y = 0); returns the generated panels [Q][4][3] in the same stored form (a triangle repeats its
+    last vertex), facing up.  Steps:
+
+    - waterline segments (interior.rs:158-214): the edges lying in z0 (within tol = 1e-6 max(reference
+      length, |vertex coordinates|)) of the non-horizontal panels (|n_h| >= 1e-6), oriented along
+      z x n_h, mapped to the quadrant x, y >= 0 by the sign of the coordinate sums on symmetric axes;
+    - chains and loops (interior.rs:217-272), open chains closed along the symmetry axes through the
+      quadrant corner (interior.rs:274-340), repeated points dropped (interior.rs:343-357);
+    - contours that cross or touch, openings, or a region whose waterline a centroid ray meets twice
+      raise ValueError, as the reference does."""
+    v = np.asarray(verts, dtype=np.float64).reshape(-1, 4, 3)
+    tol = 1e-6 * max(reference_length, float(np.abs(v).max()) if v.size else 0.0)
+    segs = []
+    total = 0.0
+    for q in v:
+        n = np.cross(q[2] - q[0], q[3] - q[1])
+        nn = np.linalg.norm(n)
+        n = n / nn if nn > 0 else n
+        if np.hypot(n[0], n[1]) < 1e-6:
+            continue
+        d = (-n[1], n[0])
+        for i in range(4):
+            u, w = q[i], q[(i + 1) % 4]
+            if abs(u[2] - z0) > tol or abs(w[2] - z0) > tol:
+                continue
+            a, b = (u[0], u[1]), (w[0], w[1])
+            if _dist(a, b) <= tol:
+                continue
+            if (b[0] - a[0]) * d[0] + (b[1] - a[1]) * d[1] < 0.0:
+                a, b = b, a
+            segs.append([a, b])
+            total += _dist(a, b)
+    if not segs:
+        raise ValueError("the wetted surface has no waterline")
+    mx = sum(s[0][0] + s[1][0] for s in segs)
+    my = sum(s[0][1] + s[1][1] for s in segs)
+    sx = -1.0 if isx and mx < 0.0 else 1.0
+    sy = -1.0 if isy and my < 0.0 else 1.0
+    for s in segs:
+        s[0] = (sx * s[0][0], sy * s[0][1])
+        s[1] = (sx * s[1][0], sy * s[1][1])
+        if sx * sy < 0.0:
+            s[0], s[1] = s[1], s[0]
+    # chains (from a segment without a predecessor) and closed loops
+    n = len(segs)
+    nxt, prv = [-1] * n, [-1] * n
+    for i in range(n):
+        for j in range(n):
+            if i == j or _dist(segs[i][1], segs[j][0]) > tol:
+                continue
+            if nxt[i] >= 0 or prv[j] >= 0:
+                raise ValueError("waterline contours touch or cross")
+            nxt[i], prv[j] = j, i
+    used = [False] * n
+    chains, loops = [], []
+    for s in range(n):
+        if prv[s] >= 0:
+            continue
+        c, k = [segs[s][0]], s
+        while k >= 0:
+            used[k] = True
+            c.append(segs[k][1])
+            k = nxt[k]
+        chains.append(c)
+    for s in range(n):
+        if used[s]:
+            continue
+        c, k = [], s
+        while not used[k]:
+            used[k] = True
+            c.append(segs[k][0])
+            k = nxt[k]
+            if k < 0:
+                raise RuntimeError("broken waterline loop")
+        loops.append(c)
+    ax_x, ax_y = bool(isy), bool(isx)
+
+    def on_x(p):
+        return ax_x and abs(p[1]) <= tol and (p[0] >= -tol or not ax_y)
+
+    def on_y(p):
+        return ax_y and abs(p[0]) <= tol and (p[1] >= -tol or not ax_x)
+
+    def key_start(p):
+        return (0, p[0]) if on_x(p) else (1, -p[1])
+
+    def key_end(p):
+        return (1, -p[1]) if on_y(p) else (0, p[0])
+
+    for c in chains:
+        if not (on_x(c[0]) or on_y(c[0])) or not (on_x(c[-1]) or on_y(c[-1])):
+            raise ValueError("the waterline does not close")
+    cused = [False] * len(chains)
+    for c0 in range(len(chains)):
+        if cused[c0]:
+            continue
+        lp, c = [], c0
+        while True:
+            cused[c] = True
+            lp.extend(chains[c])
+            ke = key_end(chains[c][-1])
+            best, wrap = -1, False
+            for pas in range(2):
+                if best >= 0:
+                    break
+                for d in range(len(chains)):
+                    if cused[d] and d != c0:
+                        continue
+                    ks = key_start(chains[d][0])
+                    if pas == 0 and ks < ke:
+                        continue
+                    if best < 0 or ks < key_start(chains[best][0]):
+                        best = d
+                wrap = pas == 1
+            if best < 0:
+                raise ValueError("the waterline does not close")
+            ks = key_start(chains[best][0])
+            if ke[0] == 0 and ks[0] == 1 and not wrap:
+                raise ValueError("the waterline does not close")
+            if wrap:
+                if not (ax_x and ax_y):
+                    raise ValueError("the waterline does not close")
+                lp.append((0.0, 0.0))
+            if best == c0:
+                break
+            c = best
+        loops.append(lp)
+    for i, lp in enumerate(loops):
+        c = []
+        for p in lp:
+            if not c or _dist(c[-1], p) > tol:
+                c.append(p)
+        while len(c) > 1 and _dist(c[0], c[-1]) <= tol:
+            c.pop()
+        loops[i] = c
+    if _loops_meet(loops, tol):
+        raise ValueError("waterline contours cross or touch")
+    outers = [lp for lp in loops if len(lp) >= 3 and _signed_area(lp) > 0.0]
+    holes = [lp for lp in loops if len(lp) >= 3 and not _signed_area(lp) > 0.0]
+    if not outers:
+        raise ValueError("no enclosed region")
+    for h in holes:
+        if not any(_inside(o, h[0]) for o in outers):
+            raise ValueError("a waterline contour lies outside the body")
+        raise ValueError("a waterplane region has an opening (a moonpool)")
+    out = []
+
+    def mapped(cs):
+        w = np.zeros((4, 3))
+        for k, p in enumerate(cs):
+            w[k] = (sx * p[0], sy * p[1], z0)
+        if sx * sy < 0.0:
+            w[:len(cs)] = w[:len(cs)][::-1]
+        if len(cs) == 3:
+            w[3] = w[2]
+        return w
+
+    for lp in outers:
+        a = cx = cy = 0.0
+        on_y0 = on_x0 = False
+        m = len(lp)
+        for i in range(m):
+            p, q = lp[i], lp[(i + 1) % m]
+            cr = p[0] * q[1] - p[1] * q[0]
+            a += 0.5 * cr
+            cx += (p[0] + q[0]) * cr / 6.0
+            cy += (p[1] + q[1]) * cr / 6.0
+            on_y0 = on_y0 or (ax_x and abs(p[1]) <= tol and abs(q[1]) <= tol)
+            on_x0 = on_x0 or (ax_y and abs(p[0]) <= tol and abs(q[0]) <= tol)
+        c = [cx / a, cy / a]
+        if on_x0:
+            c[0] = 0.0
+        if on_y0:
+            c[1] = 0.0
+        fan, ray, seg = [], 0.0, 0.0
+        for i in range(m):
+            p, q = lp[i], lp[(i + 1) % m]
+            s = _orient(c, p, q)
+            if abs(s) <= tol * _dist(p, q):
+                continue
+            if s < 0.0:
+                raise ValueError("a ray from the centroid of a waterplane region meets its waterline more than once")
+            fan.append((p, q))
+            ray += 0.5 * (_dist(c, p) + _dist(c, q))
+            seg += _dist(p, q)
+        if not fan:
+            raise ValueError("no enclosed region")
+        N = max(1, int(np.ceil(ray / seg - 1e-9)))
+        t = [1.0 if k == N else float(np.sin(0.5 * np.pi * k / N)) for k in range(N + 1)]
+
+        def at(p, s):
+            return (c[0] + s * (p[0] - c[0]), c[1] + s * (p[1] - c[1]))
+
+        for p, q in fan:
+            out.append(mapped([tuple(c), at(p, t[1]), at(q, t[1])]))
+            for k in range(1, N):
+                out.append(mapped([at(p, t[k]), at(p, t[k + 1]), at(q, t[k + 1]), at(q, t[k])]))
+    return np.array(out)
+
+
 # ------------------------------------------------------------------ field points
 def field_influence(panels, kinds, pts, depth, omega, grav=GRAVITY, logint=True, tol=1e-4):
     """(S, D) [P][N] complex128: the influence of every panel at every field point."""

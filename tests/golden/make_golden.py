@@ -17,6 +17,10 @@ Every fixture is a compressed .npz of numbers the reference's test suite holds o
 - lo_cylinder_field.npz  the reference solver's own field-point outputs of its regression problem
   lo_cylinder_field_body_points (the same cylinder held fixed, three points: the elevation at z = 0
   and p / (rho g) below, per radiation column and heading, complex64)
+- lo_cylinder_interior.npz  the reference solver's own outputs of its regression problem
+  lo_cylinder_interior (the quarter cylinder of lo_cylinder_drift held fixed, its interior free
+  surface generated by the 'graded' method: A, B, X, FK, SC, the Haskind force and the field-point
+  velocities at three points, float32 / complex64 as stored)
 - meshes.npz         SHA-256 digests and small copies of the reference's procedural meshes
   (tests/python/meshes.py imported from the reference) for the configs' bodies
 """
@@ -75,6 +79,12 @@ def main(argv):
     keep = ["omegas", "headings", "field_points", "field_points_pressure_radiation", "field_points_pressure_incident",
             "field_points_pressure_scattering", "field_points_pressure_diffraction"]
     np.savez_compressed(HERE / "lo_cylinder_field.npz", **{k: d[k] for k in keep})
+    d = np.load(data / "regression" / "lo_cylinder_interior.npz")
+    keep = ["omegas", "headings", "added_mass", "radiation_damping", "excitation_diffraction",
+            "excitation_froude_krylov", "excitation_scattering", "excitation_haskind", "field_points",
+            "field_points_velocity_radiation", "field_points_velocity_incident",
+            "field_points_velocity_scattering", "field_points_velocity_diffraction"]
+    np.savez_compressed(HERE / "lo_cylinder_interior.npz", **{k: d[k] for k in keep})
     sys.path.insert(0, str(root / "tests" / "python"))
     import meshes  # the reference's procedural meshes (numpy only)
 
