@@ -77,7 +77,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
     uint64_t* empty = full + GSTAGES;
     uint64_t* tfull = empty + GSTAGES;  // [2]
     uint64_t* tempty = tfull + 2;       // [2]
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 2);
+    uint64_t* drain = tempty + 2;       // the MMA warp's last commit (every issued MMA complete)
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(drain + 1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int mt = (g.M + GBM - 1) / GBM, nt = (g.Nc + GBN - 1) / GBN;
     const int ntiles = mt * nt * g.batch;
@@ -92,6 +93,7 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
             tc::mbar_init(&tfull[b], 1);
             tc::mbar_init(&tempty[b], 4);  // one arrival per epilogue warp
         }
+        tc::mbar_init(drain, 1);
         tc::fence_barrier_init();
         tc::prefetch_tensormap(&mapA);
         tc::prefetch_tensormap(&mapB);
@@ -136,6 +138,13 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
                         tc::tma_load_4d(sB + s * GBN * GBK, &mapB, &full[s], kk, n0, 0, f);
                 }
             }
+            // every load still in flight lands before the CTA leaves (also after an error): the last
+            // phase armed on each stage completes (bounded)
+            for (int k = kc_global > GSTAGES ? kc_global - GSTAGES : 0; k < kc_global; k++)
+                if (!tc::mbar_wait(&full[k % GSTAGES], (k / GSTAGES) & 1)) {
+                    atomicExch(g.err, 6);
+                    break;
+                }
         }
     } else if (warp == 1) {
         if (lane == 0) {
@@ -175,6 +184,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
                 tc::mma_commit(&tfull[b]);
                 if (bad) break;
             }
+            // every issued MMA completes before TMEM is freed (also after an error; bounded)
+            tc::mma_commit(drain);
+            if (!tc::mbar_wait(drain, 0)) atomicExch(g.err, 7);
         }
     } else {
         // epilogue warps 2..5: TMEM lane quadrant (warp % 4), rows 32 (warp % 4) .. + 32 of the tile;
@@ -271,6 +283,8 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
     }
     tc::tc_fence_before();
     __syncthreads();
+    // freed even when a drain wait above gave up (err set, the results discarded): a CTA that left
+    // holding TMEM would stall every later allocation on its SM
     if (warp == 0) tc::tmem_dealloc(tmem, 2 * GBN);
 }
 

@@ -63,3 +63,22 @@ def test_statics_noalloc_rejects_more_panels_than_its_scratch():
         nv.statics_noalloc(buf.data_ptr(), None, 2049, buf.data_ptr())
     assert nv.STATUS_NAMES[e.value.status] == "HB_ERR_VALUE"
     assert "2048" in e.value.message
+
+
+def test_statics_noalloc_allocates_no_device_memory():
+    """After warm-up calls (module loading), further calls leave the device's free memory unchanged:
+    the entry writes only the caller's buffer and its fixed device scratch."""
+    torch = pytest.importorskip("torch")
+    v = meshes.cylinder(1.0, 0.5, 24, 8, 8)
+    N = len(v)
+    dv = torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64).reshape(-1)).cuda()
+    dst = torch.empty(4 * N * N, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for depth in (3.0, math.inf):  # both depth forms loaded (lazy module loading may allocate)
+        nv.statics_noalloc(dv.data_ptr(), None, N, dst.data_ptr(), depth=depth, stream=stream)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for depth in (3.0, math.inf):
+        nv.statics_noalloc(dv.data_ptr(), None, N, dst.data_ptr(), depth=depth, stream=stream)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
