@@ -286,18 +286,27 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     int dev = 0, n_sm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    const int dsmem = (int)df2_smem_bytes();
-    cudaFuncSetAttribute(k_diag_factor2, cudaFuncAttributeMaxDynamicSharedMemorySize, dsmem);
+    const int dsmem = (int)df_smem_bytes();
+    cudaFuncSetAttribute(k_diag_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, dsmem);
     cudaFuncSetAttribute(k_tri_step<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(8));
     cudaFuncSetAttribute(k_tri_step<10>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(10));
     cudaFuncSetAttribute(k_tri_step<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(12));
     cudaFuncSetAttribute(k_tri_step<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(16));
     // the persistent sweeps: as many CTAs as fit at once
-    const int nr_sweep = nrhs <= 8 ? 8 : nrhs <= 10 ? 10 : nrhs <= 12 ? 12 : nrhs <= 16 ? 16 : 32;
+    // (the sweep's products are FP32-FMA bound beyond 16 columns: no more padded columns than needed)
+    const int nr_sweep = nrhs <= 8    ? 8
+                         : nrhs <= 10 ? 10
+                         : nrhs <= 12 ? 12
+                         : nrhs <= 16 ? 16
+                         : nrhs <= 20 ? 20
+                         : nrhs <= 24 ? 24
+                                      : 32;
     const void* sweep_fn = nr_sweep == 8    ? (const void*)k_tri_sweep<8>
                            : nr_sweep == 10 ? (const void*)k_tri_sweep<10>
                            : nr_sweep == 12 ? (const void*)k_tri_sweep<12>
                            : nr_sweep == 16 ? (const void*)k_tri_sweep<16>
+                           : nr_sweep == 20 ? (const void*)k_tri_sweep<20>
+                           : nr_sweep == 24 ? (const void*)k_tri_sweep<24>
                                             : (const void*)k_tri_sweep<32>;
     cudaFuncSetAttribute(sweep_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tri_smem_bytes(nr_sweep));
     int sweep_per_sm = 0;
@@ -316,9 +325,12 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
     const int nz = (Nm + GEMV_CHUNK - 1) / GEMV_CHUNK;
     double2* part = (double2*)ws.get(WS_PART, (size_t)nz * BS * nrhs * Nm * 16);
     if (!part) MIXED_FAIL(HB_ERR_INTERNAL, "device memory allocation failed for the mixed form", -1);
-    for (auto fn : {(const void*)k_cgemv_tma<8>, (const void*)k_cgemv_tma<10>, (const void*)k_cgemv_tma<12>,
-                    (const void*)k_cgemv_tma<16>})
+    for (auto fn : {(const void*)k_cgemv_tma<4>, (const void*)k_cgemv_tma<8>, (const void*)k_cgemv_tma<10>,
+                    (const void*)k_cgemv_tma<12>, (const void*)k_cgemv_tma<16>})
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gv_smem_bytes<16>());
+    // the column width of a chunk of w right-hand sides (the products are FP64-FMA bound: the padded
+    // columns of the last chunk cost as much as real ones)
+    auto chunk_width = [](int w) { return w <= 4 ? 4 : w <= 8 ? 8 : w <= 10 ? 10 : w <= 12 ? 12 : 16; };
     // the TMA form (its maps cover exactly the matrices and vectors of the batch), beyond 16 right-hand
     // sides in column chunks of 16 (the matrix streamed once a chunk); the register form if a map fails
     auto gemv_tma = [&](const float* Mm, const double2* xv, int ldx, int nb, int nzt, cudaStream_t s) -> bool {
@@ -326,16 +338,17 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         const uint64_t dm[4] = {(uint64_t)Np, (uint64_t)Np, 2, (uint64_t)nb};
         const uint64_t sm[3] = {(uint64_t)Np * 4, NP2 * 4, MB * 4};
         const uint32_t bm[4] = {GV_ROWS, GV_COLS, 1, 1};
-        const int nr = nrhs <= 8 ? 8 : nrhs <= 10 ? 10 : nrhs <= 12 ? 12 : 16;
-        const uint64_t dx[4] = {2 * (uint64_t)ldx, (uint64_t)nrhs, (uint64_t)nb, 1};
-        const uint64_t sx[3] = {(uint64_t)ldx * 16, (uint64_t)nrhs * ldx * 16, (uint64_t)nb * nrhs * ldx * 16};
-        const uint32_t bx[4] = {2 * GV_COLS, (uint32_t)nr, 1, 1};
-        if (!make_map_box(&mM, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)Mm, dm, sm, bm) ||
-            !make_map_box(&mX, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void*)xv, dx, sx, bx))
-            return false;
+        if (!make_map_box(&mM, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)Mm, dm, sm, bm)) return false;
         dim3 g((Nm + GV_ROWS - 1) / GV_ROWS, nb, nzt);
         for (int c0 = 0; c0 < nrhs; c0 += 16) {
-            if (nr == 8)
+            const int nr = chunk_width(std::min(16, nrhs - c0));
+            const uint64_t dx[4] = {2 * (uint64_t)ldx, (uint64_t)nrhs, (uint64_t)nb, 1};
+            const uint64_t sx[3] = {(uint64_t)ldx * 16, (uint64_t)nrhs * ldx * 16, (uint64_t)nb * nrhs * ldx * 16};
+            const uint32_t bx[4] = {2 * GV_COLS, (uint32_t)nr, 1, 1};
+            if (!make_map_box(&mX, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void*)xv, dx, sx, bx)) return false;
+            if (nr == 4)
+                k_cgemv_tma<4><<<g, GV_THREADS, gv_smem_bytes<4>(), s>>>(mM, mX, Nm, nrhs, c0, part, nb, err);
+            else if (nr == 8)
                 k_cgemv_tma<8><<<g, GV_THREADS, gv_smem_bytes<8>(), s>>>(mM, mX, Nm, nrhs, c0, part, nb, err);
             else if (nr == 10)
                 k_cgemv_tma<10><<<g, GV_THREADS, gv_smem_bytes<10>(), s>>>(mM, mX, Nm, nrhs, c0, part, nb, err);
@@ -347,8 +360,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         return true;
     };
     const int nz_tma = (Nm + GV_CHUNK - 1) / GV_CHUNK;
-    for (auto fn : {(const void*)k_cgemv32_tma<8>, (const void*)k_cgemv32_tma<10>, (const void*)k_cgemv32_tma<12>,
-                    (const void*)k_cgemv32_tma<16>})
+    for (auto fn : {(const void*)k_cgemv32_tma<4>, (const void*)k_cgemv32_tma<8>, (const void*)k_cgemv32_tma<10>,
+                    (const void*)k_cgemv32_tma<12>, (const void*)k_cgemv32_tma<16>})
         cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gv32_smem_bytes<16>());
     // r = rk - M d with the complex64 correction d (FP32 products, FP64 sums; beyond 16 columns in chunks):
     // the residual after a correction that is small against the solution
@@ -357,17 +370,24 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         const uint64_t dm[4] = {(uint64_t)Np, (uint64_t)Np, 2, (uint64_t)nb};
         const uint64_t sm[3] = {(uint64_t)Np * 4, NP2 * 4, MB * 4};
         const uint32_t bm[4] = {GV_ROWS, GV_COLS, 1, 1};
-        const int nr = nrhs <= 8 ? 8 : nrhs <= 10 ? 10 : nrhs <= 12 ? 12 : 16;
         const uint64_t dd[4] = {2 * (uint64_t)Np, (uint64_t)nrhs, (uint64_t)nb, 1};
         const uint64_t sd[3] = {(uint64_t)Np * 8, (uint64_t)nrhs * Np * 8, (uint64_t)nb * nrhs * Np * 8};
-        const uint32_t bd[4] = {2 * GV_COLS, (uint32_t)nr, 1, 1};
-        if (!make_map_box(&mM, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)Mm, dm, sm, bm) ||
-            !make_map_box(&mD, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)dv, dd, sd, bd))
-            return false;
+        if (!make_map_box(&mM, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)Mm, dm, sm, bm)) return false;
+        CUtensorMap mDc[2];  // the map of each chunk width (a full chunk, the last one)
+        const int nrc[2] = {chunk_width(std::min(16, nrhs)), chunk_width(nrhs - (nrhs - 1) / 16 * 16)};
+        for (int q = 0; q < 2; q++) {
+            const uint32_t bd[4] = {2 * GV_COLS, (uint32_t)nrc[q], 1, 1};
+            if (!make_map_box(&mDc[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, (void*)dv, dd, sd, bd)) return false;
+        }
         P.begin(s);
         dim3 g((Nm + GV_ROWS - 1) / GV_ROWS, nb, nz_tma);
         for (int c0 = 0; c0 < nrhs; c0 += 16) {
-            if (nr == 8)
+            const bool last = c0 + 16 >= nrhs;
+            const int nr = nrc[last];
+            mD = mDc[last];
+            if (nr == 4)
+                k_cgemv32_tma<4><<<g, GV_THREADS, gv32_smem_bytes<4>(), s>>>(mM, mD, Nm, nrhs, c0, part, nb, err);
+            else if (nr == 8)
                 k_cgemv32_tma<8><<<g, GV_THREADS, gv32_smem_bytes<8>(), s>>>(mM, mD, Nm, nrhs, c0, part, nb, err);
             else if (nr == 10)
                 k_cgemv32_tma<10><<<g, GV_THREADS, gv32_smem_bytes<10>(), s>>>(mM, mD, Nm, nrhs, c0, part, nb, err);
@@ -422,6 +442,10 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                     k_tri_sweep<12><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
                 else if (nr_sweep == 16)
                     k_tri_sweep<16><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
+                else if (nr_sweep == 20)
+                    k_tri_sweep<20><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
+                else if (nr_sweep == 24)
+                    k_tri_sweep<24><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
                 else
                     k_tri_sweep<32><<<grid, TRI_THREADS, sm, s>>>(Np, MB, W, DINV, nrhs, xv, nb, up, tctrl, err);
                 (*launches)++;
@@ -534,7 +558,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             };
             auto diag = [&](const Half& h, int k0) {
                 P.begin(h.st);
-                k_diag_factor2<<<2 * h.nb, DF2_THREADS, dsmem, h.st>>>(W + (size_t)h.f0 * MB, Np, MB, k0,
+                k_diag_factor<<<2 * h.nb, DF_THREADS, dsmem, h.st>>>(W + (size_t)h.f0 * MB, Np, MB, k0,
                                                                   PL + (size_t)h.f0 * NBL * 2 * NBL,
                                                                   PU + (size_t)h.f0 * 4 * NBL * NBL,
                                                                   DINV + (size_t)h.f0 * nblk * NBL * NBL, err);

@@ -288,565 +288,366 @@ __global__ void __launch_bounds__(GEMM_THREADS, 1) k_gemm_tf32(const __grid_cons
     if (warp == 0) tc::tmem_dealloc(tmem, 2 * GBN);
 }
 
-// ---- diagonal block: M11 = L11 U11 (no pivoting) in shared memory, then L11^-1 and U11^-1.
-// One CTA of DF_THREADS per matrix.  Writes the factors back, L11^-1 as [Lr | Li] rows (the A operand
-// of GEMM2, [F][NBL][2 NBL]), U11^-1 in the block-real K-major form (the B operand of GEMM1,
-// [F][2 NBL][2 NBL]) and both inverses per block for the triangular solves.  A pivot of modulus
-// below 1e-30 sets err (the mixed form then reports the frequency; the FP64 form pivots).
-//
-// Blocked by 32 columns: per panel, all sixteen warps factor the 32 columns (a lane per column, rows
-// shared round-robin, one CTA barrier per pivot), then U12 = L_pp^-1 A12 by forward substitution (a
-// warp per column) and the trailing update A22 -= L21 U12.  After the panels, eight warps invert the
-// four 32 x 32 unit lower and four upper diagonal blocks at once (warp-synchronous, into a scratch),
-// and the inverses of the whole 128 x 128 factors are assembled from them in three block-column stages.
+// ---- the diagonal block: M11 = L11 U11 (no pivoting), then L11^-1 and U11^-1.  Two CTAs per matrix
+// (blockIdx.x = 2 f + side) factor the same block in their own shared memory; side 0 then forms L^-1
+// (and writes the factors back to W), side 1 U^-1.  Outputs: PL ([Lr | Li] rows of L^-1, the A operand
+// of GEMM2, [F][NBL][2 NBL]), PU (U^-1 in the block-real K-major form, the B operand of GEMM1,
+// [F][2 NBL][2 NBL]) and DINV (U^-1 on and above the diagonal, L^-1 below it, per block, for the
+// triangular solves).  A pivot of modulus below 1e-15 sets err (the mixed form then reports the
+// frequency; the FP64 form pivots).
 constexpr int DF_THREADS = 512, DF_LD = NBL + 1, DF_BLK = 32, DF_NB = NBL / DF_BLK, DF_SLD = DF_BLK + 1;
-constexpr size_t df_smem_bytes() { return (size_t)(NBL * DF_LD + 2 * DF_NB * DF_BLK * DF_SLD) * sizeof(float2); }
 
 __device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
+// complex multiply-adds as four FMA instructions (no separate product and sum)
 __device__ __forceinline__ void cfma_sub(float2& x, float2 a, float2 b) {  // x -= a b
-    x.x -= a.x * b.x - a.y * b.y;
-    x.y -= a.x * b.y + a.y * b.x;
+    x.x = fmaf(-a.x, b.x, x.x);
+    x.x = fmaf(a.y, b.y, x.x);
+    x.y = fmaf(-a.x, b.y, x.y);
+    x.y = fmaf(-a.y, b.x, x.y);
 }
 __device__ __forceinline__ void cfma_add(float2& x, float2 a, float2 b) {  // x += a b
-    x.x += a.x * b.x - a.y * b.y;
-    x.y += a.x * b.y + a.y * b.x;
+    x.x = fmaf(a.x, b.x, x.x);
+    x.x = fmaf(-a.y, b.y, x.x);
+    x.y = fmaf(a.x, b.y, x.y);
+    x.y = fmaf(a.y, b.x, x.y);
 }
 
-// sum_{kb <= k < ke} a(k) b(k) with four independent partial sums (short dependency chains: these
-// loops read their operands from shared memory and are latency-bound otherwise).
-template <class FA, class FB>
-__device__ __forceinline__ float2 cdot4(int kb, int ke, FA a, FB b) {
-    float2 s0 = make_float2(0.f, 0.f), s1 = s0, s2 = s0, s3 = s0;
-    int k = kb;
-    for (; k + 4 <= ke; k += 4) {
-        cfma_add(s0, a(k), b(k));
-        cfma_add(s1, a(k + 1), b(k + 1));
-        cfma_add(s2, a(k + 2), b(k + 2));
-        cfma_add(s3, a(k + 3), b(k + 3));
+// LU by 16-column panels: the 16 x 16 diagonal block by one warp in registers (lane = row, the pivot
+// row published through shared memory, no CTA barrier per pivot), then L21 = A21 U11^-1 (a lane per
+// row) and U12 = L11^-1 A12 (a lane per column) by independent substitutions, then A22 -= L21 U12 by
+// all warps in register tiles.  Inverses: the eight 16 x 16 diagonal blocks inverted in registers and
+// put in place, then the off-diagonal blocks by the block recursion inv([[A, 0], [C, B]]) =
+// [[A^-1, 0], [-B^-1 C A^-1, B^-1]] (16 -> 32 -> 64 -> 128; for U the transposed pattern), each level
+// two products of block-triangular operands through a shared scratch.  (Fully unrolled code run by a
+// single warp, and per-pivot shuffles, were measured slower than these short register recursions.)
+constexpr int DF3_TLD = 2 * DF_BLK + 1, DF3_P = 16;  // DF3_P: LU panel width
+constexpr int DF3_TSZ = DF_NB * DF_BLK * DF_SLD;  // the scratch: 4 blocks of 32 x DF_SLD (>= 64 x DF3_TLD)
+static_assert(DF3_TSZ >= 2 * DF_BLK * DF3_TLD, "scratch holds the 64 x 64 product");
+constexpr size_t df_smem_bytes() { return (size_t)(NBL * DF_LD + DF3_TSZ + NBL) * sizeof(float2); }
+
+__device__ __forceinline__ float2 crecip(float2 d) {  // 1 / d by one reciprocal of |d|^2
+    const float r = __frcp_rn(d.x * d.x + d.y * d.y);
+    return make_float2(d.x * r, -d.y * r);
+}
+
+// A22 -= L21 U12 over rows and columns b0 .. NBL - 1 (n2 = NBL - b0 = 16 TR = 32 TC), k over the panel
+// c0 .. c0 + 31: warp w the rows b0 + 16 a + w, lane the columns b0 + 32 b + lane.
+template <int TR, int TC>
+__device__ __forceinline__ void df3_trailing(float2* blk, int c0, int b0) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float2 acc[TR][TC];
+#pragma unroll
+    for (int a = 0; a < TR; a++)
+#pragma unroll
+        for (int b = 0; b < TC; b++) acc[a][b] = make_float2(0.f, 0.f);
+#pragma unroll 4
+    for (int k = 0; k < DF3_P; k++) {
+        float2 l[TR], u[TC];
+#pragma unroll
+        for (int a = 0; a < TR; a++) l[a] = blk[(b0 + 16 * a + warp) * DF_LD + c0 + k];
+#pragma unroll
+        for (int b = 0; b < TC; b++) u[b] = blk[(c0 + k) * DF_LD + min(b0 + 32 * b + lane, NBL - 1)];
+#pragma unroll
+        for (int a = 0; a < TR; a++)
+#pragma unroll
+            for (int b = 0; b < TC; b++) cfma_add(acc[a][b], l[a], u[b]);
     }
-    for (; k < ke; k++) cfma_add(s0, a(k), b(k));
-    return make_float2((s0.x + s1.x) + (s2.x + s3.x), (s0.y + s1.y) + (s2.y + s3.y));
+#pragma unroll
+    for (int a = 0; a < TR; a++)
+#pragma unroll
+        for (int b = 0; b < TC; b++)
+            if (b0 + 32 * b + lane < NBL) {
+                float2& x = blk[(b0 + 16 * a + warp) * DF_LD + b0 + 32 * b + lane];
+                x = make_float2(x.x - acc[a][b].x, x.y - acc[a][b].y);
+            }
 }
 
-// Warp-synchronous inverse of the 32 x 32 upper block U (diagonal included) at A (leading
-// dimension DF_LD) into X (leading dimension DF_SLD): X U = I, column by column, lane i owns row i.
-__device__ __forceinline__ void df_inv_upper32(const float2* A, float2* X) {
-    const int i = threadIdx.x & 31;
-    for (int j = 0; j < DF_BLK; j++) {
-        const float2 d = A[j * DF_LD + j];
-        const float dd = d.x * d.x + d.y * d.y;
-        const float2 inv = make_float2(d.x / dd, -d.y / dd);
-        float2 t = make_float2(0.f, 0.f);
-        if (i < j)  // X(i, j) = -(sum_{i <= k < j} X(i, k) U(k, j)) / U(j, j)
-            t = cdot4(i, j, [&](int k) { return X[i * DF_SLD + k]; }, [&](int k) { return A[k * DF_LD + j]; });
+// Step J of a 16 x 16 LU by lanes 0..15 of a warp (lane = row, a = the lane's row; lanes 16..31 hold
+// zeros): the pivot row published through shared memory (row, 16 entries), rcp[J] = 1 / U(J, J), ok
+// false on a pivot of modulus below 1e-15.  Recursion keeps every register index constant; no
+// branch around the updates (lanes at or above the pivot subtract zero).
+template <int J>
+__device__ __forceinline__ void df3_lu16_step(float2 (&a)[DF3_P], int lane, float2* row, float2* rcp, bool& ok) {
+    if constexpr (J < DF3_P) {
+        if (lane == J)
+#pragma unroll
+            for (int k = J; k < DF3_P; k++) row[k] = a[k];
         __syncwarp();
-        if (i < j) X[i * DF_SLD + j] = make_float2(-(t.x * inv.x - t.y * inv.y), -(t.x * inv.y + t.y * inv.x));
-        if (i == j) X[j * DF_SLD + j] = inv;
-        if (i > j) X[i * DF_SLD + j] = make_float2(0.f, 0.f);
+        const float2 d = row[J];
+        ok = ok && d.x * d.x + d.y * d.y > 1e-30f;
+        const float2 inv = crecip(d);
+        if (lane == 0) rcp[J] = inv;
+        const float2 l = cmulf(a[J], inv);
+        const float2 lm = lane > J ? l : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int k = J + 1; k < DF3_P; k++) cfma_sub(a[k], lm, row[k]);
+        if (lane > J) a[J] = l;
         __syncwarp();
+        df3_lu16_step<J + 1>(a, lane, row, rcp, ok);
     }
 }
 
-// Warp-synchronous inverse of the 32 x 32 unit lower block L at A into X: Y L = I from the last
-// column, Y(i, j) = -sum_{j < k <= i} Y(i, k) L(k, j) for i > j.
-__device__ __forceinline__ void df_inv_lower32(const float2* A, float2* X) {
-    const int i = threadIdx.x & 31;
-    for (int j = DF_BLK - 1; j >= 0; j--) {
-        float2 t = make_float2(0.f, 0.f);
-        if (i > j) {
-            const float2 a = A[i * DF_LD + j];  // k = i: Y(i, i) = 1
-            t = cdot4(j + 1, i, [&](int k) { return X[i * DF_SLD + k]; }, [&](int k) { return A[k * DF_LD + j]; });
-            t.x += a.x;
-            t.y += a.y;
+// x = x U^-1 for the upper 16 x 16 block at Ub (leading dimension DF_LD; rcp[k] = 1 / U(k, k)): step K
+// finishes x[K] and removes it from the later unknowns.
+template <int K>
+__device__ __forceinline__ void df3_urow16_step(float2 (&x)[DF3_P], const float2* Ub, const float2* rcp) {
+    if constexpr (K < DF3_P) {
+        x[K] = cmulf(x[K], rcp[K]);
+#pragma unroll
+        for (int j = K + 1; j < DF3_P; j++) cfma_sub(x[j], x[K], Ub[K * DF_LD + j]);
+        df3_urow16_step<K + 1>(x, Ub, rcp);
+    }
+}
+
+// x = x L^-1 for the unit lower 16 x 16 block at Lb, from the last column: step K (x[K] final) removes
+// x[K] from the earlier unknowns.
+template <int K>
+__device__ __forceinline__ void df3_lrow16_back_step(float2 (&x)[DF3_P], const float2* Lb) {
+    if constexpr (K > 0) {
+#pragma unroll
+        for (int j = 0; j < K; j++) cfma_sub(x[j], x[K], Lb[K * DF_LD + j]);
+        df3_lrow16_back_step<K - 1>(x, Lb);
+    }
+}
+
+// y = L^-1 y for the unit lower 16 x 16 block at Lb, step K removing y[K] from the later unknowns.
+template <int K>
+__device__ __forceinline__ void df3_lcol16_step(float2 (&y)[DF3_P], const float2* Lb) {
+    if constexpr (K < DF3_P - 1) {
+#pragma unroll
+        for (int j = K + 1; j < DF3_P; j++) cfma_sub(y[j], Lb[j * DF_LD + K], y[K]);
+        df3_lcol16_step<K + 1>(y, Lb);
+    }
+}
+
+// Block-triangular operand patterns of df3_product (block = 32 x 32): which k of the sum are nonzero
+// for the output tile in block row ib, block column jb of C.
+enum Df3Tri { DF3_B_LOWER, DF3_A_LOWER, DF3_B_UPPER, DF3_A_UPPER };
+
+// C(m x m) = sgn A(m x m) B(m x m), m = 32 or 64, A and B of leading dimensions lda, ldb, C of ldc;
+// threads tid0 .. tid0 + nthr - 1, each a 2 x 2 tile: rows 2 ri + {0, 1}, columns cj + {0, 16} of a
+// 32 x 32 output block (consecutive lanes read consecutive columns of B).
+__device__ __forceinline__ void df3_product(const float2* A, int lda, const float2* B, int ldb, float2* C, int ldc,
+                                            int m, Df3Tri tri, float sgn, int tid, int nthr) {
+    const int nbk = m / DF_BLK, tiles = nbk * nbk * 256;
+    for (int t = tid; t < tiles; t += nthr) {
+        const int blkid = t / 256, w = t % 256, ib = blkid / nbk, jb = blkid % nbk;
+        const int i0 = ib * DF_BLK + 2 * (w / 16), j0 = jb * DF_BLK + (w % 16);
+        int klo = 0, khi = m;
+        if (tri == DF3_B_LOWER) klo = jb * DF_BLK;
+        if (tri == DF3_A_LOWER) khi = (ib + 1) * DF_BLK;
+        if (tri == DF3_B_UPPER) khi = (jb + 1) * DF_BLK;
+        if (tri == DF3_A_UPPER) klo = ib * DF_BLK;
+        float2 c00 = make_float2(0.f, 0.f), c01 = c00, c10 = c00, c11 = c00;
+#pragma unroll 4
+        for (int k = klo; k < khi; k++) {
+            const float2 a0 = A[i0 * lda + k], a1 = A[(i0 + 1) * lda + k];
+            const float2 b0 = B[k * ldb + j0], b1 = B[k * ldb + j0 + 16];
+            cfma_add(c00, a0, b0);
+            cfma_add(c01, a0, b1);
+            cfma_add(c10, a1, b0);
+            cfma_add(c11, a1, b1);
         }
-        __syncwarp();
-        if (i > j) X[i * DF_SLD + j] = make_float2(-t.x, -t.y);
-        if (i == j) X[j * DF_SLD + j] = make_float2(1.f, 0.f);
-        if (i < j) X[i * DF_SLD + j] = make_float2(0.f, 0.f);
-        __syncwarp();
+        C[i0 * ldc + j0] = make_float2(sgn * c00.x, sgn * c00.y);
+        C[i0 * ldc + j0 + 16] = make_float2(sgn * c01.x, sgn * c01.y);
+        C[(i0 + 1) * ldc + j0] = make_float2(sgn * c10.x, sgn * c10.y);
+        C[(i0 + 1) * ldc + j0 + 16] = make_float2(sgn * c11.x, sgn * c11.y);
     }
 }
 
 __global__ void __launch_bounds__(DF_THREADS) k_diag_factor(float* __restrict__ W, int Np, size_t bstride, int k0,
-                                                            float* __restrict__ PL, float* __restrict__ PU,
-                                                            float2* __restrict__ DINV, int* __restrict__ err) {
-    extern __shared__ float2 df_smem[];
-    float2* blk = df_smem;                    // [NBL][DF_LD]
-    float2* Li = blk + NBL * DF_LD;           // [DF_NB][DF_BLK][DF_SLD]: inverses of the diagonal L blocks
-    float2* Ui = Li + DF_NB * DF_BLK * DF_SLD;  // the same for U
-    const int f = blockIdx.x;
-    float* Wr = W + (size_t)f * bstride;
-    float* Wi = Wr + (size_t)Np * Np;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) {
-        const int r = t / NBL, c = t % NBL;
-        const size_t o = (size_t)(k0 + r) * Np + k0 + c;
-        blk[r * DF_LD + c] = make_float2(Wr[o], Wi[o]);
-    }
-    __syncthreads();
-    for (int pb = 0; pb < DF_NB; pb++) {
-        const int c0 = pb * DF_BLK;
-        // ---- panel: columns c0 .. c0 + 31, rows c0 .. NBL - 1; lane = column, warp w owns rows
-        // c0 + w + DF_WARPS q (a few rows a warp, one CTA barrier per pivot)
-        constexpr int DF_WARPS = DF_THREADS / 32;
-        for (int j = 0; j < DF_BLK; j++) {
-            const int c = c0 + j;
-            __syncthreads();  // row c is final
-            const float2 d = blk[c * DF_LD + c];
-            const float dd = d.x * d.x + d.y * d.y;
-            if (threadIdx.x == 0 && !(dd > 1e-30f)) atomicExch(err, 10);
-            const float2 inv = make_float2(d.x / dd, -d.y / dd);
-            const float2 u = blk[c * DF_LD + c0 + lane];
-            int r = c + 1 + (((c0 + warp - (c + 1)) % DF_WARPS) + DF_WARPS) % DF_WARPS;
-            for (; r < NBL; r += DF_WARPS) {
-                const float2 l = cmulf(blk[r * DF_LD + c], inv);
-                if (lane > j) cfma_sub(blk[r * DF_LD + c0 + lane], l, u);
-                __syncwarp();
-                if (lane == j) blk[r * DF_LD + c] = l;
-            }
-        }
-        __syncthreads();
-        const int n2 = NBL - c0 - DF_BLK;
-        if (n2 == 0) break;
-        // ---- U12 = L_pp^-1 A12 (rows c0 .. c0 + 31, columns c0 + 32 ..) by forward substitution with the
-        // unit lower L_pp: a warp per column, lane = row, the lane's row of L_pp in registers, each solved
-        // entry broadcast by shuffles
-        {
-            float2 lrow[DF_BLK];
-#pragma unroll
-            for (int j = 0; j < DF_BLK; j++)
-                lrow[j] = j < lane ? blk[(c0 + lane) * DF_LD + c0 + j] : make_float2(0.f, 0.f);
-            for (int cc = c0 + DF_BLK + warp; cc < NBL; cc += DF_WARPS) {
-                float2 v = blk[(c0 + lane) * DF_LD + cc];
-#pragma unroll
-                for (int j = 0; j < DF_BLK - 1; j++) {
-                    const float2 xj = make_float2(__shfl_sync(0xffffffffu, v.x, j), __shfl_sync(0xffffffffu, v.y, j));
-                    cfma_sub(v, lrow[j], xj);  // lrow[j] = 0 for j >= lane
-                }
-                blk[(c0 + lane) * DF_LD + cc] = v;
-            }
-            __syncthreads();
-        }
-        // ---- trailing update A22 -= L21 U12
-        for (int t = threadIdx.x; t < n2 * n2; t += DF_THREADS) {
-            const int r = c0 + DF_BLK + t / n2, cc = c0 + DF_BLK + t % n2;
-            float2 a = blk[r * DF_LD + cc];
-            const float2 p = cdot4(0, DF_BLK, [&](int k) { return blk[r * DF_LD + c0 + k]; },
-                                   [&](int k) { return blk[(c0 + k) * DF_LD + cc]; });
-            blk[r * DF_LD + cc] = make_float2(a.x - p.x, a.y - p.y);
-        }
-        __syncthreads();
-    }
-    // ---- inverses of the four 32 x 32 diagonal blocks of L and of U: eight warps, one block each
-    if (warp < DF_NB)
-        df_inv_lower32(blk + warp * DF_BLK * DF_LD + warp * DF_BLK, Li + warp * DF_BLK * DF_SLD);
-    else if (warp < 2 * DF_NB)
-        df_inv_upper32(blk + (warp - DF_NB) * DF_BLK * DF_LD + (warp - DF_NB) * DF_BLK,
-                       Ui + (warp - DF_NB) * DF_BLK * DF_SLD);
-    // the factors back to W
-    for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) {
-        const int r = t / NBL, c = t % NBL;
-        const size_t o = (size_t)(k0 + r) * Np + k0 + c;
-        Wr[o] = blk[r * DF_LD + c].x;
-        Wi[o] = blk[r * DF_LD + c].y;
-    }
-    __syncthreads();
-    // ---- the off-diagonal blocks of U^-1 (threads 0..255) and L^-1 (threads 256..511), in place in
-    // blk, one block column per stage: U^-1(I, J) = -(sum_{I <= K < J} X(I, K) U(K, J)) X(J, J) for
-    // J = 1, 2, 3; L^-1(I, J) = -(sum_{J < K <= I} Y(I, K) L(K, J)) Y(J, J) for J = 2, 1, 0.
-    // X(I, K) / Y(I, K) are diagonal-block inverses (scratch) or blocks of earlier stages (blk).
-    const bool upper = threadIdx.x < DF_THREADS / 2;
-    const int tu = threadIdx.x % (DF_THREADS / 2);
-    for (int st = 1; st < DF_NB; st++) {
-        const int J = upper ? st : DF_NB - 1 - st;
-        const int nI = st;  // blocks I of this column: I < J (upper) or I > J (lower)
-        constexpr int MAXE = (DF_NB - 1) * DF_BLK * DF_BLK / (DF_THREADS / 2);  // 12
-        float2 v[MAXE];
-        // T(I, J) = sum_K X(I, K) U(K, J)
-#pragma unroll
-        for (int e = 0; e < MAXE; e++) {
-            const int t = tu + e * (DF_THREADS / 2);
-            v[e] = make_float2(0.f, 0.f);
-            if (t < nI * DF_BLK * DF_BLK) {
-                const int bi = t / (DF_BLK * DF_BLK), i = (t / DF_BLK) % DF_BLK, j = t % DF_BLK;
-                const int I = upper ? bi : J + 1 + bi;
-                const int row = I * DF_BLK + i, col = J * DF_BLK + j;
-                float2 a = make_float2(0.f, 0.f);
-                const int Kb = upper ? I : J + 1, Ke = upper ? J - 1 : I;
-                for (int K = Kb; K <= Ke; K++) {
-                    const float2* Xd = (upper ? Ui : Li) + K * DF_BLK * DF_SLD;  // X(K, K) when K == I
-                    const float2 p = cdot4(
-                        0, DF_BLK,
-                        [&](int k) { return (K == I) ? Xd[i * DF_SLD + k] : blk[row * DF_LD + K * DF_BLK + k]; },
-                        [&](int k) { return blk[(K * DF_BLK + k) * DF_LD + col]; });
-                    a.x += p.x;
-                    a.y += p.y;
-                }
-                v[e] = a;
-            }
-        }
-        __syncthreads();
-        // X(I, J) = -T(I, J) X(J, J): T staged in blk (block (I, J)), then the product back
-#pragma unroll
-        for (int e = 0; e < MAXE; e++) {
-            const int t = tu + e * (DF_THREADS / 2);
-            if (t < nI * DF_BLK * DF_BLK) {
-                const int bi = t / (DF_BLK * DF_BLK), i = (t / DF_BLK) % DF_BLK, j = t % DF_BLK;
-                const int I = upper ? bi : J + 1 + bi;
-                blk[(I * DF_BLK + i) * DF_LD + J * DF_BLK + j] = v[e];
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int e = 0; e < MAXE; e++) {
-            const int t = tu + e * (DF_THREADS / 2);
-            if (t < nI * DF_BLK * DF_BLK) {
-                const int bi = t / (DF_BLK * DF_BLK), i = (t / DF_BLK) % DF_BLK, j = t % DF_BLK;
-                const int I = upper ? bi : J + 1 + bi;
-                const float2* Xj = (upper ? Ui : Li) + J * DF_BLK * DF_SLD;
-                const float2 a = cdot4(0, DF_BLK, [&](int k) { return blk[(I * DF_BLK + i) * DF_LD + J * DF_BLK + k]; },
-                                       [&](int k) { return Xj[k * DF_SLD + j]; });
-                v[e] = make_float2(-a.x, -a.y);
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int e = 0; e < MAXE; e++) {
-            const int t = tu + e * (DF_THREADS / 2);
-            if (t < nI * DF_BLK * DF_BLK) {
-                const int bi = t / (DF_BLK * DF_BLK), i = (t / DF_BLK) % DF_BLK, j = t % DF_BLK;
-                const int I = upper ? bi : J + 1 + bi;
-                blk[(I * DF_BLK + i) * DF_LD + J * DF_BLK + j] = v[e];
-            }
-        }
-        __syncthreads();
-    }
-    // inverse entry (i, c): U^-1 for i <= c, L^-1 (unit diagonal) for i > c
-    auto inv_at = [&](int i, int c) -> float2 {
-        const int bi = i / DF_BLK, bc = c / DF_BLK;
-        if (bi == bc) {
-            const float2* X = (i <= c ? Ui : Li) + bi * DF_BLK * DF_SLD;
-            return X[(i % DF_BLK) * DF_SLD + c % DF_BLK];
-        }
-        return blk[i * DF_LD + c];
-    };
-    {
-        float2* D = DINV + ((size_t)f * (Np / NBL) + k0 / NBL) * NBL * NBL;
-        for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) D[t] = inv_at(t / NBL, t % NBL);
-    }
-    float* PLf = PL + (size_t)f * NBL * 2 * NBL;
-    float* PUf = PU + (size_t)f * 2 * NBL * 2 * NBL;
-    for (int t = threadIdx.x; t < NBL * NBL; t += blockDim.x) {
-        {  // [Lr | Li] rows of L^-1 (c fastest: coalesced)
-            const int i = t / NBL, c = t % NBL;
-            const float2 l = i > c ? inv_at(i, c) : make_float2(i == c ? 1.f : 0.f, 0.f);
-            PLf[(size_t)i * 2 * NBL + c] = l.x;
-            PLf[(size_t)i * 2 * NBL + NBL + c] = l.y;
-        }
-        {  // U^-1 block-real K-major (i fastest: coalesced): row c: [Ur(:, c); -Ui(:, c)], row NBL + c: [Ui(:, c); Ur(:, c)]
-            const int c = t / NBL, i = t % NBL;
-            const float2 u = i <= c ? inv_at(i, c) : make_float2(0.f, 0.f);  // U^-1(i, c)
-            PUf[(size_t)c * 2 * NBL + i] = u.x;
-            PUf[(size_t)c * 2 * NBL + NBL + i] = -u.y;
-            PUf[(size_t)(NBL + c) * 2 * NBL + i] = u.y;
-            PUf[(size_t)(NBL + c) * 2 * NBL + NBL + i] = u.x;
-        }
-    }
-}
-
-// Two CTAs per matrix (blockIdx.x = 2 f + side), each factoring the same 128 x 128 diagonal block of
-// M = A^T in its own shared memory (M = L U, no pivoting), then side 0 forms L^-1 (and writes the
-// factors back to W) and side 1 forms U^-1: the inverses, as much work as the factorization, run on two
-// SMs at once.  Outputs as k_diag_factor's: PL ([Lr | Li] rows of L^-1), PU (U^-1 block-real K-major),
-// DINV (U^-1 on and above the diagonal, L^-1 below it).
-//
-// The factorization, blocked by 32 columns: the panel's rows are held in registers (warp w the rows
-// c0 + w + 16 q, lane the column), each pivot row published through shared memory with one CTA barrier
-// a column; U12 = L_pp^-1 A12 by forward substitution (a warp per column); the trailing update A22 -=
-// L21 U12 in 4 x 4 register tiles.  The inverses: the four 32 x 32 diagonal blocks by one warp each
-// (a lane per row, the row in registers), then the off-diagonal blocks block column by block column
-// (U^-1(I, J) = -(sum_{I <= K < J} X(I, K) U(K, J)) X(J, J); L^-1(I, J) = -(sum_{J < K <= I} Y(I, K)
-// L(K, J)) Y(J, J)) in 2 x 2 register tiles.
-constexpr int DF2_THREADS = 512;
-constexpr size_t df2_smem_bytes() {
-    return (size_t)(NBL * DF_LD + DF_NB * DF_BLK * DF_SLD + 2 * DF_BLK) * sizeof(float2);
-}
-
-// Y = L^-1 of the unit lower 32 x 32 block at A (leading dimension DF_LD) into X (DF_SLD): lane i holds
-// row i of Y, the columns from the last: Y(i, j) = -sum_{j < k <= i} Y(i, k) L(k, j).
-__device__ __forceinline__ void df2_inv_lower32(const float2* A, float2* X) {
-    const int i = threadIdx.x & 31;
-    float2 y[DF_BLK];
-#pragma unroll
-    for (int k = 0; k < DF_BLK; k++) y[k] = make_float2(k == i ? 1.f : 0.f, 0.f);
-#pragma unroll
-    for (int j = DF_BLK - 2; j >= 0; j--) {
-        float2 t = make_float2(0.f, 0.f);
-#pragma unroll
-        for (int k = j + 1; k < DF_BLK; k++) cfma_add(t, y[k], A[k * DF_LD + j]);  // y[k] = 0 for k > i
-        if (i > j) y[j] = make_float2(-t.x, -t.y);
-    }
-#pragma unroll
-    for (int k = 0; k < DF_BLK; k++) X[i * DF_SLD + k] = y[k];
-}
-
-// X = U^-1 of the upper 32 x 32 block at A into X: lane i holds row i of X, the columns from the
-// first: X(i, j) = (delta_ij - sum_{i <= k < j} X(i, k) U(k, j)) / U(j, j).
-__device__ __forceinline__ void df2_inv_upper32(const float2* A, float2* X) {
-    const int i = threadIdx.x & 31;
-    float2 x[DF_BLK];
-#pragma unroll
-    for (int j = 0; j < DF_BLK; j++) {
-        float2 t = make_float2(j == i ? 1.f : 0.f, 0.f);
-#pragma unroll
-        for (int k = 0; k < j; k++) cfma_sub(t, x[k], A[k * DF_LD + j]);  // x[k] = 0 for k < i
-        const float2 d = A[j * DF_LD + j];
-        const float dd = d.x * d.x + d.y * d.y;
-        const float2 inv = make_float2(d.x / dd, -d.y / dd);
-        x[j] = j < i ? make_float2(0.f, 0.f) : cmulf(t, inv);
-    }
-#pragma unroll
-    for (int k = 0; k < DF_BLK; k++) X[i * DF_SLD + k] = x[k];
-}
-
-__global__ void __launch_bounds__(DF2_THREADS) k_diag_factor2(float* __restrict__ W, int Np, size_t bstride, int k0,
                                                               float* __restrict__ PL, float* __restrict__ PU,
                                                               float2* __restrict__ DINV, int* __restrict__ err) {
     extern __shared__ float2 df_smem[];
-    float2* blk = df_smem;                        // [NBL][DF_LD]
-    float2* Xd = blk + NBL * DF_LD;               // [DF_NB][DF_BLK][DF_SLD]: this side's diagonal-block inverses
-    float2* prow = Xd + DF_NB * DF_BLK * DF_SLD;  // [2][DF_BLK]: the published pivot rows
+    float2* blk = df_smem;                   // [NBL][DF_LD]: the block, then its factors, then the inverse
+    float2* T = blk + NBL * DF_LD;  // scratch: the diagonal-block inverses, then the products of the recursion
+    float2* rcp = T + DF3_TSZ;      // [NBL]: 1 / U(j, j)
     const int f = blockIdx.x >> 1, side = blockIdx.x & 1;
+    const bool upper = side == 1;
     float* Wr = W + (size_t)f * bstride;
     float* Wi = Wr + (size_t)Np * Np;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int NWARP = DF2_THREADS / 32;  // 16
-    for (int t = threadIdx.x; t < NBL * NBL; t += DF2_THREADS) {
-        const int r = t / NBL, c = t % NBL;
+    // the block in 16-byte loads (rows of 128 entries, k0 and Np multiples of 128), 16 in flight a thread
+#pragma unroll 8
+    for (int t = threadIdx.x; t < NBL * NBL / 4; t += DF_THREADS) {
+        const int r = t / (NBL / 4), c = 4 * (t % (NBL / 4));
         const size_t o = (size_t)(k0 + r) * Np + k0 + c;
-        blk[r * DF_LD + c] = make_float2(Wr[o], Wi[o]);
+        const float4 re = *reinterpret_cast<const float4*>(Wr + o), im = *reinterpret_cast<const float4*>(Wi + o);
+        float2* d = blk + r * DF_LD + c;
+        d[0] = make_float2(re.x, im.x);
+        d[1] = make_float2(re.y, im.y);
+        d[2] = make_float2(re.z, im.z);
+        d[3] = make_float2(re.w, im.w);
     }
     __syncthreads();
-    for (int pb = 0; pb < DF_NB; pb++) {
-        const int c0 = pb * DF_BLK;
-        // ---- panel: rows c0 .. NBL - 1 of columns c0 .. c0 + 31 in registers
-        float2 v[NBL / NWARP];
+#pragma unroll 1
+    for (int pb = 0; pb < NBL / DF3_P; pb++) {
+        const int c0 = pb * DF3_P, b0 = c0 + DF3_P, n2 = NBL - b0;
+        if (warp == 0) {  // the 16 x 16 diagonal block: lane = row (lanes 16..31 carry zeros, write nothing)
+            float2* P = blk + c0 * DF_LD + c0;
+            float2 a[DF3_P];
 #pragma unroll
-        for (int q = 0; q < NBL / NWARP; q++) {
-            const int r = c0 + warp + NWARP * q;
-            v[q] = r < NBL ? blk[r * DF_LD + c0 + lane] : make_float2(0.f, 0.f);
-        }
-        if (warp == 0) prow[lane] = v[0];
-        for (int j = 0; j < DF_BLK; j++) {
-            const int c = c0 + j;
-            __syncthreads();  // pivot row c published in prow[j & 1]
-            const float2 u = prow[(j & 1) * DF_BLK + lane];
-            const float2 d = prow[(j & 1) * DF_BLK + j];
-            const float dd = d.x * d.x + d.y * d.y;
-            if (threadIdx.x == 0 && !(dd > 1e-30f)) atomicExch(err, 10);
-            const float2 inv = make_float2(d.x / dd, -d.y / dd);
+            for (int k = 0; k < DF3_P; k++) a[k] = lane < DF3_P ? P[lane * DF_LD + k] : make_float2(0.f, 0.f);
+            bool ok = true;
+            df3_lu16_step<0>(a, lane, T, rcp + c0, ok);
+            if (lane == 0 && !ok) atomicExch(err, 10);
+            if (lane < DF3_P)
 #pragma unroll
-            for (int q = 0; q < NBL / NWARP; q++) {
-                const int r = c0 + warp + NWARP * q;
-                if (r > c && r < NBL) {  // warp-uniform
-                    const float2 a = make_float2(__shfl_sync(0xffffffffu, v[q].x, j), __shfl_sync(0xffffffffu, v[q].y, j));
-                    const float2 l = cmulf(a, inv);
-                    if (lane == j) v[q] = l;
-                    if (lane > j) cfma_sub(v[q], l, u);
-                }
-            }
-            if (j + 1 < DF_BLK && warp == (j + 1) % NWARP)  // row c + 1 is final: publish it
-                prow[((j + 1) & 1) * DF_BLK + lane] = ((j + 1) / NWARP) ? v[1] : v[0];
-        }
-#pragma unroll
-        for (int q = 0; q < NBL / NWARP; q++) {
-            const int r = c0 + warp + NWARP * q;
-            if (r < NBL) blk[r * DF_LD + c0 + lane] = v[q];
+                for (int k = 0; k < DF3_P; k++) P[lane * DF_LD + k] = a[k];
         }
         __syncthreads();
-        const int n2 = NBL - c0 - DF_BLK;
         if (n2 == 0) break;
-        // ---- U12 = L_pp^-1 A12: a warp per column, lane = row, the lane's row of L_pp in registers
-        {
-            float2 lrow[DF_BLK];
+        const int nw = (n2 + 31) / 32;  // warps of each substitution
+        if (warp >= 1 && warp <= nw) {  // L21 = A21 U11^-1: lane = row
+            const int i = b0 + 32 * (warp - 1) + lane;
+            if (i < NBL) {
+                float2 x[DF3_P];
 #pragma unroll
-            for (int j = 0; j < DF_BLK; j++)
-                lrow[j] = j < lane ? blk[(c0 + lane) * DF_LD + c0 + j] : make_float2(0.f, 0.f);
-            for (int cc = c0 + DF_BLK + warp; cc < NBL; cc += NWARP) {
-                float2 x = blk[(c0 + lane) * DF_LD + cc];
+                for (int k = 0; k < DF3_P; k++) x[k] = blk[i * DF_LD + c0 + k];
+                df3_urow16_step<0>(x, blk + c0 * DF_LD + c0, rcp + c0);
 #pragma unroll
-                for (int j = 0; j < DF_BLK - 1; j++) {
-                    const float2 xj = make_float2(__shfl_sync(0xffffffffu, x.x, j), __shfl_sync(0xffffffffu, x.y, j));
-                    cfma_sub(x, lrow[j], xj);  // lrow[j] = 0 for j >= lane
-                }
-                blk[(c0 + lane) * DF_LD + cc] = x;
+                for (int k = 0; k < DF3_P; k++) blk[i * DF_LD + c0 + k] = x[k];
+            }
+        } else if (warp >= 5 && warp < 5 + nw) {  // U12 = L11^-1 A12: lane = column
+            const int cc = b0 + 32 * (warp - 5) + lane;
+            if (cc < NBL) {
+                float2 y[DF3_P];
+#pragma unroll
+                for (int k = 0; k < DF3_P; k++) y[k] = blk[(c0 + k) * DF_LD + cc];
+                df3_lcol16_step<0>(y, blk + c0 * DF_LD + c0);
+#pragma unroll
+                for (int k = 0; k < DF3_P; k++) blk[(c0 + k) * DF_LD + cc] = y[k];
             }
         }
         __syncthreads();
-        // ---- A22 -= L21 U12 in 4 x 4 tiles
-        {
-            const int tc = n2 / 4, ntile = tc * tc, b0 = c0 + DF_BLK;
-            for (int t = threadIdx.x; t < ntile; t += DF2_THREADS) {
-                const int rb = b0 + 4 * (t / tc), cb = b0 + 4 * (t % tc);
-                float2 acc[4][4];
-#pragma unroll
-                for (int a = 0; a < 4; a++)
-#pragma unroll
-                    for (int b = 0; b < 4; b++) acc[a][b] = make_float2(0.f, 0.f);
-#pragma unroll 4
-                for (int k = 0; k < DF_BLK; k++) {
-                    float2 av[4], bv[4];
-#pragma unroll
-                    for (int a = 0; a < 4; a++) av[a] = blk[(rb + a) * DF_LD + c0 + k];
-#pragma unroll
-                    for (int b = 0; b < 4; b++) bv[b] = blk[(c0 + k) * DF_LD + cb + b];
-#pragma unroll
-                    for (int a = 0; a < 4; a++)
-#pragma unroll
-                        for (int b = 0; b < 4; b++) cfma_add(acc[a][b], av[a], bv[b]);
-                }
-#pragma unroll
-                for (int a = 0; a < 4; a++)
-#pragma unroll
-                    for (int b = 0; b < 4; b++) {
-                        float2& x = blk[(rb + a) * DF_LD + cb + b];
-                        x = make_float2(x.x - acc[a][b].x, x.y - acc[a][b].y);
-                    }
-            }
+        switch (n2 / DF3_P) {  // A22 -= L21 U12 (k over the 16 panel columns)
+            case 7: df3_trailing<7, 4>(blk, c0, b0); break;
+            case 6: df3_trailing<6, 3>(blk, c0, b0); break;
+            case 5: df3_trailing<5, 3>(blk, c0, b0); break;
+            case 4: df3_trailing<4, 2>(blk, c0, b0); break;
+            case 3: df3_trailing<3, 2>(blk, c0, b0); break;
+            case 2: df3_trailing<2, 1>(blk, c0, b0); break;
+            default: df3_trailing<1, 1>(blk, c0, b0); break;
         }
         __syncthreads();
     }
-    // ---- the factors back to W (side 0), the diagonal-block inverses of this side's triangle
+    // ---- the factors back to W (side 0)
     if (side == 0)
-        for (int t = threadIdx.x; t < NBL * NBL; t += DF2_THREADS) {
-            const int r = t / NBL, c = t % NBL;
+#pragma unroll 8
+        for (int t = threadIdx.x; t < NBL * NBL / 4; t += DF_THREADS) {
+            const int r = t / (NBL / 4), c = 4 * (t % (NBL / 4));
             const size_t o = (size_t)(k0 + r) * Np + k0 + c;
-            Wr[o] = blk[r * DF_LD + c].x;
-            Wi[o] = blk[r * DF_LD + c].y;
+            const float2* d = blk + r * DF_LD + c;
+            *reinterpret_cast<float4*>(Wr + o) = make_float4(d[0].x, d[1].x, d[2].x, d[3].x);
+            *reinterpret_cast<float4*>(Wi + o) = make_float4(d[0].y, d[1].y, d[2].y, d[3].y);
         }
-    if (warp < DF_NB) {
-        const float2* Ab = blk + warp * DF_BLK * DF_LD + warp * DF_BLK;
-        if (side == 0)
-            df2_inv_lower32(Ab, Xd + warp * DF_BLK * DF_SLD);
+    __syncthreads();
+    // ---- the inverse of this side's factor, in place in blk
+    // the eight 16 x 16 diagonal blocks (warp w: block w, lane = row of its inverse, in registers)
+    constexpr int P = DF3_P, PL16 = DF3_P + 1;
+    if (warp < NBL / P) {
+        const float2* Ab = blk + warp * P * DF_LD + warp * P;
+        float2 x[P];
+#pragma unroll
+        for (int k = 0; k < P; k++) x[k] = make_float2(k == lane ? 1.f : 0.f, 0.f);
+        if (!upper)
+            df3_lrow16_back_step<P - 1>(x, Ab);
         else
-            df2_inv_upper32(Ab, Xd + warp * DF_BLK * DF_SLD);
+            df3_urow16_step<0>(x, Ab, rcp + warp * P);
+        if (lane < P)
+#pragma unroll
+            for (int k = 0; k < P; k++) T[(warp * P + lane) * PL16 + k] = x[k];
     }
     __syncthreads();
-    // ---- the off-diagonal blocks of the inverse, in place in blk, one block column per stage; 2 x 2
-    // tiles, at most DF_NB - 1 blocks a stage (768 tiles): two per thread
-    const bool upper = side == 1;
-    for (int st = 1; st < DF_NB; st++) {
-        const int J = upper ? st : DF_NB - 1 - st;
-        const int nI = st, ntile = nI * (DF_BLK / 2) * (DF_BLK / 2);
-        float2 tv[2][2][2];
-        // T(I, J) = sum_K X(I, K) U(K, J)  (upper: I <= K < J)  or  sum_K Y(I, K) L(K, J)  (lower: J < K <= I)
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-            const int t = threadIdx.x + e * DF2_THREADS;
-#pragma unroll
-            for (int a = 0; a < 2; a++) tv[e][a][0] = tv[e][a][1] = make_float2(0.f, 0.f);
-            if (t < ntile) {
-                const int bi = t / 256, i0 = 2 * ((t / 16) % 16), j0 = 2 * (t % 16);
-                const int I = upper ? bi : J + 1 + bi;
-                const int Kb = upper ? I : J + 1, Ke = upper ? J - 1 : I;
-                for (int K = Kb; K <= Ke; K++) {
-                    const bool diag = K == I;  // X(I, I) from the scratch, else the block stored in blk
-                    const float2* Xs = diag ? Xd + I * DF_BLK * DF_SLD + i0 * DF_SLD
-                                            : blk + (I * DF_BLK + i0) * DF_LD + K * DF_BLK;
-                    const int xld = diag ? DF_SLD : DF_LD;
-                    const float2* Bs = blk + (K * DF_BLK) * DF_LD + J * DF_BLK + j0;
-#pragma unroll 4
-                    for (int k = 0; k < DF_BLK; k++) {
-                        const float2 x0 = Xs[k], x1 = Xs[xld + k];
-                        const float2 b0 = Bs[k * DF_LD], b1 = Bs[k * DF_LD + 1];
-                        cfma_add(tv[e][0][0], x0, b0);
-                        cfma_add(tv[e][0][1], x0, b1);
-                        cfma_add(tv[e][1][0], x1, b0);
-                        cfma_add(tv[e][1][1], x1, b1);
-                    }
-                }
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-            const int t = threadIdx.x + e * DF2_THREADS;
-            if (t < ntile) {
-                const int bi = t / 256, i0 = 2 * ((t / 16) % 16), j0 = 2 * (t % 16);
-                const int I = upper ? bi : J + 1 + bi;
-#pragma unroll
-                for (int a = 0; a < 2; a++)
-#pragma unroll
-                    for (int b = 0; b < 2; b++) blk[(I * DF_BLK + i0 + a) * DF_LD + J * DF_BLK + j0 + b] = tv[e][a][b];
-            }
-        }
-        __syncthreads();
-        // X(I, J) = -T(I, J) X(J, J)
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-            const int t = threadIdx.x + e * DF2_THREADS;
-#pragma unroll
-            for (int a = 0; a < 2; a++) tv[e][a][0] = tv[e][a][1] = make_float2(0.f, 0.f);
-            if (t < ntile) {
-                const int bi = t / 256, i0 = 2 * ((t / 16) % 16), j0 = 2 * (t % 16);
-                const int I = upper ? bi : J + 1 + bi;
-                const float2* Ts = blk + (I * DF_BLK + i0) * DF_LD + J * DF_BLK;
-                const float2* Xj = Xd + J * DF_BLK * DF_SLD + j0;
-#pragma unroll 4
-                for (int k = 0; k < DF_BLK; k++) {
-                    const float2 x0 = Ts[k], x1 = Ts[DF_LD + k];
-                    const float2 b0 = Xj[k * DF_SLD], b1 = Xj[k * DF_SLD + 1];
-                    cfma_sub(tv[e][0][0], x0, b0);
-                    cfma_sub(tv[e][0][1], x0, b1);
-                    cfma_sub(tv[e][1][0], x1, b0);
-                    cfma_sub(tv[e][1][1], x1, b1);
-                }
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-            const int t = threadIdx.x + e * DF2_THREADS;
-            if (t < ntile) {
-                const int bi = t / 256, i0 = 2 * ((t / 16) % 16), j0 = 2 * (t % 16);
-                const int I = upper ? bi : J + 1 + bi;
-#pragma unroll
-                for (int a = 0; a < 2; a++)
-#pragma unroll
-                    for (int b = 0; b < 2; b++) blk[(I * DF_BLK + i0 + a) * DF_LD + J * DF_BLK + j0 + b] = tv[e][a][b];
-            }
-        }
-        __syncthreads();
+    // ... into place, with zeros in the other triangle's 16-block of each 32 x 32 diagonal block
+    for (int t = threadIdx.x; t < NBL * P; t += DF_THREADS) {
+        const int w = t / (P * P), i = (t / P) % P, k = t % P;
+        blk[(w * P + i) * DF_LD + w * P + k] = T[(w * P + i) * PL16 + k];
+        const int z = w ^ 1;  // the partner block of the 32-block
+        if ((z > w) == !upper) blk[(w * P + i) * DF_LD + z * P + k] = make_float2(0.f, 0.f);
     }
+    __syncthreads();
+    // 32-level: the four pairs at once (128 threads each); lower X(I, J) = -X(I, I) L(I, J) X(J, J) for
+    // (I, J) = (2q + 1, 2q), upper Y(I, J) = -Y(I, I) U(I, J) Y(J, J) for (2q, 2q + 1) (16-blocks)
+    {
+        const int q = threadIdx.x / 128, tq = threadIdx.x % 128;
+        const int I = (upper ? 2 * q : 2 * q + 1) * P, J = (upper ? 2 * q + 1 : 2 * q) * P;
+        float2* Tq = T + q * P * PL16;
+        // T = L(I, J) X(J, J), then X(I, J) = -X(I, I) T: two 16 x 16 outputs a thread
+#pragma unroll
+        for (int pass = 0; pass < 2; pass++) {
+            const float2* A = pass == 0 ? blk + I * DF_LD + J : blk + I * DF_LD + I;
+            const int lda = DF_LD;
+            const float2* B = pass == 0 ? blk + J * DF_LD + J : Tq;
+            const int ldb = pass == 0 ? DF_LD : PL16;
+            const int r = tq / 8, c0 = (tq % 8) * 2;  // rows 0..15, column pairs
+            float2 c00 = make_float2(0.f, 0.f), c01 = c00;
+#pragma unroll 4
+            for (int k = 0; k < P; k++) {
+                const float2 a = A[r * lda + k];
+                cfma_add(c00, a, B[k * ldb + c0]);
+                cfma_add(c01, a, B[k * ldb + c0 + 1]);
+            }
+            __syncthreads();  // (pass 0) every thread's reads of L(I, J) done; (pass 1) of T
+            if (pass == 0) {
+                Tq[r * PL16 + c0] = c00;
+                Tq[r * PL16 + c0 + 1] = c01;
+            } else {
+                blk[(I + r) * DF_LD + J + c0] = make_float2(-c00.x, -c00.y);
+                blk[(I + r) * DF_LD + J + c0 + 1] = make_float2(-c01.x, -c01.y);
+            }
+            __syncthreads();
+        }
+    }
+    // 64-level: the two pairs of 32-blocks at once (256 threads each); lower: X(I, J) = -X(I, I) L(I, J)
+    // X(J, J) for (I, J) = (1, 0), (3, 2); upper: Y(I, J) = -Y(I, I) U(I, J) Y(J, J) for (0, 1), (2, 3)
+    {
+        const int q = threadIdx.x / 256, tq = threadIdx.x % 256;
+        const int d0 = 2 * q * DF_BLK, d1 = d0 + DF_BLK;  // the pair's two diagonal blocks
+        const int I = upper ? d0 : d1, J = upper ? d1 : d0;
+        float2* Tq = T + q * DF_BLK * DF3_TLD;  // [32][DF3_TLD] rows of the pair's scratch
+        df3_product(blk + I * DF_LD + J, DF_LD, blk + J * DF_LD + J, DF_LD, Tq, DF3_TLD, DF_BLK,
+                    upper ? DF3_B_UPPER : DF3_B_LOWER, 1.f, tq, 256);
+        __syncthreads();
+        df3_product(blk + I * DF_LD + I, DF_LD, Tq, DF3_TLD, blk + I * DF_LD + J, DF_LD, DF_BLK,
+                    upper ? DF3_A_UPPER : DF3_A_LOWER, -1.f, tq, 256);
+    }
+    __syncthreads();
+    // 128-level: lower X21 = -X22 (L21 X11), upper Y12 = -Y11 (U12 Y22), 64 x 64 blocks
+    {
+        const int h = 2 * DF_BLK;
+        const int I = upper ? 0 : h, J = upper ? h : 0;
+        df3_product(blk + I * DF_LD + J, DF_LD, blk + J * DF_LD + J, DF_LD, T, DF3_TLD, h,
+                    upper ? DF3_B_UPPER : DF3_B_LOWER, 1.f, threadIdx.x, DF_THREADS);
+        __syncthreads();
+        df3_product(blk + I * DF_LD + I, DF_LD, T, DF3_TLD, blk + I * DF_LD + J, DF_LD, h,
+                    upper ? DF3_A_UPPER : DF3_A_LOWER, -1.f, threadIdx.x, DF_THREADS);
+    }
+    __syncthreads();
     // ---- outputs: this side's triangle of the inverse
-    auto inv_at = [&](int i, int c) -> float2 {  // U^-1 (i <= c, side 1) or L^-1 (i > c, side 0)
-        const int bi = i / DF_BLK, bc = c / DF_BLK;
-        if (bi == bc) return Xd[bi * DF_BLK * DF_SLD + (i % DF_BLK) * DF_SLD + c % DF_BLK];
-        return blk[i * DF_LD + c];
-    };
     {
         float2* D = DINV + ((size_t)f * (Np / NBL) + k0 / NBL) * NBL * NBL;
-        for (int t = threadIdx.x; t < NBL * NBL; t += DF2_THREADS) {
+        for (int t = threadIdx.x; t < NBL * NBL; t += DF_THREADS) {
             const int i = t / NBL, c = t % NBL;
-            if ((i > c) == !upper) D[t] = inv_at(i, c);
+            if ((i > c) == !upper) D[t] = blk[i * DF_LD + c];
         }
     }
     if (!upper) {
         float* PLf = PL + (size_t)f * NBL * 2 * NBL;
-        for (int t = threadIdx.x; t < NBL * NBL; t += DF2_THREADS) {  // [Lr | Li] rows of L^-1 (c fastest)
+        for (int t = threadIdx.x; t < NBL * NBL; t += DF_THREADS) {  // [Lr | Li] rows of L^-1 (c fastest)
             const int i = t / NBL, c = t % NBL;
-            const float2 l = i > c ? inv_at(i, c) : make_float2(i == c ? 1.f : 0.f, 0.f);
+            const float2 l = i > c ? blk[i * DF_LD + c] : make_float2(i == c ? 1.f : 0.f, 0.f);
             PLf[(size_t)i * 2 * NBL + c] = l.x;
             PLf[(size_t)i * 2 * NBL + NBL + c] = l.y;
         }
     } else {
         float* PUf = PU + (size_t)f * 2 * NBL * 2 * NBL;
-        for (int t = threadIdx.x; t < NBL * NBL; t += DF2_THREADS) {
+        for (int t = threadIdx.x; t < NBL * NBL; t += DF_THREADS) {
             // U^-1 block-real K-major (i fastest): row c: [Ur(:, c); -Ui(:, c)], row NBL + c: [Ui(:, c); Ur(:, c)]
             const int c = t / NBL, i = t % NBL;
-            const float2 u = i <= c ? inv_at(i, c) : make_float2(0.f, 0.f);
+            const float2 u = i <= c ? blk[i * DF_LD + c] : make_float2(0.f, 0.f);
             PUf[(size_t)c * 2 * NBL + i] = u.x;
             PUf[(size_t)c * 2 * NBL + NBL + i] = -u.y;
             PUf[(size_t)(NBL + c) * 2 * NBL + i] = u.y;
