@@ -374,9 +374,8 @@ def ours(args, world, rank, local, pg):
         line["fp64_fallback_frequencies"] = fallbacks
     if precision == nv.HBG_MIXED and not args.no_plain and bodies:
         line["plain_fp64"], plain = plain_comparison(nv, mine, bodies, depth, device)
-        if args.surrogate_steps > 0 and CASE in SINGLE_BODY:
-            v, omegas = workload()
-            line["surrogate"] = surrogate_comparison(nv, v, omegas, device, plain[0], args.surrogate_steps)
+    if precision == nv.HBG_MIXED and world == 1 and args.surrogate_steps > 0:
+        line["surrogate"] = surrogate_comparison(nv, device, args.surrogate_steps)
     if world == 1 and not args.no_cpu_baseline and CASE in SINGLE_BODY:
         line["cpu_baseline"] = cpu_baseline_quick()
     return line
@@ -424,36 +423,52 @@ def scaled_error(got, ref):
     return float((np.abs(np.asarray(got) - ref) / scale).max())
 
 
-def surrogate_comparison(nv, v, omegas, device, plain, train_steps):
-    """The learned part measured on the same job: train the wave-term network on the device (its own
-    kernels, samples of the table evaluation), solve the job with it as the wave term of the mixed
-    assembly, and report its throughput and its A, B, X error against the FP64 form, plus the device
-    time of one million network and table evaluations."""
+def surrogate_comparison(nv, device, train_steps):
+    """The learned part measured against the table evaluation it would replace, on the three-cylinder
+    array (3 x 4096 panels, infinite depth; three of its 32 frequencies): train the wave-term network on
+    the device (its own kernels, 2^22 samples of the table and series evaluation over K R < 100,
+    -K (z + zeta) < 50), solve the frequencies in the mixed form with the table and with the network as
+    the wave term (tensor cores, tcgen05), and report each one's assembly time and A, B, X error against
+    the FP64 form, the device time of one million evaluations of each, and the roofline bound of the
+    network: its FLOPs per pair over the BF16 tensor peak, against the table's measured time per pair."""
     import ctypes
 
-    p, nm, rep = nv.surrogate_train(n_train=1 << 20, batch=8192, steps=train_steps, lr=2e-3, seed=1,
+    from hydrobem_b200 import meshes
+
+    samples = 1 << 22
+    p, nm, rep = nv.surrogate_train(n_train=samples, batch=8192, steps=train_steps, lr=2e-3, seed=1,
                                     n_val=1 << 16)
-    body = nv.Body(v, omegas, HEADINGS)
-    arr = (nv.HbgProblem * 1)(body.problem())
-    opt = nv.default_options(precision=nv.HBG_MIXED, depth=DEPTH, device=device, surrogate=nv.surrogate_blob(p, nm))
-    L = nv.lib()
-    nv.check(L.hbg_solve_batch(arr, 1, ctypes.byref(opt)))  # warm-up
-    ms = []
-    for _ in range(2):
-        nv.check(L.hbg_solve_batch(arr, 1, ctypes.byref(opt)))
-        ms.append(nv.last_profile()["total"])
-    pairs = nv.last_surrogate_pairs()
-    got = body.results()
+    v, pb, centers = meshes.cylinder_array()
+    omegas = np.sqrt(np.linspace(0.1, 2.0, 32) * meshes.GRAVITY)[[0, 15, 31]]
+    N, F = len(v), len(omegas)
+    kw = dict(panel_body=pb, rotation_centers=centers, device=device)
+    ref = nv.solve(v, omegas, [0.0], precision=nv.HBG_FP64, **kw)
+    out = {}
+    for name, sg in (("table", None), ("network", nv.surrogate_blob(p, nm))):
+        extra = {} if sg is None else {"surrogate": sg}
+        nv.solve(v, omegas, [0.0], precision=nv.HBG_MIXED, **kw, **extra)  # warm-up
+        got = nv.solve(v, omegas, [0.0], precision=nv.HBG_MIXED, **kw, **extra)
+        prof = nv.last_profile()
+        err = {k: scaled_error(got[k], ref[k]) for k in ("A", "B", "X")}
+        out[name] = {"assembly_ms": round(prof["assembly"], 3), "job_ms": round(prof["total"], 3),
+                     "pairs_from_network": int(nv.last_surrogate_pairs()), "err_vs_fp64": err,
+                     "meets_1e-5": bool(max(err.values()) <= 1e-5)}
     rng = np.random.default_rng(5)
-    xy = np.expm1(rng.uniform(0.0, 1.0, (1 << 20, 2)) * np.log(31.0))
+    u = rng.uniform(0.0, 1.0, (1 << 20, 2))
+    xy = np.column_stack([np.expm1(u[:, 0] * np.log1p(100.0)), np.expm1(u[:, 1] * np.log1p(50.0))])
     _, _, (ms_net, ms_tab) = nv.surrogate_eval(p, nm, xy)
-    err = {k: scaled_error(got[k], plain[k]) for k in ("A", "B", "X")}
-    step = float(np.mean(ms))
-    return {"value": len(omegas) / (step * 1e-3), "ms_per_step": step, "pairs_from_network": int(pairs),
-            "err_vs_fp64": err, "meets_1e-5": bool(max(err.values()) <= 1e-5),
-            "train": {"steps": train_steps, "samples": 1 << 20, "device_ms": round(rep["train_ms"], 1),
+    pairs = F * N * (N + 1) // 2  # pair kernels of the assembly (one per unordered pair and frequency)
+    flops = 2 * (3 * 128 + 3 * 128 * 128 + 128 * 6)
+    peaks, kind = measured_peaks()
+    return {"workload": f"three-cylinder array, {N} panels, {F} frequencies K a = 0.1, 1.05, 2, infinite depth",
+            "table": out["table"], "network": out["network"],
+            "train": {"steps": train_steps, "samples": samples, "device_ms": round(rep["train_ms"], 1),
                       "val_rms_over_spread": {k: round(x, 5) for k, x in rep["val_rms_over_spread"].items()}},
-            "eval_ms_per_1M_points": {"network": round(ms_net, 3), "table": round(ms_tab, 3)}}
+            "eval_ms_per_1M_points": {"network": round(ms_net, 3), "table": round(ms_tab, 3)},
+            "roofline": {"network_flops_per_pair": flops, "bf16_peak_tflops": peaks["bf16_tflops"], "peak_kind": kind,
+                         "network_bound_ps_per_pair": round(flops / (peaks["bf16_tflops"] * 1e12) * 1e12, 2),
+                         "table_ps_per_pair": round(out["table"]["assembly_ms"] * 1e-3 / pairs * 1e12, 2),
+                         "network_ps_per_pair": round(out["network"]["assembly_ms"] * 1e-3 / pairs * 1e12, 2)}}
 
 
 def cpu_baseline_quick():

@@ -1305,8 +1305,9 @@ extern "C" HbStatus hbg_surrogate_eval(const float* params, const float* norm, i
     try {
         if (!params || !norm || !xy || !ms2) return fail({HB_ERR_ARGUMENT, "null argument"});
         if (n < 1) return fail({HB_ERR_VALUE, "n must be positive"});
-        for (int32_t i = 0; i < 2 * n; i++)
-            if (!(xy[i] >= 0.0 && xy[i] < 30.0)) return fail({HB_ERR_VALUE, "points must lie in the trained domain [0, 30)^2"});
+        for (int32_t i = 0; i < n; i++)
+            if (!(xy[2 * i] >= 0.0 && xy[2 * i] < 100.0 && xy[2 * i + 1] >= 0.0 && xy[2 * i + 1] < 50.0))
+                return fail({HB_ERR_VALUE, "points must lie in the trained domain [0, 100) x [0, 50)"});
         current_device_ready();
         const char* msg = "";
         int rc = surrogate_eval(params, norm, n, xy, out_net, out_table, ms2, &msg);

@@ -281,7 +281,7 @@ void launch_sg_pack(const float* params_norm, uint8_t* img, cudaStream_t s);
 size_t sg_image_bytes();
 void launch_assemble_f32_sg(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
                             const float* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
-                            const uint8_t* img, unsigned long long* counts, cudaStream_t s);
+                            const uint8_t* img, unsigned long long* counts, int* err, cudaStream_t s);
 // pairs (unordered, over all frequencies) whose wave term came from the network in the last mixed solve
 inline long long& last_surrogate_pairs() {
     static thread_local long long n = 0;

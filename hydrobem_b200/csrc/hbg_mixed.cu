@@ -526,7 +526,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             }
             P.begin(s);
             if (sg)
-                launch_assemble_f32_sg(pv, st, nb, dfi, dfd, tiles_f, fpt, fin, S32, A32, Np, sg_img, sg_count, s);
+                launch_assemble_f32_sg(pv, st, nb, dfi, dfd, tiles_f, fpt, fin, S32, A32, Np, sg_img, sg_count, err, s);
             else
                 launch_assemble_f32(pv, st, nb, dfi, dfd, tiles_f, fpt, fin, S32, A32, Np, s);
             if (G > 1) {

@@ -1,21 +1,25 @@
 // hbg_surrogate.cu -- the learned part of the mixed form: an MLP surrogate of the regular part of the
 // infinite-depth wave term of the Green function, trained on the device by this file's own forward
-// and backward kernels on samples of the library's own table evaluation, and evaluated on the
-// tensor cores (mma.sync BF16, FP32 accumulation).
+// and backward kernels on samples of the library's own table and series evaluation, and evaluated on
+// the 5th-generation tensor cores (tcgen05.mma kind::f16, BF16 operands, FP32 accumulators in TMEM).
 //
-// What it learns.  In the table region X = K R, Y = -K (z + zeta) in [0, 30)^2 the wave term is
-// (green_inf.rs:316-368, identity form)
+// What it learns.  For X = K R in [0, 100) and Y = -K (z + zeta) in [0, 50) the wave term is
+// (green_inf.rs:316-368)
 //     F  = S + g,   S = -2 e^-Y J0(X) (log(Y + R0) + gamma - log 2),   R0 = sqrt(X^2 + Y^2),
 // S holding the logarithmic singularity at R0 = 0 in closed form.  The network maps the inputs
-// (u, v, w) = (2 log1p(X) / log 31 - 1, 2 log1p(Y) / log 31 - 1, 1 / (K h)) -- w = 0 for infinite
-// depth -- to six outputs: g, dg/dX, dg/dY (the regular real part and its radial and vertical
-// derivatives) and I, dI/dX, dI/dY (the imaginary part -2 pi e^-Y J0(X) and its derivatives), each
-// standardized by its mean and spread over the training set.  Architecture 3 -> 128 -> 128 -> 128
-// -> 128 -> 6, SiLU, weights rounded to BF16 in the forward pass (FP32 master copy and Adam
-// moments), activations rounded to BF16 between layers, FP32 accumulation.  Outside [0, 30)^2 the
+// (u, v, w) = (2 log1p(X) / log 101 - 1, 2 log1p(Y) / log 51 - 1, 0) to six outputs: g, dg/dX, dg/dY
+// (the regular real part and its radial and vertical derivatives) and I, dI/dX, dI/dY (the imaginary
+// part -2 pi e^-Y J0(X) and its derivatives), each standardized by its mean and spread over the
+// training set.  The third input stays 0: the term replaced is the same function at every depth (in
+// finite depth it enters the kernel as F(K R, K v3), green_fin.rs:1051-1071, the depth-dependent parts
+// being the per-frequency tiles), so a K h input would carry nothing.  Architecture 3 -> 128 -> 128 ->
+// 128 -> 128 -> 6, SiLU, weights rounded to BF16 in the forward pass (FP32 master copy and Adam
+// moments), activations rounded to BF16 between layers, FP32 accumulation.  Outside the domain the
 // table/series evaluation is used.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+
+#include "hbg_tc.cuh"
 
 #include <cmath>
 #include <vector>
@@ -29,7 +33,8 @@ constexpr int SG_OFF_W1 = SG_OFF_B0 + SG_H;
 constexpr int SG_LAYER_HH = SG_H * SG_H + SG_H;  // W and b of a hidden layer
 constexpr int SG_OFF_W4 = SG_OFF_W1 + 3 * SG_LAYER_HH, SG_OFF_B4 = SG_OFF_W4 + SG_OUT * SG_H;
 constexpr int SG_PARAMS = SG_OFF_B4 + SG_OUT;  // 50,822
-constexpr double SG_XMAX = 30.0;
+// the trained domain: X = K R in [0, 100), Y = -K (z + zeta) in [0, 50)
+constexpr double SG_XMAX = 100.0, SG_YMAX = 50.0;
 static_assert(SURROGATE_FLOATS == SG_PARAMS + 2 * SG_OUT, "parameters then means and spreads");
 
 __host__ __device__ inline int sg_off_w(int l) { return l == 0 ? SG_OFF_W0 : l < 4 ? SG_OFF_W1 + (l - 1) * SG_LAYER_HH : SG_OFF_W4; }
@@ -47,18 +52,17 @@ __device__ __forceinline__ float silu_d(float z) {
 }
 
 __device__ __forceinline__ void sg_inputs(double X, double Y, float* in) {
-    const double L = log(1.0 + SG_XMAX);
-    in[0] = (float)(2.0 * log1p(X) / L - 1.0);
-    in[1] = (float)(2.0 * log1p(Y) / L - 1.0);
-    in[2] = 0.f;  // 1 / (K h): infinite depth
+    in[0] = (float)(2.0 * log1p(X) / log1p(SG_XMAX) - 1.0);
+    in[1] = (float)(2.0 * log1p(Y) / log1p(SG_YMAX) - 1.0);
+    in[2] = 0.f;  // the replaced term has no depth dependence (see the header)
 }
 
 // The six targets at (X, Y) from the table evaluation (FP64).
 __device__ void sg_targets(double X, double Y, double* t) {
     const Wave w = wave_kernel<false>(X, Y);
-    double f[4];
-    table1d(X, f);
-    const double j0 = f[0], j1 = f[1], eY = exp(-Y), R0 = sqrt(X * X + Y * Y);
+    double j0, j1;
+    bessel_j01<false>(X, j0, j1);
+    const double eY = exp(-Y), R0 = sqrt(X * X + Y * Y);
     const double lg = log(Y + R0) + (GAMMA - LOG2);
     const double S = -2.0 * eY * j0 * lg;
     const double SX = 2.0 * eY * j1 * lg - 2.0 * eY * j0 * X / (R0 * (Y + R0));
@@ -82,15 +86,14 @@ __device__ __forceinline__ double halton(uint64_t i, int b) {
     return r;
 }
 
-// Samples i0 + 1 .. i0 + n of the 2-D Halton sequence, log-spaced over [0, 30)^2:
-// X = (31^u - 1), Y = (31^v - 1); inputs [n][3] (FP32) and FP64 targets [n][6].
+// Samples i0 + 1 .. i0 + n of the 2-D Halton sequence, log-spaced over the domain:
+// X = 101^u - 1, Y = 51^v - 1; inputs [n][3] (FP32) and FP64 targets [n][6].
 __global__ void k_sg_samples(int n, uint64_t i0, float* __restrict__ in, double* __restrict__ tg,
                              double* __restrict__ xy) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint64_t h = i0 + (uint64_t)i + 1;
-    const double L = log(1.0 + SG_XMAX);
-    const double X = expm1(halton(h, 2) * L), Y = expm1(halton(h, 3) * L);
+    const double X = expm1(halton(h, 2) * log1p(SG_XMAX)), Y = expm1(halton(h, 3) * log1p(SG_YMAX));
     sg_inputs(X, Y, in + 3 * (size_t)i);
     sg_targets(X, Y, tg + 6 * (size_t)i);
     if (xy) {
@@ -295,19 +298,29 @@ struct SgTrainer {
 };
 
 // ---------------------------------------------------------------- inference on the tensor cores
-// A warp evaluates 16 samples per pass: each layer is a 16 x 128 by 128 x 128 product of
-// mma.sync m16n8k16 BF16 tiles; the FP32 accumulator fragments of one layer become, after bias,
-// SiLU and rounding, the BF16 A fragments of the next without leaving registers.  Weights in
-// shared memory as BF16 rows padded to 136 entries (conflict-free B fragment reads).
-constexpr int SG_LD = SG_H + 8;
-constexpr size_t SG_SMEM = (size_t)(SG_H * 16 + 3 * SG_H * SG_LD + 8 * SG_LD) * 2 + (size_t)(4 * SG_H + 8) * 4;
+// 5th-generation tensor cores: a CTA of 256 threads evaluates 256 samples a pass as two 128-row tiles.
+// Layer 0 (3 -> 128) on the CUDA cores; each hidden layer is, per tile, eight tcgen05.mma of
+// kind::f16 (BF16 operands, M 128, N 128, K 16) from shared memory into a TMEM accumulator (FP32);
+// thread r of a tile reads its row back (tcgen05.ld), adds the bias, applies SiLU, rounds to BF16
+// and writes the row into the shared A tile of the next layer; the output layer is one more MMA
+// (N 16, six used).  Operands are K-major in the 128-byte swizzle layout: rows of 128 bytes (64
+// BF16 of K), 16-byte units XOR-ed with the row index mod 8, two K halves 16 KB apart per tile.
+//
+// The packed weight image, copied whole into each persistent CTA's shared memory: W1..W3 as B
+// operands [128 rows j][K 128] (32 KB each), W4 [16 rows, 6 used][K 128] (4 KB), then FP32: W0
+// [128][3], biases b0..b3 [4][128] and b4 [8] (BF16-rounded values), output means and spreads [12].
+constexpr int SG_TILE_BYTES = SG_H * SG_H * 2;  // one 128 x 128 BF16 operand
+constexpr size_t SG_IMG_W4 = 3 * (size_t)SG_TILE_BYTES;
+constexpr size_t SG_IMG_F = SG_IMG_W4 + 16 * SG_H * 2;
+constexpr int SG_F_W0 = 0, SG_F_B = SG_H * SG_IN, SG_F_N = SG_F_B + 4 * SG_H + 8;
+constexpr size_t SG_IMG_BYTES = (SG_IMG_F + (size_t)(SG_F_N + 2 * SG_OUT) * 4 + 1023) / 1024 * 1024;
+// dynamic shared memory of a network CTA: alignment slack, the image, two A tiles, the mbarrier
+constexpr size_t SG_TC_SMEM = 1024 + SG_IMG_BYTES + 2 * (size_t)SG_TILE_BYTES + 16;
+constexpr uint32_t SG_TMEM_COLS = 512;  // accumulators: tiles at columns 0 and 128, outputs at 256 and 288
 
-__device__ __forceinline__ void mma_bf16_16816(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-        "{%0, %1, %2, %3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+// byte offset of element (row, k) in a K-major 128-byte-swizzled operand of `rows` rows, K = 128
+__host__ __device__ constexpr size_t sg_sw_off(int rows, int row, int k) {
+    return (size_t)(k / 64) * rows * 128 + (size_t)row * 128 + (size_t)((((k % 64) / 8) ^ (row & 7)) * 16) + (k % 8) * 2;
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
@@ -315,224 +328,197 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return *reinterpret_cast<const uint32_t*>(&h);
 }
 
-// out [n][6] (FP32, de-standardized by mean/spread norm[0..5], norm[6..11]) from inputs [n][3].
-__global__ void __launch_bounds__(256) k_sg_infer(int n, const float* __restrict__ params, const float* __restrict__ norm,
-                                                  const float* __restrict__ in, float* __restrict__ out) {
-    extern __shared__ __align__(16) uint8_t sg_smem[];
-    __nv_bfloat16* w0 = reinterpret_cast<__nv_bfloat16*>(sg_smem);  // [H][16] (k padded)
-    __nv_bfloat16* wh = w0 + SG_H * 16;                              // 3 x [H][SG_LD]
-    __nv_bfloat16* w4 = wh + 3 * SG_H * SG_LD;                       // [8][SG_LD] (rows 6, 7 zero)
-    float* bias = reinterpret_cast<float*>(w4 + 8 * SG_LD);          // b0..b3 [4][H], b4 [8]
-    for (int t = threadIdx.x; t < SG_H * 16; t += blockDim.x) {
-        const int j = t / 16, k = t % 16;
-        w0[t] = __float2bfloat16_rn(k < SG_IN ? params[SG_OFF_W0 + j * SG_IN + k] : 0.f);
-    }
-    for (int t = threadIdx.x; t < 3 * SG_H * SG_LD; t += blockDim.x) {
-        const int l = t / (SG_H * SG_LD), r = t % (SG_H * SG_LD), j = r / SG_LD, k = r % SG_LD;
-        wh[t] = __float2bfloat16_rn(k < SG_H ? params[sg_off_w(l + 1) + j * SG_H + k] : 0.f);
-    }
-    for (int t = threadIdx.x; t < 8 * SG_LD; t += blockDim.x) {
-        const int j = t / SG_LD, k = t % SG_LD;
-        w4[t] = __float2bfloat16_rn(j < SG_OUT && k < SG_H ? params[SG_OFF_W4 + j * SG_H + k] : 0.f);
-    }
-    for (int t = threadIdx.x; t < 4 * SG_H + 8; t += blockDim.x)
-        bias[t] = bf16r(t < 4 * SG_H ? params[sg_off_b(t / SG_H) + t % SG_H]
-                                     : (t - 4 * SG_H < SG_OUT ? params[SG_OFF_B4 + t - 4 * SG_H] : 0.f));
-    __syncthreads();
-    const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
-    const int warps = gridDim.x * (blockDim.x >> 5), wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const uint32_t* w0u = reinterpret_cast<const uint32_t*>(w0);
-    const uint32_t* whu = reinterpret_cast<const uint32_t*>(wh);
-    const uint32_t* w4u = reinterpret_cast<const uint32_t*>(w4);
-    for (int s0 = wid * 16; s0 < n; s0 += warps * 16) {
-        // layer 0: A = [u v w 0 ...] (k padded to 16)
-        uint32_t a[8][4];
-        {
-            const int r0 = s0 + g, r1 = s0 + g + 8;
-            float x0 = 0.f, x1 = 0.f, y0 = 0.f, y1 = 0.f;
-            if (tq < 2) {
-                const int c = 2 * tq;
-                if (r0 < n) {
-                    x0 = in[3 * (size_t)r0 + c];
-                    y0 = c + 1 < SG_IN ? in[3 * (size_t)r0 + c + 1] : 0.f;
-                }
-                if (r1 < n) {
-                    x1 = in[3 * (size_t)r1 + c];
-                    y1 = c + 1 < SG_IN ? in[3 * (size_t)r1 + c + 1] : 0.f;
-                }
-            }
-            uint32_t a0[4] = {pack_bf16(x0, y0), pack_bf16(x1, y1), 0u, 0u};
-            float acc[16][4];
-#pragma unroll
-            for (int nt = 0; nt < 16; nt++) {
-                acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-                const int j = nt * 8 + g;
-                mma_bf16_16816(acc[nt], a0, w0u[(j * 16 + 2 * tq) / 2], w0u[(j * 16 + 2 * tq + 8) / 2]);
-            }
-#pragma unroll
-            for (int kt = 0; kt < 8; kt++) {
-                const int c0 = (2 * kt) * 8 + 2 * tq, c1 = (2 * kt + 1) * 8 + 2 * tq;
-                const float* b = bias;
-                a[kt][0] = pack_bf16(silu(acc[2 * kt][0] + b[c0]), silu(acc[2 * kt][1] + b[c0 + 1]));
-                a[kt][1] = pack_bf16(silu(acc[2 * kt][2] + b[c0]), silu(acc[2 * kt][3] + b[c0 + 1]));
-                a[kt][2] = pack_bf16(silu(acc[2 * kt + 1][0] + b[c1]), silu(acc[2 * kt + 1][1] + b[c1 + 1]));
-                a[kt][3] = pack_bf16(silu(acc[2 * kt + 1][2] + b[c1]), silu(acc[2 * kt + 1][3] + b[c1 + 1]));
-            }
-        }
-        // hidden layers 1..3
-#pragma unroll 1
-        for (int l = 0; l < 3; l++) {
-            const uint32_t* W = whu + (size_t)l * SG_H * SG_LD / 2;
-            float acc[16][4];
-#pragma unroll
-            for (int nt = 0; nt < 16; nt++) {
-                acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-                const int j = nt * 8 + g;
-#pragma unroll
-                for (int kt = 0; kt < 8; kt++)
-                    mma_bf16_16816(acc[nt], a[kt], W[(j * SG_LD + kt * 16 + 2 * tq) / 2],
-                                   W[(j * SG_LD + kt * 16 + 2 * tq + 8) / 2]);
-            }
-            const float* b = bias + (l + 1) * SG_H;
-#pragma unroll
-            for (int kt = 0; kt < 8; kt++) {
-                const int c0 = (2 * kt) * 8 + 2 * tq, c1 = (2 * kt + 1) * 8 + 2 * tq;
-                a[kt][0] = pack_bf16(silu(acc[2 * kt][0] + b[c0]), silu(acc[2 * kt][1] + b[c0 + 1]));
-                a[kt][1] = pack_bf16(silu(acc[2 * kt][2] + b[c0]), silu(acc[2 * kt][3] + b[c0 + 1]));
-                a[kt][2] = pack_bf16(silu(acc[2 * kt + 1][0] + b[c1]), silu(acc[2 * kt + 1][1] + b[c1 + 1]));
-                a[kt][3] = pack_bf16(silu(acc[2 * kt + 1][2] + b[c1]), silu(acc[2 * kt + 1][3] + b[c1 + 1]));
-            }
-        }
-        // output layer: one n-tile of 8 (6 used)
-        float o[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-        for (int kt = 0; kt < 8; kt++)
-            mma_bf16_16816(o, a[kt], w4u[(g * SG_LD + kt * 16 + 2 * tq) / 2], w4u[(g * SG_LD + kt * 16 + 2 * tq + 8) / 2]);
-        const float* b4 = bias + 4 * SG_H;
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int r = s0 + g + (q >= 2 ? 8 : 0), c = 2 * tq + (q & 1);
-            if (r < n && c < SG_OUT) out[(size_t)r * SG_OUT + c] = norm[c] + norm[SG_OUT + c] * (o[q] + b4[c]);
-        }
-    }
+__host__ __device__ constexpr uint32_t sg_idesc_bf16(int M, int N) {
+    return (1u << 4)      // D format F32
+           | (1u << 7)    // A format BF16
+           | (1u << 10)   // B format BF16
+           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
-
-// ---------------------------------------------------------------- the network inside the assembly
-// The packed weight image (global memory, copied whole into each persistent CTA's shared memory):
-// w0 [H][16] BF16 (k padded), w1..w3 [H][SG_LD] BF16, w4 [8][SG_LD] BF16 (rows 6, 7 zero), biases
-// FP32 [4 H + 8] (BF16-rounded values), output means and spreads FP32 [12].
-constexpr size_t SG_IMG_WH = (size_t)SG_H * 16 * 2;
-constexpr size_t SG_IMG_W4 = SG_IMG_WH + (size_t)3 * SG_H * SG_LD * 2;
-constexpr size_t SG_IMG_B = SG_IMG_W4 + (size_t)8 * SG_LD * 2;
-constexpr size_t SG_IMG_N = SG_IMG_B + (size_t)(4 * SG_H + 8) * 4;
-constexpr size_t SG_IMG_BYTES = (SG_IMG_N + 2 * SG_OUT * 4 + 15) / 16 * 16;
-static_assert(SG_IMG_B % 16 == 0, "biases at a 16-byte boundary");
 
 __global__ void k_sg_pack(const float* __restrict__ params, const float* __restrict__ norm, uint8_t* __restrict__ img) {
-    __nv_bfloat16* w0 = reinterpret_cast<__nv_bfloat16*>(img);
-    __nv_bfloat16* wh = reinterpret_cast<__nv_bfloat16*>(img + SG_IMG_WH);
-    __nv_bfloat16* w4 = reinterpret_cast<__nv_bfloat16*>(img + SG_IMG_W4);
-    float* bias = reinterpret_cast<float*>(img + SG_IMG_B);
-    float* nm = reinterpret_cast<float*>(img + SG_IMG_N);
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x, st = gridDim.x * blockDim.x;
-    for (int t = t0; t < SG_H * 16; t += st) {
-        const int j = t / 16, k = t % 16;
-        w0[t] = __float2bfloat16_rn(k < SG_IN ? params[SG_OFF_W0 + j * SG_IN + k] : 0.f);
+    for (int t = t0; t < 3 * SG_H * SG_H; t += st) {
+        const int l = t / (SG_H * SG_H), j = (t / SG_H) % SG_H, k = t % SG_H;
+        *reinterpret_cast<__nv_bfloat16*>(img + (size_t)l * SG_TILE_BYTES + sg_sw_off(SG_H, j, k)) =
+            __float2bfloat16_rn(params[sg_off_w(l + 1) + j * SG_H + k]);
     }
-    for (int t = t0; t < 3 * SG_H * SG_LD; t += st) {
-        const int l = t / (SG_H * SG_LD), r = t % (SG_H * SG_LD), j = r / SG_LD, k = r % SG_LD;
-        wh[t] = __float2bfloat16_rn(k < SG_H ? params[sg_off_w(l + 1) + j * SG_H + k] : 0.f);
+    for (int t = t0; t < 16 * SG_H; t += st) {
+        const int j = t / SG_H, k = t % SG_H;
+        *reinterpret_cast<__nv_bfloat16*>(img + SG_IMG_W4 + sg_sw_off(16, j, k)) =
+            __float2bfloat16_rn(j < SG_OUT ? params[SG_OFF_W4 + j * SG_H + k] : 0.f);
     }
-    for (int t = t0; t < 8 * SG_LD; t += st) {
-        const int j = t / SG_LD, k = t % SG_LD;
-        w4[t] = __float2bfloat16_rn(j < SG_OUT && k < SG_H ? params[SG_OFF_W4 + j * SG_H + k] : 0.f);
-    }
+    float* f = reinterpret_cast<float*>(img + SG_IMG_F);
+    for (int t = t0; t < SG_H * SG_IN; t += st) f[SG_F_W0 + t] = bf16r(params[SG_OFF_W0 + t]);
     for (int t = t0; t < 4 * SG_H + 8; t += st)
-        bias[t] = bf16r(t < 4 * SG_H ? params[sg_off_b(t / SG_H) + t % SG_H]
-                                     : (t - 4 * SG_H < SG_OUT ? params[SG_OFF_B4 + t - 4 * SG_H] : 0.f));
-    for (int t = t0; t < 2 * SG_OUT; t += st) nm[t] = norm[t];
+        f[SG_F_B + t] = bf16r(t < 4 * SG_H ? params[sg_off_b(t / SG_H) + t % SG_H]
+                                           : (t - 4 * SG_H < SG_OUT ? params[SG_OFF_B4 + t - 4 * SG_H] : 0.f));
+    for (int t = t0; t < 2 * SG_OUT; t += st) f[SG_F_N + t] = norm[t];
 }
 
-// One forward pass for the 32 lanes of a warp (each lane's inputs u, v; w = 0), lanes 0-15 and
-// 16-31 as two m16 tiles of mma.sync m16n8k16 BF16; out6 = the de-standardized outputs of the
-// lane's own sample.  Every lane of the warp must call it.
-__device__ __forceinline__ void sg_warp_mlp(const uint8_t* img, float u, float v, float* out6) {
-    const uint32_t* w0u = reinterpret_cast<const uint32_t*>(img);
-    const uint32_t* whu = reinterpret_cast<const uint32_t*>(img + SG_IMG_WH);
-    const uint32_t* w4u = reinterpret_cast<const uint32_t*>(img + SG_IMG_W4);
-    const float* bias = reinterpret_cast<const float*>(img + SG_IMG_B);
-    const float* nm = reinterpret_cast<const float*>(img + SG_IMG_N);
-    const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
-#pragma unroll 1
-    for (int mt = 0; mt < 2; mt++) {
-        const float u0 = __shfl_sync(0xffffffffu, u, mt * 16 + g), v0 = __shfl_sync(0xffffffffu, v, mt * 16 + g);
-        const float u1 = __shfl_sync(0xffffffffu, u, mt * 16 + g + 8), v1 = __shfl_sync(0xffffffffu, v, mt * 16 + g + 8);
-        uint32_t a[8][4];
-        {
-            const uint32_t a0[4] = {tq == 0 ? pack_bf16(u0, v0) : 0u, tq == 0 ? pack_bf16(u1, v1) : 0u, 0u, 0u};
-            float acc[16][4];
+// The shared-memory side of a network CTA: the image, the two A tiles, the MMA barrier and TMEM.
+struct SgTc {
+    const uint8_t* img;
+    uint8_t* A;
+    uint64_t* bar;
+    uint32_t tmem;
+    uint32_t phase;
+};
+
+// The CTA's setup (every thread): the image copied in, the barrier, TMEM allocated (warp 0).
+__device__ __forceinline__ SgTc sg_tc_setup(uint8_t* raw, const uint8_t* __restrict__ img_g, uint32_t* tslot) {
+    uint8_t* base = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(raw) + 1023) & ~uintptr_t(1023));
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    const uint4* src = reinterpret_cast<const uint4*>(img_g);
+    uint4* dst = reinterpret_cast<uint4*>(base);
+    for (int t = tid; t < (int)(SG_IMG_BYTES / 16); t += nt) dst[t] = src[t];
+    SgTc c;
+    c.img = base;
+    c.A = base + SG_IMG_BYTES;
+    c.bar = reinterpret_cast<uint64_t*>(c.A + 2 * SG_TILE_BYTES);
+    c.phase = 0;
+    if (tid == 0) {
+        tc::mbar_init(c.bar, 1);
+        tc::fence_barrier_init();
+    }
+    if (tid < 32) tc::tmem_alloc(tslot, SG_TMEM_COLS);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    c.tmem = *tslot;
+    return c;
+}
+
+// Every MMA complete (bounded), then TMEM freed: the CTA's teardown (every thread).
+__device__ __forceinline__ void sg_tc_teardown(SgTc& c, int* err) {
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    if (tid == 0) {
+        tc::mma_commit(c.bar);
+        if (!tc::mbar_wait(c.bar, c.phase) && err) atomicExch(err, 9);
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (tid < 32) tc::tmem_dealloc(c.tmem, SG_TMEM_COLS);
+}
+
+// Row `row` of A tile `m` (128 BF16 values h[0..127] given as 64 packed pairs) into shared memory.
+__device__ __forceinline__ void sg_put_row(uint8_t* tile, int row, const uint32_t* h2) {
 #pragma unroll
-            for (int nt = 0; nt < 16; nt++) {
-                acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-                const int j = nt * 8 + g;
-                mma_bf16_16816(acc[nt], a0, w0u[(j * 16 + 2 * tq) / 2], w0u[(j * 16 + 2 * tq + 8) / 2]);
-            }
+    for (int u = 0; u < 16; u++) {  // 16-byte units of 8 values: K = 8 u .. 8 u + 7
+        const int k = 8 * u;
+        *reinterpret_cast<uint4*>(tile + sg_sw_off(SG_H, row, k)) =
+            make_uint4(h2[4 * u], h2[4 * u + 1], h2[4 * u + 2], h2[4 * u + 3]);
+    }
+}
+
+__device__ __forceinline__ float silu_fast(float z) { return __fdividef(z, 1.f + __expf(-z)); }
+
+// One pass of the network for the CTA's 256 threads (thread t: tile t / 128, row t % 128; the warps
+// of a tile are the four TMEM lane quarters): inputs (u, v) of the thread's sample, out6 its six
+// de-standardized outputs.  Every thread of the CTA calls it.  false when an MMA wait timed out.
+__device__ bool sg_tc_forward(SgTc& c, float u, float v, float* out6) {
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int m = tid >> 7, row = tid & 127, quad = (tid >> 5) & 3;
+    uint8_t* tile = c.A + (size_t)m * SG_TILE_BYTES;
+    const float* f = reinterpret_cast<const float*>(c.img + SG_IMG_F);
+    const float* W0 = f + SG_F_W0;
+    const float* bias = f + SG_F_B;
+    bool ok = true;
+    // layer 0 on the CUDA cores (inputs rounded to BF16 as in training; w = 0)
+    {
+        const float ub = bf16r(u), vb = bf16r(v);
+        uint32_t h2[64];
 #pragma unroll
-            for (int kt = 0; kt < 8; kt++) {
-                const int c0 = (2 * kt) * 8 + 2 * tq, c1 = (2 * kt + 1) * 8 + 2 * tq;
-                a[kt][0] = pack_bf16(silu(acc[2 * kt][0] + bias[c0]), silu(acc[2 * kt][1] + bias[c0 + 1]));
-                a[kt][1] = pack_bf16(silu(acc[2 * kt][2] + bias[c0]), silu(acc[2 * kt][3] + bias[c0 + 1]));
-                a[kt][2] = pack_bf16(silu(acc[2 * kt + 1][0] + bias[c1]), silu(acc[2 * kt + 1][1] + bias[c1 + 1]));
-                a[kt][3] = pack_bf16(silu(acc[2 * kt + 1][2] + bias[c1]), silu(acc[2 * kt + 1][3] + bias[c1 + 1]));
-            }
+        for (int j2 = 0; j2 < 64; j2++) {
+            const int j = 2 * j2;
+            const float z0 = fmaf(W0[3 * j], ub, fmaf(W0[3 * j + 1], vb, bias[j]));
+            const float z1 = fmaf(W0[3 * j + 3], ub, fmaf(W0[3 * j + 4], vb, bias[j + 1]));
+            h2[j2] = pack_bf16(silu_fast(z0), silu_fast(z1));
         }
-#pragma unroll 1
-        for (int l = 0; l < 3; l++) {
-            const uint32_t* W = whu + (size_t)l * SG_H * SG_LD / 2;
-            float acc[16][4];
+        sg_put_row(tile, row, h2);
+    }
+    const uint32_t taccum = c.tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)m * SG_H;
+    for (int l = 1; l <= 4; l++) {
+        tc::fence_proxy_async_smem();  // the A rows written by this thread, visible to the tensor core
+        __syncthreads();
+        if (tid == 0) {
+            tc::tc_fence_after();
+            const bool last = l == 4;
+            const uint32_t idesc = last ? sg_idesc_bf16(128, 16) : sg_idesc_bf16(128, SG_H);
+            const uint8_t* B = last ? c.img + SG_IMG_W4 : c.img + (size_t)(l - 1) * SG_TILE_BYTES;
+            const int brows = last ? 16 : SG_H;
+            for (int mm = 0; mm < 2; mm++) {
+                const uint32_t a0 = tc::smem_u32(c.A + (size_t)mm * SG_TILE_BYTES), b0 = tc::smem_u32(B);
+                const uint32_t d = c.tmem + (last ? 256u + 32u * mm : (uint32_t)mm * SG_H);
 #pragma unroll
-            for (int nt = 0; nt < 16; nt++) {
-                acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-                const int j = nt * 8 + g;
-#pragma unroll
-                for (int kt = 0; kt < 8; kt++)
-                    mma_bf16_16816(acc[nt], a[kt], W[(j * SG_LD + kt * 16 + 2 * tq) / 2],
-                                   W[(j * SG_LD + kt * 16 + 2 * tq + 8) / 2]);
+                for (int kk = 0; kk < SG_H / 16; kk++) {
+                    const uint32_t ko = (uint32_t)(kk / 4) * 128u * 128u + (uint32_t)(kk % 4) * 32u;
+                    const uint32_t kb = (uint32_t)(kk / 4) * (uint32_t)brows * 128u + (uint32_t)(kk % 4) * 32u;
+                    tc::mma_f16(d, tc::desc_kmajor_sw128(a0 + ko), tc::desc_kmajor_sw128(b0 + kb), idesc, kk > 0);
+                }
             }
-            const float* b = bias + (l + 1) * SG_H;
-#pragma unroll
-            for (int kt = 0; kt < 8; kt++) {
-                const int c0 = (2 * kt) * 8 + 2 * tq, c1 = (2 * kt + 1) * 8 + 2 * tq;
-                a[kt][0] = pack_bf16(silu(acc[2 * kt][0] + b[c0]), silu(acc[2 * kt][1] + b[c0 + 1]));
-                a[kt][1] = pack_bf16(silu(acc[2 * kt][2] + b[c0]), silu(acc[2 * kt][3] + b[c0 + 1]));
-                a[kt][2] = pack_bf16(silu(acc[2 * kt + 1][0] + b[c1]), silu(acc[2 * kt + 1][1] + b[c1 + 1]));
-                a[kt][3] = pack_bf16(silu(acc[2 * kt + 1][2] + b[c1]), silu(acc[2 * kt + 1][3] + b[c1 + 1]));
-            }
+            tc::mma_commit(c.bar);
         }
-        float o[4] = {0.f, 0.f, 0.f, 0.f};
+        const bool done = tc::mbar_wait(c.bar, c.phase);
+        c.phase ^= 1u;
+        ok = ok && done;
+        tc::tc_fence_after();
+        if (l < 4) {  // bias, SiLU, BF16: the next layer's A row
+            const float* b = bias + l * SG_H;
+            uint32_t h2[64];
 #pragma unroll
-        for (int kt = 0; kt < 8; kt++)
-            mma_bf16_16816(o, a[kt], w4u[(g * SG_LD + kt * 16 + 2 * tq) / 2], w4u[(g * SG_LD + kt * 16 + 2 * tq + 8) / 2]);
-        // row r of the tile (lane mt * 16 + r) holds column c at lane 4 (r % 8) + c / 2, register
-        // (c % 2) + 2 (r / 8)
-        const int r = lane - mt * 16;
+            for (int q = 0; q < 4; q++) {
+                float acc[32];
+                tc::tmem_ld32(taccum + 32 * q, acc);
 #pragma unroll
-        for (int c = 0; c < SG_OUT; c++) {
-            const int src = 4 * (r & 7) + c / 2;
-            const float lo = __shfl_sync(0xffffffffu, o[c & 1], src & 31);
-            const float hi = __shfl_sync(0xffffffffu, o[2 + (c & 1)], src & 31);
-            if (r >= 0 && r < 16) out6[c] = nm[c] + nm[SG_OUT + c] * ((r < 8 ? lo : hi) + bias[4 * SG_H + c]);
+                for (int e = 0; e < 16; e++)
+                    h2[16 * q + e] = pack_bf16(silu_fast(acc[2 * e] + b[32 * q + 2 * e]),
+                                               silu_fast(acc[2 * e + 1] + b[32 * q + 2 * e + 1]));
+            }
+            tc::tc_fence_before();
+            sg_put_row(tile, row, h2);
+        } else {
+            float acc[32];
+            tc::tmem_ld32(c.tmem + ((uint32_t)(quad * 32) << 16) + 256u + 32u * m, acc);
+            const float* nm = f + SG_F_N;
+#pragma unroll
+            for (int q = 0; q < SG_OUT; q++) out6[q] = nm[q] + nm[SG_OUT + q] * (acc[q] + bias[4 * SG_H + q]);
+            tc::tc_fence_before();
         }
     }
+    __syncthreads();  // every accumulator read before a later pass's MMAs overwrite TMEM
+    return ok;
+}
+
+// out [n][6] (FP32, de-standardized) from inputs [n][3]: persistent CTAs of 256 threads, 256 samples
+// a pass.  err (may be null) set to 9 if an MMA wait timed out.
+__global__ void __launch_bounds__(256, 1) k_sg_infer_tc(int n, const uint8_t* __restrict__ img_g,
+                                                        const float* __restrict__ in, float* __restrict__ out,
+                                                        int* __restrict__ err) {
+    extern __shared__ uint8_t sg_raw[];
+    __shared__ uint32_t tslot;
+    SgTc c = sg_tc_setup(sg_raw, img_g, &tslot);
+    const int tid = threadIdx.x;
+    bool ok = true;
+    for (int s0 = blockIdx.x * 256; s0 < n; s0 += gridDim.x * 256) {
+        const int i = s0 + tid;
+        const float u = i < n ? in[3 * (size_t)i] : 0.f, v = i < n ? in[3 * (size_t)i + 1] : 0.f;
+        float o[SG_OUT];
+        ok = sg_tc_forward(c, u, v, o) && ok;
+        if (i < n)
+#pragma unroll
+            for (int q = 0; q < SG_OUT; q++) out[(size_t)i * SG_OUT + q] = o[q];
+    }
+    if (!ok && err) atomicExch(err, 9);
+    sg_tc_teardown(c, err);
 }
 
 // The wave term from the network's outputs: the logarithmic part in closed form (J0, J1 from the
-// 1-D table), the regular part and the imaginary part from the network, FY by the identity
+// 1-D table below X = 30, the Hankel asymptotics above), the regular part and the imaginary part from the network, FY by the identity
 // FY = -F - 2 / R0.
 __device__ inline Wave sg_wave(double X, double Y, const float* o) {
-    double f[4];
-    table1d(X, f);
-    const double j0 = f[0], j1 = f[1], eY = exp(-Y), R0 = sqrt(X * X + Y * Y);
+    double j0, j1;
+    bessel_j01<false>(X, j0, j1);
+    const double eY = exp(-Y), R0 = sqrt(X * X + Y * Y);
     const double lg = log(Y + R0) + (GAMMA - LOG2);
     Wave w;
     w.F = -2.0 * eY * j0 * lg + (double)o[0];
@@ -545,24 +531,22 @@ __device__ inline Wave sg_wave(double X, double Y, const float* o) {
     return w;
 }
 
-// The mixed-form assembly with the network as the wave term inside its domain (X, Y < 30, R0 > 0;
-// the tables outside): persistent CTAs (the weight image is loaded once per CTA), work items
-// (tile pair, frequency) taken round-robin; the per-item work is k_assemble's.
+// The mixed-form assembly with the network as the wave term inside its domain (X < 100, Y < 50,
+// R0 > 0; the tables and series outside): persistent CTAs (the weight image loaded once per CTA, TMEM
+// held for the launch), work items (tile pair, frequency) taken round-robin; the per-item work is
+// k_assemble's, the network run for the CTA's 256 pairs of each row group at once.
 template <bool FINITE>
 __global__ void __launch_bounds__(256, 1) k_assemble_sg(PanelsView pv, const double* __restrict__ st,
                                                        const FreqInfo* __restrict__ fi, const FdParams* __restrict__ fdp,
                                                        const float* __restrict__ tiles, const double* __restrict__ fpt,
                                                        OutF32 out, int F, const uint8_t* __restrict__ img_g,
-                                                       unsigned long long* __restrict__ counts) {
-    extern __shared__ __align__(16) uint8_t img[];
+                                                       unsigned long long* __restrict__ counts, int* __restrict__ err) {
+    extern __shared__ uint8_t sg_raw[];
     __shared__ double sT[4][32][33];
+    __shared__ uint32_t tslot;
     if (pv.invalid()) return;  // invalid panels: the solve reports them
-    {
-        const uint4* src = reinterpret_cast<const uint4*>(img_g);
-        uint4* dst = reinterpret_cast<uint4*>(img);
-        for (int t = threadIdx.y * 32 + threadIdx.x; t < (int)(SG_IMG_BYTES / 16); t += 256) dst[t] = src[t];
-    }
-    __syncthreads();
+    SgTc c = sg_tc_setup(sg_raw, img_g, &tslot);
+    bool ok = true;
     const int N = pv.N;
     const int nt = (N + 31) / 32, ntp = nt * (nt + 1) / 2;
     const size_t NN = (size_t)N * N;
@@ -616,13 +600,12 @@ __global__ void __launch_bounds__(256, 1) k_assemble_sg(PanelsView pv, const dou
             double dx = xk[0] - xn[0], dy = xk[1] - xn[1];
             double R = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
             const double X = K * R, Y = -K * (xk[2] + xn[2]);
-            const bool inb = live && X < SG_XMAX && Y < SG_XMAX && (X > 0.0 || Y > 0.0);
+            const bool inb = live && X < SG_XMAX && Y < SG_YMAX && (X > 0.0 || Y > 0.0);
             float o6[SG_OUT] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            __syncwarp();
-            if (__any_sync(0xffffffffu, inb)) {
+            if (__syncthreads_or(inb)) {  // the CTA's 256 pairs through the network at once
                 float in3[3];
                 sg_inputs(X, Y, in3);
-                sg_warp_mlp(img, in3[0], in3[1], o6);
+                ok = sg_tc_forward(c, in3[0], in3[1], o6) && ok;
             }
             if (!live) continue;
             used += inb;
@@ -663,6 +646,8 @@ __global__ void __launch_bounds__(256, 1) k_assemble_sg(PanelsView pv, const dou
     // pairs whose wave term came from the network
     for (int o = 16; o > 0; o >>= 1) used += __shfl_xor_sync(0xffffffffu, used, o);
     if ((threadIdx.x & 31) == 0) atomicAdd(counts, used);
+    if (!ok) atomicExch(err, 9);
+    sg_tc_teardown(c, err);
 }
 
 void launch_sg_pack(const float* params_norm, uint8_t* img, cudaStream_t s) {
@@ -673,17 +658,17 @@ size_t sg_image_bytes() { return SG_IMG_BYTES; }
 
 void launch_assemble_f32_sg(const PanelsView& pv, const double* st, int F, const FreqInfo* fi, const FdParams* fd,
                             const float* tiles, const double* fpt, bool finite, float* S, float* A, int Np,
-                            const uint8_t* img, unsigned long long* counts, cudaStream_t s) {
+                            const uint8_t* img, unsigned long long* counts, int* err, cudaStream_t s) {
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     OutF32 o{S, A, 2 * (size_t)Np * Np, Np};
     if (finite) {
-        cudaFuncSetAttribute(k_assemble_sg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG_IMG_BYTES);
-        k_assemble_sg<true><<<nsm, dim3(32, 8), SG_IMG_BYTES, s>>>(pv, st, fi, fd, tiles, fpt, o, F, img, counts);
+        cudaFuncSetAttribute(k_assemble_sg<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG_TC_SMEM);
+        k_assemble_sg<true><<<nsm, dim3(32, 8), SG_TC_SMEM, s>>>(pv, st, fi, fd, tiles, fpt, o, F, img, counts, err);
     } else {
-        cudaFuncSetAttribute(k_assemble_sg<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG_IMG_BYTES);
-        k_assemble_sg<false><<<nsm, dim3(32, 8), SG_IMG_BYTES, s>>>(pv, st, fi, fd, tiles, fpt, o, F, img, counts);
+        cudaFuncSetAttribute(k_assemble_sg<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG_TC_SMEM);
+        k_assemble_sg<false><<<nsm, dim3(32, 8), SG_TC_SMEM, s>>>(pv, st, fi, fd, tiles, fpt, o, F, img, counts, err);
     }
 }
 
@@ -815,8 +800,22 @@ int surrogate_train(int64_t n_train, int batch, int steps, double lr0, uint64_t 
         hn[SG_OUT + c] = (float)hs[c];
     }
     cudaMemcpyAsync(dn, hn, sizeof hn, cudaMemcpyHostToDevice, s);
-    cudaFuncSetAttribute(k_sg_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG_SMEM);
-    k_sg_infer<<<148, 256, SG_SMEM, s>>>((int)n_val, tr.p, dn, vin, vout);
+    DevArr dimg, derr;
+    uint8_t* img = dimg.alloc<uint8_t>(SG_IMG_BYTES);
+    int* ierr = derr.alloc<int>(1);
+    if (!img || !ierr) {
+        *msg = "surrogate training: device allocation failed";
+        return HB_ERR_INTERNAL;
+    }
+    cudaMemsetAsync(ierr, 0, sizeof(int), s);
+    k_sg_pack<<<64, 256, 0, s>>>(tr.p, dn, img);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(k_sg_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG_TC_SMEM);
+    k_sg_infer_tc<<<nsm, 256, SG_TC_SMEM, s>>>((int)n_val, img, vin, vout, ierr);
+    int herr = 0;
+    cudaMemcpyAsync(&herr, ierr, sizeof(int), cudaMemcpyDeviceToHost, s);
     std::vector<float> ho((size_t)n_val * SG_OUT);
     std::vector<double> hv((size_t)n_val * SG_OUT);
     cudaMemcpyAsync(ho.data(), vout, ho.size() * 4, cudaMemcpyDeviceToHost, s);
@@ -825,8 +824,8 @@ int surrogate_train(int64_t n_train, int batch, int steps, double lr0, uint64_t 
     cudaStreamSynchronize(s);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (cudaGetLastError() != cudaSuccess) {
-        *msg = "CUDA error in surrogate training";
+    if (cudaGetLastError() != cudaSuccess || herr != 0) {
+        *msg = herr ? "surrogate training: a tensor-core wait of the validation timed out" : "CUDA error in surrogate training";
         return HB_ERR_INTERNAL;
     }
     for (int c = 0; c < 2 * SG_OUT; c++) norm_out[c] = hn[c];
@@ -905,7 +904,16 @@ int surrogate_eval(const float* params, const float* norm, int n, const double* 
     cudaMemcpy(x, xy, (size_t)n * 16, cudaMemcpyHostToDevice);
     cudaMemcpy(p, params, SG_PARAMS * 4, cudaMemcpyHostToDevice);
     cudaMemcpy(nm, norm, 2 * SG_OUT * 4, cudaMemcpyHostToDevice);
-    cudaFuncSetAttribute(k_sg_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG_SMEM);
+    DevArr dimg, derr;
+    uint8_t* img = dimg.alloc<uint8_t>(SG_IMG_BYTES);
+    int* ierr = derr.alloc<int>(1);
+    if (!img || !ierr) {
+        *msg = "device allocation failed";
+        return HB_ERR_INTERNAL;
+    }
+    cudaMemset(ierr, 0, sizeof(int));
+    k_sg_pack<<<64, 256>>>(p, nm, img);
+    cudaFuncSetAttribute(k_sg_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SG_TC_SMEM);
     int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -926,7 +934,7 @@ int surrogate_eval(const float* params, const float* norm, int n, const double* 
     // the network's time includes forming its inputs from (X, Y)
     ms2[0] = timed([&] {
         k_sg_inputs<<<nb, 256>>>(n, x, in);
-        k_sg_infer<<<2 * nsm, 256, SG_SMEM>>>(n, p, nm, in, o);
+        k_sg_infer_tc<<<nsm, 256, SG_TC_SMEM>>>(n, img, in, o, ierr);
     });
     ms2[1] = timed([&] { k_sg_table<<<nb, 256>>>(n, x, tg); });
     cudaEventDestroy(e0);
@@ -937,8 +945,10 @@ int surrogate_eval(const float* params, const float* norm, int n, const double* 
         for (size_t i = 0; i < h.size(); i++) out_net[i] = h[i];
     }
     if (out_table) cudaMemcpy(out_table, tg, (size_t)n * SG_OUT * 8, cudaMemcpyDeviceToHost);
-    if (cudaGetLastError() != cudaSuccess) {
-        *msg = "CUDA error in the surrogate evaluation";
+    int herr = 0;
+    cudaMemcpy(&herr, ierr, sizeof(int), cudaMemcpyDeviceToHost);
+    if (cudaGetLastError() != cudaSuccess || herr != 0) {
+        *msg = herr ? "a tensor-core wait of the surrogate evaluation timed out" : "CUDA error in the surrogate evaluation";
         return HB_ERR_INTERNAL;
     }
     return 0;

@@ -471,7 +471,7 @@ def surrogate_grad(params, inputs, targets):
 
 
 def surrogate_eval(params, norm, xy):
-    """(network [n][6], table [n][6], (ms network, ms table)) at points xy [n][2] in [0, 30)^2."""
+    """(network [n][6], table [n][6], (ms network, ms table)) at points xy [n][2] in [0, 100) x [0, 50)."""
     fpp = ctypes.POINTER(ctypes.c_float)
     p = np.ascontiguousarray(params, np.float32)
     nm = np.ascontiguousarray(norm, np.float32)

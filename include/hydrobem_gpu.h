@@ -296,9 +296,10 @@ HbStatus hbg_debug_lu_f64(int32_t n, int32_t batch, const double *A, int32_t nrh
 HbStatus hbg_measure_peaks(double *out3);
 
 /* ---- the learned part: an MLP surrogate of the regular part of the infinite-depth wave term
- * (inputs X = K R, Y = -K (z + zeta) in [0, 30)^2, log-scaled, and 1 / (K h) = 0; outputs g, g_X, g_Y
- * with g = F + 2 e^-Y J0(X) (log(Y + R0) + gamma - log 2), and I, I_X, I_Y), 3 -> 128 x 4 -> 6,
- * SiLU, BF16 weights, FP32 accumulation.  No counterpart in the reference (it replaces the table
+ * (inputs X = K R in [0, 100), Y = -K (z + zeta) in [0, 50), log-scaled, and a third input 0; outputs
+ * g, g_X, g_Y with g = F + 2 e^-Y J0(X) (log(Y + R0) + gamma - log 2), and I, I_X, I_Y),
+ * 3 -> 128 x 4 -> 6, SiLU, BF16 weights, FP32 accumulation, evaluated by tcgen05.mma (TMEM
+ * accumulators).  No counterpart in the reference (it replaces the table
  * evaluation of green_inf.rs:316-368 inside its domain, the table remaining the fallback and the
  * judge of its error).  params: 50822 floats; norm: 12 floats (means, spreads of the outputs). */
 
@@ -316,7 +317,7 @@ HbStatus hbg_surrogate_grad(const float *params, int32_t n, const float *inputs,
                             double *loss);
 
 /* The network (tensor cores) and the table evaluation at the same n points xy [n][2] = (X, Y) in
- * [0, 30)^2: out_net, out_table [n][6] (either may be NULL); ms2 = device milliseconds of each over
+ * [0, 100) x [0, 50): out_net, out_table [n][6] (either may be NULL); ms2 = device milliseconds of each over
  * the n points (points resident on the device). */
 HbStatus hbg_surrogate_eval(const float *params, const float *norm, int32_t n, const double *xy, double *out_net,
                             double *out_table, double *ms2);

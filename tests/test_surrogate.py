@@ -1,6 +1,9 @@
 """The learned part: the wave-term surrogate's training kernels against a CPU computation of the same
-network (gradients), its training on the library's own table evaluation, and what the trained network
-gains, or loses, against the table evaluation it would replace (device time per evaluation, error)."""
+network (gradients), its training on 2^22 samples of the library's own table and series evaluation
+over X = K R < 100, Y = -K (z + zeta) < 50, its inference on the tensor cores (tcgen05.mma, TMEM
+accumulators), and a measured comparison with the table evaluation it would replace: device time per
+evaluation and error on the same points, then assembly time and A, B, X error of the three-cylinder
+array solved with each."""
 
 from __future__ import annotations
 
@@ -90,18 +93,29 @@ def test_training_gradients_match_cpu():
             assert err < 2e-3, (l, a, err)
 
 
+XMAX, YMAX = 100.0, 50.0  # the trained domain
+
+
+def domain_points(rng, n):
+    """n points log-spaced over the trained domain, as the training samples are."""
+    u = rng.uniform(0.0, 1.0, (n, 2))
+    return np.column_stack([np.expm1(u[:, 0] * np.log1p(XMAX)), np.expm1(u[:, 1] * np.log1p(YMAX))])
+
+
 @pytest.fixture(scope="module")
 def trained():
-    return nv.surrogate_train(n_train=1 << 18, batch=4096, steps=1500, lr=2e-3, seed=3, n_val=1 << 14)
+    return nv.surrogate_train(n_train=1 << 22, batch=8192, steps=3000, lr=2e-3, seed=3, n_val=1 << 15)
 
 
 def test_training_fits_the_table(trained):
     p, nm, rep = trained
     assert np.isfinite(p).all()
-    assert rep["loss_last"] < 0.02 * rep["loss_first"], rep
-    # a BF16 network: percent-level agreement with the table, far from the 1e-5 of the solve
+    assert rep["loss_last"] < 0.1 * rep["loss_first"], rep
+    # a BF16 network of 50 822 parameters over X < 100, Y < 50 (J0(X) oscillates sixteen times there):
+    # agreement with the table at the level of a few to thirty percent of each output's spread, four
+    # orders of magnitude from the 1e-5 of the solve
     for k, v in rep["val_rms_over_spread"].items():
-        assert v < 0.2, (k, rep)
+        assert v < 0.5, (k, rep)
 
 
 def test_network_against_the_table_it_would_replace(trained):
@@ -110,7 +124,7 @@ def test_network_against_the_table_it_would_replace(trained):
     p, nm, rep = trained
     rng = np.random.default_rng(11)
     n = 1 << 20
-    xy = np.expm1(rng.uniform(0.0, 1.0, (n, 2)) * np.log(31.0))
+    xy = domain_points(rng, n)
     net, tab, (ms_net, ms_tab) = nv.surrogate_eval(p, nm, xy)
     assert np.isfinite(net).all() and np.isfinite(tab).all()
     assert ms_net > 0 and ms_tab > 0
@@ -128,8 +142,9 @@ def test_network_against_the_table_it_would_replace(trained):
 
 def test_points_outside_the_trained_domain_are_refused(trained):
     p, nm, _ = trained
-    with pytest.raises(nv.HydroBEMError):
-        nv.surrogate_eval(p, nm, np.array([[31.0, 1.0]]))
+    for pt in ([101.0, 1.0], [5.0, 51.0], [-1.0, 1.0]):
+        with pytest.raises(nv.HydroBEMError):
+            nv.surrogate_eval(p, nm, np.array([pt]))
 
 
 def _scaled_error(got, ref, floor=1e-3):
@@ -138,24 +153,38 @@ def _scaled_error(got, ref, floor=1e-3):
     return float((np.abs(np.asarray(got) - ref) / scale).max())
 
 
-@pytest.mark.parametrize("depth", [math.inf, 3.0])
-def test_network_as_the_wave_term_of_the_mixed_assembly(trained, depth):
-    """The mixed solve with the network inside the assembly: it serves the pairs of its domain, the
-    solve stays finite, and A, B, X move from the table solve by the network's own error, far above
-    the 1e-5 of the solve -- which is why the tables stay the default."""
+def _assembly_ms():
+    return nv.last_profile()["assembly"]
+
+
+def test_network_against_the_table_on_the_three_cylinder_array(trained):
+    """The measured comparison on the three interacting cylinders (the array of the benchmark cases at
+    a quarter of its panels, infinite depth, four frequencies K a = 0.1 .. 2): the same mixed solve
+    with the table evaluation and with the network as the wave term.  Measured: the assembly phase of
+    each (the network's FLOPs per pair, 1.006e5, bound it from below at the tensor-core peak), and the
+    A, B, X error of each against the FP64 form.  The table meets the 1e-5 bar and the network does
+    not: its error is its own (percent level), which is why the table stays the default."""
     p, nm, _ = trained
-    v = meshes.cylinder(1.0, 0.5, 32, 8, 8)
-    omegas = 2.0 * math.pi / np.array([2.0, 4.0, 8.0])
-    ref = nv.solve(v, omegas, [0.0], depth=depth, precision=nv.HBG_MIXED)
-    assert nv.last_surrogate_pairs() == 0
-    got = nv.solve(v, omegas, [0.0], depth=depth, precision=nv.HBG_MIXED, surrogate=nv.surrogate_blob(p, nm))
-    used = nv.last_surrogate_pairs()
+    v, body, centers = meshes.cylinder_array(32, 16, 16)
+    omegas = np.sqrt(np.array([0.1, 0.5, 1.0, 2.0]) * meshes.GRAVITY)
+    kw = dict(panel_body=body, rotation_centers=centers)
+    ref = nv.solve(v, omegas, [0.0], precision=nv.HBG_FP64, **kw)
+    times = {}
+    for name, sg in (("table", None), ("network", nv.surrogate_blob(p, nm))):
+        extra = {} if sg is None else {"surrogate": sg}
+        nv.solve(v, omegas, [0.0], precision=nv.HBG_MIXED, **kw, **extra)  # warm-up
+        got = nv.solve(v, omegas, [0.0], precision=nv.HBG_MIXED, **kw, **extra)
+        times[name] = (_assembly_ms(), nv.last_surrogate_pairs(),
+                       {k: _scaled_error(got[k], ref[k]) for k in ("A", "B", "X")})
+    (t_tab, n_tab, e_tab), (t_net, n_net, e_net) = times["table"], times["network"]
     N = len(v)
-    assert 0 < used <= len(omegas) * N * (N + 1) // 2
-    errs = {k: _scaled_error(got[k], ref[k]) for k in ("A", "B", "X")}
-    assert all(np.isfinite(got[k]).all() for k in ("A", "B", "X"))
-    assert max(errs.values()) < 1.0, errs
-    print(f"\nnetwork in the assembly (depth {depth}): {used} pairs; error vs the table solve {errs}")
+    assert n_tab == 0 and 0 < n_net <= len(omegas) * N * (N + 1) // 2
+    assert t_tab > 0 and t_net > 0
+    assert max(e_tab.values()) <= 1e-5, e_tab
+    assert all(np.isfinite(x) for x in e_net.values())
+    assert max(e_net.values()) > max(e_tab.values()), (e_net, e_tab)
+    print(f"\nthree-cylinder array, {N} panels, {len(omegas)} frequencies: assembly {t_tab:.2f} ms (table) "
+          f"vs {t_net:.2f} ms (network, {n_net} pairs); error vs FP64 table {e_tab} network {e_net}")
 
 
 def test_network_refused_in_the_fp64_form(trained):
