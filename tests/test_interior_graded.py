@@ -151,7 +151,7 @@ def test_gpu_graded_interior_through_the_model_abi(golden, precision, tol):
         m.add("bodies", "body")
         m.text("bodies/body", "mesh", "cyl")
         m.text("bodies/body", "interior_surface", "graded")
-        m.text("options", "precision", precision)
+        m.text("options", "gpu_precision", precision)
         m.reals("environment", "omegas", golden["omegas"])
         m.reals("environment", "headings", golden["headings"])
         res = m.solve()
