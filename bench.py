@@ -47,6 +47,8 @@ DRAM_TRAFFIC = {("mixed", "assemble"): 32.5e9}
 
 CASE_LABELS = {
     "c2": WORKLOAD,
+    "c1": "cylinder r=1 m d=0.5 m, 512 panels (32x8 side + 32x8 bottom), infinite depth, 10 periods 2-11 s, "
+          "heading 0 deg",
     "medium": "cylinder r=1 m d=0.5 m, 4096 panels, h=5 m, 8 periods 1.5-20 s, 4 headings (profiling cut)",
     "small": "cylinder r=1 m d=0.5 m, 2048 panels (32x16 side + 32x16 bottom), h=5 m, 4 periods 1.5-20 s, "
              "4 headings (profiling cut)",
@@ -60,7 +62,12 @@ CASE_LABELS = {
 }
 # one-body cases: with N GPUs every rank solves its own copy of the job (weak scaling); the others are
 # fixed workloads whose (body, frequency) units are split over the ranks (strong scaling)
-SINGLE_BODY = ("c2", "medium", "small", "tiny")
+SINGLE_BODY = ("c2", "c1", "medium", "small", "tiny")
+
+
+def case_depth_headings():
+    """(depth, headings in degrees) of a one-body case."""
+    return (math.inf, [0.0]) if CASE == "c1" else (DEPTH, HEADINGS)
 
 
 CASE = "c2"
@@ -78,6 +85,8 @@ def workload():
         return meshes.cylinder(1.0, 0.5, 64, 32, 32), 2.0 * math.pi / np.linspace(1.5, 20.0, 8)
     if CASE == "tiny":
         return meshes.cylinder(1.0, 0.5, 8, 2, 2), 2.0 * math.pi / np.linspace(1.5, 20.0, 3)
+    if CASE == "c1":
+        return meshes.cylinder(1.0, 0.5, 32, 8, 8), 2.0 * math.pi / np.arange(2.0, 12.0)
     v = meshes.cylinder(1.0, 0.5, 64, 32, 32)
     periods = np.linspace(1.5, 20.0, N_PERIODS)
     return v, 2.0 * math.pi / periods
@@ -89,7 +98,8 @@ def case_problems():
 
     if CASE in SINGLE_BODY:
         v, omegas = workload()
-        return [dict(vertices=v, omegas=omegas, headings_deg=HEADINGS)], DEPTH
+        depth, heads = case_depth_headings()
+        return [dict(vertices=v, omegas=omegas, headings_deg=heads)], depth
     if CASE == "c3":
         return [dict(vertices=v, omegas=om, headings_deg=[0.0, 45.0]) for v, om in meshes.uneven_bodies(64)], math.inf
     if CASE == "c4":
@@ -214,15 +224,16 @@ def cpu_job(production=True):
     from oracle import oracle as O
 
     v, omegas = workload()
-    heads = np.radians(HEADINGS)
+    depth, heads_deg = case_depth_headings()
+    heads = np.radians(heads_deg)
     O.lib()
     t0 = time.perf_counter()
     pan = O.make_panels(v)
     with O.ProductionMode(production):
-        st = O.statics(pan, None, DEPTH)
+        st = O.statics(pan, None, depth)
     t1 = time.perf_counter()
     for w in omegas:
-        O.solve_frequency(pan, None, st, DEPTH, w, heads, production=production)
+        O.solve_frequency(pan, None, st, depth, w, heads, production=production)
     t2 = time.perf_counter()
     return t2 - t0, t1 - t0, (t2 - t1) / len(omegas)
 
@@ -233,7 +244,7 @@ def cpu_reference(args, world, rank, pg):
     if rank != 0:
         return None
     if CASE not in SINGLE_BODY:
-        return {"impl": "reference", "unavailable": "the CPU reference arm times the one-body cases (c2, medium, "
+        return {"impl": "reference", "unavailable": "the CPU reference arm times the one-body cases (c2, c1, medium, "
                                                     "small, tiny)"}
     cores = host_cores()
     for _ in range(min(args.warmup, 1)):
@@ -244,7 +255,7 @@ def cpu_reference(args, world, rank, pg):
     value = F / job
     sample = (f"the whole job every step: statics ({np.mean([t[1] for t in times]):.2f} s) + all {F} frequencies "
               f"({np.mean([t[2] for t in times]):.3f} s each); {cores} threads on {cpu_model()}")
-    line = {"metric": "freq solves/s at N=4096", "value": value, "unit": "freq solves/s", "n_gpus": world,
+    line = {"metric": "freq solves/s at N=4096" if CASE == "c2" else "freq solves/s", "value": value, "unit": "freq solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": job * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c64+f32", "data": "synthetic",
             "config": {"workload": CASE_LABELS[CASE],
