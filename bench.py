@@ -209,10 +209,14 @@ def cpu_model():
 
 
 def host_cores():
+    """The threads the CPU baseline uses: OMP_NUM_THREADS when set (the oracle's OpenMP and OpenBLAS
+    follow it), else the cores this process may run on."""
     try:
-        return len(os.sched_getaffinity(0))
+        n = len(os.sched_getaffinity(0))
     except AttributeError:
-        return os.cpu_count()
+        n = os.cpu_count()
+    env = os.environ.get("OMP_NUM_THREADS", "")
+    return min(n, int(env)) if env.isdigit() and int(env) > 0 else n
 
 
 def cpu_job(production=True):
