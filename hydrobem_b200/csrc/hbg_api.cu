@@ -532,8 +532,11 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     Workspace& ws = workspace();
     WsBuf dverts(ws, WS_VERTS), dkind(ws, WS_KIND), dplanes(ws, WS_PLANES), dbad(ws, WS_BAD), dst(ws, WS_ST),
         dwork(ws, WS_WORK), dnwork(ws, WS_NWORK), dpbody(ws, WS_PBODY), drcen(ws, WS_RCEN), drig(ws, WS_RIGID),
-        dhyd(ws, WS_HYD);
+        dhyd(ws, WS_HYD), dtiers(ws, WS_TIERS);
     const bool multi = nbod > 1 && pr.body.panel_body;
+    // the mixed form with the reference's production statics rule: the panels' float32 Gauss tiers
+    const bool prod_statics = opt.precision == HBG_MIXED && opt.statics_rule == HBG_STATICS_PRODUCTION;
+    if (prod_statics) dtiers.alloc(sizeof(float) * TIER_FLOATS_HOST * (size_t)N);
     if (multi) dpbody.alloc(sizeof(int32_t) * N);
     if (pr.body.rotation_centers) drcen.alloc(sizeof(double) * 3 * nbod);
     // the rigid data [n_bodies][RIGID_PER_BODY] then the additional stiffness and damping (D x D each); the
@@ -599,11 +602,13 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         EventTimer t(s, &prof[0]);
         KernelProfiler& P = profiler();
         P.begin(s);
-        launch_panel_geometry(N, dverts.as<double>(), dkind.as<int32_t>(), dplanes.as<double>(), dbad.as<int32_t>(), s);
+        launch_panel_geometry(N, dverts.as<double>(), dkind.as<int32_t>(), dplanes.as<double>(), dbad.as<int32_t>(), s,
+                              prod_statics ? dtiers.as<float>() : nullptr);
         P.end(KF_GEOMETRY, 0.0, s);
         g_launches++;
         PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
         pv.G = G;
+        if (prod_statics) pv.tiers = dtiers.as<float>();
         if (hydro) {  // the hydrostatics and motion matrices of every body, once per problem
             if (rigid)
                 CUDA_OK(cudaMemcpyAsync(drig.p, rigid_host.data(), sizeof(double) * rigid_host.size(),
@@ -1003,6 +1008,7 @@ extern "C" void hbg_default_options(HbgOptions* opt) {
     opt->device = 0;
     opt->cancel = nullptr;
     opt->surrogate = nullptr;
+    opt->statics_rule = HBG_STATICS_ACCURATE;
 }
 
 extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_problems, const HbgOptions* opt) {
@@ -1022,6 +1028,11 @@ extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_proble
             return fail({HB_ERR_VALUE, "unknown precision form"});
         if (opt->surrogate && opt->precision != HBG_MIXED)
             return fail({HB_ERR_VALUE, "the wave-term network is an option of the mixed form only"});
+        if (opt->statics_rule != HBG_STATICS_ACCURATE && opt->statics_rule != HBG_STATICS_PRODUCTION)
+            return fail({HB_ERR_VALUE, "unknown statics rule"});
+        if (opt->statics_rule == HBG_STATICS_PRODUCTION && opt->precision != HBG_MIXED)
+            return fail({HB_ERR_UNSUPPORTED, "the production statics rule is an option of the mixed form (the FP64 "
+                                             "form is the reference's double-precision path)"});
         if (!(opt->gravity > 0.0) || !(opt->density > 0.0) || opt->log_tolerance < 0.0)
             return fail({HB_ERR_VALUE, "gravity and density must be positive, log_tolerance nonnegative"});
         int ndev = 0;
@@ -1151,9 +1162,15 @@ extern "C" HbStatus hbg_debug_matrices(const HbgBody* body, double omega, const 
         CUDA_OK(cudaMemcpy(dkind.p, kinds.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice));
         int32_t big = 0x7fffffff;
         CUDA_OK(cudaMemcpy(dbad.p, &big, sizeof big, cudaMemcpyHostToDevice));
-        launch_panel_geometry(N, dverts.as<double>(), dkind.as<int32_t>(), dplanes.as<double>(), dbad.as<int32_t>(), s);
+        // the statics by the reference's production rule on request; the matrices FP64 either way
+        const bool prod = opt->statics_rule == HBG_STATICS_PRODUCTION;
+        DevBuf dtiers;
+        if (prod) dtiers.alloc(sizeof(float) * TIER_FLOATS_HOST * (size_t)N);
+        launch_panel_geometry(N, dverts.as<double>(), dkind.as<int32_t>(), dplanes.as<double>(), dbad.as<int32_t>(), s,
+                              prod ? dtiers.as<float>() : nullptr);
         PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};
         pv.G = G;
+        if (prod) pv.tiers = dtiers.as<float>();
         const size_t NS = (size_t)Nm * N, NN = (size_t)Nm * Nm;
         dst.alloc(sizeof(double) * 4 * NS);
         const int cap = std::max(1 << 16, 16 * N);
@@ -1161,7 +1178,7 @@ extern "C" HbStatus hbg_debug_matrices(const HbgBody* body, double omega, const 
         dnwork.alloc(sizeof(int32_t));
         CUDA_OK(cudaMemset(dnwork.p, 0, sizeof(int32_t)));
         launch_statics(pv, depth, opt->logarithmic, opt->log_tolerance, dst.as<double>(), dwork.as<int32_t>(),
-                       dnwork.as<int32_t>(), cap, s);
+                       dnwork.as<int32_t>(), cap, s, prod);
         int32_t nwork = 0;
         CUDA_OK(cudaMemcpy(&nwork, dnwork.p, sizeof nwork, cudaMemcpyDeviceToHost));
         if (nwork > cap) return fail({HB_ERR_INTERNAL, "worklist overflow"});

@@ -84,6 +84,9 @@ struct PanelsView {
     // field points as the statics' rows instead of the sector's centroids: nrows points (x, y, z)
     const double* rows = nullptr;
     int nrows = 0;
+    // the mixed form: each panel's float32 Gauss tiers ([N][TIER_FLOATS]); the statics then follow the
+    // reference's production rule (null: its double-precision rule)
+    const float* tiers = nullptr;
     __device__ __forceinline__ bool invalid() const { return bad && *(volatile const int32_t*)bad != PANELS_VALID; }
     // generalized normal of rigid mode `mode` (body mode / 6: surge, sway, heave, roll, pitch, yaw about
     // its rotation centre) on panel j: zero on the panels of the other bodies

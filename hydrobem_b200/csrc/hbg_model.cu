@@ -71,6 +71,7 @@ struct HbModel {
     bool logarithmic = true;
     double log_tolerance = 1e-4;
     std::string precision = "fp64";
+    std::string statics_rule = "accurate";  // gpu_statics_rule: accurate or production (mixed form)
     int64_t device = 0;
     bool motion = false;
     bool field_pressure = false;
@@ -779,6 +780,12 @@ extern "C" HbStatus hb_set_text(HbModel* model, uint64_t object, const char* ite
             model->frequency_input = v;
             return HB_OK;
         }
+        if (object == OBJ_OPTIONS && it == "gpu_statics_rule") {
+            if (v != "accurate" && v != "production")
+                return refuse(HB_ERR_VALUE, "gpu_statics_rule is accurate or production");
+            model->statics_rule = v;
+            return HB_OK;
+        }
         if (object == OBJ_OPTIONS && it == "gpu_precision") {
             if (v != "fp64" && v != "mixed") return refuse(HB_ERR_VALUE, "gpu_precision is fp64 or mixed");
             model->precision = v;
@@ -884,6 +891,7 @@ extern "C" HbStatus hb_model_solve(HbModel* model, HbProgressFn progress, void* 
             }
             heads = model->headings;
             opt.precision = model->precision == "mixed" ? HBG_MIXED : HBG_FP64;
+            opt.statics_rule = model->statics_rule == "production" ? HBG_STATICS_PRODUCTION : HBG_STATICS_ACCURATE;
             opt.logarithmic = model->logarithmic;
             opt.log_tolerance = model->log_tolerance;
             opt.gravity = model->gravity;

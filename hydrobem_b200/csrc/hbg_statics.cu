@@ -39,8 +39,17 @@ __device__ __forceinline__ void bilinear(const double vt[4][3], double u, double
 }
 
 // ------------------------------------------------------------------ geometry
+// The reference's production rule of the Rankine integrals (panel_integrals.rs:190-216, 288-363): per
+// panel the float32 Gauss tiers of orders 3, 4, 5, 6 (points of the bilinear map relative to the
+// centroid, weights scaled to the exact area), each block padded with zero weights to a multiple of 8:
+// tier_len(t) points at tier_off(t), planes x, y, z, w of tier_len(t) floats each.
+constexpr int TIER_FLOATS = 416;
+static_assert(TIER_FLOATS == TIER_FLOATS_HOST, "the host's tier buffer size");
+__device__ __forceinline__ int tier_off(int t) { return t == 0 ? 0 : t == 1 ? 64 : t == 2 ? 128 : 256; }
+__device__ __forceinline__ int tier_len(int t) { return t <= 1 ? 16 : t == 2 ? 32 : 40; }
+
 __global__ void k_panel_geometry(int N, const double* __restrict__ verts, const int32_t* __restrict__ kind,
-                                 double* __restrict__ P, int32_t* __restrict__ bad) {
+                                 double* __restrict__ P, int32_t* __restrict__ bad, float* __restrict__ tiers) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= N) return;
     double raw[4][3];
@@ -180,6 +189,31 @@ __global__ void k_panel_geometry(int N, const double* __restrict__ verts, const 
             sum += gw[3 * i + k];
         }
     for (int k = 0; k < 9; k++) W(P_GW + k, gw[k] * (area / sum));
+    if (tiers) {
+        float* tb = tiers + (size_t)j * TIER_FLOATS;
+        for (int t = 0; t < 4; t++) {
+            const int n = 3 + t, len = tier_len(t);
+            float* b = tb + tier_off(t);
+            double wsum = 0.0;
+            for (int i = 0; i < n; i++)
+                for (int k = 0; k < n; k++) {
+                    double x[3], jac;
+                    bilinear(q, c_glx[n][i], c_glx[n][k], x, jac);
+                    wsum += c_glw[n][i] * c_glw[n][k] * jac;
+                }
+            for (int i = 0; i < n; i++)
+                for (int k = 0; k < n; k++) {
+                    double x[3], jac;
+                    bilinear(q, c_glx[n][i], c_glx[n][k], x, jac);
+                    const int e = i * n + k;
+                    b[e] = (float)(x[0] - cent[0]);
+                    b[len + e] = (float)(x[1] - cent[1]);
+                    b[2 * len + e] = (float)(x[2] - cent[2]);
+                    b[3 * len + e] = (float)(c_glw[n][i] * c_glw[n][k] * jac * area / wsum);
+                }
+            for (int e = n * n; e < len; e++) b[e] = b[len + e] = b[2 * len + e] = b[3 * len + e] = 0.f;
+        }
+    }
 }
 
 // ------------------------------------------------------------------ Rankine closed forms
@@ -209,11 +243,13 @@ __device__ __forceinline__ void load_panel(const PanelsView& pv, int j, PanelReg
     }
 }
 
-// panel_integrals.rs:226-275 (closed forms; beyond 1000 radii the 3 x 3 rule)
-__device__ inline void rankine(const PanelsView& pv, int j, const PanelRegs& p, const double* x, double& S, double& D) {
+// panel_integrals.rs:226-275 (closed forms; beyond `far` radii the 3 x 3 rule: 1000 in the reference's
+// double-precision mode, 12 in its production mode)
+__device__ inline void rankine(const PanelsView& pv, int j, const PanelRegs& p, const double* x, double& S, double& D,
+                               double far = 1000.0) {
     double rc[3] = {x[0] - p.c[0], x[1] - p.c[1], x[2] - p.c[2]};
     double dist = norm3(rc);
-    if (dist > 1000.0 * p.radius) {
+    if (dist > far * p.radius) {
         double s = 0.0, dd = 0.0;
         for (int k = 0; k < 9; k++) {
             double r[3];
@@ -330,21 +366,6 @@ __device__ __forceinline__ void rankine_gauss_f32(const PanelsView& pv, int j, c
     D = dd;
 }
 
-// Rankine integrals at x: the closed forms, or the FP32 rule for a far point (mixed form only).
-template <bool MIXED>
-__device__ __forceinline__ void rankine_at(const PanelsView& pv, int j, const PanelRegs& p, const double* x, double& S,
-                                           double& D) {
-    if constexpr (MIXED) {
-        const double t0 = x[0] - p.c[0], t1 = x[1] - p.c[1], t2 = x[2] - p.c[2];
-        const double far = MIX_FAR * p.radius;
-        if (t0 * t0 + t1 * t1 + t2 * t2 > far * far) {
-            rankine_gauss_f32(pv, j, p, x, S, D);
-            return;
-        }
-    }
-    rankine(pv, j, p, x, S, D);
-}
-
 // log_gauss with the integrand log(R - dz) and its normal derivative in FP32 (positions, weights and
 // sums in FP64): R - dz = R + |dz| for an image above the panel, so no cancellation.
 __device__ inline void log_gauss_f32(const PanelRegs& p, const double* image, int order, double& L, double& Ld) {
@@ -368,6 +389,88 @@ __device__ inline void log_gauss_f32(const PanelRegs& p, const double* image, in
     L = l;
     Ld = ld;
 }
+
+// ---- the reference's production rule (the mixed form)
+// panel_integrals.rs:288-300 rankine_tier: 0 (order 3) beyond 8 radii, 1 (order 4) from 4, 2 (order 5)
+// from 3, 3 (order 6) from 2; -1 (the closed forms) within 2
+__device__ __forceinline__ int rankine_tier(double r) {
+    return r >= 8.0 ? 0 : r >= 4.0 ? 1 : r >= 3.0 ? 2 : r >= 2.0 ? 3 : -1;
+}
+
+// panel_integrals.rs:305-357 rankine_gauss: the tier's rule in float32 on the point taken relative to the
+// centroid in double, eight accumulator lanes summed in double (the reference's lane order)
+__device__ inline void rankine_gauss_tier(const PanelRegs& p, const float* __restrict__ tq, const double* x, int t,
+                                          double& S, double& D) {
+    const int len = tier_len(t);
+    const float* b = tq + tier_off(t);
+    const float px = (float)(x[0] - p.c[0]), py = (float)(x[1] - p.c[1]), pz = (float)(x[2] - p.c[2]);
+    const float nx = (float)p.n[0], ny = (float)p.n[1], nz = (float)p.n[2];
+    float sacc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, dacc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    for (int k = 0; k < len; k += 8)
+#pragma unroll
+        for (int l = 0; l < 8; l++) {
+            const float rx = px - b[k + l], ry = py - b[len + k + l], rz = pz - b[2 * len + k + l];
+            const float w = b[3 * len + k + l];
+            const float r2 = __fmaf_rn(rz, rz, __fmaf_rn(rx, rx, ry * ry));
+            const float ir = 1.0f / sqrtf(r2);
+            const float nr = __fmaf_rn(nz, rz, __fmaf_rn(nx, rx, ny * ry));
+            sacc[l] = __fmaf_rn(w, ir, sacc[l]);
+            dacc[l] = __fmaf_rn(w * nr, ir * (ir * ir), dacc[l]);
+        }
+    double s = 0.0, d = 0.0;
+#pragma unroll
+    for (int l = 0; l < 8; l++) {
+        s += (double)sacc[l];
+        d += (double)dacc[l];
+    }
+    S = s;
+    D = d;
+}
+
+// Rankine integrals at x: with the tiers, panel_integrals.rs:359-363 rankine_any of the production mode
+// (the tiers, or the closed forms within 2 radii); the mixed form's own rule otherwise (the closed
+// forms, the FP32 3 x 3 rule beyond MIX_FAR radii); the FP64 form the closed forms.
+template <bool MIXED>
+__device__ __forceinline__ void rankine_at(const PanelsView& pv, int j, const PanelRegs& p, const double* x, double& S,
+                                           double& D) {
+    if constexpr (MIXED) {
+        const double t0 = x[0] - p.c[0], t1 = x[1] - p.c[1], t2 = x[2] - p.c[2];
+        if (pv.tiers) {  // the production rule
+            const double rc[3] = {t0, t1, t2};
+            const int t = rankine_tier(norm3(rc) / p.radius);
+            if (t >= 0) {
+                rankine_gauss_tier(p, pv.tiers + (size_t)j * TIER_FLOATS, x, t, S, D);
+                return;
+            }
+        } else {  // the mixed form's own rule: the closed forms within MIX_FAR radii
+            const double far = MIX_FAR * p.radius;
+            if (t0 * t0 + t1 * t1 + t2 * t2 > far * far) {
+                rankine_gauss_f32(pv, j, p, x, S, D);
+                return;
+            }
+        }
+    }
+    rankine(pv, j, p, x, S, D);
+}
+
+// panel_integrals.rs:380-392: in the production mode the log integral of an image farther than 12 radii
+// by the panel's 3 x 3 rule in double
+__device__ inline void log_far_3x3(const PanelsView& pv, int j, const PanelRegs& p, const double* image, double& L,
+                                   double& Ld) {
+    double l = 0.0, ld = 0.0;
+    for (int k = 0; k < 9; k++) {
+        const double xi[3] = {pv.at(P_GX + 3 * k, j), pv.at(P_GX + 3 * k + 1, j), pv.at(P_GX + 3 * k + 2, j)};
+        double psi, dpsi;
+        psi_terms(xi, image, p.n, psi, dpsi);
+        const double w = pv.at(P_GW + k, j);
+        l += w * psi;
+        ld += w * dpsi;
+    }
+    L = l;
+    Ld = ld;
+}
+
+__device__ __forceinline__ double to_f32(double v) { return (double)(float)v; }
 
 // lo_static.rs:47-55 log_pair
 __device__ __forceinline__ bool log_pair(const PanelRegs& p, const double* x, double tol) {
@@ -401,8 +504,9 @@ __device__ inline double log_in_plane(const PanelRegs& p, const double* x) {
 // One (row k, panel j) pair: rs, rd and (unless adaptive) dl, dd.  lo_static.rs:59-119
 // Four planes of Nr x N (rows k < Nr = N / G, the sector's points, or the Nr field points; every panel
 // j), entry at k + j Nr.
-// MIXED: the mixed form's variant (far Rankine points and the order-4 log rule in FP32, above); the
-// FP64 form runs the reference's arithmetic to the bit.
+// MIXED: the mixed form's variant (far Rankine points and the order-4 log rule in FP32, above; with
+// pv.tiers the reference's production rule instead, rows in float32); the FP64 form runs the reference's
+// double-precision arithmetic to the bit.
 template <bool MIXED>
 __global__ void __launch_bounds__(256, 2) k_statics(PanelsView pv, double depth, int logint, double tol,
                                                  double* __restrict__ st, int32_t* __restrict__ work,
@@ -428,14 +532,20 @@ __global__ void __launch_bounds__(256, 2) k_statics(PanelsView pv, double depth,
         double s2, d2, s4, d4, s5, d5, s6, d6;
         rankine_at<MIXED>(pv, j, p, p1, s2, d2);
         rankine_at<MIXED>(pv, j, p, p3, s4, d4);
-        rankine_at<MIXED>(pv, j, p, p4, s5, d5);
-        rankine_at<MIXED>(pv, j, p, p5, s6, d6);
+        if (MIXED && pv.tiers) {  // production: the two deep images by the 3 x 3 rule beyond 12 radii
+            rankine(pv, j, p, p4, s5, d5, 12.0);  // (lo_static.rs:82-88)
+            rankine(pv, j, p, p5, s6, d6, 12.0);
+        } else {
+            rankine_at<MIXED>(pv, j, p, p4, s5, d5);
+            rankine_at<MIXED>(pv, j, p, p5, s6, d6);
+        }
         sr += (s2 + s4) + s5 + s6;
         dr += (d2 + d4) + d5 + d6;
     }
+    const bool prod = MIXED && pv.tiers;  // the production rows are stored in float32
     size_t NN = (size_t)Nr * N, o = (size_t)k + (size_t)j * Nr;
-    st[o] = sr;
-    st[NN + o] = dr;
+    st[o] = prod ? to_f32(sr) : sr;
+    st[NN + o] = prod ? to_f32(dr) : dr;
     double dl = 0.0, dd = 0.0;
     bool use_log = logint && log_pair(p, x, tol);
     if (use_log && pv.kind[j] == 1 && x[2] == 0.0) {
@@ -444,10 +554,14 @@ __global__ void __launch_bounds__(256, 2) k_statics(PanelsView pv, double depth,
         double Rr = norm3(t);
         dl = Rr > 0.0 ? L - p.area * log(Rr) : L;
     } else if (use_log) {
-        int order = log_order(p, xb);
+        const double tb[3] = {xb[0] - p.c[0], xb[1] - p.c[1], xb[2] - p.c[2]};
+        const bool far3 = prod && norm3(tb) > 12.0 * p.radius;
+        int order = far3 ? 3 : log_order(p, xb);
         if (order > 0) {
             double L, Ld, psi, dpsi;
-            if (MIXED && order == 4)
+            if (far3)
+                log_far_3x3(pv, j, p, xb, L, Ld);
+            else if (MIXED && !prod && order == 4)
                 log_gauss_f32(p, xb, order, L, Ld);
             else
                 log_gauss(p, xb, order, L, Ld);
@@ -462,8 +576,8 @@ __global__ void __launch_bounds__(256, 2) k_statics(PanelsView pv, double depth,
             }
         }
     }
-    st[2 * NN + o] = dl;
-    st[3 * NN + o] = dd;
+    st[2 * NN + o] = prod ? to_f32(dl) : dl;
+    st[3 * NN + o] = prod ? to_f32(dd) : dd;
 }
 
 // 4 x 4 Gauss rule of a cell of the parameter square (panel_integrals.rs:80-98)
@@ -578,8 +692,9 @@ __device__ void adaptive_pair(const PanelsView& pv, const int32_t* __restrict__ 
         psi_terms(p.c, xb, p.n, psi, dpsi);
         const int Nr = pv.rows ? pv.nrows : N / pv.G;
         size_t NN = (size_t)Nr * N, o = (size_t)k + (size_t)j * Nr;
-        st[2 * NN + o] = acc0 - p.area * psi;
-        st[3 * NN + o] = acc1 - p.area * dpsi;
+        const double vl = acc0 - p.area * psi, vd = acc1 - p.area * dpsi;
+        st[2 * NN + o] = pv.tiers ? to_f32(vl) : vl;  // the production rows in float32
+        st[3 * NN + o] = pv.tiers ? to_f32(vd) : vd;
     }
 }
 
@@ -616,8 +731,8 @@ __global__ void __launch_bounds__(AD_WARPS * 32) k_statics_adaptive_q(PanelsView
 
 // ------------------------------------------------------------------ host launchers
 void launch_panel_geometry(int N, const double* verts, const int32_t* kind, double* planes, int32_t* bad,
-                           cudaStream_t s) {
-    k_panel_geometry<<<(N + 127) / 128, 128, 0, s>>>(N, verts, kind, planes, bad);
+                           cudaStream_t s, float* tiers) {
+    k_panel_geometry<<<(N + 127) / 128, 128, 0, s>>>(N, verts, kind, planes, bad, tiers);
 }
 
 void launch_statics(const PanelsView& pv, double depth, int logint, double tol, double* st, int32_t* work,

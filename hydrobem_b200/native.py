@@ -21,6 +21,7 @@ STATUS_NAMES = {1: "HB_ERR_VALUE", 2: "HB_ERR_TYPE", 3: "HB_ERR_UNSUPPORTED", 4:
                 5: "HB_ERR_CANCELLED", 6: "HB_ERR_INTERNAL", 7: "HB_ERR_ARGUMENT", 8: "HB_ERR_NUMERICAL",
                 9: "HB_ERR_IO", 10: "HB_ERR_EXISTS"}
 HBG_FP64, HBG_MIXED = 0, 1
+HBG_STATICS_ACCURATE, HBG_STATICS_PRODUCTION = 0, 1
 HBG_WET, HBG_INTERIOR = 0, 1
 
 dp = ctypes.POINTER(ctypes.c_double)
@@ -72,7 +73,7 @@ class HbgOptions(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("logarithmic", ctypes.c_int32), ("log_tolerance", ctypes.c_double),
                 ("gravity", ctypes.c_double), ("density", ctypes.c_double), ("depth", ctypes.c_double),
                 ("max_batch", ctypes.c_int32), ("device", ctypes.c_int32), ("cancel", ip),
-                ("surrogate", ctypes.POINTER(ctypes.c_float))]
+                ("surrogate", ctypes.POINTER(ctypes.c_float)), ("statics_rule", ctypes.c_int32)]
 
 
 class HbLocation(ctypes.Structure):

@@ -54,13 +54,17 @@ typedef int32_t HbStatus;
  * caller built against hydrobem.h and comparing with its HB_ABI_VERSION accepts this library. */
 #define HB_ABI_VERSION 8
 /* The revision of this library's own hbg_* entry points and structs (hbg_library_version()). */
-#define HBG_ABI_VERSION 7
+#define HBG_ABI_VERSION 8
 
 /* ==================================================================== batched entry */
 
 /* precision forms of the solve */
 #define HBG_FP64 0  /* FP64 assembly, FP64 LU: the correctness oracle form */
 #define HBG_MIXED 1 /* complex64 matrices, reduced-precision tensor-core LU, FP64 refinement */
+/* HbgOptions.statics_rule, the mixed form's Rankine rule */
+#define HBG_STATICS_ACCURATE 0   /* closed forms within 20 panel radii, float32 3 x 3 rule beyond (default) */
+#define HBG_STATICS_PRODUCTION 1 /* the reference's production rule: float32 Gauss tiers from 2 radii,
+                                  * float32 rows (panel_integrals.rs:190-216, 288-363) */
 
 /* panel kinds (crates/hydrobem/src/low_order.rs:224-238; only these reach this route) */
 #define HBG_WET 0      /* wetted body surface */
@@ -190,6 +194,7 @@ typedef struct HbgOptions {
     const float *surrogate;       /* optional, mixed form only: a trained wave-term network (50822
                                    * parameters then 12 output means/spreads, as hbg_surrogate_train
                                    * returns them) used in the assembly inside its domain; NULL: tables */
+    int32_t statics_rule;         /* mixed form only: HBG_STATICS_ACCURATE (default) or HBG_STATICS_PRODUCTION */
 } HbgOptions;
 
 /* Defaults of the reference's schema (document_schema.rs:202-232). */
@@ -268,7 +273,9 @@ typedef struct HbMeshOptions {
  * N*N (re, im) pairs) of one body at one frequency, FP64 form.  Any output pointer may be NULL.
  * With body->symmetry (G = 2 or 4 sectors of n = n_panels): the statics of the sector rows against
  * all G n panels (entry (k, j) at k + j n, n G n doubles per plane), and the G sector matrices S_c,
- * A_c one after the other (n*n pairs each).
+ * A_c one after the other (n*n pairs each).  With opt->statics_rule HBG_STATICS_PRODUCTION the statics
+ * follow the reference's production rule (float32 Gauss tiers, float32 rows); the matrices are FP64
+ * either way.
  * Replaces no reference interface (it exposes compute_static, lo_static.rs:254-308, and
  * Frequency::matrices, lo_frequency.rs:276-312, for the parity tests). */
 HbStatus hbg_debug_matrices(const HbgBody *body, double omega, const HbgOptions *opt, double *statics, double *S,
