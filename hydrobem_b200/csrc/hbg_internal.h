@@ -344,5 +344,8 @@ int lu_factor_f64(int N, int F, double2* A, size_t mat_stride, int32_t* ipiv, in
                   int64_t* launches);
 int lu_solve_f64(int N, int F, const double2* LU, size_t mat_stride, const int32_t* ipiv, int nrhs, const double2* B,
                  double2* X, cudaStream_t s);
+// the factorization's schedule for the calls that follow (process-wide): the batch in `groups` groups of
+// matrices on side streams (1 to 8), and look-ahead (panel b + 1 factored beside panel b's update) on or off
+void lu_f64_schedule(int groups, int lookahead);
 
 }  // namespace hbg

@@ -15,11 +15,14 @@ __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_doub
 __device__ __forceinline__ double cabs2(double2 a) { return a.x * a.x + a.y * a.y; }
 
 // Blocking of the factorization: panels of LU_NB columns, each factored recursively (halves) down to
-// strips of at most LU_BASE columns; the matrices of a batch in LU_F64_GROUPS groups on side streams,
-// so that one group's strips (one CTA per matrix) run beside the other groups' trailing updates.
+// strips of at most LU_BASE columns.  The default schedule takes the whole batch as one group (every
+// launch covers all its matrices) with look-ahead: the next panel is factored on a high-priority stream
+// beside the trailing update of the current one.  Measured on the 40 matrices of order 4096 of the
+// benchmark job: 322 ms, against 333 / 345 / 353 ms for 2 / 3 / 4 groups and 340 ms without look-ahead.
 constexpr int LU_NB = 128;
 constexpr int LU_BASE = 8;
-constexpr int LU_F64_GROUPS = 4;
+constexpr int LU_F64_GROUPS = 1;      // the default schedule's groups
+constexpr int LU_F64_MAX_GROUPS = 8;
 
 // ------------------------------------------------------------------ base strip
 // Columns c0 .. c0 + w - 1 (w <= LU_BASE), rows c0 .. N - 1, one CTA per matrix: for each column the
@@ -258,47 +261,59 @@ static void launch_lu_trsm(int N, int F, int c0, int n1, int cb, int ce, const d
 // right-hand sides in the substitution), complex128 column-major, leading dimension N.  The complex product as a real
 // one on the interleaved (re, im) layout: C_r (2M x n) -= Ahat (2M x 2K) B_r (2K x n), where B_r and C_r
 // are the matrices' own memory read as doubles and Ahat(2r + c, 2k + c') is a_r, -a_i, a_i, a_r for
-// (c, c') = (0, 0), (0, 1), (1, 0), (1, 1), read on the fly from A's interleaved tile.  Tiles of 64 x 64
-// complex per CTA, eight warps of 32 real rows x 32 columns (4 x 4 m8n8k4 f64 tiles each), K staged by
-// cp.async in chunks of 16 complex (double-buffered, zero-filled beyond the edges), the sum subtracted
-// from C in place.
-constexpr int ZG_M = 64, ZG_N = 64, ZG_K = 16;
-constexpr int ZG_AP = 2 * ZG_M + 8;  // doubles per k-column of the A tile (padded: conflict-free fragments)
-constexpr int ZG_BP = 2 * ZG_K + 4;  // doubles per column of the B tile
-constexpr int ZG_SMEM = (2 * ZG_K * ZG_AP + 2 * ZG_N * ZG_BP) * 8;
+// (c, c') = (0, 0), (0, 1), (1, 0), (1, 1), read on the fly from A's interleaved tile.  Tiles of 64 complex
+// rows x 32 WN columns per CTA, 4 x WN warps of 32 real rows x 32 columns (4 x 4 m8n8k4 f64 tiles each), K
+// staged by cp.async in chunks of 16 complex (double-buffered, zero-filled beyond the edges).  The sums
+// are staged through shared memory (the operand buffers, free by then) so that C is read and written in
+// whole columns with all of a thread's loads in flight together: one memory round trip per tile, which
+// is what a tall, narrow product of the recursion (K and n of 8 to 64) costs most.  WN = 2 (64 columns,
+// two CTAs an SM) for the wide trailing updates, WN = 1 (32 columns, four CTAs an SM) for narrow ones.
+template <int WN>
+struct ZgTile {
+    static constexpr int T = 128 * WN;     // threads: 4 x WN warps
+    static constexpr int ZM = 64;          // complex rows of the tile
+    static constexpr int ZN = 32 * WN;     // columns of the tile
+    static constexpr int ZK = 16;          // complex k of a staged chunk
+    static constexpr int AP = 2 * ZM + 8;  // doubles per k-column of the A tile (padded: conflict-free fragments)
+    static constexpr int BP = 2 * ZK + 4;  // doubles per column of the B tile
+    static constexpr int CP = 2 * ZM + 4;  // doubles per column of the staged sums (4 mod 16: two wavefronts a store)
+    static constexpr int SMEM = 2 * (ZK * AP + ZN * BP) * 8;
+    static_assert(ZN * CP * 8 <= SMEM, "the staged sums fit in the operand buffers");
+};
+constexpr int ZG_NARROW = 1024;  // products of at most this many columns take the 32-column tiles
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool ok) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(sa), "l"(gmem), "r"(ok ? 16 : 0) : "memory");
 }
 
-__global__ void __launch_bounds__(256, 2) k_lu_zgemm(int N, const double2* Aall, size_t astride, double2* Call,
-                                                     size_t cstride, int r0, int c0, int k0, int M, int n, int K) {
+template <int WN>
+__global__ void __launch_bounds__(128 * WN, 4 / WN) k_lu_zgemm(int N, const double2* Aall, size_t astride, double2* Call,
+                                                             size_t cstride, int r0, int c0, int k0, int M, int n, int K) {
+    using G = ZgTile<WN>;
     extern __shared__ double zg_smem[];
-    double* As = zg_smem;                      // [2][ZG_K][ZG_AP]
-    double* Bs = zg_smem + 2 * ZG_K * ZG_AP;   // [2][ZG_N][ZG_BP]
+    double* As = zg_smem;                      // [2][ZK][AP]
+    double* Bs = zg_smem + 2 * G::ZK * G::AP;  // [2][ZN][BP]
     const int f = blockIdx.z;
     const double2* A = Aall + (size_t)f * astride;  // the A operand (rows r0 .., columns k0 ..)
     double2* C = Call + (size_t)f * cstride;        // the B operand (rows k0 .., columns c0 ..) and C
-    const int tm = blockIdx.x * ZG_M, tn = blockIdx.y * ZG_N;
+    const int tm = blockIdx.x * G::ZM, tn = blockIdx.y * G::ZN;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, wm = warp & 3, wn = warp >> 2;
-    const int nchunk = (K + ZG_K - 1) / ZG_K;
+    const int nchunk = (K + G::ZK - 1) / G::ZK;
     auto load = [&](int buf, int kc) {
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int idx = tid + 256 * q;
-            {  // A: k-column kk, complex row rr
-                const int kk = idx >> 6, rr = idx & 63, kg = kc * ZG_K + kk;
-                const bool ok = tm + rr < M && kg < K;
-                const double2* src = ok ? A + (size_t)(r0 + tm + rr) + (size_t)(k0 + kg) * N : A;
-                cp_async16(As + (size_t)(buf * ZG_K + kk) * ZG_AP + 2 * rr, src, ok);
-            }
-            {  // B: column cc, complex row kk
-                const int cc = idx >> 4, kk = idx & 15, kg = kc * ZG_K + kk;
-                const bool ok = tn + cc < n && kg < K;
-                const double2* src = ok ? C + (size_t)(k0 + kg) + (size_t)(c0 + tn + cc) * N : C;
-                cp_async16(Bs + (size_t)(buf * ZG_N + cc) * ZG_BP + 2 * kk, src, ok);
-            }
+        for (int q = 0; q < G::ZK * G::ZM / G::T; q++) {  // A: k-column kk, complex row rr
+            const int idx = tid + G::T * q, kk = idx / G::ZM, rr = idx % G::ZM, kg = kc * G::ZK + kk;
+            const bool ok = tm + rr < M && kg < K;
+            const double2* src = ok ? A + (size_t)(r0 + tm + rr) + (size_t)(k0 + kg) * N : A;
+            cp_async16(As + (size_t)(buf * G::ZK + kk) * G::AP + 2 * rr, src, ok);
+        }
+#pragma unroll
+        for (int q = 0; q < G::ZK * G::ZN / G::T; q++) {  // B: column cc, complex row kk
+            const int idx = tid + G::T * q, cc = idx / G::ZK, kk = idx % G::ZK, kg = kc * G::ZK + kk;
+            const bool ok = tn + cc < n && kg < K;
+            const double2* src = ok ? C + (size_t)(k0 + kg) + (size_t)(c0 + tn + cc) * N : C;
+            cp_async16(Bs + (size_t)(buf * G::ZN + cc) * G::BP + 2 * kk, src, ok);
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
@@ -316,20 +331,20 @@ __global__ void __launch_bounds__(256, 2) k_lu_zgemm(int N, const double2* Aall,
             asm volatile("cp.async.wait_group 0;" ::: "memory");
         }
         __syncthreads();
-        const double* Ab = As + (size_t)(kc & 1) * ZG_K * ZG_AP;
-        const double* Bb = Bs + (size_t)(kc & 1) * ZG_N * ZG_BP;
+        const double* Ab = As + (size_t)(kc & 1) * G::ZK * G::AP;
+        const double* Bb = Bs + (size_t)(kc & 1) * G::ZN * G::BP;
 #pragma unroll
-        for (int ks = 0; ks < 2 * ZG_K / 4; ks++) {
+        for (int ks = 0; ks < 2 * G::ZK / 4; ks++) {
             const int kq = 4 * ks + (lane & 3), k = kq >> 1, cpart = kq & 1;
             double a[4], b[4];
 #pragma unroll
             for (int i = 0; i < 4; i++) {
                 const int R = wm * 32 + 8 * i + (lane >> 2);
-                const double v = Ab[k * ZG_AP + (R ^ cpart)];
+                const double v = Ab[k * G::AP + (R ^ cpart)];
                 a[i] = ((R & 1) == 0 && cpart) ? -v : v;
             }
 #pragma unroll
-            for (int j = 0; j < 4; j++) b[j] = Bb[(wn * 32 + 8 * j + (lane >> 2)) * ZG_BP + kq];
+            for (int j = 0; j < 4; j++) b[j] = Bb[(wn * 32 + 8 * j + (lane >> 2)) * G::BP + kq];
 #pragma unroll
             for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -338,30 +353,73 @@ __global__ void __launch_bounds__(256, 2) k_lu_zgemm(int N, const double2* Aall,
                                  : "+d"(acc[i][j][0]), "+d"(acc[i][j][1])
                                  : "d"(a[i]), "d"(b[j]));
         }
-        __syncthreads();  // the buffer is refilled by the next iteration's load
+        __syncthreads();  // the buffer is refilled by the next iteration's load (or holds the sums below)
     }
+    // the sums, column by column (real row R = 2 r + part), then C -= them a whole column at a time
+    double* Cs = zg_smem;
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int R = wm * 32 + 8 * i + (lane >> 2), crow = tm + (R >> 1);
-        if (crow >= M) continue;
+    for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++)
 #pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const int ccol = tn + wn * 32 + 8 * j + 2 * (lane & 3) + e;
-                if (ccol < n) {
-                    double* c = reinterpret_cast<double*>(C + (size_t)(r0 + crow) + (size_t)(c0 + ccol) * N) + (R & 1);
-                    *c -= acc[i][j][e];
-                }
-            }
+            for (int e = 0; e < 2; e++)
+                Cs[(wn * 32 + 8 * j + 2 * (lane & 3) + e) * G::CP + wm * 32 + 8 * i + (lane >> 2)] = acc[i][j][e];
+    __syncthreads();
+    constexpr int PER = G::ZM * G::ZN / G::T;
+    double2 cv[PER];
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+        const int idx = tid + G::T * q, r = idx % G::ZM, c = idx / G::ZM;
+        if (tm + r < M && tn + c < n) cv[q] = C[(size_t)(r0 + tm + r) + (size_t)(c0 + tn + c) * N];
+    }
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+        const int idx = tid + G::T * q, r = idx % G::ZM, c = idx / G::ZM;
+        if (tm + r < M && tn + c < n) {
+            const double2 sum = *reinterpret_cast<const double2*>(Cs + c * G::CP + 2 * r);
+            C[(size_t)(r0 + tm + r) + (size_t)(c0 + tn + c) * N] = make_double2(cv[q].x - sum.x, cv[q].y - sum.y);
+        }
+    }
+}
+
+static void lu_zgemm_attributes() {
+    cudaFuncSetAttribute(k_lu_zgemm<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ZgTile<1>::SMEM);
+    cudaFuncSetAttribute(k_lu_zgemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ZgTile<2>::SMEM);
+}
+
+// C -= A B over the batch of F matrices (the arguments of k_lu_zgemm), the tile width by the column count
+static void launch_lu_zgemm(int N, int F, const double2* A, size_t astride, double2* C, size_t cstride, int r0, int c0,
+                            int k0, int M, int n, int K, cudaStream_t s) {
+    if (M <= 0 || n <= 0 || K <= 0) return;
+    if (n <= ZG_NARROW) {
+        using G = ZgTile<1>;
+        k_lu_zgemm<1><<<dim3((M + G::ZM - 1) / G::ZM, (n + G::ZN - 1) / G::ZN, F), G::T, G::SMEM, s>>>(
+            N, A, astride, C, cstride, r0, c0, k0, M, n, K);
+    } else {
+        using G = ZgTile<2>;
+        k_lu_zgemm<2><<<dim3((M + G::ZM - 1) / G::ZM, (n + G::ZN - 1) / G::ZN, F), G::T, G::SMEM, s>>>(
+            N, A, astride, C, cstride, r0, c0, k0, M, n, K);
     }
 }
 
 // ------------------------------------------------------------------ the factorization
 namespace {
+// The schedule: the matrices of a batch in `groups` groups, and with look-ahead each group on two streams
+// -- the panel stream factors panel b + 1 (after the update of its own columns) while the update stream
+// applies panel b to the columns beyond it (linalg.rs:134-185's look-ahead, with streams for threads).
+struct LuF64Schedule {
+    int groups = LU_F64_GROUPS;
+    int lookahead = 1;
+};
+LuF64Schedule& lu_f64_schedule_ref() {
+    static LuF64Schedule s;
+    return s;
+}
+
 struct LuF64Streams {
-    cudaStream_t s[LU_F64_GROUPS] = {};
-    cudaEvent_t fork = nullptr, join[LU_F64_GROUPS] = {};
+    cudaStream_t p[LU_F64_MAX_GROUPS] = {}, u[LU_F64_MAX_GROUPS] = {};
+    cudaEvent_t fork = nullptr, ep[LU_F64_MAX_GROUPS] = {}, eu[LU_F64_MAX_GROUPS] = {};
+    cudaEvent_t joinp[LU_F64_MAX_GROUPS] = {}, joinu[LU_F64_MAX_GROUPS] = {};
     bool ok = false;
 };
 LuF64Streams& lu_f64_streams() {
@@ -372,11 +430,21 @@ LuF64Streams& lu_f64_streams() {
     LuF64Streams& x = t[d];
     if (!x.ok) {
         bool ok = true;
-        for (int i = 0; i < LU_F64_GROUPS; i++) {
-            ok = ok && cudaStreamCreateWithFlags(&x.s[i], cudaStreamNonBlocking) == cudaSuccess;
-            ok = ok && cudaEventCreateWithFlags(&x.join[i], cudaEventDisableTiming) == cudaSuccess;
+        auto ev = [&](cudaEvent_t* e) { ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess; };
+        // the panel streams at the highest priority: a panel's CTAs take the first SM slots that the
+        // update stream's trailing product frees, so the panel chain stays ahead of the products
+        int lo = 0, hi = 0;
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        for (int i = 0; i < LU_F64_MAX_GROUPS; i++) {
+            ok = ok && cudaStreamCreateWithPriority(&x.p[i], cudaStreamNonBlocking, hi) == cudaSuccess;
+            ok = ok && cudaStreamCreateWithFlags(&x.u[i], cudaStreamNonBlocking) == cudaSuccess;
+            ev(&x.ep[i]);
+            ev(&x.eu[i]);
+            ev(&x.joinp[i]);
+            ev(&x.joinu[i]);
         }
-        x.ok = ok && cudaEventCreateWithFlags(&x.fork, cudaEventDisableTiming) == cudaSuccess;
+        ev(&x.fork);
+        x.ok = ok;
     }
     return x;
 }
@@ -387,10 +455,11 @@ struct LuF64 {
     size_t stride;
     int32_t* ipiv;
     int32_t* info;
-    cudaStream_t s;
+    cudaStream_t sp, su;  // panel stream, update stream (the same without look-ahead)
+    cudaEvent_t ep, eu;   // the panel stream's part of a step done, the update stream's part done
     int64_t* launches;
 
-    void laswp(int r0, int r1, int ca, int cb, int cc, int cd) {
+    void laswp(cudaStream_t s, int r0, int r1, int ca, int cb, int cc, int cd) {
         const int cols = (cb - ca) + (cd - cc);
         if (cols <= 0 || r1 <= r0) return;
         KernelProfiler& P = profiler();
@@ -399,7 +468,7 @@ struct LuF64 {
         P.end(KF_LU_LASWP, (double)F * cols * (r1 - r0) * 64.0, s);
         (*launches)++;
     }
-    void trsm(int c0, int n1, int cb, int ce) {
+    void trsm(cudaStream_t s, int c0, int n1, int cb, int ce) {
         if (ce <= cb || n1 <= 1) return;
         KernelProfiler& P = profiler();
         P.begin(s);
@@ -408,12 +477,11 @@ struct LuF64 {
         P.end(KF_LU_TRSM, (double)F * 4.0 * n1 * (double)n1 * (ce - cb), s);
         (*launches)++;
     }
-    void gemm(int r0, int c0, int k0, int M, int n, int K) {
+    void gemm(cudaStream_t s, int r0, int c0, int k0, int M, int n, int K) {
         if (M <= 0 || n <= 0 || K <= 0) return;
         KernelProfiler& P = profiler();
         P.begin(s);
-        k_lu_zgemm<<<dim3((M + ZG_M - 1) / ZG_M, (n + ZG_N - 1) / ZG_N, F), 256, ZG_SMEM, s>>>(N, A, stride, A, stride, r0,
-                                                                                              c0, k0, M, n, K);
+        launch_lu_zgemm(N, F, A, stride, A, stride, r0, c0, k0, M, n, K, s);
         // complex C -= A B: 8 M n K real flops
         P.end(KF_LU_GEMM, (double)F * 8.0 * M * (double)n * K, s);
         (*launches)++;
@@ -426,34 +494,68 @@ struct LuF64 {
         if (w <= LU_BASE) {
             KernelProfiler& P = profiler();
             const double m = N - c0;
-            P.begin(s);
-            k_lu_base<<<F, 512, 0, s>>>(N, c0, w, pk0, pnb, A, stride, ipiv, info);
-            P.end(KF_LU_PANEL, (double)F * 8.0 * (m * w * w - (double)w * w * w / 3.0), s);
+            P.begin(sp);
+            k_lu_base<<<F, 512, 0, sp>>>(N, c0, w, pk0, pnb, A, stride, ipiv, info);
+            P.end(KF_LU_PANEL, (double)F * 8.0 * (m * w * w - (double)w * w * w / 3.0), sp);
             (*launches)++;
             return;
         }
         const int n1 = w / 2 / LU_BASE * LU_BASE > 0 ? w / 2 / LU_BASE * LU_BASE : w / 2, n2 = w - n1;
         panel(c0, n1);
-        trsm(c0, n1, c0 + n1, c0 + w);
-        gemm(c0 + n1, c0 + n1, c0, N - c0 - n1, n2, n1);
+        trsm(sp, c0, n1, c0 + n1, c0 + w);
+        gemm(sp, c0 + n1, c0 + n1, c0, N - c0 - n1, n2, n1);
         panel(c0 + n1, n2);
     }
+    // right-looking, one stream: panel, interchanges, block row, trailing update
     void factor() {
         for (int k0 = 0; k0 < N; k0 += LU_NB) {
             const int nb = std::min(LU_NB, N - k0);
             pk0 = k0;
             pnb = nb;
             panel(k0, nb);
-            laswp(k0, k0 + nb, 0, k0, k0 + nb, N);
-            trsm(k0, nb, k0 + nb, N);
-            gemm(k0 + nb, k0 + nb, k0, N - k0 - nb, N - k0 - nb, nb);
+            laswp(sp, k0, k0 + nb, 0, k0, k0 + nb, N);
+            trsm(sp, k0, nb, k0 + nb, N);
+            gemm(sp, k0 + nb, k0 + nb, k0, N - k0 - nb, N - k0 - nb, nb);
+        }
+    }
+    // with look-ahead: step b's panel stream factors panel b (columns k0 .. k1) and signals the update
+    // stream, which swaps rows and solves the block row on the columns k2 .. N and applies panel b to
+    // them; the panel stream meanwhile waits for the update stream's step b - 1 (which wrote columns k1 ..
+    // and read panel b - 1's factor columns that these interchanges reach), then applies panel b to the
+    // left columns and to panel b + 1's columns (k1 .. k2) and goes on to panel b + 1 while the update
+    // stream's product of step b runs.  Every column range is written by one stream at a time, in the
+    // order of the plain schedule, so the factors are the same to the bit.
+    void factor_lookahead() {
+        for (int k0 = 0, b = 0; k0 < N; k0 += LU_NB, b++) {
+            const int nb = std::min(LU_NB, N - k0), k1 = k0 + nb, k2 = std::min(N, k1 + LU_NB);
+            pk0 = k0;
+            pnb = nb;
+            panel(k0, nb);
+            if (k2 < N) {
+                cudaEventRecord(ep, sp);
+                cudaStreamWaitEvent(su, ep, 0);
+                laswp(su, k0, k1, k2, N, 0, 0);
+                trsm(su, k0, nb, k2, N);
+                gemm(su, k1, k2, k0, N - k1, N - k2, nb);
+            }
+            if (b > 0) cudaStreamWaitEvent(sp, eu, 0);
+            if (k2 < N) cudaEventRecord(eu, su);
+            laswp(sp, k0, k1, 0, k0, k1, k2);
+            trsm(sp, k0, nb, k1, k2);
+            gemm(sp, k1, k1, k0, N - k1, k2 - k1, nb);
         }
     }
 };
 }  // namespace
 
+void lu_f64_schedule(int groups, int lookahead) {
+    LuF64Schedule& s = lu_f64_schedule_ref();
+    s.groups = std::max(1, std::min(groups, LU_F64_MAX_GROUPS));
+    s.lookahead = lookahead ? 1 : 0;
+}
+
 static void lu_f64_attributes() {
-    cudaFuncSetAttribute(k_lu_zgemm, cudaFuncAttributeMaxDynamicSharedMemorySize, ZG_SMEM);
+    lu_zgemm_attributes();
     cudaFuncSetAttribute(k_lu_trsm<4, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(sizeof(double2) * LU_NB * (LU_NB - 1) / 2));
     cudaFuncSetAttribute(k_lu_trsm<4, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -465,18 +567,27 @@ int lu_factor_f64(int N, int F, double2* A, size_t stride, int32_t* ipiv, int32_
     lu_f64_attributes();
     cudaMemsetAsync(info, 0, sizeof(int32_t) * F, s);
     LuF64Streams& side = lu_f64_streams();
-    const int ng = side.ok ? std::min(LU_F64_GROUPS, F) : 1;
-    if (ng <= 1) {
-        LuF64{N, F, A, stride, ipiv, info, s, launches}.factor();
+    const LuF64Schedule& sched = lu_f64_schedule_ref();
+    if (!side.ok) {  // no side streams: one group, no look-ahead, on the caller's stream
+        LuF64{N, F, A, stride, ipiv, info, s, s, nullptr, nullptr, launches}.factor();
         return 0;
     }
+    const int ng = std::max(1, std::min(sched.groups, F));
     cudaEventRecord(side.fork, s);
     for (int g = 0, f0 = 0; g < ng; g++) {
         const int fg = F / ng + (g < F % ng ? 1 : 0);
-        cudaStreamWaitEvent(side.s[g], side.fork, 0);
-        LuF64{N, fg, A + (size_t)f0 * stride, stride, ipiv + (size_t)f0 * N, info + f0, side.s[g], launches}.factor();
-        cudaEventRecord(side.join[g], side.s[g]);
-        cudaStreamWaitEvent(s, side.join[g], 0);
+        cudaStreamWaitEvent(side.p[g], side.fork, 0);
+        cudaStreamWaitEvent(side.u[g], side.fork, 0);
+        LuF64 lu{N, fg, A + (size_t)f0 * stride, stride, ipiv + (size_t)f0 * N, info + f0, side.p[g], side.u[g],
+                 side.ep[g], side.eu[g], launches};
+        if (sched.lookahead)
+            lu.factor_lookahead();
+        else
+            lu.factor();
+        cudaEventRecord(side.joinp[g], side.p[g]);
+        cudaEventRecord(side.joinu[g], side.u[g]);
+        cudaStreamWaitEvent(s, side.joinp[g], 0);
+        cudaStreamWaitEvent(s, side.joinu[g], 0);
         f0 += fg;
     }
     return 0;
@@ -520,9 +631,7 @@ int lu_solve_f64(int N, int F, const double2* LU, size_t stride, const int32_t* 
     k_lu_permute<<<F, 512, smem, s>>>(N, ipiv, nrhs, B, X);
     const size_t xs = (size_t)nrhs * N;
     auto update = [&](int r0, int k0, int M, int K) {
-        if (M > 0)
-            k_lu_zgemm<<<dim3((M + ZG_M - 1) / ZG_M, 1, F), 256, ZG_SMEM, s>>>(N, LU, stride, X, xs, r0, 0, k0, M, nrhs,
-                                                                                K);
+        launch_lu_zgemm(N, F, LU, stride, X, xs, r0, 0, k0, M, nrhs, K, s);
     };
     for (int b0 = 0; b0 < N; b0 += LU_NB) {  // L y = P b
         const int nb = std::min(LU_NB, N - b0);
