@@ -387,8 +387,10 @@ def ours(args, world, rank, local, pg):
         line["refinement"] = ir
     if fallbacks is not None:
         line["fp64_fallback_frequencies"] = fallbacks
+    if precision == nv.HBG_FP64:  # over the timed steps' LU phase (the kernel-timed step's is inflated)
+        line["lu"] = lu_rate(nv, {"lu": float(np.mean([p[2] for p in dev_phases]))}, pipe_peaks)
     if precision == nv.HBG_MIXED and not args.no_plain and bodies:
-        line["plain_fp64"], plain = plain_comparison(nv, mine, bodies, depth, device)
+        line["plain_fp64"], plain = plain_comparison(nv, mine, bodies, depth, device, pipe_peaks)
     if precision == nv.HBG_MIXED and world == 1 and args.surrogate_steps > 0:
         line["surrogate"] = surrogate_comparison(nv, device, args.surrogate_steps)
     if world == 1 and not args.no_cpu_baseline and CASE in SINGLE_BODY:
@@ -396,7 +398,20 @@ def ours(args, world, rank, local, pg):
     return line
 
 
-def plain_comparison(nv, mine, mixed_bodies, depth, device, max_solves=400):
+def lu_rate(nv, phases, pipe_peaks):
+    """The FP64 form's factorizations of the last solve: real flops (the panel, triangular-solve and
+    product launches' counted work), their rate over the LU phase, and that rate over the measured FP64
+    peaks (FMA and warp MMA)."""
+    prof = nv.kernel_profile()
+    flops = sum(prof[k][2] for k in ("lu_panel", "lu_trsm", "lu_gemm"))
+    ms = phases.get("lu", 0.0)
+    tf = flops / (ms * 1e-3) / 1e12 if ms > 0 else None
+    return {"flops": flops, "ms": round(ms, 2), "tflops": tf,
+            "frac_of_fp64_fma": tf / pipe_peaks["fp64_fma"] if tf else None,
+            "frac_of_fp64_mma": tf / pipe_peaks["fp64_mma"] if tf else None}
+
+
+def plain_comparison(nv, mine, mixed_bodies, depth, device, pipe_peaks, max_solves=400):
     """The plain FP64 form of the same problems (the correctness oracle of the mixed form): its
     throughput, the speed-up of the mixed form, and the error of the mixed A, B, X against it (per entry,
     over the entry's largest modulus across frequencies, floor 1e-3 of the quantity's peak).  When the job
@@ -422,8 +437,9 @@ def plain_comparison(nv, mine, mixed_bodies, depth, device, max_solves=400):
     nf = sum(len(m["omegas"]) for m in sub)
     err = {k: max(scaled_error(np.asarray(mx[k])[:len(pl[k])], pl[k]) for mx, pl in zip(mixed, plain))
            for k in ("A", "B", "X", "HK")}
+    phases = nv.last_profile()
     out = {"value": nf / (step * 1e-3), "ms_per_step": step, "err_vs_fp64": err,
-           "phases_ms": {k: round(x, 2) for k, x in nv.last_profile().items()}}
+           "phases_ms": {k: round(x, 2) for k, x in phases.items()}, "lu": lu_rate(nv, phases, pipe_peaks)}
     if keep is not None:
         out["frequencies"] = f"the first {keep} of each problem ({nf} solves)"
     return out, plain
