@@ -291,7 +291,7 @@ def ours(args, world, rank, local, pg):
     precision = nv.HBG_MIXED if args.precision == "mixed" else nv.HBG_FP64
     bodies = [nv.Body(**m) for m in mine]
     arr = (nv.HbgProblem * max(len(bodies), 1))(*[b.problem() for b in bodies])
-    opt = nv.default_options(precision=precision, depth=depth, device=device)
+    opt = nv.default_options(precision=precision, depth=depth, device=device, concurrency=args.concurrency)
     import ctypes
 
     L = nv.lib()
@@ -528,6 +528,8 @@ def main():
     ap.add_argument("--surrogate-steps", type=int, default=4000,
                     help="training steps of the wave-term network measured beside the mixed form (0: skip)")
     ap.add_argument("--case", default="c2", choices=list(CASE_LABELS))
+    ap.add_argument("--concurrency", type=int, default=0,
+                    help="problems of the job solved at once (0: the library's tuner; 1: one after another)")
     args = ap.parse_args()
     global CASE
     CASE = args.case

@@ -5,11 +5,16 @@
 // assembly of S and A, boundary values, right-hand sides, LU, substitution and forces, all on one
 // stream, results copied back once per batch.  The host only computes per-frequency scalars
 // (dispersion roots and the finite-depth power table, solve_common.rs:44-71) and checks statuses.
+#include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/hydrobem_gpu.h"
@@ -252,6 +257,7 @@ static DeviceCtx& device_ctx(int dev) {
     set_constants(glx, glw, d.tab);
     set_constants_statics(glx, glw);
     CUDA_OK(cudaGetLastError());
+    lu_tune_device(dev);  // before any solve's work is queued on the device
     d.ready = true;
     return d;
 }
@@ -758,13 +764,14 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         struct BatchChoice {
             int N = -1, G = -1, nrhs = -1, fin = -1, F = -1, B = 0;
             int64_t max_batch = -2;
+            size_t budget = 0;
         };
         static thread_local BatchChoice last[16];
         int dev_b = 0;
         cudaGetDevice(&dev_b);
         BatchChoice& c = last[dev_b < 0 || dev_b >= 16 ? 0 : dev_b];
         const bool same = c.N == N && c.G == G && c.nrhs == nrhs && c.fin == (int)fin && c.F == F &&
-                          c.max_batch == opt.max_batch;
+                          c.max_batch == opt.max_batch && c.budget == hbm_budget();
         const size_t mats = NN * G * (size_t)std::max(c.B, 0);
         if (same && c.B > 0 && ws.bytes[WS_S] >= sizeof(double2) * mats && ws.bytes[WS_A] >= sizeof(double2) * mats) {
             B = c.B;
@@ -772,10 +779,12 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
             size_t freeb = 0, totalb = 0;
             CUDA_OK(cudaMemGetInfo(&freeb, &totalb));
             const size_t reusable = ws.bytes[WS_S] + ws.bytes[WS_A];
-            B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)(freeb + reusable)) / per_freq);
+            size_t avail = (size_t)(0.85 * (double)(freeb + reusable));
+            if (hbm_budget() > 0) avail = std::min(avail, hbm_budget());
+            B = (int)std::max<size_t>(1, avail / per_freq);
             if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
             B = std::min(B, F);
-            c = BatchChoice{N, G, nrhs, (int)fin, F, B, opt.max_batch};
+            c = BatchChoice{N, G, nrhs, (int)fin, F, B, opt.max_batch, hbm_budget()};
         }
     }
     const size_t BS = (size_t)B * G;  // systems per batch
@@ -1005,10 +1014,233 @@ extern "C" void hbg_default_options(HbgOptions* opt) {
     opt->density = 1000.0;
     opt->depth = INFINITY;
     opt->max_batch = 0;
+    opt->concurrency = 0;
     opt->device = 0;
     opt->cancel = nullptr;
     opt->surrogate = nullptr;
     opt->statics_rule = HBG_STATICS_ACCURATE;
+}
+
+// ------------------------------------------------------------------ the cross-body work queue
+// Several problems of one call solved at once: K pipelines, each a host thread of a pool kept per device
+// for the life of the process (so that its thread-local workspace, streams and side streams persist
+// across calls like the calling thread's own), with its own stream and 1/K of the free device memory.
+// The problems go costliest first to the next free pipeline: the reference's worker pool over
+// independent units (parallel.rs:31-109), with the device's streams for threads.
+namespace {
+class PipelinePool {
+public:
+    explicit PipelinePool(int dev) : dev_(dev) {}
+    // job(w) on pipelines w = 0 .. k - 1; returns when all have finished (calls are serialised)
+    void run(int k, const std::function<void(int)>& job) {
+        std::lock_guard<std::mutex> one(run_m_);
+        std::unique_lock<std::mutex> lk(m_);
+        while ((int)threads_ < k) {
+            const int w = threads_++;
+            std::thread([this, w] { loop(w); }).detach();
+        }
+        job_ = &job;
+        k_ = k;
+        left_ = k;
+        gen_++;
+        cv_.notify_all();
+        done_.wait(lk, [this] { return left_ == 0; });
+        job_ = nullptr;
+    }
+    int threads() {
+        std::lock_guard<std::mutex> lk(m_);
+        return threads_;
+    }
+
+private:
+    void loop(int w) {
+        cudaSetDevice(dev_);
+        uint64_t seen = 0;
+        for (;;) {
+            const std::function<void(int)>* job = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [&] { return gen_ != seen; });
+                seen = gen_;
+                if (w >= k_) continue;
+                job = job_;
+            }
+            (*job)(w);
+            std::lock_guard<std::mutex> lk(m_);
+            if (--left_ == 0) done_.notify_all();
+        }
+    }
+    int dev_;
+    std::mutex run_m_, m_;
+    std::condition_variable cv_, done_;
+    const std::function<void(int)>* job_ = nullptr;
+    int threads_ = 0, k_ = 0, left_ = 0;
+    uint64_t gen_ = 0;
+};
+
+// the pool of a device (created on first use when `create`; kept for the process: its threads never exit)
+PipelinePool* pipeline_pool_ptr(int dev, bool create) {
+    static std::mutex m;
+    static PipelinePool* pools[16] = {};
+    std::lock_guard<std::mutex> lk(m);
+    if (!pools[dev] && create) pools[dev] = new PipelinePool(dev);
+    return pools[dev];
+}
+PipelinePool& pipeline_pool(int dev) { return *pipeline_pool_ptr(dev, true); }
+
+cudaStream_t& pipeline_stream() {
+    static thread_local cudaStream_t s = nullptr;
+    return s;
+}
+
+// What a pipeline hands back: its phase times, counters and kernel-family records, and the workspace
+// it holds afterwards (part of the memory the next call shares out).
+struct PipelineStats {
+    double phase[5] = {};
+    int64_t launches = 0, fallbacks = 0;
+    long long sg_pairs = 0;
+    int ir_iterations = 0;
+    double kms[KF_COUNT] = {}, kwork[KF_COUNT] = {};
+    int64_t klaunches[KF_COUNT] = {};
+    size_t held = 0;
+};
+size_t g_pool_held[16];  // per device: the pipelines' workspace bytes after the last concurrent call
+
+// The modelled cost of a problem (the LU of each system against its assembly, per frequency): the order
+// in which the pipelines take the problems.
+double problem_cost(const HbgProblem& p) {
+    const int G = p.body.symmetry == HBG_SYM_BOTH ? 4 : p.body.symmetry != HBG_SYM_NONE ? 2 : 1;
+    const double n = (double)p.body.n_panels;
+    return (double)std::max<int64_t>(p.n_omega, 1) * G * (n * n * n + 1.0e3 * G * n * n);
+}
+}  // namespace
+
+// The pipelines for a call that leaves the choice to the library: two when the call has several problems
+// none of which is large (the 64 uneven bodies of 840-5928 panels, 16 frequencies each, mixed form:
+// 450 / 545 / 538 / 513 frequency solves/s with 1 / 2 / 3 / 4 pipelines; the small bodies' triangular
+// sweeps and refinement are latency-bound chains that another body's products fill in), else one (a large
+// problem keeps the whole memory for its frequency batches).
+static int tuned_concurrency(const HbgProblem* problems, int64_t n, const HbgOptions& opt) {
+    (void)opt;
+    if (n < 2) return 1;
+    for (int64_t p = 0; p < n; p++) {
+        const int G = problems[p].body.symmetry == HBG_SYM_BOTH ? 4 : problems[p].body.symmetry != HBG_SYM_NONE ? 2 : 1;
+        if (problems[p].body.n_panels * G > 8192) return 1;
+    }
+    return 2;
+}
+
+// The problems of a call on K pipelines (K >= 2): the device time from the first queued operation to
+// the last, the phases summed over the pipelines, the counters added up; on failure the failure of the
+// lowest problem index is returned (problems after it may have been solved, as with one pipeline those
+// before it).
+static void solve_concurrent(const HbgProblem* problems, int64_t n, const HbgOptions& opt, int K) {
+    const int dev = opt.device;
+    PipelinePool& pool = pipeline_pool(dev);
+    std::vector<int64_t> order((size_t)n);
+    for (int64_t i = 0; i < n; i++) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int64_t a, int64_t b) { return problem_cost(problems[a]) > problem_cost(problems[b]); });
+    size_t freeb = 0, totalb = 0;
+    CUDA_OK(cudaMemGetInfo(&freeb, &totalb));
+    const size_t budget = (size_t)(0.85 * (double)(freeb + g_pool_held[dev]) / K);
+    std::vector<PipelineStats> stats((size_t)K);
+    std::vector<cudaEvent_t> ends((size_t)K, nullptr);
+    cudaStream_t s0;
+    CUDA_OK(cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (auto& e : ends) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    cudaEventRecord(e0, s0);
+    const bool prof_on = profiler().on;
+    std::atomic<int64_t> next{0};
+    std::atomic<bool> failed{false};
+    std::mutex fm;
+    Failure first{HB_OK, ""};
+    int64_t first_at = -1;
+    auto record = [&](const Failure& f, int64_t p) {
+        std::lock_guard<std::mutex> lk(fm);
+        if (first_at < 0 || p < first_at) first = f, first_at = p;
+        failed = true;
+    };
+    std::function<void(int)> job = [&](int w) {
+        PipelineStats& st = stats[(size_t)w];
+        hbm_budget() = budget;
+        for (int i = 0; i < 6; i++) g_profile[i] = 0.0;
+        g_launches = 0;
+        last_fallback_count() = 0;
+        last_surrogate_pairs() = 0;
+        KernelProfiler& P = profiler();
+        P.reset();
+        P.on = prof_on;
+        phase_timers().flush();
+        solve_begin().recorded = false;
+        solve_end().recorded = false;
+        cudaStream_t& s = pipeline_stream();
+        if (!s && cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+            s = nullptr;
+            record(Failure{HB_ERR_INTERNAL, "CUDA: a pipeline stream could not be created"}, -1);
+        }
+        if (s) {
+            cudaStreamWaitEvent(s, e0, 0);
+            int64_t p = -1;
+            try {
+                for (;;) {
+                    if (failed.load()) break;
+                    const int64_t i = next.fetch_add(1);
+                    if (i >= n) break;
+                    p = order[(size_t)i];
+                    solve_problem(problems[p], opt, p, s);
+                }
+            } catch (const Failure& f) {
+                record(f, p);
+            } catch (const std::exception& e) {
+                record(Failure{HB_ERR_INTERNAL, std::string("internal error: ") + e.what(), p}, p);
+            } catch (...) {
+                record(Failure{HB_ERR_INTERNAL, "internal error", p}, p);
+            }
+            cudaEventRecord(ends[(size_t)w], s);
+            cudaStreamSynchronize(s);
+        }
+        phase_timers().flush();
+        P.flush();
+        for (int i = 0; i < 5; i++) st.phase[i] = g_profile[i];
+        st.launches = g_launches;
+        st.fallbacks = last_fallback_count();
+        st.sg_pairs = last_surrogate_pairs();
+        st.ir_iterations = last_ir_iterations();
+        for (int i = 0; i < KF_COUNT; i++) st.kms[i] = P.ms[i], st.kwork[i] = P.work[i], st.klaunches[i] = P.launches[i];
+        st.held = workspace().held();
+        hbm_budget() = 0;
+    };
+    pool.run(K, job);
+    for (auto& e : ends) cudaStreamWaitEvent(s0, e, 0);
+    cudaEventRecord(e1, s0);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    KernelProfiler& P = profiler();
+    size_t held = 0;
+    int ir = 0;
+    for (const PipelineStats& st : stats) {
+        for (int i = 0; i < 5; i++) g_profile[i] += st.phase[i];
+        g_launches += st.launches;
+        last_fallback_count() += st.fallbacks;
+        last_surrogate_pairs() += st.sg_pairs;
+        ir = std::max(ir, st.ir_iterations);
+        for (int i = 0; i < KF_COUNT; i++) P.ms[i] += st.kms[i], P.work[i] += st.kwork[i], P.launches[i] += st.klaunches[i];
+        held += st.held;
+    }
+    last_ir_iterations() = ir;
+    last_ir_history().n = 0;
+    g_pool_held[dev] = held;
+    g_profile[5] = ms;
+    for (auto& e : ends) cudaEventDestroy(e);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s0);
+    if (failed.load()) throw first;
 }
 
 extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_problems, const HbgOptions* opt) {
@@ -1035,12 +1267,21 @@ extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_proble
                                              "form is the reference's double-precision path)"});
         if (!(opt->gravity > 0.0) || !(opt->density > 0.0) || opt->log_tolerance < 0.0)
             return fail({HB_ERR_VALUE, "gravity and density must be positive, log_tolerance nonnegative"});
+        if (opt->concurrency < 0 || opt->concurrency > 8) return fail({HB_ERR_VALUE, "concurrency outside 0..8"});
         int ndev = 0;
         if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
             return fail({HB_ERR_UNSUPPORTED, "no CUDA device: this library runs the path on the GPU only"});
         if (opt->device < 0 || opt->device >= ndev) return fail({HB_ERR_ARGUMENT, "device ordinal out of range"});
         CUDA_OK(cudaSetDevice(opt->device));
         device_ctx(opt->device);
+        const int K = (int)std::min<int64_t>(opt->concurrency > 0 ? opt->concurrency
+                                                                  : tuned_concurrency(problems, n_problems, *opt),
+                                             n_problems);
+        if (K >= 2) {
+            phase_timers().flush();
+            solve_concurrent(problems, n_problems, *opt, K);
+            return HB_OK;
+        }
         cudaStream_t s;
         CUDA_OK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
         cudaEvent_t e0, e1;
@@ -1109,6 +1350,13 @@ extern "C" HbStatus hbg_release_workspace(void) {
             cudaSetDevice(d);
             g_ws[d]->release();
             cudaSetDevice(cur);
+        }
+    // and the buffers of the device's pipelines (concurrent solves)
+    for (int d = 0; d < 16; d++)
+        if (PipelinePool* pool = pipeline_pool_ptr(d, false)) {
+            const int k = pool->threads();
+            if (k > 0) pool->run(k, [](int) { workspace().release(); });
+            g_pool_held[d] = 0;
         }
     return HB_OK;
 }
@@ -1367,6 +1615,13 @@ extern "C" HbStatus hbg_last_ir_history(double* ratios32, int32_t* n) {
 extern "C" HbStatus hbg_last_ir_iterations(int32_t* n) {
     if (!n) return fail({HB_ERR_ARGUMENT, "null argument"});
     *n = last_ir_iterations();
+    return HB_OK;
+}
+
+extern "C" HbStatus hbg_tuned_tiles(int32_t device, int32_t* state, int32_t* wide, float* us) {
+    if (!state || !wide || !us) return fail({HB_ERR_ARGUMENT, "null argument"});
+    if (device < 0 || device >= 16) return fail({HB_ERR_ARGUMENT, "device ordinal out of range"});
+    *state = lu_tuned_tiles(device, wide, us);
     return HB_OK;
 }
 

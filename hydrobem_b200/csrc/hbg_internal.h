@@ -181,6 +181,13 @@ struct PhaseTimers {
         pend.clear();
     }
 };
+// The device memory the solves of this host thread may hold in their workspace (0: no limit beyond 85 %
+// of the free memory): a pipeline's share when several problems are solved at once.
+inline size_t& hbm_budget() {
+    static thread_local size_t b = 0;
+    return b;
+}
+
 inline PhaseTimers& phase_timers() {
     static thread_local PhaseTimers t;
     return t;
@@ -347,5 +354,10 @@ int lu_solve_f64(int N, int F, const double2* LU, size_t mat_stride, const int32
 // the factorization's schedule for the calls that follow (process-wide): the batch in `groups` groups of
 // matrices on side streams (1 to 8), and look-ahead (panel b + 1 factored beside panel b's update) on or off
 void lu_f64_schedule(int groups, int lookahead);
+// the FP64 products' tile widths of a device, timed once when the device is first used; and the table
+// (per width bucket n <= 8, 16, ..., 2048, 4096: 64-column tile or not, and the two timings in
+// microseconds): 0 before the tuning, 1 heuristic (the timing could not run), 2 measured
+void lu_tune_device(int dev);
+int lu_tuned_tiles(int dev, int32_t* wide, float* us);
 
 }  // namespace hbg

@@ -5,6 +5,8 @@
 //
 // Matrices are column-major complex128 (entry (i, j) at i + j N), matrix f at A + f * stride.
 // ipiv[f * N + i] is the 0-based row swapped with row i at step i (LAPACK's layout).
+#include <atomic>
+
 #include "hbg_device.cuh"
 #include "hbg_internal.h"
 
@@ -387,11 +389,30 @@ static void lu_zgemm_attributes() {
     cudaFuncSetAttribute(k_lu_zgemm<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ZgTile<2>::SMEM);
 }
 
-// C -= A B over the batch of F matrices (the arguments of k_lu_zgemm), the tile width by the column count
-static void launch_lu_zgemm(int N, int F, const double2* A, size_t astride, double2* C, size_t cstride, int r0, int c0,
-                            int k0, int M, int n, int K, cudaStream_t s) {
-    if (M <= 0 || n <= 0 || K <= 0) return;
-    if (n <= ZG_NARROW) {
+// The tile width of a product of n columns, autotuned per device: when the device is first used
+// (before any solve's work is queued on it) both widths are timed on a product of each width bucket
+// n <= 8, 16, ..., 2048 and 4096 (2048 rows, K = min(n, 128), four matrices, the best of three launches
+// each, on scratch buffers freed afterwards) and the 64-column tile is taken where it is at least 2 %
+// faster.  Until then, or if the timing cannot run, products of at most ZG_NARROW columns take the
+// 32-column tile (the choice the measurements on the benchmark's shapes gave).
+constexpr int ZG_TUNE_BUCKETS = 10;
+struct ZgTune {
+    std::atomic<bool> ready{false};
+    bool measured = false;
+    bool wide[ZG_TUNE_BUCKETS] = {};
+    float us[ZG_TUNE_BUCKETS][2] = {};
+};
+static ZgTune g_zg_tune[16];
+
+static int zg_bucket(int n) {
+    int b = 0;
+    while (b < ZG_TUNE_BUCKETS - 1 && n > (8 << b)) b++;
+    return b;
+}
+
+static void launch_lu_zgemm_wn(bool wide, int N, int F, const double2* A, size_t astride, double2* C, size_t cstride,
+                               int r0, int c0, int k0, int M, int n, int K, cudaStream_t s) {
+    if (!wide) {
         using G = ZgTile<1>;
         k_lu_zgemm<1><<<dim3((M + G::ZM - 1) / G::ZM, (n + G::ZN - 1) / G::ZN, F), G::T, G::SMEM, s>>>(
             N, A, astride, C, cstride, r0, c0, k0, M, n, K);
@@ -400,6 +421,78 @@ static void launch_lu_zgemm(int N, int F, const double2* A, size_t astride, doub
         k_lu_zgemm<2><<<dim3((M + G::ZM - 1) / G::ZM, (n + G::ZN - 1) / G::ZN, F), G::T, G::SMEM, s>>>(
             N, A, astride, C, cstride, r0, c0, k0, M, n, K);
     }
+}
+
+// C -= A B over the batch of F matrices (the arguments of k_lu_zgemm), the tile width as tuned
+static void launch_lu_zgemm(int N, int F, const double2* A, size_t astride, double2* C, size_t cstride, int r0, int c0,
+                            int k0, int M, int n, int K, cudaStream_t s) {
+    if (M <= 0 || n <= 0 || K <= 0) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const ZgTune& t = g_zg_tune[dev < 0 || dev >= 16 ? 0 : dev];
+    const bool wide = t.ready.load(std::memory_order_acquire) ? t.wide[zg_bucket(n)] : n > ZG_NARROW;
+    launch_lu_zgemm_wn(wide, N, F, A, astride, C, cstride, r0, c0, k0, M, n, K, s);
+}
+
+void lu_tune_device(int dev) {
+    if (dev < 0 || dev >= 16) return;
+    ZgTune& t = g_zg_tune[dev];
+    if (t.ready.load(std::memory_order_acquire)) return;
+    for (int b = 0; b < ZG_TUNE_BUCKETS; b++) t.wide[b] = (8 << b) > ZG_NARROW;
+    constexpr int M = 2048, F = 4, KMAX = 128, NMAX = 8 << (ZG_TUNE_BUCKETS - 1);
+    const int N = M + KMAX;  // leading dimension: B in rows 0 .. K - 1, C in rows KMAX .. N - 1
+    const size_t astride = (size_t)N * KMAX, cstride = (size_t)N * NMAX;
+    double2 *A = nullptr, *C = nullptr;
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    bool ok = cudaMalloc(&A, sizeof(double2) * astride * F) == cudaSuccess &&
+              cudaMalloc(&C, sizeof(double2) * cstride * F) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+    if (ok) {
+        lu_zgemm_attributes();
+        ok = cudaMemsetAsync(A, 0, sizeof(double2) * astride * F, s) == cudaSuccess &&
+             cudaMemsetAsync(C, 0, sizeof(double2) * cstride * F, s) == cudaSuccess;
+        for (int b = 0; ok && b < ZG_TUNE_BUCKETS; b++) {
+            const int n = 8 << b, K = std::min(n, KMAX);
+            for (int w = 0; w < 2; w++) {
+                float best = 1e30f;
+                launch_lu_zgemm_wn(w == 1, N, F, A, astride, C, cstride, KMAX, 0, 0, M, n, K, s);
+                for (int r = 0; r < 3 && ok; r++) {
+                    cudaEventRecord(e0, s);
+                    launch_lu_zgemm_wn(w == 1, N, F, A, astride, C, cstride, KMAX, 0, 0, M, n, K, s);
+                    cudaEventRecord(e1, s);
+                    float ms = 0.f;
+                    ok = cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+                    best = std::min(best, ms);
+                }
+                t.us[b][w] = 1e3f * best;
+            }
+            t.wide[b] = t.us[b][1] < 0.98f * t.us[b][0];
+        }
+        t.measured = ok;
+        if (!ok)
+            for (int b = 0; b < ZG_TUNE_BUCKETS; b++) t.wide[b] = (8 << b) > ZG_NARROW;
+    }
+    cudaGetLastError();  // a failed timing leaves the heuristic choice, not an error for the solve
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s) cudaStreamDestroy(s);
+    if (A) cudaFree(A);
+    if (C) cudaFree(C);
+    t.ready.store(true, std::memory_order_release);
+}
+
+int lu_tuned_tiles(int dev, int32_t* wide, float* us) {
+    if (dev < 0 || dev >= 16) return 0;
+    const ZgTune& t = g_zg_tune[dev];
+    if (!t.ready.load(std::memory_order_acquire)) return 0;
+    for (int b = 0; b < ZG_TUNE_BUCKETS; b++) {
+        wide[b] = t.wide[b] ? 1 : 0;
+        us[2 * b] = t.us[b][0];
+        us[2 * b + 1] = t.us[b][1];
+    }
+    return t.measured ? 2 : 1;
 }
 
 // ------------------------------------------------------------------ the factorization

@@ -22,14 +22,14 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 static EncodeTiledFn encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    if (!fn) {
+    static const EncodeTiledFn fn = [] {  // resolved once, thread-safe (the pipelines of a batch share it)
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    }
+            return reinterpret_cast<EncodeTiledFn>(p);
+        return (EncodeTiledFn) nullptr;
+    }();
     return fn;
 }
 
@@ -183,13 +183,14 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
         struct BatchChoice {
             int N = -1, G = -1, nrhs = -1, fin = -1, F = -1, B = 0;
             int64_t max_batch = -2;
+            size_t budget = 0;
         };
         static thread_local BatchChoice last[16];
         int dev_b = 0;
         cudaGetDevice(&dev_b);
         BatchChoice& c = last[dev_b < 0 || dev_b >= 16 ? 0 : dev_b];
         const bool same = c.N == N && c.G == G && c.nrhs == nrhs && c.fin == (int)fin && c.F == F &&
-                          c.max_batch == opt.max_batch;
+                          c.max_batch == opt.max_batch && c.budget == hbm_budget();
         const size_t mats = MB * (size_t)std::max(c.B, 0) * G * 4;
         if (same && c.B > 0 && ws.bytes[WS_S32] >= mats && ws.bytes[WS_W] >= mats) {
             B = c.B;
@@ -198,10 +199,12 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
             if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess)
                 MIXED_FAIL(HB_ERR_INTERNAL, "cudaMemGetInfo failed", -1);
             freeb += ws.bytes[WS_S32] + ws.bytes[WS_A32] + ws.bytes[WS_W] + ws.bytes[WS_DINV];
-            B = (int)std::max<size_t>(1, (size_t)(0.85 * (double)freeb) / per);
+            size_t avail = (size_t)(0.85 * (double)freeb);
+            if (hbm_budget() > 0) avail = std::min(avail, hbm_budget());
+            B = (int)std::max<size_t>(1, avail / per);
             if (opt.max_batch > 0) B = std::min(B, (int)opt.max_batch);
             B = std::min(B, F);
-            c = BatchChoice{N, G, nrhs, (int)fin, F, B, opt.max_batch};
+            c = BatchChoice{N, G, nrhs, (int)fin, F, B, opt.max_batch, hbm_budget()};
         }
     }
     const size_t nblk = (size_t)Np / NBL;

@@ -73,7 +73,8 @@ class HbgOptions(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("logarithmic", ctypes.c_int32), ("log_tolerance", ctypes.c_double),
                 ("gravity", ctypes.c_double), ("density", ctypes.c_double), ("depth", ctypes.c_double),
                 ("max_batch", ctypes.c_int32), ("device", ctypes.c_int32), ("cancel", ip),
-                ("surrogate", ctypes.POINTER(ctypes.c_float)), ("statics_rule", ctypes.c_int32)]
+                ("surrogate", ctypes.POINTER(ctypes.c_float)), ("statics_rule", ctypes.c_int32),
+                ("concurrency", ctypes.c_int32)]
 
 
 class HbLocation(ctypes.Structure):
@@ -95,7 +96,7 @@ EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
            "hbg_statics_noalloc", "hbg_measure_peaks", "hbg_last_ir_history", "hbg_surrogate_train",
            "hbg_surrogate_grad", "hbg_surrogate_eval", "hbg_last_surrogate_pairs", "hbg_read_gdf", "hbg_gdf_free",
-           "hb_model_load_mesh", "hbg_last_fallback_count", "hbg_debug_lu_f64", "hb_model_panels"]
+           "hb_model_load_mesh", "hbg_last_fallback_count", "hbg_debug_lu_f64", "hb_model_panels", "hbg_tuned_tiles"]
 
 _lib = None
 
@@ -430,6 +431,20 @@ def measure_peaks() -> dict:
     out = np.zeros(3)
     check(lib().hbg_measure_peaks(out.ctypes.data_as(dp)))
     return {"fp64_fma": float(out[0]), "fp64_mma": float(out[1]), "tf32_tcgen05": float(out[2])}
+
+
+def tuned_tiles(device: int = 0) -> dict:
+    """The FP64 products' tile widths the library's tuner chose on a device: state (0 not tuned yet, 1
+    default, 2 measured), and per width bucket (n <= 8, 16, ..., 2048, 4096) the choice (64 or 32 columns)
+    and the two timings in microseconds."""
+    state = ctypes.c_int32()
+    wide = np.zeros(10, np.int32)
+    us = np.zeros(20, np.float32)
+    check(lib().hbg_tuned_tiles(device, ctypes.byref(state), wide.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                us.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+    widths = [8 << b for b in range(10)]
+    return {"state": state.value, "columns": {w: (64 if x else 32) for w, x in zip(widths, wide)},
+            "us": {w: (float(us[2 * b]), float(us[2 * b + 1])) for b, w in enumerate(widths)}}
 
 
 def last_ir_history() -> list:

@@ -54,7 +54,7 @@ typedef int32_t HbStatus;
  * caller built against hydrobem.h and comparing with its HB_ABI_VERSION accepts this library. */
 #define HB_ABI_VERSION 8
 /* The revision of this library's own hbg_* entry points and structs (hbg_library_version()). */
-#define HBG_ABI_VERSION 8
+#define HBG_ABI_VERSION 9
 
 /* ==================================================================== batched entry */
 
@@ -195,6 +195,11 @@ typedef struct HbgOptions {
                                    * parameters then 12 output means/spreads, as hbg_surrogate_train
                                    * returns them) used in the assembly inside its domain; NULL: tables */
     int32_t statics_rule;         /* mixed form only: HBG_STATICS_ACCURATE (default) or HBG_STATICS_PRODUCTION */
+    int32_t concurrency;          /* problems of one call solved at once on the device, each on its own
+                                   * stream and share of the free memory, the next problem to the next free
+                                   * pipeline, the costliest first (the reference's worker pool,
+                                   * parallel.rs:31-109): 0 (default) chosen by the tuner from the problems'
+                                   * sizes, 1 one after another, 2..8 that many */
 } HbgOptions;
 
 /* Defaults of the reference's schema (document_schema.rs:202-232). */
@@ -409,6 +414,14 @@ typedef int32_t (*HbProgressFn)(const HbProgress *progress, void *user);
 
 /* hydrobem.h:233: returns HB_ABI_VERSION (8), the ABI of the reference header this subset mirrors */
 uint32_t hb_abi_version(void);
+/* No counterpart in the reference: the tile widths the library's tuner chose for the FP64 form's complex
+ * products on a device, timed once when the device is first used (before any solve's work is queued):
+ * per width bucket b = 0..9 (products of n <= 8, 16, ..., 2048 columns, then 4096), wide[b] = 1 for the
+ * 64-column tile, 0 for the 32-column one, us[2b], us[2b + 1] the two timings (microseconds, 2048 rows,
+ * K = min(n, 128), four matrices).  state: 0 not tuned yet, 1 the default choice (the timing could not
+ * run), 2 measured. */
+HbStatus hbg_tuned_tiles(int32_t device, int32_t *state, int32_t *wide, float *us);
+
 /* No counterpart in the reference: the revision of the hbg_* entry points (HBG_ABI_VERSION). */
 uint32_t hbg_library_version(void);
 /* hydrobem.h:247, 256 */

@@ -37,7 +37,7 @@ def test_abi_version_and_defaults():
     # the reference's HB_ABI_VERSION (crates/hydrobem-c/src/info.rs:15): a caller built against
     # hydrobem.h compares hb_abi_version() with it
     assert L.hb_abi_version() == 8
-    assert L.hbg_library_version() == 8
+    assert L.hbg_library_version() == 9
     o = nv.default_options()
     assert o.precision == nv.HBG_FP64 and o.logarithmic == 1
     assert o.log_tolerance == 1e-4 and o.gravity == 9.80665 and o.density == 1000.0

@@ -57,3 +57,22 @@ def test_singular_matrix_reported():
     with pytest.raises(nv.HydroBEMError) as e:
         nv.debug_lu_f64(A, np.ones((1, n, 1)))
     assert e.value.status == 8  # HB_ERR_NUMERICAL
+
+
+@pytest.mark.gpu
+def test_product_tiles_are_tuned_on_the_device():
+    """The tuner times both tile widths of the FP64 product per width bucket when the device is first used;
+    the choice follows the timings, and the narrow products of the panel recursion (8 to 32 columns, whose
+    64-column tiles would be mostly empty) take the 32-column tile."""
+    from hydrobem_b200 import native as nv
+
+    rng = np.random.default_rng(3)
+    A = rng.standard_normal((1, 40, 40)) + 1j * rng.standard_normal((1, 40, 40))
+    B = rng.standard_normal((1, 40, 2)) + 1j * rng.standard_normal((1, 40, 2))
+    nv.debug_lu_f64(A, B)  # the device is in use from here on
+    t = nv.tuned_tiles(0)
+    assert t["state"] == 2
+    for n, (narrow, wide) in t["us"].items():
+        assert narrow > 0.0 and wide > 0.0
+        assert t["columns"][n] == (64 if wide < 0.98 * narrow else 32)
+    assert all(t["columns"][n] == 32 for n in (8, 16, 32))
