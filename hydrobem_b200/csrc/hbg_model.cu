@@ -10,12 +10,16 @@
 // decomposition.  Items and routes outside this subset are refused with HB_ERR_UNSUPPORTED, as the
 // reference refuses routes it lacks.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cmath>
+#include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 namespace hbg {
@@ -261,7 +265,21 @@ static bool inside(const Loop& l, P2 x) {
     return c;
 }
 
-static std::vector<double> lid(const std::vector<double>& v, bool isx, bool isy, double z0, std::string& why) {
+// The waterplane regions of the stored panels in the quadrant x, y >= 0 (interior.rs:139-153, 358-391):
+// counter-clockwise outer contours, each with its clockwise holes (a hole belongs to the smallest outer
+// contour around it); (sx, sy) maps back to the stored side; target the mean waterline segment length;
+// merge: collinear points merged (the waterline generator; the fan keeps them).  False with the reason.
+struct Regions {
+    std::vector<Loop> outers;
+    std::vector<std::vector<Loop>> holes;
+    double sx = 1.0, sy = 1.0, target = 0.0, tol = 0.0, z0 = 0.0;
+    bool ax_x = false, ax_y = false;
+};
+
+static Loop merge_collinear(const Loop& l, double tol);
+
+static bool regions(const std::vector<double>& v, bool isx, bool isy, double z0, bool merge, Regions& g,
+                    std::string& why) {
     constexpr double SLOPE = 1e-6, PLANE_TOL = 1e-6;
     const size_t P = v.size() / 12;
     double ext = 1.0;  // the mesh reference length
@@ -286,7 +304,10 @@ static std::vector<double> lid(const std::vector<double>& v, bool isx, bool isy,
             segs.push_back({a, b});
         }
     }
-    if (segs.empty()) return why = "the wetted surface has no waterline", std::vector<double>{};
+    if (segs.empty()) return why = "the wetted surface has no waterline", false;
+    double total = 0.0;
+    for (auto& s : segs) total += dist(s.first, s.second);
+    g.target = total / (double)segs.size();
     double mx = 0.0, my = 0.0;
     for (auto& s : segs) mx += s.first.x + s.second.x, my += s.first.y + s.second.y;
     const double sx = isx && mx < 0.0 ? -1.0 : 1.0, sy = isy && my < 0.0 ? -1.0 : 1.0;
@@ -301,7 +322,7 @@ static std::vector<double> lid(const std::vector<double>& v, bool isx, bool isy,
     for (size_t i = 0; i < n; i++)
         for (size_t j = 0; j < n; j++) {
             if (i == j || dist(segs[i].second, segs[j].first) > tol) continue;
-            if (nxt[i] >= 0 || prv[j] >= 0) return why = "waterline contours touch or cross", std::vector<double>{};
+            if (nxt[i] >= 0 || prv[j] >= 0) return why = "waterline contours touch or cross", false;
             nxt[i] = (long)j;
             prv[j] = (long)i;
         }
@@ -323,7 +344,7 @@ static std::vector<double> lid(const std::vector<double>& v, bool isx, bool isy,
             used[k] = true;
             c.push_back(segs[k].first);
             k = nxt[k];
-            if (k < 0) return why = "broken waterline loop", std::vector<double>{};
+            if (k < 0) return why = "broken waterline loop", false;
         }
         loops.push_back(c);
     }
@@ -336,7 +357,7 @@ static std::vector<double> lid(const std::vector<double>& v, bool isx, bool isy,
     auto key_end = [&](P2 p) { return on_y(p) ? std::make_pair(1, -p.y) : std::make_pair(0, p.x); };
     const std::string open = "the waterline does not close";
     for (auto& c : chains)
-        if (!(on_x(c.front()) || on_y(c.front())) || !(on_x(c.back()) || on_y(c.back()))) return why = open, std::vector<double>{};
+        if (!(on_x(c.front()) || on_y(c.front())) || !(on_x(c.back()) || on_y(c.back()))) return why = open, false;
     std::vector<bool> cused(chains.size(), false);
     for (size_t c0 = 0; c0 < chains.size(); c0++) {
         if (cused[c0]) continue;
@@ -356,10 +377,10 @@ static std::vector<double> lid(const std::vector<double>& v, bool isx, bool isy,
                 }
                 wrap = pass == 1;
             }
-            if (best < 0) return why = open, std::vector<double>{};
-            if (ke.first == 0 && key_start(chains[best].front()).first == 1 && !wrap) return why = open, std::vector<double>{};
+            if (best < 0) return why = open, false;
+            if (ke.first == 0 && key_start(chains[best].front()).first == 1 && !wrap) return why = open, false;
             if (wrap) {
-                if (!(ax_x && ax_y)) return why = open, std::vector<double>{};
+                if (!(ax_x && ax_y)) return why = open, false;
                 l.push_back(P2{0.0, 0.0});
             }
             if ((size_t)best == c0) break;
@@ -373,32 +394,54 @@ static std::vector<double> lid(const std::vector<double>& v, bool isx, bool isy,
         for (P2 p : l)
             if (c.empty() || dist(c.back(), p) > tol) c.push_back(p);
         while (c.size() > 1 && dist(c.front(), c.back()) <= tol) c.pop_back();
-        l = c;
+        l = merge ? merge_collinear(c, tol) : c;
     }
-    if (loops_meet(loops, tol)) return why = "waterline contours cross or touch", std::vector<double>{};
-    // interior.rs:360-391 outer loops (counter-clockwise); an opening refuses the fan
-    std::vector<Loop> outers, holes;
+    if (loops_meet(loops, tol)) return why = "waterline contours cross or touch", false;
+    // interior.rs:360-391 outer loops (counter-clockwise) and the holes of each
+    std::vector<Loop> holes;
     for (auto& l : loops)
-        if (l.size() >= 3) (signed_area(l) > 0.0 ? outers : holes).push_back(l);
-    if (outers.empty()) return why = "no enclosed region", std::vector<double>{};
+        if (l.size() >= 3) (signed_area(l) > 0.0 ? g.outers : holes).push_back(l);
+    if (g.outers.empty()) return why = "no enclosed region", false;
+    g.holes.assign(g.outers.size(), {});
     for (auto& h : holes) {
-        bool owned = false;
-        for (auto& o : outers) owned = owned || inside(o, h[0]);
-        if (!owned) return why = "a waterline contour lies outside the body", std::vector<double>{};
-        return why = "a waterplane region has an opening (a moonpool); use 'waterline'", std::vector<double>{};
+        long owner = -1;
+        for (size_t o = 0; o < g.outers.size(); o++)
+            if (inside(g.outers[o], h[0]) &&
+                (owner < 0 || std::fabs(signed_area(g.outers[o])) < std::fabs(signed_area(g.outers[owner]))))
+                owner = (long)o;
+        if (owner < 0) return why = "a waterline contour lies outside the body", false;
+        g.holes[owner].push_back(h);
     }
+    g.sx = sx;
+    g.sy = sy;
+    g.tol = tol;
+    g.z0 = z0;
+    g.ax_x = ax_x;
+    g.ax_y = ax_y;
+    return true;
+}
+
+// interior.rs:394-409 a polygon (3 or 4 corners, counter-clockwise in the quadrant) as a stored panel
+static void emit_panel(const Regions& g, const P2* cs, int k, std::vector<double>& out) {
+    double w[4][3];
+    for (int i = 0; i < k; i++) w[i][0] = g.sx * cs[i].x, w[i][1] = g.sy * cs[i].y, w[i][2] = g.z0;
+    if (g.sx * g.sy < 0.0) std::reverse(&w[0], &w[k]);
+    if (k == 3)
+        for (int d = 0; d < 3; d++) w[3][d] = w[2][d];
+    for (int i = 0; i < 4; i++)
+        for (int d = 0; d < 3; d++) out.push_back(w[i][d]);
+}
+
+static std::vector<double> lid(const std::vector<double>& v, bool isx, bool isy, double z0, std::string& why) {
+    Regions g;
+    if (!regions(v, isx, isy, z0, false, g, why)) return {};
+    const double tol = g.tol;
+    const bool ax_x = g.ax_x, ax_y = g.ax_y;
+    const std::vector<Loop>& outers = g.outers;
+    for (const auto& hs : g.holes)
+        if (!hs.empty()) return why = "a waterplane region has an opening (a moonpool); use 'waterline'", std::vector<double>{};
     std::vector<double> out;
-    // interior.rs:394-409 a polygon of the quadrant as a stored panel
-    auto emit = [&](std::initializer_list<P2> cs) {
-        double w[4][3];
-        int k = 0;
-        for (P2 p : cs) w[k][0] = sx * p.x, w[k][1] = sy * p.y, w[k][2] = z0, k++;
-        if (sx * sy < 0.0) std::reverse(&w[0], &w[k]);
-        if (k == 3)
-            for (int d = 0; d < 3; d++) w[3][d] = w[2][d];
-        for (int i = 0; i < 4; i++)
-            for (int d = 0; d < 3; d++) out.push_back(w[i][d]);
-    };
+    auto emit = [&](std::initializer_list<P2> cs) { emit_panel(g, cs.begin(), (int)cs.size(), out); };
     // interior.rs:447-517 the fan of each region
     for (const Loop& l : outers) {
         double a = 0.0, cx = 0.0, cy = 0.0;
@@ -438,6 +481,433 @@ static std::vector<double> lid(const std::vector<double>& v, bool isx, bool isy,
             for (int k = 1; k < N; k++) emit({at(p, t[k]), at(p, t[k + 1]), at(q, t[k + 1]), at(q, t[k])});
         }
     }
+    return out;
+}
+
+// ------------------------------------------------------------------ waterline generator
+// polygon.rs:154-700 and interior.rs:408-434: the regions (collinear points merged, holes kept)
+// triangulated -- every hole bridged to the outer loop, the bridged polygon cut into ears, Lawson flips
+// to the constrained Delaunay triangulation -- then refined (Ruppert's circumcentre insertion with
+// Shewchuk's rules) to edges of at most twice the mean waterline segment and angles of at least 25
+// degrees, in one fixed order of insertions, so the same triangles on every run.
+
+// polygon.rs:154-170 the loop without the vertices within tol of the line through their neighbours
+static Loop merge_collinear(const Loop& l, double tol) {
+    Loop c = l;
+    bool changed = true;
+    while (changed && c.size() > 3) {
+        changed = false;
+        for (size_t i = 0; i < c.size(); i++) {
+            const size_t n = c.size();
+            const P2 a = c[(i + n - 1) % n], b = c[i], d = c[(i + 1) % n];
+            if (std::fabs(orient(a, b, d)) <= tol * dist(a, d)) {
+                c.erase(c.begin() + (long)i);
+                changed = true;
+                break;
+            }
+        }
+    }
+    return c;
+}
+
+// polygon.rs:220-258 the holes merged into the outer loop (the rightmost hole first), each by a bridge
+// from its rightmost vertex (the last of equal ones) to the nearest vertex visible from it (the first
+// of equal ones), preferably to its right
+static bool bridge(const Loop& outer, std::vector<Loop> holes, double eps, Loop& poly) {
+    poly = outer;
+    auto right = [](const Loop& l) {
+        double r = -INFINITY;
+        for (const P2& p : l) r = std::max(r, p.x);
+        return r;
+    };
+    std::stable_sort(holes.begin(), holes.end(), [&](const Loop& a, const Loop& b) { return right(b) < right(a); });
+    for (size_t hi = 0; hi < holes.size(); hi++) {
+        const Loop& h = holes[hi];
+        size_t mi = 0;
+        for (size_t i = 0; i < h.size(); i++)
+            if (h[i].x >= h[mi].x) mi = i;
+        const P2 m = h[mi];
+        const size_t n = poly.size();
+        auto visible = [&](size_t k) {
+            const P2 p = poly[k];
+            for (size_t e = 0; e < n; e++)
+                if (!(e == k || (e + 1) % n == k) && meet(m, p, poly[e], poly[(e + 1) % n])) return false;
+            for (size_t e = 0; e < h.size(); e++)
+                if (!(e == mi || (e + 1) % h.size() == mi) && meet(m, p, h[e], h[(e + 1) % h.size()])) return false;
+            for (size_t l = hi + 1; l < holes.size(); l++)
+                for (size_t e = 0; e < holes[l].size(); e++)
+                    if (meet(m, p, holes[l][e], holes[l][(e + 1) % holes[l].size()])) return false;
+            return true;
+        };
+        long best = -1;
+        for (int pass = 0; pass < 2 && best < 0; pass++)
+            for (size_t k = 0; k < n; k++)
+                if ((pass == 1 || poly[k].x >= m.x - eps) && visible(k) &&
+                    (best < 0 || dist(poly[k], m) < dist(poly[best], m)))
+                    best = (long)k;
+        if (best < 0) return false;
+        Loop next(poly.begin(), poly.begin() + best + 1);
+        for (size_t k = 0; k <= h.size(); k++) next.push_back(h[(mi + k) % h.size()]);
+        next.insert(next.end(), poly.begin() + best, poly.end());
+        poly = next;
+    }
+    return true;
+}
+
+using Tri = std::array<long, 3>;
+
+// polygon.rs:262-306 ear clipping of the counter-clockwise bridged polygon; straight corners dropped
+static bool ears(const Loop& poly, double eps, std::vector<Tri>& out) {
+    auto straight = [](P2 a, P2 b, P2 c) { return std::fabs(orient(a, b, c)) <= 1e-12 * dist(a, b) * dist(b, c); };
+    std::vector<long> idx(poly.size());
+    for (size_t i = 0; i < idx.size(); i++) idx[i] = (long)i;
+    while (idx.size() > 3) {
+        const size_t n = idx.size();
+        bool clipped = false;
+        for (size_t i = 0; i < n; i++) {
+            const long ia = idx[(i + n - 1) % n], ib = idx[i], ic = idx[(i + 1) % n];
+            const P2 a = poly[ia], b = poly[ib], c = poly[ic];
+            if (straight(a, b, c)) {
+                idx.erase(idx.begin() + (long)i);
+                clipped = true;
+                break;
+            }
+            if (orient(a, b, c) < 0.0) continue;  // reflex
+            auto at = [&](P2 x, P2 y) { return std::fabs(x.x - y.x) <= eps && std::fabs(x.y - y.y) <= eps; };
+            bool ear = true;
+            for (long k : idx) {
+                const P2 x = poly[k];
+                if (!(at(x, a) || at(x, b) || at(x, c) ||
+                      !(orient(a, b, x) > 0.0 && orient(b, c, x) > 0.0 && orient(c, a, x) > 0.0))) {
+                    ear = false;
+                    break;
+                }
+            }
+            if (ear) {
+                out.push_back({ia, ib, ic});
+                idx.erase(idx.begin() + (long)i);
+                clipped = true;
+                break;
+            }
+        }
+        if (!clipped) return false;
+    }
+    if (idx.size() == 3 && !straight(poly[idx[0]], poly[idx[1]], poly[idx[2]])) out.push_back({idx[0], idx[1], idx[2]});
+    return true;
+}
+
+static double incircle(P2 pa, P2 pb, P2 pc, P2 pd) {
+    const double adx = pa.x - pd.x, ady = pa.y - pd.y, bdx = pb.x - pd.x, bdy = pb.y - pd.y;
+    const double cdx = pc.x - pd.x, cdy = pc.y - pd.y;
+    return (adx * adx + ady * ady) * (bdx * cdy - cdx * bdy) - (bdx * bdx + bdy * bdy) * (adx * cdy - cdx * ady) +
+           (cdx * cdx + cdy * cdy) * (adx * bdy - bdx * ady);
+}
+
+using EdgeKey = std::pair<long, long>;
+static EdgeKey ekey(long a, long b) { return {std::min(a, b), std::max(a, b)}; }
+constexpr long NONE = -1;
+
+// polygon.rs:310-388 Lawson flips to the constrained Delaunay triangulation, in place
+static bool delaunay_flips(const Loop& p, std::vector<Tri>& tris) {
+    std::map<EdgeKey, std::array<long, 2>> owners;
+    std::vector<EdgeKey> fixed;
+    for (size_t t = 0; t < tris.size(); t++)
+        for (int e = 0; e < 3; e++) {
+            const EdgeKey k = ekey(tris[t][e], tris[t][(e + 1) % 3]);
+            auto it = owners.try_emplace(k, std::array<long, 2>{NONE, NONE}).first;
+            if (it->second[0] == NONE)
+                it->second[0] = (long)t;
+            else if (it->second[1] == NONE)
+                it->second[1] = (long)t;
+            else
+                fixed.push_back(k);
+        }
+    for (auto& k : fixed) owners[k] = {NONE, NONE};
+    const size_t limit = std::max<size_t>(tris.size() * tris.size(), 16);
+    size_t flips = 0;
+    for (;;) {
+        bool flipped = false;
+        for (size_t t = 0; t < tris.size(); t++)
+            for (int e = 0; e < 3; e++) {
+                const long a = tris[t][e], b = tris[t][(e + 1) % 3], c = tris[t][(e + 2) % 3];
+                const auto o = owners.at(ekey(a, b));
+                const long u = o[0] == (long)t ? o[1] : o[0];
+                if (u == NONE || u > (long)t) continue;
+                int f = -1;
+                for (int g = 0; g < 3 && f < 0; g++)
+                    if (tris[u][g] == b && tris[u][(g + 1) % 3] == a) f = g;
+                if (f < 0) return false;
+                const long d = tris[u][(f + 2) % 3];
+                const double ob = orient(p[a], p[b], p[c]);
+                if (incircle(p[a], p[b], p[c], p[d]) > 1e-12 * ob * ob && orient(p[c], p[d], p[b]) > 0.0 &&
+                    orient(p[d], p[c], p[a]) > 0.0) {
+                    tris[t] = {c, d, b};
+                    tris[u] = {d, c, a};
+                    owners.erase(ekey(a, b));
+                    owners[ekey(c, d)] = {(long)t, u};
+                    const std::array<std::tuple<EdgeKey, long, long>, 2> fix = {
+                        std::make_tuple(ekey(d, b), u, (long)t), std::make_tuple(ekey(c, a), (long)t, u)};
+                    for (auto& [edge, from, to] : fix)
+                        for (long& x : owners.at(edge))
+                            if (x == from) x = to;
+                    flipped = true;
+                    if (++flips > limit) return false;
+                    break;  // the triangle t is new: its edges at the next pass
+                }
+            }
+        if (!flipped) return true;
+    }
+}
+
+static P2 circumcentre(P2 a, P2 b, P2 c) {
+    const double bx = b.x - a.x, by = b.y - a.y, cx = c.x - a.x, cy = c.y - a.y;
+    const double d = 2.0 * (bx * cy - by * cx);
+    const double b2 = bx * bx + by * by, c2 = cx * cx + cy * cy;
+    return P2{a.x + (cy * b2 - by * c2) / d, a.y + (bx * c2 - cx * b2) / d};
+}
+
+// polygon.rs:428-576 a triangulation under refinement
+struct Mesh2 {
+    std::vector<P2> p;
+    std::vector<Tri> t;
+    std::vector<bool> alive;
+    std::map<EdgeKey, std::array<long, 2>> owners;
+    std::map<EdgeKey, double> segs;  // boundary edges, with the length of the boundary edge each was split from
+
+    long add_tri(Tri q) {
+        const long id = (long)t.size();
+        t.push_back(q);
+        alive.push_back(true);
+        for (int e = 0; e < 3; e++) {
+            auto& o = owners.try_emplace(ekey(q[e], q[(e + 1) % 3]), std::array<long, 2>{NONE, NONE}).first->second;
+            if (o[0] == NONE)
+                o[0] = id;
+            else
+                o[1] = id;
+        }
+        return id;
+    }
+    void kill(long id) {
+        alive[id] = false;
+        const Tri q = t[id];
+        for (int e = 0; e < 3; e++) {
+            auto it = owners.find(ekey(q[e], q[(e + 1) % 3]));
+            if (it == owners.end()) continue;
+            for (long& x : it->second)
+                if (x == id) x = NONE;
+            if (it->second[0] == NONE && it->second[1] == NONE) owners.erase(it);
+        }
+    }
+    long across(long tt, long a, long b) const {
+        auto it = owners.find(ekey(a, b));
+        if (it == owners.end()) return NONE;
+        return it->second[0] == tt ? it->second[1] : it->second[0];
+    }
+    bool is_seg(long a, long b) const { return segs.count(ekey(a, b)) != 0; }
+    // the triangle holding c, walked from tt along the line from its centroid (kind 0), the first boundary
+    // edge the line meets (kind 1, in u, v), or lost (kind 2)
+    int locate(long tt, P2 c, long& out, long& u_out, long& v_out) const {
+        Tri q = t[tt];
+        const P2 g{(p[q[0]].x + p[q[1]].x + p[q[2]].x) / 3.0, (p[q[0]].y + p[q[1]].y + p[q[2]].y) / 3.0};
+        long cur = tt, from = NONE;
+        for (size_t step = 0; step < t.size() + 3; step++) {
+            q = t[cur];
+            long ex_u = NONE, ex_v = NONE, ex_n = NONE, f_u = NONE, f_v = NONE, f_n = NONE;
+            bool any = false, found = false;
+            for (int e = 0; e < 3; e++) {
+                const long u = q[e], v = q[(e + 1) % 3];
+                const double su = orient(g, c, p[u]), sv = orient(g, c, p[v]);
+                if (orient(p[u], p[v], c) < 0.0 && ((su <= 0.0 && sv >= 0.0) || (su >= 0.0 && sv <= 0.0))) {
+                    const long n = across(cur, u, v);
+                    if (!any) f_u = u, f_v = v, f_n = n, any = true;
+                    if (!found && n != from) ex_u = u, ex_v = v, ex_n = n, found = true;
+                }
+            }
+            if (!found && any) ex_u = f_u, ex_v = f_v, ex_n = f_n, found = true;
+            if (!found) {
+                bool in = true;
+                for (int e = 0; e < 3; e++) in = in && orient(p[q[e]], p[q[(e + 1) % 3]], c) >= 0.0;
+                if (!in) return 2;
+                out = cur;
+                return 0;
+            }
+            if (is_seg(ex_u, ex_v) || ex_n == NONE) {
+                u_out = ex_u;
+                v_out = ex_v;
+                return 1;
+            }
+            from = cur;
+            cur = ex_n;
+        }
+        return 2;
+    }
+    // the cavity of x from tt (triangles reachable across non-boundary edges whose circumcircles hold x)
+    // and its boundary edges in the sense of their triangles
+    void cavity(long tt, P2 x, std::vector<long>& cav, std::vector<std::pair<long, long>>& bnd) const {
+        cav.assign(1, tt);
+        auto has = [&](long n) { return std::find(cav.begin(), cav.end(), n) != cav.end(); };
+        for (size_t k = 0; k < cav.size(); k++) {
+            const Tri q = t[cav[k]];
+            for (int e = 0; e < 3; e++) {
+                const long u = q[e], v = q[(e + 1) % 3];
+                if (is_seg(u, v)) continue;
+                const long n = across(cav[k], u, v);
+                if (n == NONE || has(n)) continue;
+                const Tri r = t[n];
+                if (incircle(p[r[0]], p[r[1]], p[r[2]], x) > 0.0) cav.push_back(n);
+            }
+        }
+        bnd.clear();
+        for (long c : cav) {
+            const Tri q = t[c];
+            for (int e = 0; e < 3; e++) {
+                const long u = q[e], v = q[(e + 1) % 3];
+                const long n = across(c, u, v);
+                if (n == NONE || !has(n) || is_seg(u, v)) bnd.push_back({u, v});
+            }
+        }
+    }
+    // the cavity replaced by the fan from the new vertex x to its boundary edges but skip; false (nothing
+    // changed) when a fan triangle would not turn counter-clockwise by more than the rounding
+    bool insert(const std::vector<long>& cav, const std::vector<std::pair<long, long>>& bnd, P2 x,
+                std::pair<long, long> skip, std::vector<long>& fresh) {
+        std::vector<std::pair<long, long>> fan;
+        for (auto& uv : bnd)
+            if (uv != skip) fan.push_back(uv);
+        for (auto& [u, v] : fan) {
+            const P2 pu = p[u], pv = p[v];
+            const double l2 = (pu.x - pv.x) * (pu.x - pv.x) + (pu.y - pv.y) * (pu.y - pv.y);
+            if (orient(pu, pv, x) <= 1e-9 * l2) return false;
+        }
+        const long id = (long)p.size();
+        p.push_back(x);
+        for (long c : cav) kill(c);
+        fresh.clear();
+        for (auto& [u, v] : fan) fresh.push_back(add_tri({u, v, id}));
+        return true;
+    }
+};
+
+// polygon.rs:593-700 the triangles (counter-clockwise) of a region refined to `size` and the smallest
+// angle of 25 degrees; at most cap live triangles
+static bool triangulate_refined(const Loop& outer, const std::vector<Loop>& holes, double eps, double size, size_t cap,
+                                std::vector<std::array<P2, 3>>& out, std::string& why) {
+    Loop poly;
+    if (!bridge(outer, holes, eps, poly)) return why = "polygon triangulation: a hole without a bridge", false;
+    std::vector<Tri> tris;
+    if (!ears(poly, eps, tris)) return why = "polygon triangulation: the ear clipping failed", false;
+    Mesh2 m;
+    std::map<std::pair<uint64_t, uint64_t>, long> id_of;  // the two ends of a bridge are exact copies: one vertex
+    std::vector<long> ids;
+    for (const P2& x : poly) {
+        uint64_t bx, by;
+        std::memcpy(&bx, &x.x, 8);
+        std::memcpy(&by, &x.y, 8);
+        auto it = id_of.try_emplace({bx, by}, (long)m.p.size());
+        if (it.second) m.p.push_back(x);
+        ids.push_back(it.first->second);
+    }
+    std::vector<Tri> t;
+    for (const Tri& q : tris) t.push_back({ids[q[0]], ids[q[1]], ids[q[2]]});
+    if (!delaunay_flips(m.p, t)) return why = "polygon triangulation: the Delaunay flips do not end", false;
+    for (const Tri& q : t) m.add_tri(q);
+    double shortest = INFINITY;
+    for (size_t i = 0; i < m.t.size(); i++) {
+        const Tri q = m.t[i];
+        for (int e = 0; e < 3; e++) {
+            const long u = q[e], v = q[(e + 1) % 3];
+            if (m.across((long)i, u, v) == NONE) {
+                const double l = dist(m.p[u], m.p[v]);
+                m.segs[ekey(u, v)] = l;
+                shortest = std::min(shortest, l);
+            }
+        }
+    }
+    const double ratio = 0.5 / std::sin(25.0 * PI / 180.0);  // circumradius over the shortest edge
+    std::deque<long> queue;
+    for (size_t i = 0; i < m.t.size(); i++) queue.push_back((long)i);
+    size_t live = m.t.size();
+    std::vector<long> cav, fresh;
+    std::vector<std::pair<long, long>> bnd;
+    while (!queue.empty()) {
+        const long i = queue.front();
+        queue.pop_front();
+        if (!m.alive[i] || live > cap) continue;
+        const Tri q = m.t[i];
+        const P2 a = m.p[q[0]], b = m.p[q[1]], c = m.p[q[2]];
+        const double l0 = dist(b, c), l1 = dist(c, a), l2 = dist(a, b);
+        const double lo = std::min(std::min(l0, l1), l2), hi = std::max(std::max(l0, l1), l2);
+        const P2 cc = circumcentre(a, b, c);
+        const bool big = hi > size;
+        const bool skinny = dist(cc, a) > ratio * lo && lo >= 0.25 * shortest;
+        if (!big && !skinny) continue;
+        long t0 = NONE, su = NONE, sv = NONE;
+        const int kind = m.locate(i, cc, t0, su, sv);
+        if (kind == 2) continue;
+        bool split = kind == 1, fan = false;
+        size_t removed = 0;
+        if (kind == 0) {
+            m.cavity(t0, cc, cav, bnd);
+            for (auto& [u, v] : bnd)
+                if (m.is_seg(u, v)) {
+                    const P2 pu = m.p[u], pv = m.p[v];
+                    if ((pu.x - cc.x) * (pv.x - cc.x) + (pu.y - cc.y) * (pv.y - cc.y) < 0.0) {
+                        split = true, su = u, sv = v;
+                        break;
+                    }
+                }
+            if (!split) {
+                removed = cav.size();
+                fan = m.insert(cav, bnd, cc, {NONE, NONE}, fresh);
+            }
+        }
+        if (split) {
+            const double l = dist(m.p[su], m.p[sv]);
+            if (!(l > size || l >= 0.75 * std::min(0.5 * size, m.segs.at(ekey(su, sv))))) continue;
+            const auto s = m.owners.at(ekey(su, sv));
+            const long ts = s[0] != NONE ? s[0] : s[1];
+            const Tri qs = m.t[ts];
+            long u = NONE, v = NONE;
+            for (int e = 0; e < 3 && u == NONE; e++)
+                if (ekey(qs[e], qs[(e + 1) % 3]) == ekey(su, sv)) u = qs[e], v = qs[(e + 1) % 3];
+            const P2 mid{0.5 * (m.p[u].x + m.p[v].x), 0.5 * (m.p[u].y + m.p[v].y)};
+            m.cavity(ts, mid, cav, bnd);
+            const double from = m.segs.at(ekey(u, v));
+            if (m.insert(cav, bnd, mid, {u, v}, fresh)) {
+                const long x = (long)m.p.size() - 1;
+                m.segs.erase(ekey(u, v));
+                m.segs[ekey(u, x)] = from;
+                m.segs[ekey(x, v)] = from;
+                live += fresh.size() - cav.size();
+                for (long f : fresh) queue.push_back(f);
+                if (m.alive[i]) queue.push_back(i);
+            }
+        } else if (fan) {
+            live += fresh.size() - removed;
+            for (long f : fresh) queue.push_back(f);
+        }
+    }
+    for (size_t i = 0; i < m.t.size(); i++)
+        if (m.alive[i]) out.push_back({m.p[m.t[i][0]], m.p[m.t[i][1]], m.p[m.t[i][2]]});
+    return true;
+}
+
+// interior.rs:408-434 the waterline generator on the stored panels
+static std::vector<double> waterline_lid(const std::vector<double>& v, bool isx, bool isy, double z0, std::string& why) {
+    constexpr size_t MAX_GENERATED = 200000;  // more would make the dense system impractical
+    Regions g;
+    if (!regions(v, isx, isy, z0, true, g, why)) return {};
+    std::vector<std::array<P2, 3>> done;
+    for (size_t o = 0; o < g.outers.size(); o++) {
+        if (!triangulate_refined(g.outers[o], g.holes[o], g.tol, 2.0 * g.target, MAX_GENERATED - done.size(), done, why))
+            return {};
+        if (done.size() > MAX_GENERATED)
+            return why = "the waterplane needs more than 200000 panels of twice the mean waterline segment length; use "
+                         "'graded' or a mesh of its own",
+                   std::vector<double>{};
+    }
+    std::vector<double> out;
+    for (auto& tri : done) emit_panel(g, tri.data(), 3, out);
     return out;
 }
 
@@ -481,12 +951,14 @@ static HbStatus body_panels(const HbModel* model, const BodyObj& b, int form, st
         bv.insert(bv.end(), lv.begin(), lv.end());
         bk.resize(bv.size() / 12, HBG_INTERIOR);
     }
-    if (b.interior == "graded") {
+    if (b.interior == "graded" || b.interior == "waterline") {
         // generated on the stored panels and reflected like them (interior.rs:521-575)
         std::string why;
-        std::vector<double> lv = graded::lid(mesh->vertices, (msym & HBG_SYM_YZ) != 0, (msym & HBG_SYM_XZ) != 0,
-                                             -b.position[2], why);
-        if (!why.empty()) return refuse(HB_ERR_VALUE, "body '" + b.name + "': interior surface 'graded': " + why);
+        const bool isx = (msym & HBG_SYM_YZ) != 0, isy = (msym & HBG_SYM_XZ) != 0;
+        std::vector<double> lv = b.interior == "graded" ? graded::lid(mesh->vertices, isx, isy, -b.position[2], why)
+                                                        : graded::waterline_lid(mesh->vertices, isx, isy, -b.position[2], why);
+        if (!why.empty())
+            return refuse(HB_ERR_VALUE, "body '" + b.name + "': interior surface '" + b.interior + "': " + why);
         if (!sectors) lv = reflect(lv, mesh->symmetry);
         bv.insert(bv.end(), lv.begin(), lv.end());
         bk.resize(bv.size() / 12, HBG_INTERIOR);
@@ -810,9 +1282,9 @@ extern "C" HbStatus hb_set_text(HbModel* model, uint64_t object, const char* ite
             BodyObj& b = model->bodies[object - OBJ_BODY0];
             if (it == "mesh") return b.mesh = v, HB_OK;
             if (it == "interior_surface") {
-                if (v != "none" && v != "detect" && v != "mesh" && v != "projected" && v != "graded")
+                if (v != "none" && v != "detect" && v != "mesh" && v != "projected" && v != "graded" && v != "waterline")
                     return refuse(HB_ERR_UNSUPPORTED,
-                                  "interior_surface none, detect, projected, graded or mesh on this route");
+                                  "interior_surface none, detect, projected, graded, waterline or mesh on this route");
                 return b.interior = v, HB_OK;
             }
             if (it == "interior_surface_mesh") return b.interior_mesh = v, HB_OK;

@@ -28,7 +28,9 @@ reference's own solver outputs (``tests/data/regression/lo_cylinder_drift.npz``)
 
 from __future__ import annotations
 
+import collections
 import ctypes
+import math
 import os
 import subprocess
 from pathlib import Path
@@ -577,21 +579,10 @@ def _signed_area(loop):
     return 0.5 * sum(loop[k][0] * loop[(k + 1) % n][1] - loop[(k + 1) % n][0] * loop[k][1] for k in range(n))
 
 
-def graded_lid(verts, isx=0, isy=0, z0=0.0, reference_length=1.0):
-    """interior.rs:139-515 graded: the interior free surface fanned from the area centroid of each
-    waterplane region to its waterline segments, the rays divided at t_k = sin(pi k / (2N)).
-
-    ``verts`` [P][4][3] the stored panels of the mesh (one sector when isx / isy declare the planes
-    x = 0 / y = 0); returns the generated panels [Q][4][3] in the same stored form (a triangle repeats its
-    last vertex), facing up.  Steps:
-
-    - waterline segments (interior.rs:158-214): the edges lying in z0 (within tol = 1e-6 max(reference
-      length, |vertex coordinates|)) of the non-horizontal panels (|n_h| >= 1e-6), oriented along
-      z x n_h, mapped to the quadrant x, y >= 0 by the sign of the coordinate sums on symmetric axes;
-    - chains and loops (interior.rs:217-272), open chains closed along the symmetry axes through the
-      quadrant corner (interior.rs:274-340), repeated points dropped (interior.rs:343-357);
-    - contours that cross or touch, openings, or a region whose waterline a centroid ray meets twice
-      raise ValueError, as the reference does."""
+def _waterplane_loops(verts, isx, isy, z0, reference_length, merge_collinear):
+    """interior.rs:139-153 the closed waterline contours of the stored panels in the quadrant x, y >= 0:
+    (loops, sx, sy, target = the mean waterline segment length, ax_x, ax_y, tol); with merge_collinear
+    the collinear points of every loop are merged (the waterline generator), not for the fan."""
     v = np.asarray(verts, dtype=np.float64).reshape(-1, 4, 3)
     tol = 1e-6 * max(reference_length, float(np.abs(v).max()) if v.size else 0.0)
     segs = []
@@ -716,9 +707,29 @@ def graded_lid(verts, isx=0, isy=0, z0=0.0, reference_length=1.0):
                 c.append(p)
         while len(c) > 1 and _dist(c[0], c[-1]) <= tol:
             c.pop()
-        loops[i] = c
+        loops[i] = _merge_collinear(c, tol) if merge_collinear else c
     if _loops_meet(loops, tol):
         raise ValueError("waterline contours cross or touch")
+    return loops, sx, sy, total / len(segs), ax_x, ax_y, tol
+
+
+def graded_lid(verts, isx=0, isy=0, z0=0.0, reference_length=1.0):
+    """interior.rs:139-515 graded: the interior free surface fanned from the area centroid of each
+    waterplane region to its waterline segments, the rays divided at t_k = sin(pi k / (2N)).
+
+    ``verts`` [P][4][3] the stored panels of the mesh (one sector when isx / isy declare the planes
+    x = 0 / y = 0); returns the generated panels [Q][4][3] in the same stored form (a triangle repeats its
+    last vertex), facing up.  Steps:
+
+    - waterline segments (interior.rs:158-214): the edges lying in z0 (within tol = 1e-6 max(reference
+      length, |vertex coordinates|)) of the non-horizontal panels (|n_h| >= 1e-6), oriented along
+      z x n_h, mapped to the quadrant x, y >= 0 by the sign of the coordinate sums on symmetric axes;
+    - chains and loops (interior.rs:217-272), open chains closed along the symmetry axes through the
+      quadrant corner (interior.rs:274-340), repeated points dropped (interior.rs:343-357);
+    - contours that cross or touch, openings, or a region whose waterline a centroid ray meets twice
+      raise ValueError, as the reference does."""
+    v = np.asarray(verts, dtype=np.float64).reshape(-1, 4, 3)
+    loops, sx, sy, _, ax_x, ax_y, tol = _waterplane_loops(v, isx, isy, z0, reference_length, False)
     outers = [lp for lp in loops if len(lp) >= 3 and _signed_area(lp) > 0.0]
     holes = [lp for lp in loops if len(lp) >= 3 and not _signed_area(lp) > 0.0]
     if not outers:
@@ -929,3 +940,424 @@ def solve_body(verts, omegas, headings_deg=(), depth=np.inf, kinds=None, grav=GR
         out["drift"] = momentum_drift(omegas, headings_deg, out["kd"], out["kdt"], out["kr"], out["krt"],
                                       out.get("motions"), depth, grav, rho)
     return out
+
+
+# ------------------------------------------------------------------ the waterline generator
+# polygon.rs: holes bridged to the outer loop, ear clipping, Lawson flips, Delaunay refinement;
+# interior.rs:408-434 the regions triangulated and mapped to stored panels.
+_NONE = -1
+REFINE_MIN_ANGLE = 25.0
+MAX_GENERATED = 200000
+
+
+def _merge_collinear(loop, tol):
+    """polygon.rs:154-170 the loop without the vertices within tol of the line through their neighbours
+    (the first such vertex, again from the start, until none), at least three kept."""
+    c = list(loop)
+    changed = True
+    while changed and len(c) > 3:
+        changed = False
+        for i in range(len(c)):
+            n = len(c)
+            a, b, d = c[(i + n - 1) % n], c[i], c[(i + 1) % n]
+            if abs(_orient(a, b, d)) <= tol * _dist(a, d):
+                del c[i]
+                changed = True
+                break
+    return c
+
+
+def _bridge(outer, holes, eps):
+    """polygon.rs:220-258 the holes merged into the outer loop, the rightmost hole first, each by a bridge
+    from its rightmost vertex to the nearest visible vertex of the polygon so far (to its right if any)."""
+    poly = list(outer)
+
+    def right(lp):
+        r = -np.inf
+        for p in lp:
+            r = max(r, p[0])
+        return r
+
+    hs = sorted(holes, key=right, reverse=True)  # stable, as sort_by
+    for hi, h in enumerate(hs):
+        mi = 0
+        for i in range(len(h)):  # max_by: the last of equal maxima
+            if h[i][0] >= h[mi][0]:
+                mi = i
+        m = h[mi]
+        n = len(poly)
+        later = hs[hi + 1:]
+
+        def visible(k):
+            p = poly[k]
+            for e in range(n):
+                if not (e == k or (e + 1) % n == k) and _meet(m, p, poly[e], poly[(e + 1) % n]):
+                    return False
+            for e in range(len(h)):
+                if not (e == mi or (e + 1) % len(h) == mi) and _meet(m, p, h[e], h[(e + 1) % len(h)]):
+                    return False
+            for lp in later:
+                for e in range(len(lp)):
+                    if _meet(m, p, lp[e], lp[(e + 1) % len(lp)]):
+                        return False
+            return True
+
+        def nearest(cands):  # min_by: the first of equal minima
+            best = None
+            for k in cands:
+                if best is None or _dist(poly[k], m) < _dist(poly[best], m):
+                    best = k
+            return best
+
+        best = nearest([k for k in range(n) if poly[k][0] >= m[0] - eps and visible(k)])
+        if best is None:
+            best = nearest([k for k in range(n) if visible(k)])
+        if best is None:
+            raise RuntimeError("polygon triangulation: a hole without a bridge")
+        poly = poly[:best + 1] + [h[(mi + k) % len(h)] for k in range(len(h) + 1)] + poly[best:]
+    return poly
+
+
+def _ears(poly, eps):
+    """polygon.rs:262-306 ear clipping of the counter-clockwise bridged polygon (index triples); a
+    straight corner (sine below 1e-12) is dropped."""
+    def straight(a, b, c):
+        return abs(_orient(a, b, c)) <= 1e-12 * _dist(a, b) * _dist(b, c)
+
+    out = []
+    idx = list(range(len(poly)))
+    while len(idx) > 3:
+        n = len(idx)
+        clipped = False
+        for i in range(n):
+            ia, ib, ic = idx[(i + n - 1) % n], idx[i], idx[(i + 1) % n]
+            a, b, c = poly[ia], poly[ib], poly[ic]
+            if straight(a, b, c):
+                del idx[i]
+                clipped = True
+                break
+            if _orient(a, b, c) < 0.0:
+                continue
+
+            def at(x, y):
+                return abs(x[0] - y[0]) <= eps and abs(x[1] - y[1]) <= eps
+
+            ear = True
+            for k in idx:
+                x = poly[k]
+                if not (at(x, a) or at(x, b) or at(x, c)
+                        or not (_orient(a, b, x) > 0.0 and _orient(b, c, x) > 0.0 and _orient(c, a, x) > 0.0)):
+                    ear = False
+                    break
+            if ear:
+                out.append([ia, ib, ic])
+                del idx[i]
+                clipped = True
+                break
+        if not clipped:
+            raise RuntimeError("polygon triangulation: the ear clipping failed")
+    if len(idx) == 3 and not straight(poly[idx[0]], poly[idx[1]], poly[idx[2]]):
+        out.append([idx[0], idx[1], idx[2]])
+    return out
+
+
+def _incircle(pa, pb, pc, pd):
+    adx, ady, bdx, bdy = pa[0] - pd[0], pa[1] - pd[1], pb[0] - pd[0], pb[1] - pd[1]
+    cdx, cdy = pc[0] - pd[0], pc[1] - pd[1]
+    return ((adx * adx + ady * ady) * (bdx * cdy - cdx * bdy) - (bdx * bdx + bdy * bdy) * (adx * cdy - cdx * ady)
+            + (cdx * cdx + cdy * cdy) * (adx * bdy - bdx * ady))
+
+
+def _key(a, b):
+    return (min(a, b), max(a, b))
+
+
+def _delaunay_flips(p, tris):
+    """polygon.rs:310-388 Lawson flips to the constrained Delaunay triangulation, in place: passes over
+    the triangles, each inner edge at its later triangle, until a pass flips none."""
+    owners, fixed = {}, []
+    for t, q in enumerate(tris):
+        for e in range(3):
+            k = _key(q[e], q[(e + 1) % 3])
+            o = owners.setdefault(k, [_NONE, _NONE])
+            if o[0] == _NONE:
+                o[0] = t
+            elif o[1] == _NONE:
+                o[1] = t
+            else:
+                fixed.append(k)
+    for k in fixed:
+        owners[k] = [_NONE, _NONE]
+    limit = max(len(tris) * len(tris), 16)
+    flips = 0
+    while True:
+        flipped = False
+        for t in range(len(tris)):
+            for e in range(3):
+                a, b, c = tris[t][e], tris[t][(e + 1) % 3], tris[t][(e + 2) % 3]
+                o = owners[_key(a, b)]
+                u = o[1] if o[0] == t else o[0]
+                if u == _NONE or u > t:
+                    continue
+                f = next((f for f in range(3) if tris[u][f] == b and tris[u][(f + 1) % 3] == a), None)
+                if f is None:
+                    raise RuntimeError("polygon triangulation: two triangles turned the same way")
+                d = tris[u][(f + 2) % 3]
+                ob = _orient(p[a], p[b], p[c])
+                if (_incircle(p[a], p[b], p[c], p[d]) > 1e-12 * ob * ob and _orient(p[c], p[d], p[b]) > 0.0
+                        and _orient(p[d], p[c], p[a]) > 0.0):
+                    tris[t] = [c, d, b]
+                    tris[u] = [d, c, a]
+                    del owners[_key(a, b)]
+                    owners[_key(c, d)] = [t, u]
+                    for edge, frm, to in ((_key(d, b), u, t), (_key(c, a), t, u)):
+                        o = owners[edge]
+                        for x in range(2):
+                            if o[x] == frm:
+                                o[x] = to
+                    flipped = True
+                    flips += 1
+                    if flips > limit:
+                        raise RuntimeError("polygon triangulation: the Delaunay flips do not end")
+                    break
+        if not flipped:
+            return
+
+
+def _circumcentre(a, b, c):
+    bx, by, cx, cy = b[0] - a[0], b[1] - a[1], c[0] - a[0], c[1] - a[1]
+    d = 2.0 * (bx * cy - by * cx)
+    b2, c2 = bx * bx + by * by, cx * cx + cy * cy
+    return (a[0] + (cy * b2 - by * c2) / d, a[1] + (bx * c2 - cx * b2) / d)
+
+
+class _Mesh2:
+    """polygon.rs:428-576 a triangulation under refinement: triangles (dead ones kept), the map of each
+    edge to its two triangles, the boundary segments with the length of the edge each was split from."""
+
+    def __init__(self, p):
+        self.p, self.t, self.alive, self.owners, self.segs = p, [], [], {}, {}
+
+    def add_tri(self, q):
+        i = len(self.t)
+        self.t.append(q)
+        self.alive.append(True)
+        for e in range(3):
+            o = self.owners.setdefault(_key(q[e], q[(e + 1) % 3]), [_NONE, _NONE])
+            if o[0] == _NONE:
+                o[0] = i
+            else:
+                o[1] = i
+        return i
+
+    def kill(self, i):
+        self.alive[i] = False
+        q = self.t[i]
+        for e in range(3):
+            k = _key(q[e], q[(e + 1) % 3])
+            o = self.owners.get(k)
+            if o is not None:
+                for x in range(2):
+                    if o[x] == i:
+                        o[x] = _NONE
+                if o[0] == _NONE and o[1] == _NONE:
+                    del self.owners[k]
+
+    def across(self, t, a, b):
+        o = self.owners.get(_key(a, b))
+        if o is None:
+            return _NONE
+        return o[1] if o[0] == t else o[0]
+
+    def locate(self, t, c):
+        """('inside', t) for the triangle holding c, walked from t along the line from its centroid,
+        ('segment', u, v) for the first boundary edge the line meets, or ('lost',)."""
+        p = self.p
+        q = self.t[t]
+        g = ((p[q[0]][0] + p[q[1]][0] + p[q[2]][0]) / 3.0, (p[q[0]][1] + p[q[1]][1] + p[q[2]][1]) / 3.0)
+        cur, frm = t, _NONE
+        for _ in range(len(self.t) + 3):
+            q = self.t[cur]
+            crossed = []
+            for e in range(3):
+                u, v = q[e], q[(e + 1) % 3]
+                su, sv = _orient(g, c, p[u]), _orient(g, c, p[v])
+                if _orient(p[u], p[v], c) < 0.0 and ((su <= 0.0 and sv >= 0.0) or (su >= 0.0 and sv <= 0.0)):
+                    crossed.append((u, v, self.across(cur, u, v)))
+            ex = next((x for x in crossed if x[2] != frm), crossed[0] if crossed else None)
+            if ex is None:
+                if all(_orient(p[q[e]], p[q[(e + 1) % 3]], c) >= 0.0 for e in range(3)):
+                    return ("inside", cur)
+                return ("lost",)
+            u, v, n = ex
+            if _key(u, v) in self.segs or n == _NONE:
+                return ("segment", u, v)
+            frm, cur = cur, n
+        return ("lost",)
+
+    def cavity(self, t, x):
+        p = self.p
+        cav = [t]
+        k = 0
+        while k < len(cav):
+            q = self.t[cav[k]]
+            for e in range(3):
+                u, v = q[e], q[(e + 1) % 3]
+                if _key(u, v) in self.segs:
+                    continue
+                n = self.across(cav[k], u, v)
+                if n == _NONE or n in cav:
+                    continue
+                r = self.t[n]
+                if _incircle(p[r[0]], p[r[1]], p[r[2]], x) > 0.0:
+                    cav.append(n)
+            k += 1
+        bnd = []
+        for c in cav:
+            q = self.t[c]
+            for e in range(3):
+                u, v = q[e], q[(e + 1) % 3]
+                n = self.across(c, u, v)
+                if n == _NONE or n not in cav or _key(u, v) in self.segs:
+                    bnd.append((u, v))
+        return cav, bnd
+
+    def insert(self, cav, bnd, x, skip):
+        fan = [(u, v) for (u, v) in bnd if (u, v) != skip]
+        for u, v in fan:
+            pu, pv = self.p[u], self.p[v]
+            l2 = (pu[0] - pv[0]) * (pu[0] - pv[0]) + (pu[1] - pv[1]) * (pu[1] - pv[1])
+            if _orient(pu, pv, x) <= 1e-9 * l2:
+                return None
+        i = len(self.p)
+        self.p.append(x)
+        for c in cav:
+            self.kill(c)
+        return [self.add_tri([u, v, i]) for (u, v) in fan]
+
+
+def _triangulate_refined(outer, holes, eps, size, cap):
+    """polygon.rs:593-700 the triangles (counter-clockwise) of a region refined to `size` and the smallest
+    angle REFINE_MIN_ANGLE (Ruppert's refinement with Shewchuk's rules, in one fixed order)."""
+    poly = _bridge(outer, holes, eps)
+    tris = _ears(poly, eps)
+    p, id_of, ids = [], {}, []
+    for x in poly:  # the two ends of a bridge are exact copies: one vertex
+        k = (float(x[0]), float(x[1]))
+        if k not in id_of:
+            id_of[k] = len(p)
+            p.append(k)
+        ids.append(id_of[k])
+    t = [[ids[q[0]], ids[q[1]], ids[q[2]]] for q in tris]
+    _delaunay_flips(p, t)
+    m = _Mesh2(p)
+    for q in t:
+        m.add_tri(q)
+    shortest = np.inf
+    for i in range(len(m.t)):
+        q = m.t[i]
+        for e in range(3):
+            u, v = q[e], q[(e + 1) % 3]
+            if m.across(i, u, v) == _NONE:
+                ln = _dist(m.p[u], m.p[v])
+                m.segs[_key(u, v)] = ln
+                shortest = min(shortest, ln)
+    ratio = 0.5 / math.sin(REFINE_MIN_ANGLE * math.pi / 180.0)
+    queue = collections.deque(range(len(m.t)))
+    live = len(m.t)
+    while queue:
+        i = queue.popleft()
+        if not m.alive[i] or live > cap:
+            continue
+        q = m.t[i]
+        a, b, c = m.p[q[0]], m.p[q[1]], m.p[q[2]]
+        ls = [_dist(b, c), _dist(c, a), _dist(a, b)]
+        lo, hi = min(min(ls[0], ls[1]), ls[2]), max(max(ls[0], ls[1]), ls[2])
+        cc = _circumcentre(a, b, c)
+        big = hi > size
+        skinny = _dist(cc, a) > ratio * lo and lo >= 0.25 * shortest
+        if not big and not skinny:
+            continue
+        fan = None
+        loc = m.locate(i, cc)
+        if loc[0] == "lost":
+            continue
+        if loc[0] == "segment":
+            split = (loc[1], loc[2])
+        else:
+            cav, bnd = m.cavity(loc[1], cc)
+            split = None
+            for u, v in bnd:
+                if _key(u, v) in m.segs:
+                    pu, pv = m.p[u], m.p[v]
+                    if (pu[0] - cc[0]) * (pv[0] - cc[0]) + (pu[1] - cc[1]) * (pv[1] - cc[1]) < 0.0:
+                        split = (u, v)
+                        break
+            if split is None:
+                new = m.insert(cav, bnd, cc, None)
+                fan = None if new is None else (new, len(cav))
+        if split is not None:
+            u, v = split
+            ln = _dist(m.p[u], m.p[v])
+            if not (ln > size or ln >= 0.75 * min(0.5 * size, m.segs[_key(u, v)])):
+                continue
+            s = m.owners[_key(u, v)]
+            ts = s[0] if s[0] != _NONE else s[1]
+            qs = m.t[ts]
+            u, v = next((qs[e], qs[(e + 1) % 3]) for e in range(3) if _key(qs[e], qs[(e + 1) % 3]) == _key(u, v))
+            mid = (0.5 * (m.p[u][0] + m.p[v][0]), 0.5 * (m.p[u][1] + m.p[v][1]))
+            cav, bnd = m.cavity(ts, mid)
+            frm = m.segs[_key(u, v)]
+            new = m.insert(cav, bnd, mid, (u, v))
+            if new is not None:
+                x = len(m.p) - 1
+                del m.segs[_key(u, v)]
+                m.segs[_key(u, x)] = frm
+                m.segs[_key(x, v)] = frm
+                live += len(new) - len(cav)
+                queue.extend(new)
+                if m.alive[i]:
+                    queue.append(i)
+        elif fan is not None:
+            live += len(fan[0]) - fan[1]
+            queue.extend(fan[0])
+    return [[m.p[m.t[i][0]], m.p[m.t[i][1]], m.p[m.t[i][2]]] for i in range(len(m.t)) if m.alive[i]]
+
+
+def waterline_lid(verts, isx=0, isy=0, z0=0.0, reference_length=1.0):
+    """interior.rs:408-434 waterline: the waterplane regions (their contours with collinear points merged,
+    holes -- moonpools -- kept, each hole with the smallest outer contour around it) triangulated with
+    their holes and refined to edges of at most twice the mean waterline segment length and angles of at
+    least REFINE_MIN_ANGLE; the triangles as stored panels [Q][4][3] (the last vertex repeated), facing up.
+    More than MAX_GENERATED triangles raise ValueError, as the reference does."""
+    v = np.asarray(verts, dtype=np.float64).reshape(-1, 4, 3)
+    loops, sx, sy, target, ax_x, ax_y, tol = _waterplane_loops(v, isx, isy, z0, reference_length, True)
+    outers = [lp for lp in loops if len(lp) >= 3 and _signed_area(lp) > 0.0]
+    holes = [lp for lp in loops if len(lp) >= 3 and not _signed_area(lp) > 0.0]
+    if not outers:
+        raise ValueError("no enclosed region")
+    hole_of = [[] for _ in outers]
+    for h in holes:
+        owner = -1
+        for o in range(len(outers)):
+            if _inside(outers[o], h[0]) and (owner < 0 or abs(_signed_area(outers[o])) < abs(_signed_area(outers[owner]))):
+                owner = o
+        if owner < 0:
+            raise ValueError("a waterline contour lies outside the body")
+        hole_of[owner].append(h)
+    done = []
+    for o in range(len(outers)):
+        done.extend(_triangulate_refined(outers[o], hole_of[o], tol, 2.0 * target, MAX_GENERATED - len(done)))
+        if len(done) > MAX_GENERATED:
+            raise ValueError(f"the waterplane needs more than {MAX_GENERATED} panels of twice the mean waterline "
+                             "segment length; use 'graded' or a mesh of its own")
+    out = []
+    for tri in done:
+        w = np.zeros((4, 3))
+        for k in range(3):
+            w[k] = (sx * tri[k][0], sy * tri[k][1], z0)
+        if sx * sy < 0.0:
+            w[:3] = w[:3][::-1]
+        w[3] = w[2]
+        out.append(w)
+    return np.array(out)
