@@ -94,3 +94,18 @@ def test_release_frees_the_pipelines_buffers():
     assert after >= before
     again = solve_all(probs, precision=nv.HBG_MIXED, concurrency=3)
     assert np.isfinite(np.asarray(again[0]["A"])).all()
+
+
+@pytest.mark.gpu
+def test_cancelled_batch_on_pipelines():
+    """A set cancel flag stops every pipeline before its first batch: HB_ERR_CANCELLED, and the pipelines
+    solve again afterwards."""
+    flag = (ctypes.c_int32 * 1)(1)
+    bodies = [nv.Body(**p) for p in uneven_bodies()]
+    arr = (nv.HbgProblem * len(bodies))(*[b.problem() for b in bodies])
+    o = nv.default_options(concurrency=3)
+    o.cancel = ctypes.cast(flag, nv.ip)
+    assert nv.lib().hbg_solve_batch(arr, len(bodies), ctypes.byref(o)) == 5  # HB_ERR_CANCELLED
+    flag[0] = 0
+    nv.check(nv.lib().hbg_solve_batch(arr, len(bodies), ctypes.byref(o)))
+    assert all(np.isfinite(np.asarray(b.results()["A"])).all() for b in bodies)
