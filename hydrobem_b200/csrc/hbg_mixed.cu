@@ -114,9 +114,13 @@ constexpr double IR_TOL = 1e-9;
 constexpr int IR_MAX_IT = 30;
 
 // Corrections run back to back before the host first looks at their norms: the count the previous
-// batch of this thread needed (3 on the benchmark workload), at least 2.
+// batch of the same problem needed, IR_GUESS_START at a problem's first batch, at least 2.  Every problem
+// starts from the same count, so its corrections -- and the frequencies it hands to the FP64 form --
+// do not depend on what the host thread solved before (the pipelines of a batch take the problems in
+// an order that varies from call to call).
+constexpr int IR_GUESS_START = 3;  // the benchmark workload's count
 inline int& ir_guess() {
-    static thread_local int g = 3;
+    static thread_local int g = IR_GUESS_START;
     return g;
 }
 
@@ -157,6 +161,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                             int64_t* freq, const std::function<void()>& start, const double* motion,
                             const FieldArgs& field, std::vector<int64_t>* fallback) {
     KernelProfiler& P = profiler();
+    ir_guess() = IR_GUESS_START;
     // N panels; with symmetry sectors G systems of Nm = N / G unknowns per frequency (one of N otherwise)
     const int N = pv.N, G = pv.G, Nm = N / G, F = (int)pr.n_omega, H = (int)pr.n_heading, D = 6 * pv.nbod,
               nrhs = D + H;

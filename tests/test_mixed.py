@@ -151,18 +151,23 @@ def test_mixed_falls_back_to_fp64_where_refinement_cannot_converge():
 
 
 def test_mixed_fallback_after_corrections_beyond_the_first_look():
-    """The refinement queues as many corrections as the previous batch needed before the host looks at
-    the norms.  After a 128-panel body (one diagonal block: two corrections suffice) the shallow
-    cylinder's batch needs more than those; its systems that converge only in the corrections the host
-    adds one by one must report the outputs of their last iterate, not those read back at the first
-    look, while the ones that cannot converge go to the FP64 form."""
+    """Each problem's refinement queues three corrections before the host first looks at their norms
+    (a 128-panel body converges within them: two entries of history).  The shallow cylinder's batch needs
+    more: its systems that converge only in the corrections the host adds one by one must report the
+    outputs of their last iterate, not those read back at the first look, while the ones that cannot
+    converge go to the FP64 form.  The count does not carry over from the problem solved before."""
     small = meshes.cylinder(1.0, 0.5, 16, 4, 4)
     assert len(small) == 128
     nv.solve(small, np.array([1.0, 2.0]), [0.0], precision=nv.HBG_MIXED)
     assert len(nv.last_ir_history()) == 2, nv.last_ir_history()
     v, omegas = _c3_body(30)
     gpu = nv.solve(v, omegas, [0.0, 45.0], precision=nv.HBG_MIXED)
+    assert len(nv.last_ir_history()) > 3, nv.last_ir_history()
     assert 1 <= nv.last_fallback_count() < len(omegas)
     ref = nv.solve(v, omegas, [0.0, 45.0])
     errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= MIXED_TOL, errs
+    nv.solve(small, np.array([1.0, 2.0]), [0.0], precision=nv.HBG_MIXED)
+    again = nv.solve(v, omegas, [0.0, 45.0], precision=nv.HBG_MIXED)  # the same path after another problem
+    for k in ("A", "B", "X", "HK"):
+        assert np.array_equal(np.asarray(again[k]), np.asarray(gpu[k])), k
