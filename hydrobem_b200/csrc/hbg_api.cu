@@ -1104,7 +1104,8 @@ struct PipelineStats {
     int64_t klaunches[KF_COUNT] = {};
     size_t held = 0;
 };
-size_t g_pool_held[16];  // per device: the pipelines' workspace bytes after the last concurrent call
+// per device and pipeline: the workspace bytes it held after its last call (what it can reuse)
+std::atomic<size_t> g_pool_held[16][8];
 
 // The modelled cost of a problem (the LU of each system against its assembly, per frequency): the order
 // in which the pipelines take the problems.
@@ -1143,7 +1144,9 @@ static void solve_concurrent(const HbgProblem* problems, int64_t n, const HbgOpt
                      [&](int64_t a, int64_t b) { return problem_cost(problems[a]) > problem_cost(problems[b]); });
     size_t freeb = 0, totalb = 0;
     CUDA_OK(cudaMemGetInfo(&freeb, &totalb));
-    const size_t budget = (size_t)(0.85 * (double)(freeb + g_pool_held[dev]) / K);
+    size_t reusable = 0;  // the buffers of the pipelines this call uses (the others keep theirs)
+    for (int w = 0; w < K; w++) reusable += g_pool_held[dev][w].load();
+    const size_t budget = (size_t)(0.85 * (double)(freeb + reusable) / K);
     std::vector<PipelineStats> stats((size_t)K);
     std::vector<cudaEvent_t> ends((size_t)K, nullptr);
     cudaStream_t s0;
@@ -1212,6 +1215,7 @@ static void solve_concurrent(const HbgProblem* problems, int64_t n, const HbgOpt
         st.ir_iterations = last_ir_iterations();
         for (int i = 0; i < KF_COUNT; i++) st.kms[i] = P.ms[i], st.kwork[i] = P.work[i], st.klaunches[i] = P.launches[i];
         st.held = workspace().held();
+        g_pool_held[dev][w].store(st.held);
         hbm_budget() = 0;
     };
     pool.run(K, job);
@@ -1221,7 +1225,6 @@ static void solve_concurrent(const HbgProblem* problems, int64_t n, const HbgOpt
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     KernelProfiler& P = profiler();
-    size_t held = 0;
     int ir = 0;
     for (const PipelineStats& st : stats) {
         for (int i = 0; i < 5; i++) g_profile[i] += st.phase[i];
@@ -1230,11 +1233,9 @@ static void solve_concurrent(const HbgProblem* problems, int64_t n, const HbgOpt
         last_surrogate_pairs() += st.sg_pairs;
         ir = std::max(ir, st.ir_iterations);
         for (int i = 0; i < KF_COUNT; i++) P.ms[i] += st.kms[i], P.work[i] += st.kwork[i], P.launches[i] += st.klaunches[i];
-        held += st.held;
     }
     last_ir_iterations() = ir;
     last_ir_history().n = 0;
-    g_pool_held[dev] = held;
     g_profile[5] = ms;
     for (auto& e : ends) cudaEventDestroy(e);
     cudaEventDestroy(e0);
@@ -1356,7 +1357,7 @@ extern "C" HbStatus hbg_release_workspace(void) {
         if (PipelinePool* pool = pipeline_pool_ptr(d, false)) {
             const int k = pool->threads();
             if (k > 0) pool->run(k, [](int) { workspace().release(); });
-            g_pool_held[d] = 0;
+            for (int w = 0; w < 8; w++) g_pool_held[d][w].store(0);
         }
     return HB_OK;
 }
