@@ -1142,6 +1142,9 @@ static void solve_concurrent(const HbgProblem* problems, int64_t n, const HbgOpt
     for (int64_t i = 0; i < n; i++) order[(size_t)i] = i;
     std::stable_sort(order.begin(), order.end(),
                      [&](int64_t a, int64_t b) { return problem_cost(problems[a]) > problem_cost(problems[b]); });
+    // the calling thread's own buffers (from earlier one-after-another solves) are freed: the pipelines
+    // share the device memory, and a solve on this thread allocates again what it needs
+    workspace().release();
     size_t freeb = 0, totalb = 0;
     CUDA_OK(cudaMemGetInfo(&freeb, &totalb));
     size_t reusable = 0;  // the buffers of the pipelines this call uses (the others keep theirs)
@@ -1282,6 +1285,16 @@ extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_proble
             phase_timers().flush();
             solve_concurrent(problems, n_problems, *opt, K);
             return HB_OK;
+        }
+        // one after another on this thread: the pipelines' buffers (from an earlier concurrent call) are
+        // freed, so that this thread's batches may use the device memory
+        if (PipelinePool* pool = pipeline_pool_ptr(opt->device, false)) {
+            bool held = false;
+            for (int w = 0; w < 8; w++) held = held || g_pool_held[opt->device][w].load() > 0;
+            if (held) {
+                pool->run(pool->threads(), [](int) { workspace().release(); });
+                for (int w = 0; w < 8; w++) g_pool_held[opt->device][w].store(0);
+            }
         }
         cudaStream_t s;
         CUDA_OK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));

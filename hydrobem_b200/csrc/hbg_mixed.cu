@@ -7,6 +7,7 @@
 #include <cuda.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -126,7 +127,19 @@ inline int& ir_guess() {
 
 // Side streams for the LU of LU_GROUPS groups of a batch and their fork/join events, per device and
 // host thread (kept across solves).
-constexpr int LU_GROUPS = 4;
+constexpr int LU_GROUPS = 4;  // at most (the streams kept)
+static std::atomic<int> g_lu_groups_override{0};
+void mixed_lu_groups(int groups) { g_lu_groups_override = std::max(0, std::min(groups, LU_GROUPS)); }
+// the groups of a batch of ns systems of order Np: about eight systems a group, at most LU_GROUPS (a group's
+// launches cover its systems, so a group of a few small systems leaves its products and factors too
+// short to fill the device).  Measured: the 40 systems of order 4096 of the benchmark job 67.0 / 67.5 /
+// 68.1 ms a job with 4 / 3 / 2 groups; the 64 uneven bodies (16 systems a batch, orders 896-5632, two
+// pipelines) 1.79 s with 2 groups against 1.83 / 1.85-2.08 / 1.85-1.93 s with 1 / 3 / 4.
+static int lu_groups_for(int Np, int ns) {
+    (void)Np;
+    const int o = g_lu_groups_override.load();
+    return std::max(1, std::min(o > 0 ? o : std::min(LU_GROUPS, ns / 8), ns));
+}
 struct SideStreams {
     cudaStream_t s[LU_GROUPS + 1] = {};  // the LU groups, then the right-hand sides
     cudaEvent_t fork = nullptr, join[LU_GROUPS + 1] = {};
@@ -682,7 +695,7 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
                     trailing(h, c2, n);  // the trailing matrix, K' = 512
                 }
             };
-            const int nh = std::min(LU_GROUPS, ns);
+            const int nh = lu_groups_for(Np, ns);
             Half hs[LU_GROUPS];
             for (int i = 0, f0 = 0; i < nh; i++) {
                 const int ni = ns / nh + (i < ns % nh ? 1 : 0);

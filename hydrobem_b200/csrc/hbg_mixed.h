@@ -29,5 +29,8 @@ int mixed_solve_frequencies(const PanelsView& pv, const double* st, const HbgPro
 
 int debug_gemm_tf32(int M, int N, int K, const float* A, const float* B, float* C, bool subtract, const char** msg);
 int measure_peaks(double* out, const char** msg);
+// the mixed LU's groups of systems on side streams for the solves that follow (process-wide; 0: the
+// library's rule)
+void mixed_lu_groups(int groups);
 
 }  // namespace hbg

@@ -109,3 +109,19 @@ def test_cancelled_batch_on_pipelines():
     flag[0] = 0
     nv.check(nv.lib().hbg_solve_batch(arr, len(bodies), ctypes.byref(o)))
     assert all(np.isfinite(np.asarray(b.results()["A"])).all() for b in bodies)
+
+
+@pytest.mark.gpu
+def test_pipelines_and_the_calling_thread_hand_over_the_memory():
+    """A concurrent call after a solve on the calling thread, and a solve on the calling thread after a
+    concurrent call, each get the device memory: the buffers of the other mode are freed first."""
+    import torch
+
+    probs = uneven_bodies()
+    nv.solve_batch([nv.Body(**probs[4])], precision=nv.HBG_MIXED)  # buffers on the calling thread
+    solve_all(probs, precision=nv.HBG_MIXED, concurrency=2)
+    after_concurrent = torch.cuda.mem_get_info()[0]
+    nv.solve_batch([nv.Body(**probs[4])], precision=nv.HBG_MIXED, concurrency=1)
+    after_single = torch.cuda.mem_get_info()[0]
+    # the pipelines' buffers are gone once the calling thread solves again (its own are smaller)
+    assert after_single >= after_concurrent
