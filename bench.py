@@ -336,6 +336,7 @@ def ours(args, world, rank, local, pg):
     ir = {"iterations": nv.last_ir_iterations(), "history": [float(f"{x:.3g}") for x in nv.last_ir_history()]} \
         if precision == nv.HBG_MIXED else None
     fallbacks = nv.last_fallback_count() if precision == nv.HBG_MIXED else None
+    fallback_ms = nv.last_fallback_time() if precision == nv.HBG_MIXED else None
     pipe_peaks = nv.measure_peaks()  # FP64 FMA / FP64 MMA / TF32 tcgen05 of this device, measured here
     if rank != 0:
         return None
@@ -387,6 +388,8 @@ def ours(args, world, rank, local, pg):
         line["refinement"] = ir
     if fallbacks is not None:
         line["fp64_fallback_frequencies"] = fallbacks
+        # their FP64 solves' device time (of the kernel-timed step; summed over pipelines)
+        line["fp64_fallback_ms"] = round(fallback_ms, 2)
     if precision == nv.HBG_FP64:  # over the timed steps' LU phase (the kernel-timed step's is inflated)
         line["lu"] = lu_rate(nv, {"lu": float(np.mean([p[2] for p in dev_phases]))}, pipe_peaks)
     if precision == nv.HBG_MIXED and not args.no_plain and bodies:

@@ -720,7 +720,17 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
             HbgOptions o64 = opt;
             o64.precision = HBG_FP64;
             o64.surrogate = nullptr;
+            cudaEvent_t fb0 = nullptr, fb1 = nullptr;
+            cudaEventCreate(&fb0);
+            cudaEventCreate(&fb1);
+            cudaEventRecord(fb0, s);
             solve_problem(sub, o64, body_index, s);
+            cudaEventRecord(fb1, s);
+            float fb_ms = 0.f;
+            if (cudaEventSynchronize(fb1) == cudaSuccess && cudaEventElapsedTime(&fb_ms, fb0, fb1) == cudaSuccess)
+                last_fallback_ms() += fb_ms;
+            cudaEventDestroy(fb0);
+            cudaEventDestroy(fb1);
             for (size_t i = 0; i < nf; i++) {
                 const size_t fo = (size_t)fallback[i];
                 auto put = [&](double* dst, const std::vector<double>& src, size_t per) {
@@ -1098,6 +1108,7 @@ cudaStream_t& pipeline_stream() {
 struct PipelineStats {
     double phase[5] = {};
     int64_t launches = 0, fallbacks = 0;
+    double fallback_ms = 0.0;
     long long sg_pairs = 0;
     int ir_iterations = 0;
     double kms[KF_COUNT] = {}, kwork[KF_COUNT] = {};
@@ -1176,6 +1187,7 @@ static void solve_concurrent(const HbgProblem* problems, int64_t n, const HbgOpt
         for (int i = 0; i < 6; i++) g_profile[i] = 0.0;
         g_launches = 0;
         last_fallback_count() = 0;
+        last_fallback_ms() = 0.0;
         last_surrogate_pairs() = 0;
         KernelProfiler& P = profiler();
         P.reset();
@@ -1214,6 +1226,7 @@ static void solve_concurrent(const HbgProblem* problems, int64_t n, const HbgOpt
         for (int i = 0; i < 5; i++) st.phase[i] = g_profile[i];
         st.launches = g_launches;
         st.fallbacks = last_fallback_count();
+        st.fallback_ms = last_fallback_ms();
         st.sg_pairs = last_surrogate_pairs();
         st.ir_iterations = last_ir_iterations();
         for (int i = 0; i < KF_COUNT; i++) st.kms[i] = P.ms[i], st.kwork[i] = P.work[i], st.klaunches[i] = P.launches[i];
@@ -1233,6 +1246,7 @@ static void solve_concurrent(const HbgProblem* problems, int64_t n, const HbgOpt
         for (int i = 0; i < 5; i++) g_profile[i] += st.phase[i];
         g_launches += st.launches;
         last_fallback_count() += st.fallbacks;
+        last_fallback_ms() += st.fallback_ms;
         last_surrogate_pairs() += st.sg_pairs;
         ir = std::max(ir, st.ir_iterations);
         for (int i = 0; i < KF_COUNT; i++) P.ms[i] += st.kms[i], P.work[i] += st.kwork[i], P.launches[i] += st.klaunches[i];
@@ -1253,6 +1267,7 @@ extern "C" HbStatus hbg_solve_batch(const HbgProblem* problems, int64_t n_proble
         for (int i = 0; i < 6; i++) g_profile[i] = 0.0;
         g_launches = 0;
         last_fallback_count() = 0;
+        last_fallback_ms() = 0.0;
         profiler().reset();
         for (int64_t p = 0; p < n_problems; p++) {
             const HbgProblem& pr = problems[p];
@@ -1378,6 +1393,12 @@ extern "C" HbStatus hbg_release_workspace(void) {
 extern "C" HbStatus hbg_last_fallback_count(int64_t* count) {
     if (!count) return fail({HB_ERR_ARGUMENT, "null argument"});
     *count = last_fallback_count();
+    return HB_OK;
+}
+
+extern "C" HbStatus hbg_last_fallback_time(double* ms) {
+    if (!ms) return fail({HB_ERR_ARGUMENT, "null argument"});
+    *ms = last_fallback_ms();
     return HB_OK;
 }
 

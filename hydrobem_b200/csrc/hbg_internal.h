@@ -315,6 +315,11 @@ inline int64_t& last_fallback_count() {
     static thread_local int64_t n = 0;
     return n;
 }
+// the device time (ms) of those frequencies' FP64 solves (statics included: the whole FP64 route)
+inline double& last_fallback_ms() {
+    static thread_local double ms = 0.0;
+    return ms;
+}
 // the rigid data of the motions as uploaded, per body: mass (NaN: displaced), centre of gravity (3),
 // inertia kind, inertia (9), inertia origin (3)
 constexpr int RIGID_PER_BODY = 17;

@@ -96,7 +96,7 @@ EXPORTS = ["hbg_default_options", "hbg_solve_batch", "hbg_debug_matrices", "hbg_
            "hb_set_ints", "hb_model_solve", "hb_results_free", "hb_results_has", "hb_results_quantity",
            "hbg_statics_noalloc", "hbg_measure_peaks", "hbg_last_ir_history", "hbg_surrogate_train",
            "hbg_surrogate_grad", "hbg_surrogate_eval", "hbg_last_surrogate_pairs", "hbg_read_gdf", "hbg_gdf_free",
-           "hb_model_load_mesh", "hbg_last_fallback_count", "hbg_debug_lu_f64", "hb_model_panels", "hbg_tuned_tiles"]
+           "hb_model_load_mesh", "hbg_last_fallback_count", "hbg_debug_lu_f64", "hb_model_panels", "hbg_tuned_tiles", "hbg_last_fallback_time"]
 
 _lib = None
 
@@ -339,6 +339,13 @@ def last_fallback_count() -> int:
     c = ctypes.c_int64()
     lib().hbg_last_fallback_count(ctypes.byref(c))
     return c.value
+
+
+def last_fallback_time() -> float:
+    """Device milliseconds of the FP64 solves of those frequencies in the last solve."""
+    v = ctypes.c_double()
+    lib().hbg_last_fallback_time(ctypes.byref(v))
+    return v.value
 
 
 def last_launch_count() -> int:

@@ -234,6 +234,9 @@ HbStatus hbg_release_workspace(void);
  * contract the error, as next to an irregular frequency of a body without an interior lid) or whose
  * unpivoted LU met a zero pivot. */
 HbStatus hbg_last_fallback_count(int64_t *count);
+/* The device time in milliseconds of those frequencies' FP64 solves in the last hbg_solve_batch of this
+ * thread (summed over the pipelines of a concurrent call; each fallback solve repeats the statics). */
+HbStatus hbg_last_fallback_time(double *ms);
 
 /* The kernels launched by the last hbg_solve_batch of this thread. */
 HbStatus hbg_last_launch_count(int64_t *count);

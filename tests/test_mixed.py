@@ -145,6 +145,7 @@ def test_mixed_falls_back_to_fp64_where_refinement_cannot_converge():
     assert len(v) == 2912
     gpu = nv.solve(v, omegas, [0.0, 45.0], precision=nv.HBG_MIXED)
     assert 1 <= nv.last_fallback_count() < len(omegas)
+    assert 0.0 < nv.last_fallback_time() < nv.last_profile()["total"]
     ref = nv.solve(v, omegas, [0.0, 45.0])
     errs = {k: scaled_error(gpu[k], ref[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= MIXED_TOL, errs
