@@ -1059,6 +1059,10 @@ __device__ __forceinline__ void tri_diag_f32(const float2* __restrict__ D, float
         const int pb = half * (TB / 2);
 #pragma unroll 1
         for (int pc = 0; pc < TB / 2; pc += 16) {
+            // the chunk's rows p = pb + pc .. + 15 that this row uses (p <= i for U^-1, p > i for L^-1):
+            // none, and its loads are skipped (half of the triangle's inverse is zero)
+            const int p0 = pb + pc;
+            if (upper_t ? p0 > i : p0 + 15 <= i) continue;
             float2 dv[16];
 #pragma unroll
             for (int q = 0; q < 16; q++) dv[q] = D[(pb + pc + q) * TB + i];
