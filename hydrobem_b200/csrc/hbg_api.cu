@@ -438,6 +438,48 @@ static void mirror_sector(const HbgBody& b, int G, std::vector<double>& v, std::
     }
 }
 
+static int64_t Nm_of(const HbgProblem& p) { return p.body.n_panels; }
+
+// The panels (n of them, vertices [n][4][3]) in the Morton order of their centroids (10 bits an axis over
+// the bounding box; ties in the given order): a[j] the given index of the j-th panel.  Empty for fewer than
+// 64 panels or non-finite coordinates (the given order; the geometry reports the latter).
+static std::vector<int32_t> spatial_order(const double* v, int64_t n) {
+    if (n < 64) return {};
+    std::vector<double> c(3 * (size_t)n);
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t j = 0; j < n; j++)
+        for (int d = 0; d < 3; d++) {
+            const double* q = v + 12 * (size_t)j + d;
+            const double x = 0.25 * (q[0] + q[3] + q[6] + q[9]);
+            if (!std::isfinite(x)) return {};
+            c[3 * (size_t)j + d] = x;
+            lo[d] = std::min(lo[d], x);
+            hi[d] = std::max(hi[d], x);
+        }
+    auto spread = [](uint64_t x) {  // the 10 bits of x at every third position
+        x &= 0x3ff;
+        x = (x | (x << 16)) & 0x030000FFull;
+        x = (x | (x << 8)) & 0x0300F00Full;
+        x = (x | (x << 4)) & 0x030C30C3ull;
+        x = (x | (x << 2)) & 0x09249249ull;
+        return x;
+    };
+    std::vector<std::pair<uint64_t, int32_t>> key((size_t)n);
+    for (int64_t j = 0; j < n; j++) {
+        uint64_t code = 0;
+        for (int d = 0; d < 3; d++) {
+            const double span = hi[d] - lo[d];
+            const uint64_t q = span > 0.0 ? (uint64_t)std::min(1023.0, std::floor((c[3 * (size_t)j + d] - lo[d]) / span * 1023.0)) : 0;
+            code |= spread(q) << d;
+        }
+        key[(size_t)j] = {code, (int32_t)j};
+    }
+    std::stable_sort(key.begin(), key.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    std::vector<int32_t> a((size_t)n);
+    for (int64_t j = 0; j < n; j++) a[(size_t)j] = key[(size_t)j].second;
+    return a;
+}
+
 static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_t body_index, cudaStream_t s) {
     const int64_t N64 = pr_in.body.n_panels;
     if (N64 < 1 || N64 > 60000) throw Failure{HB_ERR_VALUE, "panel count outside 1..60000", body_index};
@@ -447,17 +489,48 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     const int G = sym == HBG_SYM_BOTH ? 4 : sym != HBG_SYM_NONE ? 2 : 1;
     if (G > 1 && opt.precision == HBG_MIXED && opt.surrogate)
         throw Failure{HB_ERR_UNSUPPORTED, "symmetry sectors with the wave-term network are not on this route", body_index};
-    HbgProblem pr = pr_in;
+    // The stored panels in the Morton order of their centroids: the 32 x 32 panel pairs of an assembly tile
+    // then lie close together, so the table cells of their wave kernels differ less across a warp (fewer
+    // L1 wavefronts per coefficient gather).  The outputs are sums over the panels: the order changes only
+    // their rounding; an invalid panel is still reported by its index in the caller's order.
+    std::vector<int32_t> perm = spatial_order(pr_in.body.vertices, Nm_of(pr_in));
+    std::vector<double> pverts;
+    std::vector<int32_t> pkinds, pbody;
+    HbgProblem pin = pr_in;
+    if (!perm.empty()) {
+        const size_t n = perm.size();
+        pverts.resize(12 * n);
+        for (size_t a = 0; a < n; a++)
+            memcpy(&pverts[12 * a], pr_in.body.vertices + 12 * (size_t)perm[a], 12 * sizeof(double));
+        pin.body.vertices = pverts.data();
+        if (pr_in.body.kinds) {
+            pkinds.resize(n);
+            for (size_t a = 0; a < n; a++) pkinds[a] = pr_in.body.kinds[perm[a]];
+            pin.body.kinds = pkinds.data();
+        }
+        if (pr_in.body.panel_body) {
+            pbody.resize(n);
+            for (size_t a = 0; a < n; a++) pbody[a] = pr_in.body.panel_body[perm[a]];
+            pin.body.panel_body = pbody.data();
+        }
+    }
+    HbgProblem pr = pin;
     std::vector<double> mverts;
     std::vector<int32_t> mkinds, mbody;
     if (G > 1) {
-        mirror_sector(pr_in.body, G, mverts, mkinds, mbody);
+        mirror_sector(pin.body, G, mverts, mkinds, mbody);
         pr.body.n_panels = N64 * G;
         pr.body.vertices = mverts.data();
         pr.body.kinds = mkinds.data();
-        pr.body.panel_body = pr_in.body.panel_body ? mbody.data() : nullptr;
+        pr.body.panel_body = pin.body.panel_body ? mbody.data() : nullptr;
     }
     const int N = (int)(N64 * G), Nm = (int)N64;
+    // the caller's index of every panel (the images of a sector after it, sector by sector)
+    std::vector<int32_t> orig;
+    if (!perm.empty()) {
+        orig.resize(N);
+        for (int j = 0; j < N; j++) orig[j] = (j / Nm) * Nm + perm[j % Nm];
+    }
     const int F = (int)pr.n_omega, H = (int)pr.n_heading;
     for (int i = 0; i < F; i++)
         if (!(pr.omegas[i] > 0.0) || !std::isfinite(pr.omegas[i]))
@@ -538,7 +611,8 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     Workspace& ws = workspace();
     WsBuf dverts(ws, WS_VERTS), dkind(ws, WS_KIND), dplanes(ws, WS_PLANES), dbad(ws, WS_BAD), dst(ws, WS_ST),
         dwork(ws, WS_WORK), dnwork(ws, WS_NWORK), dpbody(ws, WS_PBODY), drcen(ws, WS_RCEN), drig(ws, WS_RIGID),
-        dhyd(ws, WS_HYD), dtiers(ws, WS_TIERS);
+        dhyd(ws, WS_HYD), dtiers(ws, WS_TIERS), dorig(ws, WS_ORIG);
+    if (!orig.empty()) dorig.alloc(sizeof(int32_t) * N);
     const bool multi = nbod > 1 && pr.body.panel_body;
     // the mixed form with the reference's production statics rule: the panels' float32 Gauss tiers
     const bool prod_statics = opt.precision == HBG_MIXED && opt.statics_rule == HBG_STATICS_PRODUCTION;
@@ -600,6 +674,8 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         CUDA_OK(cudaMemcpyAsync(dverts.p, pr.body.vertices, sizeof(double) * 12 * N, cudaMemcpyHostToDevice, s));
         CUDA_OK(cudaMemcpyAsync(dkind.p, kinds.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
         CUDA_OK(cudaMemcpyAsync(dbad.p, &big, sizeof big, cudaMemcpyHostToDevice, s));
+        if (!orig.empty())
+            CUDA_OK(cudaMemcpyAsync(dorig.p, orig.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
         if (multi)
             CUDA_OK(cudaMemcpyAsync(dpbody.p, pr.body.panel_body, sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
         if (pr.body.rotation_centers)
@@ -609,7 +685,7 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
         KernelProfiler& P = profiler();
         P.begin(s);
         launch_panel_geometry(N, dverts.as<double>(), dkind.as<int32_t>(), dplanes.as<double>(), dbad.as<int32_t>(), s,
-                              prod_statics ? dtiers.as<float>() : nullptr);
+                              prod_statics ? dtiers.as<float>() : nullptr, orig.empty() ? nullptr : dorig.as<int32_t>());
         P.end(KF_GEOMETRY, 0.0, s);
         g_launches++;
         PanelsView pv{N, dplanes.as<double>(), dkind.as<int32_t>()};

@@ -69,7 +69,7 @@ enum WsSlot {
     WS_VERTS = 0, WS_KIND, WS_PLANES, WS_BAD, WS_ST, WS_WORK, WS_NWORK, WS_S, WS_A, WS_U, WS_RHS, WS_X, WS_PHII,
     WS_IPIV, WS_INFO, WS_FI, WS_FD, WS_TILES, WS_SCR, WS_FPT, WS_HEADS, WS_OUT, WS_S32, WS_A32, WS_W, WS_P2,
     WS_P3, WS_PL, WS_PU, WS_B, WS_XM, WS_R, WS_NORMS, WS_ERR, WS_PART, WS_DINV, WS_TILES_F, WS_SG_PARAMS,
-    WS_SG_IMG, WS_SG_COUNT, WS_TRI_CTRL, WS_RS, WS_L16, WS_P3H, WS_PBODY, WS_RCEN, WS_UP, WS_PHI, WS_RIGID, WS_HYD, WS_FPTS, WS_FST, WS_FQ, WS_TIERS, WS_COUNT
+    WS_SG_IMG, WS_SG_COUNT, WS_TRI_CTRL, WS_RS, WS_L16, WS_P3H, WS_PBODY, WS_RCEN, WS_UP, WS_PHI, WS_RIGID, WS_HYD, WS_FPTS, WS_FST, WS_FQ, WS_TIERS, WS_ORIG, WS_COUNT
 };
 
 // Page-locked host buffers of a solve: a device-to-host copy into pageable memory waits for the
@@ -253,8 +253,10 @@ void set_constants(const double glx[17][16], const double glw[17][16], const Tab
 void set_constants_statics(const double glx[17][16], const double glw[17][16]);
 // tiers (optional, [N][TIER_FLOATS_HOST]): the float32 Gauss tiers of the production Rankine rule
 constexpr int TIER_FLOATS_HOST = 416;
+// orig: the index of each panel in the caller's order (the invalid panel reported is the first in that
+// order), or null when the panels are in it
 void launch_panel_geometry(int N, const double* verts, const int32_t* kind, double* planes, int32_t* bad,
-                           cudaStream_t s, float* tiers = nullptr);
+                           cudaStream_t s, float* tiers = nullptr, const int32_t* orig = nullptr);
 // mixed: the mixed form's variant (far Rankine points and the order-4 log rule in FP32)
 void launch_statics(const PanelsView& pv, double depth, int logint, double tol, double* st, int32_t* work,
                     int32_t* nwork, int work_cap, cudaStream_t s, bool mixed = false);

@@ -49,7 +49,8 @@ __device__ __forceinline__ int tier_off(int t) { return t == 0 ? 0 : t == 1 ? 64
 __device__ __forceinline__ int tier_len(int t) { return t <= 1 ? 16 : t == 2 ? 32 : 40; }
 
 __global__ void k_panel_geometry(int N, const double* __restrict__ verts, const int32_t* __restrict__ kind,
-                                 double* __restrict__ P, int32_t* __restrict__ bad, float* __restrict__ tiers) {
+                                 double* __restrict__ P, int32_t* __restrict__ bad, float* __restrict__ tiers,
+                                 const int32_t* __restrict__ orig) {
     int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= N) return;
     double raw[4][3];
@@ -59,7 +60,7 @@ __global__ void k_panel_geometry(int N, const double* __restrict__ verts, const 
             raw[i][d] = verts[(size_t)j * 12 + 3 * i + d];
             ok = ok && isfinite(raw[i][d]);
         }
-    auto fail = [&]() { atomicMin(bad, j); };
+    auto fail = [&]() { atomicMin(bad, orig ? orig[j] : j); };  // the panel's index in the caller's order
     if (!ok) { fail(); return; }
     double t[3];
     double diameter = 0.0;
@@ -731,8 +732,8 @@ __global__ void __launch_bounds__(AD_WARPS * 32) k_statics_adaptive_q(PanelsView
 
 // ------------------------------------------------------------------ host launchers
 void launch_panel_geometry(int N, const double* verts, const int32_t* kind, double* planes, int32_t* bad,
-                           cudaStream_t s, float* tiers) {
-    k_panel_geometry<<<(N + 127) / 128, 128, 0, s>>>(N, verts, kind, planes, bad, tiers);
+                           cudaStream_t s, float* tiers, const int32_t* orig) {
+    k_panel_geometry<<<(N + 127) / 128, 128, 0, s>>>(N, verts, kind, planes, bad, tiers, orig);
 }
 
 void launch_statics(const PanelsView& pv, double depth, int logint, double tol, double* st, int32_t* work,

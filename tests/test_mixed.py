@@ -127,7 +127,8 @@ def test_mixed_large_barge_with_lid():
     fp64 = nv.solve(v, omegas, heads, kinds=kinds)
     errs = {k: scaled_error(mixed[k], fp64[k]) for k in ("A", "B", "X", "HK")}
     assert max(errs.values()) <= MIXED_TOL, (errs, hist)
-    assert hist[-1] <= 1e-7 and len(hist) <= 12, hist
+    # converged by the refinement's own test (the last correction times its contraction below 1e-9)
+    assert len(hist) <= 12 and hist[-1] * min(1.0, hist[-1] / hist[-2]) <= 1e-9, hist
 
 
 def _c3_body(index):
@@ -137,11 +138,22 @@ def _c3_body(index):
     return meshes.uneven_bodies(index + 1)[index]
 
 
+def _shallow_cylinder():
+    """Body 30 of the 64-body configuration (r = 2.7 m, draught 0.31 m, 2912 panels, no interior lid) at
+    its 16 frequencies and two more next to its irregular frequencies (K r = 9.09 and 9.40, where a scan of
+    K r in steps of 0.01 found the reduced-precision refinement diverging; it converges, in up to 20
+    corrections, at most others around them)."""
+    v, omegas = _c3_body(30)
+    r = float(np.hypot(v[..., 0], v[..., 1]).max())
+    near = np.sqrt(np.array([9.09, 9.40]) / r * meshes.GRAVITY)
+    return v, np.concatenate([omegas, near])
+
+
 def test_mixed_falls_back_to_fp64_where_refinement_cannot_converge():
     """A shallow cylinder without an interior lid (r = 2.7 m, draught 0.31 m, 2912 panels) over K r up to
     10: next to its irregular frequencies the reduced-precision factors no longer contract the error, and
     those frequencies are solved by the FP64 form; the whole answer stays within the bar."""
-    v, omegas = _c3_body(30)
+    v, omegas = _shallow_cylinder()
     assert len(v) == 2912
     gpu = nv.solve(v, omegas, [0.0, 45.0], precision=nv.HBG_MIXED)
     assert 1 <= nv.last_fallback_count() < len(omegas)
@@ -161,7 +173,7 @@ def test_mixed_fallback_after_corrections_beyond_the_first_look():
     assert len(small) == 128
     nv.solve(small, np.array([1.0, 2.0]), [0.0], precision=nv.HBG_MIXED)
     assert len(nv.last_ir_history()) == 2, nv.last_ir_history()
-    v, omegas = _c3_body(30)
+    v, omegas = _shallow_cylinder()
     gpu = nv.solve(v, omegas, [0.0, 45.0], precision=nv.HBG_MIXED)
     assert len(nv.last_ir_history()) > 3, nv.last_ir_history()
     assert 1 <= nv.last_fallback_count() < len(omegas)
