@@ -438,8 +438,6 @@ static void mirror_sector(const HbgBody& b, int G, std::vector<double>& v, std::
     }
 }
 
-static int64_t Nm_of(const HbgProblem& p) { return p.body.n_panels; }
-
 // The panels (n of them, vertices [n][4][3]) in the Morton order of their centroids (10 bits an axis over
 // the bounding box; ties in the given order): a[j] the given index of the j-th panel.  Empty for fewer than
 // 64 panels or non-finite coordinates (the given order; the geometry reports the latter).
@@ -493,7 +491,7 @@ static void solve_problem(const HbgProblem& pr_in, const HbgOptions& opt, int64_
     // then lie close together, so the table cells of their wave kernels differ less across a warp (fewer
     // L1 wavefronts per coefficient gather).  The outputs are sums over the panels: the order changes only
     // their rounding; an invalid panel is still reported by its index in the caller's order.
-    std::vector<int32_t> perm = spatial_order(pr_in.body.vertices, Nm_of(pr_in));
+    std::vector<int32_t> perm = spatial_order(pr_in.body.vertices, N64);
     std::vector<double> pverts;
     std::vector<int32_t> pkinds, pbody;
     HbgProblem pin = pr_in;
