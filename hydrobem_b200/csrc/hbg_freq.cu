@@ -215,19 +215,29 @@ __global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView 
     }
     __syncthreads();
     const int k = K0 + tx;
-    // xk: the field point of row k; ck, nk, ak: panel g k (the source of entry (n, g k))
-    double xk[3] = {0, 0, 0}, ck[3] = {0, 0, 0}, nk[3] = {0, 0, 0}, ak = 0;
-    int kindk = 0;
-    if (k < N) {
-        const int gk = g * N + k;
-        for (int d = 0; d < 3; d++) {
-            ck[d] = pv.at(P_C + d, gk);
-            nk[d] = pv.at(P_N + d, gk);
-            xk[d] = SECT ? pv.at(P_C + d, k) : ck[d];
+    // xk: the field point of row k; ck, nk, ak: panel g k (the source of entry (n, g k)); kept in shared
+    // memory (read where used: short live ranges instead of ten doubles held across the pairs)
+    __shared__ double sKd[10][32];
+    __shared__ int sKind[32];
+    if (ty == 0) {
+        double xk[3] = {0, 0, 0}, ck[3] = {0, 0, 0}, nk[3] = {0, 0, 0}, ak = 0;
+        int kindk = 0;
+        if (k < N) {
+            const int gk = g * N + k;
+            for (int d = 0; d < 3; d++) {
+                ck[d] = pv.at(P_C + d, gk);
+                nk[d] = pv.at(P_N + d, gk);
+                xk[d] = SECT ? pv.at(P_C + d, k) : ck[d];
+            }
+            ak = pv.at(P_AREA, gk);
+            kindk = pv.kind[k];
         }
-        ak = pv.at(P_AREA, gk);
-        kindk = pv.kind[k];
+        for (int d = 0; d < 3; d++) sKd[d][tx] = xk[d], sKd[3 + d][tx] = ck[d], sKd[6 + d][tx] = nk[d];
+        sKd[9][tx] = ak;
+        sKind[tx] = kindk;
     }
+    __syncthreads();
+    const volatile double(*vK)[32] = sKd;
     const FdParams* fd = FINITE ? fdp + f : nullptr;
     const typename Out::Tile* T1 = FINITE ? tiles + (size_t)f * (Out::kT1 + Out::kT2) : nullptr;
     const typename Out::Tile* T2 = FINITE ? T1 + Out::kT1 : nullptr;
@@ -248,6 +258,7 @@ __global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView 
         double an = pv.at(P_AREA, gn);
         int kindn = pv.kind[n];
         // R without contraction: the finite-depth kernel switches form at R = h/2 exactly
+        const double xk[3] = {vK[0][tx], vK[1][tx], vK[2][tx]};
         double dx = xk[0] - cn[0], dy = xk[1] - cn[1];
         double R = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
         Kern w;
@@ -259,13 +270,17 @@ __global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView 
         // entry (k, n): the field point x_k against panel g n
         size_t o1 = (size_t)k + (size_t)n * N;
         double2 s1, d1;
-        apply_kernel(__ldg(stg + o1), __ldg(stg + NN + o1), __ldg(stg + 2 * NN + o1), __ldg(stg + 3 * NN + o1), an,
-                     nn3[0], nn3[1], nn3[2], kindn, xk, cn, K, logc, w, R, false, s1, d1);
-        out.put(y, k, n, s1, make_double2((g == 0 && k == n ? free_term(kindk) : 0.0) - d1.x, -d1.y));
+        {
+            const double xk2[3] = {vK[0][tx], vK[1][tx], vK[2][tx]};
+            apply_kernel(__ldg(stg + o1), __ldg(stg + NN + o1), __ldg(stg + 2 * NN + o1), __ldg(stg + 3 * NN + o1),
+                         an, nn3[0], nn3[1], nn3[2], kindn, xk2, cn, K, logc, w, R, false, s1, d1);
+        }
+        out.put(y, k, n, s1, make_double2((g == 0 && k == n ? free_term(sKind[tx]) : 0.0) - d1.x, -d1.y));
         if (n != k) {
             double2 s2, d2;
-            apply_kernel(sT[0][tx][nl], sT[1][tx][nl], sT[2][tx][nl], sT[3][tx][nl], ak, nk[0], nk[1], nk[2], kindk,
-                         xn, ck, K, logc, w, R, true, s2, d2);
+            const double ck[3] = {vK[3][tx], vK[4][tx], vK[5][tx]};
+            apply_kernel(sT[0][tx][nl], sT[1][tx][nl], sT[2][tx][nl], sT[3][tx][nl], vK[9][tx], vK[6][tx], vK[7][tx],
+                         vK[8][tx], sKind[tx], xn, ck, K, logc, w, R, true, s2, d2);
             sT[0][tx][nl] = s2.x;
             sT[1][tx][nl] = s2.y;
             sT[2][tx][nl] = -d2.x;
