@@ -217,8 +217,26 @@ __global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView 
     const int k = K0 + tx;
     // xk: the field point of row k; ck, nk, ak: panel g k (the source of entry (n, g k)); kept in shared
     // memory (read where used: short live ranges instead of ten doubles held across the pairs)
-    __shared__ double sKd[10][32];
-    __shared__ int sKind[32];
+    __shared__ double sKd[10][32], sNd[10][32];
+    __shared__ int sKind[32], sNKind[32];
+    if (ty == 1) {  // the same for the column panels n = N0 + tx: xn, cn, nn, an
+        const int nn = N0 + tx;
+        double xn[3] = {0, 0, 0}, cn[3] = {0, 0, 0}, nv3[3] = {0, 0, 0}, an = 0;
+        int kindn = 0;
+        if (nn < N) {
+            const int gn = g * N + nn;
+            for (int d = 0; d < 3; d++) {
+                cn[d] = pv.at(P_C + d, gn);
+                nv3[d] = pv.at(P_N + d, gn);
+                xn[d] = SECT ? pv.at(P_C + d, nn) : cn[d];
+            }
+            an = pv.at(P_AREA, gn);
+            kindn = pv.kind[nn];
+        }
+        for (int d = 0; d < 3; d++) sNd[d][tx] = xn[d], sNd[3 + d][tx] = cn[d], sNd[6 + d][tx] = nv3[d];
+        sNd[9][tx] = an;
+        sNKind[tx] = kindn;
+    }
     if (ty == 0) {
         double xk[3] = {0, 0, 0}, ck[3] = {0, 0, 0}, nk[3] = {0, 0, 0}, ak = 0;
         int kindk = 0;
@@ -238,6 +256,7 @@ __global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView 
     }
     __syncthreads();
     const volatile double(*vK)[32] = sKd;
+    const volatile double(*vN)[32] = sNd;
     const FdParams* fd = FINITE ? fdp + f : nullptr;
     const typename Out::Tile* T1 = FINITE ? tiles + (size_t)f * (Out::kT1 + Out::kT2) : nullptr;
     const typename Out::Tile* T2 = FINITE ? T1 + Out::kT1 : nullptr;
@@ -248,25 +267,23 @@ __global__ void __launch_bounds__(256, Out::kF32 ? 3 : 2) k_assemble(PanelsView 
         bool live = k < N && n < N && (kb != nb || k <= n);
         if (!live) continue;
         // cn, nn3, an: panel g n (the source of entry (k, g n)); xn: the field point of row n
-        double xn[3], cn[3], nn3[3];
-        const int gn = g * N + n;
-        for (int d = 0; d < 3; d++) {
-            cn[d] = pv.at(P_C + d, gn);
-            nn3[d] = pv.at(P_N + d, gn);
-            xn[d] = SECT ? pv.at(P_C + d, n) : cn[d];
-        }
-        double an = pv.at(P_AREA, gn);
-        int kindn = pv.kind[n];
         // R without contraction: the finite-depth kernel switches form at R = h/2 exactly
         const double xk[3] = {vK[0][tx], vK[1][tx], vK[2][tx]};
-        double dx = xk[0] - cn[0], dy = xk[1] - cn[1];
-        double R = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+        double R, zn;
+        {
+            const double dx = xk[0] - vN[3][nl], dy = xk[1] - vN[4][nl];
+            R = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+            zn = vN[5][nl];
+        }
         Kern w;
         if (FINITE) {
-            w = finite_kernel<Out::kF32>(*fd, T1, T2, R, xk[2], cn[2], fp + k, fp + n, Nf);
+            w = finite_kernel<Out::kF32>(*fd, T1, T2, R, xk[2], zn, fp + k, fp + n, Nf);
         } else {
-            w = pair_kernel_inf<Out::kF32>(K, R, xk[2], cn[2]);
+            w = pair_kernel_inf<Out::kF32>(K, R, xk[2], zn);
         }
+        const double xn[3] = {vN[0][nl], vN[1][nl], vN[2][nl]}, cn[3] = {vN[3][nl], vN[4][nl], vN[5][nl]};
+        const double nn3[3] = {vN[6][nl], vN[7][nl], vN[8][nl]}, an = vN[9][nl];
+        const int kindn = sNKind[nl];
         // entry (k, n): the field point x_k against panel g n
         size_t o1 = (size_t)k + (size_t)n * N;
         double2 s1, d1;
