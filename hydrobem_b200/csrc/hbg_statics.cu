@@ -516,9 +516,13 @@ __global__ void __launch_bounds__(256, 2) k_statics(PanelsView pv, double depth,
     const int N = pv.N, Nr = pv.rows ? pv.nrows : N / pv.G;
     int k = blockIdx.x * 32 + threadIdx.x;
     int j = blockIdx.y * 8 + threadIdx.y;
+    // the panel of each warp (36 values every lane of the warp reads) in shared memory rather than in
+    // 72 registers of every lane
+    __shared__ PanelRegs sp[8];
+    if (threadIdx.x == 0 && j < N) load_panel(pv, j, sp[threadIdx.y]);
+    __syncthreads();
     if (k >= Nr || j >= N) return;
-    PanelRegs p;
-    load_panel(pv, j, p);
+    const PanelRegs& p = sp[threadIdx.y];
     double x[3];
     for (int d = 0; d < 3; d++) x[d] = pv.rows ? pv.rows[3 * k + d] : pv.at(P_C + d, k);
     double xb[3] = {x[0], x[1], -x[2]};
