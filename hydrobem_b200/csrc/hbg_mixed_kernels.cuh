@@ -861,12 +861,12 @@ __global__ void __launch_bounds__(GV_THREADS) k_cgemv_tma(const __grid_constant_
             const double mr = sMr[j * GV_ROWS + t], mi = sMi[j * GV_ROWS + t];
             const double nr = sMr[j * GV_ROWS + t + GV_WORKERS], ni = sMi[j * GV_ROWS + t + GV_WORKERS];
 #pragma unroll
-            for (int c = 0; c < NR; c++) {
+            for (int c = 0; c < NR; c++) {  // four fused multiply-adds a row (the pipe's limit)
                 const double2 v = sx[c * GV_COLS + j];
-                acc[c].x += mr * v.x - mi * v.y;
-                acc[c].y += mr * v.y + mi * v.x;
-                acd[c].x += nr * v.x - ni * v.y;
-                acd[c].y += nr * v.y + ni * v.x;
+                acc[c].x = fma(-mi, v.y, fma(mr, v.x, acc[c].x));
+                acc[c].y = fma(mi, v.x, fma(mr, v.y, acc[c].y));
+                acd[c].x = fma(-ni, v.y, fma(nr, v.x, acd[c].x));
+                acd[c].y = fma(ni, v.x, fma(nr, v.y, acd[c].y));
             }
         }
         __syncwarp();
